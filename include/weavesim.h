@@ -1,0 +1,257 @@
+/* weavesim.h — C ABI of the B200 dynamic-relaxation solver for woven (Kagome) timber gridshells.
+ *
+ * Drop-in boundary for the solver API of weave-sim's web/js solvers:
+ *   scene (laths, crossings, supports, material) -> relax -> node positions, segment frames, crossing slide
+ *   coordinates and stick/slip states.
+ * Every entry point is extern "C", takes plain pointers and sizes, never throws, and returns an int status
+ * (WS_OK = 0, < 0 on error; ws_last_error() gives the message of the last failure on the calling thread).
+ * Citations are file:line in the reference project (uwenji/weave-sim).
+ */
+#ifndef WEAVESIM_H
+#define WEAVESIM_H
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------------------------------ status codes */
+#define WS_OK 0
+#define WS_ERR_ARG -1        /* malformed argument or model (GpuSolver throws Error: web/js/solver_gpu.js:70) */
+#define WS_ERR_CUDA -2       /* a CUDA call failed */
+#define WS_ERR_NOMEM -3      /* device memory budget exhausted (admission refused) */
+#define WS_ERR_STATE -4      /* call not valid in the current state (e.g. changed clamps: solver_gpu.js:325) */
+#define WS_ERR_NODEV -5      /* no CUDA device: the library has no CPU fallback */
+
+/* per-instance status in ws_control.status */
+#define WS_RUNNING 0
+#define WS_CONVERGED 1
+#define WS_MAX_ITER 2
+#define WS_NONFINITE 3
+
+/* precision of a solver context (one template instantiation of every kernel) */
+#define WS_PREC_F64 0        /* FP64 everywhere */
+#define WS_PREC_MIXED 1      /* FP32 element math, two-float positions/frames, FP64 strain / relative rotation /
+                                contact gap, slide coordinates and reductions */
+#define WS_PREC_F32 2        /* naive FP32 everywhere */
+
+/* execution form */
+#define WS_FORM_CTA 0        /* persistent fused kernel, one thread block per instance (batched) */
+#define WS_FORM_GRID 1       /* persistent fused kernel, one instance over a cooperative grid (large instance) */
+#define WS_FORM_PLAIN 2      /* one kernel per phase per iteration, one instance (the plain GPU form) */
+
+/* ------------------------------------------------------------------------------------------------ parameters */
+/* Solver and contact parameters that the DR step reads.  Defaults: params.js:8-23 (SOLVER, CONTACT).
+ * Units are the model's (these bindings use SI: m, N, Pa). */
+typedef struct ws_params {
+  double mass_scale;      /* SOLVER.mass_scale 1.5 */
+  double damping;         /* SOLVER.damping 1.0 */
+  double tol;             /* SOLVER.tol 1e-4 (relative residual, solver_cpu.js:829-837) */
+  int32_t kinetic_damping;/* SOLVER.kinetic_damping 1 */
+  int32_t warmup_iter;    /* SOLVER.warmup_iter 300 */
+  int32_t max_iter;       /* SOLVER.max_iter 5000 */
+  int32_t contacts;       /* CpuSolver {contacts}: 1 = crossings active (solver_cpu.js:662,685) */
+  double strength;        /* CONTACT.strength: normal penalty [force/length] */
+  double stick_strength;  /* CONTACT.stick_strength: stick spring [force/length] */
+  double torsion_factor;  /* CONTACT.torsion_factor 1.0 */
+  double epsilon;         /* CONTACT.epsilon: slide step limit per iteration [length] */
+  int32_t ramp_iter;      /* CONTACT.ramp_iter 1500 */
+  int32_t disp_ramp_iter; /* prescribed support motion: anchored translations reach ws_model.anchor_target after this
+                             many iterations, linearly (0: at the first iteration).  An extension: the reference's
+                             anchors hold the position they have (solver_cpu.js:764,781). */
+  double slip_rate;       /* CONTACT.slip_rate 1.0 */
+} ws_params;
+
+/* The model of one instance: the flat state of buildState (web/js/model.js:10-75), the section stiffness per segment
+ * (strandStiffness, model.js:236-252), the loads (Loads, model.js:191-231), the resolved anchors (anchorMasks /
+ * Anchors, model.js:150-189) and the crossings (PolylineContact constructor, solver_cpu.js:62-96), before the goals
+ * (masses, inertias, clamp joints) and the contact initialisation, which every consumer builds itself. */
+typedef struct ws_model {
+  int32_t n, m, p, n_strands, K;
+  int32_t pad0;
+  const double *X;            /* [3n] current positions */
+  const double *X0;           /* [3n] displacement origin */
+  const double *Q;            /* [4m] segment frames (w, x, y, z); columns of R = [X width | Y normal | Z tangent] */
+  const double *l0;           /* [m] rest lengths */
+  const int32_t *seg_i0;      /* [m] first node of segment */
+  const int32_t *seg_i1;      /* [m] second node of segment */
+  const int32_t *seg_offset;  /* [n_strands+1] first segment of every strand */
+  const int32_t *joint_seg0;  /* [p] segment a of joint */
+  const int32_t *joint_seg1;  /* [p] segment b of joint */
+  const double *joint_len;    /* [p] Voronoi length l̄ */
+  const double *omega0;       /* [3p] rest curvature Ω0 (NULL: zeros) */
+  const double *EA, *EIx, *EIy, *GJ, *GA;   /* [m] section stiffness */
+  const double *load_const;   /* [3n] constant loads (self-weight, UDL, world point loads) */
+  int32_t n_local_loads;
+  int32_t n_anchors;
+  const int32_t *local_load_node;  /* [n_local_loads] */
+  const double *local_load_F;      /* [3 n_local_loads] in the node frame */
+  const int32_t *anchor_node;      /* [n_anchors] in resolution order */
+  const uint8_t *anchor_mask;      /* [n_anchors] bit k fixes DOF k of [X Y Z rX rY rZ] */
+  const double *anchor_target;     /* [3 n_anchors] target positions of the anchored nodes (NULL: they stay) */
+  const int32_t *cross_strand;     /* [2K] strand of side A, side B of every crossing (knots in sorted edge order) */
+  const double *cross_wk, *cross_hk;   /* [2K] section width / height of each side */
+  const double *cross_u;           /* [2K] slide coordinates (global u along the strand) */
+  const double *cross_nprev;       /* [3K] persistent contact normal */
+  const uint8_t *cross_enabled;    /* [K] */
+  const uint8_t *cross_locked;     /* [K] */
+  const double *cross_mu;          /* [K] Coulomb coefficient per crossing (the reference has one contact.mu) */
+  ws_params params;
+} ws_model;
+
+/* per-instance control block, written by the device after every iteration (the CT struct of the WebGPU solver,
+ * web/js/wgsl.js:154-172, read by GpuSolver.readControl, solver_gpu.js:374-386) */
+typedef struct ws_control {
+  int32_t iter;        /* DR iterations done */
+  int32_t status;      /* WS_RUNNING / WS_CONVERGED / WS_MAX_ITER / WS_NONFINITE */
+  int32_t rollbacks;   /* kinetic-damping resets since creation */
+  int32_t pending_zero;/* 1: the last iteration rolled back (velocities are zero, state is the previous one) */
+  double ke;           /* kinetic energy of the last iteration (0 after a reset) */
+  double ke_prev;      /* kinetic-energy peak tracker (CpuSolver.kePrev) */
+  double residual;     /* max(force part, torque part); +inf during the warm-up */
+  double res_force, res_torque, fref;
+  double e_stretch, e_shear, e_bend, e_twist, e_contact;
+} ws_control;
+
+/* ------------------------------------------------------------------------------------------------ errors */
+/* copies the message of the last failing call on this thread into buf (always NUL-terminated); returns its length */
+int ws_last_error(char *buf, size_t n);
+/* number of visible CUDA devices (0 when there is none) */
+int ws_device_count(void);
+
+/* ------------------------------------------------------------------------------------------------ scenes */
+/* Synthetic Kagome gridshell on a hexagonal plan: a triangular lattice clipped to a hexagon of `side` triangle edges
+ * (the tri_lattice pattern of examples/make_meshes.py:13-29), traced into laths by buildTopology
+ * (web/js/topology.js:78-87), subdivided, pre-offset and framed (topology.js:214-345), and flattened by buildState
+ * (model.js:10-75).  Laths per family = 2·side; triangle edge a = family spacing·2/√3. */
+typedef struct ws_kagome_cfg {
+  int32_t side;              /* hexagon side in triangle edges (laths per family / 2) */
+  int32_t subdivisions;      /* WEAVE.subdivisions: segments between neighbouring knots */
+  double edge;               /* triangle edge a [m] */
+  double width, height;      /* lath section [m] */
+  double E, G, density;      /* material [Pa, Pa, kg/m^3] */
+  double mu;                 /* Coulomb coefficient (all crossings) */
+  double mu_lo, mu_hi;       /* if mu_hi > mu_lo: per-crossing mu ~ U(mu_lo, mu_hi) from the seed */
+  double inward;             /* radial inward displacement of the perimeter lath ends [m] (scales the plan) */
+  double lift;               /* support ends lifted 0..lift [m] by a smooth seeded field (0: none) */
+  double z_noise;            /* std. dev. of the seeded z-noise of every node [m] */
+  int32_t gravity;           /* 1: self-weight on */
+  uint32_t seed;             /* xoshiro128** seed (web/js/rng.js:9-27) */
+  ws_params params;
+} ws_kagome_cfg;
+
+typedef struct ws_scene ws_scene;   /* owns the arrays of one ws_model */
+
+/* defaults: params.js:8-23 converted to SI (strength 1e4 N/mm = 1e7 N/m, epsilon 15 mm) */
+void ws_params_default(ws_params *out);
+int ws_scene_kagome(const ws_kagome_cfg *cfg, ws_scene **out);
+/* Stand-alone laths with optional knots (topologyFromPolylines, topology.js:348-363; the test fixtures of
+ * web/tests/cases.mjs:10-28).  Strand s has node_count[s] points in `points`, optional per-node normals hints,
+ * knot_count[s] knot rows in `knot_rows`; knots pair frame (sa, ka) with (sb, kb).  Anchors by frame (s, k) and
+ * DOF mask; point loads by frame with a world (local = 0) or node-frame (local = 1) force. */
+typedef struct ws_polyline_cfg {
+  int32_t n_strands;
+  const int32_t *node_count;      /* [n_strands] */
+  const double *points;           /* [3 Σ node_count] */
+  const double *normals;          /* [3 Σ node_count] or NULL (hint (0, 0, 1)) */
+  const int32_t *knot_count;      /* [n_strands] or NULL (rows 0 and n-1) */
+  const int32_t *knot_rows;       /* [Σ knot_count] */
+  int32_t n_knots;
+  const int32_t *knots;           /* [4 n_knots] sa, ka, sb, kb */
+  double thickness;               /* pre-offset thickness (unused for stand-alone laths) */
+  int32_t n_anchors;
+  const int32_t *anchor_frames;   /* [2 n_anchors] */
+  const uint8_t *anchor_masks;    /* [n_anchors] */
+  int32_t n_loads;
+  const int32_t *load_frames;     /* [2 n_loads] */
+  const double *load_F;           /* [3 n_loads] */
+  const uint8_t *load_local;      /* [n_loads] */
+  double width, height, E, G, density;
+  double mu;
+  int32_t gravity;
+  ws_params params;
+} ws_polyline_cfg;
+int ws_scene_polylines(const ws_polyline_cfg *cfg, ws_scene **out);
+/* the model view of a scene (pointers stay valid until ws_scene_free) */
+const ws_model *ws_scene_model(const ws_scene *s);
+/* per-strand node offsets [n_strands+1] and the span of the plan (largest extent of X0 in x or y) */
+const int32_t *ws_scene_node_offset(const ws_scene *s);
+double ws_scene_span(const ws_scene *s);
+void ws_scene_free(ws_scene *s);
+
+/* The goals the device will use for a model, built on the host (no GPU needed): node masses [n], static frame stiffness
+ * per body axis [3m], slide coordinates and contact normals after the contact initialisation [2K], [3K], the torque
+ * residual's reference length (CpuSolver._buildGoals, solver_cpu.js:670-710; PolylineContact.initialize,
+ * solver_cpu.js:99-139).  Any output pointer may be NULL. */
+int ws_model_goals(const ws_model *model, double *mass, double *k_rot_static, double *u, double *nprev, double *l_ref);
+
+/* ------------------------------------------------------------------------------------------------ solver */
+typedef struct ws_ctx ws_ctx;
+
+typedef struct ws_opts {
+  int32_t precision;    /* WS_PREC_* */
+  int32_t form;         /* WS_FORM_* */
+  int32_t threads;      /* threads per block (0: autotuned) */
+  int32_t device;       /* CUDA device ordinal */
+  uint64_t budget_bytes;/* device memory this context may take (0: no limit) */
+  int32_t history;      /* reserved */
+  int32_t pad0;
+} ws_opts;
+
+/* Builds the goals of every instance on the host (masses, inertias, clamps: CpuSolver._buildGoals,
+ * solver_cpu.js:670-710; contact initialisation: PolylineContact.initialize, solver_cpu.js:99-139) and uploads the
+ * batch.  Replaces `new GpuSolver(device, models, opts)` (solver_gpu.js:65-130); unlike it, the instances need not
+ * share one topology. */
+int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts *opts, ws_ctx **out);
+/* Runs up to n_iter DR iterations (CpuSolver.step, solver_cpu.js:737-841) on every instance whose mask byte is non-zero
+ * (NULL: all), each stopping at its own convergence; the control blocks of all instances go to ctl[n_instances]
+ * (NULL: not read).  Replaces GpuSolver.step (solver_gpu.js:338-361).  Asynchronous on the context's stream unless
+ * ctl is given. */
+int ws_step(ws_ctx *ctx, int32_t n_iter, const uint8_t *instance_mask, ws_control *ctl);
+int ws_read_control(ws_ctx *ctx, ws_control *ctl);
+/* State of one instance, host buffers sized by its model (any pointer may be NULL).  Replaces GpuSolver.download
+ * (solver_gpu.js:431-503). */
+typedef struct ws_state_out {
+  double *X;       /* [3n] */
+  double *Q;       /* [4m] */
+  double *V;       /* [3n] */
+  double *W;       /* [3m] body angular velocities */
+  double *u;       /* [2K] */
+  double *nprev;   /* [3K] */
+  double *slip;    /* [K] accumulated slip */
+  uint8_t *stuck;  /* [K] */
+  uint8_t *state;  /* [K] 1 = slipping in the last iteration */
+  double *Fn;      /* [K] */
+  double *Ft;      /* [K] */
+  double *gap;     /* [K] */
+  double *N;       /* [m] axial force */
+  double *Vsh;     /* [2m] shear forces */
+  double *M;       /* [3p] joint moments */
+  double *reactions; /* [3n] */
+} ws_state_out;
+int ws_download(ws_ctx *ctx, int32_t instance, ws_state_out *out);
+/* Uploads positions and frames (and zeroes velocities) of one instance from host buffers: a warm start from a state the
+ * caller holds (GpuSolver.upload, solver_gpu.js:189-198).  X [3n], Q [4m]; u [2K] may be NULL (kept). */
+int ws_upload_state(ws_ctx *ctx, int32_t instance, const double *X, const double *Q, const double *u);
+/* Warm start with new parameters (rebuildGoals + GpuSolver.updateParams, solver_cpu.js:719-732,
+ * solver_gpu.js:323-333): stiffness, loads, contact parameters and per-crossing mu of `model` replace the
+ * instance's; positions, frames, contact state stay on the device; masses and inertias are rebuilt from the current
+ * state; the kinetic-energy peak and the convergence flag are reset.  Anchored nodes move to model->X where their
+ * translation is fixed (prescribed displacement).  The topology must be the instance's. */
+int ws_set_params(ws_ctx *ctx, int32_t instance, const ws_model *model);
+/* current geometry becomes the displacement origin; slip counters restart (CpuSolver.internalize, solver_cpu.js:868;
+ * GpuSolver.internalize, solver_gpu.js:507-520) */
+int ws_internalize(ws_ctx *ctx, int32_t instance);
+/* CUDA stream of the context (cudaStream_t) */
+void *ws_stream(ws_ctx *ctx);
+/* device bytes held by the context */
+uint64_t ws_device_bytes(const ws_ctx *ctx);
+/* GPU time of the last ws_step (ms, CUDA events on the context's stream) and the number of kernel launches it made */
+int ws_last_step_stats(const ws_ctx *ctx, double *ms, int64_t *launches);
+int ws_destroy(ws_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

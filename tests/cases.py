@@ -1,0 +1,88 @@
+"""Test scenes: the constructions of the reference's web/tests/cases.mjs:10-66 (mm, N) and the gridshell workloads.
+
+* straight(L, nseg)            cases.mjs:10-13
+* cantilever(nseg, dir)        rod_bench.mjs:27-36 (60×30 mm, E 1e4 N/mm², G 625, tip load 10 N, clamped at frame (0,0))
+* crossing(load, pull, ...)    cases.mjs:14-28 (two 1000 mm laths, 10 segments, h = 30, B free in x)
+* case_by_name(name)           cases.mjs:29-50 (cantilever, cantilever_edge, torsion, cross_press/stick/slip/locked)
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+import weavesim_b200 as ws
+
+E_MM, G_MM, KAPPA = 1e4, 625.0, 5.0 / 6.0
+
+
+def mm_params(**over):
+    """the reference's defaults in its own units (params.js:8-23: strength 1e4 N/mm, epsilon 15 mm)"""
+    kw = dict(strength=1e4, stick_strength=1e4, epsilon=15.0)
+    kw.update(over)
+    return ws.default_params(**kw)
+
+
+def straight(L=1000.0, nseg=10, normals=None, anchors=(), loads=(), **kw):
+    pts = np.array([[L * i / nseg, 0.0, 0.0] for i in range(nseg + 1)])
+    return ws.polylines([pts], normals=None if normals is None else [normals], anchors=anchors, loads=loads,
+                        E=E_MM, G=G_MM, **kw)
+
+
+def cantilever(nseg=10, direction=2, P=10.0, tol=1e-10, max_iter=600000, w=60.0, h=30.0, L=1000.0):
+    md = straight(L, nseg, anchors=[((0, 0), ws.mask(1, 1, 1, 1, 1, 1))], width=w, height=h,
+                  params=mm_params(tol=tol, max_iter=max_iter, contacts=0))
+    tip = int(np.argmax(md.X[0::3]))
+    md.load_const[3 * tip + direction] -= P
+    md.tip = tip
+    return md
+
+
+def timoshenko(direction=2, P=10.0, L=1000.0, w=60.0, h=30.0):
+    I = w * h ** 3 / 12 if direction == 2 else h * w ** 3 / 12
+    return P * L ** 3 / (3 * E_MM * I) + P * L / (KAPPA * G_MM * w * h)
+
+
+def crossing(load=-50.0, pull=0.0, mu=0.35, freeB=True, nseg=10, L=1000.0, h=30.0, locked=False, **prm):
+    P = np.array([[-L / 2 + L * i / nseg, 0.0, 0.0] for i in range(nseg + 1)])
+    PB = np.array([[0.0, -L / 2 + L * i / nseg, h] for i in range(nseg + 1)])
+    mid = nseg // 2
+    fixA = ws.mask(1, 1, 1, 0, 0, 1)
+    fixB = ws.mask(0, 1, 1, 0, 0, 1) if freeB else fixA
+    prm.setdefault("max_iter", 20000)
+    md = ws.polylines([P, PB], knot_rows=[[0, mid, nseg], [0, mid, nseg]], knots=[((0, 1), (1, 1))],
+                      anchors=[((0, 0), fixA), ((0, 2), fixA), ((1, 0), fixB), ((1, 2), fixB)],
+                      loads=[((1, 1), (pull, 0.0, load), False)], mu=mu, E=E_MM, G=G_MM, params=mm_params(**prm))
+    if locked:
+        md.cross_locked[:] = 1
+    return md
+
+
+def torsion(nseg=10, L=1000.0):
+    normals = [[0.0, -math.sin(math.pi / 2 * i / nseg), math.cos(math.pi / 2 * i / nseg)] for i in range(nseg + 1)]
+    md = straight(L, nseg, normals=normals, anchors=[((0, 0), ws.mask(1, 1, 1, 1, 1, 1)), ((0, 1), ws.mask(1, 1, 1, 0, 0, 1))],
+                  params=mm_params(contacts=0, max_iter=20000))
+    return md
+
+
+def case_by_name(name):
+    if name in ("cantilever", "cantilever_edge"):
+        return cantilever(10, 2 if name == "cantilever" else 1, tol=1e-4, max_iter=20000)
+    if name == "torsion":
+        return torsion()
+    pulls = {"cross_press": 0.0, "cross_stick": 5.0, "cross_slip": 12.0, "cross_locked": 12.0}
+    if name in pulls:
+        return crossing(-50.0, pulls[name], locked=name == "cross_locked")
+    raise KeyError(name)
+
+
+def max_rel_disp_error(Xa, Xb, X0):
+    """largest |ΔX| against the largest displacement (selftest.html:53-56), floored at 1e-9 × model size"""
+    d = np.abs(Xa - X0).max()
+    s = np.abs(X0).max()
+    return np.abs(Xa - Xb).max() / max(d, 1e-9 * s, 1e-300)
+
+
+def max_node_err_span(Xa, Xb, span):
+    """max over nodes of |X_a − X_b|₂ / span"""
+    return float(np.linalg.norm((Xa - Xb).reshape(-1, 3), axis=1).max() / span)

@@ -1,0 +1,145 @@
+"""The oracle (f64 CPU restatement of web/js/solver_cpu.js) pinned by the reference's own known-answer tests.
+
+No golden vectors of this path ship with the reference (web/tests/ref_out is absent and no JS runtime exists here), so
+the oracle is pinned by the checks the reference's test scripts print and its README publishes:
+
+* rod forces and torques are the gradient of the rod energy (web/tests/rod_check.mjs:1-46, PASS below 1e-5)
+* clamped cantilever against Timoshenko: 0.50 / 0.12 / 0.03 % at 10 / 20 / 40 segments (web/README.md:72,
+  web/tests/rod_bench.mjs:27-37)
+* short deep cantilever (30 % shear): 0.09 % (web/README.md:72, rod_bench.mjs:38-46)
+* crossing cases cross_press / stick / slip / locked (web/tests/cases.mjs:14-50, rod_contact_check.mjs): by the
+  symmetry of two identical laths the crossing carries half the 50 N load; 5 N of pull sticks, 12 N exceeds μ·Fn and
+  slips (selftest.html:39-43), the locked crossing holds 12 N.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import cases
+
+
+def _qmul(a, b):
+    aw, ax, ay, az = a
+    bw, bx, by, bz = b
+    return np.array([aw * bw - ax * bx - ay * by - az * bz, aw * bx + ax * bw + ay * bz - az * by,
+                     aw * by - ax * bz + ay * bw + az * bx, aw * bz + ax * by - ay * bx + az * bw])
+
+
+def _qexp(v):
+    a = np.linalg.norm(v)
+    s = math.sin(0.5 * a) / a if a > 1e-12 else 0.5
+    return np.array([math.cos(0.5 * a), v[0] * s, v[1] * s, v[2] * s])
+
+
+def _rel_rot(qa, qb):
+    q = _qmul(np.array([qa[0], -qa[1], -qa[2], -qa[3]]), qb)
+    if q[0] < 0:
+        q = -q
+    s = np.linalg.norm(q[1:])
+    th = 2 * math.atan2(s, q[0])
+    f = th / s if s > 1e-12 else 2 / max(q[0], 1e-12)
+    return f * q[1:]
+
+
+def test_rod_forces_are_energy_gradient(ws, oracle_mod):
+    """rod_check.mjs: a bent, twisted, sheared strand with rest curvature, an anisotropic section and clamp joints;
+    forces and torques against central differences of the energy (relative error < 1e-5)."""
+    rng = np.random.default_rng(11)
+    r = lambda: rng.uniform(-1, 1)
+    md = cases.straight(1000.0, 8, params=cases.mm_params(contacts=0))
+    n, m, p = md.n, md.m, md.p
+    md.EA[:] = 1e4 * 1800
+    md.EIx[:] = 1e4 * 1.35e5
+    md.EIy[:] = 1e4 * 5.4e5
+    md.GJ[:] = 625 * 3.7e5
+    md.GA[:] = 5 / 6 * 625 * 1800
+    X = md.X.reshape(-1, 3)
+    for i in range(n):
+        X[i, 1] += 40 * math.sin(i)
+        X[i, 2] += 25 * math.cos(1.3 * i)
+    Q = md.Q.reshape(-1, 4)
+
+    def rot(Qa, j, v):
+        q = _qmul(_qexp(np.asarray(v)), Qa[j])
+        Qa[j] = q / np.linalg.norm(q)
+
+    for j in range(m):
+        rot(Q, j, [0.3 * r(), 0.3 * r(), 0.8 * r()])
+    # activation 0.4: the rest curvature keeps 60 % of the as-built one (CosseratRod constructor, rod_cosserat.js:58-66)
+    om = np.zeros(3 * p)
+    for j in range(p):
+        om[3 * j:3 * j + 3] = 0.6 * _rel_rot(Q[md.joint_seg0[j]], Q[md.joint_seg1[j]]) / md.joint_len[j]
+    md.omega0 = om
+    o = oracle_mod.Oracle(md)
+    o.set_clamps([(0, 0, 7), (n - 1, m - 1, 5)])
+    Xd = md.X.copy() + np.array([5 * r() for _ in range(3 * n)])
+    Qd = md.Q.reshape(-1, 4).copy()
+    for j in range(m):
+        rot(Qd, j, [0.2 * r(), 0.2 * r(), 0.5 * r()])
+    Qd = Qd.ravel()
+    _, F, T = o.rod_eval(Xd, Qd)
+    h = 1e-4
+    ef = 0.0
+    for i in range(3 * n):
+        Xp, Xm = Xd.copy(), Xd.copy()
+        Xp[i] += h
+        Xm[i] -= h
+        fd = -(o.rod_eval(Xp, Qd)[0] - o.rod_eval(Xm, Qd)[0]) / (2 * h)
+        ef = max(ef, abs(fd - F[i]))
+    hr = 1e-6
+    et = 0.0
+    for j in range(m):
+        for k in range(3):
+            v = [0.0, 0.0, 0.0]
+            v[k] = hr
+            Qp = Qd.reshape(-1, 4).copy()
+            rot(Qp, j, v)
+            v[k] = -hr
+            Qm = Qd.reshape(-1, 4).copy()
+            rot(Qm, j, v)
+            fd = -(o.rod_eval(Xd, Qp.ravel())[0] - o.rod_eval(Xd, Qm.ravel())[0]) / (2 * hr)
+            et = max(et, abs(fd - T[3 * j + k]))
+    assert ef / np.abs(F).max() < 1e-5
+    assert et / np.abs(T).max() < 1e-5
+
+
+def _solve(o, max_iter, chunk=5000):
+    it = 0
+    while it < max_iter:
+        if o.step(chunk):
+            break
+        it += chunk
+    return o.view()
+
+
+@pytest.mark.parametrize("nseg,direction,published", [(10, 2, 0.50), (20, 2, 0.12), (40, 2, 0.03), (10, 1, 0.50), (20, 1, 0.12)])
+def test_cantilever_against_timoshenko(oracle_mod, nseg, direction, published):
+    md = cases.cantilever(nseg, direction, max_iter=600000)
+    v = _solve(oracle_mod.Oracle(md), 600000 if nseg < 40 else 200000)
+    d = -v["X"][3 * md.tip + direction]
+    err = 100 * (d / cases.timoshenko(direction) - 1)
+    assert abs(err - published) < 0.01, err
+
+
+def test_short_deep_beam(oracle_mod):
+    md = cases.cantilever(20, 1, P=100.0, L=200.0, max_iter=600000)
+    v = _solve(oracle_mod.Oracle(md), 600000)
+    d = -v["X"][3 * md.tip + 1]
+    err = 100 * (d / cases.timoshenko(1, P=100.0, L=200.0) - 1)
+    assert abs(err - 0.09) < 0.01, err
+
+
+def test_crossing_cases(oracle_mod):
+    o = oracle_mod.Oracle(cases.crossing(-50.0, 0.0))
+    v = o.run(6000)
+    assert v["converged"] and abs(v["Fn"][0] - 25.0) < 0.25 and v["slip"][0] == 0
+    o = oracle_mod.Oracle(cases.crossing(-50.0, 5.0))
+    v = o.run(6000)
+    assert v["converged"] and v["state"][0] == 0 and abs(v["Ft"][0] - 5.0) < 0.05
+    o = oracle_mod.Oracle(cases.crossing(-50.0, 12.0))
+    v = o.run(6000)
+    assert not v["converged"] and v["state"][0] == 1 and abs(v["Ft"][0] - 0.35 * v["Fn"][0]) < 1e-6 * v["Fn"][0]
+    o = oracle_mod.Oracle(cases.crossing(-50.0, 12.0, locked=True))
+    v = o.run(6000)
+    assert v["converged"] and v["slip"][0] == 0 and abs(v["Ft"][0] - 12.0) < 0.1

@@ -1,0 +1,646 @@
+// C entry points of the solver: a context owns a batch of instances packed into one device arena, the host goals of
+// every instance (for warm starts and downloads), a CUDA stream and the graph of the plain form.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/weavesim.h"
+#include "dr_kernels.hpp"
+#include "errors.hpp"
+#include "host_goals.hpp"
+
+using namespace wsb;
+
+namespace {
+
+struct CudaError : std::runtime_error { using std::runtime_error::runtime_error; };
+#define CK(x)                                                                                                \
+  do {                                                                                                       \
+    cudaError_t e_ = (x);                                                                                    \
+    if (e_ != cudaSuccess) throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_));                 \
+  } while (0)
+
+// element counts of the whole batch
+struct Sizes { int n = 0, m = 0, p = 0, c = 0, k = 0, s = 0; };
+
+// carves typed arrays out of one allocation (base == nullptr: only counts the bytes)
+struct Carver {
+  char *base;
+  size_t off = 0;
+  template <class T> T *take(size_t count) {
+    off = (off + 255) & ~size_t(255);
+    T *p = base ? reinterpret_cast<T *>(base + off) : nullptr;
+    off += sizeof(T) * std::max<size_t>(count, 1);
+    return p;
+  }
+};
+
+template <int P>
+void layout(Dev<P> &d, Carver &cv, const Sizes &z) {
+  using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A; using U = typename Dev<P>::U; using S = typename Dev<P>::S;
+  d.ntot = z.n; d.mtot = z.m; d.ptot = z.p; d.ctot = z.c; d.ktot = z.k; d.stot = z.s;
+  const size_t n = z.n, m = z.m, p = z.p, c = z.c, k = z.k, s = z.s;
+  d.X = cv.take<S>(6 * n); d.Xlo = PrecT<P>::TWO ? cv.take<S>(6 * n) : nullptr;
+  d.V = cv.take<R>(3 * n); d.mass = cv.take<R>(n); d.lc = cv.take<R>(3 * n); d.ll = cv.take<R>(3 * n);
+  d.nflag = cv.take<uint8_t>(n); d.nsOut = cv.take<int>(n); d.nsIn = cv.take<int>(n); d.anc = cv.take<int>(n);
+  d.ancStart = cv.take<W>(3 * n); d.ancDelta = cv.take<W>(3 * n); d.react = cv.take<R>(3 * n);
+  d.Q = cv.take<S>(8 * m); d.Qlo = PrecT<P>::TWO ? cv.take<S>(8 * m) : nullptr;
+  d.Wr = cv.take<R>(3 * m);
+  d.segI0 = cv.take<int>(m); d.segI1 = cv.take<int>(m); d.jA = cv.take<int>(m); d.jB = cv.take<int>(m);
+  d.cl0 = cv.take<int>(m); d.cl1 = cv.take<int>(m); d.segStrand = cv.take<int>(m); d.segLocal = cv.take<int>(m);
+  d.l0 = cv.take<R>(m); d.EA = cv.take<R>(m); d.GA = cv.take<R>(m); d.krs = cv.take<R>(3 * m);
+  d.nF = cv.take<R>(3 * m); d.en = cv.take<R>(3 * m); d.Nax = cv.take<R>(m); d.Vsh = cv.take<R>(2 * m);
+  d.rngLo = cv.take<int>(2 * m); d.rngHi = cv.take<int>(2 * m);
+  d.jS0 = cv.take<int>(p); d.jS1 = cv.take<int>(p); d.jLen = cv.take<R>(p); d.EIx = cv.take<R>(p); d.EIy = cv.take<R>(p);
+  d.GJ = cv.take<R>(p); d.om = cv.take<R>(3 * p); d.tau = cv.take<R>(3 * p); d.kd = cv.take<R>(3 * p); d.Mj = cv.take<R>(3 * p);
+  d.cSeg = cv.take<int>(c); d.cLen = cv.take<R>(c); d.cB = cv.take<R>(3 * c); d.cQ = cv.take<W>(4 * c);
+  d.tauC = cv.take<R>(3 * c); d.cM = cv.take<R>(2 * c);
+  d.cxSegOff = cv.take<int>(2 * k); d.cxNseg = cv.take<int>(2 * k); d.wk = cv.take<R>(2 * k); d.hk = cv.take<R>(2 * k);
+  d.cw = cv.take<R>(k); d.ch = cv.take<R>(k); d.mu = cv.take<R>(k); d.cflag = cv.take<uint8_t>(k);
+  d.u = cv.take<U>(2 * k); d.nPrev = cv.take<R>(3 * k); d.slip = cv.take<A>(k); d.stuck = cv.take<uint8_t>(k);
+  d.cstate = cv.take<uint8_t>(k); d.Fn = cv.take<R>(k); d.Ft = cv.take<R>(k); d.gap = cv.take<R>(k);
+  d.sSeg = cv.take<int>(2 * k); d.sT = cv.take<R>(2 * k); d.kth = cv.take<R>(k); d.sF = cv.take<R>(6 * k); d.sTq = cv.take<R>(6 * k);
+  d.stSideOff = cv.take<int>(s); d.stSideCnt = cv.take<int>(s); d.ord = cv.take<int>(4 * k); d.ordSeg = cv.take<int>(4 * k);
+}
+
+// host -> device with conversion
+template <class T, class V>
+void put(T *dst, const V *src, size_t count, cudaStream_t st) {
+  if (!count) return;
+  std::vector<T> tmp(count);
+  for (size_t i = 0; i < count; i++) tmp[i] = T(src[i]);
+  CK(cudaMemcpyAsync(dst, tmp.data(), count * sizeof(T), cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
+}
+template <class T>
+void getv(std::vector<double> &out, const T *src, size_t count, cudaStream_t st) {
+  std::vector<T> tmp(count);
+  if (count) CK(cudaMemcpyAsync(tmp.data(), src, count * sizeof(T), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  out.resize(count);
+  for (size_t i = 0; i < count; i++) out[i] = double(tmp[i]);
+}
+
+}  // namespace
+
+struct ws_ctx {
+  int prec = 0, form = 0, threads = 0, device = 0;
+  cudaStream_t st = nullptr;
+  std::vector<HostGoals> g;
+  std::vector<InstDesc> inst;
+  std::vector<int> order;
+  Sizes z;
+  char *arena = nullptr;
+  size_t bytes = 0;
+  Dev<PREC_F64> d64{};
+  Dev<PREC_MIXED> dmx{};
+  Dev<PREC_F32> d32{};
+  InstDesc *dInst = nullptr;
+  InstCtl *dCtl = nullptr;
+  int *dOrder = nullptr;
+  uint8_t *dMask = nullptr;
+  void *dPart = nullptr;
+  PlainShape shape{};
+  cudaGraphExec_t graph = nullptr;
+  int graphIters = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double lastMs = 0;
+  int64_t lastLaunches = 0;
+  std::vector<InstCtl> ctlHost;
+};
+
+namespace {
+
+template <int P> Dev<P> &devOf(ws_ctx *c);
+template <> Dev<PREC_F64> &devOf<PREC_F64>(ws_ctx *c) { return c->d64; }
+template <> Dev<PREC_MIXED> &devOf<PREC_MIXED>(ws_ctx *c) { return c->dmx; }
+template <> Dev<PREC_F32> &devOf<PREC_F32>(ws_ctx *c) { return c->d32; }
+
+InstDesc describe(const HostGoals &g, const Sizes &off) {
+  InstDesc I{};
+  I.n0 = off.n; I.n = g.n; I.m0 = off.m; I.m = g.m; I.p0 = off.p; I.p = g.p; I.c0 = off.c; I.C = g.C;
+  I.k0 = off.k; I.K = g.K; I.s0 = off.s; I.S = g.S;
+  I.warmup = g.prm.warmup_iter; I.ramp_iter = std::max(g.prm.ramp_iter, 0); I.disp_ramp = std::max(g.prm.disp_ramp_iter, 0);
+  I.kd = g.prm.kinetic_damping ? 1 : 0; I.contacts = g.prm.contacts ? 1 : 0; I.max_iter = g.prm.max_iter > 0 ? g.prm.max_iter : 0x7fffffff;
+  I.ms = g.prm.mass_scale; I.damping = g.prm.damping; I.tol = g.prm.tol; I.strength = g.prm.strength; I.stick = g.prm.stick_strength;
+  I.tf = g.prm.torsion_factor; I.eps = g.prm.epsilon; I.slip_rate = g.prm.slip_rate; I.lRef = g.lRef; I.jLenMin = g.jLenMin;
+  return I;
+}
+
+// upload the goal arrays of instance b (everything a warm start may change)
+template <int P>
+void uploadGoals(ws_ctx *c, int b) {
+  Dev<P> &d = devOf<P>(c);
+  using R = typename Dev<P>::R; using W = typename Dev<P>::W;
+  const HostGoals &g = c->g[b];
+  const InstDesc &I = c->inst[b];
+  cudaStream_t st = c->st;
+  const size_t n = g.n, m = g.m, p = g.p, C = g.C, K = g.K;
+  put<R>(d.mass + I.n0, g.mass.data(), n, st);
+  for (int k = 0; k < 3; k++) {
+    std::vector<double> a(n), l(n);
+    for (size_t i = 0; i < n; i++) { a[i] = g.loadConst[3 * i + k]; l[i] = g.loadLocal[3 * i + k]; }
+    put<R>(d.lc + size_t(k) * d.ntot + I.n0, a.data(), n, st);
+    put<R>(d.ll + size_t(k) * d.ntot + I.n0, l.data(), n, st);
+  }
+  std::vector<uint8_t> fl(n);
+  for (size_t i = 0; i < n; i++)
+    fl[i] = (g.nodeFree[3 * i] ? 1 : 0) | (g.nodeFree[3 * i + 1] ? 2 : 0) | (g.nodeFree[3 * i + 2] ? 4 : 0) | (g.fixedAny[i] ? 8 : 0) |
+            (g.hasLocal[i] ? 16 : 0) | (g.ancIndex[i] >= 0 ? 32 : 0);
+  put<uint8_t>(d.nflag + I.n0, fl.data(), n, st);
+  // prescribed motion: slot s of this instance lives at the instance's node offset + s
+  std::vector<int> anc(n);
+  for (size_t i = 0; i < n; i++) anc[i] = g.ancIndex[i] >= 0 ? I.n0 + g.ancIndex[i] : -1;
+  put<int>(d.anc + I.n0, anc.data(), n, st);
+  const size_t ns = g.ancStart.size() / 3;
+  for (int k = 0; k < 3; k++) {
+    std::vector<double> a(ns), dl(ns);
+    for (size_t s = 0; s < ns; s++) { a[s] = g.ancStart[3 * s + k]; dl[s] = g.ancDelta[3 * s + k]; }
+    put<W>(d.ancStart + size_t(k) * d.ntot + I.n0, a.data(), ns, st);
+    put<W>(d.ancDelta + size_t(k) * d.ntot + I.n0, dl.data(), ns, st);
+  }
+  put<R>(d.EA + I.m0, g.EA.data(), m, st);
+  put<R>(d.GA + I.m0, g.GA.data(), m, st);
+  for (int k = 0; k < 3; k++) {
+    std::vector<double> a(m);
+    for (size_t j = 0; j < m; j++) a[j] = g.kRotStatic[3 * j + k];
+    put<R>(d.krs + size_t(k) * d.mtot + I.m0, a.data(), m, st);
+  }
+  put<R>(d.EIx + I.p0, g.EIx.data(), p, st);
+  put<R>(d.EIy + I.p0, g.EIy.data(), p, st);
+  put<R>(d.GJ + I.p0, g.GJ.data(), p, st);
+  for (int k = 0; k < 3; k++) {
+    std::vector<double> a(p);
+    for (size_t j = 0; j < p; j++) a[j] = g.omega0[3 * j + k];
+    put<R>(d.om + size_t(k) * d.ptot + I.p0, a.data(), p, st);
+  }
+  std::vector<int> cs(C);
+  for (size_t q = 0; q < C; q++) cs[q] = I.m0 + g.cSeg[q];
+  put<int>(d.cSeg + I.c0, cs.data(), C, st);
+  put<R>(d.cLen + I.c0, g.cLen.data(), C, st);
+  for (int k = 0; k < 3; k++) {
+    std::vector<double> a(C);
+    for (size_t q = 0; q < C; q++) a[q] = g.cB[3 * q + k];
+    put<R>(d.cB + size_t(k) * d.ctot + I.c0, a.data(), C, st);
+  }
+  for (int k = 0; k < 4; k++) {
+    std::vector<double> a(C);
+    for (size_t q = 0; q < C; q++) a[q] = g.cQ[4 * q + k];
+    put<W>(d.cQ + size_t(k) * d.ctot + I.c0, a.data(), C, st);
+  }
+  std::vector<int> c0(m), c1(m);
+  for (size_t j = 0; j < m; j++) { c0[j] = g.segClamp0[j] >= 0 ? I.c0 + g.segClamp0[j] : -1; c1[j] = g.segClamp1[j] >= 0 ? I.c0 + g.segClamp1[j] : -1; }
+  put<int>(d.cl0 + I.m0, c0.data(), m, st);
+  put<int>(d.cl1 + I.m0, c1.data(), m, st);
+  put<R>(d.mu + I.k0, g.mu.data(), K, st);
+  std::vector<uint8_t> cf(K);
+  for (size_t q = 0; q < K; q++) cf[q] = (g.enabled[q] ? 1 : 0) | (g.locked[q] ? 2 : 0);
+  put<uint8_t>(d.cflag + I.k0, cf.data(), K, st);
+}
+
+// upload the sorted side lists and segment slices of instance b into sorted-side buffer `buf`
+template <int P>
+void uploadOrder(ws_ctx *c, int b, int buf) {
+  Dev<P> &d = devOf<P>(c);
+  const HostGoals &g = c->g[b];
+  const InstDesc &I = c->inst[b];
+  const size_t K2 = 2 * size_t(d.ktot), K = g.K, m = g.m;
+  std::vector<int> ord(2 * K), lo(m), hi(m);
+  for (size_t q = 0; q < 2 * K; q++) ord[q] = 2 * I.k0 + g.ord[q];
+  for (size_t j = 0; j < m; j++) { lo[j] = 2 * I.k0 + g.rngLo[j]; hi[j] = 2 * I.k0 + g.rngHi[j]; }
+  put<int>(d.ord + buf * K2 + 2 * size_t(I.k0), ord.data(), 2 * K, c->st);
+  put<int>(d.ordSeg + buf * K2 + 2 * size_t(I.k0), g.ordSeg.data(), 2 * K, c->st);
+  put<int>(d.rngLo + size_t(buf) * d.mtot + I.m0, lo.data(), m, c->st);
+  put<int>(d.rngHi + size_t(buf) * d.mtot + I.m0, hi.data(), m, c->st);
+}
+
+// positions / frames of instance b into buffer `buf` (and its slide coordinates)
+template <int P>
+void uploadState(ws_ctx *c, int b, int buf, bool withU) {
+  Dev<P> &d = devOf<P>(c);
+  using R = typename Dev<P>::R; using W = typename Dev<P>::W; using S = typename Dev<P>::S; using U = typename Dev<P>::U;
+  const HostGoals &g = c->g[b];
+  const InstDesc &I = c->inst[b];
+  cudaStream_t st = c->st;
+  const size_t n = g.n, m = g.m, K = g.K;
+  for (int k = 0; k < 3; k++) {
+    std::vector<double> a(n);
+    for (size_t i = 0; i < n; i++) a[i] = g.X[3 * i + k];
+    std::vector<double> hi(n), lo(n);
+    for (size_t i = 0; i < n; i++) { hi[i] = double(S(W(a[i]))); lo[i] = double(S(W(a[i]) - W(S(W(a[i]))))); }
+    put<S>(d.X + size_t(buf * 3 + k) * d.ntot + I.n0, hi.data(), n, st);
+    if (PrecT<P>::TWO) put<S>(d.Xlo + size_t(buf * 3 + k) * d.ntot + I.n0, lo.data(), n, st);
+    std::vector<double> z(n, 0.0);
+    put<R>(d.V + size_t(k) * d.ntot + I.n0, z.data(), n, st);
+  }
+  for (int k = 0; k < 4; k++) {
+    std::vector<double> hi(m), lo(m);
+    for (size_t j = 0; j < m; j++) { const double a = g.Q[4 * j + k]; hi[j] = double(S(W(a))); lo[j] = double(S(W(a) - W(S(W(a))))); }
+    put<S>(d.Q + size_t(buf * 4 + k) * d.mtot + I.m0, hi.data(), m, st);
+    if (PrecT<P>::TWO) put<S>(d.Qlo + size_t(buf * 4 + k) * d.mtot + I.m0, lo.data(), m, st);
+  }
+  for (int k = 0; k < 3; k++) { std::vector<double> z(m, 0.0); put<R>(d.Wr + size_t(k) * d.mtot + I.m0, z.data(), m, st); }
+  if (withU && K) {
+    for (int side = 0; side < 2; side++) {
+      std::vector<double> a(K);
+      for (size_t q = 0; q < K; q++) a[q] = g.u[2 * q + side];
+      put<U>(d.u + size_t(side) * d.ktot + I.k0, a.data(), K, st);
+    }
+    for (int k = 0; k < 3; k++) {
+      std::vector<double> a(K);
+      for (size_t q = 0; q < K; q++) a[q] = g.nPrev[3 * q + k];
+      put<R>(d.nPrev + size_t(k) * d.ktot + I.k0, a.data(), K, st);
+    }
+  }
+}
+
+// the static arrays of instance b (topology, rest state, section constants)
+template <int P>
+void uploadStatic(ws_ctx *c, int b) {
+  Dev<P> &d = devOf<P>(c);
+  using R = typename Dev<P>::R;
+  const HostGoals &g = c->g[b];
+  const InstDesc &I = c->inst[b];
+  cudaStream_t st = c->st;
+  const size_t n = g.n, m = g.m, p = g.p, K = g.K, S = g.S;
+  auto shift = [](const std::vector<int> &v, int off) { std::vector<int> o(v.size()); for (size_t i = 0; i < v.size(); i++) o[i] = v[i] >= 0 ? v[i] + off : -1; return o; };
+  put<int>(d.nsOut + I.n0, shift(g.nodeSegOut, I.m0).data(), n, st);
+  put<int>(d.nsIn + I.n0, shift(g.nodeSegIn, I.m0).data(), n, st);
+  put<int>(d.segI0 + I.m0, shift(g.segI0, I.n0).data(), m, st);
+  put<int>(d.segI1 + I.m0, shift(g.segI1, I.n0).data(), m, st);
+  put<int>(d.jA + I.m0, shift(g.segJointA, I.p0).data(), m, st);
+  put<int>(d.jB + I.m0, shift(g.segJointB, I.p0).data(), m, st);
+  put<int>(d.segStrand + I.m0, shift(g.segStrand, I.s0).data(), m, st);
+  put<int>(d.segLocal + I.m0, g.segLocal.data(), m, st);
+  put<R>(d.l0 + I.m0, g.l0.data(), m, st);
+  put<int>(d.jS0 + I.p0, shift(g.jSeg0, I.m0).data(), p, st);
+  put<int>(d.jS1 + I.p0, shift(g.jSeg1, I.m0).data(), p, st);
+  put<R>(d.jLen + I.p0, g.jLen.data(), p, st);
+  for (int side = 0; side < 2; side++) {
+    std::vector<int> so(K), nsg(K);
+    std::vector<double> w(K), h(K);
+    for (size_t q = 0; q < K; q++) { so[q] = I.m0 + g.cxSegOff[2 * q + side]; nsg[q] = g.cxNseg[2 * q + side]; w[q] = g.wk[2 * q + side]; h[q] = g.hk[2 * q + side]; }
+    put<int>(d.cxSegOff + size_t(side) * d.ktot + I.k0, so.data(), K, st);
+    put<int>(d.cxNseg + size_t(side) * d.ktot + I.k0, nsg.data(), K, st);
+    put<R>(d.wk + size_t(side) * d.ktot + I.k0, w.data(), K, st);
+    put<R>(d.hk + size_t(side) * d.ktot + I.k0, h.data(), K, st);
+  }
+  put<R>(d.cw + I.k0, g.w.data(), K, st);
+  put<R>(d.ch + I.k0, g.h.data(), K, st);
+  std::vector<int> so(S), sc(S);
+  for (size_t s = 0; s < S; s++) { so[s] = 2 * I.k0 + g.strandSideOff[s]; sc[s] = g.strandSideCnt[s]; }
+  put<int>(d.stSideOff + I.s0, so.data(), S, st);
+  put<int>(d.stSideCnt + I.s0, sc.data(), S, st);
+  std::vector<uint8_t> one(K, 1);
+  put<uint8_t>(d.stuck + I.k0, one.data(), K, st);
+}
+
+template <int P>
+void uploadAll(ws_ctx *c) {
+  for (size_t b = 0; b < c->g.size(); b++) {
+    uploadStatic<P>(c, int(b));
+    uploadGoals<P>(c, int(b));
+    uploadState<P>(c, int(b), 0, true);
+    uploadState<P>(c, int(b), 1, false);
+    uploadOrder<P>(c, int(b), 0);
+    uploadOrder<P>(c, int(b), 1);
+  }
+}
+
+template <int P>
+void setupDev(ws_ctx *c) {
+  Carver cnt{nullptr};
+  Dev<P> &d = devOf<P>(c);
+  layout<P>(d, cnt, c->z);
+  c->bytes = cnt.off + 4096;
+  CK(cudaMalloc(&c->arena, c->bytes));
+  CK(cudaMemsetAsync(c->arena, 0, c->bytes, c->st));
+  Carver cv{c->arena};
+  layout<P>(d, cv, c->z);
+  uploadAll<P>(c);
+}
+
+void readCtl(ws_ctx *c) {
+  c->ctlHost.resize(c->inst.size());
+  CK(cudaMemcpyAsync(c->ctlHost.data(), c->dCtl, sizeof(InstCtl) * c->inst.size(), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+}
+void fillControl(const InstCtl &s, ws_control *o) {
+  o->iter = s.iter; o->status = s.status; o->rollbacks = s.rollbacks; o->pending_zero = s.pending;
+  o->ke = s.ke; o->ke_prev = s.ke_prev; o->residual = s.residual; o->res_force = s.res_f; o->res_torque = s.res_t; o->fref = s.fref;
+  o->e_stretch = s.e_stretch; o->e_shear = s.e_shear; o->e_bend = s.e_bend; o->e_twist = s.e_twist; o->e_contact = s.e_contact;
+}
+
+template <int P>
+void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
+  const int nInst = int(c->inst.size());
+  c->lastLaunches = 0;
+  CK(cudaEventRecord(c->ev0, c->st));
+  if (c->form == WS_FORM_CTA) {
+    if (mask) CK(cudaMemcpyAsync(c->dMask, mask, nInst, cudaMemcpyHostToDevice, c->st));
+    const int thr = c->threads > 0 ? c->threads : 256;
+    CK(launchBatched<P>(devOf<P>(c), c->dInst, c->dCtl, c->dOrder, nInst, nIter, mask ? c->dMask : nullptr, thr, nInst, c->st));
+    c->lastLaunches = 1;
+  } else {
+    const bool cx = c->inst[0].contacts && c->inst[0].K;
+    const int chunk = std::min(nIter, 50);
+    if (chunk > 0 && (!c->graph || c->graphIters != chunk)) {
+      if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+      cudaGraph_t gr;
+      CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+      int nl = 0;
+      for (int i = 0; i < chunk; i++) CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, c->st, &nl));
+      CK(cudaStreamEndCapture(c->st, &gr));
+      CK(cudaGraphInstantiate(&c->graph, gr, 0));
+      cudaGraphDestroy(gr);
+      c->graphIters = chunk;
+    }
+    int done = 0;
+    const int per = cx ? 5 : 3;
+    while (nIter - done >= chunk && chunk > 0) { CK(cudaGraphLaunch(c->graph, c->st)); done += chunk; c->lastLaunches += int64_t(chunk) * per; }
+    int nl = 0;
+    for (; done < nIter; done++) CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, c->st, &nl));
+    c->lastLaunches += nl;
+  }
+  CK(cudaEventRecord(c->ev1, c->st));
+}
+
+template <int P>
+void downloadImpl(ws_ctx *c, int b, ws_state_out *o) {
+  Dev<P> &d = devOf<P>(c);
+  readCtl(c);
+  const InstCtl &s = c->ctlHost[b];
+  const InstDesc &I = c->inst[b];
+  const size_t n = I.n, m = I.m, p = I.p, K = I.K;
+  std::vector<double> t, t2;
+  auto planes = [&](double *dst, int ncomp, auto *src, size_t stride, size_t off, size_t count) {
+    for (int k = 0; k < ncomp; k++) {
+      getv(t, src + size_t(k) * stride + off, count, c->st);
+      for (size_t i = 0; i < count; i++) dst[ncomp * i + k] = t[i];
+    }
+  };
+  if (o->X) {
+    for (int k = 0; k < 3; k++) {
+      getv(t, d.X + size_t(s.cur * 3 + k) * d.ntot + I.n0, n, c->st);
+      if (PrecT<P>::TWO) getv(t2, d.Xlo + size_t(s.cur * 3 + k) * d.ntot + I.n0, n, c->st);
+      for (size_t i = 0; i < n; i++) o->X[3 * i + k] = t[i] + (PrecT<P>::TWO ? t2[i] : 0.0);
+    }
+  }
+  if (o->Q) {
+    for (int k = 0; k < 4; k++) {
+      getv(t, d.Q + size_t(s.cur * 4 + k) * d.mtot + I.m0, m, c->st);
+      if (PrecT<P>::TWO) getv(t2, d.Qlo + size_t(s.cur * 4 + k) * d.mtot + I.m0, m, c->st);
+      for (size_t j = 0; j < m; j++) o->Q[4 * j + k] = t[j] + (PrecT<P>::TWO ? t2[j] : 0.0);
+    }
+  }
+  if (o->V) { if (s.pending) std::fill(o->V, o->V + 3 * n, 0.0); else planes(o->V, 3, d.V, d.ntot, I.n0, n); }
+  if (o->W) { if (s.pending) std::fill(o->W, o->W + 3 * m, 0.0); else planes(o->W, 3, d.Wr, d.mtot, I.m0, m); }
+  if (K) {
+    if (o->u) planes(o->u, 2, d.u, d.ktot, I.k0, K);
+    if (o->nprev) planes(o->nprev, 3, d.nPrev, d.ktot, I.k0, K);
+    if (o->slip) planes(o->slip, 1, d.slip, 0, I.k0, K);
+    if (o->Fn) planes(o->Fn, 1, d.Fn, 0, I.k0, K);
+    if (o->Ft) planes(o->Ft, 1, d.Ft, 0, I.k0, K);
+    if (o->gap) planes(o->gap, 1, d.gap, 0, I.k0, K);
+    if (o->stuck) { std::vector<uint8_t> v(K); CK(cudaMemcpyAsync(v.data(), d.stuck + I.k0, K, cudaMemcpyDeviceToHost, c->st)); CK(cudaStreamSynchronize(c->st)); std::copy(v.begin(), v.end(), o->stuck); }
+    if (o->state) { std::vector<uint8_t> v(K); CK(cudaMemcpyAsync(v.data(), d.cstate + I.k0, K, cudaMemcpyDeviceToHost, c->st)); CK(cudaStreamSynchronize(c->st)); std::copy(v.begin(), v.end(), o->state); }
+  }
+  if (o->N) planes(o->N, 1, d.Nax, 0, I.m0, m);
+  if (o->Vsh) planes(o->Vsh, 2, d.Vsh, d.mtot, I.m0, m);
+  if (o->M && p) planes(o->M, 3, d.Mj, d.ptot, I.p0, p);
+  if (o->reactions) planes(o->reactions, 3, d.react, d.ntot, I.n0, n);
+}
+
+// current X, Q, u, nPrev of instance b into its host goals
+template <int P>
+void pullState(ws_ctx *c, int b) {
+  HostGoals &g = c->g[b];
+  ws_state_out o{};
+  std::vector<double> X(3 * size_t(g.n)), Q(4 * size_t(g.m)), u(2 * size_t(g.K)), np(3 * size_t(g.K));
+  o.X = X.data(); o.Q = Q.data();
+  if (g.K) { o.u = u.data(); o.nprev = np.data(); }
+  downloadImpl<P>(c, b, &o);
+  g.X = X; g.Q = Q;
+  if (g.K) { g.u = u; g.nPrev = np; }
+}
+
+template <int P>
+void setParamsImpl(ws_ctx *c, int b, const ws_model *md) {
+  pullState<P>(c, b);
+  HostGoals &g = c->g[b];
+  const std::vector<int> oldSeg = g.cSeg;
+  HostGoals trial = g;
+  trial.rebuild(*md);
+  if (trial.cSeg != oldSeg) throw std::invalid_argument("the anchors changed the rotation clamps: create a new context");
+  g = std::move(trial);
+  Sizes off;
+  off.n = c->inst[b].n0; off.m = c->inst[b].m0; off.p = c->inst[b].p0; off.c = c->inst[b].c0; off.k = c->inst[b].k0; off.s = c->inst[b].s0;
+  c->inst[b] = describe(g, off);
+  CK(cudaMemcpyAsync(c->dInst + b, &c->inst[b], sizeof(InstDesc), cudaMemcpyHostToDevice, c->st));
+  uploadGoals<P>(c, b);
+  readCtl(c);
+  InstCtl s = c->ctlHost[b];
+  s.ke_prev = 0.0; s.status = WS_RUNNING; s.disp_it0 = s.iter;
+  CK(cudaMemcpyAsync(c->dCtl + b, &s, sizeof(InstCtl), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+}
+
+template <int P>
+void uploadStateImpl(ws_ctx *c, int b, const double *X, const double *Q, const double *u) {
+  HostGoals &g = c->g[b];
+  readCtl(c);
+  InstCtl s = c->ctlHost[b];
+  g.X.assign(X, X + 3 * size_t(g.n));
+  g.Q.assign(Q, Q + 4 * size_t(g.m));
+  if (u && g.K) g.u.assign(u, u + 2 * size_t(g.K));
+  uploadState<P>(c, b, s.cur, u != nullptr);
+  if (u && g.K) { g.sortSides(); uploadOrder<P>(c, b, s.obuf); }
+  s.pending = 0; s.ke_prev = 0.0; s.status = WS_RUNNING;
+  CK(cudaMemcpyAsync(c->dCtl + b, &s, sizeof(InstCtl), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+}
+
+template <int P>
+void internalizeImpl(ws_ctx *c, int b) {
+  pullState<P>(c, b);
+  HostGoals &g = c->g[b];
+  g.X0 = g.X;
+  Dev<P> &d = devOf<P>(c);
+  using A = typename Dev<P>::A;
+  if (g.K) CK(cudaMemsetAsync(d.slip + c->inst[b].k0, 0, sizeof(A) * g.K, c->st));
+  CK(cudaStreamSynchronize(c->st));
+}
+
+template <class F>
+int guarded(const char *what, F &&f) {
+  try {
+    f();
+    return WS_OK;
+  } catch (const CudaError &e) {
+    return fail(WS_ERR_CUDA, std::string(what) + ": " + e.what());
+  } catch (const std::invalid_argument &e) {
+    return fail(WS_ERR_ARG, std::string(what) + ": " + e.what());
+  } catch (const std::bad_alloc &) {
+    return fail(WS_ERR_NOMEM, std::string(what) + ": host memory exhausted");
+  } catch (const std::exception &e) {
+    return fail(WS_ERR_STATE, std::string(what) + ": " + e.what());
+  }
+}
+
+#define DISPATCH(c, FN, ...)                                  \
+  switch ((c)->prec) {                                        \
+    case WS_PREC_F64: FN<PREC_F64>(__VA_ARGS__); break;       \
+    case WS_PREC_MIXED: FN<PREC_MIXED>(__VA_ARGS__); break;   \
+    default: FN<PREC_F32>(__VA_ARGS__); break;                \
+  }
+
+void destroyCtx(ws_ctx *c) {
+  if (!c) return;
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  if (c->arena) cudaFree(c->arena);
+  if (c->dInst) cudaFree(c->dInst);
+  if (c->dCtl) cudaFree(c->dCtl);
+  if (c->dOrder) cudaFree(c->dOrder);
+  if (c->dMask) cudaFree(c->dMask);
+  if (c->dPart) cudaFree(c->dPart);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ws_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); return 0; }
+  return n;
+}
+
+int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts *opts, ws_ctx **out) {
+  if (!models || n_instances <= 0 || !out) return fail(WS_ERR_ARG, "ws_create: need at least one model and an output pointer");
+  ws_opts o{};
+  if (opts) o = *opts;
+  if (o.precision < 0 || o.precision > 2) return fail(WS_ERR_ARG, "ws_create: unknown precision");
+  if (o.form < 0 || o.form > 2) return fail(WS_ERR_ARG, "ws_create: unknown execution form");
+  if (o.form != WS_FORM_CTA && n_instances != 1) return fail(WS_ERR_ARG, "ws_create: the grid and plain forms take one instance");
+  if (o.threads < 0 || o.threads > 1024 || (o.threads % 32)) return fail(WS_ERR_ARG, "ws_create: threads must be a multiple of 32 up to 1024");
+  if (ws_device_count() <= 0) return fail(WS_ERR_NODEV, "ws_create: no CUDA device (this library has no CPU path)");
+  auto c = new ws_ctx();
+  c->prec = o.precision; c->form = o.form == WS_FORM_GRID ? WS_FORM_PLAIN : o.form; c->threads = o.threads; c->device = o.device;
+  int rc = guarded("ws_create", [&]() {
+    CK(cudaSetDevice(o.device));
+    CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&c->ev0));
+    CK(cudaEventCreate(&c->ev1));
+    c->g.resize(n_instances);
+    Sizes off;
+    for (int b = 0; b < n_instances; b++) {
+      if (!models[b]) throw std::invalid_argument("null model");
+      c->g[b].build(*models[b]);
+      c->inst.push_back(describe(c->g[b], off));
+      off.n += c->g[b].n; off.m += c->g[b].m; off.p += c->g[b].p; off.c += c->g[b].C; off.k += c->g[b].K; off.s += c->g[b].S;
+    }
+    c->z = off;
+    // longest instances first: the hardware block scheduler then balances the tail
+    c->order.resize(n_instances);
+    std::iota(c->order.begin(), c->order.end(), 0);
+    std::stable_sort(c->order.begin(), c->order.end(), [&](int a, int b) { return c->inst[a].n + c->inst[a].m > c->inst[b].n + c->inst[b].m; });
+    CK(cudaMalloc(&c->dInst, sizeof(InstDesc) * n_instances));
+    CK(cudaMalloc(&c->dCtl, sizeof(InstCtl) * n_instances));
+    CK(cudaMalloc(&c->dOrder, sizeof(int) * n_instances));
+    CK(cudaMalloc(&c->dMask, n_instances));
+    CK(cudaMemcpyAsync(c->dInst, c->inst.data(), sizeof(InstDesc) * n_instances, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->dOrder, c->order.data(), sizeof(int) * n_instances, cudaMemcpyHostToDevice, c->st));
+    std::vector<InstCtl> ctl(n_instances);
+    for (auto &s : ctl) { std::memset(&s, 0, sizeof(s)); s.status = WS_RUNNING; s.residual = INFINITY; }
+    CK(cudaMemcpyAsync(c->dCtl, ctl.data(), sizeof(InstCtl) * n_instances, cudaMemcpyHostToDevice, c->st));
+    const InstDesc &I0 = c->inst[0];
+    auto blocks = [](long long cnt, int thr) { return int(std::max<long long>(1, std::min<long long>((cnt + thr - 1) / thr, 148LL * 8))); };
+    c->shape.blocksA = blocks(I0.m + I0.p + I0.C + I0.K, 256);
+    c->shape.blocksS = blocks(I0.S, 128);
+    c->shape.blocksR = blocks(I0.m, 256);
+    c->shape.blocksD = blocks(I0.n + I0.m, 256);
+    CK(cudaMalloc(&c->dPart, sizeof(double) * (RS_NSUM + RX_NMAX) * size_t(c->shape.blocksA + c->shape.blocksD)));
+    DISPATCH(c, setupDev, c);
+    size_t total = c->bytes + (sizeof(InstDesc) + sizeof(InstCtl) + 8) * n_instances;
+    if (o.budget_bytes && total > o.budget_bytes) throw std::bad_alloc();
+    CK(cudaStreamSynchronize(c->st));
+  });
+  if (rc == WS_ERR_NOMEM && o.budget_bytes) fail(WS_ERR_NOMEM, "ws_create: the batch needs more device memory than the budget");
+  if (rc != WS_OK) { destroyCtx(c); return rc; }
+  *out = c;
+  return WS_OK;
+}
+
+int ws_step(ws_ctx *c, int32_t n_iter, const uint8_t *mask, ws_control *ctl) {
+  if (!c || n_iter < 0) return fail(WS_ERR_ARG, "ws_step: bad arguments");
+  return guarded("ws_step", [&]() {
+    CK(cudaSetDevice(c->device));
+    DISPATCH(c, stepImpl, c, n_iter, mask);
+    c->lastMs = -1;
+    if (ctl) {
+      readCtl(c);
+      for (size_t b = 0; b < c->inst.size(); b++) fillControl(c->ctlHost[b], ctl + b);
+    }
+  });
+}
+
+int ws_read_control(ws_ctx *c, ws_control *ctl) {
+  if (!c || !ctl) return fail(WS_ERR_ARG, "ws_read_control: bad arguments");
+  return guarded("ws_read_control", [&]() {
+    readCtl(c);
+    for (size_t b = 0; b < c->inst.size(); b++) fillControl(c->ctlHost[b], ctl + b);
+  });
+}
+
+int ws_download(ws_ctx *c, int32_t b, ws_state_out *o) {
+  if (!c || !o || b < 0 || b >= int(c->inst.size())) return fail(WS_ERR_ARG, "ws_download: bad instance");
+  return guarded("ws_download", [&]() { DISPATCH(c, downloadImpl, c, b, o); });
+}
+
+int ws_upload_state(ws_ctx *c, int32_t b, const double *X, const double *Q, const double *u) {
+  if (!c || !X || !Q || b < 0 || b >= int(c->inst.size())) return fail(WS_ERR_ARG, "ws_upload_state: bad arguments");
+  return guarded("ws_upload_state", [&]() { DISPATCH(c, uploadStateImpl, c, b, X, Q, u); });
+}
+
+int ws_set_params(ws_ctx *c, int32_t b, const ws_model *md) {
+  if (!c || !md || b < 0 || b >= int(c->inst.size())) return fail(WS_ERR_ARG, "ws_set_params: bad arguments");
+  return guarded("ws_set_params", [&]() { DISPATCH(c, setParamsImpl, c, b, md); });
+}
+
+int ws_internalize(ws_ctx *c, int32_t b) {
+  if (!c || b < 0 || b >= int(c->inst.size())) return fail(WS_ERR_ARG, "ws_internalize: bad instance");
+  return guarded("ws_internalize", [&]() { DISPATCH(c, internalizeImpl, c, b); });
+}
+
+void *ws_stream(ws_ctx *c) { return c ? c->st : nullptr; }
+uint64_t ws_device_bytes(const ws_ctx *c) { return c ? c->bytes : 0; }
+int ws_last_step_stats(const ws_ctx *c_, double *ms, int64_t *launches) {
+  if (!c_) return fail(WS_ERR_ARG, "ws_last_step_stats: null context");
+  ws_ctx *c = const_cast<ws_ctx *>(c_);
+  if (c->lastMs < 0) {
+    float t = 0;
+    if (cudaEventSynchronize(c->ev1) != cudaSuccess || cudaEventElapsedTime(&t, c->ev0, c->ev1) != cudaSuccess)
+      return fail(WS_ERR_CUDA, "ws_last_step_stats: event timing failed");
+    c->lastMs = t;
+  }
+  if (ms) *ms = c->lastMs;
+  if (launches) *launches = c->lastLaunches;
+  return WS_OK;
+}
+int ws_destroy(ws_ctx *c) {
+  if (!c) return WS_OK;
+  cudaSetDevice(c->device);
+  destroyCtx(c);
+  return WS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,179 @@
+// sm_100a kernels of the DR step: the persistent batched form (one thread block per instance, every phase of every
+// iteration inside one launch) and the plain form (one kernel per phase, one instance, captured as a CUDA graph).
+#include "dr_kernels.hpp"
+#include "dr_phases.cuh"
+
+namespace wsb {
+
+// ------------------------------------------------------------------------------------------------ batched form
+// Block b relaxes instance order[b] (and further instances grid-strided) for up to nIter iterations, stopping at its
+// own convergence.  Instance state lives in HBM / L2; the block's barriers separate the phases, so an instance never
+// waits on another and no kernel spins.
+template <int P>
+__global__ void __launch_bounds__(1024) k_batched(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+                                                  const int *__restrict__ order, int nInst, int nIter, const uint8_t *__restrict__ mask) {
+  using A = typename Dev<P>::A;
+  __shared__ InstCtl sc;
+  __shared__ InstDesc si;
+  __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
+  for (int bi = blockIdx.x; bi < nInst; bi += gridDim.x) {
+    const int b = order ? order[bi] : bi;
+    if (mask && !mask[b]) continue;
+    if (threadIdx.x == 0) { sc = ctl[b]; si = insts[b]; }
+    __syncthreads();
+    const InstDesc &I = si;
+    const bool cx = I.contacts && I.K;
+    const int nA = I.m + I.p + I.C + (cx ? I.K : 0);
+    for (int it = 0; it < nIter; it++) {
+      if (sc.status != WS_RUNNING) break;
+      const StepCtx sx = makeCtx<A>(I, sc);
+      Part<A> pt;
+      pt.init();
+      for (int e = threadIdx.x; e < nA; e += blockDim.x) {
+        if (e < I.m) segForce<P>(d, sx.cur, I.m0 + e, pt);
+        else if (e < I.m + I.p) jointTorque<P>(d, sx.cur, I.p0 + (e - I.m), pt);
+        else if (e < I.m + I.p + I.C) clampTorque<P>(d, sx.cur, I.c0 + (e - I.m - I.p), pt);
+        else crossing<P>(d, I, sx.cur, sx.iter, I.k0 + (e - I.m - I.p - I.C), pt);
+      }
+      __syncthreads();
+      if (cx) {
+        for (int s = threadIdx.x; s < I.S; s += blockDim.x) sortStrand<P>(d, I.s0 + s, sx.obuf, sx.onxt);
+        __syncthreads();
+        for (int j = threadIdx.x; j < I.m; j += blockDim.x) segRange<P>(d, I.m0 + j, sx.onxt);
+        __syncthreads();
+      }
+      for (int e = threadIdx.x; e < I.n + I.m; e += blockDim.x) {
+        if (e < I.n) nodeUpdate<P>(d, I, sx, I.n0 + e, pt);
+        else segUpdate<P>(d, I, sx, I.m0 + (e - I.n), pt);
+      }
+      __syncthreads();
+      blockReduce(pt, red);
+      if (threadIdx.x == 0) decide(I, sc, pt, nIter);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) ctl[b] = sc;
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ plain form
+// One kernel per phase over the elements of instance 0; block partials go to part[phase][block] and k_decide reduces
+// them in a fixed order.  Every kernel returns at once when the instance has stopped.
+template <int P>
+__global__ void __launch_bounds__(256) k_plainA(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
+                                                typename Dev<P>::A *part) {
+  using A = typename Dev<P>::A;
+  __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
+  const InstDesc I = insts[0];
+  const InstCtl c = ctl[0];
+  if (c.status != WS_RUNNING) return;
+  const bool cx = I.contacts && I.K;
+  const int nA = I.m + I.p + I.C + (cx ? I.K : 0);
+  Part<A> pt;
+  pt.init();
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nA; e += gridDim.x * blockDim.x) {
+    if (e < I.m) segForce<P>(d, c.cur, I.m0 + e, pt);
+    else if (e < I.m + I.p) jointTorque<P>(d, c.cur, I.p0 + (e - I.m), pt);
+    else if (e < I.m + I.p + I.C) clampTorque<P>(d, c.cur, I.c0 + (e - I.m - I.p), pt);
+    else crossing<P>(d, I, c.cur, c.iter, I.k0 + (e - I.m - I.p - I.C), pt);
+  }
+  blockReduce(pt, red);
+  constexpr int NV = RS_NSUM + RX_NMAX;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < RS_NSUM; i++) part[blockIdx.x * NV + i] = pt.s[i];
+    for (int i = 0; i < RX_NMAX; i++) part[blockIdx.x * NV + RS_NSUM + i] = pt.x[i];
+  }
+}
+template <int P>
+__global__ void k_plainSort(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl) {
+  const InstDesc I = insts[0];
+  const InstCtl c = ctl[0];
+  if (c.status != WS_RUNNING) return;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < I.S; s += gridDim.x * blockDim.x) sortStrand<P>(d, I.s0 + s, c.obuf, c.obuf ^ 1);
+}
+template <int P>
+__global__ void k_plainRange(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl) {
+  const InstDesc I = insts[0];
+  const InstCtl c = ctl[0];
+  if (c.status != WS_RUNNING) return;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < I.m; j += gridDim.x * blockDim.x) segRange<P>(d, I.m0 + j, c.obuf ^ 1);
+}
+template <int P>
+__global__ void __launch_bounds__(256) k_plainD(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
+                                                typename Dev<P>::A *part) {
+  using A = typename Dev<P>::A;
+  __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
+  const InstDesc I = insts[0];
+  const InstCtl c = ctl[0];
+  if (c.status != WS_RUNNING) return;
+  const StepCtx sx = makeCtx<A>(I, c);
+  Part<A> pt;
+  pt.init();
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < I.n + I.m; e += gridDim.x * blockDim.x) {
+    if (e < I.n) nodeUpdate<P>(d, I, sx, I.n0 + e, pt);
+    else segUpdate<P>(d, I, sx, I.m0 + (e - I.n), pt);
+  }
+  blockReduce(pt, red);
+  constexpr int NV = RS_NSUM + RX_NMAX;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < RS_NSUM; i++) part[blockIdx.x * NV + i] = pt.s[i];
+    for (int i = 0; i < RX_NMAX; i++) part[blockIdx.x * NV + RS_NSUM + i] = pt.x[i];
+  }
+}
+template <int P>
+__global__ void __launch_bounds__(256) k_plainDecide(const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl, const typename Dev<P>::A *part, int nParts) {
+  using A = typename Dev<P>::A;
+  __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
+  if (ctl[0].status != WS_RUNNING) return;
+  constexpr int NV = RS_NSUM + RX_NMAX;
+  Part<A> pt;
+  pt.init();
+  for (int b = threadIdx.x; b < nParts; b += blockDim.x) {
+    for (int i = 0; i < RS_NSUM; i++) pt.s[i] += part[b * NV + i];
+    for (int i = 0; i < RX_NMAX; i++) pt.x[i] = mmax(pt.x[i], part[b * NV + RS_NSUM + i]);
+  }
+  blockReduce(pt, red);
+  if (threadIdx.x == 0) {
+    InstCtl c = ctl[0];
+    decide(insts[0], c, pt, 0);
+    ctl[0] = c;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ launchers
+template <int P>
+cudaError_t launchBatched(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
+                          const uint8_t *mask, int threads, int blocks, cudaStream_t st) {
+  k_batched<P><<<blocks, threads, 0, st>>>(d, insts, ctl, order, nInst, nIter, mask);
+  return cudaGetLastError();
+}
+
+template <int P>
+cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, const PlainShape &sh, bool contacts,
+                            cudaStream_t st, int *launches) {
+  using A = typename Dev<P>::A;
+  A *pa = static_cast<A *>(part), *pd = pa + size_t(sh.blocksA) * (RS_NSUM + RX_NMAX);
+  k_plainA<P><<<sh.blocksA, 256, 0, st>>>(d, insts, ctl, pa);
+  int nl = 1;
+  if (contacts) {
+    k_plainSort<P><<<sh.blocksS, 128, 0, st>>>(d, insts, ctl);
+    k_plainRange<P><<<sh.blocksR, 256, 0, st>>>(d, insts, ctl);
+    nl += 2;
+  }
+  k_plainD<P><<<sh.blocksD, 256, 0, st>>>(d, insts, ctl, pd);
+  k_plainDecide<P><<<1, 256, 0, st>>>(insts, ctl, pa, sh.blocksA + sh.blocksD);
+  nl += 2;
+  if (launches) *launches += nl;
+  return cudaGetLastError();
+}
+
+#define WSB_INST(P)                                                                                                  \
+  template cudaError_t launchBatched<P>(const Dev<P> &, const InstDesc *, InstCtl *, const int *, int, int, const uint8_t *, \
+                                        int, int, cudaStream_t);                                                     \
+  template cudaError_t launchPlainIter<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, const PlainShape &, bool,    \
+                                          cudaStream_t, int *);
+WSB_INST(PREC_F64)
+WSB_INST(PREC_MIXED)
+WSB_INST(PREC_F32)
+
+}  // namespace wsb

@@ -1,0 +1,652 @@
+// The phases of one dynamic-relaxation iteration (CpuSolver.step, web/js/solver_cpu.js:737-841) as device functions
+// over element ranges.  Every phase writes disjoint outputs; the force gather is conflict-free (no atomics):
+//   A  elements:  segments (stretch/shear force n, e × n)          rod_cosserat.js:118-133
+//                 joints (bend/twist torque, kDyn share)           rod_cosserat.js:136-159
+//                 clamps (joints against frozen frames)            rod_cosserat.js:161-180
+//                 crossings (Hermite evaluation, normal, gap, penalty, Coulomb return mapping, slide of u on both
+//                 laths, force and lever torque per side)          solver_cpu.js:179-228, 274-282, 381-478
+//   B  strands:   crossing sides re-sorted along their strand by their new segment (insertion sort, nearly sorted)
+//   C  segments:  slice of the sorted sides on every segment (binary search)
+//   D  nodes:     F = n_out − n_in + loads + Σ sides on the two adjacent segments (weights 1 − t, t, the slices of
+//                 the previous sort); reactions, fixed DOFs, warm-up, v += F/m, x += v, prescribed support motion
+//                 segments: T = e × n ± joint torques − clamp torques + lever torques; tm = Rᵀ T; frame inertia
+//                 with the righting share of the crossings on the segment now (the new slices) and kDyn;
+//                 ω += tm / I, roll limit and roll damping, q ← q ⊗ exp(ω)
+//   E  instance:  kinetic energy, kinetic-damping roll-back, residual, convergence (one thread)
+#pragma once
+#include <cfloat>
+
+#include "../../include/weavesim.h"
+#include "dr_common.cuh"
+
+namespace wsb {
+
+static constexpr double SUPPORT_SMOOTH = 0.03;                // solver_cpu.js:16
+static constexpr double TWIST_RATE_MAX = 0.5 * SUPPORT_SMOOTH;  // solver_cpu.js:21
+static constexpr double ROLL_DAMP = 0.5;                      // solver_cpu.js:28
+
+// ------------------------------------------------------------------------------------------------ math helpers
+__device__ __forceinline__ float msqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double msqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float matan2(float y, float x) { return atan2f(y, x); }
+__device__ __forceinline__ double matan2(double y, double x) { return atan2(y, x); }
+__device__ __forceinline__ float mtanh(float x) { return tanhf(x); }
+__device__ __forceinline__ double mtanh(double x) { return tanh(x); }
+__device__ __forceinline__ void msincos(float x, float *s, float *c) { sincosf(x, s, c); }
+__device__ __forceinline__ void msincos(double x, double *s, double *c) { sincos(x, s, c); }
+__device__ __forceinline__ float mfloor(float x) { return floorf(x); }
+__device__ __forceinline__ double mfloor(double x) { return floor(x); }
+template <class T> __device__ __forceinline__ T mmin(T a, T b) { return a < b ? a : b; }
+template <class T> __device__ __forceinline__ T mmax(T a, T b) { return a > b ? a : b; }
+template <class T> __device__ __forceinline__ T mabs(T a) { return a < T(0) ? -a : a; }
+template <class T> __device__ __forceinline__ T mclamp(T v, T lo, T hi) { return mmin(mmax(v, lo), hi); }
+
+// frame [X | Y | Z] of a quaternion (normalised first): quat.js:19-27
+template <class T>
+__device__ __forceinline__ void qframe(const T q[4], T R[9]) {
+  T w = q[0], x = q[1], y = q[2], z = q[3];
+  T n = msqrt(w * w + x * x + y * y + z * z);
+  if (n == T(0)) n = T(1);
+  const T in = T(1) / n;
+  w *= in; x *= in; y *= in; z *= in;
+  R[0] = T(1) - T(2) * (y * y + z * z); R[1] = T(2) * (x * y + z * w); R[2] = T(2) * (x * z - y * w);
+  R[3] = T(2) * (x * y - z * w); R[4] = T(1) - T(2) * (x * x + z * z); R[5] = T(2) * (y * z + x * w);
+  R[6] = T(2) * (x * z + y * w); R[7] = T(2) * (y * z - x * w); R[8] = T(1) - T(2) * (x * x + y * y);
+}
+template <class T>
+__device__ __forceinline__ void qmul(const T a[4], const T b[4], T o[4]) {
+  o[0] = a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3];
+  o[1] = a[0] * b[1] + a[1] * b[0] + a[2] * b[3] - a[3] * b[2];
+  o[2] = a[0] * b[2] - a[1] * b[3] + a[2] * b[0] + a[3] * b[1];
+  o[3] = a[0] * b[3] + a[1] * b[2] - a[2] * b[1] + a[3] * b[0];
+}
+template <class T>
+__device__ __forceinline__ void qnormalize(T q[4]) {
+  T n = msqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  if (n == T(0)) n = T(1);
+  q[0] /= n; q[1] /= n; q[2] /= n; q[3] /= n;
+}
+template <class T>
+__device__ __forceinline__ void cross3(const T a[3], const T b[3], T o[3]) {
+  o[0] = a[1] * b[2] - a[2] * b[1]; o[1] = a[2] * b[0] - a[0] * b[2]; o[2] = a[0] * b[1] - a[1] * b[0];
+}
+template <class T> __device__ __forceinline__ T dot3(const T a[3], const T b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+// β of J_l⁻ᵀ(Ψ) = 1 + ½[Ψ]× + β[Ψ]×²: 1/θ² − (1 + cos θ)/(2θ sin θ), series 1/12 + θ²/720 + θ⁴/30240 near 0
+// (rod_cosserat.js:147-148 switches at 1e-3; in float the closed form cancels below ~0.3 rad, so float switches there)
+template <class T>
+__device__ __forceinline__ T jbeta(T th) {
+  const T thr = sizeof(T) == 8 ? T(1e-3) : T(0.3);
+  if (th < thr) {
+    const T t2 = th * th;
+    return sizeof(T) == 8 ? T(1.0 / 12) + t2 / T(720) : T(1.0 / 12) + t2 * (T(1.0 / 720) + t2 * T(1.0 / 30240));
+  }
+  T s, c;
+  msincos(th, &s, &c);
+  return T(1) / (th * th) - (T(1) + c) / (T(2) * th * s);
+}
+
+// ------------------------------------------------------------------------------------------------ state access
+template <int P> struct Acc {
+  using D = Dev<P>;
+  using R = typename D::R; using W = typename D::W; using S = typename D::S;
+  __device__ static __forceinline__ W xw(const D &d, int buf, int k, int i) {
+    const size_t o = size_t(buf * 3 + k) * d.ntot + i;
+    if constexpr (PrecT<P>::TWO) return W(d.X[o]) + W(d.Xlo[o]); else return W(d.X[o]);
+  }
+  __device__ static __forceinline__ R xr(const D &d, int buf, int k, int i) { return R(d.X[size_t(buf * 3 + k) * d.ntot + i]); }
+  __device__ static __forceinline__ void xs(const D &d, int buf, int k, int i, W v) {
+    const size_t o = size_t(buf * 3 + k) * d.ntot + i;
+    if constexpr (PrecT<P>::TWO) { const S hi = S(v); d.X[o] = hi; d.Xlo[o] = S(v - W(hi)); } else d.X[o] = S(v);
+  }
+  __device__ static __forceinline__ W qw(const D &d, int buf, int k, int j) {
+    const size_t o = size_t(buf * 4 + k) * d.mtot + j;
+    if constexpr (PrecT<P>::TWO) return W(d.Q[o]) + W(d.Qlo[o]); else return W(d.Q[o]);
+  }
+  __device__ static __forceinline__ R qr(const D &d, int buf, int k, int j) { return R(d.Q[size_t(buf * 4 + k) * d.mtot + j]); }
+  __device__ static __forceinline__ void qs(const D &d, int buf, int k, int j, W v) {
+    const size_t o = size_t(buf * 4 + k) * d.mtot + j;
+    if constexpr (PrecT<P>::TWO) { const S hi = S(v); d.Q[o] = hi; d.Qlo[o] = S(v - W(hi)); } else d.Q[o] = S(v);
+  }
+  // edge vector x_b − x_a formed in the wide type, returned in R
+  __device__ static __forceinline__ void edge(const D &d, int buf, int a, int b, R e[3]) {
+    for (int k = 0; k < 3; k++) e[k] = R(xw(d, buf, k, b) - xw(d, buf, k, a));
+  }
+};
+
+// reduction partials of one thread
+template <class A>
+struct Part {
+  A s[RS_NSUM];
+  A x[RX_NMAX];
+  __device__ void init() {
+    for (int i = 0; i < RS_NSUM; i++) s[i] = A(0);
+    for (int i = 0; i < RX_NMAX; i++) x[i] = A(0);
+    x[RX_FN] = -A(INFINITY);
+  }
+};
+
+// ------------------------------------------------------------------------------------------------ node helpers
+// node tangent: normalised sum of the unit chords of the adjacent segments (PolylineContact._prepare)
+template <int P>
+__device__ __forceinline__ void nodeTangent(const Dev<P> &d, int buf, int i, typename Dev<P>::R T[3]) {
+  using R = typename Dev<P>::R;
+  T[0] = T[1] = T[2] = R(0);
+  const int so = d.nsOut[i], si = d.nsIn[i];
+  for (int j : {so, si}) {
+    if (j < 0) continue;
+    R e[3];
+    Acc<P>::edge(d, buf, d.segI0[j], d.segI1[j], e);
+    const R l = mmax(msqrt(dot3(e, e)), R(1e-12));
+    for (int k = 0; k < 3; k++) T[k] += e[k] / l;
+  }
+  const R l = mmax(msqrt(dot3(T, T)), R(1e-12));
+  for (int k = 0; k < 3; k++) T[k] /= l;
+}
+// hemisphere-consistent mean of the adjacent segment frames (nodeQuats, model.js:89-105)
+template <int P>
+__device__ __forceinline__ void nodeQuat(const Dev<P> &d, int buf, int i, typename Dev<P>::R q[4]) {
+  using R = typename Dev<P>::R;
+  const int so = d.nsOut[i], si = d.nsIn[i], ref = so >= 0 ? so : si;
+  q[0] = q[1] = q[2] = q[3] = R(0);
+  if (ref < 0) return;
+  R qr[4];
+  for (int k = 0; k < 4; k++) qr[k] = Acc<P>::qr(d, buf, k, ref);
+  for (int j : {so, si}) {
+    if (j < 0) continue;
+    R qj[4];
+    for (int k = 0; k < 4; k++) qj[k] = Acc<P>::qr(d, buf, k, j);
+    const R dd = qj[0] * qr[0] + qj[1] * qr[1] + qj[2] * qr[2] + qj[3] * qr[3];
+    const R sg = dd < R(0) ? R(-1) : R(1);
+    for (int k = 0; k < 4; k++) q[k] += sg * qj[k];
+  }
+  qnormalize(q);
+}
+
+// ------------------------------------------------------------------------------------------------ phase A
+// segment j: σ = Rᵀe/l0 − e3, n = R·diag(κGA, κGA, EA)·σ (rod_cosserat.js:118-133)
+template <int P>
+__device__ __forceinline__ void segForce(const Dev<P> &d, int buf, int j, Part<typename Dev<P>::A> &pt) {
+  using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A;
+  const int a = d.segI0[j], b = d.segI1[j];
+  W ew[3], qw[4], Rw[9];
+  for (int k = 0; k < 3; k++) ew[k] = Acc<P>::xw(d, buf, k, b) - Acc<P>::xw(d, buf, k, a);
+  for (int k = 0; k < 4; k++) qw[k] = Acc<P>::qw(d, buf, k, j);
+  qframe(qw, Rw);
+  const W l0 = W(d.l0[j]);
+  const R s1 = R((Rw[0] * ew[0] + Rw[1] * ew[1] + Rw[2] * ew[2]) / l0);
+  const R s2 = R((Rw[3] * ew[0] + Rw[4] * ew[1] + Rw[5] * ew[2]) / l0);
+  const R s3 = R((Rw[6] * ew[0] + Rw[7] * ew[1] + Rw[8] * ew[2]) / l0 - W(1));
+  const R GA = d.GA[j], EA = d.EA[j];
+  const R n1 = GA * s1, n2 = GA * s2, n3 = EA * s3;
+  R Rr[9];
+  for (int k = 0; k < 9; k++) Rr[k] = R(Rw[k]);
+  const R nv[3] = {n1 * Rr[0] + n2 * Rr[3] + n3 * Rr[6], n1 * Rr[1] + n2 * Rr[4] + n3 * Rr[7], n1 * Rr[2] + n2 * Rr[5] + n3 * Rr[8]};
+  const R e[3] = {R(ew[0]), R(ew[1]), R(ew[2])};
+  R en[3];
+  cross3(e, nv, en);
+  const int mt = d.mtot;
+  for (int k = 0; k < 3; k++) { d.nF[k * mt + j] = nv[k]; d.en[k * mt + j] = en[k]; }
+  d.Nax[j] = n3; d.Vsh[j] = n1; d.Vsh[mt + j] = n2;
+  const R l0r = d.l0[j];
+  pt.s[RS_STRETCH] += A(R(0.5) * l0r * n3 * s3);
+  pt.s[RS_SHEAR] += A(R(0.5) * l0r * (n1 * s1 + n2 * s2));
+  pt.x[RX_N] = mmax(pt.x[RX_N], A(mabs(n3)));
+}
+
+// relative rotation Ψ = log(q_a* ⊗ q_b) (rod_cosserat.js:33-45); the product in the wide type, the log in R
+template <int P>
+__device__ __forceinline__ typename Dev<P>::R relRot(const typename Dev<P>::W qa[4], const typename Dev<P>::W qb[4], typename Dev<P>::R psi[3]) {
+  using R = typename Dev<P>::R; using W = typename Dev<P>::W;
+  const W ac[4] = {qa[0], -qa[1], -qa[2], -qa[3]};
+  W pw[4];
+  qmul(ac, qb, pw);
+  R w = R(pw[0]), x = R(pw[1]), y = R(pw[2]), z = R(pw[3]);
+  if (w < R(0)) { w = -w; x = -x; y = -y; z = -z; }
+  const R s = msqrt(x * x + y * y + z * z), th = R(2) * matan2(s, w);
+  const R f = s > R(1e-12) ? th / s : R(2) / mmax(w, R(1e-12));
+  psi[0] = f * x; psi[1] = f * y; psi[2] = f * z;
+  return th;
+}
+
+// J_l⁻ᵀ(Ψ) m = m + ½ Ψ × m + β Ψ × (Ψ × m)
+template <class R>
+__device__ __forceinline__ void jlinvT(const R psi[3], const R m[3], R th, R j[3]) {
+  const R beta = jbeta(th);
+  R c[3], e[3];
+  cross3(psi, m, c);
+  cross3(psi, c, e);
+  for (int k = 0; k < 3; k++) j[k] = m[k] + R(0.5) * c[k] + beta * e[k];
+}
+
+// joint jt between segments sa -> sb (rod_cosserat.js:136-159)
+template <int P>
+__device__ __forceinline__ void jointTorque(const Dev<P> &d, int buf, int jt, Part<typename Dev<P>::A> &pt) {
+  using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A;
+  const int sa = d.jS0[jt], sb = d.jS1[jt], pt_ = d.ptot;
+  W qa[4], qb[4];
+  for (int k = 0; k < 4; k++) { qa[k] = Acc<P>::qw(d, buf, k, sa); qb[k] = Acc<P>::qw(d, buf, k, sb); }
+  R psi[3];
+  const R th = relRot<P>(qa, qb, psi);
+  const R lb = d.jLen[jt];
+  const R dd[3] = {psi[0] / lb - d.om[jt], psi[1] / lb - d.om[pt_ + jt], psi[2] / lb - d.om[2 * pt_ + jt]};
+  const R EIx = d.EIx[jt], EIy = d.EIy[jt], GJ = d.GJ[jt];
+  const R mm[3] = {EIx * dd[0], EIy * dd[1], GJ * dd[2]};
+  {
+    const R q0 = psi[0] * psi[0], q1 = psi[1] * psi[1], q2 = psi[2] * psi[2], f = R(0.25) / lb;
+    d.kd[jt] = f * (EIy * q2 + GJ * q1);
+    d.kd[pt_ + jt] = f * (EIx * q2 + GJ * q0);
+    d.kd[2 * pt_ + jt] = f * (EIx * q1 + EIy * q0);
+  }
+  R jv[3];
+  jlinvT(psi, mm, th, jv);
+  R qr[4], Ra[9];
+  for (int k = 0; k < 4; k++) qr[k] = R(qa[k]);
+  qframe(qr, Ra);
+  for (int k = 0; k < 3; k++) {
+    d.tau[k * pt_ + jt] = jv[0] * Ra[k] + jv[1] * Ra[3 + k] + jv[2] * Ra[6 + k];
+    d.Mj[k * pt_ + jt] = mm[k];
+  }
+  pt.s[RS_BEND] += A(R(0.5) * lb * (mm[0] * dd[0] + mm[1] * dd[1]));
+  pt.s[RS_TWIST] += A(R(0.5) * lb * mm[2] * dd[2]);
+  pt.x[RX_M] = mmax(pt.x[RX_M], A(mmax(mabs(mm[0]), mmax(mabs(mm[1]), mabs(mm[2])))));
+}
+
+// clamp joint cc: frozen frame (side a) -> segment frame j (side b) (rod_cosserat.js:161-180)
+template <int P>
+__device__ __forceinline__ void clampTorque(const Dev<P> &d, int buf, int cc, Part<typename Dev<P>::A> &pt) {
+  using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A;
+  const int j = d.cSeg[cc], ct = d.ctot;
+  W qa[4], qb[4];
+  for (int k = 0; k < 4; k++) { qa[k] = d.cQ[k * ct + cc]; qb[k] = Acc<P>::qw(d, buf, k, j); }
+  R psi[3];
+  const R th = relRot<P>(qa, qb, psi);
+  const R lc = d.cLen[cc];
+  const R dd[3] = {psi[0] / lc, psi[1] / lc, psi[2] / lc};
+  const R mm[3] = {d.cB[cc] * dd[0], d.cB[ct + cc] * dd[1], d.cB[2 * ct + cc] * dd[2]};
+  R jv[3];
+  jlinvT(psi, mm, th, jv);
+  R qr[4], Rc[9];
+  for (int k = 0; k < 4; k++) qr[k] = R(qa[k]);
+  qframe(qr, Rc);
+  for (int k = 0; k < 3; k++) d.tauC[k * ct + cc] = jv[0] * Rc[k] + jv[1] * Rc[3 + k] + jv[2] * Rc[6 + k];
+  d.cM[cc] = mm[0]; d.cM[ct + cc] = mm[1];
+  pt.s[RS_BEND] += A(R(0.5) * lc * (mm[0] * dd[0] + mm[1] * dd[1]));
+  pt.s[RS_TWIST] += A(R(0.5) * lc * mm[2] * dd[2]);
+}
+
+// half-extent h(n) and smoothed support point r of a section (PolylineContact._support, solver_cpu.js:274-282)
+template <class R>
+__device__ __forceinline__ R support(const R Rf[9], const R n[3], R sign, R w, R h, R r[3]) {
+  const R nx = (n[0] * Rf[0] + n[1] * Rf[1] + n[2] * Rf[2]) * sign, ny = (n[0] * Rf[3] + n[1] * Rf[4] + n[2] * Rf[5]) * sign;
+  const R hh = R(0.5) * w * mabs(nx) + R(0.5) * h * mabs(ny);
+  const R ax = R(0.5) * w * mtanh(nx / R(SUPPORT_SMOOTH)), ay = R(0.5) * h * mtanh(ny / R(SUPPORT_SMOOTH));
+  for (int k = 0; k < 3; k++) r[k] = ax * Rf[k] + ay * Rf[3 + k];
+  return hh;
+}
+
+// crossing c: one evaluation of PolylineContact.apply (solver_cpu.js:381-478) without the seat law, the augmented
+// Lagrangian and the rotational friction
+template <int P>
+__device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int buf, int iter, int c, Part<typename Dev<P>::A> &pt) {
+  using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A; using U = typename Dev<P>::U;
+  const int kt_ = d.ktot;
+  const double rampN = I.ramp_iter;
+  const double rampd = rampN <= 0 ? 1.0 : fmin(1.0, 0.01 + 0.99 * double(iter) / rampN);
+  const R kn = R(rampd * I.strength), kt = R(rampd * I.stick);
+  R Pl[2][3], tg[2][3], Rf[2][9], L[2], tp[2];
+  int seg[2], base[2], nseg[2];
+  U uu[2];
+  for (int side = 0; side < 2; side++) {
+    const int o = side * kt_ + c;
+    uu[side] = d.u[o];
+    nseg[side] = d.cxNseg[o];
+    const int li = int(mmin(mmax(mfloor(uu[side]), U(0)), U(mmax(nseg[side] - 1, 0))));
+    const R t = R(mmin(mmax(uu[side] - U(li), U(0)), U(1)));
+    const int sg = d.cxSegOff[o] + li;
+    const int a = d.segI0[sg], b = d.segI1[sg];
+    R e[3], Ta[3], Tb[3];
+    Acc<P>::edge(d, buf, a, b, e);
+    const R Ls = msqrt(dot3(e, e));
+    nodeTangent<P>(d, buf, a, Ta);
+    nodeTangent<P>(d, buf, b, Tb);
+    const R t2 = t * t, t3 = t2 * t;
+    const R h10 = t3 - R(2) * t2 + t, h01 = R(-2) * t3 + R(3) * t2, h11 = t3 - t2;
+    const R d10 = R(3) * t2 - R(4) * t + R(1), d01 = R(-6) * t2 + R(6) * t, d11 = R(3) * t2 - R(2) * t;
+    for (int k = 0; k < 3; k++) {
+      Pl[side][k] = h01 * e[k] + (h10 * Ls) * Ta[k] + (h11 * Ls) * Tb[k];
+      tg[side][k] = d01 * e[k] + (d10 * Ls) * Ta[k] + (d11 * Ls) * Tb[k];
+    }
+    const R tl = mmax(msqrt(dot3(tg[side], tg[side])), R(1e-12));
+    for (int k = 0; k < 3; k++) tg[side][k] /= tl;
+    R qa[4], qb[4], q[4], Rn[9];
+    nodeQuat<P>(d, buf, a, qa);
+    nodeQuat<P>(d, buf, b, qb);
+    const R sgn = (qa[0] * qb[0] + qa[1] * qb[1] + qa[2] * qb[2] + qa[3] * qb[3]) < R(0) ? R(-1) : R(1);
+    for (int k = 0; k < 4; k++) q[k] = (R(1) - t) * qa[k] + t * sgn * qb[k];
+    qnormalize(q);
+    qframe(q, Rn);
+    R y[3] = {Rn[3], Rn[4], Rn[5]};
+    const R yt = dot3(y, tg[side]);
+    for (int k = 0; k < 3; k++) y[k] -= yt * tg[side][k];
+    const R yl = mmax(msqrt(dot3(y, y)), R(1e-12));
+    for (int k = 0; k < 3; k++) y[k] /= yl;
+    R x[3];
+    cross3(y, tg[side], x);
+    for (int k = 0; k < 3; k++) { Rf[side][k] = x[k]; Rf[side][3 + k] = y[k]; Rf[side][6 + k] = tg[side][k]; }
+    L[side] = Ls; tp[side] = t; seg[side] = sg; base[side] = a;
+  }
+  const R *tA = tg[0], *tB = tg[1];
+  // contact normal with side persistence (solver_cpu.js:396-402)
+  R nv[3];
+  cross3(tA, tB, nv);
+  R np[3] = {d.nPrev[c], d.nPrev[kt_ + c], d.nPrev[2 * kt_ + c]};
+  const R nn = msqrt(dot3(nv, nv));
+  if (nn < R(1e-6)) { nv[0] = np[0]; nv[1] = np[1]; nv[2] = np[2]; }
+  else { const R dn = mmax(nn, R(1e-12)); nv[0] /= dn; nv[1] /= dn; nv[2] /= dn; }
+  if (dot3(nv, np) < R(0)) { nv[0] = -nv[0]; nv[1] = -nv[1]; nv[2] = -nv[2]; }
+  for (int k = 0; k < 3; k++) d.nPrev[k * kt_ + c] = nv[k];
+  // gap vector P_B − P_A: the base-node difference in the wide type
+  R S[3];
+  for (int k = 0; k < 3; k++) S[k] = R(Acc<P>::xw(d, buf, k, base[1]) - Acc<P>::xw(d, buf, k, base[0])) + (Pl[1][k] - Pl[0][k]);
+  const R g = dot3(S, nv);
+  R rA[3], rB[3];
+  const R hA = support(Rf[0], nv, R(1), d.wk[c], d.hk[c], rA);
+  const R hB = support(Rf[1], nv, R(-1), d.wk[kt_ + c], d.hk[kt_ + c], rB);
+  const R pen = (hA + hB) - g;
+  const uint8_t fl = d.cflag[c];
+  const bool enabled = fl & 1, locked = fl & 2;
+  const bool active = (pen > R(0) || locked) && enabled;
+  const R Fn = active ? kn * pen : R(0);
+  // tangential spring / stick-slip: S_t = a tA + b tB
+  const R St[3] = {S[0] - g * nv[0], S[1] - g * nv[1], S[2] - g * nv[2]};
+  const R taa = dot3(tA, tA), tbb = dot3(tB, tB), tab = dot3(tA, tB);
+  const R sa = dot3(St, tA), sb = dot3(St, tB);
+  const R det = taa * tbb - tab * tab;
+  const bool ok = det > R(1e-8);
+  const R ca = ok ? (sa * tbb - sb * tab) / det : R(0), cb = ok ? (sb * taa - sa * tab) / det : R(0);
+  const R Ftv = msqrt((kt * St[0]) * (kt * St[0]) + (kt * St[1]) * (kt * St[1]) + (kt * St[2]) * (kt * St[2]));
+  const R limit = d.mu[c] * mabs(Fn);
+  const bool slip = active && ok && !locked && Ftv > limit;
+  const bool freeS = !active && ok && enabled;
+  R scale = R(0);
+  if (slip) scale = R(mclamp(I.slip_rate, 1e-3, 1.0)) * (R(1) - limit / mmax(Ftv, R(1e-12)));
+  if (freeS) scale = R(1);
+  const R eps = R(fmax(I.eps, 1e-9));
+  const R da = mclamp(ca * scale, -eps, eps), db = mclamp(cb * scale, -eps, eps);
+  const bool moved = slip || freeS;
+  if (moved) { uu[0] += U(da) / U(mmax(L[0], R(1e-12))); uu[1] -= U(db) / U(mmax(L[1], R(1e-12))); }
+  d.u[c] = mclamp(uu[0], U(0), U(nseg[0]));
+  d.u[kt_ + c] = mclamp(uu[1], U(0), U(nseg[1]));
+  if (slip) {
+    const R sx = da * tA[0] + db * tB[0], sy = da * tA[1] + db * tB[1], sz = da * tA[2] + db * tB[2];
+    d.slip[c] += A(msqrt(sx * sx + sy * sy + sz * sz));
+  }
+  d.stuck[c] = moved ? 0 : 1;
+  R Se[3] = {R(0), R(0), R(0)};
+  if (active) for (int k = 0; k < 3; k++) Se[k] = St[k] - da * tA[k] - db * tB[k];
+  const R fT[3] = {kt * Se[0], kt * Se[1], kt * Se[2]};
+  R FA[3];
+  for (int k = 0; k < 3; k++) FA[k] = -Fn * nv[k] + fT[k];
+  d.Fn[c] = Fn;
+  d.Ft[c] = msqrt(dot3(fT, fT));
+  d.cstate[c] = slip ? 1 : 0;
+  d.gap[c] = g;
+  // side records for the gathers: segment and t before the slide, force on the side, lever torque tf (r × F)
+  const R tf = R(I.tf);
+  const int K2 = 2 * kt_;
+  for (int side = 0; side < 2; side++) {
+    const int sd = 2 * c + side;
+    const R sgn = side ? R(-1) : R(1);
+    const R F[3] = {sgn * FA[0], sgn * FA[1], sgn * FA[2]};
+    R tq[3];
+    cross3(side ? rB : rA, F, tq);
+    d.sSeg[sd] = seg[side];
+    d.sT[sd] = tp[side];
+    for (int k = 0; k < 3; k++) { d.sF[k * K2 + sd] = F[k]; d.sTq[k * K2 + sd] = tf * tq[k]; }
+  }
+  // righting stiffness of the support point (addTwistStiffness, solver_cpu.js:170-176): goes to the segments the
+  // sides sit on after the slide
+  const R tfc = R(fmax(I.tf, 1e-3)), hc = d.ch[c], wc = d.cw[c];
+  d.kth[c] = tfc * ((Fn + kn * R(0.25) * hc) * (R(0.5) * wc) / R(SUPPORT_SMOOTH) + kt * (R(0.5) * hc) * (R(0.5) * hc));
+  pt.s[RS_PEN] += A(active ? kn * pen * pen : R(0));
+  pt.s[RS_TAN] += A(dot3(Se, Se));
+  pt.x[RX_FN] = mmax(pt.x[RX_FN], A(Fn));
+}
+
+// ------------------------------------------------------------------------------------------------ phase B / C
+// local segment of a side from its slide coordinate (solver_cpu.js:144-149)
+template <int P>
+__device__ __forceinline__ int sideSeg(const Dev<P> &d, int sd) {
+  using U = typename Dev<P>::U;
+  const int c = sd >> 1, side = sd & 1, o = side * d.ktot + c;
+  const U u = d.u[o];
+  const int ns = d.cxNseg[o];
+  return int(mmin(mmax(mfloor(u), U(0)), U(mmax(ns - 1, 0))));
+}
+// strand s: sides re-sorted by (segment, side id) from the order of the last iteration (insertion sort: the order
+// changes only where a crossing passes a segment end)
+template <int P>
+__device__ __forceinline__ void sortStrand(const Dev<P> &d, int s, int src, int dst) {
+  const int off = d.stSideOff[s], cnt = d.stSideCnt[s], K2 = 2 * d.ktot;
+  const int *oi = d.ord + size_t(src) * K2 + off;
+  int *oo = d.ord + size_t(dst) * K2 + off, *os = d.ordSeg + size_t(dst) * K2 + off;
+  for (int i = 0; i < cnt; i++) {
+    const int sd = oi[i], key = sideSeg<P>(d, sd);
+    int k = i;
+    while (k > 0 && (os[k - 1] > key || (os[k - 1] == key && oo[k - 1] > sd))) { oo[k] = oo[k - 1]; os[k] = os[k - 1]; k--; }
+    oo[k] = sd; os[k] = key;
+  }
+}
+template <int P>
+__device__ __forceinline__ void segRange(const Dev<P> &d, int j, int dst) {
+  const int s = d.segStrand[j], lj = d.segLocal[j], K2 = 2 * d.ktot;
+  const int off = d.stSideOff[s], cnt = d.stSideCnt[s];
+  const int *os = d.ordSeg + size_t(dst) * K2 + off;
+  int lo = 0, hi = cnt;
+  while (lo < hi) { const int mid = (lo + hi) >> 1; if (os[mid] < lj) lo = mid + 1; else hi = mid; }
+  int lo2 = lo, hi2 = cnt;
+  while (lo2 < hi2) { const int mid = (lo2 + hi2) >> 1; if (os[mid] <= lj) lo2 = mid + 1; else hi2 = mid; }
+  d.rngLo[size_t(dst) * d.mtot + j] = off + lo;
+  d.rngHi[size_t(dst) * d.mtot + j] = off + lo2;
+}
+
+// ------------------------------------------------------------------------------------------------ phase D
+struct StepCtx {
+  int cur, nxt, obuf, onxt, pending, iter, warm;
+  double dispR;      // prescribed-motion fraction of this iteration
+};
+
+template <int P>
+__device__ __forceinline__ void nodeUpdate(const Dev<P> &d, const InstDesc &I, const StepCtx &sc, int i, Part<typename Dev<P>::A> &pt) {
+  using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A;
+  const int nt = d.ntot, mt = d.mtot, K2 = 2 * d.ktot;
+  const int so = d.nsOut[i], si = d.nsIn[i];
+  const uint8_t fl = d.nflag[i];
+  R F[3] = {R(0), R(0), R(0)};
+  if (so >= 0) for (int k = 0; k < 3; k++) F[k] += d.nF[k * mt + so];
+  if (si >= 0) for (int k = 0; k < 3; k++) F[k] -= d.nF[k * mt + si];
+  R tot[3] = {d.lc[i], d.lc[nt + i], d.lc[2 * nt + i]};
+  if (fl & 16) {                          // load in the node frame (solver_cpu.js:755-758)
+    R q[4], Rn[9];
+    nodeQuat<P>(d, sc.cur, i, q);
+    qframe(q, Rn);
+    const R f0 = d.ll[i], f1 = d.ll[nt + i], f2 = d.ll[2 * nt + i];
+    for (int k = 0; k < 3; k++) tot[k] += Rn[k] * f0 + Rn[3 + k] * f1 + Rn[6 + k] * f2;
+  }
+  for (int k = 0; k < 3; k++) F[k] += tot[k];
+  pt.x[RX_LOAD] = mmax(pt.x[RX_LOAD], A(mmax(mabs(tot[0]), mmax(mabs(tot[1]), mabs(tot[2])))));
+  // crossing sides on the adjacent segments, as distributed by the last evaluation (weights 1 − t at a, t at b)
+  const bool cx = I.contacts && I.K;
+  if (cx && so >= 0) {
+    const int lo = d.rngLo[size_t(sc.obuf) * mt + so], hi = d.rngHi[size_t(sc.obuf) * mt + so];
+    for (int e = lo; e < hi; e++) {
+      const int sd = d.ord[size_t(sc.obuf) * K2 + e];
+      const R wgt = R(1) - d.sT[sd];
+      for (int k = 0; k < 3; k++) F[k] += wgt * d.sF[k * K2 + sd];
+    }
+  }
+  if (cx && si >= 0) {
+    const int lo = d.rngLo[size_t(sc.obuf) * mt + si], hi = d.rngHi[size_t(sc.obuf) * mt + si];
+    for (int e = lo; e < hi; e++) {
+      const int sd = d.ord[size_t(sc.obuf) * K2 + e];
+      const R wgt = d.sT[sd];
+      for (int k = 0; k < 3; k++) F[k] += wgt * d.sF[k * K2 + sd];
+    }
+  }
+  if (fl & 8) for (int k = 0; k < 3; k++) d.react[k * nt + i] = -F[k];
+  for (int k = 0; k < 3; k++) if (!(fl & (1 << k))) F[k] = R(0);
+  pt.x[RX_F] = mmax(pt.x[RX_F], A(msqrt(dot3(F, F))));
+  R v[3];
+  for (int k = 0; k < 3; k++) v[k] = sc.pending || sc.warm ? R(0) : d.V[k * nt + i];
+  const R m = d.mass[i];
+  if (!sc.warm) for (int k = 0; k < 3; k++) v[k] += F[k] / m;
+  if (I.damping != 1.0) for (int k = 0; k < 3; k++) v[k] *= R(I.damping);
+  for (int k = 0; k < 3; k++) if (!(fl & (1 << k))) v[k] = R(0);
+  const int ai = (fl & 32) ? d.anc[i] : -1;
+  for (int k = 0; k < 3; k++) {
+    d.V[k * nt + i] = v[k];
+    W x = Acc<P>::xw(d, sc.cur, k, i) + W(v[k]);
+    if (ai >= 0 && !(fl & (1 << k))) x = d.ancStart[size_t(k) * nt + ai] + W(sc.dispR) * d.ancDelta[size_t(k) * nt + ai];
+    Acc<P>::xs(d, sc.nxt, k, i, x);
+  }
+  pt.s[RS_KE] += A(m) * (A(v[0]) * A(v[0]) + A(v[1]) * A(v[1]) + A(v[2]) * A(v[2]));
+}
+
+template <int P>
+__device__ __forceinline__ void segUpdate(const Dev<P> &d, const InstDesc &I, const StepCtx &sc, int j, Part<typename Dev<P>::A> &pt) {
+  using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A;
+  const int mt = d.mtot, pt_ = d.ptot, ct = d.ctot, K2 = 2 * d.ktot;
+  R T[3] = {d.en[j], d.en[mt + j], d.en[2 * mt + j]};
+  R kD[3] = {R(0), R(0), R(0)};
+  const int ja = d.jA[j], jb = d.jB[j];
+  if (ja >= 0) for (int k = 0; k < 3; k++) { T[k] += d.tau[k * pt_ + ja]; kD[k] += d.kd[k * pt_ + ja]; }
+  if (jb >= 0) for (int k = 0; k < 3; k++) { T[k] -= d.tau[k * pt_ + jb]; kD[k] += d.kd[k * pt_ + jb]; }
+  const int c0 = d.cl0[j], c1 = d.cl1[j];
+  if (c0 >= 0) for (int k = 0; k < 3; k++) T[k] -= d.tauC[k * ct + c0];
+  if (c1 >= 0) for (int k = 0; k < 3; k++) T[k] -= d.tauC[k * ct + c1];
+  R kTw = R(0);
+  if (I.contacts && I.K) {
+    const int lo = d.rngLo[size_t(sc.obuf) * mt + j], hi = d.rngHi[size_t(sc.obuf) * mt + j];
+    for (int e = lo; e < hi; e++) {
+      const int sd = d.ord[size_t(sc.obuf) * K2 + e];
+      for (int k = 0; k < 3; k++) T[k] += d.sTq[k * K2 + sd];
+    }
+    const int lo2 = d.rngLo[size_t(sc.onxt) * mt + j], hi2 = d.rngHi[size_t(sc.onxt) * mt + j];
+    for (int e = lo2; e < hi2; e++) kTw += d.kth[d.ord[size_t(sc.onxt) * K2 + e] >> 1];
+  }
+  R q[4], Rm[9];
+  for (int k = 0; k < 4; k++) q[k] = Acc<P>::qr(d, sc.cur, k, j);
+  qframe(q, Rm);
+  R tm[3];
+  for (int k = 0; k < 3; k++) tm[k] = Rm[3 * k] * T[0] + Rm[3 * k + 1] * T[1] + Rm[3 * k + 2] * T[2];
+  pt.x[RX_T] = mmax(pt.x[RX_T], A(msqrt(dot3(tm, tm))));
+  const R ms = R(I.ms);
+  R w[3], I3[3];
+  for (int k = 0; k < 3; k++) {
+    I3[k] = ms * mmax(d.krs[k * mt + j] + kTw + kD[k], R(1e-12));
+    w[k] = (sc.pending ? R(0) : d.Wr[k * mt + j]) + tm[k] / I3[k];
+  }
+  w[2] = mclamp(w[2], R(-TWIST_RATE_MAX), R(TWIST_RATE_MAX));
+  if (kTw > R(0)) w[2] *= R(ROLL_DAMP);
+  if (I.damping != 1.0) for (int k = 0; k < 3; k++) w[k] *= R(I.damping);
+  for (int k = 0; k < 3; k++) d.Wr[k * mt + j] = w[k];
+  // q ← normalize(q ⊗ exp(ω)) in the wide type; the increment q ⊗ (exp(ω) − 1) is small, formed in R
+  const R a = msqrt(dot3(w, w)), half = R(0.5) * a;
+  R sh, ch;
+  msincos(half, &sh, &ch);
+  const R s = a > R(1e-12) ? sh / a : R(0.5);
+  W qn[4];
+  if constexpr (P != PREC_MIXED) {
+    const W dq[4] = {ch, w[0] * s, w[1] * s, w[2] * s};
+    W qw[4];
+    for (int k = 0; k < 4; k++) qw[k] = Acc<P>::qw(d, sc.cur, k, j);
+    qmul(qw, dq, qn);
+  } else {
+    R sq, cq;
+    msincos(R(0.5) * half, &sq, &cq);
+    const R dm1[4] = {R(-2) * sq * sq, w[0] * s, w[1] * s, w[2] * s};
+    R inc[4];
+    qmul(q, dm1, inc);
+    for (int k = 0; k < 4; k++) qn[k] = Acc<P>::qw(d, sc.cur, k, j) + W(inc[k]);
+  }
+  qnormalize(qn);
+  for (int k = 0; k < 4; k++) Acc<P>::qs(d, sc.nxt, k, j, qn[k]);
+  pt.s[RS_KE] += A(I3[0]) * A(w[0]) * A(w[0]) + A(I3[1]) * A(w[1]) * A(w[1]) + A(I3[2]) * A(w[2]) * A(w[2]);
+}
+
+// ------------------------------------------------------------------------------------------------ reductions
+template <class A>
+__device__ __forceinline__ void warpReduce(Part<A> &p) {
+  for (int o = 16; o > 0; o >>= 1) {
+    for (int i = 0; i < RS_NSUM; i++) p.s[i] += __shfl_xor_sync(0xffffffffu, p.s[i], o);
+    for (int i = 0; i < RX_NMAX; i++) p.x[i] = mmax(p.x[i], __shfl_xor_sync(0xffffffffu, p.x[i], o));
+  }
+}
+// block-wide reduction in a fixed order; the result is valid in thread 0 (smem: >= 32 * (RS_NSUM + RX_NMAX) values)
+template <class A>
+__device__ __forceinline__ void blockReduce(Part<A> &p, A *smem) {
+  warpReduce(p);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  constexpr int NV = RS_NSUM + RX_NMAX;
+  if (lane == 0) {
+    for (int i = 0; i < RS_NSUM; i++) smem[wid * NV + i] = p.s[i];
+    for (int i = 0; i < RX_NMAX; i++) smem[wid * NV + RS_NSUM + i] = p.x[i];
+  }
+  __syncthreads();
+  if (wid == 0) {
+    Part<A> q;
+    q.init();
+    if (lane < nw) {
+      for (int i = 0; i < RS_NSUM; i++) q.s[i] = smem[lane * NV + i];
+      for (int i = 0; i < RX_NMAX; i++) q.x[i] = smem[lane * NV + RS_NSUM + i];
+    }
+    warpReduce(q);
+    if (lane == 0) p = q;
+  }
+  __syncthreads();
+}
+
+// ------------------------------------------------------------------------------------------------ phase E
+// kinetic-damping decision, residual and convergence of one instance from its reduced partials (solver_cpu.js:809-837)
+template <class A>
+__device__ __forceinline__ void decide(const InstDesc &I, InstCtl &c, const Part<A> &p, int n_iter_stop) {
+  double ke = 0.5 * double(p.s[RS_KE]);
+  const bool rollback = I.kd && ke < c.ke_prev;
+  if (!isfinite(ke)) { c.status = WS_NONFINITE; }
+  if (rollback) { ke = 0.0; c.pending = 1; c.rollbacks++; }
+  else { c.pending = 0; c.cur ^= 1; }
+  c.obuf ^= 1;
+  c.ke = ke; c.ke_prev = ke;
+  c.iter += 1;
+  const double maxM = I.p ? double(p.x[RX_M]) / fmax(I.jLenMin, 1e-12) : 0.0;
+  const double maxFn = (I.contacts && I.K) ? double(p.x[RX_FN]) : 0.0;
+  const double fref = fmax(fmax(fmax(double(p.x[RX_LOAD]), double(p.x[RX_N])), fmax(maxM, maxFn)), 1e-12);
+  c.fref = fref;
+  c.res_f = I.n ? double(p.x[RX_F]) / fref : 0.0;
+  c.res_t = I.m ? double(p.x[RX_T]) / (fref * I.lRef) : 0.0;
+  const double resid = fmax(c.res_f, c.res_t);
+  c.residual = c.iter > I.warmup ? resid : INFINITY;
+  c.e_stretch = double(p.s[RS_STRETCH]); c.e_shear = double(p.s[RS_SHEAR]);
+  c.e_bend = double(p.s[RS_BEND]); c.e_twist = double(p.s[RS_TWIST]);
+  // contact energy of the iteration: ½ Σ k_n pen² + ½ k_t Σ |S_e|² with the ramp of that iteration
+  const double rampd = I.ramp_iter <= 0 ? 1.0 : fmin(1.0, 0.01 + 0.99 * double(c.iter - 1) / I.ramp_iter);
+  c.e_contact = 0.5 * double(p.s[RS_PEN]) + 0.5 * rampd * I.stick * double(p.s[RS_TAN]);
+  if (c.status == WS_RUNNING) {
+    if (c.residual <= I.tol) c.status = WS_CONVERGED;
+    else if (c.iter >= I.max_iter) c.status = WS_MAX_ITER;
+  }
+  (void)n_iter_stop;
+}
+
+template <class A>
+__device__ __forceinline__ StepCtx makeCtx(const InstDesc &I, const InstCtl &c) {
+  StepCtx sc;
+  sc.cur = c.cur; sc.nxt = c.cur ^ 1; sc.obuf = c.obuf; sc.onxt = c.obuf ^ 1; sc.pending = c.pending; sc.iter = c.iter;
+  sc.warm = (c.iter < I.warmup && I.contacts && I.K) ? 1 : 0;
+  const int start = max(c.disp_it0, (I.contacts && I.K) ? I.warmup : 0);
+  sc.dispR = I.disp_ramp > 0 ? fmin(1.0, fmax(0.0, double(c.iter - start + 1) / I.disp_ramp)) : 1.0;
+  return sc;
+}
+
+}  // namespace wsb

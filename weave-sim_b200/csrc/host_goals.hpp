@@ -1,0 +1,63 @@
+// Host-side goal assembly of one instance (f64): everything the device step needs that is built once per model or per
+// warm start — node masses and static frame inertias (CpuSolver._buildGoals, web/js/solver_cpu.js:670-710), clamp
+// joints (CosseratRod.setClamps, web/js/rod_cosserat.js:92-100), anchors (Anchors, web/js/model.js:162-189), the
+// contact initialisation (PolylineContact.initialize, web/js/solver_cpu.js:99-139) and the static gather tables
+// (segment -> joints / clamps, node -> segments, crossing sides sorted along their strand).
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "../../include/weavesim.h"
+
+namespace wsb {
+
+struct HostGoals {
+  // sizes
+  int n = 0, m = 0, p = 0, S = 0, K = 0, C = 0;
+  ws_params prm{};
+  // state (f64)
+  std::vector<double> X, X0, Q, u, nPrev;
+  // rod
+  std::vector<double> l0, jLen, omega0, EA, GA, EIx, EIy, GJ;   // EIx/EIy/GJ per joint (joint's first segment)
+  std::vector<int> segI0, segI1, jSeg0, jSeg1, segOffset;
+  // clamps (rotation anchors): segment, half length, per-axis stiffness, frozen frame, node
+  std::vector<int> cSeg, cNode;
+  std::vector<double> cLen, cB, cQ;
+  // loads
+  std::vector<double> loadConst, loadLocal;          // loadLocal [3n]: node-frame force (zero where none)
+  std::vector<uint8_t> hasLocal;
+  // anchors
+  std::vector<uint8_t> nodeFree;                     // [3n] 1 = free
+  std::vector<uint8_t> fixedAny;                     // [n]
+  std::vector<int> ancIndex;                         // [n] -> prescribed-motion slot or -1
+  std::vector<double> ancStart, ancDelta;            // [3 * slots]
+  // contact
+  std::vector<int> cxSegOff, cxNseg, cxStrand;       // [2K] first segment, segment count and strand of each side
+  std::vector<double> wk, hk, w, h, mu;
+  std::vector<uint8_t> enabled, locked;
+  // goals
+  std::vector<double> mass, kRotStatic;              // [n], [3m]
+  double lRef = 1.0, jLenMin = 1.0, loadMaxConst = 0.0;
+  // gather tables
+  std::vector<int> nodeSegOut, nodeSegIn;            // [n] segment with seg_i0 = i / seg_i1 = i (-1 none)
+  std::vector<int> segJointA, segJointB;             // [m] joint whose first / second segment this is (-1 none)
+  std::vector<int> segClamp0, segClamp1;             // [m] clamps acting on the segment (-1 none)
+  std::vector<int> segStrand, segLocal;              // [m]
+  std::vector<int> strandSideOff, strandSideCnt;     // [S] slice of the sorted side list
+  std::vector<int> ord, ordSeg;                      // [2K] side ids (2c + side) sorted by (local segment, id) per strand
+  std::vector<int> rngLo, rngHi;                     // [m] slice of ord on the segment
+
+  void build(const ws_model &md);                    // everything, including the contact initialisation
+  void rebuild(const ws_model &md);                  // warm start: new stiffness / loads / parameters, state kept
+  void sortSides();                                  // ord / ordSeg / rngLo / rngHi from u
+  int sideSegLocal(int sd) const;                    // local segment of side sd from u (solver_cpu.js:144-149)
+
+ private:
+  void loadModel(const ws_model &md, bool keepState);
+  void buildAnchors(const ws_model &md);
+  void buildTargets(const ws_model &md);
+  void buildMasses(double ramp, const std::vector<double> &Fn);
+  void contactInitialize(int sweeps = 3);
+};
+
+}  // namespace wsb

@@ -1,0 +1,134 @@
+"""GpuSolver: the reference's batched solver interface (web/js/solver_gpu.js:62-523) over the C ABI of
+include/weavesim.h.
+
+    solver = GpuSolver([model, ...], precision="mixed", form="cta")
+    ctl = solver.step(1000)             # GpuSolver.step: runs up to n iterations, each instance stops at convergence
+    state = solver.download(0)          # GpuSolver.download: positions, frames, slide coordinates, stick/slip, forces
+    solver.update_params(0, variant)    # GpuSolver.updateParams + CpuSolver.rebuildGoals: warm start
+    solver.internalize(0)               # CpuSolver.internalize / GpuSolver.internalize
+
+Unlike the reference, the instances of one solver need not share a topology (uneven gridshells in one launch).
+Every call goes to the CUDA library; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import WsControl, WsOpts, WsStateOut, check, lib
+
+STATUS = {0: "running", 1: "converged", 2: "max_iter", 3: "non_finite"}
+
+
+def device_count() -> int:
+    return int(lib().ws_device_count())
+
+
+class GpuSolver:
+    def __init__(self, models, precision="mixed", form="cta", threads=0, device=0, budget_bytes=0):
+        if not isinstance(models, (list, tuple)):
+            models = [models]
+        self.models = list(models)
+        self.B = len(self.models)
+        self._structs = [m.struct() for m in self.models]
+        arr = (C.POINTER(_lib.WsModel) * self.B)(*[C.pointer(s) for s in self._structs])
+        opts = WsOpts()
+        opts.precision = _lib.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        opts.form = _lib.FORMS[form] if isinstance(form, str) else int(form)
+        opts.threads, opts.device, opts.budget_bytes = int(threads), int(device), int(budget_bytes)
+        self.precision, self.form = precision, form
+        h = C.c_void_p()
+        check(lib().ws_create(arr, self.B, C.byref(opts), C.byref(h)), "ws_create")
+        self.h = h
+
+    # ------------------------------------------------------------------------------------------- running
+    def step(self, n_iter, instances=None, read=True):
+        """Up to n_iter DR iterations on the selected instances (all by default); returns the control blocks."""
+        mask = None
+        if instances is not None:
+            m = np.zeros(self.B, dtype=np.uint8)
+            m[list(instances)] = 1
+            mask = m.ctypes.data_as(C.POINTER(C.c_uint8))
+            self._mask = m
+        ctl = (WsControl * self.B)() if read else None
+        check(lib().ws_step(self.h, int(n_iter), mask, ctl), "ws_step")
+        return [c.as_dict() for c in ctl] if read else None
+
+    def read_control(self):
+        ctl = (WsControl * self.B)()
+        check(lib().ws_read_control(self.h, ctl), "ws_read_control")
+        return [c.as_dict() for c in ctl]
+
+    def run(self, max_iter=None, chunk=1000, instances=None):
+        """step() in chunks until every selected instance has stopped (GpuSolver in app.js / calibrate.js loops)."""
+        max_iter = max_iter or max(m.params["max_iter"] for m in self.models)
+        done = 0
+        ctl = self.read_control()
+        sel = list(range(self.B)) if instances is None else list(instances)
+        while done < max_iter:
+            k = min(chunk, max_iter - done)
+            ctl = self.step(k, instances=sel)
+            done += k
+            if all(ctl[b]["status"] != 0 for b in sel):
+                break
+        return ctl
+
+    def last_step_stats(self):
+        ms = C.c_double()
+        nl = C.c_int64()
+        check(lib().ws_last_step_stats(self.h, C.byref(ms), C.byref(nl)), "ws_last_step_stats")
+        return ms.value, nl.value
+
+    # ------------------------------------------------------------------------------------------- state
+    def download(self, b=0) -> dict:
+        md = self.models[b]
+        n, m, p, K = md.n, md.m, md.p, md.K
+        out = {"X": np.zeros(3 * n), "Q": np.zeros(4 * m), "V": np.zeros(3 * n), "W": np.zeros(3 * m),
+               "u": np.zeros(2 * K), "nprev": np.zeros(3 * K), "slip": np.zeros(K), "Fn": np.zeros(K), "Ft": np.zeros(K),
+               "gap": np.zeros(K), "N": np.zeros(m), "Vsh": np.zeros(2 * m), "M": np.zeros(3 * p),
+               "reactions": np.zeros(3 * n), "stuck": np.zeros(K, dtype=np.uint8), "state": np.zeros(K, dtype=np.uint8)}
+        so = WsStateOut()
+        for k, a in out.items():
+            ct = C.c_uint8 if a.dtype == np.uint8 else C.c_double
+            setattr(so, k, a.ctypes.data_as(C.POINTER(ct)) if a.size else None)
+        check(lib().ws_download(self.h, int(b), C.byref(so)), "ws_download")
+        return out
+
+    def upload_state(self, b, X, Q, u=None):
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        Q = np.ascontiguousarray(Q, dtype=np.float64)
+        up = None if u is None else np.ascontiguousarray(u, dtype=np.float64)
+        dp = C.POINTER(C.c_double)
+        check(lib().ws_upload_state(self.h, int(b), X.ctypes.data_as(dp), Q.ctypes.data_as(dp),
+                                    None if up is None else up.ctypes.data_as(dp)), "ws_upload_state")
+
+    def update_params(self, b, model):
+        """warm start with the stiffness, loads, friction, parameters and support targets of `model`"""
+        st = model.struct()
+        self._keep = (model, st)
+        check(lib().ws_set_params(self.h, int(b), C.byref(st)), "ws_set_params")
+        self.models[b] = model
+
+    def internalize(self, b):
+        check(lib().ws_internalize(self.h, int(b)), "ws_internalize")
+
+    @property
+    def stream(self):
+        return lib().ws_stream(self.h)
+
+    @property
+    def device_bytes(self):
+        return int(lib().ws_device_bytes(self.h))
+
+    def dispose(self):
+        h, self.h = getattr(self, "h", None), None
+        if h:
+            lib().ws_destroy(h)
+
+    def __del__(self):
+        try:
+            self.dispose()
+        except Exception:
+            pass
