@@ -38,7 +38,7 @@ extern "C" {
 
 /* execution form */
 #define WS_FORM_CTA 0        /* persistent fused kernel, one thread block per instance (batched) */
-#define WS_FORM_GRID 1       /* persistent fused kernel, one instance over a cooperative grid (large instance) */
+#define WS_FORM_GRID 1       /* persistent fused kernel, one instance over a cooperative grid with bounded grid barriers */
 #define WS_FORM_PLAIN 2      /* one kernel per phase per iteration, one instance (the plain GPU form) */
 
 /* ------------------------------------------------------------------------------------------------ parameters */
@@ -240,6 +240,10 @@ int ws_upload_state(ws_ctx *ctx, int32_t instance, const double *X, const double
  * state; the kinetic-energy peak and the convergence flag are reset.  Anchored nodes move to model->X where their
  * translation is fixed (prescribed displacement).  The topology must be the instance's. */
 int ws_set_params(ws_ctx *ctx, int32_t instance, const ws_model *model);
+/* Replaces instance b by a new model with the same element counts (a serving slot taking its next request): goals,
+ * contact initialisation, state and control are rebuilt from `model` and the iteration count restarts at 0.  The
+ * other instances keep running; no device memory is allocated. */
+int ws_load_instance(ws_ctx *ctx, int32_t instance, const ws_model *model);
 /* current geometry becomes the displacement origin; slip counters restart (CpuSolver.internalize, solver_cpu.js:868;
  * GpuSolver.internalize, solver_gpu.js:507-520) */
 int ws_internalize(ws_ctx *ctx, int32_t instance);

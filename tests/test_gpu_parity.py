@@ -30,7 +30,7 @@ def _gpu(md, prec="f64", form="cta", it=3000):
 
 
 @pytest.mark.parametrize("name", ["cantilever", "cantilever_edge", "cross_press", "cross_stick", "cross_locked"])
-@pytest.mark.parametrize("form", ["cta", "plain"])
+@pytest.mark.parametrize("form", ["cta", "plain", "grid"])
 def test_f64_matches_oracle(oracle_mod, name, form):
     md = cases.case_by_name(name)
     o = oracle_mod.Oracle(md.copy())
@@ -145,7 +145,7 @@ def test_large_shell_plain_against_oracle(oracle_mod):
     o = oracle_mod.Oracle(md.copy())
     o.step(330)
     v = o.view()
-    for prec, tol in (("f64", 1e-9), ("mixed", 1e-5)):
-        ctl, g = _gpu(md, prec, "plain", it=330)
+    for prec, form, tol in (("f64", "plain", 1e-9), ("mixed", "plain", 1e-5), ("f64", "grid", 1e-9), ("mixed", "grid", 1e-5)):
+        ctl, g = _gpu(md, prec, form, it=330)
         assert ctl["iter"] == 330
         assert cases.max_node_err_span(g["X"], v["X"], md.span) < tol

@@ -120,6 +120,7 @@ def lib():
             L.ws_upload_state.argtypes = [C.c_void_p, C.c_int32, _dp, _dp, _dp]
             L.ws_set_params.argtypes = [C.c_void_p, C.c_int32, C.POINTER(WsModel)]
             L.ws_internalize.argtypes = [C.c_void_p, C.c_int32]
+            L.ws_load_instance.argtypes = [C.c_void_p, C.c_int32, C.POINTER(WsModel)]
             L.ws_stream.argtypes = [C.c_void_p]
             L.ws_stream.restype = C.c_void_p
             L.ws_device_bytes.argtypes = [C.c_void_p]

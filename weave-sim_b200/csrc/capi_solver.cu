@@ -64,7 +64,7 @@ void layout(Dev<P> &d, Carver &cv, const Sizes &z) {
   d.cw = cv.take<R>(k); d.ch = cv.take<R>(k); d.mu = cv.take<R>(k); d.cflag = cv.take<uint8_t>(k);
   d.u = cv.take<U>(2 * k); d.nPrev = cv.take<R>(3 * k); d.slip = cv.take<A>(k); d.stuck = cv.take<uint8_t>(k);
   d.cstate = cv.take<uint8_t>(k); d.Fn = cv.take<R>(k); d.Ft = cv.take<R>(k); d.gap = cv.take<R>(k);
-  d.sSeg = cv.take<int>(2 * k); d.sT = cv.take<R>(2 * k); d.kth = cv.take<R>(k); d.sF = cv.take<R>(6 * k); d.sTq = cv.take<R>(6 * k);
+  d.sSeg = cv.take<int>(2 * k); d.sKey = cv.take<int>(2 * k); d.sStrand = cv.take<int>(2 * k); d.sT = cv.take<R>(2 * k); d.kth = cv.take<R>(k); d.sF = cv.take<R>(6 * k); d.sTq = cv.take<R>(6 * k);
   d.stSideOff = cv.take<int>(s); d.stSideCnt = cv.take<int>(s); d.ord = cv.take<int>(4 * k); d.ordSeg = cv.take<int>(4 * k);
 }
 
@@ -105,6 +105,9 @@ struct ws_ctx {
   int *dOrder = nullptr;
   uint8_t *dMask = nullptr;
   void *dPart = nullptr;
+  unsigned *dBar = nullptr;   // grid form: barrier counter + generation, and its timeout flag
+  int *dErr = nullptr;
+  int gridBlocks = 0;
   PlainShape shape{};
   cudaGraphExec_t graph = nullptr;
   int graphIters = 0;
@@ -290,6 +293,12 @@ void uploadStatic(ws_ctx *c, int b) {
     put<R>(d.wk + size_t(side) * d.ktot + I.k0, w.data(), K, st);
     put<R>(d.hk + size_t(side) * d.ktot + I.k0, h.data(), K, st);
   }
+  {
+    std::vector<int> ss(2 * K), sk(2 * K);
+    for (size_t q = 0; q < 2 * K; q++) { ss[q] = I.s0 + g.cxStrand[q]; sk[q] = g.sideSegLocal(int(q)); }
+    put<int>(d.sStrand + 2 * size_t(I.k0), ss.data(), 2 * K, st);
+    put<int>(d.sKey + 2 * size_t(I.k0), sk.data(), 2 * K, st);
+  }
   put<R>(d.cw + I.k0, g.w.data(), K, st);
   put<R>(d.ch + I.k0, g.h.data(), K, st);
   std::vector<int> so(S), sc(S);
@@ -346,6 +355,11 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
     const int thr = c->threads > 0 ? c->threads : 256;
     CK(launchBatched<P>(devOf<P>(c), c->dInst, c->dCtl, c->dOrder, nInst, nIter, mask ? c->dMask : nullptr, thr, nInst, c->st));
     c->lastLaunches = 1;
+  } else if (c->form == WS_FORM_GRID) {
+    CK(cudaMemsetAsync(c->dBar, 0, 2 * sizeof(unsigned), c->st));
+    CK(cudaMemsetAsync(c->dErr, 0, sizeof(int), c->st));
+    if (nIter > 0) CK(launchGrid<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->dBar, c->dErr, nIter, c->gridBlocks, c->st));
+    c->lastLaunches = 1;
   } else {
     const bool cx = c->inst[0].contacts && c->inst[0].K;
     const int chunk = std::min(nIter, 50);
@@ -361,13 +375,19 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
       c->graphIters = chunk;
     }
     int done = 0;
-    const int per = cx ? 5 : 3;
+    const int per = cx ? 4 : 3;
     while (nIter - done >= chunk && chunk > 0) { CK(cudaGraphLaunch(c->graph, c->st)); done += chunk; c->lastLaunches += int64_t(chunk) * per; }
     int nl = 0;
     for (; done < nIter; done++) CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, c->st, &nl));
     c->lastLaunches += nl;
   }
   CK(cudaEventRecord(c->ev1, c->st));
+  if (c->form == WS_FORM_GRID) {
+    int err = 0;
+    CK(cudaMemcpyAsync(&err, c->dErr, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (err) throw std::runtime_error("grid barrier wait exceeded its limit; the step was abandoned");
+  }
 }
 
 template <int P>
@@ -451,6 +471,34 @@ void setParamsImpl(ws_ctx *c, int b, const ws_model *md) {
 }
 
 template <int P>
+void loadInstanceImpl(ws_ctx *c, int b, const ws_model *md) {
+  HostGoals g;
+  g.build(*md);
+  const HostGoals &o = c->g[b];
+  if (g.n != o.n || g.m != o.m || g.p != o.p || g.K != o.K || g.S != o.S || g.C != o.C)
+    throw std::invalid_argument("the model's element counts differ from the slot's");
+  c->g[b] = std::move(g);
+  Sizes off;
+  off.n = c->inst[b].n0; off.m = c->inst[b].m0; off.p = c->inst[b].p0; off.c = c->inst[b].c0; off.k = c->inst[b].k0; off.s = c->inst[b].s0;
+  c->inst[b] = describe(c->g[b], off);
+  CK(cudaMemcpyAsync(c->dInst + b, &c->inst[b], sizeof(InstDesc), cudaMemcpyHostToDevice, c->st));
+  uploadStatic<P>(c, b);
+  uploadGoals<P>(c, b);
+  Dev<P> &d = devOf<P>(c);
+  using A = typename Dev<P>::A;
+  if (o.K) CK(cudaMemsetAsync(d.slip + c->inst[b].k0, 0, sizeof(A) * o.K, c->st));
+  using R = typename Dev<P>::R;
+  for (int k = 0; k < 3; k++) CK(cudaMemsetAsync(d.react + size_t(k) * d.ntot + c->inst[b].n0, 0, sizeof(R) * o.n, c->st));
+  InstCtl s;
+  std::memset(&s, 0, sizeof(s));
+  s.status = WS_RUNNING; s.residual = INFINITY;
+  uploadState<P>(c, b, 0, true);
+  uploadOrder<P>(c, b, 0);
+  CK(cudaMemcpyAsync(c->dCtl + b, &s, sizeof(InstCtl), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+}
+
+template <int P>
 void uploadStateImpl(ws_ctx *c, int b, const double *X, const double *Q, const double *u) {
   HostGoals &g = c->g[b];
   readCtl(c);
@@ -508,6 +556,8 @@ void destroyCtx(ws_ctx *c) {
   if (c->dOrder) cudaFree(c->dOrder);
   if (c->dMask) cudaFree(c->dMask);
   if (c->dPart) cudaFree(c->dPart);
+  if (c->dBar) cudaFree(c->dBar);
+  if (c->dErr) cudaFree(c->dErr);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->st) cudaStreamDestroy(c->st);
@@ -531,10 +581,10 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
   if (o.precision < 0 || o.precision > 2) return fail(WS_ERR_ARG, "ws_create: unknown precision");
   if (o.form < 0 || o.form > 2) return fail(WS_ERR_ARG, "ws_create: unknown execution form");
   if (o.form != WS_FORM_CTA && n_instances != 1) return fail(WS_ERR_ARG, "ws_create: the grid and plain forms take one instance");
-  if (o.threads < 0 || o.threads > 1024 || (o.threads % 32)) return fail(WS_ERR_ARG, "ws_create: threads must be a multiple of 32 up to 1024");
+  if (o.threads < 0 || o.threads > 512 || (o.threads % 32)) return fail(WS_ERR_ARG, "ws_create: threads must be a multiple of 32 up to 512");
   if (ws_device_count() <= 0) return fail(WS_ERR_NODEV, "ws_create: no CUDA device (this library has no CPU path)");
   auto c = new ws_ctx();
-  c->prec = o.precision; c->form = o.form == WS_FORM_GRID ? WS_FORM_PLAIN : o.form; c->threads = o.threads; c->device = o.device;
+  c->prec = o.precision; c->form = o.form; c->threads = o.threads; c->device = o.device;
   int rc = guarded("ws_create", [&]() {
     CK(cudaSetDevice(o.device));
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
@@ -566,9 +616,17 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     auto blocks = [](long long cnt, int thr) { return int(std::max<long long>(1, std::min<long long>((cnt + thr - 1) / thr, 148LL * 8))); };
     c->shape.blocksA = blocks(I0.m + I0.p + I0.C + I0.K, 256);
     c->shape.blocksS = blocks(I0.S, 128);
-    c->shape.blocksR = blocks(I0.m, 256);
+    c->shape.blocksR = blocks(I0.m + 2LL * I0.K, 256);
     c->shape.blocksD = blocks(I0.n + I0.m, 256);
-    CK(cudaMalloc(&c->dPart, sizeof(double) * (RS_NSUM + RX_NMAX) * size_t(c->shape.blocksA + c->shape.blocksD)));
+    switch (c->prec) {
+      case WS_PREC_F64: c->gridBlocks = gridBlocks<PREC_F64>(); break;
+      case WS_PREC_MIXED: c->gridBlocks = gridBlocks<PREC_MIXED>(); break;
+      default: c->gridBlocks = gridBlocks<PREC_F32>(); break;
+    }
+    CK(cudaGetLastError());
+    CK(cudaMalloc(&c->dPart, sizeof(double) * (RS_NSUM + RX_NMAX) * size_t(std::max(c->shape.blocksA + c->shape.blocksD, c->gridBlocks))));
+    CK(cudaMalloc(&c->dBar, 2 * sizeof(unsigned)));
+    CK(cudaMalloc(&c->dErr, sizeof(int)));
     DISPATCH(c, setupDev, c);
     size_t total = c->bytes + (sizeof(InstDesc) + sizeof(InstCtl) + 8) * n_instances;
     if (o.budget_bytes && total > o.budget_bytes) throw std::bad_alloc();
@@ -614,6 +672,11 @@ int ws_upload_state(ws_ctx *c, int32_t b, const double *X, const double *Q, cons
 int ws_set_params(ws_ctx *c, int32_t b, const ws_model *md) {
   if (!c || !md || b < 0 || b >= int(c->inst.size())) return fail(WS_ERR_ARG, "ws_set_params: bad arguments");
   return guarded("ws_set_params", [&]() { DISPATCH(c, setParamsImpl, c, b, md); });
+}
+
+int ws_load_instance(ws_ctx *c, int32_t b, const ws_model *md) {
+  if (!c || !md || b < 0 || b >= int(c->inst.size())) return fail(WS_ERR_ARG, "ws_load_instance: bad arguments");
+  return guarded("ws_load_instance", [&]() { DISPATCH(c, loadInstanceImpl, c, b, md); });
 }
 
 int ws_internalize(ws_ctx *c, int32_t b) {

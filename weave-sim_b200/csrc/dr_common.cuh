@@ -87,6 +87,8 @@ struct Dev {
   uint8_t *stuck, *cstate;  // [ktot]
   R *Fn, *Ft, *gap;         // [ktot]
   int *sSeg;                // [2 ktot] side records (side id sd = 2c + side)
+  int *sKey;                // [2 ktot] local segment of the side after this iteration's slide
+  int *sStrand;             // [2 ktot] strand of the side
   R *sT, *kth;              // [2 ktot], [ktot]
   R *sF, *sTq;              // [3][2 ktot]
   // strands

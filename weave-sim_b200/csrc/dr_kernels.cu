@@ -10,7 +10,7 @@ namespace wsb {
 // own convergence.  Instance state lives in HBM / L2; the block's barriers separate the phases, so an instance never
 // waits on another and no kernel spins.
 template <int P>
-__global__ void __launch_bounds__(1024) k_batched(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+__global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                                   const int *__restrict__ order, int nInst, int nIter, const uint8_t *__restrict__ mask) {
   using A = typename Dev<P>::A;
   __shared__ InstCtl sc;
@@ -37,9 +37,11 @@ __global__ void __launch_bounds__(1024) k_batched(Dev<P> d, const InstDesc *__re
       }
       __syncthreads();
       if (cx) {
-        for (int s = threadIdx.x; s < I.S; s += blockDim.x) sortStrand<P>(d, I.s0 + s, sx.obuf, sx.onxt);
-        __syncthreads();
-        for (int j = threadIdx.x; j < I.m; j += blockDim.x) segRange<P>(d, I.m0 + j, sx.onxt);
+        const int n2 = 2 * I.K;
+        for (int e = threadIdx.x; e < n2 + I.m; e += blockDim.x) {
+          if (e < n2) rankSide<P>(d, 2 * I.k0 + e, sx.obuf, sx.onxt);
+          else segCount<P>(d, I.m0 + (e - n2), sx.obuf, sx.onxt);
+        }
         __syncthreads();
       }
       for (int e = threadIdx.x; e < I.n + I.m; e += blockDim.x) {
@@ -85,18 +87,15 @@ __global__ void __launch_bounds__(256) k_plainA(Dev<P> d, const InstDesc *__rest
   }
 }
 template <int P>
-__global__ void k_plainSort(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl) {
+__global__ void __launch_bounds__(256) k_plainBC(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl) {
   const InstDesc I = insts[0];
   const InstCtl c = ctl[0];
   if (c.status != WS_RUNNING) return;
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < I.S; s += gridDim.x * blockDim.x) sortStrand<P>(d, I.s0 + s, c.obuf, c.obuf ^ 1);
-}
-template <int P>
-__global__ void k_plainRange(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl) {
-  const InstDesc I = insts[0];
-  const InstCtl c = ctl[0];
-  if (c.status != WS_RUNNING) return;
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < I.m; j += gridDim.x * blockDim.x) segRange<P>(d, I.m0 + j, c.obuf ^ 1);
+  const int n2 = 2 * I.K;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n2 + I.m; e += gridDim.x * blockDim.x) {
+    if (e < n2) rankSide<P>(d, 2 * I.k0 + e, c.obuf, c.obuf ^ 1);
+    else segCount<P>(d, I.m0 + (e - n2), c.obuf, c.obuf ^ 1);
+  }
 }
 template <int P>
 __global__ void __launch_bounds__(256) k_plainD(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
@@ -140,6 +139,92 @@ __global__ void __launch_bounds__(256) k_plainDecide(const InstDesc *__restrict_
   }
 }
 
+// ------------------------------------------------------------------------------------------------ grid form
+// Grid-wide barrier for a cooperative launch (every block resident).  The wait is bounded: past ~2^24 polls (about a
+// second) it raises *err and every block leaves its iteration loop, so a kernel never hangs the device.
+__device__ __forceinline__ bool gridSync(unsigned *bar, unsigned nb, int *err) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned g = atomicAdd(bar + 1, 0u);
+    __threadfence();
+    if (atomicAdd(bar, 1u) == nb - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      unsigned long long spins = 0;
+      while (atomicAdd(bar + 1, 0u) == g) {
+        if (++spins > (1ull << 24) || atomicAdd(err, 0) != 0) { atomicExch(err, 1); break; }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *reinterpret_cast<volatile int *>(err) == 0;
+}
+
+// One instance over the whole (co-resident) grid, every phase of up to nIter iterations in one launch: three grid
+// barriers per iteration.  Block partials go to part[block]; after the barrier every block reduces all of them in the
+// same order and takes the same kinetic-damping decision, so no further broadcast is needed.
+template <int P>
+__global__ void __launch_bounds__(256) k_grid(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+                                              typename Dev<P>::A *part, unsigned *bar, int *err, int nIter) {
+  using A = typename Dev<P>::A;
+  __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
+  __shared__ InstCtl sc;
+  __shared__ InstDesc si;
+  constexpr int NV = RS_NSUM + RX_NMAX;
+  if (threadIdx.x == 0) { sc = ctl[0]; si = insts[0]; }
+  __syncthreads();
+  const InstDesc &I = si;
+  const bool cx = I.contacts && I.K;
+  const int nA = I.m + I.p + I.C + (cx ? I.K : 0);
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+  const unsigned nb = gridDim.x;
+  for (int it = 0; it < nIter; it++) {
+    if (sc.status != WS_RUNNING) break;
+    const StepCtx sx = makeCtx<A>(I, sc);
+    Part<A> pt;
+    pt.init();
+    for (int e = gt; e < nA; e += gs) {
+      if (e < I.m) segForce<P>(d, sx.cur, I.m0 + e, pt);
+      else if (e < I.m + I.p) jointTorque<P>(d, sx.cur, I.p0 + (e - I.m), pt);
+      else if (e < I.m + I.p + I.C) clampTorque<P>(d, sx.cur, I.c0 + (e - I.m - I.p), pt);
+      else crossing<P>(d, I, sx.cur, sx.iter, I.k0 + (e - I.m - I.p - I.C), pt);
+    }
+    if (!gridSync(bar, nb, err)) break;
+    if (cx) {
+      const int n2 = 2 * I.K;
+      for (int e = gt; e < n2 + I.m; e += gs) {
+        if (e < n2) rankSide<P>(d, 2 * I.k0 + e, sx.obuf, sx.onxt);
+        else segCount<P>(d, I.m0 + (e - n2), sx.obuf, sx.onxt);
+      }
+      if (!gridSync(bar, nb, err)) break;
+    }
+    for (int e = gt; e < I.n + I.m; e += gs) {
+      if (e < I.n) nodeUpdate<P>(d, I, sx, I.n0 + e, pt);
+      else segUpdate<P>(d, I, sx, I.m0 + (e - I.n), pt);
+    }
+    blockReduce(pt, red);
+    if (threadIdx.x == 0) {
+      for (int i = 0; i < RS_NSUM; i++) part[blockIdx.x * NV + i] = pt.s[i];
+      for (int i = 0; i < RX_NMAX; i++) part[blockIdx.x * NV + RS_NSUM + i] = pt.x[i];
+    }
+    if (!gridSync(bar, nb, err)) break;
+    Part<A> q;
+    q.init();
+    for (int b = threadIdx.x; b < int(nb); b += blockDim.x) {
+      for (int i = 0; i < RS_NSUM; i++) q.s[i] += part[b * NV + i];
+      for (int i = 0; i < RX_NMAX; i++) q.x[i] = mmax(q.x[i], part[b * NV + RS_NSUM + i]);
+    }
+    blockReduce(q, red);
+    if (threadIdx.x == 0) decide(I, sc, q, nIter);
+    __syncthreads();
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl[0] = sc;
+}
+
 // ------------------------------------------------------------------------------------------------ launchers
 template <int P>
 cudaError_t launchBatched(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
@@ -156,9 +241,8 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
   k_plainA<P><<<sh.blocksA, 256, 0, st>>>(d, insts, ctl, pa);
   int nl = 1;
   if (contacts) {
-    k_plainSort<P><<<sh.blocksS, 128, 0, st>>>(d, insts, ctl);
-    k_plainRange<P><<<sh.blocksR, 256, 0, st>>>(d, insts, ctl);
-    nl += 2;
+    k_plainBC<P><<<sh.blocksR, 256, 0, st>>>(d, insts, ctl);
+    nl += 1;
   }
   k_plainD<P><<<sh.blocksD, 256, 0, st>>>(d, insts, ctl, pd);
   k_plainDecide<P><<<1, 256, 0, st>>>(insts, ctl, pa, sh.blocksA + sh.blocksD);
@@ -167,11 +251,30 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
   return cudaGetLastError();
 }
 
+template <int P>
+cudaError_t launchGrid(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, unsigned *bar, int *err, int nIter,
+                       int blocks, cudaStream_t st) {
+  using A = typename Dev<P>::A;
+  A *pa = static_cast<A *>(part);
+  void *args[] = {(void *)&d, (void *)&insts, (void *)&ctl, (void *)&pa, (void *)&bar, (void *)&err, (void *)&nIter};
+  return cudaLaunchCooperativeKernel((const void *)k_grid<P>, dim3(blocks), dim3(256), args, 0, st);
+}
+template <int P>
+int gridBlocks() {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_grid<P>, 256, 0);
+  return sms * (per > 0 ? per : 1);
+}
+
 #define WSB_INST(P)                                                                                                  \
   template cudaError_t launchBatched<P>(const Dev<P> &, const InstDesc *, InstCtl *, const int *, int, int, const uint8_t *, \
                                         int, int, cudaStream_t);                                                     \
   template cudaError_t launchPlainIter<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, const PlainShape &, bool,    \
-                                          cudaStream_t, int *);
+                                          cudaStream_t, int *);                                                        \
+  template cudaError_t launchGrid<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, unsigned *, int *, int, int, cudaStream_t); \
+  template int gridBlocks<P>();
 WSB_INST(PREC_F64)
 WSB_INST(PREC_MIXED)
 WSB_INST(PREC_F32)

@@ -15,4 +15,10 @@ template <int P>
 cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, const PlainShape &sh, bool contacts,
                             cudaStream_t st, int *launches);
 
+template <int P>
+cudaError_t launchGrid(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, unsigned *bar, int *err, int nIter,
+                       int blocks, cudaStream_t st);
+template <int P>
+int gridBlocks();
+
 }  // namespace wsb

@@ -5,8 +5,9 @@
 //                 clamps (joints against frozen frames)            rod_cosserat.js:161-180
 //                 crossings (Hermite evaluation, normal, gap, penalty, Coulomb return mapping, slide of u on both
 //                 laths, force and lever torque per side)          solver_cpu.js:179-228, 274-282, 381-478
-//   B  strands:   crossing sides re-sorted along their strand by their new segment (insertion sort, nearly sorted)
-//   C  segments:  slice of the sorted sides on every segment (binary search)
+//   BC sides:     new sorted order of the crossing sides along each strand, by rank (each side counts the sides
+//                 before it); segments: their slice of that order, by counting the keys below and equal
+//                 (both read only the keys of phase A, so they share one phase)
 //   D  nodes:     F = n_out − n_in + loads + Σ sides on the two adjacent segments (weights 1 − t, t, the slices of
 //                 the previous sort); reactions, fixed DOFs, warm-up, v += F/m, x += v, prescribed support motion
 //                 segments: T = e × n ± joint torques − clamp torques + lever torques; tm = Rᵀ T; frame inertia
@@ -378,6 +379,11 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   if (moved) { uu[0] += U(da) / U(mmax(L[0], R(1e-12))); uu[1] -= U(db) / U(mmax(L[1], R(1e-12))); }
   d.u[c] = mclamp(uu[0], U(0), U(nseg[0]));
   d.u[kt_ + c] = mclamp(uu[1], U(0), U(nseg[1]));
+  // the sides' segments after the slide: the keys of the re-sort (solver_cpu.js:144-149)
+  for (int side = 0; side < 2; side++) {
+    const U un = d.u[side * kt_ + c];
+    d.sKey[2 * c + side] = int(mmin(mmax(mfloor(un), U(0)), U(mmax(nseg[side] - 1, 0))));
+  }
   if (slip) {
     const R sx = da * tA[0] + db * tB[0], sy = da * tA[1] + db * tB[1], sz = da * tA[2] + db * tB[2];
     d.slip[c] += A(msqrt(sx * sx + sy * sy + sz * sz));
@@ -415,40 +421,38 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
 }
 
 // ------------------------------------------------------------------------------------------------ phase B / C
-// local segment of a side from its slide coordinate (solver_cpu.js:144-149)
+// Slot e of the previous sorted order: its side goes to position off + rank in the new order, rank = number of the
+// strand's sides with a smaller (segment, side id).  Every side counts independently (no serial sort, no atomics),
+// and the result is the sorted order by (segment, id) whatever the previous order was.
 template <int P>
-__device__ __forceinline__ int sideSeg(const Dev<P> &d, int sd) {
-  using U = typename Dev<P>::U;
-  const int c = sd >> 1, side = sd & 1, o = side * d.ktot + c;
-  const U u = d.u[o];
-  const int ns = d.cxNseg[o];
-  return int(mmin(mmax(mfloor(u), U(0)), U(mmax(ns - 1, 0))));
-}
-// strand s: sides re-sorted by (segment, side id) from the order of the last iteration (insertion sort: the order
-// changes only where a crossing passes a segment end)
-template <int P>
-__device__ __forceinline__ void sortStrand(const Dev<P> &d, int s, int src, int dst) {
-  const int off = d.stSideOff[s], cnt = d.stSideCnt[s], K2 = 2 * d.ktot;
-  const int *oi = d.ord + size_t(src) * K2 + off;
-  int *oo = d.ord + size_t(dst) * K2 + off, *os = d.ordSeg + size_t(dst) * K2 + off;
-  for (int i = 0; i < cnt; i++) {
-    const int sd = oi[i], key = sideSeg<P>(d, sd);
-    int k = i;
-    while (k > 0 && (os[k - 1] > key || (os[k - 1] == key && oo[k - 1] > sd))) { oo[k] = oo[k - 1]; os[k] = os[k - 1]; k--; }
-    oo[k] = sd; os[k] = key;
-  }
-}
-template <int P>
-__device__ __forceinline__ void segRange(const Dev<P> &d, int j, int dst) {
-  const int s = d.segStrand[j], lj = d.segLocal[j], K2 = 2 * d.ktot;
+__device__ __forceinline__ void rankSide(const Dev<P> &d, int e, int src, int dst) {
+  const int K2 = 2 * d.ktot;
+  const int *oi = d.ord + size_t(src) * K2;
+  const int sd = oi[e], key = d.sKey[sd], s = d.sStrand[sd];
   const int off = d.stSideOff[s], cnt = d.stSideCnt[s];
-  const int *os = d.ordSeg + size_t(dst) * K2 + off;
-  int lo = 0, hi = cnt;
-  while (lo < hi) { const int mid = (lo + hi) >> 1; if (os[mid] < lj) lo = mid + 1; else hi = mid; }
-  int lo2 = lo, hi2 = cnt;
-  while (lo2 < hi2) { const int mid = (lo2 + hi2) >> 1; if (os[mid] <= lj) lo2 = mid + 1; else hi2 = mid; }
+  int rank = 0;
+  for (int q = off; q < off + cnt; q++) {
+    const int o = oi[q], ko = d.sKey[o];
+    rank += (ko < key || (ko == key && o < sd)) ? 1 : 0;
+  }
+  d.ord[size_t(dst) * K2 + off + rank] = sd;
+  d.ordSeg[size_t(dst) * K2 + off + rank] = key;
+}
+// segment j: its slice of the new order = [off + #keys below, off + #keys below + #keys equal) among its strand's sides
+template <int P>
+__device__ __forceinline__ void segCount(const Dev<P> &d, int j, int src, int dst) {
+  const int K2 = 2 * d.ktot;
+  const int *oi = d.ord + size_t(src) * K2;
+  const int s = d.segStrand[j], lj = d.segLocal[j];
+  const int off = d.stSideOff[s], cnt = d.stSideCnt[s];
+  int lo = 0, eq = 0;
+  for (int q = off; q < off + cnt; q++) {
+    const int ko = d.sKey[oi[q]];
+    lo += ko < lj ? 1 : 0;
+    eq += ko == lj ? 1 : 0;
+  }
   d.rngLo[size_t(dst) * d.mtot + j] = off + lo;
-  d.rngHi[size_t(dst) * d.mtot + j] = off + lo2;
+  d.rngHi[size_t(dst) * d.mtot + j] = off + lo + eq;
 }
 
 // ------------------------------------------------------------------------------------------------ phase D

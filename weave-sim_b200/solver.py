@@ -111,6 +111,13 @@ class GpuSolver:
         check(lib().ws_set_params(self.h, int(b), C.byref(st)), "ws_set_params")
         self.models[b] = model
 
+    def load_instance(self, b, model):
+        """slot b takes a new model of the same element counts; its iteration count restarts at 0"""
+        st = model.struct()
+        self._keep_load = (model, st)
+        check(lib().ws_load_instance(self.h, int(b), C.byref(st)), "ws_load_instance")
+        self.models[b] = model
+
     def internalize(self, b):
         check(lib().ws_internalize(self.h, int(b)), "ws_internalize")
 
