@@ -247,6 +247,20 @@ int ws_load_instance(ws_ctx *ctx, int32_t instance, const ws_model *model);
 /* current geometry becomes the displacement origin; slip counters restart (CpuSolver.internalize, solver_cpu.js:868;
  * GpuSolver.internalize, solver_gpu.js:507-520) */
 int ws_internalize(ws_ctx *ctx, int32_t instance);
+/* Allocation-free relaxation of one small instance, for callers that cannot allocate device memory themselves (a
+ * framework that owns the GPU's memory through its own pool, a serving process that must not allocate once running).
+ * No counterpart in the reference.  The instance's whole device footprint lives in one static array of
+ * WS_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds until exit; models that need more are rejected
+ * with WS_ERR_ARG.  The call builds the goals, clears the array, uploads `model`, runs n_iter iterations of the batched
+ * kernel on `stream` (NULL: the default stream), waits for them and fills `out` and `ctl` (either may be NULL); the
+ * result equals ws_create + ws_step + ws_download with the same threads.  It allocates no device memory.
+ * The first call on a device looks up the array's device address there (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  Every call shares the array and leaves its contents behind: calls from this process take
+ * turns on a lock, but calls whose GPU work overlaps (several processes, or this entry point mixed with raw launches that
+ * touch the array) race. */
+#define WS_NOALLOC_SCRATCH_BYTES (16u << 20)
+int ws_relax_noalloc(const ws_model *model, int32_t precision, int32_t n_iter, int32_t threads, void *stream,
+                     ws_state_out *out, ws_control *ctl);
 /* CUDA stream of the context (cudaStream_t) */
 void *ws_stream(ws_ctx *ctx);
 /* device bytes held by the context */

@@ -121,6 +121,8 @@ def lib():
             L.ws_set_params.argtypes = [C.c_void_p, C.c_int32, C.POINTER(WsModel)]
             L.ws_internalize.argtypes = [C.c_void_p, C.c_int32]
             L.ws_load_instance.argtypes = [C.c_void_p, C.c_int32, C.POINTER(WsModel)]
+            L.ws_relax_noalloc.argtypes = [C.POINTER(WsModel), C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                                           C.POINTER(WsStateOut), C.POINTER(WsControl)]
             L.ws_stream.argtypes = [C.c_void_p]
             L.ws_stream.restype = C.c_void_p
             L.ws_device_bytes.argtypes = [C.c_void_p]

@@ -707,3 +707,65 @@ int ws_destroy(ws_ctx *c) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------------ caller-provided memory
+// Runs one instance whose whole device footprint (arena, descriptor, control block) lives in memory the caller hands
+// over (`base`, `cap` bytes): set-up, `n_iter` iterations of the batched kernel, download.  Used by the allocation-free
+// entry point (capi_noalloc.cu); nothing here allocates device memory.
+namespace wsb {
+
+size_t instanceFootprint(int prec, const HostGoals &g) {
+  Sizes z;
+  z.n = g.n; z.m = g.m; z.p = g.p; z.c = g.C; z.k = g.K; z.s = g.S;
+  Carver cv{nullptr};
+  switch (prec) {
+    case WS_PREC_F64: { Dev<PREC_F64> d{}; layout<PREC_F64>(d, cv, z); break; }
+    case WS_PREC_MIXED: { Dev<PREC_MIXED> d{}; layout<PREC_MIXED>(d, cv, z); break; }
+    default: { Dev<PREC_F32> d{}; layout<PREC_F32>(d, cv, z); break; }
+  }
+  const size_t tail = ((sizeof(InstDesc) + 255) & ~size_t(255)) + ((sizeof(InstCtl) + 255) & ~size_t(255));
+  return ((cv.off + 255) & ~size_t(255)) + tail;
+}
+
+template <int P>
+static void runInPlaceImpl(ws_ctx *c, char *base, int nIter, int threads, ws_state_out *out, ws_control *ctl) {
+  Carver cv{base};
+  layout<P>(devOf<P>(c), cv, c->z);
+  const size_t off = (cv.off + 255) & ~size_t(255);
+  c->dInst = reinterpret_cast<InstDesc *>(base + off);
+  c->dCtl = reinterpret_cast<InstCtl *>(base + off + ((sizeof(InstDesc) + 255) & ~size_t(255)));
+  CK(cudaMemsetAsync(base, 0, off, c->st));
+  CK(cudaMemcpyAsync(c->dInst, c->inst.data(), sizeof(InstDesc), cudaMemcpyHostToDevice, c->st));
+  InstCtl s;
+  std::memset(&s, 0, sizeof(s));
+  s.status = WS_RUNNING; s.residual = INFINITY;
+  CK(cudaMemcpyAsync(c->dCtl, &s, sizeof(InstCtl), cudaMemcpyHostToDevice, c->st));
+  uploadAll<P>(c);
+  if (nIter > 0) CK(launchBatched<P>(devOf<P>(c), c->dInst, c->dCtl, nullptr, 1, nIter, nullptr, threads, 1, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (out) downloadImpl<P>(c, 0, out);
+  if (ctl) { readCtl(c); fillControl(c->ctlHost[0], ctl); }
+}
+
+int runInPlace(int prec, const HostGoals &g, char *base, int nIter, int threads, cudaStream_t st, ws_state_out *out,
+               ws_control *ctl, std::string &err) {
+  ws_ctx tmp;                       // host-side bookkeeping only: its device pointers point into `base`
+  tmp.prec = prec; tmp.form = WS_FORM_CTA; tmp.threads = threads; tmp.st = st;
+  tmp.g.push_back(g);
+  Sizes off;
+  tmp.inst.push_back(describe(tmp.g[0], off));
+  tmp.z.n = g.n; tmp.z.m = g.m; tmp.z.p = g.p; tmp.z.c = g.C; tmp.z.k = g.K; tmp.z.s = g.S;
+  try {
+    switch (prec) {
+      case WS_PREC_F64: runInPlaceImpl<PREC_F64>(&tmp, base, nIter, threads, out, ctl); break;
+      case WS_PREC_MIXED: runInPlaceImpl<PREC_MIXED>(&tmp, base, nIter, threads, out, ctl); break;
+      default: runInPlaceImpl<PREC_F32>(&tmp, base, nIter, threads, out, ctl); break;
+    }
+  } catch (const std::exception &e) {
+    err = e.what();
+    return WS_ERR_CUDA;
+  }
+  return WS_OK;
+}
+
+}  // namespace wsb

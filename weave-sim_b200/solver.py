@@ -26,6 +26,31 @@ def device_count() -> int:
     return int(lib().ws_device_count())
 
 
+def _state_buffers(md):
+    n, m, p, K = md.n, md.m, md.p, md.K
+    out = {"X": np.zeros(3 * n), "Q": np.zeros(4 * m), "V": np.zeros(3 * n), "W": np.zeros(3 * m),
+           "u": np.zeros(2 * K), "nprev": np.zeros(3 * K), "slip": np.zeros(K), "Fn": np.zeros(K), "Ft": np.zeros(K),
+           "gap": np.zeros(K), "N": np.zeros(m), "Vsh": np.zeros(2 * m), "M": np.zeros(3 * p),
+           "reactions": np.zeros(3 * n), "stuck": np.zeros(K, dtype=np.uint8), "state": np.zeros(K, dtype=np.uint8)}
+    so = WsStateOut()
+    for k, a in out.items():
+        ct = C.c_uint8 if a.dtype == np.uint8 else C.c_double
+        setattr(so, k, a.ctypes.data_as(C.POINTER(ct)) if a.size else None)
+    return out, so
+
+
+def relax_noalloc(model, n_iter, precision="mixed", threads=256, stream=None):
+    """One small instance relaxed inside the library's static device scratch (ws_relax_noalloc): for callers that cannot
+    allocate device memory.  Returns (state, control)."""
+    st = model.struct()
+    out, so = _state_buffers(model)
+    ctl = WsControl()
+    prec = _lib.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    check(lib().ws_relax_noalloc(C.byref(st), prec, int(n_iter), int(threads), stream, C.byref(so), C.byref(ctl)),
+          "ws_relax_noalloc")
+    return out, ctl.as_dict()
+
+
 class GpuSolver:
     def __init__(self, models, precision="mixed", form="cta", threads=0, device=0, budget_bytes=0):
         if not isinstance(models, (list, tuple)):
