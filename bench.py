@@ -153,7 +153,9 @@ def run_ours(args, rank, world, local):
     barrier(world)
     total_ms = allmax(sum(times), world)
     ctl = s.read_control()[0]
-    # end to end through the C ABI with host buffers: upload state, relax one chunk, download the result
+    # end to end through the C ABI with host buffers: upload state, relax one chunk, download the result (positions,
+    # frames, slide coordinates, contact normals and stick/slip: what a caller reads back, and warm-starts from)
+    result_fields = ("X", "Q", "u", "nprev", "stuck", "state")
     st0 = s.download(0)
     X, Q, u = st0["X"].copy(), st0["Q"].copy(), st0["u"].copy()
     e2e_t = []
@@ -161,7 +163,7 @@ def run_ours(args, rank, world, local):
         t0 = time.perf_counter()
         s.upload_state(0, X, Q, u)
         s.step(args.chunk, read=False)
-        out = s.download(0)
+        out = s.download(0, fields=result_fields)
         e2e_t.append(time.perf_counter() - t0)
     h2d = X.nbytes + Q.nbytes + u.nbytes
     d2h = sum(v.nbytes for v in out.values())

@@ -11,7 +11,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libweavesim_b200.so")
+LIB_PATH = os.environ.get("WEAVESIM_B200_LIB") or os.path.join(HERE, "libweavesim_b200.so")
 
 WS_OK = 0
 WS_PREC_F64, WS_PREC_MIXED, WS_PREC_F32 = 0, 1, 2

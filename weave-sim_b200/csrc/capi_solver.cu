@@ -3,8 +3,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <numeric>
+#include <type_traits>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -115,9 +117,78 @@ struct ws_ctx {
   double lastMs = 0;
   int64_t lastLaunches = 0;
   std::vector<InstCtl> ctlHost;
+  // host staging of uploads / downloads: pinned (cudaMallocHost) in contexts made by ws_create, an ordinary host vector
+  // in the allocation-free entry point's temporary context
+  bool pinnedOK = false;
+  char *pinned = nullptr;
+  size_t pinnedCap = 0;
+  std::vector<char> pageable;
 };
 
 namespace {
+
+char *stageBuf(ws_ctx *c, size_t bytes) {
+  if (!c->pinnedOK) {
+    if (c->pageable.size() < bytes) c->pageable.resize(bytes);
+    return c->pageable.data();
+  }
+  if (c->pinnedCap < bytes) {
+    if (c->pinned) CK(cudaFreeHost(c->pinned));
+    c->pinned = nullptr;
+    c->pinnedCap = 0;
+    CK(cudaMallocHost(&c->pinned, bytes));
+    c->pinnedCap = bytes;
+  }
+  return c->pinned;
+}
+
+// device -> host in one go: planes are queued, copied asynchronously into the staging buffer, and converted to the
+// caller's interleaved f64 (or byte) arrays after a single synchronisation
+struct Fetch {
+  struct Item { const void *src; size_t bytes, off; std::function<void(const char *)> put; };
+  std::vector<Item> items;
+  size_t total = 0;
+  template <class T>
+  void planes(const T *base, size_t stride, size_t first, size_t count, int ncomp, double *dst) {
+    for (int k = 0; k < ncomp; k++) {
+      const size_t off = total;
+      total += (count * sizeof(T) + 15) & ~size_t(15);
+      items.push_back({base + size_t(k) * stride + first, count * sizeof(T), off, [=](const char *p) {
+                         const T *v = reinterpret_cast<const T *>(p);
+                         for (size_t i = 0; i < count; i++) dst[size_t(ncomp) * i + k] = double(v[i]);
+                       }});
+    }
+  }
+  // two-float planes: hi and lo added in f64
+  template <class T>
+  void pairs(const T *hi, const T *lo, size_t stride, size_t first, size_t count, int ncomp, double *dst) {
+    for (int k = 0; k < ncomp; k++) {
+      const size_t oh = total;
+      total += (count * sizeof(T) + 15) & ~size_t(15);
+      const size_t ol = total;
+      if (lo) total += (count * sizeof(T) + 15) & ~size_t(15);
+      items.push_back({hi + size_t(k) * stride + first, count * sizeof(T), oh, nullptr});
+      if (lo) items.push_back({lo + size_t(k) * stride + first, count * sizeof(T), ol, nullptr});
+      const bool two = lo != nullptr;
+      items.back().put = [=](const char *p0) {
+        const T *h = reinterpret_cast<const T *>(p0 - (two ? ol : oh) + oh);
+        const T *l = two ? reinterpret_cast<const T *>(p0) : nullptr;
+        for (size_t i = 0; i < count; i++) dst[size_t(ncomp) * i + k] = double(h[i]) + (two ? double(l[i]) : 0.0);
+      };
+    }
+  }
+  void bytes(const uint8_t *src, size_t count, uint8_t *dst) {
+    const size_t off = total;
+    total += (count + 15) & ~size_t(15);
+    items.push_back({src, count, off, [=](const char *p) { std::memcpy(dst, p, count); }});
+  }
+  void run(ws_ctx *c) {
+    char *buf = stageBuf(c, std::max<size_t>(total, 16));
+    for (auto &it : items) if (it.bytes) CK(cudaMemcpyAsync(buf + it.off, it.src, it.bytes, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (auto &it : items) if (it.put) it.put(buf + it.off);
+  }
+};
 
 template <int P> Dev<P> &devOf(ws_ctx *c);
 template <> Dev<PREC_F64> &devOf<PREC_F64>(ws_ctx *c) { return c->d64; }
@@ -222,7 +293,8 @@ void uploadOrder(ws_ctx *c, int b, int buf) {
   put<int>(d.rngHi + size_t(buf) * d.mtot + I.m0, hi.data(), m, c->st);
 }
 
-// positions / frames of instance b into buffer `buf` (and its slide coordinates)
+// positions / frames of instance b into buffer `buf` (and its slide coordinates): converted into the staging buffer,
+// copied asynchronously, one synchronisation; velocities are cleared on the device
 template <int P>
 void uploadState(ws_ctx *c, int b, int buf, bool withU) {
   Dev<P> &d = devOf<P>(c);
@@ -231,35 +303,35 @@ void uploadState(ws_ctx *c, int b, int buf, bool withU) {
   const InstDesc &I = c->inst[b];
   cudaStream_t st = c->st;
   const size_t n = g.n, m = g.m, K = g.K;
+  const int nS = PrecT<P>::TWO ? 2 : 1;
+  auto al = [](size_t x) { return (x + 15) & ~size_t(15); };
+  const size_t bytes = nS * (3 * al(n * sizeof(S)) + 4 * al(m * sizeof(S))) + (withU && K ? 2 * al(K * sizeof(U)) + 3 * al(K * sizeof(R)) : 0);
+  char *sb = stageBuf(c, std::max<size_t>(bytes, 16));
+  size_t off = 0;
+  auto stagePlane = [&](auto *dst, size_t count, auto fill) {
+    using T = std::remove_pointer_t<decltype(dst)>;
+    T *h = reinterpret_cast<T *>(sb + off);
+    for (size_t i = 0; i < count; i++) h[i] = fill(i);
+    CK(cudaMemcpyAsync(dst, h, count * sizeof(T), cudaMemcpyHostToDevice, st));
+    off += al(count * sizeof(T));
+  };
   for (int k = 0; k < 3; k++) {
-    std::vector<double> a(n);
-    for (size_t i = 0; i < n; i++) a[i] = g.X[3 * i + k];
-    std::vector<double> hi(n), lo(n);
-    for (size_t i = 0; i < n; i++) { hi[i] = double(S(W(a[i]))); lo[i] = double(S(W(a[i]) - W(S(W(a[i]))))); }
-    put<S>(d.X + size_t(buf * 3 + k) * d.ntot + I.n0, hi.data(), n, st);
-    if (PrecT<P>::TWO) put<S>(d.Xlo + size_t(buf * 3 + k) * d.ntot + I.n0, lo.data(), n, st);
-    std::vector<double> z(n, 0.0);
-    put<R>(d.V + size_t(k) * d.ntot + I.n0, z.data(), n, st);
+    stagePlane(d.X + size_t(buf * 3 + k) * d.ntot + I.n0, n, [&](size_t i) { return S(W(g.X[3 * i + k])); });
+    if (PrecT<P>::TWO)
+      stagePlane(d.Xlo + size_t(buf * 3 + k) * d.ntot + I.n0, n, [&](size_t i) { const W a = W(g.X[3 * i + k]); return S(a - W(S(a))); });
+    CK(cudaMemsetAsync(d.V + size_t(k) * d.ntot + I.n0, 0, n * sizeof(R), st));
   }
   for (int k = 0; k < 4; k++) {
-    std::vector<double> hi(m), lo(m);
-    for (size_t j = 0; j < m; j++) { const double a = g.Q[4 * j + k]; hi[j] = double(S(W(a))); lo[j] = double(S(W(a) - W(S(W(a))))); }
-    put<S>(d.Q + size_t(buf * 4 + k) * d.mtot + I.m0, hi.data(), m, st);
-    if (PrecT<P>::TWO) put<S>(d.Qlo + size_t(buf * 4 + k) * d.mtot + I.m0, lo.data(), m, st);
+    stagePlane(d.Q + size_t(buf * 4 + k) * d.mtot + I.m0, m, [&](size_t j) { return S(W(g.Q[4 * j + k])); });
+    if (PrecT<P>::TWO)
+      stagePlane(d.Qlo + size_t(buf * 4 + k) * d.mtot + I.m0, m, [&](size_t j) { const W a = W(g.Q[4 * j + k]); return S(a - W(S(a))); });
   }
-  for (int k = 0; k < 3; k++) { std::vector<double> z(m, 0.0); put<R>(d.Wr + size_t(k) * d.mtot + I.m0, z.data(), m, st); }
+  for (int k = 0; k < 3; k++) CK(cudaMemsetAsync(d.Wr + size_t(k) * d.mtot + I.m0, 0, m * sizeof(R), st));
   if (withU && K) {
-    for (int side = 0; side < 2; side++) {
-      std::vector<double> a(K);
-      for (size_t q = 0; q < K; q++) a[q] = g.u[2 * q + side];
-      put<U>(d.u + size_t(side) * d.ktot + I.k0, a.data(), K, st);
-    }
-    for (int k = 0; k < 3; k++) {
-      std::vector<double> a(K);
-      for (size_t q = 0; q < K; q++) a[q] = g.nPrev[3 * q + k];
-      put<R>(d.nPrev + size_t(k) * d.ktot + I.k0, a.data(), K, st);
-    }
+    for (int side = 0; side < 2; side++) stagePlane(d.u + size_t(side) * d.ktot + I.k0, K, [&](size_t q) { return U(g.u[2 * q + side]); });
+    for (int k = 0; k < 3; k++) stagePlane(d.nPrev + size_t(k) * d.ktot + I.k0, K, [&](size_t q) { return R(g.nPrev[3 * q + k]); });
   }
+  CK(cudaStreamSynchronize(st));
 }
 
 // the static arrays of instance b (topology, rest state, section constants)
@@ -368,17 +440,17 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
       cudaGraph_t gr;
       CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
       int nl = 0;
-      for (int i = 0; i < chunk; i++) CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, c->st, &nl));
+      for (int i = 0; i < chunk; i++) CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, c->st, &nl, c->dBar + 2));
       CK(cudaStreamEndCapture(c->st, &gr));
       CK(cudaGraphInstantiate(&c->graph, gr, 0));
       cudaGraphDestroy(gr);
       c->graphIters = chunk;
     }
     int done = 0;
-    const int per = cx ? 4 : 3;
+    const int per = cx ? 3 : 2;
     while (nIter - done >= chunk && chunk > 0) { CK(cudaGraphLaunch(c->graph, c->st)); done += chunk; c->lastLaunches += int64_t(chunk) * per; }
     int nl = 0;
-    for (; done < nIter; done++) CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, c->st, &nl));
+    for (; done < nIter; done++) CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, c->st, &nl, c->dBar + 2));
     c->lastLaunches += nl;
   }
   CK(cudaEventRecord(c->ev1, c->st));
@@ -397,43 +469,26 @@ void downloadImpl(ws_ctx *c, int b, ws_state_out *o) {
   const InstCtl &s = c->ctlHost[b];
   const InstDesc &I = c->inst[b];
   const size_t n = I.n, m = I.m, p = I.p, K = I.K;
-  std::vector<double> t, t2;
-  auto planes = [&](double *dst, int ncomp, auto *src, size_t stride, size_t off, size_t count) {
-    for (int k = 0; k < ncomp; k++) {
-      getv(t, src + size_t(k) * stride + off, count, c->st);
-      for (size_t i = 0; i < count; i++) dst[ncomp * i + k] = t[i];
-    }
-  };
-  if (o->X) {
-    for (int k = 0; k < 3; k++) {
-      getv(t, d.X + size_t(s.cur * 3 + k) * d.ntot + I.n0, n, c->st);
-      if (PrecT<P>::TWO) getv(t2, d.Xlo + size_t(s.cur * 3 + k) * d.ntot + I.n0, n, c->st);
-      for (size_t i = 0; i < n; i++) o->X[3 * i + k] = t[i] + (PrecT<P>::TWO ? t2[i] : 0.0);
-    }
-  }
-  if (o->Q) {
-    for (int k = 0; k < 4; k++) {
-      getv(t, d.Q + size_t(s.cur * 4 + k) * d.mtot + I.m0, m, c->st);
-      if (PrecT<P>::TWO) getv(t2, d.Qlo + size_t(s.cur * 4 + k) * d.mtot + I.m0, m, c->st);
-      for (size_t j = 0; j < m; j++) o->Q[4 * j + k] = t[j] + (PrecT<P>::TWO ? t2[j] : 0.0);
-    }
-  }
-  if (o->V) { if (s.pending) std::fill(o->V, o->V + 3 * n, 0.0); else planes(o->V, 3, d.V, d.ntot, I.n0, n); }
-  if (o->W) { if (s.pending) std::fill(o->W, o->W + 3 * m, 0.0); else planes(o->W, 3, d.Wr, d.mtot, I.m0, m); }
+  Fetch f;
+  if (o->X) f.pairs(d.X + size_t(s.cur * 3) * d.ntot, PrecT<P>::TWO ? d.Xlo + size_t(s.cur * 3) * d.ntot : nullptr, d.ntot, I.n0, n, 3, o->X);
+  if (o->Q) f.pairs(d.Q + size_t(s.cur * 4) * d.mtot, PrecT<P>::TWO ? d.Qlo + size_t(s.cur * 4) * d.mtot : nullptr, d.mtot, I.m0, m, 4, o->Q);
+  if (o->V) { if (s.pending) std::fill(o->V, o->V + 3 * n, 0.0); else f.planes(d.V, d.ntot, I.n0, n, 3, o->V); }
+  if (o->W) { if (s.pending) std::fill(o->W, o->W + 3 * m, 0.0); else f.planes(d.Wr, d.mtot, I.m0, m, 3, o->W); }
   if (K) {
-    if (o->u) planes(o->u, 2, d.u, d.ktot, I.k0, K);
-    if (o->nprev) planes(o->nprev, 3, d.nPrev, d.ktot, I.k0, K);
-    if (o->slip) planes(o->slip, 1, d.slip, 0, I.k0, K);
-    if (o->Fn) planes(o->Fn, 1, d.Fn, 0, I.k0, K);
-    if (o->Ft) planes(o->Ft, 1, d.Ft, 0, I.k0, K);
-    if (o->gap) planes(o->gap, 1, d.gap, 0, I.k0, K);
-    if (o->stuck) { std::vector<uint8_t> v(K); CK(cudaMemcpyAsync(v.data(), d.stuck + I.k0, K, cudaMemcpyDeviceToHost, c->st)); CK(cudaStreamSynchronize(c->st)); std::copy(v.begin(), v.end(), o->stuck); }
-    if (o->state) { std::vector<uint8_t> v(K); CK(cudaMemcpyAsync(v.data(), d.cstate + I.k0, K, cudaMemcpyDeviceToHost, c->st)); CK(cudaStreamSynchronize(c->st)); std::copy(v.begin(), v.end(), o->state); }
+    if (o->u) f.planes(d.u, d.ktot, I.k0, K, 2, o->u);
+    if (o->nprev) f.planes(d.nPrev, d.ktot, I.k0, K, 3, o->nprev);
+    if (o->slip) f.planes(d.slip, 0, I.k0, K, 1, o->slip);
+    if (o->Fn) f.planes(d.Fn, 0, I.k0, K, 1, o->Fn);
+    if (o->Ft) f.planes(d.Ft, 0, I.k0, K, 1, o->Ft);
+    if (o->gap) f.planes(d.gap, 0, I.k0, K, 1, o->gap);
+    if (o->stuck) f.bytes(d.stuck + I.k0, K, o->stuck);
+    if (o->state) f.bytes(d.cstate + I.k0, K, o->state);
   }
-  if (o->N) planes(o->N, 1, d.Nax, 0, I.m0, m);
-  if (o->Vsh) planes(o->Vsh, 2, d.Vsh, d.mtot, I.m0, m);
-  if (o->M && p) planes(o->M, 3, d.Mj, d.ptot, I.p0, p);
-  if (o->reactions) planes(o->reactions, 3, d.react, d.ntot, I.n0, n);
+  if (o->N) f.planes(d.Nax, 0, I.m0, m, 1, o->N);
+  if (o->Vsh) f.planes(d.Vsh, d.mtot, I.m0, m, 2, o->Vsh);
+  if (o->M && p) f.planes(d.Mj, d.ptot, I.p0, p, 3, o->M);
+  if (o->reactions) f.planes(d.react, d.ntot, I.n0, n, 3, o->reactions);
+  f.run(c);
 }
 
 // current X, Q, u, nPrev of instance b into its host goals
@@ -561,6 +616,7 @@ void destroyCtx(ws_ctx *c) {
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->st) cudaStreamDestroy(c->st);
+  if (c->pinned) cudaFreeHost(c->pinned);
   delete c;
 }
 
@@ -588,6 +644,7 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
   int rc = guarded("ws_create", [&]() {
     CK(cudaSetDevice(o.device));
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    c->pinnedOK = true;
     CK(cudaEventCreate(&c->ev0));
     CK(cudaEventCreate(&c->ev1));
     c->g.resize(n_instances);
@@ -625,7 +682,8 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     }
     CK(cudaGetLastError());
     CK(cudaMalloc(&c->dPart, sizeof(double) * (RS_NSUM + RX_NMAX) * size_t(std::max(c->shape.blocksA + c->shape.blocksD, c->gridBlocks))));
-    CK(cudaMalloc(&c->dBar, 2 * sizeof(unsigned)));
+    CK(cudaMalloc(&c->dBar, 4 * sizeof(unsigned)));     // [0..1] grid barrier, [2] plain form's finishing-block counter
+    CK(cudaMemsetAsync(c->dBar, 0, 4 * sizeof(unsigned), c->st));
     CK(cudaMalloc(&c->dErr, sizeof(int)));
     DISPATCH(c, setupDev, c);
     size_t total = c->bytes + (sizeof(InstDesc) + sizeof(InstCtl) + 8) * n_instances;

@@ -3,7 +3,20 @@
 #include "dr_kernels.hpp"
 #include "dr_phases.cuh"
 
+#ifndef WSB_MINB
+#define WSB_MINB 1          // minimum resident blocks per SM asked of the large-instance kernels (register budget)
+#endif
+
 namespace wsb {
+
+// element e of phase A: the crossings come first (the heaviest elements start earliest), then segments, joints, clamps
+template <int P>
+__device__ __forceinline__ void phaseA(const Dev<P> &d, const InstDesc &I, int cur, int iter, int e, int nK, Part<typename Dev<P>::A> &pt) {
+  if (e < nK) crossing<P>(d, I, cur, iter, I.k0 + e, pt);
+  else if ((e -= nK) < I.m) segForce<P>(d, cur, I.m0 + e, pt);
+  else if ((e -= I.m) < I.p) jointTorque<P>(d, cur, I.p0 + e, pt);
+  else clampTorque<P>(d, cur, I.c0 + (e - I.p), pt);
+}
 
 // ------------------------------------------------------------------------------------------------ batched form
 // Block b relaxes instance order[b] (and further instances grid-strided) for up to nIter iterations, stopping at its
@@ -29,12 +42,7 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
       const StepCtx sx = makeCtx<A>(I, sc);
       Part<A> pt;
       pt.init();
-      for (int e = threadIdx.x; e < nA; e += blockDim.x) {
-        if (e < I.m) segForce<P>(d, sx.cur, I.m0 + e, pt);
-        else if (e < I.m + I.p) jointTorque<P>(d, sx.cur, I.p0 + (e - I.m), pt);
-        else if (e < I.m + I.p + I.C) clampTorque<P>(d, sx.cur, I.c0 + (e - I.m - I.p), pt);
-        else crossing<P>(d, I, sx.cur, sx.iter, I.k0 + (e - I.m - I.p - I.C), pt);
-      }
+      for (int e = threadIdx.x; e < nA; e += blockDim.x) phaseA<P>(d, I, sx.cur, sx.iter, e, cx ? I.K : 0, pt);
       __syncthreads();
       if (cx) {
         const int n2 = 2 * I.K;
@@ -62,7 +70,7 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
 // One kernel per phase over the elements of instance 0; block partials go to part[phase][block] and k_decide reduces
 // them in a fixed order.  Every kernel returns at once when the instance has stopped.
 template <int P>
-__global__ void __launch_bounds__(256) k_plainA(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
+__global__ void __launch_bounds__(256, WSB_MINB) k_plainA(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
                                                 typename Dev<P>::A *part) {
   using A = typename Dev<P>::A;
   __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
@@ -73,12 +81,7 @@ __global__ void __launch_bounds__(256) k_plainA(Dev<P> d, const InstDesc *__rest
   const int nA = I.m + I.p + I.C + (cx ? I.K : 0);
   Part<A> pt;
   pt.init();
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nA; e += gridDim.x * blockDim.x) {
-    if (e < I.m) segForce<P>(d, c.cur, I.m0 + e, pt);
-    else if (e < I.m + I.p) jointTorque<P>(d, c.cur, I.p0 + (e - I.m), pt);
-    else if (e < I.m + I.p + I.C) clampTorque<P>(d, c.cur, I.c0 + (e - I.m - I.p), pt);
-    else crossing<P>(d, I, c.cur, c.iter, I.k0 + (e - I.m - I.p - I.C), pt);
-  }
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nA; e += gridDim.x * blockDim.x) phaseA<P>(d, I, c.cur, c.iter, e, cx ? I.K : 0, pt);
   blockReduce(pt, red);
   constexpr int NV = RS_NSUM + RX_NMAX;
   if (threadIdx.x == 0) {
@@ -97,11 +100,15 @@ __global__ void __launch_bounds__(256) k_plainBC(Dev<P> d, const InstDesc *__res
     else segCount<P>(d, I.m0 + (e - n2), c.obuf, c.obuf ^ 1);
   }
 }
+// The update kernel also closes the iteration: every block publishes its partials, and the last block to finish
+// (counted on `counter`) reduces the partials of phases A and D in a fixed order and takes the kinetic-damping decision.
 template <int P>
-__global__ void __launch_bounds__(256) k_plainD(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
-                                                typename Dev<P>::A *part) {
+__global__ void __launch_bounds__(256, WSB_MINB) k_plainD(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+                                                typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts,
+                                                unsigned *counter) {
   using A = typename Dev<P>::A;
   __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
+  __shared__ bool last;
   const InstDesc I = insts[0];
   const InstCtl c = ctl[0];
   if (c.status != WS_RUNNING) return;
@@ -117,6 +124,24 @@ __global__ void __launch_bounds__(256) k_plainD(Dev<P> d, const InstDesc *__rest
   if (threadIdx.x == 0) {
     for (int i = 0; i < RS_NSUM; i++) part[blockIdx.x * NV + i] = pt.s[i];
     for (int i = 0; i < RX_NMAX; i++) part[blockIdx.x * NV + RS_NSUM + i] = pt.x[i];
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  Part<A> q;
+  q.init();
+  for (int b = threadIdx.x; b < nParts; b += blockDim.x) {
+    for (int i = 0; i < RS_NSUM; i++) q.s[i] += __ldcg(partAll + b * NV + i);
+    for (int i = 0; i < RX_NMAX; i++) q.x[i] = mmax(q.x[i], __ldcg(partAll + b * NV + RS_NSUM + i));
+  }
+  blockReduce(q, red);
+  if (threadIdx.x == 0) {
+    InstCtl cc = c;
+    decide(I, cc, q, 0);
+    ctl[0] = cc;
+    *counter = 0;
   }
 }
 template <int P>
@@ -168,7 +193,7 @@ __device__ __forceinline__ bool gridSync(unsigned *bar, unsigned nb, int *err) {
 // barriers per iteration.  Block partials go to part[block]; after the barrier every block reduces all of them in the
 // same order and takes the same kinetic-damping decision, so no further broadcast is needed.
 template <int P>
-__global__ void __launch_bounds__(256) k_grid(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+__global__ void __launch_bounds__(256, WSB_MINB) k_grid(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                               typename Dev<P>::A *part, unsigned *bar, int *err, int nIter) {
   using A = typename Dev<P>::A;
   __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
@@ -187,12 +212,7 @@ __global__ void __launch_bounds__(256) k_grid(Dev<P> d, const InstDesc *__restri
     const StepCtx sx = makeCtx<A>(I, sc);
     Part<A> pt;
     pt.init();
-    for (int e = gt; e < nA; e += gs) {
-      if (e < I.m) segForce<P>(d, sx.cur, I.m0 + e, pt);
-      else if (e < I.m + I.p) jointTorque<P>(d, sx.cur, I.p0 + (e - I.m), pt);
-      else if (e < I.m + I.p + I.C) clampTorque<P>(d, sx.cur, I.c0 + (e - I.m - I.p), pt);
-      else crossing<P>(d, I, sx.cur, sx.iter, I.k0 + (e - I.m - I.p - I.C), pt);
-    }
+    for (int e = gt; e < nA; e += gs) phaseA<P>(d, I, sx.cur, sx.iter, e, cx ? I.K : 0, pt);
     if (!gridSync(bar, nb, err)) break;
     if (cx) {
       const int n2 = 2 * I.K;
@@ -235,7 +255,7 @@ cudaError_t launchBatched(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, 
 
 template <int P>
 cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, const PlainShape &sh, bool contacts,
-                            cudaStream_t st, int *launches) {
+                            cudaStream_t st, int *launches, unsigned *counter) {
   using A = typename Dev<P>::A;
   A *pa = static_cast<A *>(part), *pd = pa + size_t(sh.blocksA) * (RS_NSUM + RX_NMAX);
   k_plainA<P><<<sh.blocksA, 256, 0, st>>>(d, insts, ctl, pa);
@@ -244,9 +264,8 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
     k_plainBC<P><<<sh.blocksR, 256, 0, st>>>(d, insts, ctl);
     nl += 1;
   }
-  k_plainD<P><<<sh.blocksD, 256, 0, st>>>(d, insts, ctl, pd);
-  k_plainDecide<P><<<1, 256, 0, st>>>(insts, ctl, pa, sh.blocksA + sh.blocksD);
-  nl += 2;
+  k_plainD<P><<<sh.blocksD, 256, 0, st>>>(d, insts, ctl, pd, pa, sh.blocksA + sh.blocksD, counter);
+  nl += 1;
   if (launches) *launches += nl;
   return cudaGetLastError();
 }
@@ -272,7 +291,7 @@ int gridBlocks() {
   template cudaError_t launchBatched<P>(const Dev<P> &, const InstDesc *, InstCtl *, const int *, int, int, const uint8_t *, \
                                         int, int, cudaStream_t);                                                     \
   template cudaError_t launchPlainIter<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, const PlainShape &, bool,    \
-                                          cudaStream_t, int *);                                                        \
+                                          cudaStream_t, int *, unsigned *);                                                        \
   template cudaError_t launchGrid<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, unsigned *, int *, int, int, cudaStream_t); \
   template int gridBlocks<P>();
 WSB_INST(PREC_F64)

@@ -13,7 +13,7 @@ cudaError_t launchBatched(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, 
                           const uint8_t *mask, int threads, int blocks, cudaStream_t st);
 template <int P>
 cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, const PlainShape &sh, bool contacts,
-                            cudaStream_t st, int *launches);
+                            cudaStream_t st, int *launches, unsigned *counter);
 
 template <int P>
 cudaError_t launchGrid(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, unsigned *bar, int *err, int nIter,

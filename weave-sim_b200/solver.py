@@ -26,12 +26,19 @@ def device_count() -> int:
     return int(lib().ws_device_count())
 
 
-def _state_buffers(md):
+STATE_FIELDS = ("X", "Q", "V", "W", "u", "nprev", "slip", "Fn", "Ft", "gap", "N", "Vsh", "M", "reactions", "stuck", "state")
+
+
+def _state_buffers(md, fields=None):
+    """host arrays for one instance's state and the ws_state_out pointing at them; fields left out stay NULL"""
     n, m, p, K = md.n, md.m, md.p, md.K
-    out = {"X": np.zeros(3 * n), "Q": np.zeros(4 * m), "V": np.zeros(3 * n), "W": np.zeros(3 * m),
-           "u": np.zeros(2 * K), "nprev": np.zeros(3 * K), "slip": np.zeros(K), "Fn": np.zeros(K), "Ft": np.zeros(K),
-           "gap": np.zeros(K), "N": np.zeros(m), "Vsh": np.zeros(2 * m), "M": np.zeros(3 * p),
-           "reactions": np.zeros(3 * n), "stuck": np.zeros(K, dtype=np.uint8), "state": np.zeros(K, dtype=np.uint8)}
+    size = {"X": 3 * n, "Q": 4 * m, "V": 3 * n, "W": 3 * m, "u": 2 * K, "nprev": 3 * K, "slip": K, "Fn": K, "Ft": K,
+            "gap": K, "N": m, "Vsh": 2 * m, "M": 3 * p, "reactions": 3 * n, "stuck": K, "state": K}
+    names = STATE_FIELDS if fields is None else tuple(fields)
+    bad = [k for k in names if k not in size]
+    if bad:
+        raise ValueError(f"unknown state fields {bad}; known: {STATE_FIELDS}")
+    out = {k: np.zeros(size[k], dtype=np.uint8 if k in ("stuck", "state") else np.float64) for k in names}
     so = WsStateOut()
     for k, a in out.items():
         ct = C.c_uint8 if a.dtype == np.uint8 else C.c_double
@@ -107,17 +114,9 @@ class GpuSolver:
         return ms.value, nl.value
 
     # ------------------------------------------------------------------------------------------- state
-    def download(self, b=0) -> dict:
-        md = self.models[b]
-        n, m, p, K = md.n, md.m, md.p, md.K
-        out = {"X": np.zeros(3 * n), "Q": np.zeros(4 * m), "V": np.zeros(3 * n), "W": np.zeros(3 * m),
-               "u": np.zeros(2 * K), "nprev": np.zeros(3 * K), "slip": np.zeros(K), "Fn": np.zeros(K), "Ft": np.zeros(K),
-               "gap": np.zeros(K), "N": np.zeros(m), "Vsh": np.zeros(2 * m), "M": np.zeros(3 * p),
-               "reactions": np.zeros(3 * n), "stuck": np.zeros(K, dtype=np.uint8), "state": np.zeros(K, dtype=np.uint8)}
-        so = WsStateOut()
-        for k, a in out.items():
-            ct = C.c_uint8 if a.dtype == np.uint8 else C.c_double
-            setattr(so, k, a.ctypes.data_as(C.POINTER(ct)) if a.size else None)
+    def download(self, b=0, fields=None) -> dict:
+        """state of instance b (ws_download); `fields` (names of _state_buffers) limits the copy to those arrays"""
+        out, so = _state_buffers(self.models[b], fields)
         check(lib().ws_download(self.h, int(b), C.byref(so)), "ws_download")
         return out
 
