@@ -196,8 +196,11 @@ typedef struct ws_opts {
   int32_t device;       /* CUDA device ordinal */
   uint64_t budget_bytes;/* device memory this context may take (0: no limit) */
   int32_t history;      /* reserved */
-  int32_t pad0;
+  int32_t side_order;   /* WS_SIDES_AUTO: the short-slide side order when the slide limit (contact epsilon) is under half
+                           the shortest segment of the strands with crossings, else the general order;
+                           WS_SIDES_GENERAL: always the general order */
 } ws_opts;
+enum { WS_SIDES_AUTO = 0, WS_SIDES_GENERAL = 1 };
 
 /* Builds the goals of every instance on the host (masses, inertias, clamps: CpuSolver._buildGoals,
  * solver_cpu.js:670-710; contact initialisation: PolylineContact.initialize, solver_cpu.js:99-139) and uploads the
@@ -263,6 +266,10 @@ int ws_relax_noalloc(const ws_model *model, int32_t precision, int32_t n_iter, i
                      ws_state_out *out, ws_control *ctl);
 /* CUDA stream of the context (cudaStream_t) */
 void *ws_stream(ws_ctx *ctx);
+/* side order in use: 1 the short-slide order (the crossing sides are ranked inside the element kernel and a side moves
+ * at most one segment per iteration), 0 the general order (a separate ranking kernel).  No counterpart in the
+ * reference, whose GPU form re-sorts nothing (it accumulates with atomics). */
+int ws_side_order(const ws_ctx *ctx);
 /* device bytes held by the context */
 uint64_t ws_device_bytes(const ws_ctx *ctx);
 /* GPU time of the last ws_step (ms, CUDA events on the context's stream) and the number of kernel launches it made */

@@ -149,3 +149,88 @@ def test_large_shell_plain_against_oracle(oracle_mod):
         ctl, g = _gpu(md, prec, form, it=330)
         assert ctl["iter"] == 330
         assert cases.max_node_err_span(g["X"], v["X"], md.span) < tol
+
+
+# ------------------------------------------------------------------------------------------------ side orders
+# The crossing sides are kept sorted along their strands for the conflict-free gathers.  With the slide limit under half
+# the shortest segment (every scene above) a side moves at most one segment per iteration and the order is ranked
+# inside the element kernel ("short"); otherwise a separate ranking kernel re-sorts it ("general").  Both must give the
+# oracle's result; the general order is forced here on the same scenes, and reached by a warm start that raises the
+# slide limit.
+
+@pytest.mark.parametrize("name", ["cross_press", "cross_stick", "cross_locked"])
+@pytest.mark.parametrize("form", ["cta", "plain", "grid"])
+def test_general_side_order_matches_oracle(oracle_mod, name, form):
+    md = cases.case_by_name(name)
+    v = oracle_mod.Oracle(md.copy()).run(3000)
+    auto = ws.GpuSolver([md.copy()], precision="f64", form=form)
+    assert auto.side_order == "short"
+    auto.dispose()
+    s = ws.GpuSolver([md.copy()], precision="f64", form=form, side_order="general")
+    assert s.side_order == "general"
+    ctl = s.step(3000)[0]
+    g = s.download(0)
+    s.dispose()
+    assert ctl["iter"] == v["iteration"] and ctl["status"] == 1 and ctl["rollbacks"] == v["rollbacks"]
+    assert cases.max_rel_disp_error(g["X"], v["X"], v["X0"]) < 1e-9
+    assert abs(g["Fn"][0] - v["Fn"][0]) < 1e-9 * abs(v["Fn"][0])
+    assert np.array_equal(g["stuck"], v["stuck"])
+
+
+@pytest.mark.parametrize("form", ["cta", "plain", "grid"])
+def test_gridshell_general_order_trajectory(oracle_mod, form):
+    md = ws.configs.dome_small()
+    o = oracle_mod.Oracle(md.copy())
+    o.step(1000)
+    v = o.view()
+    s = ws.GpuSolver([md.copy()], precision="f64", form=form, side_order="general")
+    ctl = s.step(1000)[0]
+    g = s.download(0)
+    s.dispose()
+    assert ctl["iter"] == 1000 and ctl["rollbacks"] == v["rollbacks"]
+    assert cases.max_node_err_span(g["X"], v["X"], md.span) < 1e-9
+    assert np.abs(g["u"] - v["u"]).max() < 1e-9
+    assert np.array_equal(g["stuck"], v["stuck"])
+
+
+@pytest.mark.parametrize("form", ["cta", "plain"])
+def test_warm_start_switches_side_order(oracle_mod, form):
+    """a slide limit above half a segment (5.05 cm segments, epsilon 3 cm) switches the running instance to the general
+    order, and back; the trajectory stays the oracle's"""
+    md = ws.configs.dome_small()
+    wide = md.copy()
+    wide.params = dict(md.params, epsilon=0.03)
+    o = oracle_mod.Oracle(md.copy())
+    o.step(400)
+    o.rebuild(wide)
+    o.step(300)
+    o.rebuild(md.copy())
+    o.step(300)
+    v = o.view()
+    s = ws.GpuSolver([md.copy()], precision="f64", form=form)
+    assert s.side_order == "short"
+    s.step(400)
+    s.update_params(0, wide)
+    assert s.side_order == "general"
+    s.step(300)
+    s.update_params(0, md.copy())
+    assert s.side_order == "short"
+    ctl = s.step(300)[0]
+    g = s.download(0)
+    s.dispose()
+    assert ctl["iter"] == 1000
+    assert cases.max_node_err_span(g["X"], v["X"], md.span) < 1e-9
+    assert np.abs(g["u"] - v["u"]).max() < 1e-9
+
+
+def test_large_shell_general_order_against_oracle(oracle_mod):
+    md = ws.configs.shell_large()
+    o = oracle_mod.Oracle(md.copy())
+    o.step(330)
+    v = o.view()
+    s = ws.GpuSolver([md.copy()], precision="f64", form="plain", side_order="general")
+    ctl = s.step(330)[0]
+    g = s.download(0)
+    s.dispose()
+    assert ctl["iter"] == 330
+    assert cases.max_node_err_span(g["X"], v["X"], md.span) < 1e-9

@@ -66,19 +66,28 @@ void layout(Dev<P> &d, Carver &cv, const Sizes &z) {
   d.cw = cv.take<R>(k); d.ch = cv.take<R>(k); d.mu = cv.take<R>(k); d.cflag = cv.take<uint8_t>(k);
   d.u = cv.take<U>(2 * k); d.nPrev = cv.take<R>(3 * k); d.slip = cv.take<A>(k); d.stuck = cv.take<uint8_t>(k);
   d.cstate = cv.take<uint8_t>(k); d.Fn = cv.take<R>(k); d.Ft = cv.take<R>(k); d.gap = cv.take<R>(k);
-  d.sSeg = cv.take<int>(2 * k); d.sKey = cv.take<int>(2 * k); d.sStrand = cv.take<int>(2 * k); d.sT = cv.take<R>(2 * k); d.kth = cv.take<R>(k); d.sF = cv.take<R>(6 * k); d.sTq = cv.take<R>(6 * k);
-  d.stSideOff = cv.take<int>(s); d.stSideCnt = cv.take<int>(s); d.ord = cv.take<int>(4 * k); d.ordSeg = cv.take<int>(4 * k);
+  d.sPos = cv.take<int>(2 * k); d.sKey = cv.take<int>(4 * k); d.sStrand = cv.take<int>(2 * k); d.sT = cv.take<R>(2 * k);
+  d.kth = cv.take<R>(2 * k); d.sF = cv.take<R>(6 * k); d.sTq = cv.take<R>(6 * k);
+  d.stSideOff = cv.take<int>(s); d.stSideCnt = cv.take<int>(s); d.stSegOff = cv.take<int>(s);
+  d.ord = cv.take<int>(4 * k); d.ordSeg = cv.take<int>(4 * k);
 }
 
-// host -> device with conversion
+// host -> device with conversion, batched: put() converts into a host buffer and queues the copy; flushPuts() sends the
+// queue through the context's staging buffer with one synchronisation.  Every entry point that puts flushes before it
+// returns (and a failed one drops its queue), so nothing queued outlives the call that queued it.
+struct PendingPut { void *dst; size_t off, bytes; };
+thread_local std::vector<char> t_putHost;
+thread_local std::vector<PendingPut> t_puts;
 template <class T, class V>
-void put(T *dst, const V *src, size_t count, cudaStream_t st) {
+void put(T *dst, const V *src, size_t count, cudaStream_t) {
   if (!count) return;
-  std::vector<T> tmp(count);
-  for (size_t i = 0; i < count; i++) tmp[i] = T(src[i]);
-  CK(cudaMemcpyAsync(dst, tmp.data(), count * sizeof(T), cudaMemcpyHostToDevice, st));
-  CK(cudaStreamSynchronize(st));
+  const size_t off = t_putHost.size(), bytes = count * sizeof(T);
+  t_putHost.resize(off + ((bytes + 15) & ~size_t(15)));
+  T *h = reinterpret_cast<T *>(t_putHost.data() + off);
+  for (size_t i = 0; i < count; i++) h[i] = T(src[i]);
+  t_puts.push_back({dst, off, bytes});
 }
+void dropPuts() { t_puts.clear(); t_putHost.clear(); }
 template <class T>
 void getv(std::vector<double> &out, const T *src, size_t count, cudaStream_t st) {
   std::vector<T> tmp(count);
@@ -109,10 +118,12 @@ struct ws_ctx {
   void *dPart = nullptr;
   unsigned *dBar = nullptr;   // grid form: barrier counter + generation, and its timeout flag
   int *dErr = nullptr;
-  int gridBlocks = 0;
+  int gridBlocks[2] = {0, 0};   // grid form: co-resident blocks with the general / short-slide side order
   PlainShape shape{};
+  int sidesGeneral = 0;          // ws_opts.side_order == WS_SIDES_GENERAL
+  bool shortSides = false;       // the short-slide side order is in use
   cudaGraphExec_t graph = nullptr;
-  int graphIters = 0;
+  int graphIters = 0, graphKey = -1;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double lastMs = 0;
   int64_t lastLaunches = 0;
@@ -140,6 +151,15 @@ char *stageBuf(ws_ctx *c, size_t bytes) {
     c->pinnedCap = bytes;
   }
   return c->pinned;
+}
+
+void flushPuts(ws_ctx *c) {
+  if (t_puts.empty()) return;
+  char *buf = stageBuf(c, t_putHost.size());
+  std::memcpy(buf, t_putHost.data(), t_putHost.size());
+  for (const PendingPut &q : t_puts) CK(cudaMemcpyAsync(q.dst, buf + q.off, q.bytes, cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  dropPuts();
 }
 
 // device -> host in one go: planes are queued, copied asynchronously into the staging buffer, and converted to the
@@ -277,16 +297,19 @@ void uploadGoals(ws_ctx *c, int b) {
   put<uint8_t>(d.cflag + I.k0, cf.data(), K, st);
 }
 
-// upload the sorted side lists and segment slices of instance b into sorted-side buffer `buf`
+// upload the sorted side lists, segment slices and side keys (the segments the sides sit on now) of instance b into
+// sorted-side buffer `buf`
 template <int P>
 void uploadOrder(ws_ctx *c, int b, int buf) {
   Dev<P> &d = devOf<P>(c);
   const HostGoals &g = c->g[b];
   const InstDesc &I = c->inst[b];
   const size_t K2 = 2 * size_t(d.ktot), K = g.K, m = g.m;
-  std::vector<int> ord(2 * K), lo(m), hi(m);
-  for (size_t q = 0; q < 2 * K; q++) ord[q] = 2 * I.k0 + g.ord[q];
+  std::vector<int> ord(2 * K), lo(m), hi(m), key(2 * K);
+  for (size_t q = 0; q < 2 * K; q++) ord[q] = 2 * I.k0 + g.sidePos[g.ord[q]];
+  for (size_t q = 0; q < 2 * K; q++) key[q] = g.sideSegLocal(g.sideList[q]);
   for (size_t j = 0; j < m; j++) { lo[j] = 2 * I.k0 + g.rngLo[j]; hi[j] = 2 * I.k0 + g.rngHi[j]; }
+  put<int>(d.sKey + buf * K2 + 2 * size_t(I.k0), key.data(), 2 * K, c->st);
   put<int>(d.ord + buf * K2 + 2 * size_t(I.k0), ord.data(), 2 * K, c->st);
   put<int>(d.ordSeg + buf * K2 + 2 * size_t(I.k0), g.ordSeg.data(), 2 * K, c->st);
   put<int>(d.rngLo + size_t(buf) * d.mtot + I.m0, lo.data(), m, c->st);
@@ -366,10 +389,10 @@ void uploadStatic(ws_ctx *c, int b) {
     put<R>(d.hk + size_t(side) * d.ktot + I.k0, h.data(), K, st);
   }
   {
-    std::vector<int> ss(2 * K), sk(2 * K);
-    for (size_t q = 0; q < 2 * K; q++) { ss[q] = I.s0 + g.cxStrand[q]; sk[q] = g.sideSegLocal(int(q)); }
+    std::vector<int> ss(2 * K), sp(2 * K);
+    for (size_t q = 0; q < 2 * K; q++) { ss[q] = I.s0 + g.cxStrand[g.sideList[q]]; sp[q] = 2 * I.k0 + g.sidePos[q]; }
     put<int>(d.sStrand + 2 * size_t(I.k0), ss.data(), 2 * K, st);
-    put<int>(d.sKey + 2 * size_t(I.k0), sk.data(), 2 * K, st);
+    put<int>(d.sPos + 2 * size_t(I.k0), sp.data(), 2 * K, st);
   }
   put<R>(d.cw + I.k0, g.w.data(), K, st);
   put<R>(d.ch + I.k0, g.h.data(), K, st);
@@ -377,6 +400,9 @@ void uploadStatic(ws_ctx *c, int b) {
   for (size_t s = 0; s < S; s++) { so[s] = 2 * I.k0 + g.strandSideOff[s]; sc[s] = g.strandSideCnt[s]; }
   put<int>(d.stSideOff + I.s0, so.data(), S, st);
   put<int>(d.stSideCnt + I.s0, sc.data(), S, st);
+  std::vector<int> sg(S, 0);
+  for (size_t q = 0; q < 2 * K; q++) sg[g.cxStrand[q]] = I.m0 + g.cxSegOff[q];
+  put<int>(d.stSegOff + I.s0, sg.data(), S, st);
   std::vector<uint8_t> one(K, 1);
   put<uint8_t>(d.stuck + I.k0, one.data(), K, st);
 }
@@ -391,6 +417,19 @@ void uploadAll(ws_ctx *c) {
     uploadOrder<P>(c, int(b), 0);
     uploadOrder<P>(c, int(b), 1);
   }
+  flushPuts(c);
+}
+
+// the short-slide side order holds when, in every instance with contacts, the slide limit (epsilon) is under half the
+// shortest segment of the strands with crossings: a slide then moves a side by less than one segment per iteration
+// (a segment would have to shorten by half to break it)
+bool shortOrderOK(const ws_ctx *c) {
+  if (c->sidesGeneral) return false;
+  for (const HostGoals &g : c->g) {
+    if (!g.K || !g.prm.contacts) continue;
+    if (!(std::max(g.prm.epsilon, 1e-9) < 0.5 * g.sideSegMin())) return false;
+  }
+  return true;
 }
 
 template <int P>
@@ -425,32 +464,36 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
   if (c->form == WS_FORM_CTA) {
     if (mask) CK(cudaMemcpyAsync(c->dMask, mask, nInst, cudaMemcpyHostToDevice, c->st));
     const int thr = c->threads > 0 ? c->threads : 256;
-    CK(launchBatched<P>(devOf<P>(c), c->dInst, c->dCtl, c->dOrder, nInst, nIter, mask ? c->dMask : nullptr, thr, nInst, c->st));
+    CK(launchBatched<P>(devOf<P>(c), c->dInst, c->dCtl, c->dOrder, nInst, nIter, mask ? c->dMask : nullptr, thr, nInst, c->shortSides, c->st));
     c->lastLaunches = 1;
   } else if (c->form == WS_FORM_GRID) {
     CK(cudaMemsetAsync(c->dBar, 0, 2 * sizeof(unsigned), c->st));
     CK(cudaMemsetAsync(c->dErr, 0, sizeof(int), c->st));
-    if (nIter > 0) CK(launchGrid<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->dBar, c->dErr, nIter, c->gridBlocks, c->st));
+    if (nIter > 0)
+      CK(launchGrid<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->dBar, c->dErr, nIter, c->gridBlocks[c->shortSides], c->shortSides, c->st));
     c->lastLaunches = 1;
   } else {
     const bool cx = c->inst[0].contacts && c->inst[0].K;
+    const bool sh = c->shortSides;
     const int chunk = std::min(nIter, 50);
-    if (chunk > 0 && (!c->graph || c->graphIters != chunk)) {
+    const int key = (chunk << 2) | (cx ? 2 : 0) | (sh ? 1 : 0);
+    if (chunk > 0 && (!c->graph || c->graphKey != key)) {
       if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
       cudaGraph_t gr;
       CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
       int nl = 0;
-      for (int i = 0; i < chunk; i++) CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, c->st, &nl, c->dBar + 2));
+      for (int i = 0; i < chunk; i++) CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, c->st, &nl, c->dBar + 2));
       CK(cudaStreamEndCapture(c->st, &gr));
       CK(cudaGraphInstantiate(&c->graph, gr, 0));
       cudaGraphDestroy(gr);
       c->graphIters = chunk;
+      c->graphKey = key;
     }
     int done = 0;
-    const int per = cx ? 3 : 2;
+    const int per = (cx && !sh) ? 3 : 2;
     while (nIter - done >= chunk && chunk > 0) { CK(cudaGraphLaunch(c->graph, c->st)); done += chunk; c->lastLaunches += int64_t(chunk) * per; }
     int nl = 0;
-    for (; done < nIter; done++) CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, c->st, &nl, c->dBar + 2));
+    for (; done < nIter; done++) CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, c->st, &nl, c->dBar + 2));
     c->lastLaunches += nl;
   }
   CK(cudaEventRecord(c->ev1, c->st));
@@ -504,6 +547,22 @@ void pullState(ws_ctx *c, int b) {
   if (g.K) { g.u = u; g.nPrev = np; }
 }
 
+// a warm start may change the slide limit or switch contacts: on a change of side order, every instance's order and
+// keys are rebuilt from its current slide coordinates into the buffer its next iteration reads
+template <int P>
+void reselectOrder(ws_ctx *c) {
+  const bool ok = shortOrderOK(c);
+  if (ok == c->shortSides) return;
+  readCtl(c);
+  for (size_t b = 0; b < c->g.size(); b++) {
+    pullState<P>(c, int(b));
+    c->g[b].sortSides();
+    uploadOrder<P>(c, int(b), c->ctlHost[b].obuf);
+  }
+  flushPuts(c);
+  c->shortSides = ok;
+}
+
 template <int P>
 void setParamsImpl(ws_ctx *c, int b, const ws_model *md) {
   pullState<P>(c, b);
@@ -518,11 +577,13 @@ void setParamsImpl(ws_ctx *c, int b, const ws_model *md) {
   c->inst[b] = describe(g, off);
   CK(cudaMemcpyAsync(c->dInst + b, &c->inst[b], sizeof(InstDesc), cudaMemcpyHostToDevice, c->st));
   uploadGoals<P>(c, b);
+  flushPuts(c);
   readCtl(c);
   InstCtl s = c->ctlHost[b];
   s.ke_prev = 0.0; s.status = WS_RUNNING; s.disp_it0 = s.iter;
   CK(cudaMemcpyAsync(c->dCtl + b, &s, sizeof(InstCtl), cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
+  reselectOrder<P>(c);
 }
 
 template <int P>
@@ -548,9 +609,13 @@ void loadInstanceImpl(ws_ctx *c, int b, const ws_model *md) {
   std::memset(&s, 0, sizeof(s));
   s.status = WS_RUNNING; s.residual = INFINITY;
   uploadState<P>(c, b, 0, true);
+  // both buffers: a slice left over from the slot's previous model could point into another strand's sides
   uploadOrder<P>(c, b, 0);
+  uploadOrder<P>(c, b, 1);
+  flushPuts(c);
   CK(cudaMemcpyAsync(c->dCtl + b, &s, sizeof(InstCtl), cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
+  reselectOrder<P>(c);
 }
 
 template <int P>
@@ -562,7 +627,7 @@ void uploadStateImpl(ws_ctx *c, int b, const double *X, const double *Q, const d
   g.Q.assign(Q, Q + 4 * size_t(g.m));
   if (u && g.K) g.u.assign(u, u + 2 * size_t(g.K));
   uploadState<P>(c, b, s.cur, u != nullptr);
-  if (u && g.K) { g.sortSides(); uploadOrder<P>(c, b, s.obuf); }
+  if (u && g.K) { g.sortSides(); uploadOrder<P>(c, b, s.obuf); flushPuts(c); }
   s.pending = 0; s.ke_prev = 0.0; s.status = WS_RUNNING;
   CK(cudaMemcpyAsync(c->dCtl + b, &s, sizeof(InstCtl), cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -581,6 +646,7 @@ void internalizeImpl(ws_ctx *c, int b) {
 
 template <class F>
 int guarded(const char *what, F &&f) {
+  struct Drop { ~Drop() { dropPuts(); } } drop;     // nothing queued outlives the call, failed or not
   try {
     f();
     return WS_OK;
@@ -641,6 +707,8 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
   if (ws_device_count() <= 0) return fail(WS_ERR_NODEV, "ws_create: no CUDA device (this library has no CPU path)");
   auto c = new ws_ctx();
   c->prec = o.precision; c->form = o.form; c->threads = o.threads; c->device = o.device;
+  if (o.side_order < 0 || o.side_order > 1) { delete c; return fail(WS_ERR_ARG, "ws_create: unknown side order"); }
+  c->sidesGeneral = o.side_order == WS_SIDES_GENERAL;
   int rc = guarded("ws_create", [&]() {
     CK(cudaSetDevice(o.device));
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
@@ -672,19 +740,23 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     const InstDesc &I0 = c->inst[0];
     auto blocks = [](long long cnt, int thr) { return int(std::max<long long>(1, std::min<long long>((cnt + thr - 1) / thr, 148LL * 8))); };
     c->shape.blocksA = blocks(I0.m + I0.p + I0.C + I0.K, 256);
-    c->shape.blocksS = blocks(I0.S, 128);
+    c->shape.blocksAS = blocks(I0.m + I0.p + I0.C + 3LL * I0.K, 256);
     c->shape.blocksR = blocks(I0.m + 2LL * I0.K, 256);
     c->shape.blocksD = blocks(I0.n + I0.m, 256);
-    switch (c->prec) {
-      case WS_PREC_F64: c->gridBlocks = gridBlocks<PREC_F64>(); break;
-      case WS_PREC_MIXED: c->gridBlocks = gridBlocks<PREC_MIXED>(); break;
-      default: c->gridBlocks = gridBlocks<PREC_F32>(); break;
+    for (int sh = 0; sh < 2; sh++) {
+      switch (c->prec) {
+        case WS_PREC_F64: c->gridBlocks[sh] = gridBlocks<PREC_F64>(sh != 0); break;
+        case WS_PREC_MIXED: c->gridBlocks[sh] = gridBlocks<PREC_MIXED>(sh != 0); break;
+        default: c->gridBlocks[sh] = gridBlocks<PREC_F32>(sh != 0); break;
+      }
     }
     CK(cudaGetLastError());
-    CK(cudaMalloc(&c->dPart, sizeof(double) * (RS_NSUM + RX_NMAX) * size_t(std::max(c->shape.blocksA + c->shape.blocksD, c->gridBlocks))));
+    const int parts = std::max({c->shape.blocksAS + c->shape.blocksD, c->shape.blocksA + c->shape.blocksD, c->gridBlocks[0], c->gridBlocks[1]});
+    CK(cudaMalloc(&c->dPart, sizeof(double) * (RS_NSUM + RX_NMAX) * size_t(parts)));
     CK(cudaMalloc(&c->dBar, 4 * sizeof(unsigned)));     // [0..1] grid barrier, [2] plain form's finishing-block counter
     CK(cudaMemsetAsync(c->dBar, 0, 4 * sizeof(unsigned), c->st));
     CK(cudaMalloc(&c->dErr, sizeof(int)));
+    c->shortSides = shortOrderOK(c);
     DISPATCH(c, setupDev, c);
     size_t total = c->bytes + (sizeof(InstDesc) + sizeof(InstCtl) + 8) * n_instances;
     if (o.budget_bytes && total > o.budget_bytes) throw std::bad_alloc();
@@ -744,6 +816,7 @@ int ws_internalize(ws_ctx *c, int32_t b) {
 
 void *ws_stream(ws_ctx *c) { return c ? c->st : nullptr; }
 uint64_t ws_device_bytes(const ws_ctx *c) { return c ? c->bytes : 0; }
+int ws_side_order(const ws_ctx *c) { return c && c->shortSides ? 1 : 0; }
 int ws_last_step_stats(const ws_ctx *c_, double *ms, int64_t *launches) {
   if (!c_) return fail(WS_ERR_ARG, "ws_last_step_stats: null context");
   ws_ctx *c = const_cast<ws_ctx *>(c_);
@@ -799,7 +872,7 @@ static void runInPlaceImpl(ws_ctx *c, char *base, int nIter, int threads, ws_sta
   s.status = WS_RUNNING; s.residual = INFINITY;
   CK(cudaMemcpyAsync(c->dCtl, &s, sizeof(InstCtl), cudaMemcpyHostToDevice, c->st));
   uploadAll<P>(c);
-  if (nIter > 0) CK(launchBatched<P>(devOf<P>(c), c->dInst, c->dCtl, nullptr, 1, nIter, nullptr, threads, 1, c->st));
+  if (nIter > 0) CK(launchBatched<P>(devOf<P>(c), c->dInst, c->dCtl, nullptr, 1, nIter, nullptr, threads, 1, c->shortSides, c->st));
   CK(cudaStreamSynchronize(c->st));
   if (out) downloadImpl<P>(c, 0, out);
   if (ctl) { readCtl(c); fillControl(c->ctlHost[0], ctl); }
@@ -813,6 +886,7 @@ int runInPlace(int prec, const HostGoals &g, char *base, int nIter, int threads,
   Sizes off;
   tmp.inst.push_back(describe(tmp.g[0], off));
   tmp.z.n = g.n; tmp.z.m = g.m; tmp.z.p = g.p; tmp.z.c = g.C; tmp.z.k = g.K; tmp.z.s = g.S;
+  tmp.shortSides = shortOrderOK(&tmp);
   try {
     switch (prec) {
       case WS_PREC_F64: runInPlaceImpl<PREC_F64>(&tmp, base, nIter, threads, out, ctl); break;
@@ -820,6 +894,7 @@ int runInPlace(int prec, const HostGoals &g, char *base, int nIter, int threads,
       default: runInPlaceImpl<PREC_F32>(&tmp, base, nIter, threads, out, ctl); break;
     }
   } catch (const std::exception &e) {
+    dropPuts();
     err = e.what();
     return WS_ERR_CUDA;
   }

@@ -86,14 +86,17 @@ struct Dev {
   A *slip;                  // [ktot]
   uint8_t *stuck, *cstate;  // [ktot]
   R *Fn, *Ft, *gap;         // [ktot]
-  int *sSeg;                // [2 ktot] side records (side id sd = 2c + side)
-  int *sKey;                // [2 ktot] local segment of the side after this iteration's slide
+  // side records, indexed by side position p: the sides (sd = 2c + side) grouped by strand, ascending sd within a
+  // strand (the strand's range is [stSideOff, stSideOff + stSideCnt))
+  int *sPos;                // [2 ktot] position of side sd
+  int *sKey;                // [2][2 ktot] local segment of the side after the slide, by sorted-side buffer
   int *sStrand;             // [2 ktot] strand of the side
-  R *sT, *kth;              // [2 ktot], [ktot]
-  R *sF, *sTq;              // [3][2 ktot]
+  R *sT, *kth;              // [2 ktot] Hermite parameter before the slide; righting stiffness of the side's crossing
+  R *sF, *sTq;              // [3][2 ktot] force on the side; lever torque
   // strands
   int *stSideOff, *stSideCnt;   // [stot]
-  int *ord, *ordSeg;            // [2][2 ktot]
+  int *stSegOff;                // [stot] first (global) segment of the strand
+  int *ord, *ordSeg;            // [2][2 ktot] side positions sorted by (local segment, position) per strand; their keys
 };
 
 }  // namespace wsb

@@ -3,26 +3,77 @@
 #include "dr_kernels.hpp"
 #include "dr_phases.cuh"
 
-#ifndef WSB_MINB
-#define WSB_MINB 1          // minimum resident blocks per SM asked of the large-instance kernels (register budget)
+// Minimum resident blocks of 256 threads per SM asked of the large-instance kernels, i.e. their register budget
+// (65536 / (256 × blocks) registers a thread).  The kernels are bound by load latency at low occupancy: the update
+// kernel gains from 4 blocks (64 registers, a few spills) more than it loses; the element kernel, heavier in live
+// values, does best unbounded; the grid form at 2.
+#ifndef WSB_MINB_A
+#define WSB_MINB_A 1
+#endif
+#ifndef WSB_MINB_D
+#define WSB_MINB_D 4
+#endif
+#ifndef WSB_MINB_G
+#define WSB_MINB_G 2
 #endif
 
 namespace wsb {
 
-// element e of phase A: the crossings come first (the heaviest elements start earliest), then segments, joints, clamps
+// Programmatic dependent launch: a kernel of the plain form lets the next one be launched as soon as all its blocks
+// have started, and waits for the previous one (completion and memory) before it reads anything.  Launched without the
+// attribute, both instructions do nothing.
+__device__ __forceinline__ void waitPrevGrid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void allowNextGrid() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
+// Block partials, value-major: slot i of block b at part[i * stride + b], so the finishing block reads them coalesced.
+template <class A>
+__device__ __forceinline__ void putPart(const Part<A> &p, A *part, int b, int stride) {
+  for (int i = 0; i < RS_NSUM; i++) part[size_t(i) * stride + b] = p.s[i];
+  for (int i = 0; i < RX_NMAX; i++) part[size_t(RS_NSUM + i) * stride + b] = p.x[i];
+}
+template <class A>
+__device__ __forceinline__ void addPart(Part<A> &q, const A *part, int b, int stride) {
+  for (int i = 0; i < RS_NSUM; i++) q.s[i] += __ldcg(part + size_t(i) * stride + b);
+  for (int i = 0; i < RX_NMAX; i++) q.x[i] = mmax(q.x[i], __ldcg(part + size_t(RS_NSUM + i) * stride + b));
+}
+
+// element e of phase A: the crossings come first (the heaviest elements start earliest); under SHORT the ranks of the
+// sides follow (the order this iteration's gathers read); then segments, joints, clamps
+template <int P, bool SHORT>
+__device__ __forceinline__ void phaseA(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, int e, int nK, Part<typename Dev<P>::A> &pt) {
+  if (e < nK) { crossing<P>(d, I, sx.cur, sx.iter, sx.onxt, I.k0 + e, pt); return; }
+  e -= nK;
+  if constexpr (SHORT) {
+    if (e < 2 * nK) { rankSideShort<P>(d, 2 * I.k0 + e, sx.obuf); return; }
+    e -= 2 * nK;
+  }
+  if (e < I.m) segForce<P>(d, sx.cur, I.m0 + e, pt);
+  else if ((e -= I.m) < I.p) jointTorque<P>(d, sx.cur, I.p0 + e, pt);
+  else clampTorque<P>(d, sx.cur, I.c0 + (e - I.p), pt);
+}
+template <bool SHORT>
+__device__ __forceinline__ int countA(const InstDesc &I) {
+  const int nK = (I.contacts && I.K) ? I.K : 0;
+  return I.m + I.p + I.C + nK + (SHORT ? 2 * nK : 0);
+}
+// phase B / C of the general order: the ranks of the sides and the slices of the segments in the new order
 template <int P>
-__device__ __forceinline__ void phaseA(const Dev<P> &d, const InstDesc &I, int cur, int iter, int e, int nK, Part<typename Dev<P>::A> &pt) {
-  if (e < nK) crossing<P>(d, I, cur, iter, I.k0 + e, pt);
-  else if ((e -= nK) < I.m) segForce<P>(d, cur, I.m0 + e, pt);
-  else if ((e -= I.m) < I.p) jointTorque<P>(d, cur, I.p0 + e, pt);
-  else clampTorque<P>(d, cur, I.c0 + (e - I.p), pt);
+__device__ __forceinline__ void phaseBC(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, int e) {
+  const int n2 = 2 * I.K;
+  if (e < n2) rankSide<P>(d, 2 * I.k0 + e, sx.onxt, sx.onxt);
+  else segCount<P>(d, I.m0 + (e - n2), sx.onxt, sx.onxt);
+}
+template <int P, bool SHORT>
+__device__ __forceinline__ void phaseD(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, int e, Part<typename Dev<P>::A> &pt) {
+  if (e < I.n) nodeUpdate<P, SHORT>(d, I, sx, I.n0 + e, pt);
+  else segUpdate<P, SHORT>(d, I, sx, I.m0 + (e - I.n), pt);
 }
 
 // ------------------------------------------------------------------------------------------------ batched form
 // Block b relaxes instance order[b] (and further instances grid-strided) for up to nIter iterations, stopping at its
 // own convergence.  Instance state lives in HBM / L2; the block's barriers separate the phases, so an instance never
 // waits on another and no kernel spins.
-template <int P>
+template <int P, bool SHORT>
 __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                                   const int *__restrict__ order, int nInst, int nIter, const uint8_t *__restrict__ mask) {
   using A = typename Dev<P>::A;
@@ -36,26 +87,19 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
     __syncthreads();
     const InstDesc &I = si;
     const bool cx = I.contacts && I.K;
-    const int nA = I.m + I.p + I.C + (cx ? I.K : 0);
+    const int nA = countA<SHORT>(I);
     for (int it = 0; it < nIter; it++) {
       if (sc.status != WS_RUNNING) break;
       const StepCtx sx = makeCtx<A>(I, sc);
       Part<A> pt;
       pt.init();
-      for (int e = threadIdx.x; e < nA; e += blockDim.x) phaseA<P>(d, I, sx.cur, sx.iter, e, cx ? I.K : 0, pt);
+      for (int e = threadIdx.x; e < nA; e += blockDim.x) phaseA<P, SHORT>(d, I, sx, e, cx ? I.K : 0, pt);
       __syncthreads();
-      if (cx) {
-        const int n2 = 2 * I.K;
-        for (int e = threadIdx.x; e < n2 + I.m; e += blockDim.x) {
-          if (e < n2) rankSide<P>(d, 2 * I.k0 + e, sx.obuf, sx.onxt);
-          else segCount<P>(d, I.m0 + (e - n2), sx.obuf, sx.onxt);
-        }
+      if (!SHORT && cx) {
+        for (int e = threadIdx.x; e < 2 * I.K + I.m; e += blockDim.x) phaseBC<P>(d, I, sx, e);
         __syncthreads();
       }
-      for (int e = threadIdx.x; e < I.n + I.m; e += blockDim.x) {
-        if (e < I.n) nodeUpdate<P>(d, I, sx, I.n0 + e, pt);
-        else segUpdate<P>(d, I, sx, I.m0 + (e - I.n), pt);
-      }
+      for (int e = threadIdx.x; e < I.n + I.m; e += blockDim.x) phaseD<P, SHORT>(d, I, sx, e, pt);
       __syncthreads();
       blockReduce(pt, red);
       if (threadIdx.x == 0) decide(I, sc, pt, nIter);
@@ -67,63 +111,59 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
 }
 
 // ------------------------------------------------------------------------------------------------ plain form
-// One kernel per phase over the elements of instance 0; block partials go to part[phase][block] and k_decide reduces
-// them in a fixed order.  Every kernel returns at once when the instance has stopped.
-template <int P>
-__global__ void __launch_bounds__(256, WSB_MINB) k_plainA(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
-                                                typename Dev<P>::A *part) {
+// One kernel per phase over the elements of instance 0; block partials go to part[block] and the last block of the
+// update kernel reduces them in a fixed order.  Every kernel returns at once when the instance has stopped.
+template <int P, bool SHORT>
+__global__ void __launch_bounds__(256, WSB_MINB_A) k_plainA(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
+                                                typename Dev<P>::A *part, int partStride) {
   using A = typename Dev<P>::A;
   __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
-  const InstDesc I = insts[0];
+  waitPrevGrid();
+  allowNextGrid();
+  const InstDesc &I = insts[0];
   const InstCtl c = ctl[0];
   if (c.status != WS_RUNNING) return;
   const bool cx = I.contacts && I.K;
-  const int nA = I.m + I.p + I.C + (cx ? I.K : 0);
+  const int nA = countA<SHORT>(I);
+  const StepCtx sx = makeCtx<A>(I, c);
   Part<A> pt;
   pt.init();
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nA; e += gridDim.x * blockDim.x) phaseA<P>(d, I, c.cur, c.iter, e, cx ? I.K : 0, pt);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nA; e += gridDim.x * blockDim.x) phaseA<P, SHORT>(d, I, sx, e, cx ? I.K : 0, pt);
   blockReduce(pt, red);
-  constexpr int NV = RS_NSUM + RX_NMAX;
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < RS_NSUM; i++) part[blockIdx.x * NV + i] = pt.s[i];
-    for (int i = 0; i < RX_NMAX; i++) part[blockIdx.x * NV + RS_NSUM + i] = pt.x[i];
-  }
+  if (threadIdx.x == 0) putPart(pt, part, blockIdx.x, partStride);
 }
 template <int P>
 __global__ void __launch_bounds__(256) k_plainBC(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl) {
-  const InstDesc I = insts[0];
+  using A = typename Dev<P>::A;
+  waitPrevGrid();
+  allowNextGrid();
+  const InstDesc &I = insts[0];
   const InstCtl c = ctl[0];
   if (c.status != WS_RUNNING) return;
-  const int n2 = 2 * I.K;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n2 + I.m; e += gridDim.x * blockDim.x) {
-    if (e < n2) rankSide<P>(d, 2 * I.k0 + e, c.obuf, c.obuf ^ 1);
-    else segCount<P>(d, I.m0 + (e - n2), c.obuf, c.obuf ^ 1);
-  }
+  const StepCtx sx = makeCtx<A>(I, c);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 2 * I.K + I.m; e += gridDim.x * blockDim.x) phaseBC<P>(d, I, sx, e);
 }
 // The update kernel also closes the iteration: every block publishes its partials, and the last block to finish
 // (counted on `counter`) reduces the partials of phases A and D in a fixed order and takes the kinetic-damping decision.
-template <int P>
-__global__ void __launch_bounds__(256, WSB_MINB) k_plainD(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+template <int P, bool SHORT>
+__global__ void __launch_bounds__(256, WSB_MINB_D) k_plainD(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                                 typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts,
-                                                unsigned *counter) {
+                                                int partStride, unsigned *counter) {
   using A = typename Dev<P>::A;
   __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
   __shared__ bool last;
-  const InstDesc I = insts[0];
+  waitPrevGrid();
+  allowNextGrid();
+  const InstDesc &I = insts[0];
   const InstCtl c = ctl[0];
   if (c.status != WS_RUNNING) return;
   const StepCtx sx = makeCtx<A>(I, c);
   Part<A> pt;
   pt.init();
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < I.n + I.m; e += gridDim.x * blockDim.x) {
-    if (e < I.n) nodeUpdate<P>(d, I, sx, I.n0 + e, pt);
-    else segUpdate<P>(d, I, sx, I.m0 + (e - I.n), pt);
-  }
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < I.n + I.m; e += gridDim.x * blockDim.x) phaseD<P, SHORT>(d, I, sx, e, pt);
   blockReduce(pt, red);
-  constexpr int NV = RS_NSUM + RX_NMAX;
   if (threadIdx.x == 0) {
-    for (int i = 0; i < RS_NSUM; i++) part[blockIdx.x * NV + i] = pt.s[i];
-    for (int i = 0; i < RX_NMAX; i++) part[blockIdx.x * NV + RS_NSUM + i] = pt.x[i];
+    putPart(pt, part, blockIdx.x, partStride);
     __threadfence();
     last = atomicAdd(counter, 1u) == gridDim.x - 1;
   }
@@ -132,35 +172,13 @@ __global__ void __launch_bounds__(256, WSB_MINB) k_plainD(Dev<P> d, const InstDe
   __threadfence();
   Part<A> q;
   q.init();
-  for (int b = threadIdx.x; b < nParts; b += blockDim.x) {
-    for (int i = 0; i < RS_NSUM; i++) q.s[i] += __ldcg(partAll + b * NV + i);
-    for (int i = 0; i < RX_NMAX; i++) q.x[i] = mmax(q.x[i], __ldcg(partAll + b * NV + RS_NSUM + i));
-  }
+  for (int b = threadIdx.x; b < nParts; b += blockDim.x) addPart(q, partAll, b, partStride);
   blockReduce(q, red);
   if (threadIdx.x == 0) {
     InstCtl cc = c;
     decide(I, cc, q, 0);
     ctl[0] = cc;
     *counter = 0;
-  }
-}
-template <int P>
-__global__ void __launch_bounds__(256) k_plainDecide(const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl, const typename Dev<P>::A *part, int nParts) {
-  using A = typename Dev<P>::A;
-  __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
-  if (ctl[0].status != WS_RUNNING) return;
-  constexpr int NV = RS_NSUM + RX_NMAX;
-  Part<A> pt;
-  pt.init();
-  for (int b = threadIdx.x; b < nParts; b += blockDim.x) {
-    for (int i = 0; i < RS_NSUM; i++) pt.s[i] += part[b * NV + i];
-    for (int i = 0; i < RX_NMAX; i++) pt.x[i] = mmax(pt.x[i], part[b * NV + RS_NSUM + i]);
-  }
-  blockReduce(pt, red);
-  if (threadIdx.x == 0) {
-    InstCtl c = ctl[0];
-    decide(insts[0], c, pt, 0);
-    ctl[0] = c;
   }
 }
 
@@ -189,22 +207,22 @@ __device__ __forceinline__ bool gridSync(unsigned *bar, unsigned nb, int *err) {
   return *reinterpret_cast<volatile int *>(err) == 0;
 }
 
-// One instance over the whole (co-resident) grid, every phase of up to nIter iterations in one launch: three grid
-// barriers per iteration.  Block partials go to part[block]; after the barrier every block reduces all of them in the
-// same order and takes the same kinetic-damping decision, so no further broadcast is needed.
-template <int P>
-__global__ void __launch_bounds__(256, WSB_MINB) k_grid(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+// One instance over the whole (co-resident) grid, every phase of up to nIter iterations in one launch: two grid
+// barriers per iteration with the short-slide order, three with the general one.  Block partials go to part[block];
+// after the barrier every block reduces all of them in the same order and takes the same kinetic-damping decision, so
+// no further broadcast is needed.
+template <int P, bool SHORT>
+__global__ void __launch_bounds__(256, WSB_MINB_G) k_grid(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                               typename Dev<P>::A *part, unsigned *bar, int *err, int nIter) {
   using A = typename Dev<P>::A;
   __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
   __shared__ InstCtl sc;
   __shared__ InstDesc si;
-  constexpr int NV = RS_NSUM + RX_NMAX;
   if (threadIdx.x == 0) { sc = ctl[0]; si = insts[0]; }
   __syncthreads();
   const InstDesc &I = si;
   const bool cx = I.contacts && I.K;
-  const int nA = I.m + I.p + I.C + (cx ? I.K : 0);
+  const int nA = countA<SHORT>(I);
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
   const unsigned nb = gridDim.x;
   for (int it = 0; it < nIter; it++) {
@@ -212,32 +230,19 @@ __global__ void __launch_bounds__(256, WSB_MINB) k_grid(Dev<P> d, const InstDesc
     const StepCtx sx = makeCtx<A>(I, sc);
     Part<A> pt;
     pt.init();
-    for (int e = gt; e < nA; e += gs) phaseA<P>(d, I, sx.cur, sx.iter, e, cx ? I.K : 0, pt);
+    for (int e = gt; e < nA; e += gs) phaseA<P, SHORT>(d, I, sx, e, cx ? I.K : 0, pt);
     if (!gridSync(bar, nb, err)) break;
-    if (cx) {
-      const int n2 = 2 * I.K;
-      for (int e = gt; e < n2 + I.m; e += gs) {
-        if (e < n2) rankSide<P>(d, 2 * I.k0 + e, sx.obuf, sx.onxt);
-        else segCount<P>(d, I.m0 + (e - n2), sx.obuf, sx.onxt);
-      }
+    if (!SHORT && cx) {
+      for (int e = gt; e < 2 * I.K + I.m; e += gs) phaseBC<P>(d, I, sx, e);
       if (!gridSync(bar, nb, err)) break;
     }
-    for (int e = gt; e < I.n + I.m; e += gs) {
-      if (e < I.n) nodeUpdate<P>(d, I, sx, I.n0 + e, pt);
-      else segUpdate<P>(d, I, sx, I.m0 + (e - I.n), pt);
-    }
+    for (int e = gt; e < I.n + I.m; e += gs) phaseD<P, SHORT>(d, I, sx, e, pt);
     blockReduce(pt, red);
-    if (threadIdx.x == 0) {
-      for (int i = 0; i < RS_NSUM; i++) part[blockIdx.x * NV + i] = pt.s[i];
-      for (int i = 0; i < RX_NMAX; i++) part[blockIdx.x * NV + RS_NSUM + i] = pt.x[i];
-    }
+    if (threadIdx.x == 0) putPart(pt, part, blockIdx.x, int(nb));
     if (!gridSync(bar, nb, err)) break;
     Part<A> q;
     q.init();
-    for (int b = threadIdx.x; b < int(nb); b += blockDim.x) {
-      for (int i = 0; i < RS_NSUM; i++) q.s[i] += part[b * NV + i];
-      for (int i = 0; i < RX_NMAX; i++) q.x[i] = mmax(q.x[i], part[b * NV + RS_NSUM + i]);
-    }
+    for (int b = threadIdx.x; b < int(nb); b += blockDim.x) addPart(q, part, b, int(nb));
     blockReduce(q, red);
     if (threadIdx.x == 0) decide(I, sc, q, nIter);
     __syncthreads();
@@ -248,23 +253,46 @@ __global__ void __launch_bounds__(256, WSB_MINB) k_grid(Dev<P> d, const InstDesc
 // ------------------------------------------------------------------------------------------------ launchers
 template <int P>
 cudaError_t launchBatched(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
-                          const uint8_t *mask, int threads, int blocks, cudaStream_t st) {
-  k_batched<P><<<blocks, threads, 0, st>>>(d, insts, ctl, order, nInst, nIter, mask);
+                          const uint8_t *mask, int threads, int blocks, bool shortSides, cudaStream_t st) {
+  if (shortSides) k_batched<P, true><<<blocks, threads, 0, st>>>(d, insts, ctl, order, nInst, nIter, mask);
+  else k_batched<P, false><<<blocks, threads, 0, st>>>(d, insts, ctl, order, nInst, nIter, mask);
   return cudaGetLastError();
+}
+
+// a launch of the plain form with programmatic stream serialisation (the kernel may start while its predecessor ends)
+template <class... KArgs, class... Args>
+static cudaError_t launchPDL(void (*k)(KArgs...), int blocks, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
 }
 
 template <int P>
 cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, const PlainShape &sh, bool contacts,
-                            cudaStream_t st, int *launches, unsigned *counter) {
+                            bool shortSides, cudaStream_t st, int *launches, unsigned *counter) {
   using A = typename Dev<P>::A;
-  A *pa = static_cast<A *>(part), *pd = pa + size_t(sh.blocksA) * (RS_NSUM + RX_NMAX);
-  k_plainA<P><<<sh.blocksA, 256, 0, st>>>(d, insts, ctl, pa);
+  const bool sh2 = shortSides && contacts;
+  const int nA = sh2 ? sh.blocksAS : sh.blocksA, nParts = nA + sh.blocksD;
+  A *pa = static_cast<A *>(part), *pd = pa + nA;      // value-major rows of nParts: A's blocks, then D's
+  cudaError_t e = sh2 ? launchPDL(k_plainA<P, true>, sh.blocksAS, st, d, insts, ctl, pa, nParts)
+                      : launchPDL(k_plainA<P, false>, sh.blocksA, st, d, insts, ctl, pa, nParts);
+  if (e != cudaSuccess) return e;
   int nl = 1;
-  if (contacts) {
-    k_plainBC<P><<<sh.blocksR, 256, 0, st>>>(d, insts, ctl);
+  if (contacts && !sh2) {
+    if ((e = launchPDL(k_plainBC<P>, sh.blocksR, st, d, insts, ctl)) != cudaSuccess) return e;
     nl += 1;
   }
-  k_plainD<P><<<sh.blocksD, 256, 0, st>>>(d, insts, ctl, pd, pa, sh.blocksA + sh.blocksD, counter);
+  e = sh2 ? launchPDL(k_plainD<P, true>, sh.blocksD, st, d, insts, ctl, pd, pa, nParts, nParts, counter)
+          : launchPDL(k_plainD<P, false>, sh.blocksD, st, d, insts, ctl, pd, pa, nParts, nParts, counter);
+  if (e != cudaSuccess) return e;
   nl += 1;
   if (launches) *launches += nl;
   return cudaGetLastError();
@@ -272,28 +300,32 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
 
 template <int P>
 cudaError_t launchGrid(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, unsigned *bar, int *err, int nIter,
-                       int blocks, cudaStream_t st) {
+                       int blocks, bool shortSides, cudaStream_t st) {
   using A = typename Dev<P>::A;
   A *pa = static_cast<A *>(part);
   void *args[] = {(void *)&d, (void *)&insts, (void *)&ctl, (void *)&pa, (void *)&bar, (void *)&err, (void *)&nIter};
-  return cudaLaunchCooperativeKernel((const void *)k_grid<P>, dim3(blocks), dim3(256), args, 0, st);
+  const void *k = shortSides ? (const void *)k_grid<P, true> : (const void *)k_grid<P, false>;
+  return cudaLaunchCooperativeKernel(k, dim3(blocks), dim3(256), args, 0, st);
 }
+// co-resident blocks of the grid form: SMs × resident blocks per SM of the kernel variant that runs
 template <int P>
-int gridBlocks() {
+int gridBlocks(bool shortSides) {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_grid<P>, 256, 0);
+  if (shortSides) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_grid<P, true>, 256, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_grid<P, false>, 256, 0);
   return sms * (per > 0 ? per : 1);
 }
 
 #define WSB_INST(P)                                                                                                  \
   template cudaError_t launchBatched<P>(const Dev<P> &, const InstDesc *, InstCtl *, const int *, int, int, const uint8_t *, \
-                                        int, int, cudaStream_t);                                                     \
+                                        int, int, bool, cudaStream_t);                                               \
   template cudaError_t launchPlainIter<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, const PlainShape &, bool,    \
-                                          cudaStream_t, int *, unsigned *);                                                        \
-  template cudaError_t launchGrid<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, unsigned *, int *, int, int, cudaStream_t); \
-  template int gridBlocks<P>();
+                                          bool, cudaStream_t, int *, unsigned *);                                    \
+  template cudaError_t launchGrid<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, unsigned *, int *, int, int, bool, \
+                                     cudaStream_t);                                                                  \
+  template int gridBlocks<P>(bool);
 WSB_INST(PREC_F64)
 WSB_INST(PREC_MIXED)
 WSB_INST(PREC_F32)

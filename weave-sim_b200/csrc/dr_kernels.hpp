@@ -6,19 +6,21 @@
 
 namespace wsb {
 
-struct PlainShape { int blocksA, blocksS, blocksR, blocksD; };
+// blocks of the plain form's kernels: element phase (general order; with the side ranks of the short-slide order),
+// general side order, update phase
+struct PlainShape { int blocksA, blocksAS, blocksR, blocksD; };
 
 template <int P>
 cudaError_t launchBatched(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
-                          const uint8_t *mask, int threads, int blocks, cudaStream_t st);
+                          const uint8_t *mask, int threads, int blocks, bool shortSides, cudaStream_t st);
 template <int P>
 cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, const PlainShape &sh, bool contacts,
-                            cudaStream_t st, int *launches, unsigned *counter);
+                            bool shortSides, cudaStream_t st, int *launches, unsigned *counter);
 
 template <int P>
 cudaError_t launchGrid(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, unsigned *bar, int *err, int nIter,
-                       int blocks, cudaStream_t st);
+                       int blocks, bool shortSides, cudaStream_t st);
 template <int P>
-int gridBlocks();
+int gridBlocks(bool shortSides);
 
 }  // namespace wsb

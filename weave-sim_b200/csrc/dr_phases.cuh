@@ -289,14 +289,15 @@ __device__ __forceinline__ R support(const R Rf[9], const R n[3], R sign, R w, R
 // crossing c: one evaluation of PolylineContact.apply (solver_cpu.js:381-478) without the seat law, the augmented
 // Lagrangian and the rotational friction
 template <int P>
-__device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int buf, int iter, int c, Part<typename Dev<P>::A> &pt) {
+__device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int buf, int iter, int kb, int c, Part<typename Dev<P>::A> &pt) {
   using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A; using U = typename Dev<P>::U;
-  const int kt_ = d.ktot;
+  const int kt_ = d.ktot, K2 = 2 * kt_;
+  const int pos[2] = {d.sPos[2 * c], d.sPos[2 * c + 1]};
   const double rampN = I.ramp_iter;
   const double rampd = rampN <= 0 ? 1.0 : fmin(1.0, 0.01 + 0.99 * double(iter) / rampN);
   const R kn = R(rampd * I.strength), kt = R(rampd * I.stick);
   R Pl[2][3], tg[2][3], Rf[2][9], L[2], tp[2];
-  int seg[2], base[2], nseg[2];
+  int base[2], nseg[2];
   U uu[2];
   for (int side = 0; side < 2; side++) {
     const int o = side * kt_ + c;
@@ -335,7 +336,7 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
     R x[3];
     cross3(y, tg[side], x);
     for (int k = 0; k < 3; k++) { Rf[side][k] = x[k]; Rf[side][3 + k] = y[k]; Rf[side][6 + k] = tg[side][k]; }
-    L[side] = Ls; tp[side] = t; seg[side] = sg; base[side] = a;
+    L[side] = Ls; tp[side] = t; base[side] = a;
   }
   const R *tA = tg[0], *tB = tg[1];
   // contact normal with side persistence (solver_cpu.js:396-402)
@@ -379,10 +380,10 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   if (moved) { uu[0] += U(da) / U(mmax(L[0], R(1e-12))); uu[1] -= U(db) / U(mmax(L[1], R(1e-12))); }
   d.u[c] = mclamp(uu[0], U(0), U(nseg[0]));
   d.u[kt_ + c] = mclamp(uu[1], U(0), U(nseg[1]));
-  // the sides' segments after the slide: the keys of the re-sort (solver_cpu.js:144-149)
+  // the sides' segments after the slide (solver_cpu.js:144-149): the keys of the next sort, into key buffer kb
   for (int side = 0; side < 2; side++) {
     const U un = d.u[side * kt_ + c];
-    d.sKey[2 * c + side] = int(mmin(mmax(mfloor(un), U(0)), U(mmax(nseg[side] - 1, 0))));
+    d.sKey[size_t(kb) * K2 + pos[side]] = int(mmin(mmax(mfloor(un), U(0)), U(mmax(nseg[side] - 1, 0))));
   }
   if (slip) {
     const R sx = da * tA[0] + db * tB[0], sy = da * tA[1] + db * tB[1], sz = da * tA[2] + db * tB[2];
@@ -398,61 +399,87 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   d.Ft[c] = msqrt(dot3(fT, fT));
   d.cstate[c] = slip ? 1 : 0;
   d.gap[c] = g;
-  // side records for the gathers: segment and t before the slide, force on the side, lever torque tf (r × F)
+  // side records for the gathers: t before the slide, force on the side, lever torque tf (r × F); the righting
+  // stiffness of the support point (addTwistStiffness, solver_cpu.js:170-176) goes to the segments the sides sit on
+  // after the slide
   const R tf = R(I.tf);
-  const int K2 = 2 * kt_;
+  const R tfc = R(fmax(I.tf, 1e-3)), hc = d.ch[c], wc = d.cw[c];
+  const R kth = tfc * ((Fn + kn * R(0.25) * hc) * (R(0.5) * wc) / R(SUPPORT_SMOOTH) + kt * (R(0.5) * hc) * (R(0.5) * hc));
   for (int side = 0; side < 2; side++) {
-    const int sd = 2 * c + side;
+    const int q = pos[side];
     const R sgn = side ? R(-1) : R(1);
     const R F[3] = {sgn * FA[0], sgn * FA[1], sgn * FA[2]};
     R tq[3];
     cross3(side ? rB : rA, F, tq);
-    d.sSeg[sd] = seg[side];
-    d.sT[sd] = tp[side];
-    for (int k = 0; k < 3; k++) { d.sF[k * K2 + sd] = F[k]; d.sTq[k * K2 + sd] = tf * tq[k]; }
+    d.sT[q] = tp[side];
+    d.kth[q] = kth;
+    for (int k = 0; k < 3; k++) { d.sF[k * K2 + q] = F[k]; d.sTq[k * K2 + q] = tf * tq[k]; }
   }
-  // righting stiffness of the support point (addTwistStiffness, solver_cpu.js:170-176): goes to the segments the
-  // sides sit on after the slide
-  const R tfc = R(fmax(I.tf, 1e-3)), hc = d.ch[c], wc = d.cw[c];
-  d.kth[c] = tfc * ((Fn + kn * R(0.25) * hc) * (R(0.5) * wc) / R(SUPPORT_SMOOTH) + kt * (R(0.5) * hc) * (R(0.5) * hc));
   pt.s[RS_PEN] += A(active ? kn * pen * pen : R(0));
   pt.s[RS_TAN] += A(dot3(Se, Se));
   pt.x[RX_FN] = mmax(pt.x[RX_FN], A(Fn));
 }
 
 // ------------------------------------------------------------------------------------------------ phase B / C
-// Slot e of the previous sorted order: its side goes to position off + rank in the new order, rank = number of the
-// strand's sides with a smaller (segment, side id).  Every side counts independently (no serial sort, no atomics),
-// and the result is the sorted order by (segment, id) whatever the previous order was.
-template <int P>
-__device__ __forceinline__ void rankSide(const Dev<P> &d, int e, int src, int dst) {
-  const int K2 = 2 * d.ktot;
-  const int *oi = d.ord + size_t(src) * K2;
-  const int sd = oi[e], key = d.sKey[sd], s = d.sStrand[sd];
-  const int off = d.stSideOff[s], cnt = d.stSideCnt[s];
-  int rank = 0;
+// The order of the crossing sides along each strand, sorted by (local segment, side), built by rank: the side at
+// position p counts the sides of its strand that sort before it (no serial sort, no atomics).  Keys are read by
+// position, so a strand's keys are one contiguous run every thread of the strand reads alike.
+struct SideRank { int pos, below, equal; };
+__device__ __forceinline__ SideRank sideRank(const int *key, int p, int off, int cnt) {
+  const int k = key[p];
+  int below = 0, equal = 0, before = 0;
   for (int q = off; q < off + cnt; q++) {
-    const int o = oi[q], ko = d.sKey[o];
-    rank += (ko < key || (ko == key && o < sd)) ? 1 : 0;
+    const int kq = key[q];
+    below += kq < k ? 1 : 0;
+    equal += kq == k ? 1 : 0;
+    before += (kq == k && q < p) ? 1 : 0;
   }
-  d.ord[size_t(dst) * K2 + off + rank] = sd;
-  d.ordSeg[size_t(dst) * K2 + off + rank] = key;
+  return SideRank{off + below + before, below, equal};
+}
+// general order (any slide length): side p takes its place in sorted-side buffer dst by the keys of buffer kb (after
+// this iteration's slide); every segment's slice is then counted by segCount
+template <int P>
+__device__ __forceinline__ void rankSide(const Dev<P> &d, int p, int kb, int dst) {
+  const int K2 = 2 * d.ktot, s = d.sStrand[p];
+  const int *key = d.sKey + size_t(kb) * K2;
+  const SideRank r = sideRank(key, p, d.stSideOff[s], d.stSideCnt[s]);
+  d.ord[size_t(dst) * K2 + r.pos] = p;
+  d.ordSeg[size_t(dst) * K2 + r.pos] = key[p];
 }
 // segment j: its slice of the new order = [off + #keys below, off + #keys below + #keys equal) among its strand's sides
 template <int P>
-__device__ __forceinline__ void segCount(const Dev<P> &d, int j, int src, int dst) {
+__device__ __forceinline__ void segCount(const Dev<P> &d, int j, int kb, int dst) {
   const int K2 = 2 * d.ktot;
-  const int *oi = d.ord + size_t(src) * K2;
+  const int *key = d.sKey + size_t(kb) * K2;
   const int s = d.segStrand[j], lj = d.segLocal[j];
   const int off = d.stSideOff[s], cnt = d.stSideCnt[s];
   int lo = 0, eq = 0;
   for (int q = off; q < off + cnt; q++) {
-    const int ko = d.sKey[oi[q]];
-    lo += ko < lj ? 1 : 0;
-    eq += ko == lj ? 1 : 0;
+    const int kq = key[q];
+    lo += kq < lj ? 1 : 0;
+    eq += kq == lj ? 1 : 0;
   }
   d.rngLo[size_t(dst) * d.mtot + j] = off + lo;
   d.rngHi[size_t(dst) * d.mtot + j] = off + lo + eq;
+}
+// short-slide order (the slide limit is under half the shortest segment, so a side moves at most one segment per
+// iteration): built inside the element phase from the keys of the previous iteration (the segments the sides sit on
+// before this iteration's slide), into the buffer this iteration's gathers read.  The first side of each segment
+// writes that segment's slice; a segment without sides keeps a slice of an earlier iteration, whose entries carry
+// other keys, and the gathers skip entries whose key is not the segment's.
+template <int P>
+__device__ __forceinline__ void rankSideShort(const Dev<P> &d, int p, int buf) {
+  const int K2 = 2 * d.ktot, s = d.sStrand[p], off = d.stSideOff[s];
+  const int *key = d.sKey + size_t(buf) * K2;
+  const SideRank r = sideRank(key, p, off, d.stSideCnt[s]);
+  const int k = key[p];
+  d.ord[size_t(buf) * K2 + r.pos] = p;
+  d.ordSeg[size_t(buf) * K2 + r.pos] = k;
+  if (r.pos == off + r.below) {
+    const int j = d.stSegOff[s] + k;
+    d.rngLo[size_t(buf) * d.mtot + j] = off + r.below;
+    d.rngHi[size_t(buf) * d.mtot + j] = off + r.below + r.equal;
+  }
 }
 
 // ------------------------------------------------------------------------------------------------ phase D
@@ -461,7 +488,19 @@ struct StepCtx {
   double dispR;      // prescribed-motion fraction of this iteration
 };
 
-template <int P>
+// the sides in the slice of segment j (strand-local index lj) of sorted-side buffer ob, in sorted order; with SHORT an
+// entry counts only if it carries the segment's key (a slice left over from an earlier iteration carries other keys)
+template <bool SHORT, int P, class F>
+__device__ __forceinline__ void sidesOn(const Dev<P> &d, int ob, int j, int lj, F &&f) {
+  const int K2 = 2 * d.ktot;
+  const int lo = d.rngLo[size_t(ob) * d.mtot + j], hi = d.rngHi[size_t(ob) * d.mtot + j];
+  for (int e = lo; e < hi; e++) {
+    if (SHORT && d.ordSeg[size_t(ob) * K2 + e] != lj) continue;
+    f(d.ord[size_t(ob) * K2 + e]);
+  }
+}
+
+template <int P, bool SHORT>
 __device__ __forceinline__ void nodeUpdate(const Dev<P> &d, const InstDesc &I, const StepCtx &sc, int i, Part<typename Dev<P>::A> &pt) {
   using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A;
   const int nt = d.ntot, mt = d.mtot, K2 = 2 * d.ktot;
@@ -482,22 +521,16 @@ __device__ __forceinline__ void nodeUpdate(const Dev<P> &d, const InstDesc &I, c
   pt.x[RX_LOAD] = mmax(pt.x[RX_LOAD], A(mmax(mabs(tot[0]), mmax(mabs(tot[1]), mabs(tot[2])))));
   // crossing sides on the adjacent segments, as distributed by the last evaluation (weights 1 − t at a, t at b)
   const bool cx = I.contacts && I.K;
-  if (cx && so >= 0) {
-    const int lo = d.rngLo[size_t(sc.obuf) * mt + so], hi = d.rngHi[size_t(sc.obuf) * mt + so];
-    for (int e = lo; e < hi; e++) {
-      const int sd = d.ord[size_t(sc.obuf) * K2 + e];
-      const R wgt = R(1) - d.sT[sd];
-      for (int k = 0; k < 3; k++) F[k] += wgt * d.sF[k * K2 + sd];
-    }
-  }
-  if (cx && si >= 0) {
-    const int lo = d.rngLo[size_t(sc.obuf) * mt + si], hi = d.rngHi[size_t(sc.obuf) * mt + si];
-    for (int e = lo; e < hi; e++) {
-      const int sd = d.ord[size_t(sc.obuf) * K2 + e];
-      const R wgt = d.sT[sd];
-      for (int k = 0; k < 3; k++) F[k] += wgt * d.sF[k * K2 + sd];
-    }
-  }
+  if (cx && so >= 0)
+    sidesOn<SHORT>(d, sc.obuf, so, SHORT ? d.segLocal[so] : 0, [&](int q) {
+      const R wgt = R(1) - d.sT[q];
+      for (int k = 0; k < 3; k++) F[k] += wgt * d.sF[k * K2 + q];
+    });
+  if (cx && si >= 0)
+    sidesOn<SHORT>(d, sc.obuf, si, SHORT ? d.segLocal[si] : 0, [&](int q) {
+      const R wgt = d.sT[q];
+      for (int k = 0; k < 3; k++) F[k] += wgt * d.sF[k * K2 + q];
+    });
   if (fl & 8) for (int k = 0; k < 3; k++) d.react[k * nt + i] = -F[k];
   for (int k = 0; k < 3; k++) if (!(fl & (1 << k))) F[k] = R(0);
   pt.x[RX_F] = mmax(pt.x[RX_F], A(msqrt(dot3(F, F))));
@@ -517,7 +550,7 @@ __device__ __forceinline__ void nodeUpdate(const Dev<P> &d, const InstDesc &I, c
   pt.s[RS_KE] += A(m) * (A(v[0]) * A(v[0]) + A(v[1]) * A(v[1]) + A(v[2]) * A(v[2]));
 }
 
-template <int P>
+template <int P, bool SHORT>
 __device__ __forceinline__ void segUpdate(const Dev<P> &d, const InstDesc &I, const StepCtx &sc, int j, Part<typename Dev<P>::A> &pt) {
   using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A;
   const int mt = d.mtot, pt_ = d.ptot, ct = d.ctot, K2 = 2 * d.ktot;
@@ -531,13 +564,20 @@ __device__ __forceinline__ void segUpdate(const Dev<P> &d, const InstDesc &I, co
   if (c1 >= 0) for (int k = 0; k < 3; k++) T[k] -= d.tauC[k * ct + c1];
   R kTw = R(0);
   if (I.contacts && I.K) {
-    const int lo = d.rngLo[size_t(sc.obuf) * mt + j], hi = d.rngHi[size_t(sc.obuf) * mt + j];
-    for (int e = lo; e < hi; e++) {
-      const int sd = d.ord[size_t(sc.obuf) * K2 + e];
-      for (int k = 0; k < 3; k++) T[k] += d.sTq[k * K2 + sd];
+    const int lj = SHORT ? d.segLocal[j] : 0;
+    sidesOn<SHORT>(d, sc.obuf, j, lj, [&](int q) { for (int k = 0; k < 3; k++) T[k] += d.sTq[k * K2 + q]; });
+    if constexpr (SHORT) {
+      // the sides on segment j after the slide were, before it, on j − 1, j or j + 1 of the same strand
+      const int s = d.segStrand[j];
+      const int *key = d.sKey + size_t(sc.onxt) * K2;
+      for (int dj = -1; dj <= 1; dj++) {
+        const int jj = j + dj;
+        if (jj < 0 || jj >= mt || d.segStrand[jj] != s) continue;
+        sidesOn<true>(d, sc.obuf, jj, lj + dj, [&](int q) { if (key[q] == lj) kTw += d.kth[q]; });
+      }
+    } else {
+      sidesOn<false>(d, sc.onxt, j, 0, [&](int q) { kTw += d.kth[q]; });
     }
-    const int lo2 = d.rngLo[size_t(sc.onxt) * mt + j], hi2 = d.rngHi[size_t(sc.onxt) * mt + j];
-    for (int e = lo2; e < hi2; e++) kTw += d.kth[d.ord[size_t(sc.onxt) * K2 + e] >> 1];
   }
   R q[4], Rm[9];
   for (int k = 0; k < 4; k++) q[k] = Acc<P>::qr(d, sc.cur, k, j);

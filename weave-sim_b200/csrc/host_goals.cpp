@@ -144,10 +144,24 @@ int HostGoals::sideSegLocal(int sd) const {
   return int(std::min(std::max(std::floor(uu), 0.0), double(std::max(ns - 1, 0))));
 }
 
+double HostGoals::sideSegMin() const {
+  double mn = INFINITY;
+  std::vector<char> seen(S, 0);
+  for (int sd = 0; sd < 2 * K; sd++) {
+    if (seen[cxStrand[sd]]) continue;
+    seen[cxStrand[sd]] = 1;
+    for (int j = cxSegOff[sd]; j < cxSegOff[sd] + cxNseg[sd]; j++) mn = std::min(mn, l0[j]);
+  }
+  return mn;
+}
+
 void HostGoals::sortSides() {
   strandSideOff.assign(S, 0); strandSideCnt.assign(S, 0);
   std::vector<std::vector<int>> per(S);
   for (int sd = 0; sd < 2 * K; sd++) per[cxStrand[sd]].push_back(sd);
+  sideList.clear(); sidePos.assign(2 * K, 0);
+  for (int s = 0; s < S; s++)
+    for (int sd : per[s]) { sidePos[sd] = int(sideList.size()); sideList.push_back(sd); }
   ord.clear(); ordSeg.clear();
   for (int s = 0; s < S; s++) {
     std::vector<int> &L = per[s];

@@ -44,6 +44,7 @@ struct HostGoals {
   std::vector<int> segClamp0, segClamp1;             // [m] clamps acting on the segment (-1 none)
   std::vector<int> segStrand, segLocal;              // [m]
   std::vector<int> strandSideOff, strandSideCnt;     // [S] slice of the sorted side list
+  std::vector<int> sideList, sidePos;                // [2K] side at each position (strand-grouped, ascending id); position of each side
   std::vector<int> ord, ordSeg;                      // [2K] side ids (2c + side) sorted by (local segment, id) per strand
   std::vector<int> rngLo, rngHi;                     // [m] slice of ord on the segment
 
@@ -51,6 +52,7 @@ struct HostGoals {
   void rebuild(const ws_model &md);                  // warm start: new stiffness / loads / parameters, state kept
   void sortSides();                                  // ord / ordSeg / rngLo / rngHi from u
   int sideSegLocal(int sd) const;                    // local segment of side sd from u (solver_cpu.js:144-149)
+  double sideSegMin() const;                         // shortest rest length among the segments of strands with sides
 
  private:
   void loadModel(const ws_model &md, bool keepState);

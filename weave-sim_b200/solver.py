@@ -59,7 +59,7 @@ def relax_noalloc(model, n_iter, precision="mixed", threads=256, stream=None):
 
 
 class GpuSolver:
-    def __init__(self, models, precision="mixed", form="cta", threads=0, device=0, budget_bytes=0):
+    def __init__(self, models, precision="mixed", form="cta", threads=0, device=0, budget_bytes=0, side_order="auto"):
         if not isinstance(models, (list, tuple)):
             models = [models]
         self.models = list(models)
@@ -70,6 +70,7 @@ class GpuSolver:
         opts.precision = _lib.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
         opts.form = _lib.FORMS[form] if isinstance(form, str) else int(form)
         opts.threads, opts.device, opts.budget_bytes = int(threads), int(device), int(budget_bytes)
+        opts.side_order = {"auto": 0, "general": 1}[side_order]
         self.precision, self.form = precision, form
         h = C.c_void_p()
         check(lib().ws_create(arr, self.B, C.byref(opts), C.byref(h)), "ws_create")
@@ -148,6 +149,12 @@ class GpuSolver:
     @property
     def stream(self):
         return lib().ws_stream(self.h)
+
+    @property
+    def side_order(self):
+        """'short' when the crossing sides are ranked inside the element kernel (slides under one segment per
+        iteration), 'general' otherwise"""
+        return "short" if lib().ws_side_order(self.h) == 1 else "general"
 
     @property
     def device_bytes(self):
