@@ -6,6 +6,7 @@ FP32 element math with two-float positions/frames and FP64 reductions.  A step i
 DR iterations per second of the whole job (all ranks).  Between timed steps a 256 MiB buffer is written to flush L2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--chunk C] [--impl ours|reference]
+    python bench.py --workload precision|batch|serve      (one JSON line each; weave-sim_b200/workloads.py)
 
 --impl reference runs the reference's CPU algorithm (the f64 restatement under oracle/, the reference's JS being
 unrunnable without a JS engine) on the host cores: one replica of the workload per thread, a bounded sample of
@@ -225,6 +226,25 @@ def run_reference(args, rank, world):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_workload(args):
+    import weavesim_b200 as ws
+    from weavesim_b200 import workloads
+    t0 = time.perf_counter()
+    with ClockSampler(0) as clk:
+        if args.workload == "precision":
+            r = workloads.run_precision(instances=args.instances or 64)
+            metric = "position / slide / stick-slip agreement with FP64 after the 5000-iteration cap, and throughput"
+        elif args.workload == "batch":
+            r = workloads.run_batch(count=args.instances or 512)
+            metric = "solves/s and DR iters/s of 512 mixed gridshells to the 5000-iteration cap"
+        else:
+            r = workloads.run_serve()
+            metric = "p50/p99/p99.9 solve latency and solves/s under Poisson arrivals"
+    print(json.dumps({"workload": args.workload, "metric": metric, "result": r, "clocks": clk.summary(),
+                      "wall_s": time.perf_counter() - t0, "data": "synthetic (seeded)", "gpu": ws.device_count() > 0}),
+          flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -236,7 +256,14 @@ def main():
     ap.add_argument("--form", default="plain", choices=["plain", "grid", "cta"])
     ap.add_argument("--ref-iters", type=int, default=10, help="DR iterations per replica per step of the CPU arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="shell_large", choices=["shell_large", "precision", "batch", "serve"],
+                    help="shell_large: the headline line; the others measure the stiff-dome precision variants, the "
+                         "512-gridshell mixed batch and the serving loop (single GPU)")
+    ap.add_argument("--instances", type=int, default=0, help="instances of the precision / batch workloads")
     args = ap.parse_args()
+    if args.workload != "shell_large":
+        run_workload(args)
+        return
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "reference":
         out = run_reference(args, rank, world)

@@ -1,0 +1,126 @@
+"""Measured workloads besides the headline single-gridshell benchmark (bench.py --workload ...).
+
+* ``precision`` — stiff 3 m domes (25×3 mm laths, E 12 GPa, per-crossing μ ~ U(0.1, 0.5)), one instance per seed,
+  relaxed for the reference's default iteration cap (5000, params.js:20-23) in FP64, in the mixed policy (FP32 element
+  math, two-float state, FP64 reductions) and in naive FP32.  Reported against FP64: max node position error / span,
+  slide-coordinate error, stick/slip mismatches; and the chaos floor: FP64 against FP64 started 1 nm away.
+* ``batch`` — 512 independent gridshells drawn from a seed (laths per family U{6..40}, span U(2, 12) m, thickness
+  U(3, 6) mm, width U(30, 60) mm, E U(8, 14) GPa, μ U(0.1, 0.5), inward displacement U(3, 10) % of the span, ~5 cm
+  segments), one thread block each, relaxed together to the iteration cap.
+* ``serve`` — the serving loop under Poisson arrivals at the given rates: fresh stiff domes (new seed each) and, with
+  probability 0.3, variants (±5 % E, ±0.1 μ, ±2 % support displacement) of a resident equilibrium, warm-started.
+
+Every solve here stops at convergence (relative residual ≤ tol) or at its iteration cap, as CpuSolver.run does.
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+from . import configs, serve
+from ._lib import default_params
+from .solver import GpuSolver
+
+CAP = 5000          # the reference's default max_iter (web/js/params.js:20-23)
+
+
+def _stiff(seed, cap=CAP):
+    return configs.dome_stiff(seed=seed, params=default_params(disp_ramp_iter=3000, max_iter=cap, strength=1e5,
+                                                               stick_strength=1e5))
+
+
+def _relax(models, precision, iters, threads=512):
+    """relax a batch in the batched form; returns (per-instance states, control, GPU ms, launches)"""
+    s = GpuSolver([m.copy() for m in models], precision=precision, threads=threads)
+    ctl = s.step(iters)
+    ms, nl = s.last_step_stats()
+    st = [s.download(b, fields=("X", "u", "state", "stuck")) for b in range(len(models))]
+    s.dispose()
+    return st, ctl, ms, nl
+
+
+def _compare(a, b, models):
+    pos = [float(np.max(np.linalg.norm((x["X"] - y["X"]).reshape(-1, 3), axis=1)) / m.span) for x, y, m in zip(a, b, models)]
+    du = [float(np.max(np.abs(x["u"] - y["u"]))) if m.K else 0.0 for x, y, m in zip(a, b, models)]
+    state = [int(np.sum(x["state"] != y["state"])) for x, y in zip(a, b)]
+    stuck = [int(np.sum(x["stuck"] != y["stuck"])) for x, y in zip(a, b)]
+    return {"pos_err_span_median": float(np.median(pos)), "pos_err_span_max": float(np.max(pos)),
+            "within_1e-4_span": int(np.sum(np.array(pos) <= 1e-4)), "slide_err_max_segments": float(np.max(du)),
+            "slip_state_mismatch_total": int(np.sum(state)), "stick_mismatch_total": int(np.sum(stuck))}
+
+
+def run_precision(instances=64, iters=CAP, seed0=1):
+    models = [_stiff(seed0 + b) for b in range(instances)]
+    _relax(models[:2], "mixed", 20)                       # module load and first-launch costs out of the timings
+    out = {"instances": instances, "iterations": iters, "nodes": models[0].n, "crossings": models[0].K}
+    ref, ctl64, ms64, _ = _relax(models, "f64", iters)
+    rng = np.random.default_rng(7)
+    pert = []
+    for m in models:
+        p = m.copy()
+        p.X = p.X + 1e-9 * rng.standard_normal(p.X.shape)
+        pert.append(p)
+    floor, _, _, _ = _relax(pert, "f64", iters)
+    out["f64"] = {"gpu_ms": ms64, "inst_iters_per_s": sum(c["iter"] for c in ctl64) / (ms64 * 1e-3),
+                  "converged": sum(c["status"] == 1 for c in ctl64)}
+    out["chaos_floor_f64_1nm"] = _compare(floor, ref, models)
+    for prec in ("mixed", "f32"):
+        st, ctl, ms, _ = _relax(models, prec, iters)
+        out[prec] = dict(_compare(st, ref, models), gpu_ms=ms, converged=sum(c["status"] == 1 for c in ctl),
+                         nonfinite=sum(c["status"] == 3 for c in ctl),
+                         inst_iters_per_s=sum(c["iter"] for c in ctl) / (ms * 1e-3))
+    return out
+
+
+def run_batch(count=512, iters=CAP, precision="mixed", threads=512, seed=4):
+    models = configs.batch_mixed(count, seed=seed)
+    for m in models:
+        m.params = dict(m.params, max_iter=iters)
+    t0 = time.perf_counter()
+    s = GpuSolver(models, precision=precision, threads=threads)
+    create_s = time.perf_counter() - t0
+    ctl = s.step(iters)
+    ms, nl = s.last_step_stats()
+    dev_bytes = s.device_bytes
+    s.dispose()
+    its = sum(c["iter"] for c in ctl)
+    node_its = sum(c["iter"] * m.n for c, m in zip(ctl, models))
+    n = np.array([m.n for m in models])
+    return {"instances": count, "iteration_cap": iters, "gpu_ms": ms, "solves_per_s": count / (ms * 1e-3),
+            "inst_iters_per_s": its / (ms * 1e-3), "node_iters_per_s": node_its / (ms * 1e-3),
+            "converged": sum(c["status"] == 1 for c in ctl), "nonfinite": sum(c["status"] == 3 for c in ctl),
+            "nodes_min": int(n.min()), "nodes_median": int(np.median(n)), "nodes_max": int(n.max()),
+            "nodes_total": int(n.sum()), "crossings_total": int(sum(m.K for m in models)), "device_bytes": dev_bytes,
+            "create_s": create_s, "launches": nl}
+
+
+def run_serve(rates=(50.0, 200.0, 1000.0), counts=(300, 600, 1000), slots=296, chunk=250, budget_bytes=150 * 10 ** 9,
+              time_limit=120.0):
+    tpl = _stiff(1)
+    out = {"slots": slots, "chunk_iters": chunk, "fresh_cap": CAP, "variant_cap": 1500, "rates": []}
+    srv = serve.Server(tpl, slots=slots, chunk=chunk, budget_bytes=budget_bytes)
+    out["slots"] = srv.slots
+    # a warm bank of resident equilibria for the variants
+    seed_reqs = serve.poisson_stream(1e6, 8, seed=1, variant_share=0.0, fresh_cap=CAP)
+    srv.run(seed_reqs, time_limit=time_limit)
+    bank = list(srv.resident.values())
+    for rate, count in zip(rates, counts):
+        srv.done, srv.ticks, srv.busy_slot_ticks = [], 0, 0
+        reqs = serve.poisson_stream(rate, count, seed=int(rate), variant_share=0.3, fresh_cap=CAP, variant_cap=1500,
+                                    warm_bank=bank)
+        t0 = time.perf_counter()
+        done = srv.run(reqs, time_limit=time_limit)
+        wall = time.perf_counter() - t0
+        lat = serve.latency_summary(done)
+        fresh = [r for r in done if r.kind == "fresh"]
+        var = [r for r in done if r.kind == "variant"]
+        out["rates"].append(dict(rate_per_s=rate, requests=count, finished=len(done), wall_s=wall,
+                                 solves_per_s=len(done) / wall, fresh=len(fresh), variants=len(var),
+                                 converged=sum(r.status == 1 for r in done),
+                                 mean_busy_slots=srv.busy_slot_ticks / max(srv.ticks, 1),
+                                 p50_s=lat["p50_s"], p99_s=lat["p99_s"], p999_s=lat["p999_s"], mean_s=lat["mean_s"],
+                                 fresh_p50_s=serve.latency_summary(fresh)["p50_s"] if fresh else None,
+                                 variant_p50_s=serve.latency_summary(var)["p50_s"] if var else None))
+    srv.dispose()
+    return out
