@@ -6,7 +6,7 @@ FP32 element math with two-float positions/frames and FP64 reductions.  A step i
 DR iterations per second of the whole job (all ranks).  Between timed steps a 256 MiB buffer is written to flush L2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--chunk C] [--impl ours|reference]
-    python bench.py --workload precision|batch|serve      (one JSON line each; weave-sim_b200/workloads.py)
+    python bench.py --workload precision|batch|serve|ratio   (one JSON line each; weave-sim_b200/workloads.py)
 
 --impl reference runs the reference's CPU algorithm (the f64 restatement under oracle/, the reference's JS being
 unrunnable without a JS engine) on the host cores: one replica of the workload per thread, a bounded sample of
@@ -206,6 +206,30 @@ def cpu_replicas(iters_per_replica, threads):
     return threads * iters_per_replica / dt, dt
 
 
+def cpu_dome(iters, threads=0):
+    """CPU baseline leg of the ratio workload: the reference's CPU algorithm (oracle/, f64) on the 3 m dome, one thread
+    alone and one replica per host thread; returns (1-thread iters/s, all-thread instance iters/s, threads)"""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import weavesim_b200 as ws
+    from oracle import Oracle
+    threads = threads or os.cpu_count() or 1
+    one = Oracle(ws.configs.dome_small(seed=1))
+    one.step(1)
+    t0 = time.perf_counter()
+    one.step(iters)
+    cpu1 = iters / (time.perf_counter() - t0)
+    ors = [Oracle(ws.configs.dome_small(seed=1 + b)) for b in range(threads)]
+    for o in ors:
+        o.step(1)
+    t0 = time.perf_counter()
+    th = [threading.Thread(target=o.step, args=(iters,)) for o in ors]    # ctypes releases the GIL
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    return cpu1, threads * iters / (time.perf_counter() - t0), threads
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
@@ -237,6 +261,13 @@ def run_workload(args):
         elif args.workload == "batch":
             r = workloads.run_batch(count=args.instances or 512)
             metric = "solves/s and DR iters/s of 512 mixed gridshells to the 5000-iteration cap"
+        elif args.workload == "ratio":
+            r = workloads.run_ratio()
+            cpu1, cpuN, threads = cpu_dome(r["iterations"])
+            r.update(cpu_port_1_thread_iters_per_s=cpu1, cpu_port_threads=threads,
+                     cpu_port_all_threads_inst_iters_per_s=cpuN, batched_over_cpu_all_threads=r["batched_inst_iters_per_s"] / cpuN,
+                     batched_over_cpu_1_thread=r["batched_inst_iters_per_s"] / cpu1)
+            metric = "batched vs plain single-instance GPU form vs the CPU port, DR iters/s on the 3 m dome"
         else:
             r = workloads.run_serve()
             metric = "p50/p99/p99.9 solve latency and solves/s under Poisson arrivals"
@@ -256,7 +287,7 @@ def main():
     ap.add_argument("--form", default="plain", choices=["plain", "grid", "cta"])
     ap.add_argument("--ref-iters", type=int, default=10, help="DR iterations per replica per step of the CPU arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="shell_large", choices=["shell_large", "precision", "batch", "serve"],
+    ap.add_argument("--workload", default="shell_large", choices=["shell_large", "precision", "batch", "serve", "ratio"],
                     help="shell_large: the headline line; the others measure the stiff-dome precision variants, the "
                          "512-gridshell mixed batch and the serving loop (single GPU)")
     ap.add_argument("--instances", type=int, default=0, help="instances of the precision / batch workloads")

@@ -195,12 +195,15 @@ typedef struct ws_opts {
   int32_t threads;      /* threads per block (0: autotuned) */
   int32_t device;       /* CUDA device ordinal */
   uint64_t budget_bytes;/* device memory this context may take (0: no limit) */
-  int32_t history;      /* reserved */
+  int32_t cta_state;    /* batched form: WS_CTA_AUTO keeps each instance's changing state in shared memory when every
+                           instance of the batch fits a thread block's shared memory, else in global memory;
+                           WS_CTA_GLOBAL always in global memory */
   int32_t side_order;   /* WS_SIDES_AUTO: the short-slide side order when the slide limit (contact epsilon) is under half
                            the shortest segment of the strands with crossings, else the general order;
                            WS_SIDES_GENERAL: always the general order */
 } ws_opts;
 enum { WS_SIDES_AUTO = 0, WS_SIDES_GENERAL = 1 };
+enum { WS_CTA_AUTO = 0, WS_CTA_GLOBAL = 1 };
 
 /* Builds the goals of every instance on the host (masses, inertias, clamps: CpuSolver._buildGoals,
  * solver_cpu.js:670-710; contact initialisation: PolylineContact.initialize, solver_cpu.js:99-139) and uploads the
@@ -270,6 +273,9 @@ void *ws_stream(ws_ctx *ctx);
  * at most one segment per iteration), 0 the general order (a separate ranking kernel).  No counterpart in the
  * reference, whose GPU form re-sorts nothing (it accumulates with atomics). */
 int ws_side_order(const ws_ctx *ctx);
+/* 1 when the batched form holds its instances in shared memory (the resident form), else 0.  No counterpart in the
+ * reference. */
+int ws_cta_resident(const ws_ctx *ctx);
 /* device bytes held by the context */
 uint64_t ws_device_bytes(const ws_ctx *ctx);
 /* GPU time of the last ws_step (ms, CUDA events on the context's stream) and the number of kernel launches it made */

@@ -43,7 +43,7 @@ def timoshenko(direction=2, P=10.0, L=1000.0, w=60.0, h=30.0):
     return P * L ** 3 / (3 * E_MM * I) + P * L / (KAPPA * G_MM * w * h)
 
 
-def crossing(load=-50.0, pull=0.0, mu=0.35, freeB=True, nseg=10, L=1000.0, h=30.0, locked=False, **prm):
+def crossing(load=-50.0, pull=0.0, mu=0.35, freeB=True, nseg=10, L=1000.0, h=30.0, locked=False, local=False, **prm):
     P = np.array([[-L / 2 + L * i / nseg, 0.0, 0.0] for i in range(nseg + 1)])
     PB = np.array([[0.0, -L / 2 + L * i / nseg, h] for i in range(nseg + 1)])
     mid = nseg // 2
@@ -52,7 +52,7 @@ def crossing(load=-50.0, pull=0.0, mu=0.35, freeB=True, nseg=10, L=1000.0, h=30.
     prm.setdefault("max_iter", 20000)
     md = ws.polylines([P, PB], knot_rows=[[0, mid, nseg], [0, mid, nseg]], knots=[((0, 1), (1, 1))],
                       anchors=[((0, 0), fixA), ((0, 2), fixA), ((1, 0), fixB), ((1, 2), fixB)],
-                      loads=[((1, 1), (pull, 0.0, load), False)], mu=mu, E=E_MM, G=G_MM, params=mm_params(**prm))
+                      loads=[((1, 1), (pull, 0.0, load), local)], mu=mu, E=E_MM, G=G_MM, params=mm_params(**prm))
     if locked:
         md.cross_locked[:] = 1
     return md

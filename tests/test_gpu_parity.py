@@ -234,3 +234,59 @@ def test_large_shell_general_order_against_oracle(oracle_mod):
     s.dispose()
     assert ctl["iter"] == 330
     assert cases.max_node_err_span(g["X"], v["X"], md.span) < 1e-9
+
+
+# ------------------------------------------------------------------------------------------------ resident form
+# The batched form keeps an instance's changing state in shared memory when the batch fits a thread block.  With the
+# same block size it runs the same arithmetic in the same order as the form with global state, so the two agree bit
+# for bit, across launch boundaries (state written back and reloaded) and kinetic-damping roll-backs.
+
+def _two_launches(md, prec, threads, **kw):
+    s = ws.GpuSolver([md.copy()], precision=prec, threads=threads, **kw)
+    res = s.resident
+    s.step(400)
+    ctl = s.step(300)[0]
+    g = s.download(0)
+    s.dispose()
+    return res, ctl, g
+
+
+@pytest.mark.parametrize("prec,name,side_order", [("mixed", "dome", "auto"), ("mixed", "dome", "general"),
+                                                  ("f64", "cross_stick", "auto"), ("f64", "cross_stick", "general"),
+                                                  ("f32", "dome", "auto"), ("mixed", "cantilever", "auto")])
+def test_resident_equals_global_state(prec, name, side_order):
+    md = ws.configs.dome_small() if name == "dome" else cases.case_by_name(name)
+    r1, c1, a = _two_launches(md, prec, 256, side_order=side_order)
+    r2, c2, b = _two_launches(md, prec, 256, side_order=side_order, cta_state="global")
+    assert r1 and not r2
+    assert c1["iter"] == c2["iter"] and c1["rollbacks"] == c2["rollbacks"] and c1["residual"] == c2["residual"]
+    for k in ("X", "Q", "V", "W", "u", "nprev", "slip", "Fn", "Ft", "gap", "stuck", "state", "N", "M", "reactions"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_resident_f64_matches_oracle_with_roll_backs(oracle_mod):
+    md = cases.case_by_name("cross_press")
+    v = oracle_mod.Oracle(md.copy()).run(3000)
+    s = ws.GpuSolver([md.copy()], precision="f64")
+    assert s.resident
+    ctl = s.step(3000)[0]
+    g = s.download(0)
+    s.dispose()
+    assert ctl["iter"] == v["iteration"] and ctl["rollbacks"] == v["rollbacks"] and ctl["rollbacks"] > 0
+    assert cases.max_rel_disp_error(g["X"], v["X"], v["X0"]) < 1e-9
+
+
+@pytest.mark.parametrize("form", ["cta", "plain"])
+def test_node_frame_load_matches_oracle(oracle_mod, form):
+    """a load given in the node frame (solver_cpu.js:755-758) rotates with the lath; in the resident form the nodes
+    read the frames before the segments update them"""
+    md = cases.crossing(0.0, 0.0, local=True)
+    md.local_load_F[:] = [8.0, -50.0, 3.0]
+    v = oracle_mod.Oracle(md.copy()).run(3000)
+    s = ws.GpuSolver([md.copy()], precision="f64", form=form)
+    ctl = s.step(3000)[0]
+    g = s.download(0)
+    s.dispose()
+    assert len(md.local_load_node) == 1
+    assert ctl["iter"] == v["iteration"] and ctl["rollbacks"] == v["rollbacks"]
+    assert cases.max_rel_disp_error(g["X"], v["X"], v["X0"]) < 1e-9

@@ -78,7 +78,7 @@ class WsControl(C.Structure):
 
 class WsOpts(C.Structure):
     _fields_ = [("precision", C.c_int32), ("form", C.c_int32), ("threads", C.c_int32), ("device", C.c_int32),
-                ("budget_bytes", C.c_uint64), ("history", C.c_int32), ("side_order", C.c_int32)]
+                ("budget_bytes", C.c_uint64), ("cta_state", C.c_int32), ("side_order", C.c_int32)]
 
 
 class WsStateOut(C.Structure):
@@ -125,6 +125,8 @@ def lib():
                                            C.POINTER(WsStateOut), C.POINTER(WsControl)]
             L.ws_stream.argtypes = [C.c_void_p]
             L.ws_stream.restype = C.c_void_p
+            L.ws_cta_resident.argtypes = [C.c_void_p]
+            L.ws_cta_resident.restype = C.c_int
             L.ws_side_order.argtypes = [C.c_void_p]
             L.ws_side_order.restype = C.c_int
             L.ws_device_bytes.argtypes = [C.c_void_p]

@@ -46,6 +46,8 @@ template <int P>
 void layout(Dev<P> &d, Carver &cv, const Sizes &z) {
   using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A; using U = typename Dev<P>::U; using S = typename Dev<P>::S;
   d.ntot = z.n; d.mtot = z.m; d.ptot = z.p; d.ctot = z.c; d.ktot = z.k; d.stot = z.s;
+  d.nS = z.n; d.xB = 3 * z.n; d.mS = z.m; d.qB = 4 * z.m; d.pS = z.p; d.cS = z.c; d.kS = z.k;
+  d.sS = d.kB = d.oB = 2 * z.k; d.rB = z.m;
   const size_t n = z.n, m = z.m, p = z.p, c = z.c, k = z.k, s = z.s;
   d.X = cv.take<S>(6 * n); d.Xlo = PrecT<P>::TWO ? cv.take<S>(6 * n) : nullptr;
   d.V = cv.take<R>(3 * n); d.mass = cv.take<R>(n); d.lc = cv.take<R>(3 * n); d.ll = cv.take<R>(3 * n);
@@ -121,6 +123,8 @@ struct ws_ctx {
   int gridBlocks[2] = {0, 0};   // grid form: co-resident blocks with the general / short-slide side order
   PlainShape shape{};
   int sidesGeneral = 0;          // ws_opts.side_order == WS_SIDES_GENERAL
+  int ctaGlobal = 0;             // ws_opts.cta_state == WS_CTA_GLOBAL
+  size_t residentBytes = 0;      // batched form: dynamic shared memory of the resident form (0: global state)
   bool shortSides = false;       // the short-slide side order is in use
   cudaGraphExec_t graph = nullptr;
   int graphIters = 0, graphKey = -1;
@@ -221,6 +225,8 @@ InstDesc describe(const HostGoals &g, const Sizes &off) {
   I.k0 = off.k; I.K = g.K; I.s0 = off.s; I.S = g.S;
   I.warmup = g.prm.warmup_iter; I.ramp_iter = std::max(g.prm.ramp_iter, 0); I.disp_ramp = std::max(g.prm.disp_ramp_iter, 0);
   I.kd = g.prm.kinetic_damping ? 1 : 0; I.contacts = g.prm.contacts ? 1 : 0; I.max_iter = g.prm.max_iter > 0 ? g.prm.max_iter : 0x7fffffff;
+  I.localLoads = 0;
+  for (uint8_t h : g.hasLocal) I.localLoads |= h ? 1 : 0;
   I.ms = g.prm.mass_scale; I.damping = g.prm.damping; I.tol = g.prm.tol; I.strength = g.prm.strength; I.stick = g.prm.stick_strength;
   I.tf = g.prm.torsion_factor; I.eps = g.prm.epsilon; I.slip_rate = g.prm.slip_rate; I.lRef = g.lRef; I.jLenMin = g.jLenMin;
   return I;
@@ -463,8 +469,15 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
   CK(cudaEventRecord(c->ev0, c->st));
   if (c->form == WS_FORM_CTA) {
     if (mask) CK(cudaMemcpyAsync(c->dMask, mask, nInst, cudaMemcpyHostToDevice, c->st));
-    const int thr = c->threads > 0 ? c->threads : 256;
-    CK(launchBatched<P>(devOf<P>(c), c->dInst, c->dCtl, c->dOrder, nInst, nIter, mask ? c->dMask : nullptr, thr, nInst, c->shortSides, c->st));
+    if (c->residentBytes) {
+      const int thr = c->threads > 0 ? std::min(c->threads, 512) : 512;
+      CK(launchResident<P>(devOf<P>(c), c->dInst, c->dCtl, c->dOrder, nInst, nIter, mask ? c->dMask : nullptr, thr,
+                           c->residentBytes, c->shortSides, c->st));
+    } else {
+      const int thr = c->threads > 0 ? c->threads : 256;
+      CK(launchBatched<P>(devOf<P>(c), c->dInst, c->dCtl, c->dOrder, nInst, nIter, mask ? c->dMask : nullptr, thr, nInst,
+                          c->shortSides, c->st));
+    }
     c->lastLaunches = 1;
   } else if (c->form == WS_FORM_GRID) {
     CK(cudaMemsetAsync(c->dBar, 0, 2 * sizeof(unsigned), c->st));
@@ -547,6 +560,19 @@ void pullState(ws_ctx *c, int b) {
   if (g.K) { g.u = u; g.nPrev = np; }
 }
 
+// the batched form keeps its instances in shared memory when the largest fits a block (re-evaluated when the side
+// order changes, as the layout depends on it)
+template <int P>
+void selectResident(ws_ctx *c) {
+  c->residentBytes = 0;
+  if (c->form != WS_FORM_CTA || c->ctaGlobal) return;
+  size_t need = 0;
+  for (const InstDesc &I : c->inst) need = std::max<size_t>(need, residentLayout<P>(I.n, I.m, I.p, I.C, I.K, c->shortSides).bytes);
+  size_t granted = 0;
+  CK(residentPrepare<P>(need, c->shortSides, &granted));
+  c->residentBytes = granted;
+}
+
 // a warm start may change the slide limit or switch contacts: on a change of side order, every instance's order and
 // keys are rebuilt from its current slide coordinates into the buffer its next iteration reads
 template <int P>
@@ -561,6 +587,7 @@ void reselectOrder(ws_ctx *c) {
   }
   flushPuts(c);
   c->shortSides = ok;
+  selectResident<P>(c);
 }
 
 template <int P>
@@ -709,6 +736,8 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
   c->prec = o.precision; c->form = o.form; c->threads = o.threads; c->device = o.device;
   if (o.side_order < 0 || o.side_order > 1) { delete c; return fail(WS_ERR_ARG, "ws_create: unknown side order"); }
   c->sidesGeneral = o.side_order == WS_SIDES_GENERAL;
+  if (o.cta_state < 0 || o.cta_state > 1) { delete c; return fail(WS_ERR_ARG, "ws_create: unknown cta_state"); }
+  c->ctaGlobal = o.cta_state == WS_CTA_GLOBAL;
   int rc = guarded("ws_create", [&]() {
     CK(cudaSetDevice(o.device));
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
@@ -758,6 +787,7 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     CK(cudaMalloc(&c->dErr, sizeof(int)));
     c->shortSides = shortOrderOK(c);
     DISPATCH(c, setupDev, c);
+    DISPATCH(c, selectResident, c);
     size_t total = c->bytes + (sizeof(InstDesc) + sizeof(InstCtl) + 8) * n_instances;
     if (o.budget_bytes && total > o.budget_bytes) throw std::bad_alloc();
     CK(cudaStreamSynchronize(c->st));
@@ -817,6 +847,7 @@ int ws_internalize(ws_ctx *c, int32_t b) {
 void *ws_stream(ws_ctx *c) { return c ? c->st : nullptr; }
 uint64_t ws_device_bytes(const ws_ctx *c) { return c ? c->bytes : 0; }
 int ws_side_order(const ws_ctx *c) { return c && c->shortSides ? 1 : 0; }
+int ws_cta_resident(const ws_ctx *c) { return c && c->residentBytes ? 1 : 0; }
 int ws_last_step_stats(const ws_ctx *c_, double *ms, int64_t *launches) {
   if (!c_) return fail(WS_ERR_ARG, "ws_last_step_stats: null context");
   ws_ctx *c = const_cast<ws_ctx *>(c_);

@@ -28,7 +28,7 @@ template <> struct PrecT<PREC_F32> { using R = float; using W = float; using A =
 // per-instance description (host-written, read-only on the device)
 struct InstDesc {
   int n0, n, m0, m, p0, p, c0, C, k0, K, s0, S;   // first global element and count: nodes, segments, joints, clamps, crossings, strands
-  int warmup, ramp_iter, disp_ramp, kd, contacts, max_iter;
+  int warmup, ramp_iter, disp_ramp, kd, contacts, max_iter, localLoads;   // localLoads: some node carries a node-frame load
   double ms, damping, tol, strength, stick, tf, eps, slip_rate, lRef, jLenMin;
 };
 
@@ -49,6 +49,11 @@ struct Dev {
   using T = PrecT<P>;
   using R = typename T::R; using W = typename T::W; using A = typename T::A; using U = typename T::U; using S = typename T::S;
   int ntot, mtot, ptot, ctot, ktot, stot;
+  // Plane and buffer strides of the arrays that change every iteration.  In the global layout they follow the totals
+  // (nS = ntot, xB = 3 ntot, mS = mtot, qB = 4 mtot, pS = ptot, cS = ctot, kS = ktot, sS = kB = oB = 2 ktot,
+  // rB = mtot); the resident form points those arrays into shared memory with one instance's counts as strides (and
+  // buffer strides of 0 where it works in place).
+  int nS, xB, mS, qB, pS, cS, kS, sS, kB, oB, rB;
   // nodes: planes [buf][3][ntot] (lo planes only for MIXED)
   S *X, *Xlo;
   R *V;            // [3][ntot]
@@ -98,5 +103,37 @@ struct Dev {
   int *stSegOff;                // [stot] first (global) segment of the strand
   int *ord, *ordSeg;            // [2][2 ktot] side positions sorted by (local segment, position) per strand; their keys
 };
+
+// Shared-memory layout of one instance in the resident form: byte offsets of the arrays that change every iteration
+// (one buffer of positions and frames, updated in place), from the instance's element counts.  The host sizes the
+// launch with the same function.  The side order keeps one buffer of the order and slices in the short-slide variant,
+// two in the general one.
+struct ResLayout {
+  unsigned X, Xlo, V, Q, Qlo, Wr, nF, en, tau, kd, tauC, u, nPrev, sKey, sT, kth, sF, sTq, ord, ordSeg, rngLo, rngHi, bytes;
+};
+__host__ __device__ inline unsigned resTake(unsigned &o, size_t bytes) {
+  const unsigned r = o;
+  o += unsigned((bytes + 15) & ~size_t(15));
+  return r;
+}
+template <int P>
+__host__ __device__ inline ResLayout residentLayout(int n, int m, int p, int C, int K, bool shortSides) {
+  using R = typename PrecT<P>::R; using S = typename PrecT<P>::S; using U = typename PrecT<P>::U;
+  const bool two = PrecT<P>::TWO;
+  const size_t N = n, M = m, J = p, CC = C, K2 = 2 * size_t(K), nb = shortSides ? 1 : 2;
+  ResLayout L{};
+  unsigned o = 0;
+  L.X = resTake(o, 3 * N * sizeof(S)); L.Xlo = two ? resTake(o, 3 * N * sizeof(S)) : 0; L.V = resTake(o, 3 * N * sizeof(R));
+  L.Q = resTake(o, 4 * M * sizeof(S)); L.Qlo = two ? resTake(o, 4 * M * sizeof(S)) : 0; L.Wr = resTake(o, 3 * M * sizeof(R));
+  L.nF = resTake(o, 3 * M * sizeof(R)); L.en = resTake(o, 3 * M * sizeof(R));
+  L.tau = resTake(o, 3 * J * sizeof(R)); L.kd = resTake(o, 3 * J * sizeof(R)); L.tauC = resTake(o, 3 * CC * sizeof(R));
+  L.u = resTake(o, K2 * sizeof(U)); L.nPrev = resTake(o, 3 * size_t(K) * sizeof(R));
+  L.sKey = resTake(o, 2 * K2 * sizeof(int)); L.sT = resTake(o, K2 * sizeof(R)); L.kth = resTake(o, K2 * sizeof(R));
+  L.sF = resTake(o, 3 * K2 * sizeof(R)); L.sTq = resTake(o, 3 * K2 * sizeof(R));
+  L.ord = resTake(o, nb * K2 * sizeof(int)); L.ordSeg = resTake(o, nb * K2 * sizeof(int));
+  L.rngLo = resTake(o, nb * M * sizeof(int)); L.rngHi = resTake(o, nb * M * sizeof(int));
+  L.bytes = o;
+  return L;
+}
 
 }  // namespace wsb

@@ -110,6 +110,196 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
   }
 }
 
+// ------------------------------------------------------------------------------------------------ resident form
+// The batched form with each instance's changing state held in shared memory for the whole launch: positions,
+// frames, velocities, the element results of phase A, the side records, the order and the slide coordinates.  Static
+// data (topology, stiffness, loads) is read from global memory through L1; outputs that only a download reads (axial
+// and shear forces, moments, contact forces, reactions, slip) are written to global memory as they are produced.
+// Positions and frames are updated in place; the values they had at the start of the iteration go to a global backup
+// buffer, and a kinetic-damping roll-back copies them back.
+
+// the instance's shared-memory view: the changing arrays point into `sm`, offset so that the global element indices
+// of the phase code land on the instance's local rows
+template <int P>
+__device__ __forceinline__ Dev<P> residentView(const Dev<P> &d, const InstDesc &I, unsigned char *sm, const ResLayout &L, bool shortSides) {
+  using R = typename Dev<P>::R; using S = typename Dev<P>::S; using U = typename Dev<P>::U;
+  Dev<P> v = d;
+  const int k2 = 2 * I.k0;
+  v.X = reinterpret_cast<S *>(sm + L.X) - I.n0;
+  v.Xlo = PrecT<P>::TWO ? reinterpret_cast<S *>(sm + L.Xlo) - I.n0 : nullptr;
+  v.V = reinterpret_cast<R *>(sm + L.V) - I.n0;
+  v.Q = reinterpret_cast<S *>(sm + L.Q) - I.m0;
+  v.Qlo = PrecT<P>::TWO ? reinterpret_cast<S *>(sm + L.Qlo) - I.m0 : nullptr;
+  v.Wr = reinterpret_cast<R *>(sm + L.Wr) - I.m0;
+  v.nF = reinterpret_cast<R *>(sm + L.nF) - I.m0;
+  v.en = reinterpret_cast<R *>(sm + L.en) - I.m0;
+  v.tau = reinterpret_cast<R *>(sm + L.tau) - I.p0;
+  v.kd = reinterpret_cast<R *>(sm + L.kd) - I.p0;
+  v.tauC = reinterpret_cast<R *>(sm + L.tauC) - I.c0;
+  v.u = reinterpret_cast<U *>(sm + L.u) - I.k0;
+  v.nPrev = reinterpret_cast<R *>(sm + L.nPrev) - I.k0;
+  v.sKey = reinterpret_cast<int *>(sm + L.sKey) - k2;
+  v.sT = reinterpret_cast<R *>(sm + L.sT) - k2;
+  v.kth = reinterpret_cast<R *>(sm + L.kth) - k2;
+  v.sF = reinterpret_cast<R *>(sm + L.sF) - k2;
+  v.sTq = reinterpret_cast<R *>(sm + L.sTq) - k2;
+  v.ord = reinterpret_cast<int *>(sm + L.ord) - k2;
+  v.ordSeg = reinterpret_cast<int *>(sm + L.ordSeg) - k2;
+  v.rngLo = reinterpret_cast<int *>(sm + L.rngLo) - I.m0;
+  v.rngHi = reinterpret_cast<int *>(sm + L.rngHi) - I.m0;
+  v.nS = I.n; v.xB = 0; v.mS = I.m; v.qB = 0; v.pS = I.p; v.cS = I.C; v.kS = I.K;
+  v.sS = v.kB = 2 * I.K;
+  v.oB = shortSides ? 0 : 2 * I.K;
+  v.rB = shortSides ? 0 : I.m;
+  return v;
+}
+
+// copy `planes` planes of `count` elements from array a (plane stride as, first element a0) to array b (bs, b0)
+template <class T>
+__device__ __forceinline__ void copyPlanes(T *b, int bs, const T *a, int as, int first, int count, int planes) {
+  for (int e = threadIdx.x; e < planes * count; e += blockDim.x) {
+    const int k = e / count, i = first + e % count;
+    b[size_t(k) * bs + i] = a[size_t(k) * as + i];
+  }
+}
+
+// global -> shared at the start of a launch (g: the global view, v: the instance's shared view); positions and
+// frames from buffer `home`
+template <int P, bool SHORT>
+__device__ void residentLoad(const Dev<P> &g, const Dev<P> &v, const InstDesc &I, const InstCtl &c, int home) {
+  copyPlanes(v.X, v.nS, g.X + size_t(home) * g.xB, g.nS, I.n0, I.n, 3);
+  if constexpr (PrecT<P>::TWO) copyPlanes(v.Xlo, v.nS, g.Xlo + size_t(home) * g.xB, g.nS, I.n0, I.n, 3);
+  copyPlanes(v.V, v.nS, g.V, g.nS, I.n0, I.n, 3);
+  copyPlanes(v.Q, v.mS, g.Q + size_t(home) * g.qB, g.mS, I.m0, I.m, 4);
+  if constexpr (PrecT<P>::TWO) copyPlanes(v.Qlo, v.mS, g.Qlo + size_t(home) * g.qB, g.mS, I.m0, I.m, 4);
+  copyPlanes(v.Wr, v.mS, g.Wr, g.mS, I.m0, I.m, 3);
+  if (!I.K) return;
+  copyPlanes(v.u, v.kS, g.u, g.kS, I.k0, I.K, 2);
+  copyPlanes(v.nPrev, v.kS, g.nPrev, g.kS, I.k0, I.K, 3);
+  const int k2 = 2 * I.k0, K2 = 2 * I.K;
+  // the keys of the sides before the next slide; the order and slices the next iteration reads (or, short order,
+  // the slices an earlier iteration left: a valid base for the segments without sides)
+  copyPlanes(v.sKey + size_t(c.obuf) * v.kB, 0, g.sKey + size_t(c.obuf) * g.kB, 0, k2, K2, 1);
+  copyPlanes(v.rngLo + size_t(SHORT ? 0 : c.obuf) * v.rB, 0, g.rngLo + size_t(c.obuf) * g.rB, 0, I.m0, I.m, 1);
+  copyPlanes(v.rngHi + size_t(SHORT ? 0 : c.obuf) * v.rB, 0, g.rngHi + size_t(c.obuf) * g.rB, 0, I.m0, I.m, 1);
+  if constexpr (!SHORT) {
+    copyPlanes(v.ord + size_t(c.obuf) * v.oB, 0, g.ord + size_t(c.obuf) * g.oB, 0, k2, K2, 1);
+    copyPlanes(v.ordSeg + size_t(c.obuf) * v.oB, 0, g.ordSeg + size_t(c.obuf) * g.oB, 0, k2, K2, 1);
+  }
+}
+
+// shared -> global at the end of a launch, into the buffers the control block names
+template <int P, bool SHORT>
+__device__ void residentStore(const Dev<P> &g, const Dev<P> &v, const InstDesc &I, const InstCtl &c) {
+  copyPlanes(g.X + size_t(c.cur) * g.xB, g.nS, v.X, v.nS, I.n0, I.n, 3);
+  if constexpr (PrecT<P>::TWO) copyPlanes(g.Xlo + size_t(c.cur) * g.xB, g.nS, v.Xlo, v.nS, I.n0, I.n, 3);
+  copyPlanes(g.V, g.nS, v.V, v.nS, I.n0, I.n, 3);
+  copyPlanes(g.Q + size_t(c.cur) * g.qB, g.mS, v.Q, v.mS, I.m0, I.m, 4);
+  if constexpr (PrecT<P>::TWO) copyPlanes(g.Qlo + size_t(c.cur) * g.qB, g.mS, v.Qlo, v.mS, I.m0, I.m, 4);
+  copyPlanes(g.Wr, g.mS, v.Wr, v.mS, I.m0, I.m, 3);
+  if (!I.K) return;
+  copyPlanes(g.u, g.kS, v.u, v.kS, I.k0, I.K, 2);
+  copyPlanes(g.nPrev, g.kS, v.nPrev, v.kS, I.k0, I.K, 3);
+  const int k2 = 2 * I.k0, K2 = 2 * I.K;
+  copyPlanes(g.sKey + size_t(c.obuf) * g.kB, 0, v.sKey + size_t(c.obuf) * v.kB, 0, k2, K2, 1);
+  copyPlanes(g.rngLo + size_t(c.obuf) * g.rB, 0, v.rngLo + size_t(SHORT ? 0 : c.obuf) * v.rB, 0, I.m0, I.m, 1);
+  copyPlanes(g.rngHi + size_t(c.obuf) * g.rB, 0, v.rngHi + size_t(SHORT ? 0 : c.obuf) * v.rB, 0, I.m0, I.m, 1);
+  if constexpr (!SHORT) {
+    copyPlanes(g.ord + size_t(c.obuf) * g.oB, 0, v.ord + size_t(c.obuf) * v.oB, 0, k2, K2, 1);
+    copyPlanes(g.ordSeg + size_t(c.obuf) * g.oB, 0, v.ordSeg + size_t(c.obuf) * v.oB, 0, k2, K2, 1);
+  }
+}
+
+// positions / frames of node i or segment j between the shared view and global buffer bk (backup or restore)
+template <int P>
+__device__ __forceinline__ void backupNode(const Dev<P> &g, const Dev<P> &v, int bk, int i, bool restore) {
+  for (int k = 0; k < 3; k++) {
+    const size_t go = size_t(bk) * g.xB + size_t(k) * g.nS + i, so = size_t(k) * v.nS + i;
+    if (restore) { v.X[so] = g.X[go]; if constexpr (PrecT<P>::TWO) v.Xlo[so] = g.Xlo[go]; }
+    else { g.X[go] = v.X[so]; if constexpr (PrecT<P>::TWO) g.Xlo[go] = v.Xlo[so]; }
+  }
+}
+template <int P>
+__device__ __forceinline__ void backupSeg(const Dev<P> &g, const Dev<P> &v, int bk, int j, bool restore) {
+  for (int k = 0; k < 4; k++) {
+    const size_t go = size_t(bk) * g.qB + size_t(k) * g.mS + j, so = size_t(k) * v.mS + j;
+    if (restore) { v.Q[so] = g.Q[go]; if constexpr (PrecT<P>::TWO) v.Qlo[so] = g.Qlo[go]; }
+    else { g.Q[go] = v.Q[so]; if constexpr (PrecT<P>::TWO) g.Qlo[go] = v.Qlo[so]; }
+  }
+}
+
+template <int P, bool SHORT>
+__global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+                                                      const int *__restrict__ order, int nInst, int nIter, const uint8_t *__restrict__ mask) {
+  using A = typename Dev<P>::A;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ InstCtl sc;
+  __shared__ InstDesc si;
+  __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
+  for (int bi = blockIdx.x; bi < nInst; bi += gridDim.x) {
+    const int b = order ? order[bi] : bi;
+    if (mask && !mask[b]) continue;
+    if (threadIdx.x == 0) { sc = ctl[b]; si = insts[b]; }
+    __syncthreads();
+    const InstDesc &I = si;
+    const ResLayout L = residentLayout<P>(I.n, I.m, I.p, I.C, I.K, SHORT);
+    const Dev<P> v = residentView<P>(d, I, smem, L, SHORT);
+    const int bk = sc.cur ^ 1;          // global buffer that holds the start of each iteration (roll-back)
+    residentLoad<P, SHORT>(d, v, I, sc, sc.cur);
+    __syncthreads();
+    const bool cx = I.contacts && I.K;
+    const int nA = countA<SHORT>(I);
+    for (int it = 0; it < nIter; it++) {
+      if (sc.status != WS_RUNNING) break;
+      StepCtx sx = makeCtx<A>(I, sc);
+      sx.cur = sx.nxt = 0;              // in place
+      Part<A> pt;
+      pt.init();
+      for (int e = threadIdx.x; e < nA; e += blockDim.x) phaseA<P, SHORT>(v, I, sx, e, cx ? I.K : 0, pt);
+      __syncthreads();
+      if (!SHORT && cx) {
+        for (int e = threadIdx.x; e < 2 * I.K + I.m; e += blockDim.x) phaseBC<P>(v, I, sx, e);
+        __syncthreads();
+      }
+      if (I.localLoads) {               // node-frame loads read the frames before the segments update them
+        for (int e = threadIdx.x; e < I.n; e += blockDim.x) {
+          if (I.kd) backupNode<P>(d, v, bk, I.n0 + e, false);
+          nodeUpdate<P, SHORT>(v, I, sx, I.n0 + e, pt);
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < I.m; e += blockDim.x) {
+          if (I.kd) backupSeg<P>(d, v, bk, I.m0 + e, false);
+          segUpdate<P, SHORT>(v, I, sx, I.m0 + e, pt);
+        }
+      } else {
+        for (int e = threadIdx.x; e < I.n + I.m; e += blockDim.x) {
+          if (e < I.n) {
+            if (I.kd) backupNode<P>(d, v, bk, I.n0 + e, false);
+            nodeUpdate<P, SHORT>(v, I, sx, I.n0 + e, pt);
+          } else {
+            if (I.kd) backupSeg<P>(d, v, bk, I.m0 + (e - I.n), false);
+            segUpdate<P, SHORT>(v, I, sx, I.m0 + (e - I.n), pt);
+          }
+        }
+      }
+      __syncthreads();
+      blockReduce(pt, red);
+      if (threadIdx.x == 0) decide(I, sc, pt, nIter);
+      __syncthreads();
+      if (sc.pending) {                 // roll-back: the positions and frames of the iteration's start
+        for (int e = threadIdx.x; e < I.n + I.m; e += blockDim.x) {
+          if (e < I.n) backupNode<P>(d, v, bk, I.n0 + e, true);
+          else backupSeg<P>(d, v, bk, I.m0 + (e - I.n), true);
+        }
+        __syncthreads();
+      }
+    }
+    residentStore<P, SHORT>(d, v, I, sc);
+    if (threadIdx.x == 0) ctl[b] = sc;
+    __syncthreads();
+  }
+}
+
 // ------------------------------------------------------------------------------------------------ plain form
 // One kernel per phase over the elements of instance 0; block partials go to part[block] and the last block of the
 // update kernel reduces them in a fixed order.  Every kernel returns at once when the instance has stopped.
@@ -259,6 +449,31 @@ cudaError_t launchBatched(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, 
   return cudaGetLastError();
 }
 
+// dynamic shared memory of the resident form for a batch whose largest instance needs `bytes` (0 when it does not fit
+// on this device); sets the kernel's limit to it
+template <int P>
+cudaError_t residentPrepare(size_t bytes, bool shortSides, size_t *granted) {
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa{};
+  cudaError_t e = shortSides ? cudaFuncGetAttributes(&fa, k_resident<P, true>) : cudaFuncGetAttributes(&fa, k_resident<P, false>);
+  if (e != cudaSuccess) return e;
+  *granted = 0;
+  if (bytes + fa.sharedSizeBytes > size_t(optin)) return cudaSuccess;
+  e = shortSides ? cudaFuncSetAttribute(k_resident<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes))
+                 : cudaFuncSetAttribute(k_resident<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+  if (e == cudaSuccess) *granted = bytes;
+  return e;
+}
+template <int P>
+cudaError_t launchResident(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
+                           const uint8_t *mask, int threads, size_t smemBytes, bool shortSides, cudaStream_t st) {
+  if (shortSides) k_resident<P, true><<<nInst, threads, smemBytes, st>>>(d, insts, ctl, order, nInst, nIter, mask);
+  else k_resident<P, false><<<nInst, threads, smemBytes, st>>>(d, insts, ctl, order, nInst, nIter, mask);
+  return cudaGetLastError();
+}
+
 // a launch of the plain form with programmatic stream serialisation (the kernel may start while its predecessor ends)
 template <class... KArgs, class... Args>
 static cudaError_t launchPDL(void (*k)(KArgs...), int blocks, cudaStream_t st, Args... args) {
@@ -325,7 +540,10 @@ int gridBlocks(bool shortSides) {
                                           bool, cudaStream_t, int *, unsigned *);                                    \
   template cudaError_t launchGrid<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, unsigned *, int *, int, int, bool, \
                                      cudaStream_t);                                                                  \
-  template int gridBlocks<P>(bool);
+  template int gridBlocks<P>(bool);                                                                                 \
+  template cudaError_t residentPrepare<P>(size_t, bool, size_t *);                                                   \
+  template cudaError_t launchResident<P>(const Dev<P> &, const InstDesc *, InstCtl *, const int *, int, int, const uint8_t *, \
+                                         int, size_t, bool, cudaStream_t);
 WSB_INST(PREC_F64)
 WSB_INST(PREC_MIXED)
 WSB_INST(PREC_F32)

@@ -22,5 +22,12 @@ cudaError_t launchGrid(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, voi
                        int blocks, bool shortSides, cudaStream_t st);
 template <int P>
 int gridBlocks(bool shortSides);
+// resident form: checks that `bytes` of dynamic shared memory fit a block on this device and opts the kernel in
+// (*granted = bytes), else *granted = 0
+template <int P>
+cudaError_t residentPrepare(size_t bytes, bool shortSides, size_t *granted);
+template <int P>
+cudaError_t launchResident(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
+                           const uint8_t *mask, int threads, size_t smemBytes, bool shortSides, cudaStream_t st);
 
 }  // namespace wsb

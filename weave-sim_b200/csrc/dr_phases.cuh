@@ -92,21 +92,21 @@ template <int P> struct Acc {
   using D = Dev<P>;
   using R = typename D::R; using W = typename D::W; using S = typename D::S;
   __device__ static __forceinline__ W xw(const D &d, int buf, int k, int i) {
-    const size_t o = size_t(buf * 3 + k) * d.ntot + i;
+    const size_t o = size_t(buf) * d.xB + size_t(k) * d.nS + i;
     if constexpr (PrecT<P>::TWO) return W(d.X[o]) + W(d.Xlo[o]); else return W(d.X[o]);
   }
-  __device__ static __forceinline__ R xr(const D &d, int buf, int k, int i) { return R(d.X[size_t(buf * 3 + k) * d.ntot + i]); }
+  __device__ static __forceinline__ R xr(const D &d, int buf, int k, int i) { return R(d.X[size_t(buf) * d.xB + size_t(k) * d.nS + i]); }
   __device__ static __forceinline__ void xs(const D &d, int buf, int k, int i, W v) {
-    const size_t o = size_t(buf * 3 + k) * d.ntot + i;
+    const size_t o = size_t(buf) * d.xB + size_t(k) * d.nS + i;
     if constexpr (PrecT<P>::TWO) { const S hi = S(v); d.X[o] = hi; d.Xlo[o] = S(v - W(hi)); } else d.X[o] = S(v);
   }
   __device__ static __forceinline__ W qw(const D &d, int buf, int k, int j) {
-    const size_t o = size_t(buf * 4 + k) * d.mtot + j;
+    const size_t o = size_t(buf) * d.qB + size_t(k) * d.mS + j;
     if constexpr (PrecT<P>::TWO) return W(d.Q[o]) + W(d.Qlo[o]); else return W(d.Q[o]);
   }
-  __device__ static __forceinline__ R qr(const D &d, int buf, int k, int j) { return R(d.Q[size_t(buf * 4 + k) * d.mtot + j]); }
+  __device__ static __forceinline__ R qr(const D &d, int buf, int k, int j) { return R(d.Q[size_t(buf) * d.qB + size_t(k) * d.mS + j]); }
   __device__ static __forceinline__ void qs(const D &d, int buf, int k, int j, W v) {
-    const size_t o = size_t(buf * 4 + k) * d.mtot + j;
+    const size_t o = size_t(buf) * d.qB + size_t(k) * d.mS + j;
     if constexpr (PrecT<P>::TWO) { const S hi = S(v); d.Q[o] = hi; d.Qlo[o] = S(v - W(hi)); } else d.Q[o] = S(v);
   }
   // edge vector x_b − x_a formed in the wide type, returned in R
@@ -186,9 +186,9 @@ __device__ __forceinline__ void segForce(const Dev<P> &d, int buf, int j, Part<t
   const R e[3] = {R(ew[0]), R(ew[1]), R(ew[2])};
   R en[3];
   cross3(e, nv, en);
-  const int mt = d.mtot;
-  for (int k = 0; k < 3; k++) { d.nF[k * mt + j] = nv[k]; d.en[k * mt + j] = en[k]; }
-  d.Nax[j] = n3; d.Vsh[j] = n1; d.Vsh[mt + j] = n2;
+  const int ms = d.mS;
+  for (int k = 0; k < 3; k++) { d.nF[k * ms + j] = nv[k]; d.en[k * ms + j] = en[k]; }
+  d.Nax[j] = n3; d.Vsh[j] = n1; d.Vsh[d.mtot + j] = n2;
   const R l0r = d.l0[j];
   pt.s[RS_STRETCH] += A(R(0.5) * l0r * n3 * s3);
   pt.s[RS_SHEAR] += A(R(0.5) * l0r * (n1 * s1 + n2 * s2));
@@ -236,8 +236,8 @@ __device__ __forceinline__ void jointTorque(const Dev<P> &d, int buf, int jt, Pa
   {
     const R q0 = psi[0] * psi[0], q1 = psi[1] * psi[1], q2 = psi[2] * psi[2], f = R(0.25) / lb;
     d.kd[jt] = f * (EIy * q2 + GJ * q1);
-    d.kd[pt_ + jt] = f * (EIx * q2 + GJ * q0);
-    d.kd[2 * pt_ + jt] = f * (EIx * q1 + EIy * q0);
+    d.kd[d.pS + jt] = f * (EIx * q2 + GJ * q0);
+    d.kd[2 * d.pS + jt] = f * (EIx * q1 + EIy * q0);
   }
   R jv[3];
   jlinvT(psi, mm, th, jv);
@@ -245,7 +245,7 @@ __device__ __forceinline__ void jointTorque(const Dev<P> &d, int buf, int jt, Pa
   for (int k = 0; k < 4; k++) qr[k] = R(qa[k]);
   qframe(qr, Ra);
   for (int k = 0; k < 3; k++) {
-    d.tau[k * pt_ + jt] = jv[0] * Ra[k] + jv[1] * Ra[3 + k] + jv[2] * Ra[6 + k];
+    d.tau[k * d.pS + jt] = jv[0] * Ra[k] + jv[1] * Ra[3 + k] + jv[2] * Ra[6 + k];
     d.Mj[k * pt_ + jt] = mm[k];
   }
   pt.s[RS_BEND] += A(R(0.5) * lb * (mm[0] * dd[0] + mm[1] * dd[1]));
@@ -270,7 +270,7 @@ __device__ __forceinline__ void clampTorque(const Dev<P> &d, int buf, int cc, Pa
   R qr[4], Rc[9];
   for (int k = 0; k < 4; k++) qr[k] = R(qa[k]);
   qframe(qr, Rc);
-  for (int k = 0; k < 3; k++) d.tauC[k * ct + cc] = jv[0] * Rc[k] + jv[1] * Rc[3 + k] + jv[2] * Rc[6 + k];
+  for (int k = 0; k < 3; k++) d.tauC[k * d.cS + cc] = jv[0] * Rc[k] + jv[1] * Rc[3 + k] + jv[2] * Rc[6 + k];
   d.cM[cc] = mm[0]; d.cM[ct + cc] = mm[1];
   pt.s[RS_BEND] += A(R(0.5) * lc * (mm[0] * dd[0] + mm[1] * dd[1]));
   pt.s[RS_TWIST] += A(R(0.5) * lc * mm[2] * dd[2]);
@@ -291,7 +291,7 @@ __device__ __forceinline__ R support(const R Rf[9], const R n[3], R sign, R w, R
 template <int P>
 __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int buf, int iter, int kb, int c, Part<typename Dev<P>::A> &pt) {
   using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A; using U = typename Dev<P>::U;
-  const int kt_ = d.ktot, K2 = 2 * kt_;
+  const int kt_ = d.ktot, ks = d.kS, K2 = d.sS;
   const int pos[2] = {d.sPos[2 * c], d.sPos[2 * c + 1]};
   const double rampN = I.ramp_iter;
   const double rampd = rampN <= 0 ? 1.0 : fmin(1.0, 0.01 + 0.99 * double(iter) / rampN);
@@ -301,7 +301,7 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   U uu[2];
   for (int side = 0; side < 2; side++) {
     const int o = side * kt_ + c;
-    uu[side] = d.u[o];
+    uu[side] = d.u[side * ks + c];
     nseg[side] = d.cxNseg[o];
     const int li = int(mmin(mmax(mfloor(uu[side]), U(0)), U(mmax(nseg[side] - 1, 0))));
     const R t = R(mmin(mmax(uu[side] - U(li), U(0)), U(1)));
@@ -342,12 +342,12 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   // contact normal with side persistence (solver_cpu.js:396-402)
   R nv[3];
   cross3(tA, tB, nv);
-  R np[3] = {d.nPrev[c], d.nPrev[kt_ + c], d.nPrev[2 * kt_ + c]};
+  R np[3] = {d.nPrev[c], d.nPrev[ks + c], d.nPrev[2 * ks + c]};
   const R nn = msqrt(dot3(nv, nv));
   if (nn < R(1e-6)) { nv[0] = np[0]; nv[1] = np[1]; nv[2] = np[2]; }
   else { const R dn = mmax(nn, R(1e-12)); nv[0] /= dn; nv[1] /= dn; nv[2] /= dn; }
   if (dot3(nv, np) < R(0)) { nv[0] = -nv[0]; nv[1] = -nv[1]; nv[2] = -nv[2]; }
-  for (int k = 0; k < 3; k++) d.nPrev[k * kt_ + c] = nv[k];
+  for (int k = 0; k < 3; k++) d.nPrev[k * ks + c] = nv[k];
   // gap vector P_B − P_A: the base-node difference in the wide type
   R S[3];
   for (int k = 0; k < 3; k++) S[k] = R(Acc<P>::xw(d, buf, k, base[1]) - Acc<P>::xw(d, buf, k, base[0])) + (Pl[1][k] - Pl[0][k]);
@@ -379,11 +379,11 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   const bool moved = slip || freeS;
   if (moved) { uu[0] += U(da) / U(mmax(L[0], R(1e-12))); uu[1] -= U(db) / U(mmax(L[1], R(1e-12))); }
   d.u[c] = mclamp(uu[0], U(0), U(nseg[0]));
-  d.u[kt_ + c] = mclamp(uu[1], U(0), U(nseg[1]));
+  d.u[ks + c] = mclamp(uu[1], U(0), U(nseg[1]));
   // the sides' segments after the slide (solver_cpu.js:144-149): the keys of the next sort, into key buffer kb
   for (int side = 0; side < 2; side++) {
-    const U un = d.u[side * kt_ + c];
-    d.sKey[size_t(kb) * K2 + pos[side]] = int(mmin(mmax(mfloor(un), U(0)), U(mmax(nseg[side] - 1, 0))));
+    const U un = d.u[side * ks + c];
+    d.sKey[size_t(kb) * d.kB + pos[side]] = int(mmin(mmax(mfloor(un), U(0)), U(mmax(nseg[side] - 1, 0))));
   }
   if (slip) {
     const R sx = da * tA[0] + db * tB[0], sy = da * tA[1] + db * tB[1], sz = da * tA[2] + db * tB[2];
@@ -440,17 +440,16 @@ __device__ __forceinline__ SideRank sideRank(const int *key, int p, int off, int
 // this iteration's slide); every segment's slice is then counted by segCount
 template <int P>
 __device__ __forceinline__ void rankSide(const Dev<P> &d, int p, int kb, int dst) {
-  const int K2 = 2 * d.ktot, s = d.sStrand[p];
-  const int *key = d.sKey + size_t(kb) * K2;
+  const int s = d.sStrand[p];
+  const int *key = d.sKey + size_t(kb) * d.kB;
   const SideRank r = sideRank(key, p, d.stSideOff[s], d.stSideCnt[s]);
-  d.ord[size_t(dst) * K2 + r.pos] = p;
-  d.ordSeg[size_t(dst) * K2 + r.pos] = key[p];
+  d.ord[size_t(dst) * d.oB + r.pos] = p;
+  d.ordSeg[size_t(dst) * d.oB + r.pos] = key[p];
 }
 // segment j: its slice of the new order = [off + #keys below, off + #keys below + #keys equal) among its strand's sides
 template <int P>
 __device__ __forceinline__ void segCount(const Dev<P> &d, int j, int kb, int dst) {
-  const int K2 = 2 * d.ktot;
-  const int *key = d.sKey + size_t(kb) * K2;
+  const int *key = d.sKey + size_t(kb) * d.kB;
   const int s = d.segStrand[j], lj = d.segLocal[j];
   const int off = d.stSideOff[s], cnt = d.stSideCnt[s];
   int lo = 0, eq = 0;
@@ -459,8 +458,8 @@ __device__ __forceinline__ void segCount(const Dev<P> &d, int j, int kb, int dst
     lo += kq < lj ? 1 : 0;
     eq += kq == lj ? 1 : 0;
   }
-  d.rngLo[size_t(dst) * d.mtot + j] = off + lo;
-  d.rngHi[size_t(dst) * d.mtot + j] = off + lo + eq;
+  d.rngLo[size_t(dst) * d.rB + j] = off + lo;
+  d.rngHi[size_t(dst) * d.rB + j] = off + lo + eq;
 }
 // short-slide order (the slide limit is under half the shortest segment, so a side moves at most one segment per
 // iteration): built inside the element phase from the keys of the previous iteration (the segments the sides sit on
@@ -469,16 +468,16 @@ __device__ __forceinline__ void segCount(const Dev<P> &d, int j, int kb, int dst
 // other keys, and the gathers skip entries whose key is not the segment's.
 template <int P>
 __device__ __forceinline__ void rankSideShort(const Dev<P> &d, int p, int buf) {
-  const int K2 = 2 * d.ktot, s = d.sStrand[p], off = d.stSideOff[s];
-  const int *key = d.sKey + size_t(buf) * K2;
+  const int s = d.sStrand[p], off = d.stSideOff[s];
+  const int *key = d.sKey + size_t(buf) * d.kB;
   const SideRank r = sideRank(key, p, off, d.stSideCnt[s]);
   const int k = key[p];
-  d.ord[size_t(buf) * K2 + r.pos] = p;
-  d.ordSeg[size_t(buf) * K2 + r.pos] = k;
+  d.ord[size_t(buf) * d.oB + r.pos] = p;
+  d.ordSeg[size_t(buf) * d.oB + r.pos] = k;
   if (r.pos == off + r.below) {
     const int j = d.stSegOff[s] + k;
-    d.rngLo[size_t(buf) * d.mtot + j] = off + r.below;
-    d.rngHi[size_t(buf) * d.mtot + j] = off + r.below + r.equal;
+    d.rngLo[size_t(buf) * d.rB + j] = off + r.below;
+    d.rngHi[size_t(buf) * d.rB + j] = off + r.below + r.equal;
   }
 }
 
@@ -492,23 +491,22 @@ struct StepCtx {
 // entry counts only if it carries the segment's key (a slice left over from an earlier iteration carries other keys)
 template <bool SHORT, int P, class F>
 __device__ __forceinline__ void sidesOn(const Dev<P> &d, int ob, int j, int lj, F &&f) {
-  const int K2 = 2 * d.ktot;
-  const int lo = d.rngLo[size_t(ob) * d.mtot + j], hi = d.rngHi[size_t(ob) * d.mtot + j];
+  const int lo = d.rngLo[size_t(ob) * d.rB + j], hi = d.rngHi[size_t(ob) * d.rB + j];
   for (int e = lo; e < hi; e++) {
-    if (SHORT && d.ordSeg[size_t(ob) * K2 + e] != lj) continue;
-    f(d.ord[size_t(ob) * K2 + e]);
+    if (SHORT && d.ordSeg[size_t(ob) * d.oB + e] != lj) continue;
+    f(d.ord[size_t(ob) * d.oB + e]);
   }
 }
 
 template <int P, bool SHORT>
 __device__ __forceinline__ void nodeUpdate(const Dev<P> &d, const InstDesc &I, const StepCtx &sc, int i, Part<typename Dev<P>::A> &pt) {
   using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A;
-  const int nt = d.ntot, mt = d.mtot, K2 = 2 * d.ktot;
+  const int nt = d.ntot, ns = d.nS, ms = d.mS, K2 = d.sS;
   const int so = d.nsOut[i], si = d.nsIn[i];
   const uint8_t fl = d.nflag[i];
   R F[3] = {R(0), R(0), R(0)};
-  if (so >= 0) for (int k = 0; k < 3; k++) F[k] += d.nF[k * mt + so];
-  if (si >= 0) for (int k = 0; k < 3; k++) F[k] -= d.nF[k * mt + si];
+  if (so >= 0) for (int k = 0; k < 3; k++) F[k] += d.nF[k * ms + so];
+  if (si >= 0) for (int k = 0; k < 3; k++) F[k] -= d.nF[k * ms + si];
   R tot[3] = {d.lc[i], d.lc[nt + i], d.lc[2 * nt + i]};
   if (fl & 16) {                          // load in the node frame (solver_cpu.js:755-758)
     R q[4], Rn[9];
@@ -535,14 +533,14 @@ __device__ __forceinline__ void nodeUpdate(const Dev<P> &d, const InstDesc &I, c
   for (int k = 0; k < 3; k++) if (!(fl & (1 << k))) F[k] = R(0);
   pt.x[RX_F] = mmax(pt.x[RX_F], A(msqrt(dot3(F, F))));
   R v[3];
-  for (int k = 0; k < 3; k++) v[k] = sc.pending || sc.warm ? R(0) : d.V[k * nt + i];
+  for (int k = 0; k < 3; k++) v[k] = sc.pending || sc.warm ? R(0) : d.V[k * ns + i];
   const R m = d.mass[i];
   if (!sc.warm) for (int k = 0; k < 3; k++) v[k] += F[k] / m;
   if (I.damping != 1.0) for (int k = 0; k < 3; k++) v[k] *= R(I.damping);
   for (int k = 0; k < 3; k++) if (!(fl & (1 << k))) v[k] = R(0);
   const int ai = (fl & 32) ? d.anc[i] : -1;
   for (int k = 0; k < 3; k++) {
-    d.V[k * nt + i] = v[k];
+    d.V[k * ns + i] = v[k];
     W x = Acc<P>::xw(d, sc.cur, k, i) + W(v[k]);
     if (ai >= 0 && !(fl & (1 << k))) x = d.ancStart[size_t(k) * nt + ai] + W(sc.dispR) * d.ancDelta[size_t(k) * nt + ai];
     Acc<P>::xs(d, sc.nxt, k, i, x);
@@ -553,15 +551,15 @@ __device__ __forceinline__ void nodeUpdate(const Dev<P> &d, const InstDesc &I, c
 template <int P, bool SHORT>
 __device__ __forceinline__ void segUpdate(const Dev<P> &d, const InstDesc &I, const StepCtx &sc, int j, Part<typename Dev<P>::A> &pt) {
   using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A;
-  const int mt = d.mtot, pt_ = d.ptot, ct = d.ctot, K2 = 2 * d.ktot;
-  R T[3] = {d.en[j], d.en[mt + j], d.en[2 * mt + j]};
+  const int mt = d.mtot, sm = d.mS, ps = d.pS, cs = d.cS, K2 = d.sS;
+  R T[3] = {d.en[j], d.en[sm + j], d.en[2 * sm + j]};
   R kD[3] = {R(0), R(0), R(0)};
   const int ja = d.jA[j], jb = d.jB[j];
-  if (ja >= 0) for (int k = 0; k < 3; k++) { T[k] += d.tau[k * pt_ + ja]; kD[k] += d.kd[k * pt_ + ja]; }
-  if (jb >= 0) for (int k = 0; k < 3; k++) { T[k] -= d.tau[k * pt_ + jb]; kD[k] += d.kd[k * pt_ + jb]; }
+  if (ja >= 0) for (int k = 0; k < 3; k++) { T[k] += d.tau[k * ps + ja]; kD[k] += d.kd[k * ps + ja]; }
+  if (jb >= 0) for (int k = 0; k < 3; k++) { T[k] -= d.tau[k * ps + jb]; kD[k] += d.kd[k * ps + jb]; }
   const int c0 = d.cl0[j], c1 = d.cl1[j];
-  if (c0 >= 0) for (int k = 0; k < 3; k++) T[k] -= d.tauC[k * ct + c0];
-  if (c1 >= 0) for (int k = 0; k < 3; k++) T[k] -= d.tauC[k * ct + c1];
+  if (c0 >= 0) for (int k = 0; k < 3; k++) T[k] -= d.tauC[k * cs + c0];
+  if (c1 >= 0) for (int k = 0; k < 3; k++) T[k] -= d.tauC[k * cs + c1];
   R kTw = R(0);
   if (I.contacts && I.K) {
     const int lj = SHORT ? d.segLocal[j] : 0;
@@ -569,7 +567,7 @@ __device__ __forceinline__ void segUpdate(const Dev<P> &d, const InstDesc &I, co
     if constexpr (SHORT) {
       // the sides on segment j after the slide were, before it, on j − 1, j or j + 1 of the same strand
       const int s = d.segStrand[j];
-      const int *key = d.sKey + size_t(sc.onxt) * K2;
+      const int *key = d.sKey + size_t(sc.onxt) * d.kB;
       for (int dj = -1; dj <= 1; dj++) {
         const int jj = j + dj;
         if (jj < 0 || jj >= mt || d.segStrand[jj] != s) continue;
@@ -589,12 +587,12 @@ __device__ __forceinline__ void segUpdate(const Dev<P> &d, const InstDesc &I, co
   R w[3], I3[3];
   for (int k = 0; k < 3; k++) {
     I3[k] = ms * mmax(d.krs[k * mt + j] + kTw + kD[k], R(1e-12));
-    w[k] = (sc.pending ? R(0) : d.Wr[k * mt + j]) + tm[k] / I3[k];
+    w[k] = (sc.pending ? R(0) : d.Wr[k * sm + j]) + tm[k] / I3[k];
   }
   w[2] = mclamp(w[2], R(-TWIST_RATE_MAX), R(TWIST_RATE_MAX));
   if (kTw > R(0)) w[2] *= R(ROLL_DAMP);
   if (I.damping != 1.0) for (int k = 0; k < 3; k++) w[k] *= R(I.damping);
-  for (int k = 0; k < 3; k++) d.Wr[k * mt + j] = w[k];
+  for (int k = 0; k < 3; k++) d.Wr[k * sm + j] = w[k];
   // q ← normalize(q ⊗ exp(ω)) in the wide type; the increment q ⊗ (exp(ω) − 1) is small, formed in R
   const R a = msqrt(dot3(w, w)), half = R(0.5) * a;
   R sh, ch;

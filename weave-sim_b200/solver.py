@@ -59,7 +59,8 @@ def relax_noalloc(model, n_iter, precision="mixed", threads=256, stream=None):
 
 
 class GpuSolver:
-    def __init__(self, models, precision="mixed", form="cta", threads=0, device=0, budget_bytes=0, side_order="auto"):
+    def __init__(self, models, precision="mixed", form="cta", threads=0, device=0, budget_bytes=0, side_order="auto",
+                 cta_state="auto"):
         if not isinstance(models, (list, tuple)):
             models = [models]
         self.models = list(models)
@@ -71,6 +72,7 @@ class GpuSolver:
         opts.form = _lib.FORMS[form] if isinstance(form, str) else int(form)
         opts.threads, opts.device, opts.budget_bytes = int(threads), int(device), int(budget_bytes)
         opts.side_order = {"auto": 0, "general": 1}[side_order]
+        opts.cta_state = {"auto": 0, "global": 1}[cta_state]
         self.precision, self.form = precision, form
         h = C.c_void_p()
         check(lib().ws_create(arr, self.B, C.byref(opts), C.byref(h)), "ws_create")
@@ -149,6 +151,11 @@ class GpuSolver:
     @property
     def stream(self):
         return lib().ws_stream(self.h)
+
+    @property
+    def resident(self):
+        """True when the batched form holds its instances in shared memory"""
+        return bool(lib().ws_cta_resident(self.h))
 
     @property
     def side_order(self):

@@ -7,6 +7,7 @@
 * ``batch`` — 512 independent gridshells drawn from a seed (laths per family U{6..40}, span U(2, 12) m, thickness
   U(3, 6) mm, width U(30, 60) mm, E U(8, 14) GPa, μ U(0.1, 0.5), inward displacement U(3, 10) % of the span, ~5 cm
   segments), one thread block each, relaxed together to the iteration cap.
+* ``ratio`` — the batched form (592 domes) against the plain single-instance form on the 3 m dome.
 * ``serve`` — the serving loop under Poisson arrivals at the given rates: fresh stiff domes (new seed each) and, with
   probability 0.3, variants (±5 % E, ±0.1 μ, ±2 % support displacement) of a resident equilibrium, warm-started.
 
@@ -50,27 +51,61 @@ def _compare(a, b, models):
             "slip_state_mismatch_total": int(np.sum(state)), "stick_mismatch_total": int(np.sum(stuck))}
 
 
-def run_precision(instances=64, iters=CAP, seed0=1):
+def run_precision(instances=64, iters=CAP, seed0=1, horizons=(500, 1000, 2000, 3000, 5000)):
+    """FP64, FP64 started 1 nm away (the chaos floor), mixed and naive FP32 stepped side by side; at every horizon the
+    three are compared with FP64"""
     models = [_stiff(seed0 + b) for b in range(instances)]
     _relax(models[:2], "mixed", 20)                       # module load and first-launch costs out of the timings
-    out = {"instances": instances, "iterations": iters, "nodes": models[0].n, "crossings": models[0].K}
-    ref, ctl64, ms64, _ = _relax(models, "f64", iters)
     rng = np.random.default_rng(7)
     pert = []
     for m in models:
         p = m.copy()
         p.X = p.X + 1e-9 * rng.standard_normal(p.X.shape)
         pert.append(p)
-    floor, _, _, _ = _relax(pert, "f64", iters)
-    out["f64"] = {"gpu_ms": ms64, "inst_iters_per_s": sum(c["iter"] for c in ctl64) / (ms64 * 1e-3),
-                  "converged": sum(c["status"] == 1 for c in ctl64)}
-    out["chaos_floor_f64_1nm"] = _compare(floor, ref, models)
-    for prec in ("mixed", "f32"):
-        st, ctl, ms, _ = _relax(models, prec, iters)
-        out[prec] = dict(_compare(st, ref, models), gpu_ms=ms, converged=sum(c["status"] == 1 for c in ctl),
-                         nonfinite=sum(c["status"] == 3 for c in ctl),
-                         inst_iters_per_s=sum(c["iter"] for c in ctl) / (ms * 1e-3))
+    runs = {"f64": GpuSolver([m.copy() for m in models], precision="f64", threads=512),
+            "chaos_floor_f64_1nm": GpuSolver(pert, precision="f64", threads=512),
+            "mixed": GpuSolver([m.copy() for m in models], precision="mixed", threads=512),
+            "f32": GpuSolver([m.copy() for m in models], precision="f32", threads=512)}
+    gpu_ms = {k: 0.0 for k in runs}
+    ctl = {}
+    out = {"instances": instances, "iterations": iters, "nodes": models[0].n, "crossings": models[0].K, "horizons": []}
+    done = 0
+    for h in [h for h in horizons if h <= iters]:
+        st = {}
+        for k, s in runs.items():
+            ctl[k] = s.step(h - done)
+            gpu_ms[k] += s.last_step_stats()[0]
+            st[k] = [s.download(b, fields=("X", "u", "state", "stuck")) for b in range(instances)]
+        done = h
+        row = {"iteration": h}
+        for k in ("chaos_floor_f64_1nm", "mixed", "f32"):
+            row[k] = _compare(st[k], st["f64"], models)
+        out["horizons"].append(row)
+    for k, s in runs.items():
+        out[k] = {"gpu_ms": gpu_ms[k], "inst_iters_per_s": sum(c["iter"] for c in ctl[k]) / (gpu_ms[k] * 1e-3),
+                  "converged": sum(c["status"] == 1 for c in ctl[k]), "nonfinite": sum(c["status"] == 3 for c in ctl[k])}
+        s.dispose()
     return out
+
+
+def run_ratio(batch=592, iters=400):
+    """the batched form against the plain single-instance GPU form on the 3 m dome (mixed precision)"""
+    models = [configs.dome_small(seed=1 + b) for b in range(batch)]
+    s = GpuSolver([models[0].copy()], precision="mixed", form="plain")
+    s.step(20)
+    s.step(iters, read=False)
+    ms_plain = s.last_step_stats()[0]
+    s.dispose()
+    s = GpuSolver(models, precision="mixed", threads=512)
+    s.step(10)
+    s.step(iters, read=False)
+    ms_batch = s.last_step_stats()[0]
+    s.dispose()
+    plain = iters / (ms_plain * 1e-3)
+    batched = batch * iters / (ms_batch * 1e-3)
+    return {"workload": "dome_small (1176 nodes, 156 crossings), mixed precision", "iterations": iters,
+            "plain_single_iters_per_s": plain, "batched_instances": batch, "batched_inst_iters_per_s": batched,
+            "batched_over_plain": batched / plain}
 
 
 def run_batch(count=512, iters=CAP, precision="mixed", threads=512, seed=4):
