@@ -57,7 +57,7 @@ void layout(Dev<P> &d, Carver &cv, const Sizes &z) {
   d.Wr = cv.take<R>(3 * m);
   d.segI0 = cv.take<int>(m); d.segI1 = cv.take<int>(m); d.jA = cv.take<int>(m); d.jB = cv.take<int>(m);
   d.cl0 = cv.take<int>(m); d.cl1 = cv.take<int>(m); d.segStrand = cv.take<int>(m); d.segLocal = cv.take<int>(m);
-  d.l0 = cv.take<R>(m); d.EA = cv.take<R>(m); d.GA = cv.take<R>(m); d.krs = cv.take<R>(3 * m);
+  d.l0 = cv.take<R>(m); d.il0 = cv.take<W>(m); d.EA = cv.take<R>(m); d.GA = cv.take<R>(m); d.krs = cv.take<R>(3 * m);
   d.nF = cv.take<R>(3 * m); d.en = cv.take<R>(3 * m); d.Nax = cv.take<R>(m); d.Vsh = cv.take<R>(2 * m);
   d.rngLo = cv.take<int>(2 * m); d.rngHi = cv.take<int>(2 * m);
   d.jS0 = cv.take<int>(p); d.jS1 = cv.take<int>(p); d.jLen = cv.take<R>(p); d.EIx = cv.take<R>(p); d.EIy = cv.take<R>(p);
@@ -367,7 +367,7 @@ void uploadState(ws_ctx *c, int b, int buf, bool withU) {
 template <int P>
 void uploadStatic(ws_ctx *c, int b) {
   Dev<P> &d = devOf<P>(c);
-  using R = typename Dev<P>::R;
+  using R = typename Dev<P>::R; using W = typename Dev<P>::W;
   const HostGoals &g = c->g[b];
   const InstDesc &I = c->inst[b];
   cudaStream_t st = c->st;
@@ -382,6 +382,11 @@ void uploadStatic(ws_ctx *c, int b) {
   put<int>(d.segStrand + I.m0, shift(g.segStrand, I.s0).data(), m, st);
   put<int>(d.segLocal + I.m0, g.segLocal.data(), m, st);
   put<R>(d.l0 + I.m0, g.l0.data(), m, st);
+  {
+    std::vector<double> il(m);
+    for (size_t j = 0; j < m; j++) il[j] = 1.0 / g.l0[j];
+    put<W>(d.il0 + I.m0, il.data(), m, st);
+  }
   put<int>(d.jS0 + I.p0, shift(g.jSeg0, I.m0).data(), p, st);
   put<int>(d.jS1 + I.p0, shift(g.jSeg1, I.m0).data(), p, st);
   put<R>(d.jLen + I.p0, g.jLen.data(), p, st);

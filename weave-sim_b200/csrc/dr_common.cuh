@@ -69,6 +69,7 @@ struct Dev {
   R *Wr;           // [3][mtot]
   int *segI0, *segI1, *jA, *jB, *cl0, *cl1, *segStrand, *segLocal;
   R *l0, *EA, *GA, *krs;    // krs [3][mtot]
+  W *il0;                   // 1 / l0 in the wide type (the mixed policy's strain)
   R *nF, *en;      // [3][mtot] segment force n and e × n
   R *Nax, *Vsh;    // [mtot], [2][mtot]
   int *rngLo, *rngHi;       // [2][mtot]

@@ -69,6 +69,71 @@ __device__ __forceinline__ void phaseD(const Dev<P> &d, const InstDesc &I, const
   else segUpdate<P, SHORT>(d, I, sx, I.m0 + (e - I.n), pt);
 }
 
+// ------------------------------------------------------------------------------------------------ balanced warps
+// Inside one block, a phase's elements are split over the warps by cost: the elements come in runs of one kind
+// (crossings, side ranks, segments, ...), each run cut into chunks of 32 (one element a lane, so a chunk never mixes
+// kinds), and warp w takes the chunks whose cost midpoint falls in its equal share of the phase's total cost.  Every
+// warp's range is contiguous.  The split is a function of the element counts and the block size only, so the
+// per-thread partial sums, and with them every reduction, are the same from run to run.  Relative costs are rough
+// instruction counts of one element.
+struct PhaseRun { int count, cost; };
+enum { COST_CROSSING = 40, COST_RANK = 3, COST_SEGMENT = 5, COST_JOINT = 8, COST_CLAMP = 8, COST_NODE_UPD = 3,
+       COST_SEG_UPD = 5, COST_SLICE = 3 };
+
+// chunks i in [0, nc) of a run starting at cumulative cost cb whose midpoint, doubled and scaled by the warp count,
+// nw·(2·cb + (2i + 1)·cost), lies below x
+__device__ __forceinline__ int chunksBelow(long long x, long long cb, int cost, int nw, int nc) {
+  const long long num = x - 2LL * nw * cb - (long long)nw * cost;
+  if (num <= 0) return 0;
+  const long long den = 2LL * nw * cost;
+  const long long c = (num + den - 1) / den;
+  return int(c < nc ? c : nc);
+}
+template <int NR, class F>
+__device__ __forceinline__ void forBalanced(const PhaseRun (&runs)[NR], F &&f) {
+  const int nw = blockDim.x >> 5, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  long long total = 0;
+  for (int r = 0; r < NR; r++) total += (long long)((runs[r].count + 31) >> 5) * runs[r].cost;
+  long long cb = 0;
+  for (int r = 0; r < NR; r++) {
+    const int nc = (runs[r].count + 31) >> 5, cost = runs[r].cost;
+    if (nc > 0) {
+      const int i0 = chunksBelow(2LL * w * total, cb, cost, nw, nc), i1 = chunksBelow(2LL * (w + 1) * total, cb, cost, nw, nc);
+      for (int i = i0; i < i1; i++) {
+        const int e = i * 32 + lane;
+        if (e < runs[r].count) f(r, e);
+      }
+    }
+    cb += (long long)nc * cost;
+  }
+}
+
+// phase A of one instance over the block: crossings, side ranks (short order), segments, joints, clamps
+template <int P, bool SHORT>
+__device__ __forceinline__ void blockPhaseA(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, Part<typename Dev<P>::A> &pt) {
+  const int nK = (I.contacts && I.K) ? I.K : 0;
+  const PhaseRun runs[5] = {{nK, COST_CROSSING}, {SHORT ? 2 * nK : 0, COST_RANK}, {I.m, COST_SEGMENT}, {I.p, COST_JOINT},
+                            {I.C, COST_CLAMP}};
+  forBalanced(runs, [&](int r, int e) {
+    switch (r) {
+      case 0: crossing<P>(d, I, sx.cur, sx.iter, sx.onxt, I.k0 + e, pt); break;
+      case 1: rankSideShort<P>(d, 2 * I.k0 + e, sx.obuf); break;
+      case 2: segForce<P>(d, sx.cur, I.m0 + e, pt); break;
+      case 3: jointTorque<P>(d, sx.cur, I.p0 + e, pt); break;
+      default: clampTorque<P>(d, sx.cur, I.c0 + e, pt); break;
+    }
+  });
+}
+// phase B / C (general order) of one instance over the block
+template <int P>
+__device__ __forceinline__ void blockPhaseBC(const Dev<P> &d, const InstDesc &I, const StepCtx &sx) {
+  const PhaseRun runs[2] = {{2 * I.K, COST_RANK}, {I.m, COST_SLICE}};
+  forBalanced(runs, [&](int r, int e) {
+    if (r == 0) rankSide<P>(d, 2 * I.k0 + e, sx.onxt, sx.onxt);
+    else segCount<P>(d, I.m0 + e, sx.onxt, sx.onxt);
+  });
+}
+
 // ------------------------------------------------------------------------------------------------ batched form
 // Block b relaxes instance order[b] (and further instances grid-strided) for up to nIter iterations, stopping at its
 // own convergence.  Instance state lives in HBM / L2; the block's barriers separate the phases, so an instance never
@@ -87,19 +152,24 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
     __syncthreads();
     const InstDesc &I = si;
     const bool cx = I.contacts && I.K;
-    const int nA = countA<SHORT>(I);
     for (int it = 0; it < nIter; it++) {
       if (sc.status != WS_RUNNING) break;
       const StepCtx sx = makeCtx<A>(I, sc);
       Part<A> pt;
       pt.init();
-      for (int e = threadIdx.x; e < nA; e += blockDim.x) phaseA<P, SHORT>(d, I, sx, e, cx ? I.K : 0, pt);
+      blockPhaseA<P, SHORT>(d, I, sx, pt);
       __syncthreads();
       if (!SHORT && cx) {
-        for (int e = threadIdx.x; e < 2 * I.K + I.m; e += blockDim.x) phaseBC<P>(d, I, sx, e);
+        blockPhaseBC<P>(d, I, sx);
         __syncthreads();
       }
-      for (int e = threadIdx.x; e < I.n + I.m; e += blockDim.x) phaseD<P, SHORT>(d, I, sx, e, pt);
+      {
+        const PhaseRun runs[2] = {{I.n, COST_NODE_UPD}, {I.m, COST_SEG_UPD}};
+        forBalanced(runs, [&](int r, int e) {
+          if (r == 0) nodeUpdate<P, SHORT>(d, I, sx, I.n0 + e, pt);
+          else segUpdate<P, SHORT>(d, I, sx, I.m0 + e, pt);
+        });
+      }
       __syncthreads();
       blockReduce(pt, red);
       if (threadIdx.x == 0) decide(I, sc, pt, nIter);
@@ -248,39 +318,35 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
     residentLoad<P, SHORT>(d, v, I, sc, sc.cur);
     __syncthreads();
     const bool cx = I.contacts && I.K;
-    const int nA = countA<SHORT>(I);
     for (int it = 0; it < nIter; it++) {
       if (sc.status != WS_RUNNING) break;
       StepCtx sx = makeCtx<A>(I, sc);
       sx.cur = sx.nxt = 0;              // in place
       Part<A> pt;
       pt.init();
-      for (int e = threadIdx.x; e < nA; e += blockDim.x) phaseA<P, SHORT>(v, I, sx, e, cx ? I.K : 0, pt);
+      blockPhaseA<P, SHORT>(v, I, sx, pt);
       __syncthreads();
       if (!SHORT && cx) {
-        for (int e = threadIdx.x; e < 2 * I.K + I.m; e += blockDim.x) phaseBC<P>(v, I, sx, e);
+        blockPhaseBC<P>(v, I, sx);
         __syncthreads();
       }
-      if (I.localLoads) {               // node-frame loads read the frames before the segments update them
-        for (int e = threadIdx.x; e < I.n; e += blockDim.x) {
+      auto upd = [&](int r, int e) {
+        if (r == 0) {
           if (I.kd) backupNode<P>(d, v, bk, I.n0 + e, false);
           nodeUpdate<P, SHORT>(v, I, sx, I.n0 + e, pt);
-        }
-        __syncthreads();
-        for (int e = threadIdx.x; e < I.m; e += blockDim.x) {
+        } else {
           if (I.kd) backupSeg<P>(d, v, bk, I.m0 + e, false);
           segUpdate<P, SHORT>(v, I, sx, I.m0 + e, pt);
         }
+      };
+      if (I.localLoads) {               // node-frame loads read the frames before the segments update them
+        const PhaseRun nodes[2] = {{I.n, COST_NODE_UPD}, {0, COST_SEG_UPD}}, segs[2] = {{0, COST_NODE_UPD}, {I.m, COST_SEG_UPD}};
+        forBalanced(nodes, upd);
+        __syncthreads();
+        forBalanced(segs, upd);
       } else {
-        for (int e = threadIdx.x; e < I.n + I.m; e += blockDim.x) {
-          if (e < I.n) {
-            if (I.kd) backupNode<P>(d, v, bk, I.n0 + e, false);
-            nodeUpdate<P, SHORT>(v, I, sx, I.n0 + e, pt);
-          } else {
-            if (I.kd) backupSeg<P>(d, v, bk, I.m0 + (e - I.n), false);
-            segUpdate<P, SHORT>(v, I, sx, I.m0 + (e - I.n), pt);
-          }
-        }
+        const PhaseRun runs[2] = {{I.n, COST_NODE_UPD}, {I.m, COST_SEG_UPD}};
+        forBalanced(runs, upd);
       }
       __syncthreads();
       blockReduce(pt, red);

@@ -42,13 +42,28 @@ template <class T> __device__ __forceinline__ T mmax(T a, T b) { return a > b ? 
 template <class T> __device__ __forceinline__ T mabs(T a) { return a < T(0) ? -a : a; }
 template <class T> __device__ __forceinline__ T mclamp(T v, T lo, T hi) { return mmin(mmax(v, lo), hi); }
 
-// frame [X | Y | Z] of a quaternion (normalised first): quat.js:19-27
+// Scale that takes a near-unit quaternion of squared norm n2 = 1 + δ to unit length: 1/√(1 + δ) = 1 − δ/2 + 3δ²/8
+// + O(δ³), the binomial series.  Used on frames stored as two floats and renormalised every iteration (|δ| below
+// ~1e-7), where the remainder is under the double rounding of the result; the exact form is kept everywhere else.
 template <class T>
+__device__ __forceinline__ T nearUnitScale(T n2) {
+  const T dl = n2 - T(1);
+  return T(1) + dl * (T(-0.5) + T(0.375) * dl);
+}
+
+// frame [X | Y | Z] of a quaternion (normalised first): quat.js:19-27; NU: q is near unit (see nearUnitScale)
+template <class T, bool NU = false>
 __device__ __forceinline__ void qframe(const T q[4], T R[9]) {
   T w = q[0], x = q[1], y = q[2], z = q[3];
-  T n = msqrt(w * w + x * x + y * y + z * z);
-  if (n == T(0)) n = T(1);
-  const T in = T(1) / n;
+  const T n2 = w * w + x * x + y * y + z * z;
+  T in;
+  if constexpr (NU) {
+    in = nearUnitScale(n2);
+  } else {
+    T n = msqrt(n2);
+    if (n == T(0)) n = T(1);
+    in = T(1) / n;
+  }
   w *= in; x *= in; y *= in; z *= in;
   R[0] = T(1) - T(2) * (y * y + z * z); R[1] = T(2) * (x * y + z * w); R[2] = T(2) * (x * z - y * w);
   R[3] = T(2) * (x * y - z * w); R[4] = T(1) - T(2) * (x * x + z * z); R[5] = T(2) * (y * z + x * w);
@@ -61,11 +76,17 @@ __device__ __forceinline__ void qmul(const T a[4], const T b[4], T o[4]) {
   o[2] = a[0] * b[2] - a[1] * b[3] + a[2] * b[0] + a[3] * b[1];
   o[3] = a[0] * b[3] + a[1] * b[2] - a[2] * b[1] + a[3] * b[0];
 }
-template <class T>
+template <class T, bool NU = false>
 __device__ __forceinline__ void qnormalize(T q[4]) {
-  T n = msqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
-  if (n == T(0)) n = T(1);
-  q[0] /= n; q[1] /= n; q[2] /= n; q[3] /= n;
+  const T n2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+  if constexpr (NU) {
+    const T f = nearUnitScale(n2);
+    q[0] *= f; q[1] *= f; q[2] *= f; q[3] *= f;
+  } else {
+    T n = msqrt(n2);
+    if (n == T(0)) n = T(1);
+    q[0] /= n; q[1] /= n; q[2] /= n; q[3] /= n;
+  }
 }
 template <class T>
 __device__ __forceinline__ void cross3(const T a[3], const T b[3], T o[3]) {
@@ -173,11 +194,20 @@ __device__ __forceinline__ void segForce(const Dev<P> &d, int buf, int j, Part<t
   W ew[3], qw[4], Rw[9];
   for (int k = 0; k < 3; k++) ew[k] = Acc<P>::xw(d, buf, k, b) - Acc<P>::xw(d, buf, k, a);
   for (int k = 0; k < 4; k++) qw[k] = Acc<P>::qw(d, buf, k, j);
-  qframe(qw, Rw);
-  const W l0 = W(d.l0[j]);
-  const R s1 = R((Rw[0] * ew[0] + Rw[1] * ew[1] + Rw[2] * ew[2]) / l0);
-  const R s2 = R((Rw[3] * ew[0] + Rw[4] * ew[1] + Rw[5] * ew[2]) / l0);
-  const R s3 = R((Rw[6] * ew[0] + Rw[7] * ew[1] + Rw[8] * ew[2]) / l0 - W(1));
+  R s1, s2, s3;
+  if constexpr (P == PREC_MIXED) {      // two-float frames are near unit; the inverse rest length is kept in f64
+    qframe<W, true>(qw, Rw);
+    const W il = d.il0[j];
+    s1 = R((Rw[0] * ew[0] + Rw[1] * ew[1] + Rw[2] * ew[2]) * il);
+    s2 = R((Rw[3] * ew[0] + Rw[4] * ew[1] + Rw[5] * ew[2]) * il);
+    s3 = R((Rw[6] * ew[0] + Rw[7] * ew[1] + Rw[8] * ew[2]) * il - W(1));
+  } else {
+    qframe(qw, Rw);
+    const W l0 = W(d.l0[j]);
+    s1 = R((Rw[0] * ew[0] + Rw[1] * ew[1] + Rw[2] * ew[2]) / l0);
+    s2 = R((Rw[3] * ew[0] + Rw[4] * ew[1] + Rw[5] * ew[2]) / l0);
+    s3 = R((Rw[6] * ew[0] + Rw[7] * ew[1] + Rw[8] * ew[2]) / l0 - W(1));
+  }
   const R GA = d.GA[j], EA = d.EA[j];
   const R n1 = GA * s1, n2 = GA * s2, n3 = EA * s3;
   R Rr[9];
@@ -612,7 +642,7 @@ __device__ __forceinline__ void segUpdate(const Dev<P> &d, const InstDesc &I, co
     qmul(q, dm1, inc);
     for (int k = 0; k < 4; k++) qn[k] = Acc<P>::qw(d, sc.cur, k, j) + W(inc[k]);
   }
-  qnormalize(qn);
+  qnormalize<W, P == PREC_MIXED>(qn);
   for (int k = 0; k < 4; k++) Acc<P>::qs(d, sc.nxt, k, j, qn[k]);
   pt.s[RS_KE] += A(I3[0]) * A(w[0]) * A(w[0]) + A(I3[1]) * A(w[1]) * A(w[1]) + A(I3[2]) * A(w[2]) * A(w[2]);
 }
