@@ -68,7 +68,8 @@ void layout(Dev<P> &d, Carver &cv, const Sizes &z) {
   d.cw = cv.take<R>(k); d.ch = cv.take<R>(k); d.mu = cv.take<R>(k); d.cflag = cv.take<uint8_t>(k);
   d.u = cv.take<U>(2 * k); d.nPrev = cv.take<R>(3 * k); d.slip = cv.take<A>(k); d.stuck = cv.take<uint8_t>(k);
   d.cstate = cv.take<uint8_t>(k); d.Fn = cv.take<R>(k); d.Ft = cv.take<R>(k); d.gap = cv.take<R>(k);
-  d.sPos = cv.take<int>(2 * k); d.sKey = cv.take<int>(4 * k); d.sStrand = cv.take<int>(2 * k); d.sT = cv.take<R>(2 * k);
+  d.sPos = cv.take<int>(2 * k); d.sKey = cv.take<int>(4 * k); d.sInv = cv.take<int>(4 * k); d.sKeyS = cv.take<int>(2 * k);
+  d.sStrand = cv.take<int>(2 * k); d.sT = cv.take<R>(2 * k);
   d.kth = cv.take<R>(2 * k); d.sF = cv.take<R>(6 * k); d.sTq = cv.take<R>(6 * k);
   d.stSideOff = cv.take<int>(s); d.stSideCnt = cv.take<int>(s); d.stSegOff = cv.take<int>(s);
   d.ord = cv.take<int>(4 * k); d.ordSeg = cv.take<int>(4 * k);
@@ -127,7 +128,8 @@ struct ws_ctx {
   size_t residentBytes = 0;      // batched form: dynamic shared memory of the resident form (0: global state)
   bool shortSides = false;       // the short-slide side order is in use
   cudaGraphExec_t graph = nullptr;
-  int graphIters = 0, graphKey = -1;
+  int graphIters = 0, graphKey = -1, graphLaunches = 0;
+  PlainFork fork{};              // plain form: the crossing kernel's stream and the fork / join events
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double lastMs = 0;
   int64_t lastLaunches = 0;
@@ -311,12 +313,14 @@ void uploadOrder(ws_ctx *c, int b, int buf) {
   const HostGoals &g = c->g[b];
   const InstDesc &I = c->inst[b];
   const size_t K2 = 2 * size_t(d.ktot), K = g.K, m = g.m;
-  std::vector<int> ord(2 * K), lo(m), hi(m), key(2 * K);
+  std::vector<int> ord(2 * K), lo(m), hi(m), key(2 * K), inv(2 * K);
   for (size_t q = 0; q < 2 * K; q++) ord[q] = 2 * I.k0 + g.sidePos[g.ord[q]];
+  for (size_t q = 0; q < 2 * K; q++) inv[g.sidePos[g.ord[q]]] = 2 * I.k0 + int(q);
   for (size_t q = 0; q < 2 * K; q++) key[q] = g.sideSegLocal(g.sideList[q]);
   for (size_t j = 0; j < m; j++) { lo[j] = 2 * I.k0 + g.rngLo[j]; hi[j] = 2 * I.k0 + g.rngHi[j]; }
   put<int>(d.sKey + buf * K2 + 2 * size_t(I.k0), key.data(), 2 * K, c->st);
   put<int>(d.ord + buf * K2 + 2 * size_t(I.k0), ord.data(), 2 * K, c->st);
+  put<int>(d.sInv + buf * K2 + 2 * size_t(I.k0), inv.data(), 2 * K, c->st);
   put<int>(d.ordSeg + buf * K2 + 2 * size_t(I.k0), g.ordSeg.data(), 2 * K, c->st);
   put<int>(d.rngLo + size_t(buf) * d.mtot + I.m0, lo.data(), m, c->st);
   put<int>(d.rngHi + size_t(buf) * d.mtot + I.m0, hi.data(), m, c->st);
@@ -467,6 +471,11 @@ void fillControl(const InstCtl &s, ws_control *o) {
   o->e_stretch = s.e_stretch; o->e_shear = s.e_shear; o->e_bend = s.e_bend; o->e_twist = s.e_twist; o->e_contact = s.e_contact;
 }
 
+#ifndef WSB_PLAIN_FORK
+#define WSB_PLAIN_FORK 1     // the plain form's element phase as two kernels on forked branches (0: one kernel)
+#endif
+const PlainFork *plainFork(const ws_ctx *c) { return (WSB_PLAIN_FORK && c->fork.side) ? &c->fork : nullptr; }
+
 template <int P>
 void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
   const int nInst = int(c->inst.size());
@@ -500,18 +509,20 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
       cudaGraph_t gr;
       CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
       int nl = 0;
-      for (int i = 0; i < chunk; i++) CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, c->st, &nl, c->dBar + 2));
+      for (int i = 0; i < chunk; i++)
+        CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, c->st, &nl, c->dBar + 2, plainFork(c)));
       CK(cudaStreamEndCapture(c->st, &gr));
       CK(cudaGraphInstantiate(&c->graph, gr, 0));
       cudaGraphDestroy(gr);
       c->graphIters = chunk;
       c->graphKey = key;
+      c->graphLaunches = nl;
     }
     int done = 0;
-    const int per = (cx && !sh) ? 3 : 2;
-    while (nIter - done >= chunk && chunk > 0) { CK(cudaGraphLaunch(c->graph, c->st)); done += chunk; c->lastLaunches += int64_t(chunk) * per; }
+    while (nIter - done >= chunk && chunk > 0) { CK(cudaGraphLaunch(c->graph, c->st)); done += chunk; c->lastLaunches += c->graphLaunches; }
     int nl = 0;
-    for (; done < nIter; done++) CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, c->st, &nl, c->dBar + 2));
+    for (; done < nIter; done++)
+      CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, c->st, &nl, c->dBar + 2, plainFork(c)));
     c->lastLaunches += nl;
   }
   CK(cudaEventRecord(c->ev1, c->st));
@@ -714,6 +725,9 @@ void destroyCtx(ws_ctx *c) {
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->st) cudaStreamDestroy(c->st);
+  if (c->fork.side) cudaStreamDestroy(c->fork.side);
+  if (c->fork.fork) cudaEventDestroy(c->fork.fork);
+  if (c->fork.join) cudaEventDestroy(c->fork.join);
   if (c->pinned) cudaFreeHost(c->pinned);
   delete c;
 }
@@ -746,6 +760,11 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
   int rc = guarded("ws_create", [&]() {
     CK(cudaSetDevice(o.device));
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    if (o.form == WS_FORM_PLAIN) {
+      CK(cudaStreamCreateWithFlags(&c->fork.side, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&c->fork.fork, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&c->fork.join, cudaEventDisableTiming));
+    }
     c->pinnedOK = true;
     CK(cudaEventCreate(&c->ev0));
     CK(cudaEventCreate(&c->ev1));
@@ -774,7 +793,9 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     const InstDesc &I0 = c->inst[0];
     auto blocks = [](long long cnt, int thr) { return int(std::max<long long>(1, std::min<long long>((cnt + thr - 1) / thr, 148LL * 8))); };
     c->shape.blocksA = blocks(I0.m + I0.p + I0.C + I0.K, 256);
-    c->shape.blocksAS = blocks(I0.m + I0.p + I0.C + 3LL * I0.K, 256);
+    c->shape.blocksDS = blocks(I0.n + I0.m + 2LL * I0.K, 256);
+    c->shape.blocksX = blocks(I0.K, 128);
+    c->shape.blocksY = blocks(I0.m + I0.p + I0.C, 256);
     c->shape.blocksR = blocks(I0.m + 2LL * I0.K, 256);
     c->shape.blocksD = blocks(I0.n + I0.m, 256);
     for (int sh = 0; sh < 2; sh++) {
@@ -785,7 +806,9 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
       }
     }
     CK(cudaGetLastError());
-    const int parts = std::max({c->shape.blocksAS + c->shape.blocksD, c->shape.blocksA + c->shape.blocksD, c->gridBlocks[0], c->gridBlocks[1]});
+    const int parts = std::max({c->shape.blocksA + c->shape.blocksDS, c->shape.blocksA + c->shape.blocksD,
+                                c->shape.blocksX + c->shape.blocksY + std::max(c->shape.blocksD, c->shape.blocksDS), c->gridBlocks[0],
+                                c->gridBlocks[1]});
     CK(cudaMalloc(&c->dPart, sizeof(double) * (RS_NSUM + RX_NMAX) * size_t(parts)));
     CK(cudaMalloc(&c->dBar, 4 * sizeof(unsigned)));     // [0..1] grid barrier, [2] plain form's finishing-block counter
     CK(cudaMemsetAsync(c->dBar, 0, 4 * sizeof(unsigned), c->st));

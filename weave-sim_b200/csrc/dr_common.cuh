@@ -96,9 +96,12 @@ struct Dev {
   // strand (the strand's range is [stSideOff, stSideOff + stSideCnt))
   int *sPos;                // [2 ktot] position of side sd
   int *sKey;                // [2][2 ktot] local segment of the side after the slide, by sorted-side buffer
+  int *sInv;                // [2][2 ktot] short order: the side's position in the sorted order of that buffer
+  int *sKeyS;               // [2 ktot] short order: the key after the slide, at the side's sorted position
   int *sStrand;             // [2 ktot] strand of the side
   R *sT, *kth;              // [2 ktot] Hermite parameter before the slide; righting stiffness of the side's crossing
   R *sF, *sTq;              // [3][2 ktot] force on the side; lever torque
+                            // (side records: at the strand position, or with the short order at the sorted position)
   // strands
   int *stSideOff, *stSideCnt;   // [stot]
   int *stSegOff;                // [stot] first (global) segment of the strand
@@ -107,10 +110,11 @@ struct Dev {
 
 // Shared-memory layout of one instance in the resident form: byte offsets of the arrays that change every iteration
 // (one buffer of positions and frames, updated in place), from the instance's element counts.  The host sizes the
-// launch with the same function.  The side order keeps one buffer of the order and slices in the short-slide variant,
-// two in the general one.
+// launch with the same function.  The side order keeps two buffers (this iteration's and the next's); the short-slide
+// variant keeps sorted positions and the keys at them, the general one the sorted list of side positions.
 struct ResLayout {
-  unsigned X, Xlo, V, Q, Qlo, Wr, nF, en, tau, kd, tauC, u, nPrev, sKey, sT, kth, sF, sTq, ord, ordSeg, rngLo, rngHi, bytes;
+  unsigned X, Xlo, V, Q, Qlo, Wr, nF, en, tau, kd, tauC, u, nPrev, sKey, sInv, sKeyS, sT, kth, sF, sTq, ord, ordSeg, rngLo,
+      rngHi, bytes;
 };
 __host__ __device__ inline unsigned resTake(unsigned &o, size_t bytes) {
   const unsigned r = o;
@@ -121,7 +125,7 @@ template <int P>
 __host__ __device__ inline ResLayout residentLayout(int n, int m, int p, int C, int K, bool shortSides) {
   using R = typename PrecT<P>::R; using S = typename PrecT<P>::S; using U = typename PrecT<P>::U;
   const bool two = PrecT<P>::TWO;
-  const size_t N = n, M = m, J = p, CC = C, K2 = 2 * size_t(K), nb = shortSides ? 1 : 2;
+  const size_t N = n, M = m, J = p, CC = C, K2 = 2 * size_t(K);
   ResLayout L{};
   unsigned o = 0;
   L.X = resTake(o, 3 * N * sizeof(S)); L.Xlo = two ? resTake(o, 3 * N * sizeof(S)) : 0; L.V = resTake(o, 3 * N * sizeof(R));
@@ -129,10 +133,12 @@ __host__ __device__ inline ResLayout residentLayout(int n, int m, int p, int C, 
   L.nF = resTake(o, 3 * M * sizeof(R)); L.en = resTake(o, 3 * M * sizeof(R));
   L.tau = resTake(o, 3 * J * sizeof(R)); L.kd = resTake(o, 3 * J * sizeof(R)); L.tauC = resTake(o, 3 * CC * sizeof(R));
   L.u = resTake(o, K2 * sizeof(U)); L.nPrev = resTake(o, 3 * size_t(K) * sizeof(R));
-  L.sKey = resTake(o, 2 * K2 * sizeof(int)); L.sT = resTake(o, K2 * sizeof(R)); L.kth = resTake(o, K2 * sizeof(R));
+  L.sKey = resTake(o, 2 * K2 * sizeof(int));
+  L.sInv = resTake(o, (shortSides ? 2 : 0) * K2 * sizeof(int)); L.sKeyS = resTake(o, (shortSides ? 1 : 0) * K2 * sizeof(int));
+  L.sT = resTake(o, K2 * sizeof(R)); L.kth = resTake(o, K2 * sizeof(R));
   L.sF = resTake(o, 3 * K2 * sizeof(R)); L.sTq = resTake(o, 3 * K2 * sizeof(R));
-  L.ord = resTake(o, nb * K2 * sizeof(int)); L.ordSeg = resTake(o, nb * K2 * sizeof(int));
-  L.rngLo = resTake(o, nb * M * sizeof(int)); L.rngHi = resTake(o, nb * M * sizeof(int));
+  L.ord = resTake(o, (shortSides ? 0 : 2) * K2 * sizeof(int)); L.ordSeg = resTake(o, 2 * K2 * sizeof(int));
+  L.rngLo = resTake(o, 2 * M * sizeof(int)); L.rngHi = resTake(o, 2 * M * sizeof(int));
   L.bytes = o;
   return L;
 }

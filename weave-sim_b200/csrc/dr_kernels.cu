@@ -13,6 +13,9 @@
 #ifndef WSB_MINB_D
 #define WSB_MINB_D 4
 #endif
+#ifndef WSB_MINB_Y
+#define WSB_MINB_Y 2
+#endif
 #ifndef WSB_MINB_G
 #define WSB_MINB_G 2
 #endif
@@ -37,24 +40,23 @@ __device__ __forceinline__ void addPart(Part<A> &q, const A *part, int b, int st
   for (int i = 0; i < RX_NMAX; i++) q.x[i] = mmax(q.x[i], __ldcg(part + size_t(RS_NSUM + i) * stride + b));
 }
 
-// element e of phase A: the crossings come first (the heaviest elements start earliest); under SHORT the ranks of the
-// sides follow (the order this iteration's gathers read); then segments, joints, clamps
+// element e of phase A: the crossings come first (the heaviest elements start earliest), then segments, joints, clamps
 template <int P, bool SHORT>
 __device__ __forceinline__ void phaseA(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, int e, int nK, Part<typename Dev<P>::A> &pt) {
-  if (e < nK) { crossing<P>(d, I, sx.cur, sx.iter, sx.onxt, I.k0 + e, pt); return; }
+  if (e < nK) { crossing<P, SHORT>(d, I, sx.cur, sx.iter, sx.onxt, sx.obuf, I.k0 + e, pt); return; }
   e -= nK;
-  if constexpr (SHORT) {
-    if (e < 2 * nK) { rankSideShort<P>(d, 2 * I.k0 + e, sx.obuf); return; }
-    e -= 2 * nK;
-  }
   if (e < I.m) segForce<P>(d, sx.cur, I.m0 + e, pt);
   else if ((e -= I.m) < I.p) jointTorque<P>(d, sx.cur, I.p0 + e, pt);
   else clampTorque<P>(d, sx.cur, I.c0 + (e - I.p), pt);
 }
-template <bool SHORT>
 __device__ __forceinline__ int countA(const InstDesc &I) {
   const int nK = (I.contacts && I.K) ? I.K : 0;
-  return I.m + I.p + I.C + nK + (SHORT ? 2 * nK : 0);
+  return I.m + I.p + I.C + nK;
+}
+// elements of phase D: nodes, segments and, with the short order, the ranks of the sides (the next iteration's order)
+template <bool SHORT>
+__device__ __forceinline__ int countD(const InstDesc &I) {
+  return I.n + I.m + ((SHORT && I.contacts && I.K) ? 2 * I.K : 0);
 }
 // phase B / C of the general order: the ranks of the sides and the slices of the segments in the new order
 template <int P>
@@ -66,7 +68,8 @@ __device__ __forceinline__ void phaseBC(const Dev<P> &d, const InstDesc &I, cons
 template <int P, bool SHORT>
 __device__ __forceinline__ void phaseD(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, int e, Part<typename Dev<P>::A> &pt) {
   if (e < I.n) nodeUpdate<P, SHORT>(d, I, sx, I.n0 + e, pt);
-  else segUpdate<P, SHORT>(d, I, sx, I.m0 + (e - I.n), pt);
+  else if ((e -= I.n) < I.m) segUpdate<P, SHORT>(d, I, sx, I.m0 + e, pt);
+  else rankSideShort<P>(d, 2 * I.k0 + (e - I.m), sx.onxt);
 }
 
 // ------------------------------------------------------------------------------------------------ balanced warps
@@ -108,18 +111,16 @@ __device__ __forceinline__ void forBalanced(const PhaseRun (&runs)[NR], F &&f) {
   }
 }
 
-// phase A of one instance over the block: crossings, side ranks (short order), segments, joints, clamps
+// phase A of one instance over the block: crossings, segments, joints, clamps
 template <int P, bool SHORT>
 __device__ __forceinline__ void blockPhaseA(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, Part<typename Dev<P>::A> &pt) {
   const int nK = (I.contacts && I.K) ? I.K : 0;
-  const PhaseRun runs[5] = {{nK, COST_CROSSING}, {SHORT ? 2 * nK : 0, COST_RANK}, {I.m, COST_SEGMENT}, {I.p, COST_JOINT},
-                            {I.C, COST_CLAMP}};
+  const PhaseRun runs[4] = {{nK, COST_CROSSING}, {I.m, COST_SEGMENT}, {I.p, COST_JOINT}, {I.C, COST_CLAMP}};
   forBalanced(runs, [&](int r, int e) {
     switch (r) {
-      case 0: crossing<P>(d, I, sx.cur, sx.iter, sx.onxt, I.k0 + e, pt); break;
-      case 1: rankSideShort<P>(d, 2 * I.k0 + e, sx.obuf); break;
-      case 2: segForce<P>(d, sx.cur, I.m0 + e, pt); break;
-      case 3: jointTorque<P>(d, sx.cur, I.p0 + e, pt); break;
+      case 0: crossing<P, SHORT>(d, I, sx.cur, sx.iter, sx.onxt, sx.obuf, I.k0 + e, pt); break;
+      case 1: segForce<P>(d, sx.cur, I.m0 + e, pt); break;
+      case 2: jointTorque<P>(d, sx.cur, I.p0 + e, pt); break;
       default: clampTorque<P>(d, sx.cur, I.c0 + e, pt); break;
     }
   });
@@ -164,10 +165,11 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
         __syncthreads();
       }
       {
-        const PhaseRun runs[2] = {{I.n, COST_NODE_UPD}, {I.m, COST_SEG_UPD}};
+        const PhaseRun runs[3] = {{I.n, COST_NODE_UPD}, {I.m, COST_SEG_UPD}, {(SHORT && cx) ? 2 * I.K : 0, COST_RANK}};
         forBalanced(runs, [&](int r, int e) {
           if (r == 0) nodeUpdate<P, SHORT>(d, I, sx, I.n0 + e, pt);
-          else segUpdate<P, SHORT>(d, I, sx, I.m0 + e, pt);
+          else if (r == 1) segUpdate<P, SHORT>(d, I, sx, I.m0 + e, pt);
+          else rankSideShort<P>(d, 2 * I.k0 + e, sx.onxt);
         });
       }
       __syncthreads();
@@ -209,6 +211,8 @@ __device__ __forceinline__ Dev<P> residentView(const Dev<P> &d, const InstDesc &
   v.u = reinterpret_cast<U *>(sm + L.u) - I.k0;
   v.nPrev = reinterpret_cast<R *>(sm + L.nPrev) - I.k0;
   v.sKey = reinterpret_cast<int *>(sm + L.sKey) - k2;
+  v.sInv = reinterpret_cast<int *>(sm + L.sInv) - k2;
+  v.sKeyS = reinterpret_cast<int *>(sm + L.sKeyS) - k2;
   v.sT = reinterpret_cast<R *>(sm + L.sT) - k2;
   v.kth = reinterpret_cast<R *>(sm + L.kth) - k2;
   v.sF = reinterpret_cast<R *>(sm + L.sF) - k2;
@@ -218,9 +222,9 @@ __device__ __forceinline__ Dev<P> residentView(const Dev<P> &d, const InstDesc &
   v.rngLo = reinterpret_cast<int *>(sm + L.rngLo) - I.m0;
   v.rngHi = reinterpret_cast<int *>(sm + L.rngHi) - I.m0;
   v.nS = I.n; v.xB = 0; v.mS = I.m; v.qB = 0; v.pS = I.p; v.cS = I.C; v.kS = I.K;
-  v.sS = v.kB = 2 * I.K;
-  v.oB = shortSides ? 0 : 2 * I.K;
-  v.rB = shortSides ? 0 : I.m;
+  v.sS = v.kB = v.oB = 2 * I.K;
+  v.rB = I.m;
+  (void)shortSides;
   return v;
 }
 
@@ -246,16 +250,17 @@ __device__ void residentLoad(const Dev<P> &g, const Dev<P> &v, const InstDesc &I
   if (!I.K) return;
   copyPlanes(v.u, v.kS, g.u, g.kS, I.k0, I.K, 2);
   copyPlanes(v.nPrev, v.kS, g.nPrev, g.kS, I.k0, I.K, 3);
-  const int k2 = 2 * I.k0, K2 = 2 * I.K;
-  // the keys of the sides before the next slide; the order and slices the next iteration reads (or, short order,
-  // the slices an earlier iteration left: a valid base for the segments without sides)
-  copyPlanes(v.sKey + size_t(c.obuf) * v.kB, 0, g.sKey + size_t(c.obuf) * g.kB, 0, k2, K2, 1);
-  copyPlanes(v.rngLo + size_t(SHORT ? 0 : c.obuf) * v.rB, 0, g.rngLo + size_t(c.obuf) * g.rB, 0, I.m0, I.m, 1);
-  copyPlanes(v.rngHi + size_t(SHORT ? 0 : c.obuf) * v.rB, 0, g.rngHi + size_t(c.obuf) * g.rB, 0, I.m0, I.m, 1);
-  if constexpr (!SHORT) {
-    copyPlanes(v.ord + size_t(c.obuf) * v.oB, 0, g.ord + size_t(c.obuf) * g.oB, 0, k2, K2, 1);
-    copyPlanes(v.ordSeg + size_t(c.obuf) * v.oB, 0, g.ordSeg + size_t(c.obuf) * g.oB, 0, k2, K2, 1);
-  }
+  const int k2 = 2 * I.k0, K2 = 2 * I.K, ob = c.obuf;
+  // the side order the next iteration reads: keys at the sorted positions, the segments' slices (with the short order
+  // some slices are an earlier iteration's, which the keys mark), and the sorted positions (short) or the sorted list
+  // of side positions (general)
+  // both slice buffers: the short order rewrites only the slices of segments with sides, and the rest must stay the
+  // (valid, older) slices of the global buffers
+  copyPlanes(v.ordSeg + size_t(ob) * v.oB, 0, g.ordSeg + size_t(ob) * g.oB, 0, k2, K2, 1);
+  copyPlanes(v.rngLo, v.rB, g.rngLo, g.rB, I.m0, I.m, 2);
+  copyPlanes(v.rngHi, v.rB, g.rngHi, g.rB, I.m0, I.m, 2);
+  if constexpr (SHORT) copyPlanes(v.sInv + size_t(ob) * v.kB, 0, g.sInv + size_t(ob) * g.kB, 0, k2, K2, 1);
+  else copyPlanes(v.ord + size_t(ob) * v.oB, 0, g.ord + size_t(ob) * g.oB, 0, k2, K2, 1);
 }
 
 // shared -> global at the end of a launch, into the buffers the control block names
@@ -270,14 +275,12 @@ __device__ void residentStore(const Dev<P> &g, const Dev<P> &v, const InstDesc &
   if (!I.K) return;
   copyPlanes(g.u, g.kS, v.u, v.kS, I.k0, I.K, 2);
   copyPlanes(g.nPrev, g.kS, v.nPrev, v.kS, I.k0, I.K, 3);
-  const int k2 = 2 * I.k0, K2 = 2 * I.K;
-  copyPlanes(g.sKey + size_t(c.obuf) * g.kB, 0, v.sKey + size_t(c.obuf) * v.kB, 0, k2, K2, 1);
-  copyPlanes(g.rngLo + size_t(c.obuf) * g.rB, 0, v.rngLo + size_t(SHORT ? 0 : c.obuf) * v.rB, 0, I.m0, I.m, 1);
-  copyPlanes(g.rngHi + size_t(c.obuf) * g.rB, 0, v.rngHi + size_t(SHORT ? 0 : c.obuf) * v.rB, 0, I.m0, I.m, 1);
-  if constexpr (!SHORT) {
-    copyPlanes(g.ord + size_t(c.obuf) * g.oB, 0, v.ord + size_t(c.obuf) * v.oB, 0, k2, K2, 1);
-    copyPlanes(g.ordSeg + size_t(c.obuf) * g.oB, 0, v.ordSeg + size_t(c.obuf) * v.oB, 0, k2, K2, 1);
-  }
+  const int k2 = 2 * I.k0, K2 = 2 * I.K, ob = c.obuf;
+  copyPlanes(g.ordSeg + size_t(ob) * g.oB, 0, v.ordSeg + size_t(ob) * v.oB, 0, k2, K2, 1);
+  copyPlanes(g.rngLo, g.rB, v.rngLo, v.rB, I.m0, I.m, 2);
+  copyPlanes(g.rngHi, g.rB, v.rngHi, v.rB, I.m0, I.m, 2);
+  if constexpr (SHORT) copyPlanes(g.sInv + size_t(ob) * g.kB, 0, v.sInv + size_t(ob) * v.kB, 0, k2, K2, 1);
+  else copyPlanes(g.ord + size_t(ob) * g.oB, 0, v.ord + size_t(ob) * v.oB, 0, k2, K2, 1);
 }
 
 // positions / frames of node i or segment j between the shared view and global buffer bk (backup or restore)
@@ -334,18 +337,22 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
         if (r == 0) {
           if (I.kd) backupNode<P>(d, v, bk, I.n0 + e, false);
           nodeUpdate<P, SHORT>(v, I, sx, I.n0 + e, pt);
-        } else {
+        } else if (r == 1) {
           if (I.kd) backupSeg<P>(d, v, bk, I.m0 + e, false);
           segUpdate<P, SHORT>(v, I, sx, I.m0 + e, pt);
+        } else {
+          rankSideShort<P>(v, 2 * I.k0 + e, sx.onxt);
         }
       };
+      const int nR = (SHORT && cx) ? 2 * I.K : 0;
       if (I.localLoads) {               // node-frame loads read the frames before the segments update them
-        const PhaseRun nodes[2] = {{I.n, COST_NODE_UPD}, {0, COST_SEG_UPD}}, segs[2] = {{0, COST_NODE_UPD}, {I.m, COST_SEG_UPD}};
+        const PhaseRun nodes[3] = {{I.n, COST_NODE_UPD}, {0, COST_SEG_UPD}, {nR, COST_RANK}};
+        const PhaseRun segs[3] = {{0, COST_NODE_UPD}, {I.m, COST_SEG_UPD}, {0, COST_RANK}};
         forBalanced(nodes, upd);
         __syncthreads();
         forBalanced(segs, upd);
       } else {
-        const PhaseRun runs[2] = {{I.n, COST_NODE_UPD}, {I.m, COST_SEG_UPD}};
+        const PhaseRun runs[3] = {{I.n, COST_NODE_UPD}, {I.m, COST_SEG_UPD}, {nR, COST_RANK}};
         forBalanced(runs, upd);
       }
       __syncthreads();
@@ -369,24 +376,43 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
 // ------------------------------------------------------------------------------------------------ plain form
 // One kernel per phase over the elements of instance 0; block partials go to part[block] and the last block of the
 // update kernel reduces them in a fixed order.  Every kernel returns at once when the instance has stopped.
-template <int P, bool SHORT>
-__global__ void __launch_bounds__(256, WSB_MINB_A) k_plainA(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
-                                                typename Dev<P>::A *part, int partStride) {
+// The element phase, whole (PART 0) or split in two kernels that run side by side on forked branches of the graph:
+// the crossings (PART 1), whose long per-element code needs many registers, and the segments, joints and clamps
+// (PART 2), which then run at the occupancy of their own, smaller register budget.
+template <int P, bool SHORT, int PART>
+__device__ __forceinline__ void plainA(const Dev<P> &d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
+                                       typename Dev<P>::A *part, int partStride) {
   using A = typename Dev<P>::A;
   __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
-  waitPrevGrid();
-  allowNextGrid();
   const InstDesc &I = insts[0];
   const InstCtl c = ctl[0];
   if (c.status != WS_RUNNING) return;
-  const bool cx = I.contacts && I.K;
-  const int nA = countA<SHORT>(I);
+  const int nK = (I.contacts && I.K) ? I.K : 0;
+  const int nA = PART == 1 ? nK : PART == 2 ? I.m + I.p + I.C : countA(I);
+  const int base = PART == 2 ? nK : 0;
   const StepCtx sx = makeCtx<A>(I, c);
   Part<A> pt;
   pt.init();
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nA; e += gridDim.x * blockDim.x) phaseA<P, SHORT>(d, I, sx, e, cx ? I.K : 0, pt);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nA; e += gridDim.x * blockDim.x) phaseA<P, SHORT>(d, I, sx, base + e, nK, pt);
   blockReduce(pt, red);
   if (threadIdx.x == 0) putPart(pt, part, blockIdx.x, partStride);
+}
+template <int P, bool SHORT>
+__global__ void __launch_bounds__(256, WSB_MINB_A) k_plainA(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
+                                                typename Dev<P>::A *part, int partStride) {
+  waitPrevGrid();
+  allowNextGrid();
+  plainA<P, SHORT, 0>(d, insts, ctl, part, partStride);
+}
+template <int P, bool SHORT>
+__global__ void __launch_bounds__(128) k_plainX(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
+                                                typename Dev<P>::A *part, int partStride) {
+  plainA<P, SHORT, 1>(d, insts, ctl, part, partStride);
+}
+template <int P, bool SHORT>
+__global__ void __launch_bounds__(256, WSB_MINB_Y) k_plainY(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
+                                                typename Dev<P>::A *part, int partStride) {
+  plainA<P, SHORT, 2>(d, insts, ctl, part, partStride);
 }
 template <int P>
 __global__ void __launch_bounds__(256) k_plainBC(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl) {
@@ -416,7 +442,8 @@ __global__ void __launch_bounds__(256, WSB_MINB_D) k_plainD(Dev<P> d, const Inst
   const StepCtx sx = makeCtx<A>(I, c);
   Part<A> pt;
   pt.init();
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < I.n + I.m; e += gridDim.x * blockDim.x) phaseD<P, SHORT>(d, I, sx, e, pt);
+  const int nD = countD<SHORT>(I);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nD; e += gridDim.x * blockDim.x) phaseD<P, SHORT>(d, I, sx, e, pt);
   blockReduce(pt, red);
   if (threadIdx.x == 0) {
     putPart(pt, part, blockIdx.x, partStride);
@@ -478,7 +505,7 @@ __global__ void __launch_bounds__(256, WSB_MINB_G) k_grid(Dev<P> d, const InstDe
   __syncthreads();
   const InstDesc &I = si;
   const bool cx = I.contacts && I.K;
-  const int nA = countA<SHORT>(I);
+  const int nA = countA(I), nD = countD<SHORT>(I);
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
   const unsigned nb = gridDim.x;
   for (int it = 0; it < nIter; it++) {
@@ -492,7 +519,7 @@ __global__ void __launch_bounds__(256, WSB_MINB_G) k_grid(Dev<P> d, const InstDe
       for (int e = gt; e < 2 * I.K + I.m; e += gs) phaseBC<P>(d, I, sx, e);
       if (!gridSync(bar, nb, err)) break;
     }
-    for (int e = gt; e < I.n + I.m; e += gs) phaseD<P, SHORT>(d, I, sx, e, pt);
+    for (int e = gt; e < nD; e += gs) phaseD<P, SHORT>(d, I, sx, e, pt);
     blockReduce(pt, red);
     if (threadIdx.x == 0) putPart(pt, part, blockIdx.x, int(nb));
     if (!gridSync(bar, nb, err)) break;
@@ -558,12 +585,36 @@ static cudaError_t launchPDL(void (*k)(KArgs...), int blocks, cudaStream_t st, A
 
 template <int P>
 cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, const PlainShape &sh, bool contacts,
-                            bool shortSides, cudaStream_t st, int *launches, unsigned *counter) {
+                            bool shortSides, cudaStream_t st, int *launches, unsigned *counter, const PlainFork *fork) {
   using A = typename Dev<P>::A;
   const bool sh2 = shortSides && contacts;
-  const int nA = sh2 ? sh.blocksAS : sh.blocksA, nParts = nA + sh.blocksD;
-  A *pa = static_cast<A *>(part), *pd = pa + nA;      // value-major rows of nParts: A's blocks, then D's
-  cudaError_t e = sh2 ? launchPDL(k_plainA<P, true>, sh.blocksAS, st, d, insts, ctl, pa, nParts)
+  if (fork && contacts) {
+    // crossings on a forked branch, segments / joints / clamps on the main one, joined before the update
+    const int nD = sh2 ? sh.blocksDS : sh.blocksD, nParts = sh.blocksX + sh.blocksY + nD;
+    A *px = static_cast<A *>(part), *py = px + sh.blocksX, *pd = py + sh.blocksY;
+    cudaError_t e;
+    if ((e = cudaEventRecord(fork->fork, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(fork->side, fork->fork, 0)) != cudaSuccess) return e;
+    if (sh2) k_plainX<P, true><<<sh.blocksX, 128, 0, fork->side>>>(d, insts, ctl, px, nParts);
+    else k_plainX<P, false><<<sh.blocksX, 128, 0, fork->side>>>(d, insts, ctl, px, nParts);
+    if ((e = cudaEventRecord(fork->join, fork->side)) != cudaSuccess) return e;
+    if (sh2) k_plainY<P, true><<<sh.blocksY, 256, 0, st>>>(d, insts, ctl, py, nParts);
+    else k_plainY<P, false><<<sh.blocksY, 256, 0, st>>>(d, insts, ctl, py, nParts);
+    if ((e = cudaStreamWaitEvent(st, fork->join, 0)) != cudaSuccess) return e;
+    int nl = 2;
+    if (!sh2) {
+      k_plainBC<P><<<sh.blocksR, 256, 0, st>>>(d, insts, ctl);
+      nl += 1;
+    }
+    if (sh2) k_plainD<P, true><<<sh.blocksDS, 256, 0, st>>>(d, insts, ctl, pd, px, nParts, nParts, counter);
+    else k_plainD<P, false><<<sh.blocksD, 256, 0, st>>>(d, insts, ctl, pd, px, nParts, nParts, counter);
+    nl += 1;
+    if (launches) *launches += nl;
+    return cudaGetLastError();
+  }
+  const int nD = sh2 ? sh.blocksDS : sh.blocksD, nParts = sh.blocksA + nD;
+  A *pa = static_cast<A *>(part), *pd = pa + sh.blocksA;      // value-major rows of nParts: A's blocks, then D's
+  cudaError_t e = sh2 ? launchPDL(k_plainA<P, true>, sh.blocksA, st, d, insts, ctl, pa, nParts)
                       : launchPDL(k_plainA<P, false>, sh.blocksA, st, d, insts, ctl, pa, nParts);
   if (e != cudaSuccess) return e;
   int nl = 1;
@@ -571,7 +622,7 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
     if ((e = launchPDL(k_plainBC<P>, sh.blocksR, st, d, insts, ctl)) != cudaSuccess) return e;
     nl += 1;
   }
-  e = sh2 ? launchPDL(k_plainD<P, true>, sh.blocksD, st, d, insts, ctl, pd, pa, nParts, nParts, counter)
+  e = sh2 ? launchPDL(k_plainD<P, true>, sh.blocksDS, st, d, insts, ctl, pd, pa, nParts, nParts, counter)
           : launchPDL(k_plainD<P, false>, sh.blocksD, st, d, insts, ctl, pd, pa, nParts, nParts, counter);
   if (e != cudaSuccess) return e;
   nl += 1;
@@ -603,7 +654,7 @@ int gridBlocks(bool shortSides) {
   template cudaError_t launchBatched<P>(const Dev<P> &, const InstDesc *, InstCtl *, const int *, int, int, const uint8_t *, \
                                         int, int, bool, cudaStream_t);                                               \
   template cudaError_t launchPlainIter<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, const PlainShape &, bool,    \
-                                          bool, cudaStream_t, int *, unsigned *);                                    \
+                                          bool, cudaStream_t, int *, unsigned *, const PlainFork *);                 \
   template cudaError_t launchGrid<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, unsigned *, int *, int, int, bool, \
                                      cudaStream_t);                                                                  \
   template int gridBlocks<P>(bool);                                                                                 \

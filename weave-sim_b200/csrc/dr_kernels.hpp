@@ -6,16 +6,19 @@
 
 namespace wsb {
 
-// blocks of the plain form's kernels: element phase (general order; with the side ranks of the short-slide order),
-// general side order, update phase
-struct PlainShape { int blocksA, blocksAS, blocksR, blocksD; };
+// blocks of the plain form's kernels: element phase, general side order, update phase (general order; with the side
+// ranks of the short-slide order)
+struct PlainShape { int blocksA, blocksR, blocksD, blocksDS, blocksX, blocksY; };
+// a second stream and two events: the element phase forks into a crossing kernel on `side` and a rod kernel on the
+// main stream, joined before the update kernel
+struct PlainFork { cudaStream_t side; cudaEvent_t fork, join; };
 
 template <int P>
 cudaError_t launchBatched(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
                           const uint8_t *mask, int threads, int blocks, bool shortSides, cudaStream_t st);
 template <int P>
 cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, const PlainShape &sh, bool contacts,
-                            bool shortSides, cudaStream_t st, int *launches, unsigned *counter);
+                            bool shortSides, cudaStream_t st, int *launches, unsigned *counter, const PlainFork *fork);
 
 template <int P>
 cudaError_t launchGrid(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, unsigned *bar, int *err, int nIter,

@@ -318,17 +318,26 @@ __device__ __forceinline__ R support(const R Rf[9], const R n[3], R sign, R w, R
 
 // crossing c: one evaluation of PolylineContact.apply (solver_cpu.js:381-478) without the seat law, the augmented
 // Lagrangian and the rotational friction
-template <int P>
-__device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int buf, int iter, int kb, int c, Part<typename Dev<P>::A> &pt) {
+// kb: the buffer that receives the keys after the slide (the next sorted order's); ob: this iteration's sorted order.
+// Side records go to the side's strand position (general order) or, with SHORT, straight to its position in this
+// iteration's sorted order, so the gathers read them without an indirection.
+template <int P, bool SHORT>
+__device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int buf, int iter, int kb, int ob, int c, Part<typename Dev<P>::A> &pt) {
   using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A; using U = typename Dev<P>::U;
   const int kt_ = d.ktot, ks = d.kS, K2 = d.sS;
   const int pos[2] = {d.sPos[2 * c], d.sPos[2 * c + 1]};
+  int rec[2] = {pos[0], pos[1]};
+  if constexpr (SHORT) {
+    rec[0] = d.sInv[size_t(ob) * d.kB + pos[0]];
+    rec[1] = d.sInv[size_t(ob) * d.kB + pos[1]];
+  }
   const double rampN = I.ramp_iter;
   const double rampd = rampN <= 0 ? 1.0 : fmin(1.0, 0.01 + 0.99 * double(iter) / rampN);
   const R kn = R(rampd * I.strength), kt = R(rampd * I.stick);
   R Pl[2][3], tg[2][3], Rf[2][9], L[2], tp[2];
   int base[2], nseg[2];
   U uu[2];
+  #pragma unroll
   for (int side = 0; side < 2; side++) {
     const int o = side * kt_ + c;
     uu[side] = d.u[side * ks + c];
@@ -411,9 +420,12 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   d.u[c] = mclamp(uu[0], U(0), U(nseg[0]));
   d.u[ks + c] = mclamp(uu[1], U(0), U(nseg[1]));
   // the sides' segments after the slide (solver_cpu.js:144-149): the keys of the next sort, into key buffer kb
+  #pragma unroll
   for (int side = 0; side < 2; side++) {
     const U un = d.u[side * ks + c];
-    d.sKey[size_t(kb) * d.kB + pos[side]] = int(mmin(mmax(mfloor(un), U(0)), U(mmax(nseg[side] - 1, 0))));
+    const int key = int(mmin(mmax(mfloor(un), U(0)), U(mmax(nseg[side] - 1, 0))));
+    d.sKey[size_t(kb) * d.kB + pos[side]] = key;
+    if constexpr (SHORT) d.sKeyS[rec[side]] = key;
   }
   if (slip) {
     const R sx = da * tA[0] + db * tB[0], sy = da * tA[1] + db * tB[1], sz = da * tA[2] + db * tB[2];
@@ -435,8 +447,9 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   const R tf = R(I.tf);
   const R tfc = R(fmax(I.tf, 1e-3)), hc = d.ch[c], wc = d.cw[c];
   const R kth = tfc * ((Fn + kn * R(0.25) * hc) * (R(0.5) * wc) / R(SUPPORT_SMOOTH) + kt * (R(0.5) * hc) * (R(0.5) * hc));
+  #pragma unroll
   for (int side = 0; side < 2; side++) {
-    const int q = pos[side];
+    const int q = rec[side];
     const R sgn = side ? R(-1) : R(1);
     const R F[3] = {sgn * FA[0], sgn * FA[1], sgn * FA[2]};
     R tq[3];
@@ -492,22 +505,23 @@ __device__ __forceinline__ void segCount(const Dev<P> &d, int j, int kb, int dst
   d.rngHi[size_t(dst) * d.rB + j] = off + lo + eq;
 }
 // short-slide order (the slide limit is under half the shortest segment, so a side moves at most one segment per
-// iteration): built inside the element phase from the keys of the previous iteration (the segments the sides sit on
-// before this iteration's slide), into the buffer this iteration's gathers read.  The first side of each segment
-// writes that segment's slice; a segment without sides keeps a slice of an earlier iteration, whose entries carry
-// other keys, and the gathers skip entries whose key is not the segment's.
+// iteration): built in the update phase from the keys this iteration's slide produced, into buffer kb, the order the
+// next iteration's crossings write their side records into and its gathers read.  Side p's sorted position goes to
+// sInv, its key to ordSeg; the first side of each segment writes that segment's slice.  A segment without sides
+// keeps a slice of an earlier iteration, whose entries carry other keys, and the gathers skip entries whose key is
+// not the segment's.
 template <int P>
-__device__ __forceinline__ void rankSideShort(const Dev<P> &d, int p, int buf) {
+__device__ __forceinline__ void rankSideShort(const Dev<P> &d, int p, int kb) {
   const int s = d.sStrand[p], off = d.stSideOff[s];
-  const int *key = d.sKey + size_t(buf) * d.kB;
+  const int *key = d.sKey + size_t(kb) * d.kB;
   const SideRank r = sideRank(key, p, off, d.stSideCnt[s]);
   const int k = key[p];
-  d.ord[size_t(buf) * d.oB + r.pos] = p;
-  d.ordSeg[size_t(buf) * d.oB + r.pos] = k;
+  d.sInv[size_t(kb) * d.kB + p] = r.pos;
+  d.ordSeg[size_t(kb) * d.oB + r.pos] = k;
   if (r.pos == off + r.below) {
     const int j = d.stSegOff[s] + k;
-    d.rngLo[size_t(buf) * d.rB + j] = off + r.below;
-    d.rngHi[size_t(buf) * d.rB + j] = off + r.below + r.equal;
+    d.rngLo[size_t(kb) * d.rB + j] = off + r.below;
+    d.rngHi[size_t(kb) * d.rB + j] = off + r.below + r.equal;
   }
 }
 
@@ -517,14 +531,18 @@ struct StepCtx {
   double dispR;      // prescribed-motion fraction of this iteration
 };
 
-// the sides in the slice of segment j (strand-local index lj) of sorted-side buffer ob, in sorted order; with SHORT an
-// entry counts only if it carries the segment's key (a slice left over from an earlier iteration carries other keys)
+// the side records in the slice of segment j (strand-local index lj) of sorted-side buffer ob, in sorted order: with
+// SHORT the records sit at the sorted positions, and an entry counts only if it carries the segment's key (a slice left
+// over from an earlier iteration carries other keys); in the general order the entries name the records' positions
 template <bool SHORT, int P, class F>
 __device__ __forceinline__ void sidesOn(const Dev<P> &d, int ob, int j, int lj, F &&f) {
   const int lo = d.rngLo[size_t(ob) * d.rB + j], hi = d.rngHi[size_t(ob) * d.rB + j];
   for (int e = lo; e < hi; e++) {
-    if (SHORT && d.ordSeg[size_t(ob) * d.oB + e] != lj) continue;
-    f(d.ord[size_t(ob) * d.oB + e]);
+    if constexpr (SHORT) {
+      if (d.ordSeg[size_t(ob) * d.oB + e] == lj) f(e);
+    } else {
+      f(d.ord[size_t(ob) * d.oB + e]);
+    }
   }
 }
 
@@ -597,11 +615,10 @@ __device__ __forceinline__ void segUpdate(const Dev<P> &d, const InstDesc &I, co
     if constexpr (SHORT) {
       // the sides on segment j after the slide were, before it, on j − 1, j or j + 1 of the same strand
       const int s = d.segStrand[j];
-      const int *key = d.sKey + size_t(sc.onxt) * d.kB;
       for (int dj = -1; dj <= 1; dj++) {
         const int jj = j + dj;
         if (jj < 0 || jj >= mt || d.segStrand[jj] != s) continue;
-        sidesOn<true>(d, sc.obuf, jj, lj + dj, [&](int q) { if (key[q] == lj) kTw += d.kth[q]; });
+        sidesOn<true>(d, sc.obuf, jj, lj + dj, [&](int q) { if (d.sKeyS[q] == lj) kTw += d.kth[q]; });
       }
     } else {
       sidesOn<false>(d, sc.onxt, j, 0, [&](int q) { kTw += d.kth[q]; });
