@@ -394,7 +394,9 @@ __device__ __forceinline__ void plainA(const Dev<P> &d, const InstDesc *__restri
   Part<A> pt;
   pt.init();
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nA; e += gridDim.x * blockDim.x) phaseA<P, SHORT>(d, I, sx, base + e, nK, pt);
-  blockReduce(pt, red);
+  constexpr unsigned SM = PART == 1 ? SUMS_CROSS : PART == 2 ? SUMS_ROD : (SUMS_CROSS | SUMS_ROD);
+  constexpr unsigned XM = PART == 1 ? MAXS_CROSS : PART == 2 ? MAXS_ROD : (MAXS_CROSS | MAXS_ROD);
+  blockReduce<SM, XM>(pt, red);
   if (threadIdx.x == 0) putPart(pt, part, blockIdx.x, partStride);
 }
 template <int P, bool SHORT>
@@ -444,7 +446,7 @@ __global__ void __launch_bounds__(256, WSB_MINB_D) k_plainD(Dev<P> d, const Inst
   pt.init();
   const int nD = countD<SHORT>(I);
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nD; e += gridDim.x * blockDim.x) phaseD<P, SHORT>(d, I, sx, e, pt);
-  blockReduce(pt, red);
+  blockReduce<SUMS_UPDATE, MAXS_UPDATE>(pt, red);
   if (threadIdx.x == 0) {
     putPart(pt, part, blockIdx.x, partStride);
     __threadfence();

@@ -546,21 +546,32 @@ __device__ __forceinline__ void sidesOn(const Dev<P> &d, int ob, int j, int lj, 
   }
 }
 
+// Both updates read everything first and store at the end, so no store stands between a load and the loads after it
+// (the compiler must assume they alias) and the loads of one element go out together.  Arrays that never change during
+// a step (topology, masses, loads, stiffness) are read through the read-only path; they live in global memory in every
+// form.
+template <class T> __device__ __forceinline__ T ro(const T *p) { return __ldg(p); }
+
 template <int P, bool SHORT>
 __device__ __forceinline__ void nodeUpdate(const Dev<P> &d, const InstDesc &I, const StepCtx &sc, int i, Part<typename Dev<P>::A> &pt) {
   using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A;
   const int nt = d.ntot, ns = d.nS, ms = d.mS, K2 = d.sS;
-  const int so = d.nsOut[i], si = d.nsIn[i];
-  const uint8_t fl = d.nflag[i];
+  const int so = ro(d.nsOut + i), si = ro(d.nsIn + i);
+  const uint8_t fl = ro(d.nflag + i);
+  const R m = ro(d.mass + i);
+  R tot[3] = {ro(d.lc + i), ro(d.lc + nt + i), ro(d.lc + 2 * nt + i)};
+  const int ai = (fl & 32) ? ro(d.anc + i) : -1;
+  W x[3], v0[3] = {W(0), W(0), W(0)};
+  for (int k = 0; k < 3; k++) x[k] = Acc<P>::xw(d, sc.cur, k, i);
+  if (!(sc.pending || sc.warm)) for (int k = 0; k < 3; k++) v0[k] = W(d.V[k * ns + i]);
   R F[3] = {R(0), R(0), R(0)};
   if (so >= 0) for (int k = 0; k < 3; k++) F[k] += d.nF[k * ms + so];
   if (si >= 0) for (int k = 0; k < 3; k++) F[k] -= d.nF[k * ms + si];
-  R tot[3] = {d.lc[i], d.lc[nt + i], d.lc[2 * nt + i]};
   if (fl & 16) {                          // load in the node frame (solver_cpu.js:755-758)
     R q[4], Rn[9];
     nodeQuat<P>(d, sc.cur, i, q);
     qframe(q, Rn);
-    const R f0 = d.ll[i], f1 = d.ll[nt + i], f2 = d.ll[2 * nt + i];
+    const R f0 = ro(d.ll + i), f1 = ro(d.ll + nt + i), f2 = ro(d.ll + 2 * nt + i);
     for (int k = 0; k < 3; k++) tot[k] += Rn[k] * f0 + Rn[3 + k] * f1 + Rn[6 + k] * f2;
   }
   for (int k = 0; k < 3; k++) F[k] += tot[k];
@@ -568,30 +579,31 @@ __device__ __forceinline__ void nodeUpdate(const Dev<P> &d, const InstDesc &I, c
   // crossing sides on the adjacent segments, as distributed by the last evaluation (weights 1 − t at a, t at b)
   const bool cx = I.contacts && I.K;
   if (cx && so >= 0)
-    sidesOn<SHORT>(d, sc.obuf, so, SHORT ? d.segLocal[so] : 0, [&](int q) {
+    sidesOn<SHORT>(d, sc.obuf, so, SHORT ? ro(d.segLocal + so) : 0, [&](int q) {
       const R wgt = R(1) - d.sT[q];
       for (int k = 0; k < 3; k++) F[k] += wgt * d.sF[k * K2 + q];
     });
   if (cx && si >= 0)
-    sidesOn<SHORT>(d, sc.obuf, si, SHORT ? d.segLocal[si] : 0, [&](int q) {
+    sidesOn<SHORT>(d, sc.obuf, si, SHORT ? ro(d.segLocal + si) : 0, [&](int q) {
       const R wgt = d.sT[q];
       for (int k = 0; k < 3; k++) F[k] += wgt * d.sF[k * K2 + q];
     });
-  if (fl & 8) for (int k = 0; k < 3; k++) d.react[k * nt + i] = -F[k];
+  const R react[3] = {-F[0], -F[1], -F[2]};
   for (int k = 0; k < 3; k++) if (!(fl & (1 << k))) F[k] = R(0);
   pt.x[RX_F] = mmax(pt.x[RX_F], A(msqrt(dot3(F, F))));
   R v[3];
-  for (int k = 0; k < 3; k++) v[k] = sc.pending || sc.warm ? R(0) : d.V[k * ns + i];
-  const R m = d.mass[i];
+  for (int k = 0; k < 3; k++) v[k] = R(v0[k]);
   if (!sc.warm) for (int k = 0; k < 3; k++) v[k] += F[k] / m;
   if (I.damping != 1.0) for (int k = 0; k < 3; k++) v[k] *= R(I.damping);
   for (int k = 0; k < 3; k++) if (!(fl & (1 << k))) v[k] = R(0);
-  const int ai = (fl & 32) ? d.anc[i] : -1;
+  for (int k = 0; k < 3; k++) {
+    x[k] += W(v[k]);
+    if (ai >= 0 && !(fl & (1 << k))) x[k] = ro(d.ancStart + size_t(k) * nt + ai) + W(sc.dispR) * ro(d.ancDelta + size_t(k) * nt + ai);
+  }
+  if (fl & 8) for (int k = 0; k < 3; k++) d.react[k * nt + i] = react[k];
   for (int k = 0; k < 3; k++) {
     d.V[k * ns + i] = v[k];
-    W x = Acc<P>::xw(d, sc.cur, k, i) + W(v[k]);
-    if (ai >= 0 && !(fl & (1 << k))) x = d.ancStart[size_t(k) * nt + ai] + W(sc.dispR) * d.ancDelta[size_t(k) * nt + ai];
-    Acc<P>::xs(d, sc.nxt, k, i, x);
+    Acc<P>::xs(d, sc.nxt, k, i, x[k]);
   }
   pt.s[RS_KE] += A(m) * (A(v[0]) * A(v[0]) + A(v[1]) * A(v[1]) + A(v[2]) * A(v[2]));
 }
@@ -600,24 +612,28 @@ template <int P, bool SHORT>
 __device__ __forceinline__ void segUpdate(const Dev<P> &d, const InstDesc &I, const StepCtx &sc, int j, Part<typename Dev<P>::A> &pt) {
   using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A;
   const int mt = d.mtot, sm = d.mS, ps = d.pS, cs = d.cS, K2 = d.sS;
+  const int ja = ro(d.jA + j), jb = ro(d.jB + j), c0 = ro(d.cl0 + j), c1 = ro(d.cl1 + j);
+  const R krs[3] = {ro(d.krs + j), ro(d.krs + mt + j), ro(d.krs + 2 * mt + j)};
+  W qw[4];
+  for (int k = 0; k < 4; k++) qw[k] = Acc<P>::qw(d, sc.cur, k, j);
+  R w0[3] = {R(0), R(0), R(0)};
+  if (!sc.pending) for (int k = 0; k < 3; k++) w0[k] = d.Wr[k * sm + j];
   R T[3] = {d.en[j], d.en[sm + j], d.en[2 * sm + j]};
   R kD[3] = {R(0), R(0), R(0)};
-  const int ja = d.jA[j], jb = d.jB[j];
   if (ja >= 0) for (int k = 0; k < 3; k++) { T[k] += d.tau[k * ps + ja]; kD[k] += d.kd[k * ps + ja]; }
   if (jb >= 0) for (int k = 0; k < 3; k++) { T[k] -= d.tau[k * ps + jb]; kD[k] += d.kd[k * ps + jb]; }
-  const int c0 = d.cl0[j], c1 = d.cl1[j];
   if (c0 >= 0) for (int k = 0; k < 3; k++) T[k] -= d.tauC[k * cs + c0];
   if (c1 >= 0) for (int k = 0; k < 3; k++) T[k] -= d.tauC[k * cs + c1];
   R kTw = R(0);
   if (I.contacts && I.K) {
-    const int lj = SHORT ? d.segLocal[j] : 0;
+    const int lj = SHORT ? ro(d.segLocal + j) : 0;
     sidesOn<SHORT>(d, sc.obuf, j, lj, [&](int q) { for (int k = 0; k < 3; k++) T[k] += d.sTq[k * K2 + q]; });
     if constexpr (SHORT) {
       // the sides on segment j after the slide were, before it, on j − 1, j or j + 1 of the same strand
-      const int s = d.segStrand[j];
+      const int s = ro(d.segStrand + j);
       for (int dj = -1; dj <= 1; dj++) {
         const int jj = j + dj;
-        if (jj < 0 || jj >= mt || d.segStrand[jj] != s) continue;
+        if (jj < 0 || jj >= mt || ro(d.segStrand + jj) != s) continue;
         sidesOn<true>(d, sc.obuf, jj, lj + dj, [&](int q) { if (d.sKeyS[q] == lj) kTw += d.kth[q]; });
       }
     } else {
@@ -625,7 +641,7 @@ __device__ __forceinline__ void segUpdate(const Dev<P> &d, const InstDesc &I, co
     }
   }
   R q[4], Rm[9];
-  for (int k = 0; k < 4; k++) q[k] = Acc<P>::qr(d, sc.cur, k, j);
+  for (int k = 0; k < 4; k++) q[k] = R(qw[k]);
   qframe(q, Rm);
   R tm[3];
   for (int k = 0; k < 3; k++) tm[k] = Rm[3 * k] * T[0] + Rm[3 * k + 1] * T[1] + Rm[3 * k + 2] * T[2];
@@ -633,13 +649,12 @@ __device__ __forceinline__ void segUpdate(const Dev<P> &d, const InstDesc &I, co
   const R ms = R(I.ms);
   R w[3], I3[3];
   for (int k = 0; k < 3; k++) {
-    I3[k] = ms * mmax(d.krs[k * mt + j] + kTw + kD[k], R(1e-12));
-    w[k] = (sc.pending ? R(0) : d.Wr[k * sm + j]) + tm[k] / I3[k];
+    I3[k] = ms * mmax(krs[k] + kTw + kD[k], R(1e-12));
+    w[k] = w0[k] + tm[k] / I3[k];
   }
   w[2] = mclamp(w[2], R(-TWIST_RATE_MAX), R(TWIST_RATE_MAX));
   if (kTw > R(0)) w[2] *= R(ROLL_DAMP);
   if (I.damping != 1.0) for (int k = 0; k < 3; k++) w[k] *= R(I.damping);
-  for (int k = 0; k < 3; k++) d.Wr[k * sm + j] = w[k];
   // q ← normalize(q ⊗ exp(ω)) in the wide type; the increment q ⊗ (exp(ω) − 1) is small, formed in R
   const R a = msqrt(dot3(w, w)), half = R(0.5) * a;
   R sh, ch;
@@ -648,8 +663,6 @@ __device__ __forceinline__ void segUpdate(const Dev<P> &d, const InstDesc &I, co
   W qn[4];
   if constexpr (P != PREC_MIXED) {
     const W dq[4] = {ch, w[0] * s, w[1] * s, w[2] * s};
-    W qw[4];
-    for (int k = 0; k < 4; k++) qw[k] = Acc<P>::qw(d, sc.cur, k, j);
     qmul(qw, dq, qn);
   } else {
     R sq, cq;
@@ -657,40 +670,61 @@ __device__ __forceinline__ void segUpdate(const Dev<P> &d, const InstDesc &I, co
     const R dm1[4] = {R(-2) * sq * sq, w[0] * s, w[1] * s, w[2] * s};
     R inc[4];
     qmul(q, dm1, inc);
-    for (int k = 0; k < 4; k++) qn[k] = Acc<P>::qw(d, sc.cur, k, j) + W(inc[k]);
+    for (int k = 0; k < 4; k++) qn[k] = qw[k] + W(inc[k]);
   }
   qnormalize<W, P == PREC_MIXED>(qn);
+  for (int k = 0; k < 3; k++) d.Wr[k * sm + j] = w[k];
   for (int k = 0; k < 4; k++) Acc<P>::qs(d, sc.nxt, k, j, qn[k]);
   pt.s[RS_KE] += A(I3[0]) * A(w[0]) * A(w[0]) + A(I3[1]) * A(w[1]) * A(w[1]) + A(I3[2]) * A(w[2]) * A(w[2]);
 }
 
 // ------------------------------------------------------------------------------------------------ reductions
-template <class A>
+// Slot sets: a kernel that feeds only some slots reduces only those (SM: sum slots, XM: max slots, bit i for slot i);
+// the others keep their identity values (0, or −∞ for RX_FN), so the result is the same as reducing every slot.
+constexpr unsigned SUMS_ALL = (1u << RS_NSUM) - 1, MAXS_ALL = (1u << RX_NMAX) - 1;
+constexpr unsigned SUMS_UPDATE = 1u << RS_KE, MAXS_UPDATE = (1u << RX_F) | (1u << RX_T) | (1u << RX_LOAD);
+constexpr unsigned SUMS_CROSS = (1u << RS_PEN) | (1u << RS_TAN), MAXS_CROSS = 1u << RX_FN;
+constexpr unsigned SUMS_ROD = (1u << RS_STRETCH) | (1u << RS_SHEAR) | (1u << RS_BEND) | (1u << RS_TWIST),
+                   MAXS_ROD = (1u << RX_N) | (1u << RX_M);
+
+template <unsigned SM = SUMS_ALL, unsigned XM = MAXS_ALL, class A>
 __device__ __forceinline__ void warpReduce(Part<A> &p) {
   for (int o = 16; o > 0; o >>= 1) {
-    for (int i = 0; i < RS_NSUM; i++) p.s[i] += __shfl_xor_sync(0xffffffffu, p.s[i], o);
-    for (int i = 0; i < RX_NMAX; i++) p.x[i] = mmax(p.x[i], __shfl_xor_sync(0xffffffffu, p.x[i], o));
+#pragma unroll
+    for (int i = 0; i < RS_NSUM; i++)
+      if (SM & (1u << i)) p.s[i] += __shfl_xor_sync(0xffffffffu, p.s[i], o);
+#pragma unroll
+    for (int i = 0; i < RX_NMAX; i++)
+      if (XM & (1u << i)) p.x[i] = mmax(p.x[i], __shfl_xor_sync(0xffffffffu, p.x[i], o));
   }
 }
 // block-wide reduction in a fixed order; the result is valid in thread 0 (smem: >= 32 * (RS_NSUM + RX_NMAX) values)
-template <class A>
+template <unsigned SM = SUMS_ALL, unsigned XM = MAXS_ALL, class A>
 __device__ __forceinline__ void blockReduce(Part<A> &p, A *smem) {
-  warpReduce(p);
+  warpReduce<SM, XM>(p);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
   constexpr int NV = RS_NSUM + RX_NMAX;
   if (lane == 0) {
-    for (int i = 0; i < RS_NSUM; i++) smem[wid * NV + i] = p.s[i];
-    for (int i = 0; i < RX_NMAX; i++) smem[wid * NV + RS_NSUM + i] = p.x[i];
+#pragma unroll
+    for (int i = 0; i < RS_NSUM; i++)
+      if (SM & (1u << i)) smem[wid * NV + i] = p.s[i];
+#pragma unroll
+    for (int i = 0; i < RX_NMAX; i++)
+      if (XM & (1u << i)) smem[wid * NV + RS_NSUM + i] = p.x[i];
   }
   __syncthreads();
   if (wid == 0) {
     Part<A> q;
     q.init();
     if (lane < nw) {
-      for (int i = 0; i < RS_NSUM; i++) q.s[i] = smem[lane * NV + i];
-      for (int i = 0; i < RX_NMAX; i++) q.x[i] = smem[lane * NV + RS_NSUM + i];
+#pragma unroll
+      for (int i = 0; i < RS_NSUM; i++)
+        if (SM & (1u << i)) q.s[i] = smem[lane * NV + i];
+#pragma unroll
+      for (int i = 0; i < RX_NMAX; i++)
+        if (XM & (1u << i)) q.x[i] = smem[lane * NV + RS_NSUM + i];
     }
-    warpReduce(q);
+    warpReduce<SM, XM>(q);
     if (lane == 0) p = q;
   }
   __syncthreads();
