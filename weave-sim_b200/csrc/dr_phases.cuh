@@ -148,17 +148,21 @@ struct Part {
   }
 };
 
+// Arrays that never change during a step (topology, masses, loads, stiffness, crossing constants) are read through the
+// read-only path; they live in global memory in every form.
+template <class T> __device__ __forceinline__ T ro(const T *p) { return __ldg(p); }
+
 // ------------------------------------------------------------------------------------------------ node helpers
 // node tangent: normalised sum of the unit chords of the adjacent segments (PolylineContact._prepare)
 template <int P>
 __device__ __forceinline__ void nodeTangent(const Dev<P> &d, int buf, int i, typename Dev<P>::R T[3]) {
   using R = typename Dev<P>::R;
   T[0] = T[1] = T[2] = R(0);
-  const int so = d.nsOut[i], si = d.nsIn[i];
+  const int so = ro(d.nsOut + i), si = ro(d.nsIn + i);
   for (int j : {so, si}) {
     if (j < 0) continue;
     R e[3];
-    Acc<P>::edge(d, buf, d.segI0[j], d.segI1[j], e);
+    Acc<P>::edge(d, buf, ro(d.segI0 + j), ro(d.segI1 + j), e);
     const R l = mmax(msqrt(dot3(e, e)), R(1e-12));
     for (int k = 0; k < 3; k++) T[k] += e[k] / l;
   }
@@ -169,7 +173,7 @@ __device__ __forceinline__ void nodeTangent(const Dev<P> &d, int buf, int i, typ
 template <int P>
 __device__ __forceinline__ void nodeQuat(const Dev<P> &d, int buf, int i, typename Dev<P>::R q[4]) {
   using R = typename Dev<P>::R;
-  const int so = d.nsOut[i], si = d.nsIn[i], ref = so >= 0 ? so : si;
+  const int so = ro(d.nsOut + i), si = ro(d.nsIn + i), ref = so >= 0 ? so : si;
   q[0] = q[1] = q[2] = q[3] = R(0);
   if (ref < 0) return;
   R qr[4];
@@ -190,25 +194,25 @@ __device__ __forceinline__ void nodeQuat(const Dev<P> &d, int buf, int i, typena
 template <int P>
 __device__ __forceinline__ void segForce(const Dev<P> &d, int buf, int j, Part<typename Dev<P>::A> &pt) {
   using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A;
-  const int a = d.segI0[j], b = d.segI1[j];
+  const int a = ro(d.segI0 + j), b = ro(d.segI1 + j);
   W ew[3], qw[4], Rw[9];
   for (int k = 0; k < 3; k++) ew[k] = Acc<P>::xw(d, buf, k, b) - Acc<P>::xw(d, buf, k, a);
   for (int k = 0; k < 4; k++) qw[k] = Acc<P>::qw(d, buf, k, j);
   R s1, s2, s3;
   if constexpr (P == PREC_MIXED) {      // two-float frames are near unit; the inverse rest length is kept in f64
     qframe<W, true>(qw, Rw);
-    const W il = d.il0[j];
+    const W il = ro(d.il0 + j);
     s1 = R((Rw[0] * ew[0] + Rw[1] * ew[1] + Rw[2] * ew[2]) * il);
     s2 = R((Rw[3] * ew[0] + Rw[4] * ew[1] + Rw[5] * ew[2]) * il);
     s3 = R((Rw[6] * ew[0] + Rw[7] * ew[1] + Rw[8] * ew[2]) * il - W(1));
   } else {
     qframe(qw, Rw);
-    const W l0 = W(d.l0[j]);
+    const W l0 = W(ro(d.l0 + j));
     s1 = R((Rw[0] * ew[0] + Rw[1] * ew[1] + Rw[2] * ew[2]) / l0);
     s2 = R((Rw[3] * ew[0] + Rw[4] * ew[1] + Rw[5] * ew[2]) / l0);
     s3 = R((Rw[6] * ew[0] + Rw[7] * ew[1] + Rw[8] * ew[2]) / l0 - W(1));
   }
-  const R GA = d.GA[j], EA = d.EA[j];
+  const R GA = ro(d.GA + j), EA = ro(d.EA + j);
   const R n1 = GA * s1, n2 = GA * s2, n3 = EA * s3;
   R Rr[9];
   for (int k = 0; k < 9; k++) Rr[k] = R(Rw[k]);
@@ -219,7 +223,7 @@ __device__ __forceinline__ void segForce(const Dev<P> &d, int buf, int j, Part<t
   const int ms = d.mS;
   for (int k = 0; k < 3; k++) { d.nF[k * ms + j] = nv[k]; d.en[k * ms + j] = en[k]; }
   d.Nax[j] = n3; d.Vsh[j] = n1; d.Vsh[d.mtot + j] = n2;
-  const R l0r = d.l0[j];
+  const R l0r = ro(d.l0 + j);
   pt.s[RS_STRETCH] += A(R(0.5) * l0r * n3 * s3);
   pt.s[RS_SHEAR] += A(R(0.5) * l0r * (n1 * s1 + n2 * s2));
   pt.x[RX_N] = mmax(pt.x[RX_N], A(mabs(n3)));
@@ -254,14 +258,14 @@ __device__ __forceinline__ void jlinvT(const R psi[3], const R m[3], R th, R j[3
 template <int P>
 __device__ __forceinline__ void jointTorque(const Dev<P> &d, int buf, int jt, Part<typename Dev<P>::A> &pt) {
   using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A;
-  const int sa = d.jS0[jt], sb = d.jS1[jt], pt_ = d.ptot;
+  const int sa = ro(d.jS0 + jt), sb = ro(d.jS1 + jt), pt_ = d.ptot;
   W qa[4], qb[4];
   for (int k = 0; k < 4; k++) { qa[k] = Acc<P>::qw(d, buf, k, sa); qb[k] = Acc<P>::qw(d, buf, k, sb); }
   R psi[3];
   const R th = relRot<P>(qa, qb, psi);
-  const R lb = d.jLen[jt];
-  const R dd[3] = {psi[0] / lb - d.om[jt], psi[1] / lb - d.om[pt_ + jt], psi[2] / lb - d.om[2 * pt_ + jt]};
-  const R EIx = d.EIx[jt], EIy = d.EIy[jt], GJ = d.GJ[jt];
+  const R lb = ro(d.jLen + jt);
+  const R dd[3] = {psi[0] / lb - ro(d.om + jt), psi[1] / lb - ro(d.om + pt_ + jt), psi[2] / lb - ro(d.om + 2 * pt_ + jt)};
+  const R EIx = ro(d.EIx + jt), EIy = ro(d.EIy + jt), GJ = ro(d.GJ + jt);
   const R mm[3] = {EIx * dd[0], EIy * dd[1], GJ * dd[2]};
   {
     const R q0 = psi[0] * psi[0], q1 = psi[1] * psi[1], q2 = psi[2] * psi[2], f = R(0.25) / lb;
@@ -287,14 +291,14 @@ __device__ __forceinline__ void jointTorque(const Dev<P> &d, int buf, int jt, Pa
 template <int P>
 __device__ __forceinline__ void clampTorque(const Dev<P> &d, int buf, int cc, Part<typename Dev<P>::A> &pt) {
   using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A;
-  const int j = d.cSeg[cc], ct = d.ctot;
+  const int j = ro(d.cSeg + cc), ct = d.ctot;
   W qa[4], qb[4];
-  for (int k = 0; k < 4; k++) { qa[k] = d.cQ[k * ct + cc]; qb[k] = Acc<P>::qw(d, buf, k, j); }
+  for (int k = 0; k < 4; k++) { qa[k] = ro(d.cQ + k * ct + cc); qb[k] = Acc<P>::qw(d, buf, k, j); }
   R psi[3];
   const R th = relRot<P>(qa, qb, psi);
-  const R lc = d.cLen[cc];
+  const R lc = ro(d.cLen + cc);
   const R dd[3] = {psi[0] / lc, psi[1] / lc, psi[2] / lc};
-  const R mm[3] = {d.cB[cc] * dd[0], d.cB[ct + cc] * dd[1], d.cB[2 * ct + cc] * dd[2]};
+  const R mm[3] = {ro(d.cB + cc) * dd[0], ro(d.cB + ct + cc) * dd[1], ro(d.cB + 2 * ct + cc) * dd[2]};
   R jv[3];
   jlinvT(psi, mm, th, jv);
   R qr[4], Rc[9];
@@ -325,27 +329,35 @@ template <int P, bool SHORT>
 __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int buf, int iter, int kb, int ob, int c, Part<typename Dev<P>::A> &pt) {
   using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A; using U = typename Dev<P>::U;
   const int kt_ = d.ktot, ks = d.kS, K2 = d.sS;
-  const int pos[2] = {d.sPos[2 * c], d.sPos[2 * c + 1]};
+  // everything the crossing reads, before anything it writes
+  const int pos[2] = {ro(d.sPos + 2 * c), ro(d.sPos + 2 * c + 1)};
   int rec[2] = {pos[0], pos[1]};
   if constexpr (SHORT) {
     rec[0] = d.sInv[size_t(ob) * d.kB + pos[0]];
     rec[1] = d.sInv[size_t(ob) * d.kB + pos[1]];
   }
+  const R np[3] = {d.nPrev[c], d.nPrev[ks + c], d.nPrev[2 * ks + c]};
+  const uint8_t fl = ro(d.cflag + c);
+  const R muc = ro(d.mu + c), wkA = ro(d.wk + c), hkA = ro(d.hk + c), wkB = ro(d.wk + kt_ + c), hkB = ro(d.hk + kt_ + c);
+  const R hc = ro(d.ch + c), wc = ro(d.cw + c);
+  const A slip0 = d.slip[c];
   const double rampN = I.ramp_iter;
   const double rampd = rampN <= 0 ? 1.0 : fmin(1.0, 0.01 + 0.99 * double(iter) / rampN);
   const R kn = R(rampd * I.strength), kt = R(rampd * I.stick);
   R Pl[2][3], tg[2][3], Rf[2][9], L[2], tp[2];
-  int base[2], nseg[2];
+  int nseg[2];
+  W xa[2][3];                           // base node of each side's segment, for the gap in the wide type
   U uu[2];
   #pragma unroll
   for (int side = 0; side < 2; side++) {
     const int o = side * kt_ + c;
     uu[side] = d.u[side * ks + c];
-    nseg[side] = d.cxNseg[o];
+    nseg[side] = ro(d.cxNseg + o);
     const int li = int(mmin(mmax(mfloor(uu[side]), U(0)), U(mmax(nseg[side] - 1, 0))));
     const R t = R(mmin(mmax(uu[side] - U(li), U(0)), U(1)));
-    const int sg = d.cxSegOff[o] + li;
-    const int a = d.segI0[sg], b = d.segI1[sg];
+    const int sg = ro(d.cxSegOff + o) + li;
+    const int a = ro(d.segI0 + sg), b = ro(d.segI1 + sg);
+    for (int k = 0; k < 3; k++) xa[side][k] = Acc<P>::xw(d, buf, k, a);
     R e[3], Ta[3], Tb[3];
     Acc<P>::edge(d, buf, a, b, e);
     const R Ls = msqrt(dot3(e, e));
@@ -375,27 +387,24 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
     R x[3];
     cross3(y, tg[side], x);
     for (int k = 0; k < 3; k++) { Rf[side][k] = x[k]; Rf[side][3 + k] = y[k]; Rf[side][6 + k] = tg[side][k]; }
-    L[side] = Ls; tp[side] = t; base[side] = a;
+    L[side] = Ls; tp[side] = t;
   }
   const R *tA = tg[0], *tB = tg[1];
   // contact normal with side persistence (solver_cpu.js:396-402)
   R nv[3];
   cross3(tA, tB, nv);
-  R np[3] = {d.nPrev[c], d.nPrev[ks + c], d.nPrev[2 * ks + c]};
   const R nn = msqrt(dot3(nv, nv));
   if (nn < R(1e-6)) { nv[0] = np[0]; nv[1] = np[1]; nv[2] = np[2]; }
   else { const R dn = mmax(nn, R(1e-12)); nv[0] /= dn; nv[1] /= dn; nv[2] /= dn; }
   if (dot3(nv, np) < R(0)) { nv[0] = -nv[0]; nv[1] = -nv[1]; nv[2] = -nv[2]; }
-  for (int k = 0; k < 3; k++) d.nPrev[k * ks + c] = nv[k];
   // gap vector P_B − P_A: the base-node difference in the wide type
   R S[3];
-  for (int k = 0; k < 3; k++) S[k] = R(Acc<P>::xw(d, buf, k, base[1]) - Acc<P>::xw(d, buf, k, base[0])) + (Pl[1][k] - Pl[0][k]);
+  for (int k = 0; k < 3; k++) S[k] = R(xa[1][k] - xa[0][k]) + (Pl[1][k] - Pl[0][k]);
   const R g = dot3(S, nv);
   R rA[3], rB[3];
-  const R hA = support(Rf[0], nv, R(1), d.wk[c], d.hk[c], rA);
-  const R hB = support(Rf[1], nv, R(-1), d.wk[kt_ + c], d.hk[kt_ + c], rB);
+  const R hA = support(Rf[0], nv, R(1), wkA, hkA, rA);
+  const R hB = support(Rf[1], nv, R(-1), wkB, hkB, rB);
   const R pen = (hA + hB) - g;
-  const uint8_t fl = d.cflag[c];
   const bool enabled = fl & 1, locked = fl & 2;
   const bool active = (pen > R(0) || locked) && enabled;
   const R Fn = active ? kn * pen : R(0);
@@ -407,7 +416,7 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   const bool ok = det > R(1e-8);
   const R ca = ok ? (sa * tbb - sb * tab) / det : R(0), cb = ok ? (sb * taa - sa * tab) / det : R(0);
   const R Ftv = msqrt((kt * St[0]) * (kt * St[0]) + (kt * St[1]) * (kt * St[1]) + (kt * St[2]) * (kt * St[2]));
-  const R limit = d.mu[c] * mabs(Fn);
+  const R limit = muc * mabs(Fn);
   const bool slip = active && ok && !locked && Ftv > limit;
   const bool freeS = !active && ok && enabled;
   R scale = R(0);
@@ -417,36 +426,40 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   const R da = mclamp(ca * scale, -eps, eps), db = mclamp(cb * scale, -eps, eps);
   const bool moved = slip || freeS;
   if (moved) { uu[0] += U(da) / U(mmax(L[0], R(1e-12))); uu[1] -= U(db) / U(mmax(L[1], R(1e-12))); }
-  d.u[c] = mclamp(uu[0], U(0), U(nseg[0]));
-  d.u[ks + c] = mclamp(uu[1], U(0), U(nseg[1]));
-  // the sides' segments after the slide (solver_cpu.js:144-149): the keys of the next sort, into key buffer kb
-  #pragma unroll
-  for (int side = 0; side < 2; side++) {
-    const U un = d.u[side * ks + c];
-    const int key = int(mmin(mmax(mfloor(un), U(0)), U(mmax(nseg[side] - 1, 0))));
-    d.sKey[size_t(kb) * d.kB + pos[side]] = key;
-    if constexpr (SHORT) d.sKeyS[rec[side]] = key;
-  }
+  const U un[2] = {mclamp(uu[0], U(0), U(nseg[0])), mclamp(uu[1], U(0), U(nseg[1]))};
+  A slipNew = slip0;
   if (slip) {
     const R sx = da * tA[0] + db * tB[0], sy = da * tA[1] + db * tB[1], sz = da * tA[2] + db * tB[2];
-    d.slip[c] += A(msqrt(sx * sx + sy * sy + sz * sz));
+    slipNew += A(msqrt(sx * sx + sy * sy + sz * sz));
   }
-  d.stuck[c] = moved ? 0 : 1;
   R Se[3] = {R(0), R(0), R(0)};
   if (active) for (int k = 0; k < 3; k++) Se[k] = St[k] - da * tA[k] - db * tB[k];
   const R fT[3] = {kt * Se[0], kt * Se[1], kt * Se[2]};
   R FA[3];
   for (int k = 0; k < 3; k++) FA[k] = -Fn * nv[k] + fT[k];
-  d.Fn[c] = Fn;
-  d.Ft[c] = msqrt(dot3(fT, fT));
-  d.cstate[c] = slip ? 1 : 0;
-  d.gap[c] = g;
   // side records for the gathers: t before the slide, force on the side, lever torque tf (r × F); the righting
   // stiffness of the support point (addTwistStiffness, solver_cpu.js:170-176) goes to the segments the sides sit on
   // after the slide
   const R tf = R(I.tf);
-  const R tfc = R(fmax(I.tf, 1e-3)), hc = d.ch[c], wc = d.cw[c];
+  const R tfc = R(fmax(I.tf, 1e-3));
   const R kth = tfc * ((Fn + kn * R(0.25) * hc) * (R(0.5) * wc) / R(SUPPORT_SMOOTH) + kt * (R(0.5) * hc) * (R(0.5) * hc));
+  // stores
+  for (int k = 0; k < 3; k++) d.nPrev[k * ks + c] = nv[k];
+  d.u[c] = un[0];
+  d.u[ks + c] = un[1];
+  d.slip[c] = slipNew;
+  d.stuck[c] = moved ? 0 : 1;
+  d.Fn[c] = Fn;
+  d.Ft[c] = msqrt(dot3(fT, fT));
+  d.cstate[c] = slip ? 1 : 0;
+  d.gap[c] = g;
+  // the sides' segments after the slide (solver_cpu.js:144-149): the keys of the next sort, into key buffer kb
+  #pragma unroll
+  for (int side = 0; side < 2; side++) {
+    const int key = int(mmin(mmax(mfloor(un[side]), U(0)), U(mmax(nseg[side] - 1, 0))));
+    d.sKey[size_t(kb) * d.kB + pos[side]] = key;
+    if constexpr (SHORT) d.sKeyS[rec[side]] = key;
+  }
   #pragma unroll
   for (int side = 0; side < 2; side++) {
     const int q = rec[side];
@@ -547,10 +560,7 @@ __device__ __forceinline__ void sidesOn(const Dev<P> &d, int ob, int j, int lj, 
 }
 
 // Both updates read everything first and store at the end, so no store stands between a load and the loads after it
-// (the compiler must assume they alias) and the loads of one element go out together.  Arrays that never change during
-// a step (topology, masses, loads, stiffness) are read through the read-only path; they live in global memory in every
-// form.
-template <class T> __device__ __forceinline__ T ro(const T *p) { return __ldg(p); }
+// (the compiler must assume they alias) and the loads of one element go out together.
 
 template <int P, bool SHORT>
 __device__ __forceinline__ void nodeUpdate(const Dev<P> &d, const InstDesc &I, const StepCtx &sc, int i, Part<typename Dev<P>::A> &pt) {
