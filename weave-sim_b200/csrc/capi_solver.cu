@@ -728,6 +728,8 @@ void destroyCtx(ws_ctx *c) {
   if (c->fork.side) cudaStreamDestroy(c->fork.side);
   if (c->fork.fork) cudaEventDestroy(c->fork.fork);
   if (c->fork.join) cudaEventDestroy(c->fork.join);
+  if (c->fork.fork2) cudaEventDestroy(c->fork.fork2);
+  if (c->fork.join2) cudaEventDestroy(c->fork.join2);
   if (c->pinned) cudaFreeHost(c->pinned);
   delete c;
 }
@@ -764,6 +766,8 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
       CK(cudaStreamCreateWithFlags(&c->fork.side, cudaStreamNonBlocking));
       CK(cudaEventCreateWithFlags(&c->fork.fork, cudaEventDisableTiming));
       CK(cudaEventCreateWithFlags(&c->fork.join, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&c->fork.fork2, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&c->fork.join2, cudaEventDisableTiming));
     }
     c->pinnedOK = true;
     CK(cudaEventCreate(&c->ev0));
@@ -796,6 +800,9 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     c->shape.blocksDS = blocks(I0.n + I0.m + 2LL * I0.K, 256);
     c->shape.blocksX = blocks(I0.K, 128);
     c->shape.blocksY = blocks(I0.m + I0.p + I0.C, 256);
+    c->shape.blocksDN = blocks(I0.n, 256);
+    c->shape.blocksDM = blocks(I0.m, 256);
+    c->shape.blocksDMS = blocks(I0.m + 2LL * I0.K, 256);
     c->shape.blocksR = blocks(I0.m + 2LL * I0.K, 256);
     c->shape.blocksD = blocks(I0.n + I0.m, 256);
     for (int sh = 0; sh < 2; sh++) {
@@ -807,7 +814,8 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     }
     CK(cudaGetLastError());
     const int parts = std::max({c->shape.blocksA + c->shape.blocksDS, c->shape.blocksA + c->shape.blocksD,
-                                c->shape.blocksX + c->shape.blocksY + std::max(c->shape.blocksD, c->shape.blocksDS), c->gridBlocks[0],
+                                c->shape.blocksX + c->shape.blocksY + c->shape.blocksDN + std::max(c->shape.blocksDM, c->shape.blocksDMS),
+                                c->gridBlocks[0],
                                 c->gridBlocks[1]});
     CK(cudaMalloc(&c->dPart, sizeof(double) * (RS_NSUM + RX_NMAX) * size_t(parts)));
     CK(cudaMalloc(&c->dBar, 4 * sizeof(unsigned)));     // [0..1] grid barrier, [2] plain form's finishing-block counter

@@ -4,9 +4,9 @@
 #include "dr_phases.cuh"
 
 // Minimum resident blocks of 256 threads per SM asked of the large-instance kernels, i.e. their register budget
-// (65536 / (256 × blocks) registers a thread).  The kernels are bound by load latency at low occupancy: the update
-// kernel gains from 4 blocks (64 registers, a few spills) more than it loses; the element kernel, heavier in live
-// values, does best unbounded; the grid form at 2.
+// (65536 / (256 × blocks) registers a thread), each chosen by measurement on the 20 m shell: the whole element kernel
+// unbounded (the crossing code is heavy in live values), its rod half (Y) at 2, the whole update kernel at 4 (64
+// registers, a few spills), its node and segment halves (DN, DM) at 3, the grid form at 2.
 #ifndef WSB_MINB_A
 #define WSB_MINB_A 1
 #endif
@@ -15,6 +15,12 @@
 #endif
 #ifndef WSB_MINB_Y
 #define WSB_MINB_Y 2
+#endif
+#ifndef WSB_MINB_DN
+#define WSB_MINB_DN 3
+#endif
+#ifndef WSB_MINB_DM
+#define WSB_MINB_DM 3
 #endif
 #ifndef WSB_MINB_G
 #define WSB_MINB_G 2
@@ -428,29 +434,33 @@ __global__ void __launch_bounds__(256) k_plainBC(Dev<P> d, const InstDesc *__res
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 2 * I.K + I.m; e += gridDim.x * blockDim.x) phaseBC<P>(d, I, sx, e);
 }
 // The update kernel also closes the iteration: every block publishes its partials, and the last block to finish
-// (counted on `counter`) reduces the partials of phases A and D in a fixed order and takes the kinetic-damping decision.
-template <int P, bool SHORT>
-__global__ void __launch_bounds__(256, WSB_MINB_D) k_plainD(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
-                                                typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts,
-                                                int partStride, unsigned *counter) {
+// (counted on `counter` over all `nBlocks` blocks of the update phase) reduces the partials of phases A and D in a
+// fixed order and takes the kinetic-damping decision.  Every block reads the control block before it counts itself,
+// so the last block's write cannot race a reader.  The phase runs whole (PART 0) or split in two kernels on forked
+// branches: the nodes (PART 1) and the segments with the side ranks (PART 2), each at its own register budget.
+template <int P, bool SHORT, int PART>
+__device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+                                       typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts, int partStride,
+                                       unsigned *counter, unsigned nBlocks) {
   using A = typename Dev<P>::A;
   __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
   __shared__ bool last;
-  waitPrevGrid();
-  allowNextGrid();
   const InstDesc &I = insts[0];
   const InstCtl c = ctl[0];
   if (c.status != WS_RUNNING) return;
   const StepCtx sx = makeCtx<A>(I, c);
   Part<A> pt;
   pt.init();
-  const int nD = countD<SHORT>(I);
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nD; e += gridDim.x * blockDim.x) phaseD<P, SHORT>(d, I, sx, e, pt);
-  blockReduce<SUMS_UPDATE, MAXS_UPDATE>(pt, red);
+  const int nD = PART == 1 ? I.n : PART == 2 ? countD<SHORT>(I) - I.n : countD<SHORT>(I);
+  const int base = PART == 2 ? I.n : 0;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nD; e += gridDim.x * blockDim.x) phaseD<P, SHORT>(d, I, sx, base + e, pt);
+  constexpr unsigned SM = SUMS_UPDATE;
+  constexpr unsigned XM = PART == 1 ? ((1u << RX_F) | (1u << RX_LOAD)) : PART == 2 ? (1u << RX_T) : MAXS_UPDATE;
+  blockReduce<SM, XM>(pt, red);
   if (threadIdx.x == 0) {
     putPart(pt, part, blockIdx.x, partStride);
     __threadfence();
-    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    last = atomicAdd(counter, 1u) == nBlocks - 1;
   }
   __syncthreads();
   if (!last) return;
@@ -465,6 +475,26 @@ __global__ void __launch_bounds__(256, WSB_MINB_D) k_plainD(Dev<P> d, const Inst
     ctl[0] = cc;
     *counter = 0;
   }
+}
+template <int P, bool SHORT>
+__global__ void __launch_bounds__(256, WSB_MINB_D) k_plainD(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+                                                typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts,
+                                                int partStride, unsigned *counter) {
+  waitPrevGrid();
+  allowNextGrid();
+  plainD<P, SHORT, 0>(d, insts, ctl, part, partAll, nParts, partStride, counter, gridDim.x);
+}
+template <int P, bool SHORT>
+__global__ void __launch_bounds__(256, WSB_MINB_DN) k_plainDN(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+                                                  typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts,
+                                                  int partStride, unsigned *counter, unsigned nBlocks) {
+  plainD<P, SHORT, 1>(d, insts, ctl, part, partAll, nParts, partStride, counter, nBlocks);
+}
+template <int P, bool SHORT>
+__global__ void __launch_bounds__(256, WSB_MINB_DM) k_plainDM(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+                                                  typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts,
+                                                  int partStride, unsigned *counter, unsigned nBlocks) {
+  plainD<P, SHORT, 2>(d, insts, ctl, part, partAll, nParts, partStride, counter, nBlocks);
 }
 
 // ------------------------------------------------------------------------------------------------ grid form
@@ -591,9 +621,11 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
   using A = typename Dev<P>::A;
   const bool sh2 = shortSides && contacts;
   if (fork && contacts) {
-    // crossings on a forked branch, segments / joints / clamps on the main one, joined before the update
-    const int nD = sh2 ? sh.blocksDS : sh.blocksD, nParts = sh.blocksX + sh.blocksY + nD;
-    A *px = static_cast<A *>(part), *py = px + sh.blocksX, *pd = py + sh.blocksY;
+    // crossings on a forked branch, segments / joints / clamps on the main one, joined before the update; the update
+    // forks again: nodes on the side branch, segments and side ranks on the main one
+    const int nDM = sh2 ? sh.blocksDMS : sh.blocksDM, nParts = sh.blocksX + sh.blocksY + sh.blocksDN + nDM;
+    A *px = static_cast<A *>(part), *py = px + sh.blocksX, *pn = py + sh.blocksY, *pm = pn + sh.blocksDN;
+    const unsigned nB = unsigned(sh.blocksDN + nDM);
     cudaError_t e;
     if ((e = cudaEventRecord(fork->fork, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(fork->side, fork->fork, 0)) != cudaSuccess) return e;
@@ -608,9 +640,15 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
       k_plainBC<P><<<sh.blocksR, 256, 0, st>>>(d, insts, ctl);
       nl += 1;
     }
-    if (sh2) k_plainD<P, true><<<sh.blocksDS, 256, 0, st>>>(d, insts, ctl, pd, px, nParts, nParts, counter);
-    else k_plainD<P, false><<<sh.blocksD, 256, 0, st>>>(d, insts, ctl, pd, px, nParts, nParts, counter);
-    nl += 1;
+    if ((e = cudaEventRecord(fork->fork2, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(fork->side, fork->fork2, 0)) != cudaSuccess) return e;
+    if (sh2) k_plainDN<P, true><<<sh.blocksDN, 256, 0, fork->side>>>(d, insts, ctl, pn, px, nParts, nParts, counter, nB);
+    else k_plainDN<P, false><<<sh.blocksDN, 256, 0, fork->side>>>(d, insts, ctl, pn, px, nParts, nParts, counter, nB);
+    if ((e = cudaEventRecord(fork->join2, fork->side)) != cudaSuccess) return e;
+    if (sh2) k_plainDM<P, true><<<sh.blocksDMS, 256, 0, st>>>(d, insts, ctl, pm, px, nParts, nParts, counter, nB);
+    else k_plainDM<P, false><<<sh.blocksDM, 256, 0, st>>>(d, insts, ctl, pm, px, nParts, nParts, counter, nB);
+    if ((e = cudaStreamWaitEvent(st, fork->join2, 0)) != cudaSuccess) return e;
+    nl += 2;
     if (launches) *launches += nl;
     return cudaGetLastError();
   }

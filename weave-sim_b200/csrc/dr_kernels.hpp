@@ -8,10 +8,11 @@ namespace wsb {
 
 // blocks of the plain form's kernels: element phase, general side order, update phase (general order; with the side
 // ranks of the short-slide order)
-struct PlainShape { int blocksA, blocksR, blocksD, blocksDS, blocksX, blocksY; };
-// a second stream and two events: the element phase forks into a crossing kernel on `side` and a rod kernel on the
-// main stream, joined before the update kernel
-struct PlainFork { cudaStream_t side; cudaEvent_t fork, join; };
+struct PlainShape { int blocksA, blocksR, blocksD, blocksDS, blocksX, blocksY, blocksDN, blocksDM, blocksDMS; };
+// a second stream and events: the element phase forks into a crossing kernel on `side` and a rod kernel on the main
+// stream, joined before the update, which forks again into a node kernel on `side` and a segment kernel on the main
+// stream, joined at the end of the iteration
+struct PlainFork { cudaStream_t side; cudaEvent_t fork, join, fork2, join2; };
 
 template <int P>
 cudaError_t launchBatched(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
