@@ -39,6 +39,11 @@ def bytes_per_iter(n, m, K):
     return 112 * n + 168 * m + 96 * K
 
 
+# DRAM bytes (read + write) of one iteration of this workload in the mixed plain form, summed over its four kernels from
+# a cold-cache `ncu --set full` capture of one launch each (the plain-form summary under profiles/)
+TRAFFIC_PER_ITER = (5.39 + 9.79 + 6.36 + 10.74) * 1e6
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -48,7 +53,7 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs"""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms while the timed region runs"""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -59,7 +64,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                                          "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except OSError:
@@ -180,8 +185,11 @@ def run_ours(args, rank, world, local):
         "value": value, "ms_per_step": total_ms / args.steps, "launches": launches, "ctl": ctl,
         "e2e": {"value": world * args.chunk / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_kind": f"{peak_kind} hbm_gbs", "bytes_per_iter": bpi,
-                     "note": "algorithmic state bytes per DR iteration / device time per iteration (whole step)"},
+                     "traffic": TRAFFIC_PER_ITER if args.precision == "mixed" and args.form == "plain" else None,
+                     "peak_kind": f"{peak_kind} hbm_gbs", "bytes_per_iter": bpi,
+                     "note": "one DR iteration (four kernels, two pairs on forked graph branches) is the unit: algorithmic "
+                             "state bytes per iteration / device time per iteration; traffic = DRAM bytes read + written "
+                             "per iteration, summed over the four kernels from one cold-cache ncu capture"},
         "clocks": clk.summary(), "sizes": {"n": n, "m": m, "K": K},
     }
 
@@ -279,7 +287,7 @@ def run_workload(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--chunk", type=int, default=200, help="DR iterations per step")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
