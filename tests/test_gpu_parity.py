@@ -313,3 +313,28 @@ def test_node_frame_load_matches_oracle(oracle_mod, form):
     assert len(md.local_load_node) == 1
     assert ctl["iter"] == v["iteration"] and ctl["rollbacks"] == v["rollbacks"]
     assert cases.max_rel_disp_error(g["X"], v["X"], v["X0"]) < 1e-9
+
+
+def test_upload_rebuilds_side_order():
+    """ws_upload_state with new slide coordinates rebuilds the side order on the device; the short order (ranked from
+    the keys) and the general one (ranked and every slice counted), batched and plain, all continue alike"""
+    md = ws.configs.dome_small()
+    s0 = ws.GpuSolver([md.copy()], precision="f64")
+    s0.step(300)
+    st = s0.download(0)
+    s0.dispose()
+    u = st["u"].copy()
+    u[::7] = np.maximum(u[::7] - 0.6, 0.0)              # some sides move back across a segment end
+    res = []
+    for form, order in (("cta", "auto"), ("cta", "general"), ("plain", "auto"), ("plain", "general")):
+        s = ws.GpuSolver([md.copy()], precision="f64", form=form, side_order=order)
+        s.step(300)
+        s.upload_state(0, st["X"], st["Q"], u)
+        back = s.download(0, fields=("X", "u", "V"))
+        assert np.array_equal(back["u"], u) and np.array_equal(back["X"], st["X"]) and not back["V"].any()
+        s.step(200)
+        res.append(s.download(0))
+        s.dispose()
+    for r in res[1:]:
+        assert cases.max_node_err_span(r["X"], res[0]["X"], md.span) < 1e-9
+        assert np.abs(r["u"] - res[0]["u"]).max() < 1e-9

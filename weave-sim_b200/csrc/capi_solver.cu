@@ -140,6 +140,8 @@ struct ws_ctx {
   char *pinned = nullptr;
   size_t pinnedCap = 0;
   std::vector<char> pageable;
+  unsigned char *dXfer = nullptr;   // device side of uploads / downloads (contexts made by ws_create)
+  size_t xferCap = 0;
 };
 
 namespace {
@@ -157,6 +159,17 @@ char *stageBuf(ws_ctx *c, size_t bytes) {
     c->pinnedCap = bytes;
   }
   return c->pinned;
+}
+
+unsigned char *xferBuf(ws_ctx *c, size_t bytes) {
+  if (c->xferCap < bytes) {
+    if (c->dXfer) CK(cudaFree(c->dXfer));
+    c->dXfer = nullptr;
+    c->xferCap = 0;
+    CK(cudaMalloc(&c->dXfer, bytes));
+    c->xferCap = bytes;
+  }
+  return c->dXfer;
 }
 
 void flushPuts(ws_ctx *c) {
@@ -534,8 +547,42 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
   }
 }
 
+// download through the device: the requested fields are packed on the GPU in the caller's interleaved layout (the
+// buffer selection and the roll-back flag read there), copied in one piece and split into the caller's arrays
+template <int P>
+void downloadPacked(ws_ctx *c, int b, ws_state_out *o) {
+  const InstDesc &I = c->inst[b];
+  PackList L{};
+  size_t off = 0, elems = 0;
+  struct Dst { void *p; size_t off, bytes; };
+  std::vector<Dst> dst;
+  auto add = [&](int kind, int count, int ncomp, void *p, bool bytes1) {
+    if (!p || count <= 0) return;
+    PackField &F = L.f[L.nf++];
+    F.kind = kind; F.count = count; F.ncomp = ncomp; F.off = (long long)off;
+    const size_t by = size_t(count) * ncomp * (bytes1 ? 1 : sizeof(double));
+    dst.push_back({p, off, by});
+    off += (by + 15) & ~size_t(15);
+    elems = std::max(elems, size_t(count) * ncomp);
+  };
+  add(PF_X, I.n, 3, o->X, false); add(PF_Q, I.m, 4, o->Q, false); add(PF_V, I.n, 3, o->V, false);
+  add(PF_W, I.m, 3, o->W, false); add(PF_U, I.K, 2, o->u, false); add(PF_NPREV, I.K, 3, o->nprev, false);
+  add(PF_SLIP, I.K, 1, o->slip, false); add(PF_FN, I.K, 1, o->Fn, false); add(PF_FT, I.K, 1, o->Ft, false);
+  add(PF_GAP, I.K, 1, o->gap, false); add(PF_N, I.m, 1, o->N, false); add(PF_VSH, I.m, 2, o->Vsh, false);
+  add(PF_M, I.p, 3, o->M, false); add(PF_REACT, I.n, 3, o->reactions, false);
+  add(PF_STUCK, I.K, 1, o->stuck, true); add(PF_STATE, I.K, 1, o->state, true);
+  if (!L.nf) return;
+  unsigned char *dv = xferBuf(c, off);
+  CK(launchPack<P>(devOf<P>(c), c->dInst, c->dCtl, b, L, elems, dv, c->st));
+  char *h = stageBuf(c, off);
+  CK(cudaMemcpyAsync(h, dv, off, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  for (const Dst &q : dst) std::memcpy(q.p, h + q.off, q.bytes);
+}
+
 template <int P>
 void downloadImpl(ws_ctx *c, int b, ws_state_out *o) {
+  if (c->pinnedOK) { downloadPacked<P>(c, b, o); return; }
   Dev<P> &d = devOf<P>(c);
   readCtl(c);
   const InstCtl &s = c->ctlHost[b];
@@ -661,8 +708,28 @@ void loadInstanceImpl(ws_ctx *c, int b, const ws_model *md) {
   reselectOrder<P>(c);
 }
 
+// upload through the device: the caller's arrays go up as they are, one copy, and the GPU splits them into planes,
+// clears the velocities, resets the control block and (with u) rebuilds the side order from the new slide coordinates.
+// The host goals keep their older copy of the state; every consumer of it pulls the current state first.
+template <int P>
+void uploadStatePacked(ws_ctx *c, int b, const double *X, const double *Q, const double *u) {
+  const InstDesc &I = c->inst[b];
+  const size_t nX = 3 * size_t(I.n), nQ = 4 * size_t(I.m), nU = (u && I.K) ? 2 * size_t(I.K) : 0;
+  const size_t bytes = (nX + nQ + nU) * sizeof(double);
+  char *h = stageBuf(c, bytes);
+  std::memcpy(h, X, nX * sizeof(double));
+  std::memcpy(h + nX * sizeof(double), Q, nQ * sizeof(double));
+  if (nU) std::memcpy(h + (nX + nQ) * sizeof(double), u, nU * sizeof(double));
+  unsigned char *dv = xferBuf(c, bytes);
+  CK(cudaMemcpyAsync(dv, h, bytes, cudaMemcpyHostToDevice, c->st));
+  CK(launchUnpack<P>(devOf<P>(c), c->dInst, c->dCtl, b, reinterpret_cast<const double *>(dv), I.n, I.m, I.K, nU > 0, true,
+                     c->shortSides, c->st));
+  CK(cudaStreamSynchronize(c->st));
+}
+
 template <int P>
 void uploadStateImpl(ws_ctx *c, int b, const double *X, const double *Q, const double *u) {
+  if (c->pinnedOK) { uploadStatePacked<P>(c, b, X, Q, u); return; }
   HostGoals &g = c->g[b];
   readCtl(c);
   InstCtl s = c->ctlHost[b];
@@ -731,6 +798,7 @@ void destroyCtx(ws_ctx *c) {
   if (c->fork.fork2) cudaEventDestroy(c->fork.fork2);
   if (c->fork.join2) cudaEventDestroy(c->fork.join2);
   if (c->pinned) cudaFreeHost(c->pinned);
+  if (c->dXfer) cudaFree(c->dXfer);
   delete c;
 }
 

@@ -1,5 +1,7 @@
 // sm_100a kernels of the DR step: the persistent batched form (one thread block per instance, every phase of every
 // iteration inside one launch) and the plain form (one kernel per phase, one instance, captured as a CUDA graph).
+#include <algorithm>
+
 #include "dr_kernels.hpp"
 #include "dr_phases.cuh"
 
@@ -565,6 +567,123 @@ __global__ void __launch_bounds__(256, WSB_MINB_G) k_grid(Dev<P> d, const InstDe
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl[0] = sc;
 }
 
+// ------------------------------------------------------------------------------------------------ transfers
+// Upload: the caller's interleaved f64 state of instance b (X [3n], Q [4m], then u [2K] when given) goes to the device
+// as it is; this kernel splits it into the planes (two-float in the mixed policy) of the position / frame buffer the
+// control block names, clears the velocities and restarts the kinetic-damping peak.  The order of the sides is
+// rebuilt from the new slide coordinates by k_keysFromU and the ranking kernels that follow.
+template <int P>
+__global__ void __launch_bounds__(256) k_unpack(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl, int b,
+                                                const double *__restrict__ in, int withU) {
+  using R = typename Dev<P>::R; using W = typename Dev<P>::W; using U = typename Dev<P>::U;
+  const InstDesc &I = insts[b];
+  const int cur = ctl[b].cur;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+  const int nX = 3 * I.n, nQ = 4 * I.m, nU = withU ? 2 * I.K : 0;
+  for (int e = gt; e < nX; e += gs) {
+    const int i = I.n0 + e / 3, k = e % 3;
+    Acc<P>::xs(d, cur, k, i, W(in[e]));
+    d.V[size_t(k) * d.nS + i] = R(0);
+  }
+  for (int e = gt; e < nQ; e += gs) {
+    const int j = I.m0 + e / 4, k = e % 4;
+    Acc<P>::qs(d, cur, k, j, W(in[nX + e]));
+    if (k < 3) d.Wr[size_t(k) * d.mS + j] = R(0);
+  }
+  for (int e = gt; e < nU; e += gs) d.u[size_t(e % 2) * d.kS + I.k0 + e / 2] = U(in[nX + nQ + e]);
+  if (gt == 0) {
+    ctl[b].pending = 0;
+    ctl[b].ke_prev = 0.0;
+    ctl[b].status = WS_RUNNING;
+  }
+}
+// the segment each side sits on now (solver_cpu.js:144-149), from the slide coordinates, into key buffer obuf
+template <int P>
+__global__ void __launch_bounds__(256) k_keysFromU(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl, int b) {
+  using U = typename Dev<P>::U;
+  const InstDesc &I = insts[b];
+  const int ob = ctl[b].obuf;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 2 * I.K; e += gridDim.x * blockDim.x) {
+    const int c = I.k0 + e / 2, side = e % 2;
+    const U un = d.u[size_t(side) * d.kS + c];
+    const int ns = d.cxNseg[side * d.ktot + c];
+    d.sKey[size_t(ob) * d.kB + d.sPos[2 * c + side]] = int(mmin(mmax(mfloor(un), U(0)), U(mmax(ns - 1, 0))));
+  }
+}
+// the order of buffer obuf from its keys: sorted positions / keys / slices (short order) or the sorted list and every
+// segment's slice (general order)
+template <int P, bool SHORT>
+__global__ void __launch_bounds__(256) k_rankOrder(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl, int b) {
+  const InstDesc &I = insts[b];
+  const int ob = ctl[b].obuf;
+  const int n2 = 2 * I.K, nE = SHORT ? n2 : n2 + I.m;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nE; e += gridDim.x * blockDim.x) {
+    if (SHORT) rankSideShort<P>(d, 2 * I.k0 + e, ob);
+    else if (e < n2) rankSide<P>(d, 2 * I.k0 + e, ob, ob);
+    else segCount<P>(d, I.m0 + (e - n2), ob, ob);
+  }
+}
+
+// Download: the requested fields of instance b, interleaved per element as the caller's arrays are (f64, or bytes for
+// the stick / slip flags), packed one after another into `out` for a single copy to the host.
+template <int P>
+__global__ void __launch_bounds__(256) k_pack(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl, int b,
+                                              PackList L, unsigned char *__restrict__ out) {
+  const InstDesc &I = insts[b];
+  const InstCtl c = ctl[b];
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+  for (int f = 0; f < L.nf; f++) {
+    const PackField F = L.f[f];
+    const int total = F.count * F.ncomp;
+    double *od = reinterpret_cast<double *>(out + F.off);
+    unsigned char *ob = out + F.off;
+    for (int e = gt; e < total; e += gs) {
+      const int i = e / F.ncomp, k = e % F.ncomp;
+      switch (F.kind) {
+        case PF_X: od[e] = double(Acc<P>::xw(d, c.cur, k, I.n0 + i)); break;
+        case PF_Q: od[e] = double(Acc<P>::qw(d, c.cur, k, I.m0 + i)); break;
+        case PF_V: od[e] = c.pending ? 0.0 : double(d.V[size_t(k) * d.nS + I.n0 + i]); break;
+        case PF_W: od[e] = c.pending ? 0.0 : double(d.Wr[size_t(k) * d.mS + I.m0 + i]); break;
+        case PF_U: od[e] = double(d.u[size_t(k) * d.kS + I.k0 + i]); break;
+        case PF_NPREV: od[e] = double(d.nPrev[size_t(k) * d.kS + I.k0 + i]); break;
+        case PF_SLIP: od[e] = double(d.slip[I.k0 + i]); break;
+        case PF_FN: od[e] = double(d.Fn[I.k0 + i]); break;
+        case PF_FT: od[e] = double(d.Ft[I.k0 + i]); break;
+        case PF_GAP: od[e] = double(d.gap[I.k0 + i]); break;
+        case PF_N: od[e] = double(d.Nax[I.m0 + i]); break;
+        case PF_VSH: od[e] = double(d.Vsh[size_t(k) * d.mtot + I.m0 + i]); break;
+        case PF_M: od[e] = double(d.Mj[size_t(k) * d.ptot + I.p0 + i]); break;
+        case PF_REACT: od[e] = double(d.react[size_t(k) * d.ntot + I.n0 + i]); break;
+        case PF_STUCK: ob[e] = d.stuck[I.k0 + i]; break;
+        default: ob[e] = d.cstate[I.k0 + i]; break;
+      }
+    }
+  }
+}
+
+template <int P>
+cudaError_t launchUnpack(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, int b, const double *in, int n, int m, int K,
+                         bool withU, bool rebuildOrder, bool shortSides, cudaStream_t st) {
+  const int work = std::max(3 * n, std::max(4 * m, 2 * K));
+  const int blocks = std::max(1, std::min((work + 255) / 256, 148 * 8));
+  k_unpack<P><<<blocks, 256, 0, st>>>(d, insts, ctl, b, in, withU ? 1 : 0);
+  if (withU && rebuildOrder && K) {
+    const int kb = std::max(1, std::min((2 * K + 255) / 256, 148 * 8));
+    k_keysFromU<P><<<kb, 256, 0, st>>>(d, insts, ctl, b);
+    const int rb = std::max(1, std::min((2 * K + (shortSides ? 0 : m) + 255) / 256, 148 * 8));
+    if (shortSides) k_rankOrder<P, true><<<rb, 256, 0, st>>>(d, insts, ctl, b);
+    else k_rankOrder<P, false><<<rb, 256, 0, st>>>(d, insts, ctl, b);
+  }
+  return cudaGetLastError();
+}
+template <int P>
+cudaError_t launchPack(const Dev<P> &d, const InstDesc *insts, const InstCtl *ctl, int b, const PackList &L, size_t elems,
+                       unsigned char *out, cudaStream_t st) {
+  const int blocks = int(std::max<size_t>(1, std::min<size_t>((elems + 255) / 256, 148 * 8)));
+  k_pack<P><<<blocks, 256, 0, st>>>(d, insts, ctl, b, L, out);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------------------------------------ launchers
 template <int P>
 cudaError_t launchBatched(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
@@ -698,6 +817,10 @@ int gridBlocks(bool shortSides) {
   template cudaError_t launchGrid<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, unsigned *, int *, int, int, bool, \
                                      cudaStream_t);                                                                  \
   template int gridBlocks<P>(bool);                                                                                 \
+  template cudaError_t launchUnpack<P>(const Dev<P> &, const InstDesc *, InstCtl *, int, const double *, int, int, int, bool, \
+                                       bool, bool, cudaStream_t);                                                    \
+  template cudaError_t launchPack<P>(const Dev<P> &, const InstDesc *, const InstCtl *, int, const PackList &, size_t,      \
+                                     unsigned char *, cudaStream_t);                                                 \
   template cudaError_t residentPrepare<P>(size_t, bool, size_t *);                                                   \
   template cudaError_t launchResident<P>(const Dev<P> &, const InstDesc *, InstCtl *, const int *, int, int, const uint8_t *, \
                                          int, size_t, bool, cudaStream_t);

@@ -30,6 +30,16 @@ int gridBlocks(bool shortSides);
 // (*granted = bytes), else *granted = 0
 template <int P>
 cudaError_t residentPrepare(size_t bytes, bool shortSides, size_t *granted);
+// host <-> device transfers of one instance's state (interleaved per element, as the C ABI's arrays are)
+enum { PF_X, PF_Q, PF_V, PF_W, PF_U, PF_NPREV, PF_SLIP, PF_FN, PF_FT, PF_GAP, PF_N, PF_VSH, PF_M, PF_REACT, PF_STUCK, PF_STATE };
+struct PackField { int kind, count, ncomp; long long off; };   // off: byte offset in the packed buffer
+struct PackList { PackField f[16]; int nf; };
+template <int P>
+cudaError_t launchUnpack(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, int b, const double *in, int n, int m, int K,
+                         bool withU, bool rebuildOrder, bool shortSides, cudaStream_t st);
+template <int P>
+cudaError_t launchPack(const Dev<P> &d, const InstDesc *insts, const InstCtl *ctl, int b, const PackList &L, size_t elems,
+                       unsigned char *out, cudaStream_t st);
 template <int P>
 cudaError_t launchResident(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
                            const uint8_t *mask, int threads, size_t smemBytes, bool shortSides, cudaStream_t st);
