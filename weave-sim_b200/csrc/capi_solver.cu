@@ -864,13 +864,13 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     CK(cudaMemcpyAsync(c->dCtl, ctl.data(), sizeof(InstCtl) * n_instances, cudaMemcpyHostToDevice, c->st));
     const InstDesc &I0 = c->inst[0];
     auto blocks = [](long long cnt, int thr) { return int(std::max<long long>(1, std::min<long long>((cnt + thr - 1) / thr, 148LL * 8))); };
-    c->shape.blocksA = blocks(I0.m + I0.p + I0.C + I0.K, 256);
+    c->shape.blocksA = blocks(I0.m + I0.p + I0.C + 2LL * I0.K, 256);
     c->shape.blocksDS = blocks(I0.n + I0.m + 2LL * I0.K, 256);
-    c->shape.blocksX = blocks(I0.K, 128);
+    c->shape.blocksX = blocks(2LL * I0.K, 128);
     c->shape.blocksY = blocks(I0.m + I0.p + I0.C, 256);
     c->shape.blocksDN = blocks(I0.n, 256);
+    c->shape.blocksDNS = blocks(I0.n + 2LL * I0.K, 256);
     c->shape.blocksDM = blocks(I0.m, 256);
-    c->shape.blocksDMS = blocks(I0.m + 2LL * I0.K, 256);
     c->shape.blocksR = blocks(I0.m + 2LL * I0.K, 256);
     c->shape.blocksD = blocks(I0.n + I0.m, 256);
     for (int sh = 0; sh < 2; sh++) {
@@ -882,7 +882,7 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     }
     CK(cudaGetLastError());
     const int parts = std::max({c->shape.blocksA + c->shape.blocksDS, c->shape.blocksA + c->shape.blocksD,
-                                c->shape.blocksX + c->shape.blocksY + c->shape.blocksDN + std::max(c->shape.blocksDM, c->shape.blocksDMS),
+                                c->shape.blocksX + c->shape.blocksY + std::max(c->shape.blocksDN, c->shape.blocksDNS) + c->shape.blocksDM,
                                 c->gridBlocks[0],
                                 c->gridBlocks[1]});
     CK(cudaMalloc(&c->dPart, sizeof(double) * (RS_NSUM + RX_NMAX) * size_t(parts)));

@@ -48,18 +48,19 @@ __device__ __forceinline__ void addPart(Part<A> &q, const A *part, int b, int st
   for (int i = 0; i < RX_NMAX; i++) q.x[i] = mmax(q.x[i], __ldcg(part + size_t(RS_NSUM + i) * stride + b));
 }
 
-// element e of phase A: the crossings come first (the heaviest elements start earliest), then segments, joints, clamps
+// element e of phase A: the crossings come first (the heaviest elements start earliest; two adjacent elements, one a
+// side, per crossing), then segments, joints, clamps
 template <int P, bool SHORT>
 __device__ __forceinline__ void phaseA(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, int e, int nK, Part<typename Dev<P>::A> &pt) {
-  if (e < nK) { crossing<P, SHORT>(d, I, sx.cur, sx.iter, sx.onxt, sx.obuf, I.k0 + e, pt); return; }
-  e -= nK;
+  if (e < 2 * nK) { crossing<P, SHORT>(d, I, sx.cur, sx.iter, sx.onxt, sx.obuf, I.k0 + (e >> 1), e & 1, pt); return; }
+  e -= 2 * nK;
   if (e < I.m) segForce<P>(d, sx.cur, I.m0 + e, pt);
   else if ((e -= I.m) < I.p) jointTorque<P>(d, sx.cur, I.p0 + e, pt);
   else clampTorque<P>(d, sx.cur, I.c0 + (e - I.p), pt);
 }
 __device__ __forceinline__ int countA(const InstDesc &I) {
   const int nK = (I.contacts && I.K) ? I.K : 0;
-  return I.m + I.p + I.C + nK;
+  return I.m + I.p + I.C + 2 * nK;
 }
 // elements of phase D: nodes, segments and, with the short order, the ranks of the sides (the next iteration's order)
 template <bool SHORT>
@@ -88,7 +89,7 @@ __device__ __forceinline__ void phaseD(const Dev<P> &d, const InstDesc &I, const
 // per-thread partial sums, and with them every reduction, are the same from run to run.  Relative costs are rough
 // instruction counts of one element.
 struct PhaseRun { int count, cost; };
-enum { COST_CROSSING = 40, COST_RANK = 3, COST_SEGMENT = 5, COST_JOINT = 8, COST_CLAMP = 8, COST_NODE_UPD = 3,
+enum { COST_CROSSING = 24, COST_RANK = 3, COST_SEGMENT = 5, COST_JOINT = 8, COST_CLAMP = 8, COST_NODE_UPD = 3,
        COST_SEG_UPD = 5, COST_SLICE = 3 };
 
 // chunks i in [0, nc) of a run starting at cumulative cost cb whose midpoint, doubled and scaled by the warp count,
@@ -123,10 +124,10 @@ __device__ __forceinline__ void forBalanced(const PhaseRun (&runs)[NR], F &&f) {
 template <int P, bool SHORT>
 __device__ __forceinline__ void blockPhaseA(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, Part<typename Dev<P>::A> &pt) {
   const int nK = (I.contacts && I.K) ? I.K : 0;
-  const PhaseRun runs[4] = {{nK, COST_CROSSING}, {I.m, COST_SEGMENT}, {I.p, COST_JOINT}, {I.C, COST_CLAMP}};
+  const PhaseRun runs[4] = {{2 * nK, COST_CROSSING}, {I.m, COST_SEGMENT}, {I.p, COST_JOINT}, {I.C, COST_CLAMP}};
   forBalanced(runs, [&](int r, int e) {
     switch (r) {
-      case 0: crossing<P, SHORT>(d, I, sx.cur, sx.iter, sx.onxt, sx.obuf, I.k0 + e, pt); break;
+      case 0: crossing<P, SHORT>(d, I, sx.cur, sx.iter, sx.onxt, sx.obuf, I.k0 + (e >> 1), e & 1, pt); break;
       case 1: segForce<P>(d, sx.cur, I.m0 + e, pt); break;
       case 2: jointTorque<P>(d, sx.cur, I.p0 + e, pt); break;
       default: clampTorque<P>(d, sx.cur, I.c0 + e, pt); break;
@@ -396,8 +397,8 @@ __device__ __forceinline__ void plainA(const Dev<P> &d, const InstDesc *__restri
   const InstCtl c = ctl[0];
   if (c.status != WS_RUNNING) return;
   const int nK = (I.contacts && I.K) ? I.K : 0;
-  const int nA = PART == 1 ? nK : PART == 2 ? I.m + I.p + I.C : countA(I);
-  const int base = PART == 2 ? nK : 0;
+  const int nA = PART == 1 ? 2 * nK : PART == 2 ? I.m + I.p + I.C : countA(I);
+  const int base = PART == 2 ? 2 * nK : 0;
   const StepCtx sx = makeCtx<A>(I, c);
   Part<A> pt;
   pt.init();
@@ -439,7 +440,7 @@ __global__ void __launch_bounds__(256) k_plainBC(Dev<P> d, const InstDesc *__res
 // (counted on `counter` over all `nBlocks` blocks of the update phase) reduces the partials of phases A and D in a
 // fixed order and takes the kinetic-damping decision.  Every block reads the control block before it counts itself,
 // so the last block's write cannot race a reader.  The phase runs whole (PART 0) or split in two kernels on forked
-// branches: the nodes (PART 1) and the segments with the side ranks (PART 2), each at its own register budget.
+// branches: the nodes with the side ranks (PART 1) and the segments (PART 2), each at its own register budget.
 template <int P, bool SHORT, int PART>
 __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                        typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts, int partStride,
@@ -453,9 +454,14 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
   const StepCtx sx = makeCtx<A>(I, c);
   Part<A> pt;
   pt.init();
-  const int nD = PART == 1 ? I.n : PART == 2 ? countD<SHORT>(I) - I.n : countD<SHORT>(I);
-  const int base = PART == 2 ? I.n : 0;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nD; e += gridDim.x * blockDim.x) phaseD<P, SHORT>(d, I, sx, base + e, pt);
+  const int nR = countD<SHORT>(I) - I.n - I.m;
+  const int nD = PART == 1 ? I.n + nR : PART == 2 ? I.m : countD<SHORT>(I);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nD; e += gridDim.x * blockDim.x) {
+    if (PART == 0) phaseD<P, SHORT>(d, I, sx, e, pt);
+    else if (PART == 2) segUpdate<P, SHORT>(d, I, sx, I.m0 + e, pt);
+    else if (e < I.n) nodeUpdate<P, SHORT>(d, I, sx, I.n0 + e, pt);
+    else rankSideShort<P>(d, 2 * I.k0 + (e - I.n), sx.onxt);
+  }
   constexpr unsigned SM = SUMS_UPDATE;
   constexpr unsigned XM = PART == 1 ? ((1u << RX_F) | (1u << RX_LOAD)) : PART == 2 ? (1u << RX_T) : MAXS_UPDATE;
   blockReduce<SM, XM>(pt, red);
@@ -742,9 +748,9 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
   if (fork && contacts) {
     // crossings on a forked branch, segments / joints / clamps on the main one, joined before the update; the update
     // forks again: nodes on the side branch, segments and side ranks on the main one
-    const int nDM = sh2 ? sh.blocksDMS : sh.blocksDM, nParts = sh.blocksX + sh.blocksY + sh.blocksDN + nDM;
-    A *px = static_cast<A *>(part), *py = px + sh.blocksX, *pn = py + sh.blocksY, *pm = pn + sh.blocksDN;
-    const unsigned nB = unsigned(sh.blocksDN + nDM);
+    const int nDN = sh2 ? sh.blocksDNS : sh.blocksDN, nParts = sh.blocksX + sh.blocksY + nDN + sh.blocksDM;
+    A *px = static_cast<A *>(part), *py = px + sh.blocksX, *pn = py + sh.blocksY, *pm = pn + nDN;
+    const unsigned nB = unsigned(nDN + sh.blocksDM);
     cudaError_t e;
     if ((e = cudaEventRecord(fork->fork, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(fork->side, fork->fork, 0)) != cudaSuccess) return e;
@@ -761,10 +767,10 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
     }
     if ((e = cudaEventRecord(fork->fork2, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(fork->side, fork->fork2, 0)) != cudaSuccess) return e;
-    if (sh2) k_plainDN<P, true><<<sh.blocksDN, 256, 0, fork->side>>>(d, insts, ctl, pn, px, nParts, nParts, counter, nB);
+    if (sh2) k_plainDN<P, true><<<sh.blocksDNS, 256, 0, fork->side>>>(d, insts, ctl, pn, px, nParts, nParts, counter, nB);
     else k_plainDN<P, false><<<sh.blocksDN, 256, 0, fork->side>>>(d, insts, ctl, pn, px, nParts, nParts, counter, nB);
     if ((e = cudaEventRecord(fork->join2, fork->side)) != cudaSuccess) return e;
-    if (sh2) k_plainDM<P, true><<<sh.blocksDMS, 256, 0, st>>>(d, insts, ctl, pm, px, nParts, nParts, counter, nB);
+    if (sh2) k_plainDM<P, true><<<sh.blocksDM, 256, 0, st>>>(d, insts, ctl, pm, px, nParts, nParts, counter, nB);
     else k_plainDM<P, false><<<sh.blocksDM, 256, 0, st>>>(d, insts, ctl, pm, px, nParts, nParts, counter, nB);
     if ((e = cudaStreamWaitEvent(st, fork->join2, 0)) != cudaSuccess) return e;
     nl += 2;

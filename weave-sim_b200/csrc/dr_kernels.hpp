@@ -8,7 +8,7 @@ namespace wsb {
 
 // blocks of the plain form's kernels: element phase, general side order, update phase (general order; with the side
 // ranks of the short-slide order)
-struct PlainShape { int blocksA, blocksR, blocksD, blocksDS, blocksX, blocksY, blocksDN, blocksDM, blocksDMS; };
+struct PlainShape { int blocksA, blocksR, blocksD, blocksDS, blocksX, blocksY, blocksDN, blocksDNS, blocksDM; };
 // a second stream and events: the element phase forks into a crossing kernel on `side` and a rod kernel on the main
 // stream, joined before the update, which forks again into a node kernel on `side` and a segment kernel on the main
 // stream, joined at the end of the iteration

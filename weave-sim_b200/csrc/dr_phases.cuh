@@ -321,21 +321,22 @@ __device__ __forceinline__ R support(const R Rf[9], const R n[3], R sign, R w, R
 }
 
 // crossing c: one evaluation of PolylineContact.apply (solver_cpu.js:381-478) without the seat law, the augmented
-// Lagrangian and the rotational friction
+// Lagrangian and the rotational friction, by two adjacent lanes of a warp, one a side.  Each lane evaluates its side
+// (Hermite point and tangent with node tangents and frames from the neighbours, the nlerp frame); the lanes swap those
+// results with pair shuffles and both run the contact law on the same values (the same instructions on the same inputs,
+// so the same results).  Each lane writes its side's records and key; the side-0 lane writes the crossing's own
+// outputs and adds to the reductions.  Side records go to the side's strand position (general order) or, with SHORT,
+// straight to its position in this iteration's sorted order, so the gathers read them without an indirection.
 // kb: the buffer that receives the keys after the slide (the next sorted order's); ob: this iteration's sorted order.
-// Side records go to the side's strand position (general order) or, with SHORT, straight to its position in this
-// iteration's sorted order, so the gathers read them without an indirection.
 template <int P, bool SHORT>
-__device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int buf, int iter, int kb, int ob, int c, Part<typename Dev<P>::A> &pt) {
+__device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int buf, int iter, int kb, int ob, int c, int side,
+                                         Part<typename Dev<P>::A> &pt) {
   using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A; using U = typename Dev<P>::U;
   const int kt_ = d.ktot, ks = d.kS, K2 = d.sS;
+  const unsigned pair = 3u << ((threadIdx.x & 31) & 30);
   // everything the crossing reads, before anything it writes
-  const int pos[2] = {ro(d.sPos + 2 * c), ro(d.sPos + 2 * c + 1)};
-  int rec[2] = {pos[0], pos[1]};
-  if constexpr (SHORT) {
-    rec[0] = d.sInv[size_t(ob) * d.kB + pos[0]];
-    rec[1] = d.sInv[size_t(ob) * d.kB + pos[1]];
-  }
+  const int pos = ro(d.sPos + 2 * c + side);
+  const int rec = SHORT ? d.sInv[size_t(ob) * d.kB + pos] : pos;
   const R np[3] = {d.nPrev[c], d.nPrev[ks + c], d.nPrev[2 * ks + c]};
   const uint8_t fl = ro(d.cflag + c);
   const R muc = ro(d.mu + c), wkA = ro(d.wk + c), hkA = ro(d.hk + c), wkB = ro(d.wk + kt_ + c), hkB = ro(d.hk + kt_ + c);
@@ -344,20 +345,18 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   const double rampN = I.ramp_iter;
   const double rampd = rampN <= 0 ? 1.0 : fmin(1.0, 0.01 + 0.99 * double(iter) / rampN);
   const R kn = R(rampd * I.strength), kt = R(rampd * I.stick);
-  R Pl[2][3], tg[2][3], Rf[2][9], L[2], tp[2];
-  int nseg[2];
-  W xa[2][3];                           // base node of each side's segment, for the gap in the wide type
-  U uu[2];
-  #pragma unroll
-  for (int side = 0; side < 2; side++) {
-    const int o = side * kt_ + c;
-    uu[side] = d.u[side * ks + c];
-    nseg[side] = ro(d.cxNseg + o);
-    const int li = int(mmin(mmax(mfloor(uu[side]), U(0)), U(mmax(nseg[side] - 1, 0))));
-    const R t = R(mmin(mmax(uu[side] - U(li), U(0)), U(1)));
+  // this lane's side
+  const int o = side * kt_ + c;
+  U uu = d.u[side * ks + c];
+  const int nseg = ro(d.cxNseg + o);
+  R Pm[3], Tm[3], Xm[3], Ym[3], Lm, tpm;
+  W xm[3];                              // base node of the side's segment, for the gap in the wide type
+  {
+    const int li = int(mmin(mmax(mfloor(uu), U(0)), U(mmax(nseg - 1, 0))));
+    const R t = R(mmin(mmax(uu - U(li), U(0)), U(1)));
     const int sg = ro(d.cxSegOff + o) + li;
     const int a = ro(d.segI0 + sg), b = ro(d.segI1 + sg);
-    for (int k = 0; k < 3; k++) xa[side][k] = Acc<P>::xw(d, buf, k, a);
+    for (int k = 0; k < 3; k++) xm[k] = Acc<P>::xw(d, buf, k, a);
     R e[3], Ta[3], Tb[3];
     Acc<P>::edge(d, buf, a, b, e);
     const R Ls = msqrt(dot3(e, e));
@@ -367,11 +366,11 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
     const R h10 = t3 - R(2) * t2 + t, h01 = R(-2) * t3 + R(3) * t2, h11 = t3 - t2;
     const R d10 = R(3) * t2 - R(4) * t + R(1), d01 = R(-6) * t2 + R(6) * t, d11 = R(3) * t2 - R(2) * t;
     for (int k = 0; k < 3; k++) {
-      Pl[side][k] = h01 * e[k] + (h10 * Ls) * Ta[k] + (h11 * Ls) * Tb[k];
-      tg[side][k] = d01 * e[k] + (d10 * Ls) * Ta[k] + (d11 * Ls) * Tb[k];
+      Pm[k] = h01 * e[k] + (h10 * Ls) * Ta[k] + (h11 * Ls) * Tb[k];
+      Tm[k] = d01 * e[k] + (d10 * Ls) * Ta[k] + (d11 * Ls) * Tb[k];
     }
-    const R tl = mmax(msqrt(dot3(tg[side], tg[side])), R(1e-12));
-    for (int k = 0; k < 3; k++) tg[side][k] /= tl;
+    const R tl = mmax(msqrt(dot3(Tm, Tm)), R(1e-12));
+    for (int k = 0; k < 3; k++) Tm[k] /= tl;
     R qa[4], qb[4], q[4], Rn[9];
     nodeQuat<P>(d, buf, a, qa);
     nodeQuat<P>(d, buf, b, qb);
@@ -380,14 +379,32 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
     qnormalize(q);
     qframe(q, Rn);
     R y[3] = {Rn[3], Rn[4], Rn[5]};
-    const R yt = dot3(y, tg[side]);
-    for (int k = 0; k < 3; k++) y[k] -= yt * tg[side][k];
+    const R yt = dot3(y, Tm);
+    for (int k = 0; k < 3; k++) y[k] -= yt * Tm[k];
     const R yl = mmax(msqrt(dot3(y, y)), R(1e-12));
     for (int k = 0; k < 3; k++) y[k] /= yl;
-    R x[3];
-    cross3(y, tg[side], x);
-    for (int k = 0; k < 3; k++) { Rf[side][k] = x[k]; Rf[side][3 + k] = y[k]; Rf[side][6 + k] = tg[side][k]; }
-    L[side] = Ls; tp[side] = t;
+    cross3(y, Tm, Xm);
+    for (int k = 0; k < 3; k++) Ym[k] = y[k];
+    Lm = Ls; tpm = t;
+  }
+  // the partner's side, and both sides in order (selects, so every array index stays a constant)
+  R Pl[2][3], tg[2][3], Rf[2][9], L[2];
+  W xa[2][3];
+  const bool s1 = side != 0;
+  for (int k = 0; k < 3; k++) {
+    const R po = __shfl_xor_sync(pair, Pm[k], 1), to = __shfl_xor_sync(pair, Tm[k], 1);
+    const R xo = __shfl_xor_sync(pair, Xm[k], 1), yo = __shfl_xor_sync(pair, Ym[k], 1);
+    const W wo = __shfl_xor_sync(pair, xm[k], 1);
+    Pl[0][k] = s1 ? po : Pm[k]; Pl[1][k] = s1 ? Pm[k] : po;
+    tg[0][k] = s1 ? to : Tm[k]; tg[1][k] = s1 ? Tm[k] : to;
+    xa[0][k] = s1 ? wo : xm[k]; xa[1][k] = s1 ? xm[k] : wo;
+    Rf[0][k] = s1 ? xo : Xm[k]; Rf[1][k] = s1 ? Xm[k] : xo;
+    Rf[0][3 + k] = s1 ? yo : Ym[k]; Rf[1][3 + k] = s1 ? Ym[k] : yo;
+    Rf[0][6 + k] = tg[0][k]; Rf[1][6 + k] = tg[1][k];
+  }
+  {
+    const R lo = __shfl_xor_sync(pair, Lm, 1);
+    L[0] = s1 ? lo : Lm; L[1] = s1 ? Lm : lo;
   }
   const R *tA = tg[0], *tB = tg[1];
   // contact normal with side persistence (solver_cpu.js:396-402)
@@ -425,8 +442,8 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   const R eps = R(fmax(I.eps, 1e-9));
   const R da = mclamp(ca * scale, -eps, eps), db = mclamp(cb * scale, -eps, eps);
   const bool moved = slip || freeS;
-  if (moved) { uu[0] += U(da) / U(mmax(L[0], R(1e-12))); uu[1] -= U(db) / U(mmax(L[1], R(1e-12))); }
-  const U un[2] = {mclamp(uu[0], U(0), U(nseg[0])), mclamp(uu[1], U(0), U(nseg[1]))};
+  if (moved) uu += side ? -U(db) / U(mmax(L[1], R(1e-12))) : U(da) / U(mmax(L[0], R(1e-12)));
+  const U un = mclamp(uu, U(0), U(nseg));
   A slipNew = slip0;
   if (slip) {
     const R sx = da * tA[0] + db * tB[0], sy = da * tA[1] + db * tB[1], sz = da * tA[2] + db * tB[2];
@@ -443,37 +460,33 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   const R tf = R(I.tf);
   const R tfc = R(fmax(I.tf, 1e-3));
   const R kth = tfc * ((Fn + kn * R(0.25) * hc) * (R(0.5) * wc) / R(SUPPORT_SMOOTH) + kt * (R(0.5) * hc) * (R(0.5) * hc));
-  // stores
-  for (int k = 0; k < 3; k++) d.nPrev[k * ks + c] = nv[k];
-  d.u[c] = un[0];
-  d.u[ks + c] = un[1];
-  d.slip[c] = slipNew;
-  d.stuck[c] = moved ? 0 : 1;
-  d.Fn[c] = Fn;
-  d.Ft[c] = msqrt(dot3(fT, fT));
-  d.cstate[c] = slip ? 1 : 0;
-  d.gap[c] = g;
-  // the sides' segments after the slide (solver_cpu.js:144-149): the keys of the next sort, into key buffer kb
-  #pragma unroll
-  for (int side = 0; side < 2; side++) {
-    const int key = int(mmin(mmax(mfloor(un[side]), U(0)), U(mmax(nseg[side] - 1, 0))));
-    d.sKey[size_t(kb) * d.kB + pos[side]] = key;
-    if constexpr (SHORT) d.sKeyS[rec[side]] = key;
+  // stores: the crossing's own outputs from the side-0 lane, each side's slide coordinate, key and records from its lane
+  if (side == 0) {
+    for (int k = 0; k < 3; k++) d.nPrev[k * ks + c] = nv[k];
+    d.slip[c] = slipNew;
+    d.stuck[c] = moved ? 0 : 1;
+    d.Fn[c] = Fn;
+    d.Ft[c] = msqrt(dot3(fT, fT));
+    d.cstate[c] = slip ? 1 : 0;
+    d.gap[c] = g;
+    pt.s[RS_PEN] += A(active ? kn * pen * pen : R(0));
+    pt.s[RS_TAN] += A(dot3(Se, Se));
+    pt.x[RX_FN] = mmax(pt.x[RX_FN], A(Fn));
   }
-  #pragma unroll
-  for (int side = 0; side < 2; side++) {
-    const int q = rec[side];
+  d.u[side * ks + c] = un;
+  // the side's segment after the slide (solver_cpu.js:144-149): the key of the next sort, into key buffer kb
+  const int key = int(mmin(mmax(mfloor(un), U(0)), U(mmax(nseg - 1, 0))));
+  d.sKey[size_t(kb) * d.kB + pos] = key;
+  if constexpr (SHORT) d.sKeyS[rec] = key;
+  {
     const R sgn = side ? R(-1) : R(1);
     const R F[3] = {sgn * FA[0], sgn * FA[1], sgn * FA[2]};
     R tq[3];
     cross3(side ? rB : rA, F, tq);
-    d.sT[q] = tp[side];
-    d.kth[q] = kth;
-    for (int k = 0; k < 3; k++) { d.sF[k * K2 + q] = F[k]; d.sTq[k * K2 + q] = tf * tq[k]; }
+    d.sT[rec] = tpm;
+    d.kth[rec] = kth;
+    for (int k = 0; k < 3; k++) { d.sF[k * K2 + rec] = F[k]; d.sTq[k * K2 + rec] = tf * tq[k]; }
   }
-  pt.s[RS_PEN] += A(active ? kn * pen * pen : R(0));
-  pt.s[RS_TAN] += A(dot3(Se, Se));
-  pt.x[RX_FN] = mmax(pt.x[RX_FN], A(Fn));
 }
 
 // ------------------------------------------------------------------------------------------------ phase B / C
