@@ -61,6 +61,8 @@ typedef struct ws_params {
                              many iterations, linearly (0: at the first iteration).  An extension: the reference's
                              anchors hold the position they have (solver_cpu.js:764,781). */
   double slip_rate;       /* CONTACT.slip_rate 1.0 */
+  double edge_threshold;  /* CONTACT.edge_threshold 0.5: a side bears on an edge when |tanh(n·X/0.03) tanh(n·Y/0.03)| exceeds
+                             it (W1 classification, solver_cpu.js:231-271) */
 } ws_params;
 
 /* The model of one instance: the flat state of buildState (web/js/model.js:10-75), the section stiffness per segment
@@ -97,6 +99,9 @@ typedef struct ws_model {
   const uint8_t *cross_enabled;    /* [K] */
   const uint8_t *cross_locked;     /* [K] */
   const double *cross_mu;          /* [K] Coulomb coefficient per crossing (the reference has one contact.mu) */
+  const double *cross_fc90, *cross_E90, *cross_H;  /* [2K] timber of each side across the grain: crushing strength,
+                                        modulus, hardness (PolylineContact's matOf, solver_cpu.js:71-76); NULL: the
+                                        reference's defaults 8, 800, 30 (N/mm²) */
   ws_params params;
 } ws_model;
 
@@ -235,6 +240,14 @@ typedef struct ws_state_out {
   double *Vsh;     /* [2m] shear forces */
   double *M;       /* [3p] joint moments */
   double *reactions; /* [3n] */
+  /* W1 classification of the last evaluation (PolylineContact._classify, solver_cpu.js:231-271; buildResults,
+   * solver_cpu.js:903-905) */
+  uint8_t *ctype;  /* [K] 0 face-face, 1 edge-face, 2 edge-edge */
+  double *theta;   /* [K] crossing angle asin|t_A × t_B| */
+  double *phi;     /* [2K] roll of each side's section against the contact plane */
+  double *area;    /* [K] nominal contact area */
+  double *pressure;/* [K] */
+  double *util;    /* [K] pressure against hardness (face-face), fc90 (edge-face) or 1 (edge-edge) */
 } ws_state_out;
 int ws_download(ws_ctx *ctx, int32_t instance, ws_state_out *out);
 /* Uploads positions and frames (and zeroes velocities) of one instance from host buffers: a warm start from a state the

@@ -262,6 +262,9 @@ struct Contact {
   std::vector<double> wk, hk, w, h, mu;
   std::vector<uint8_t> locked, enabled;
   std::vector<double> Fn, Ft, state, gap, mid, Tn, Qn;
+  std::vector<double> fc90, E90, Hs;                     // [2K] timber across the grain (solver_cpu.js:71-76)
+  std::vector<int> ctype, faceSide;                      // W1 outputs (solver_cpu.js:87-88)
+  std::vector<double> phi, theta, Anom, pressure, util;
   double energy = 0, ramp = 1.0;
   Side ev[2];
 
@@ -276,6 +279,10 @@ struct Contact {
     locked.assign(md.cross_locked, md.cross_locked + K);
     enabled.assign(md.cross_enabled, md.cross_enabled + K);
     mu.assign(md.cross_mu, md.cross_mu + K);
+    auto side = [&](const double *a, double dflt) { return a ? std::vector<double>(a, a + 2 * K) : std::vector<double>(2 * size_t(K), dflt); };
+    fc90 = side(md.cross_fc90, 8.0); E90 = side(md.cross_E90, 800.0); Hs = side(md.cross_H, 30.0);
+    ctype.assign(K, 0); faceSide.assign(K, -1); phi.assign(2 * size_t(K), 0); theta.assign(K, 0);
+    Anom.assign(K, 0); pressure.assign(K, 0); util.assign(K, 0);
     Fn.assign(K, 0); Ft.assign(K, 0); state.assign(K, 0); gap.assign(K, 0); mid.assign(3 * size_t(K), 0);
     energy = 0; ramp = 1.0;
     ev[0].resize(K); ev[1].resize(K);
@@ -420,6 +427,52 @@ struct Contact {
     for (int k = 0; k < 3; k++) r[k] = ax * Xa[k] + ay * Ya[k];
     return hh;
   }
+  // W1: contact type per crossing from the roll of each section against the contact plane n (solver_cpu.js:231-271)
+  void classify(const std::vector<double> &n) {
+    const Side &A = ev[0], &B = ev[1];
+    std::vector<double> cFace(2 * size_t(K)), Z0(2 * size_t(K));
+    std::vector<uint8_t> edge(2 * size_t(K));
+    for (int c = 0; c < K; c++) {
+      for (int side = 0; side < 2; side++) {
+        const double *R = side == 0 ? &A.R[9 * size_t(c)] : &B.R[9 * size_t(c)];
+        const double sg = side == 0 ? 1.0 : -1.0;
+        const size_t i = 2 * size_t(c) + side;
+        const double *nc = &n[3 * size_t(c)];
+        const double nx = (nc[0] * R[0] + nc[1] * R[1] + nc[2] * R[2]) * sg;
+        const double ny = (nc[0] * R[3] + nc[1] * R[4] + nc[2] * R[5]) * sg;
+        const double sx = std::fabs(std::tanh(nx / SUPPORT_SMOOTH)), sy = std::fabs(std::tanh(ny / SUPPORT_SMOOTH));
+        edge[i] = sx * sy > p.edge_threshold ? 1 : 0;
+        const bool yFace = std::fabs(ny) >= std::fabs(nx);
+        cFace[i] = yFace ? wk[i] : hk[i];
+        Z0[i] = yFace ? hk[i] : wk[i];
+        phi[i] = std::atan(std::min(std::fabs(nx), std::fabs(ny)) / std::max(std::max(std::fabs(nx), std::fabs(ny)), 1e-12));
+      }
+      const double *tA = &A.t[3 * size_t(c)], *tB = &B.t[3 * size_t(c)];
+      const double cr[3] = {tA[1] * tB[2] - tA[2] * tB[1], tA[2] * tB[0] - tA[0] * tB[2], tA[0] * tB[1] - tA[1] * tB[0]};
+      const double sinT = std::min(std::max(std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]), 1e-6), 1.0);
+      theta[c] = std::asin(sinT);
+      const int nEdge = edge[2 * size_t(c)] + edge[2 * size_t(c) + 1];
+      ctype[c] = nEdge;
+      faceSide[c] = nEdge == 1 ? (edge[2 * size_t(c) + 1] ? 0 : 1) : -1;
+      const double fn = std::fabs(Fn[c]);
+      double Aa = cFace[2 * size_t(c)] * cFace[2 * size_t(c) + 1] / sinT, pres = fn / std::max(Aa, 1e-12);
+      double ut = pres / std::max(std::min(Hs[2 * size_t(c)], Hs[2 * size_t(c) + 1]), 1e-12);
+      if (nEdge == 1) {
+        const int fs = faceSide[c], es = 1 - fs;
+        const double ell = cFace[2 * size_t(c) + fs] / sinT, kap = E90[2 * size_t(c) + fs] / std::max(Z0[2 * size_t(c) + fs], 1e-12);
+        const double phiE = std::max(phi[2 * size_t(c) + es], 1e-4);
+        const double b = std::sqrt(2.0 * fn / std::max(ell * kap * phiE, 1e-12));
+        const bool full = b >= cFace[2 * size_t(c) + es];
+        const double Afe = full ? cFace[2 * size_t(c)] * cFace[2 * size_t(c) + 1] / sinT : b * ell;
+        const double pfe = full ? fn / std::max(Afe, 1e-12) : kap * phiE * b;
+        Aa = Afe; pres = pfe; ut = pfe / std::max(fc90[2 * size_t(c) + es], 1e-12);
+      } else if (nEdge == 2) {
+        const double fc = std::min(fc90[2 * size_t(c)], fc90[2 * size_t(c) + 1]);
+        Aa = fn / std::max(fc, 1e-12); pres = fc * (fn > 0 ? 1 : 0); ut = fn > 0 ? 1.0 : 0.0;
+      }
+      Anom[c] = Aa; pressure[c] = pres; util[c] = ut;
+    }
+  }
   // solver_cpu.js:381-478 (seat law, augmented Lagrangian and rotational friction off)
   void apply(St &st, double *F, double *T) {
     if (!K) return;
@@ -484,6 +537,7 @@ struct Contact {
       ePen[c] = active ? kn * pen * pen : 0.0;
       eTan[c] = Se[0] * Se[0] + Se[1] * Se[1] + Se[2] * Se[2];
     }
+    classify(nA);                                        // solver_cpu.js:460
     for (int c = 0; c < K; c++) { const size_t i = A.a[c]; const double wt = 1 - A.tp[c]; for (int k = 0; k < 3; k++) F[3 * i + k] += wt * FA[3 * size_t(c) + k]; }
     for (int c = 0; c < K; c++) { const size_t i = A.b[c]; const double wt = A.tp[c]; for (int k = 0; k < 3; k++) F[3 * i + k] += wt * FA[3 * size_t(c) + k]; }
     for (int c = 0; c < K; c++) { const size_t i = B.a[c]; const double wt = 1 - B.tp[c]; for (int k = 0; k < 3; k++) F[3 * i + k] += wt * FB[3 * size_t(c) + k]; }
@@ -737,6 +791,8 @@ struct orc_view {
   double e_stretch, e_shear, e_bend, e_twist, e_contact;
   double *X, *X0, *V, *Q, *W, *u, *nprev, *slip, *Fn, *Ft, *gap, *state, *N, *Vsh, *M, *reactions, *mass, *inertia3, *k_rot_static, *F, *T, *tm;
   uint8_t *stuck;
+  int32_t *ctype;
+  double *theta, *phi, *area, *pressure, *util;
 };
 
 void *orc_create(const ws_model *md) {
@@ -765,6 +821,9 @@ void orc_view_get(void *h, orc_view *v) {
   v->u = st.u.data(); v->nprev = st.nPrev.data(); v->slip = st.slip.data(); v->stuck = st.stuck.data();
   v->Fn = s->hasContact ? s->contact.Fn.data() : nullptr; v->Ft = s->hasContact ? s->contact.Ft.data() : nullptr;
   v->gap = s->hasContact ? s->contact.gap.data() : nullptr; v->state = s->hasContact ? s->contact.state.data() : nullptr;
+  v->ctype = s->hasContact ? s->contact.ctype.data() : nullptr; v->theta = s->hasContact ? s->contact.theta.data() : nullptr;
+  v->phi = s->hasContact ? s->contact.phi.data() : nullptr; v->area = s->hasContact ? s->contact.Anom.data() : nullptr;
+  v->pressure = s->hasContact ? s->contact.pressure.data() : nullptr; v->util = s->hasContact ? s->contact.util.data() : nullptr;
   v->N = s->rod.N.data(); v->Vsh = s->rod.Vs.data(); v->M = s->rod.M.data(); v->reactions = s->reactions.data();
   v->mass = s->mass.data(); v->inertia3 = s->inertia3.data(); v->k_rot_static = s->kRotStatic.data();
   v->F = s->F.data(); v->T = s->T.data(); v->tm = s->tm.data();

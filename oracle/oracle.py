@@ -24,7 +24,8 @@ class OrcView(C.Structure):
                                           "e_stretch", "e_shear", "e_bend", "e_twist", "e_contact")] + \
                [(k, _dp) for k in ("X", "X0", "V", "Q", "W", "u", "nprev", "slip", "Fn", "Ft", "gap", "state", "N",
                                    "Vsh", "M", "reactions", "mass", "inertia3", "k_rot_static", "F", "T", "tm")] + \
-               [("stuck", C.POINTER(C.c_uint8))]
+               [("stuck", C.POINTER(C.c_uint8)), ("ctype", C.POINTER(C.c_int32))] + \
+               [(k, _dp) for k in ("theta", "phi", "area", "pressure", "util")]
 
 
 _lib = None
@@ -118,6 +119,11 @@ class Oracle:
             out[k] = a.copy() if copy else a
         st = _arr(v.stuck, K) if K else np.zeros(0, dtype=np.uint8)
         out["stuck"] = np.array(st, dtype=np.uint8)
+        hc = K and v.has_contact
+        out["ctype"] = np.ctypeslib.as_array(v.ctype, shape=(K,)).astype(np.uint8) if hc else np.zeros(0, dtype=np.uint8)
+        for k, s_ in (("theta", K), ("phi", 2 * K), ("area", K), ("pressure", K), ("util", K)):
+            a = _arr(getattr(v, k), s_) if hc else np.zeros(0)
+            out[k] = a.copy() if copy else a
         return out
 
     def rod_eval(self, X, Q):

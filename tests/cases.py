@@ -43,14 +43,18 @@ def timoshenko(direction=2, P=10.0, L=1000.0, w=60.0, h=30.0):
     return P * L ** 3 / (3 * E_MM * I) + P * L / (KAPPA * G_MM * w * h)
 
 
-def crossing(load=-50.0, pull=0.0, mu=0.35, freeB=True, nseg=10, L=1000.0, h=30.0, locked=False, local=False, **prm):
+def crossing(load=-50.0, pull=0.0, mu=0.35, freeB=True, nseg=10, L=1000.0, h=30.0, locked=False, local=False, roll=(0.0, 0.0),
+             **prm):
     P = np.array([[-L / 2 + L * i / nseg, 0.0, 0.0] for i in range(nseg + 1)])
     PB = np.array([[0.0, -L / 2 + L * i / nseg, h] for i in range(nseg + 1)])
     mid = nseg // 2
     fixA = ws.mask(1, 1, 1, 0, 0, 1)
     fixB = ws.mask(0, 1, 1, 0, 0, 1) if freeB else fixA
     prm.setdefault("max_iter", 20000)
-    md = ws.polylines([P, PB], knot_rows=[[0, mid, nseg], [0, mid, nseg]], knots=[((0, 1), (1, 1))],
+    # section normals: z, rolled by roll[s] radians about the lath's own axis (A runs along x, B along y)
+    nA = np.tile([0.0, -math.sin(roll[0]), math.cos(roll[0])], (nseg + 1, 1))
+    nB = np.tile([math.sin(roll[1]), 0.0, math.cos(roll[1])], (nseg + 1, 1))
+    md = ws.polylines([P, PB], normals=[nA, nB], knot_rows=[[0, mid, nseg], [0, mid, nseg]], knots=[((0, 1), (1, 1))],
                       anchors=[((0, 0), fixA), ((0, 2), fixA), ((1, 0), fixB), ((1, 2), fixB)],
                       loads=[((1, 1), (pull, 0.0, load), local)], mu=mu, E=E_MM, G=G_MM, params=mm_params(**prm))
     if locked:

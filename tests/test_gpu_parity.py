@@ -6,6 +6,8 @@ Tolerances, per precision policy:
   (the reference's published GPU-vs-CPU band at convergence is 3–6e-4, web/README.md:79-80); gridshell trajectory
   max node error < 1e-5 · span (the acceptance gate is 1e-4 · span).
 """
+import math
+
 import numpy as np
 import pytest
 
@@ -344,3 +346,40 @@ def test_upload_rebuilds_side_order():
     for r in res[1:]:
         assert cases.max_node_err_span(r["X"], res[0]["X"], md.span) < 1e-9
         assert np.abs(r["u"] - res[0]["u"]).max() < 1e-9
+
+
+@pytest.mark.parametrize("roll,ctype", [((0.0, 0.0), 0), ((0.0, 40.0), 1), ((40.0, 0.0), 1), ((40.0, 40.0), 2)])
+@pytest.mark.parametrize("form", ["cta", "plain", "grid"])
+def test_classification_matches_oracle(oracle_mod, roll, ctype, form):
+    """the W1 contact type, crossing angle, section rolls, contact area, pressure and utilisation of a crossing of two
+    laths rolled about their axes (face on face, edge on face either way, edge on edge), computed on the device from
+    the last evaluation (PolylineContact._classify, solver_cpu.js:231-271)"""
+    md = cases.crossing(-50.0, 0.0, roll=tuple(math.radians(r) for r in roll))
+    v = oracle_mod.Oracle(md.copy()).run(3000)
+    ctl, g = _gpu(md, "f64", form)
+    assert ctl["iter"] == v["iteration"]
+    assert v["ctype"][0] == ctype and np.array_equal(g["ctype"], v["ctype"])
+    # theta = asin(|tA × tB|) loses half the digits near a right angle: the sine is compared
+    assert np.allclose(np.sin(g["theta"]), np.sin(v["theta"]), rtol=1e-9, atol=0.0)
+    for k in ("area", "pressure", "util"):
+        assert np.allclose(g[k], v[k], rtol=1e-9, atol=0.0), k
+    assert np.allclose(g["phi"], v["phi"], rtol=1e-9, atol=1e-10)
+
+
+def test_classification_gridshell_matches_oracle(oracle_mod):
+    """every crossing of the small dome after 1000 iterations: the device classification equals the oracle's"""
+    md = ws.configs.dome_small()
+    o = oracle_mod.Oracle(md.copy())
+    o.step(1000)
+    v = o.view()
+    s = ws.GpuSolver([md.copy()], precision="f64")
+    s.step(1000)
+    g = s.download(0, fields=("ctype", "theta", "phi", "area", "pressure", "util", "Fn"))
+    s.dispose()
+    assert np.abs(g["Fn"] - v["Fn"]).max() < 1e-9 * np.abs(v["Fn"]).max()
+    assert np.array_equal(g["ctype"], v["ctype"])
+    assert np.abs(np.sin(g["theta"]) - np.sin(v["theta"])).max() < 1e-9
+    for k in ("area", "pressure", "util"):
+        scale = np.abs(v[k]).max()
+        assert np.abs(g[k] - v[k]).max() < 1e-8 * scale, k
+    assert np.abs(g["phi"] - v["phi"]).max() < 1e-8

@@ -143,3 +143,43 @@ def test_crossing_cases(oracle_mod):
     o = oracle_mod.Oracle(cases.crossing(-50.0, 12.0, locked=True))
     v = o.run(6000)
     assert v["converged"] and v["slip"][0] == 0 and abs(v["Ft"][0] - 12.0) < 0.1
+
+
+# ------------------------------------------------------------------------------------------------ W1 classification
+# PolylineContact._classify (solver_cpu.js:231-271): laths crossing flat at right angles bear face on face; a lath
+# rolled about its own axis (here 40°) bears on an edge of its section; two rolled laths bear edge on edge.
+def _classified(oracle_mod, roll):
+    md = cases.crossing(-50.0, 0.0, roll=roll)
+    v = oracle_mod.Oracle(md.copy()).run(3000)
+    return md, v
+
+
+def test_classification_face_on_face(oracle_mod):
+    md, v = _classified(oracle_mod, (0.0, 0.0))
+    assert v["ctype"][0] == 0
+    assert abs(v["theta"][0] - math.pi / 2) < 1e-6
+    assert np.all(np.abs(v["phi"]) < 1e-3)
+    assert abs(v["area"][0] - 60.0 * 60.0 / math.sin(v["theta"][0])) < 1e-9 * 3600
+    assert abs(v["pressure"][0] - abs(v["Fn"][0]) / v["area"][0]) < 1e-12
+    assert abs(v["util"][0] - v["pressure"][0] / 30.0) < 1e-12
+
+
+def test_classification_edge_on_face(oracle_mod):
+    md, v = _classified(oracle_mod, (0.0, math.radians(40.0)))
+    assert v["ctype"][0] == 1
+    assert abs(v["phi"][1] - math.radians(40.0)) < 0.02          # the rolled side's section (it turns back ~0.6° under load)
+    # the edge's embedment into the face side (A: face width 60, depth 30, E90 800), edge side B (fc90 8)
+    Fn, sinT = abs(v["Fn"][0]), math.sin(v["theta"][0])
+    ell, kap, phiE = 60.0 / sinT, 800.0 / 30.0, max(v["phi"][1], 1e-4)
+    b = math.sqrt(2.0 * Fn / (ell * kap * phiE))
+    area = 60.0 * 60.0 / sinT if b >= 60.0 else b * ell
+    pres = Fn / area if b >= 60.0 else kap * phiE * b
+    assert abs(v["area"][0] - area) < 1e-9 * area and abs(v["pressure"][0] - pres) < 1e-9 * pres
+    assert abs(v["util"][0] - pres / 8.0) < 1e-9 * pres
+
+
+def test_classification_edge_on_edge(oracle_mod):
+    md, v = _classified(oracle_mod, (math.radians(40.0), math.radians(40.0)))
+    assert v["ctype"][0] == 2
+    Fn = abs(v["Fn"][0])
+    assert Fn > 0 and abs(v["area"][0] - Fn / 8.0) < 1e-12 * Fn and v["pressure"][0] == 8.0 and v["util"][0] == 1.0

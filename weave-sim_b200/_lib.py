@@ -30,7 +30,7 @@ class WsParams(C.Structure):
                 ("kinetic_damping", C.c_int32), ("warmup_iter", C.c_int32), ("max_iter", C.c_int32),
                 ("contacts", C.c_int32), ("strength", C.c_double), ("stick_strength", C.c_double),
                 ("torsion_factor", C.c_double), ("epsilon", C.c_double), ("ramp_iter", C.c_int32),
-                ("disp_ramp_iter", C.c_int32), ("slip_rate", C.c_double)]
+                ("disp_ramp_iter", C.c_int32), ("slip_rate", C.c_double), ("edge_threshold", C.c_double)]
 
 
 PARAM_KEYS = [f[0] for f in WsParams._fields_ if not f[0].startswith("pad")]
@@ -46,7 +46,8 @@ class WsModel(C.Structure):
                 ("local_load_node", _ip), ("local_load_F", _dp), ("anchor_node", _ip), ("anchor_mask", _bp),
                 ("anchor_target", _dp),
                 ("cross_strand", _ip), ("cross_wk", _dp), ("cross_hk", _dp), ("cross_u", _dp), ("cross_nprev", _dp),
-                ("cross_enabled", _bp), ("cross_locked", _bp), ("cross_mu", _dp), ("params", WsParams)]
+                ("cross_enabled", _bp), ("cross_locked", _bp), ("cross_mu", _dp),
+                ("cross_fc90", _dp), ("cross_E90", _dp), ("cross_H", _dp), ("params", WsParams)]
 
 
 class WsKagomeCfg(C.Structure):
@@ -84,7 +85,8 @@ class WsOpts(C.Structure):
 class WsStateOut(C.Structure):
     _fields_ = [(k, _dp) for k in ("X", "Q", "V", "W", "u", "nprev", "slip")] + \
                [("stuck", _bp), ("state", _bp)] + \
-               [(k, _dp) for k in ("Fn", "Ft", "gap", "N", "Vsh", "M", "reactions")]
+               [(k, _dp) for k in ("Fn", "Ft", "gap", "N", "Vsh", "M", "reactions")] + \
+               [("ctype", _bp)] + [(k, _dp) for k in ("theta", "phi", "area", "pressure", "util")]
 
 
 _lib = None
@@ -175,11 +177,12 @@ class Model:
     built from them (loads, anchors, stiffness, parameters)."""
 
     FLOAT = ("X", "X0", "Q", "l0", "joint_len", "omega0", "EA", "EIx", "EIy", "GJ", "GA", "load_const",
-             "local_load_F", "cross_wk", "cross_hk", "cross_u", "cross_nprev", "cross_mu", "anchor_target")
+             "local_load_F", "cross_wk", "cross_hk", "cross_u", "cross_nprev", "cross_mu", "anchor_target",
+             "cross_fc90", "cross_E90", "cross_H")
     INT = ("seg_i0", "seg_i1", "seg_offset", "joint_seg0", "joint_seg1", "local_load_node", "anchor_node",
            "cross_strand")
     BYTE = ("anchor_mask", "cross_enabled", "cross_locked")
-    OPTIONAL = ("omega0", "anchor_target")      # NULL in the C struct: None here
+    OPTIONAL = ("omega0", "anchor_target", "cross_fc90", "cross_E90", "cross_H")   # NULL in the C struct: None here
 
     def __init__(self):
         self.n = self.m = self.p = self.n_strands = self.K = 0
@@ -199,7 +202,7 @@ class Model:
                  "seg_i0": self.m, "seg_i1": self.m, "seg_offset": self.n_strands + 1, "joint_seg0": self.p,
                  "joint_seg1": self.p, "local_load_node": nl, "anchor_node": na, "cross_strand": 2 * self.K,
                  "anchor_mask": na, "cross_enabled": self.K, "cross_locked": self.K,
-                 "anchor_target": 3 * na}
+                 "anchor_target": 3 * na, "cross_fc90": 2 * self.K, "cross_E90": 2 * self.K, "cross_H": 2 * self.K}
         for k, dt in [(k, np.float64) for k in cls.FLOAT] + [(k, np.int32) for k in cls.INT] + \
                      [(k, np.uint8) for k in cls.BYTE]:
             ptr, n = getattr(md, k), sizes[k]

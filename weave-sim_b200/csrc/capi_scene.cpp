@@ -31,7 +31,7 @@ void ws_params_default(ws_params *p) {
   std::memset(p, 0, sizeof(*p));
   p->mass_scale = 1.5; p->damping = 1.0; p->tol = 1e-4; p->kinetic_damping = 1; p->warmup_iter = 300; p->max_iter = 5000;
   p->contacts = 1; p->strength = 1e7; p->stick_strength = 1e7; p->torsion_factor = 1.0; p->epsilon = 0.015;
-  p->ramp_iter = 1500; p->slip_rate = 1.0;
+  p->ramp_iter = 1500; p->slip_rate = 1.0; p->edge_threshold = 0.5;
 }
 
 int ws_scene_kagome(const ws_kagome_cfg *cfg, ws_scene **out) {

@@ -73,6 +73,9 @@ void layout(Dev<P> &d, Carver &cv, const Sizes &z) {
   d.kth = cv.take<R>(2 * k); d.sF = cv.take<R>(6 * k); d.sTq = cv.take<R>(6 * k);
   d.stSideOff = cv.take<int>(s); d.stSideCnt = cv.take<int>(s); d.stSegOff = cv.take<int>(s);
   d.ord = cv.take<int>(4 * k); d.ordSeg = cv.take<int>(4 * k);
+  d.fc90 = cv.take<R>(2 * k); d.E90 = cv.take<R>(2 * k); d.Hs = cv.take<R>(2 * k); d.sProj = cv.take<R>(4 * k); d.sinT = cv.take<R>(k);
+  d.ctype = cv.take<uint8_t>(k); d.theta = cv.take<R>(k); d.area = cv.take<R>(k); d.pres = cv.take<R>(k);
+  d.util = cv.take<R>(k); d.phiS = cv.take<R>(2 * k);
 }
 
 // host -> device with conversion, batched: put() converts into a host buffer and queues the copy; flushPuts() sends the
@@ -244,6 +247,7 @@ InstDesc describe(const HostGoals &g, const Sizes &off) {
   for (uint8_t h : g.hasLocal) I.localLoads |= h ? 1 : 0;
   I.ms = g.prm.mass_scale; I.damping = g.prm.damping; I.tol = g.prm.tol; I.strength = g.prm.strength; I.stick = g.prm.stick_strength;
   I.tf = g.prm.torsion_factor; I.eps = g.prm.epsilon; I.slip_rate = g.prm.slip_rate; I.lRef = g.lRef; I.jLenMin = g.jLenMin;
+  I.edgeThr = g.prm.edge_threshold;
   return I;
 }
 
@@ -409,8 +413,12 @@ void uploadStatic(ws_ctx *c, int b) {
   put<R>(d.jLen + I.p0, g.jLen.data(), p, st);
   for (int side = 0; side < 2; side++) {
     std::vector<int> so(K), nsg(K);
-    std::vector<double> w(K), h(K);
+    std::vector<double> w(K), h(K), fc(K), e9(K), hs(K);
     for (size_t q = 0; q < K; q++) { so[q] = I.m0 + g.cxSegOff[2 * q + side]; nsg[q] = g.cxNseg[2 * q + side]; w[q] = g.wk[2 * q + side]; h[q] = g.hk[2 * q + side]; }
+    for (size_t q = 0; q < K; q++) { fc[q] = g.fc90[2 * q + side]; e9[q] = g.E90[2 * q + side]; hs[q] = g.Hs[2 * q + side]; }
+    put<R>(d.fc90 + size_t(side) * d.ktot + I.k0, fc.data(), K, st);
+    put<R>(d.E90 + size_t(side) * d.ktot + I.k0, e9.data(), K, st);
+    put<R>(d.Hs + size_t(side) * d.ktot + I.k0, hs.data(), K, st);
     put<int>(d.cxSegOff + size_t(side) * d.ktot + I.k0, so.data(), K, st);
     put<int>(d.cxNseg + size_t(side) * d.ktot + I.k0, nsg.data(), K, st);
     put<R>(d.wk + size_t(side) * d.ktot + I.k0, w.data(), K, st);
@@ -547,6 +555,9 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
   }
 }
 
+// the W1 classification is computed on the device when a download asks for any of its outputs
+bool wantsClass(const ws_state_out *o) { return o->ctype || o->theta || o->phi || o->area || o->pressure || o->util; }
+
 // download through the device: the requested fields are packed on the GPU in the caller's interleaved layout (the
 // buffer selection and the roll-back flag read there), copied in one piece and split into the caller's arrays
 template <int P>
@@ -571,7 +582,10 @@ void downloadPacked(ws_ctx *c, int b, ws_state_out *o) {
   add(PF_GAP, I.K, 1, o->gap, false); add(PF_N, I.m, 1, o->N, false); add(PF_VSH, I.m, 2, o->Vsh, false);
   add(PF_M, I.p, 3, o->M, false); add(PF_REACT, I.n, 3, o->reactions, false);
   add(PF_STUCK, I.K, 1, o->stuck, true); add(PF_STATE, I.K, 1, o->state, true);
+  add(PF_CTYPE, I.K, 1, o->ctype, true); add(PF_THETA, I.K, 1, o->theta, false); add(PF_PHI, I.K, 2, o->phi, false);
+  add(PF_AREA, I.K, 1, o->area, false); add(PF_PRES, I.K, 1, o->pressure, false); add(PF_UTIL, I.K, 1, o->util, false);
   if (!L.nf) return;
+  if (wantsClass(o)) CK(launchClassify<P>(devOf<P>(c), c->dInst, b, I.K, c->st));
   unsigned char *dv = xferBuf(c, off);
   CK(launchPack<P>(devOf<P>(c), c->dInst, c->dCtl, b, L, elems, dv, c->st));
   char *h = stageBuf(c, off);
@@ -602,6 +616,15 @@ void downloadImpl(ws_ctx *c, int b, ws_state_out *o) {
     if (o->gap) f.planes(d.gap, 0, I.k0, K, 1, o->gap);
     if (o->stuck) f.bytes(d.stuck + I.k0, K, o->stuck);
     if (o->state) f.bytes(d.cstate + I.k0, K, o->state);
+    if (wantsClass(o)) {
+      CK(launchClassify<P>(d, c->dInst, b, I.K, c->st));
+      if (o->ctype) f.bytes(d.ctype + I.k0, K, o->ctype);
+      if (o->theta) f.planes(d.theta, 0, I.k0, K, 1, o->theta);
+      if (o->phi) f.planes(d.phiS, 0, 2 * size_t(I.k0), 2 * K, 1, o->phi);
+      if (o->area) f.planes(d.area, 0, I.k0, K, 1, o->area);
+      if (o->pressure) f.planes(d.pres, 0, I.k0, K, 1, o->pressure);
+      if (o->util) f.planes(d.util, 0, I.k0, K, 1, o->util);
+    }
   }
   if (o->N) f.planes(d.Nax, 0, I.m0, m, 1, o->N);
   if (o->Vsh) f.planes(d.Vsh, d.mtot, I.m0, m, 2, o->Vsh);

@@ -29,7 +29,7 @@ template <> struct PrecT<PREC_F32> { using R = float; using W = float; using A =
 struct InstDesc {
   int n0, n, m0, m, p0, p, c0, C, k0, K, s0, S;   // first global element and count: nodes, segments, joints, clamps, crossings, strands
   int warmup, ramp_iter, disp_ramp, kd, contacts, max_iter, localLoads;   // localLoads: some node carries a node-frame load
-  double ms, damping, tol, strength, stick, tf, eps, slip_rate, lRef, jLenMin;
+  double ms, damping, tol, strength, stick, tf, eps, slip_rate, lRef, jLenMin, edgeThr;
 };
 
 // per-instance control (device-written every iteration)
@@ -92,6 +92,12 @@ struct Dev {
   A *slip;                  // [ktot]
   uint8_t *stuck, *cstate;  // [ktot]
   R *Fn, *Ft, *gap;         // [ktot]
+  R *fc90, *E90, *Hs;       // [2][ktot] timber of each side across the grain (W1 classification)
+  R *sProj;                 // [2][2 ktot] contact normal in each side's section frame (x, y; sd = 2c + side), last evaluation
+  R *sinT;                  // [ktot] |tA × tB| clipped to [1e-6, 1] at the last evaluation
+  uint8_t *ctype;           // [ktot] W1 outputs, filled when a download asks for them
+  R *theta, *area, *pres, *util;   // [ktot]
+  R *phiS;                  // [2 ktot]
   // side records, indexed by side position p: the sides (sd = 2c + side) grouped by strand, ascending sd within a
   // strand (the strand's range is [stSideOff, stSideOff + stSideCnt))
   int *sPos;                // [2 ktot] position of side sd

@@ -630,6 +630,13 @@ __global__ void __launch_bounds__(256) k_rankOrder(Dev<P> d, const InstDesc *__r
   }
 }
 
+// the W1 classification of every crossing of instance b from its last evaluation (outputs of a download)
+template <int P>
+__global__ void __launch_bounds__(256) k_classify(Dev<P> d, const InstDesc *__restrict__ insts, int b) {
+  const InstDesc &I = insts[b];
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < I.K; e += gridDim.x * blockDim.x) classify<P>(d, I, I.k0 + e);
+}
+
 // Download: the requested fields of instance b, interleaved per element as the caller's arrays are (f64, or bytes for
 // the stick / slip flags), packed one after another into `out` for a single copy to the host.
 template <int P>
@@ -661,7 +668,13 @@ __global__ void __launch_bounds__(256) k_pack(Dev<P> d, const InstDesc *__restri
         case PF_M: od[e] = double(d.Mj[size_t(k) * d.ptot + I.p0 + i]); break;
         case PF_REACT: od[e] = double(d.react[size_t(k) * d.ntot + I.n0 + i]); break;
         case PF_STUCK: ob[e] = d.stuck[I.k0 + i]; break;
-        default: ob[e] = d.cstate[I.k0 + i]; break;
+        case PF_STATE: ob[e] = d.cstate[I.k0 + i]; break;
+        case PF_CTYPE: ob[e] = d.ctype[I.k0 + i]; break;
+        case PF_THETA: od[e] = double(d.theta[I.k0 + i]); break;
+        case PF_PHI: od[e] = double(d.phiS[2 * (I.k0 + i) + k]); break;
+        case PF_AREA: od[e] = double(d.area[I.k0 + i]); break;
+        case PF_PRES: od[e] = double(d.pres[I.k0 + i]); break;
+        default: od[e] = double(d.util[I.k0 + i]); break;
       }
     }
   }
@@ -680,6 +693,12 @@ cudaError_t launchUnpack(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, i
     if (shortSides) k_rankOrder<P, true><<<rb, 256, 0, st>>>(d, insts, ctl, b);
     else k_rankOrder<P, false><<<rb, 256, 0, st>>>(d, insts, ctl, b);
   }
+  return cudaGetLastError();
+}
+template <int P>
+cudaError_t launchClassify(const Dev<P> &d, const InstDesc *insts, int b, int K, cudaStream_t st) {
+  if (K <= 0) return cudaSuccess;
+  k_classify<P><<<std::max(1, std::min((K + 255) / 256, 148 * 8)), 256, 0, st>>>(d, insts, b);
   return cudaGetLastError();
 }
 template <int P>
@@ -827,6 +846,7 @@ int gridBlocks(bool shortSides) {
                                        bool, bool, cudaStream_t);                                                    \
   template cudaError_t launchPack<P>(const Dev<P> &, const InstDesc *, const InstCtl *, int, const PackList &, size_t,      \
                                      unsigned char *, cudaStream_t);                                                 \
+  template cudaError_t launchClassify<P>(const Dev<P> &, const InstDesc *, int, int, cudaStream_t);                \
   template cudaError_t residentPrepare<P>(size_t, bool, size_t *);                                                   \
   template cudaError_t launchResident<P>(const Dev<P> &, const InstDesc *, InstCtl *, const int *, int, int, const uint8_t *, \
                                          int, size_t, bool, cudaStream_t);

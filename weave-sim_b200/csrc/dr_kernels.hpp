@@ -31,9 +31,13 @@ int gridBlocks(bool shortSides);
 template <int P>
 cudaError_t residentPrepare(size_t bytes, bool shortSides, size_t *granted);
 // host <-> device transfers of one instance's state (interleaved per element, as the C ABI's arrays are)
-enum { PF_X, PF_Q, PF_V, PF_W, PF_U, PF_NPREV, PF_SLIP, PF_FN, PF_FT, PF_GAP, PF_N, PF_VSH, PF_M, PF_REACT, PF_STUCK, PF_STATE };
+enum { PF_X, PF_Q, PF_V, PF_W, PF_U, PF_NPREV, PF_SLIP, PF_FN, PF_FT, PF_GAP, PF_N, PF_VSH, PF_M, PF_REACT, PF_STUCK, PF_STATE,
+       PF_CTYPE, PF_THETA, PF_PHI, PF_AREA, PF_PRES, PF_UTIL };
 struct PackField { int kind, count, ncomp; long long off; };   // off: byte offset in the packed buffer
-struct PackList { PackField f[16]; int nf; };
+struct PackList { PackField f[24]; int nf; };
+// the W1 classification of instance b's crossings into the device output arrays
+template <int P>
+cudaError_t launchClassify(const Dev<P> &d, const InstDesc *insts, int b, int K, cudaStream_t st);
 template <int P>
 cudaError_t launchUnpack(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, int b, const double *in, int n, int m, int K,
                          bool withU, bool rebuildOrder, bool shortSides, cudaStream_t st);

@@ -32,6 +32,8 @@ __device__ __forceinline__ double msqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float matan2(float y, float x) { return atan2f(y, x); }
 __device__ __forceinline__ double matan2(double y, double x) { return atan2(y, x); }
 __device__ __forceinline__ float mtanh(float x) { return tanhf(x); }
+__device__ __forceinline__ float masin(float x) { return asinf(x); }
+__device__ __forceinline__ double masin(double x) { return asin(x); }
 __device__ __forceinline__ double mtanh(double x) { return tanh(x); }
 __device__ __forceinline__ void msincos(float x, float *s, float *c) { sincosf(x, s, c); }
 __device__ __forceinline__ void msincos(double x, double *s, double *c) { sincos(x, s, c); }
@@ -159,13 +161,14 @@ __device__ __forceinline__ void nodeTangent(const Dev<P> &d, int buf, int i, typ
   using R = typename Dev<P>::R;
   T[0] = T[1] = T[2] = R(0);
   const int so = ro(d.nsOut + i), si = ro(d.nsIn + i);
-  for (int j : {so, si}) {
-    if (j < 0) continue;
+  auto chord = [&](int j) {
     R e[3];
     Acc<P>::edge(d, buf, ro(d.segI0 + j), ro(d.segI1 + j), e);
     const R l = mmax(msqrt(dot3(e, e)), R(1e-12));
     for (int k = 0; k < 3; k++) T[k] += e[k] / l;
-  }
+  };
+  if (so >= 0) chord(so);
+  if (si >= 0) chord(si);
   const R l = mmax(msqrt(dot3(T, T)), R(1e-12));
   for (int k = 0; k < 3; k++) T[k] /= l;
 }
@@ -178,14 +181,15 @@ __device__ __forceinline__ void nodeQuat(const Dev<P> &d, int buf, int i, typena
   if (ref < 0) return;
   R qr[4];
   for (int k = 0; k < 4; k++) qr[k] = Acc<P>::qr(d, buf, k, ref);
-  for (int j : {so, si}) {
-    if (j < 0) continue;
+  auto add = [&](int j) {
     R qj[4];
     for (int k = 0; k < 4; k++) qj[k] = Acc<P>::qr(d, buf, k, j);
     const R dd = qj[0] * qr[0] + qj[1] * qr[1] + qj[2] * qr[2] + qj[3] * qr[3];
     const R sg = dd < R(0) ? R(-1) : R(1);
     for (int k = 0; k < 4; k++) q[k] += sg * qj[k];
-  }
+  };
+  if (so >= 0) add(so);
+  if (si >= 0) add(si);
   qnormalize(q);
 }
 
@@ -474,6 +478,13 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
     pt.x[RX_FN] = mmax(pt.x[RX_FN], A(Fn));
   }
   d.u[side * ks + c] = un;
+  {
+    // what the W1 classification needs of this evaluation: the normal in the side's section frame, the crossing angle
+    const R sg = side ? R(-1) : R(1);
+    d.sProj[2 * c + side] = dot3(nv, Xm) * sg;
+    d.sProj[2 * size_t(kt_) + 2 * c + side] = dot3(nv, Ym) * sg;
+    if (side == 0) d.sinT[c] = mmin(mmax(nn, R(1e-6)), R(1));
+  }
   // the side's segment after the slide (solver_cpu.js:144-149): the key of the next sort, into key buffer kb
   const int key = int(mmin(mmax(mfloor(un), U(0)), U(mmax(nseg - 1, 0))));
   d.sKey[size_t(kb) * d.kB + pos] = key;
@@ -487,6 +498,49 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
     d.kth[rec] = kth;
     for (int k = 0; k < 3; k++) { d.sF[k * K2 + rec] = F[k]; d.sTq[k * K2 + rec] = tf * tq[k]; }
   }
+}
+
+// W1: the contact type of crossing c from the roll of each section against the contact plane, from the normal in each
+// side's section frame, the crossing angle and the normal force of its last evaluation (PolylineContact._classify,
+// solver_cpu.js:231-271; outputs only, nothing of the iteration reads them)
+template <int P>
+__device__ __forceinline__ void classify(const Dev<P> &d, const InstDesc &I, int c) {
+  using R = typename Dev<P>::R;
+  const int kt_ = d.ktot, K2 = 2 * kt_;
+  R cFace[2], Z0[2], phi[2];
+  int edge[2];
+  for (int side = 0; side < 2; side++) {
+    const int sd = 2 * c + side, o = side * kt_ + c;
+    const R nx = d.sProj[sd], ny = d.sProj[K2 + sd];
+    const R sx = mabs(mtanh(nx / R(SUPPORT_SMOOTH))), sy = mabs(mtanh(ny / R(SUPPORT_SMOOTH)));
+    edge[side] = sx * sy > R(I.edgeThr) ? 1 : 0;
+    const bool yFace = mabs(ny) >= mabs(nx);
+    cFace[side] = yFace ? d.wk[o] : d.hk[o];
+    Z0[side] = yFace ? d.hk[o] : d.wk[o];
+    phi[side] = matan2(mmin(mabs(nx), mabs(ny)), mmax(mmax(mabs(nx), mabs(ny)), R(1e-12)));
+    d.phiS[sd] = phi[side];
+  }
+  const R sinT = d.sinT[c];
+  const int nEdge = edge[0] + edge[1];
+  const R Fn = mabs(d.Fn[c]);
+  R Aa = cFace[0] * cFace[1] / sinT, pres = Fn / mmax(Aa, R(1e-12));
+  R ut = pres / mmax(mmin(d.Hs[c], d.Hs[kt_ + c]), R(1e-12));
+  if (nEdge == 1) {
+    const int fs = edge[1] ? 0 : 1, es = 1 - fs;
+    const R ell = cFace[fs] / sinT, kap = d.E90[fs * kt_ + c] / mmax(Z0[fs], R(1e-12));
+    const R phiE = mmax(phi[es], R(1e-4));
+    const R b = msqrt(R(2) * Fn / mmax(ell * kap * phiE, R(1e-12)));
+    const bool full = b >= cFace[es];
+    const R Afe = full ? cFace[0] * cFace[1] / sinT : b * ell;
+    const R pfe = full ? Fn / mmax(Afe, R(1e-12)) : kap * phiE * b;
+    Aa = Afe; pres = pfe; ut = pfe / mmax(d.fc90[es * kt_ + c], R(1e-12));
+  } else if (nEdge == 2) {
+    const R fc = mmin(d.fc90[c], d.fc90[kt_ + c]);
+    Aa = Fn / mmax(fc, R(1e-12)); pres = Fn > R(0) ? fc : R(0); ut = Fn > R(0) ? R(1) : R(0);
+  }
+  d.ctype[c] = uint8_t(nEdge);
+  d.theta[c] = masin(sinT);
+  d.area[c] = Aa; d.pres[c] = pres; d.util[c] = ut;
 }
 
 // ------------------------------------------------------------------------------------------------ phase B / C

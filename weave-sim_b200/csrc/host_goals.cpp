@@ -72,6 +72,9 @@ void HostGoals::loadModel(const ws_model &md, bool keepState) {
   w.resize(K); h.resize(K);
   for (int c = 0; c < K; c++) { w[c] = 0.5 * (wk[2 * c] + wk[2 * c + 1]); h[c] = 0.5 * (hk[2 * c] + hk[2 * c + 1]); }
   mu = copyOf(md.cross_mu, K);
+  // N/mm² defaults of the classification (solver_cpu.js:231-271)
+  auto orDefault = [&](const double *p, double v) { return p ? copyOf(p, 2 * size_t(K)) : std::vector<double>(2 * size_t(K), v); };
+  fc90 = orDefault(md.cross_fc90, 8.0); E90 = orDefault(md.cross_E90, 800.0); Hs = orDefault(md.cross_H, 30.0);
   enabled = copyOf(md.cross_enabled, K); locked = copyOf(md.cross_locked, K);
 }
 

@@ -34,6 +34,7 @@ struct HostGoals {
   // contact
   std::vector<int> cxSegOff, cxNseg, cxStrand;       // [2K] first segment, segment count and strand of each side
   std::vector<double> wk, hk, w, h, mu;
+  std::vector<double> fc90, E90, Hs;                 // [2K] timber across the grain, each side (W1 classification)
   std::vector<uint8_t> enabled, locked;
   // goals
   std::vector<double> mass, kRotStatic;              // [n], [3m]

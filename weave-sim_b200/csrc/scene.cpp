@@ -612,6 +612,9 @@ void Scene::fillModel() {
   m.cross_strand = st.crossStrand.data(); m.cross_wk = wk.data(); m.cross_hk = hk.data();
   m.cross_u = st.u.data(); m.cross_nprev = st.nPrev.data();
   m.cross_enabled = enabled.data(); m.cross_locked = locked.data(); m.cross_mu = mu.data();
+  m.cross_fc90 = fc90.size() == 2 * size_t(st.K) && st.K ? fc90.data() : nullptr;
+  m.cross_E90 = E90.size() == 2 * size_t(st.K) && st.K ? E90.data() : nullptr;
+  m.cross_H = H.size() == 2 * size_t(st.K) && st.K ? H.data() : nullptr;
   m.params = params;
 }
 
@@ -620,6 +623,9 @@ void Scene::setUniformSection(double w, double h, double E, double G, double den
   Section s = sectionStiffness(w, h, E, G);
   EA.assign(st.m, s.EA); EIx.assign(st.m, s.EIx); EIy.assign(st.m, s.EIy); GJ.assign(st.m, s.GJ); GA.assign(st.m, s.GA);
   wk.assign(2 * size_t(st.K), w); hk.assign(2 * size_t(st.K), h);
+  // across the grain, in the proportions of the reference's default timber (params.js:6: E 10000, fc90 8, E90 800,
+  // H 30), so that any unit system of E carries over
+  fc90.assign(2 * size_t(st.K), 8e-4 * E); E90.assign(2 * size_t(st.K), 0.08 * E); H.assign(2 * size_t(st.K), 3e-3 * E);
   loadConst.assign(3 * size_t(st.n), 0.0);
   if (gravity) {
     const double g[3] = {0.0, 0.0, -1.0};

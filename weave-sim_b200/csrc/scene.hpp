@@ -91,6 +91,7 @@ struct Scene {
   Topology topo;
   State st;
   std::vector<double> EA, EIx, EIy, GJ, GA, omega0, loadConst, localF, wk, hk, mu, anchorTarget;
+  std::vector<double> fc90, E90, H;          // [2K] timber of each crossing side across the grain
   std::vector<int> localNode, anchorNode;
   std::vector<uint8_t> anchorMask, enabled, locked;
   ws_params params{};

@@ -26,19 +26,21 @@ def device_count() -> int:
     return int(lib().ws_device_count())
 
 
-STATE_FIELDS = ("X", "Q", "V", "W", "u", "nprev", "slip", "Fn", "Ft", "gap", "N", "Vsh", "M", "reactions", "stuck", "state")
+STATE_FIELDS = ("X", "Q", "V", "W", "u", "nprev", "slip", "Fn", "Ft", "gap", "N", "Vsh", "M", "reactions", "stuck", "state",
+                "ctype", "theta", "phi", "area", "pressure", "util")
 
 
 def _state_buffers(md, fields=None):
     """host arrays for one instance's state and the ws_state_out pointing at them; fields left out stay NULL"""
     n, m, p, K = md.n, md.m, md.p, md.K
     size = {"X": 3 * n, "Q": 4 * m, "V": 3 * n, "W": 3 * m, "u": 2 * K, "nprev": 3 * K, "slip": K, "Fn": K, "Ft": K,
-            "gap": K, "N": m, "Vsh": 2 * m, "M": 3 * p, "reactions": 3 * n, "stuck": K, "state": K}
+            "gap": K, "N": m, "Vsh": 2 * m, "M": 3 * p, "reactions": 3 * n, "stuck": K, "state": K,
+            "ctype": K, "theta": K, "phi": 2 * K, "area": K, "pressure": K, "util": K}
     names = STATE_FIELDS if fields is None else tuple(fields)
     bad = [k for k in names if k not in size]
     if bad:
         raise ValueError(f"unknown state fields {bad}; known: {STATE_FIELDS}")
-    out = {k: np.zeros(size[k], dtype=np.uint8 if k in ("stuck", "state") else np.float64) for k in names}
+    out = {k: np.zeros(size[k], dtype=np.uint8 if k in ("stuck", "state", "ctype") else np.float64) for k in names}
     so = WsStateOut()
     for k, a in out.items():
         ct = C.c_uint8 if a.dtype == np.uint8 else C.c_double
