@@ -63,6 +63,17 @@ typedef struct ws_params {
   double slip_rate;       /* CONTACT.slip_rate 1.0 */
   double edge_threshold;  /* CONTACT.edge_threshold 0.5: a side bears on an edge when |tanh(n·X/0.03) tanh(n·Y/0.03)| exceeds
                              it (W1 classification, solver_cpu.js:231-271) */
+  /* contact extensions (params.js:10-14); all off by default */
+  int32_t augmented;      /* CONTACT.augmented 0: augmented-Lagrangian gap, Fn = max(0, λ + k_n·pen) (solver_cpu.js:414-418) */
+  int32_t al_every;       /* CONTACT.al_every 600: Uzawa update of λ every al_every iterations after the ramp
+                             (solver_cpu.js:819-821, 484-506) */
+  int32_t rot_friction;   /* CONTACT.rot_friction 0: W2 rotational friction about the contact normal (solver_cpu.js:347-379) */
+  int32_t seat_law;       /* CONTACT.seat_law: 0 'off', 1 'L1' (W3 directional seat law, solver_cpu.js:283-344) */
+  int32_t seat_gap;       /* CONTACT.seat_gap 1: the seat depth closes the section gap (solver_cpu.js:410) */
+  int32_t dent_after_iter;/* CONTACT.dent_after_iter -1: seats form from this iteration on; -1 = warmup_iter + ramp_iter of
+                             the model the instance was created from (solver_cpu.js:329,686) */
+  double rot_factor;      /* CONTACT.rot_factor 1.0: W2 moment limit rot_factor·μ·|Fn|·r_eq */
+  double dent_rate;       /* CONTACT.dent_rate 0.01: share of the estimated seat depth added per iteration */
 } ws_params;
 
 /* The model of one instance: the flat state of buildState (web/js/model.js:10-75), the section stiffness per segment
@@ -248,6 +259,11 @@ typedef struct ws_state_out {
   double *area;    /* [K] nominal contact area */
   double *pressure;/* [K] */
   double *util;    /* [K] pressure against hardness (face-face), fc90 (edge-face) or 1 (edge-edge) */
+  /* contact extensions (buildResults, solver_cpu.js:906-908) */
+  double *lambda;  /* [K] augmented-Lagrangian multiplier λ */
+  double *dent;    /* [K] seat depth: the dents of both sides + the edge-on-face embedment */
+  double *M_rot;   /* [K] W2 scissor moment about the contact normal */
+  double *rot_slip;/* [K] accumulated W2 rotational slip [rad] */
 } ws_state_out;
 int ws_download(ws_ctx *ctx, int32_t instance, ws_state_out *out);
 /* Uploads positions and frames (and zeroes velocities) of one instance from host buffers: a warm start from a state the

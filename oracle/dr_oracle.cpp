@@ -30,6 +30,10 @@ static const double SUPPORT_SMOOTH = 0.03;
 static const double TWIST_RATE_MAX = 0.5 * SUPPORT_SMOOTH;
 static const double ROLL_DAMP = 0.5;
 static const double INF = std::numeric_limits<double>::infinity();
+static const double AL_FREE_MIN = 0.25;               // solver_cpu.js:33
+static const double PI = 3.141592653589793;           // Math.PI
+// Math.sign: −1, 0 or +1 (0 for ±0)
+static double jsSign(double v) { return v > 0 ? 1.0 : (v < 0 ? -1.0 : 0.0); }
 
 // ------------------------------------------------------------------------------------------------ quat.js
 static void qnormalize(double *q) {
@@ -265,6 +269,17 @@ struct Contact {
   std::vector<double> fc90, E90, Hs;                     // [2K] timber across the grain (solver_cpu.js:71-76)
   std::vector<int> ctype, faceSide;                      // W1 outputs (solver_cpu.js:87-88)
   std::vector<double> phi, theta, Anom, pressure, util;
+  std::vector<double> cFace;                             // [2K] contact face width of each side (the _classify result)
+  // contact extensions (solver_cpu.js:84-92): the multiplier λ (st.lam, model.js:10-75) and the penetration summed
+  // since its last update; W3 seat depths, climbs and wall slopes per side, edge-on-face embedment per crossing; W2
+  // reference angle, rotational slip and moment
+  std::vector<double> lam, penAcc;
+  int penN = 0;
+  std::vector<double> dent, climb, tanpsi, dentE, theta0, rotSlip, Mrot;
+  std::vector<uint8_t> nodeFixed;
+  std::vector<double> dentSum;                           // [K] the seat depth buildResults reports (solver_cpu.js:906)
+  double rotEnergy = 0;
+  int dentAfterDefault = 1500;
   double energy = 0, ramp = 1.0;
   Side ev[2];
 
@@ -282,7 +297,11 @@ struct Contact {
     auto side = [&](const double *a, double dflt) { return a ? std::vector<double>(a, a + 2 * K) : std::vector<double>(2 * size_t(K), dflt); };
     fc90 = side(md.cross_fc90, 8.0); E90 = side(md.cross_E90, 800.0); Hs = side(md.cross_H, 30.0);
     ctype.assign(K, 0); faceSide.assign(K, -1); phi.assign(2 * size_t(K), 0); theta.assign(K, 0);
-    Anom.assign(K, 0); pressure.assign(K, 0); util.assign(K, 0);
+    Anom.assign(K, 0); pressure.assign(K, 0); util.assign(K, 0); cFace.assign(2 * size_t(K), 0);
+    lam.assign(K, 0); penAcc.assign(K, 0); penN = 0;
+    dent.assign(2 * size_t(K), 0); climb.assign(2 * size_t(K), 0); tanpsi.assign(2 * size_t(K), 1.0); dentE.assign(K, 0);
+    theta0.assign(K, std::numeric_limits<double>::quiet_NaN()); rotSlip.assign(K, 0); Mrot.assign(K, 0); rotEnergy = 0;
+    dentAfterDefault = md.params.warmup_iter + md.params.ramp_iter;      // solver_cpu.js:686
     Fn.assign(K, 0); Ft.assign(K, 0); state.assign(K, 0); gap.assign(K, 0); mid.assign(3 * size_t(K), 0);
     energy = 0; ramp = 1.0;
     ev[0].resize(K); ev[1].resize(K);
@@ -397,14 +416,161 @@ struct Contact {
     offsets();
     st.nPrev = nv;
   }
-  // solver_cpu.js:151-167 (rot_friction off)
+  // solver_cpu.js:151-167
   void addStiffness(const St &st, std::vector<double> &kNode, std::vector<double> &kSeg) const {
     const double k = p.strength + p.stick_strength;
     for (int side = 0; side < 2; side++) {
       for (int c = 0; c < K; c++) { int seg; double t; segmentOf(st, side, c, seg, t); kNode[st.segI0[seg]] += k; }
       for (int c = 0; c < K; c++) { int seg; double t; segmentOf(st, side, c, seg, t); kNode[st.segI1[seg]] += k; }
     }
+    if (p.rot_friction) {
+      for (int side = 0; side < 2; side++)
+        for (int pass = 0; pass < 2; pass++)
+          for (int c = 0; c < K; c++) {
+            int seg; double t;
+            segmentOf(st, side, c, seg, t);
+            const double kr = p.stick_strength * (0.38 * 0.38) * wk[2 * size_t(c)] * wk[2 * size_t(c) + 1] / 0.5;
+            const double l = std::max(st.l0[seg], 1e-12);
+            kNode[pass ? st.segI1[seg] : st.segI0[seg]] += kr / (l * l);
+          }
+    }
     addTwistStiffness(st, kSeg);
+  }
+  // fixed-node mask from the anchors (setFixed, solver_cpu.js:481)
+  void setFixed(const std::vector<uint8_t> &nodeFree) {
+    nodeFixed.assign(nodeFree.size() / 3, 0);
+    for (size_t i = 0; i < nodeFixed.size(); i++) nodeFixed[i] = (nodeFree[3 * i] || nodeFree[3 * i + 1] || nodeFree[3 * i + 2]) ? 0 : 1;
+  }
+  // free weight of the contact point on `side` (freeWeight, solver_cpu.js:483-487)
+  double freeWeight(const St &st, int side, int c) const {
+    int seg; double t;
+    segmentOf(st, side, c, seg, t);
+    const int a = st.segI0[seg], b = st.segI1[seg];
+    return (nodeFixed[a] ? 0.0 : (1 - t) * (1 - t)) + (nodeFixed[b] ? 0.0 : t * t);
+  }
+  // crushing capacity of the face overlap (capForce, solver_cpu.js:489)
+  double capForce(int c) const {
+    return std::min(fc90[2 * size_t(c)], fc90[2 * size_t(c) + 1]) * wk[2 * size_t(c)] * wk[2 * size_t(c) + 1] / std::max(std::sin(theta[c]), 1e-6);
+  }
+  // safeguarded Uzawa value (alValue, solver_cpu.js:492-497)
+  static double alValue(double l, double penMean, double kn, bool lockedC, bool enabledC, bool pinned, double cap) {
+    if (!enabledC || pinned) return 0;
+    double v = l + kn * penMean;
+    if (!lockedC) v = std::max(v, 0.0);
+    return std::min(std::max(v, -cap), cap);
+  }
+  // Uzawa step on the window-mean penetration (updateMultipliers, solver_cpu.js:499-506)
+  void updateMultipliers(const St &st) {
+    const double kn = ramp * p.strength, nw = std::max(penN, 1);
+    for (int c = 0; c < K; c++) {
+      const bool pinned = freeWeight(st, 0, c) < AL_FREE_MIN || freeWeight(st, 1, c) < AL_FREE_MIN;
+      lam[c] = alValue(lam[c], penAcc[c] / nw, kn, locked[c], enabled[c], pinned, capForce(c));
+    }
+    std::fill(penAcc.begin(), penAcc.end(), 0.0);
+    penN = 0;
+  }
+  // W3: slope of the wall a sliding side climbs (_walls, solver_cpu.js:284-292)
+  static double walls(int sideCut, const double *R, const double *n, const double *m) {
+    const double sg = sideCut == 0 ? 1.0 : -1.0;
+    const double *X = R, *Y = R + 3;
+    const double nx = (n[0] * X[0] + n[1] * X[1] + n[2] * X[2]) * sg, ny = (n[0] * Y[0] + n[1] * Y[1] + n[2] * Y[2]) * sg;
+    double fx[3], fy[3];
+    for (int k = 0; k < 3; k++) { fx[k] = jsSign(nx) * X[k]; fy[k] = jsSign(ny) * Y[k]; }
+    const double *f = (fx[0] * m[0] + fx[1] * m[1] + fx[2] * m[2]) > 0 ? fx : fy;
+    const double cosPsi = std::min(std::max(std::fabs(f[0] * n[0] + f[1] * n[1] + f[2] * n[2]), 1e-6), 1.0);
+    return std::tan(std::acos(cosPsi));
+  }
+  // n × t, normalised (the wall direction across the cutting side)
+  static void wallAxis(const double *n, const double *tCut, double *m) {
+    m[0] = n[1] * tCut[2] - n[2] * tCut[1]; m[1] = n[2] * tCut[0] - n[0] * tCut[2]; m[2] = n[0] * tCut[1] - n[1] * tCut[0];
+    const double ml = std::max(std::sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]), 1e-12);
+    m[0] /= ml; m[1] /= ml; m[2] /= ml;
+  }
+  // W3: friction coefficient against the slide direction with the seats' walls (_seatFriction, solver_cpu.js:294-313)
+  double seatFriction(int c, const double *St_, const double *n, const double *tA, const double *tB) {
+    const double mu0 = mu[c];
+    double muD = mu0;
+    const double norm = std::sqrt(St_[0] * St_[0] + St_[1] * St_[1] + St_[2] * St_[2]);
+    const double dn = std::max(norm, 1e-12), dhat[3] = {St_[0] / dn, St_[1] / dn, St_[2] / dn};
+    const bool has = norm > 1e-12;
+    for (int j = 0; j < 2; j++) {
+      if (!(dent[2 * size_t(c) + j] > 0 && has)) continue;
+      const double *tCut = j == 0 ? tB : tA;
+      const double *Rcut = j == 0 ? &ev[1].R[9 * size_t(c)] : &ev[0].R[9 * size_t(c)];
+      double m[3];
+      wallAxis(n, tCut, m);
+      const double sgn = j == 0 ? 1.0 : -1.0;
+      const double dj = (dhat[0] * m[0] + dhat[1] * m[1] + dhat[2] * m[2]) * sgn;
+      const double wallDir[3] = {jsSign(dj) * m[0] * sgn, jsSign(dj) * m[1] * sgn, jsSign(dj) * m[2] * sgn};
+      const double tp = walls(1 - j, Rcut, n, wallDir);
+      tanpsi[2 * size_t(c) + j] = tp;
+      const double add = std::fabs(dj) * (mu0 * tp < 1.0 ? (mu0 + tp) / std::max(1.0 - mu0 * tp, 1e-6) - mu0 : 9.0 * mu0);
+      muD += std::min(add, 9.0 * mu0);
+    }
+    return muD;
+  }
+  // W3: climb out of the seats, seat growth under an edge (_seatUpdate, solver_cpu.js:315-344)
+  void seatUpdate(const St &st, int c, bool slip, double da, double db, const double *tA, const double *tB, const double *n,
+                  double fn, bool active) {
+    const double inc[3] = {da * tA[0] - db * tB[0], da * tA[1] - db * tB[1], da * tA[2] - db * tB[2]};
+    for (int j = 0; j < 2; j++) {
+      double m[3];
+      wallAxis(n, j == 0 ? tB : tA, m);
+      const double step = (inc[0] * m[0] + inc[1] * m[1] + inc[2] * m[2]) * (j == 0 ? 1.0 : -1.0);
+      const size_t i = 2 * size_t(c) + j;
+      const bool has = dent[i] > 0;
+      if (has && slip) climb[i] += step;
+      if (has && std::fabs(climb[i]) >= dent[i] / std::max(tanpsi[i], 1e-6)) { dent[i] = 0; climb[i] = 0; }
+    }
+    const int after = p.dent_after_iter >= 0 ? p.dent_after_iter : dentAfterDefault;
+    if (st.iteration < after) return;
+    const double sinp0 = std::sin(phi[2 * size_t(c)]) * std::cos(phi[2 * size_t(c)]);
+    const double sinp1 = std::sin(phi[2 * size_t(c) + 1]) * std::cos(phi[2 * size_t(c) + 1]);
+    const double sinT = std::sin(theta[c]);
+    if (ctype[c] == 2 && active && !locked[c]) {
+      const double fc = std::min(fc90[2 * size_t(c)], fc90[2 * size_t(c) + 1]);
+      const double dEst = std::sqrt(std::fabs(fn) / std::max(fc, 1e-12) * sinT * sinp0 * sinp1);
+      for (int j = 0; j < 2; j++) { const double cur = dent[2 * size_t(c) + j]; dent[2 * size_t(c) + j] = std::max(cur, std::min(cur + p.dent_rate * dEst, dEst)); }
+    }
+    if (ctype[c] == 1 && active && !locked[c]) {
+      const int fs = faceSide[c], es = 1 - fs;
+      const double ell = cFace[2 * size_t(c) + fs] / std::max(sinT, 1e-6);
+      const double dE = std::fabs(fn) / std::max(fc90[2 * size_t(c) + es] * ell, 1e-12) * (es == 0 ? sinp0 : sinp1);
+      dentE[c] = std::max(dentE[c], dE);
+    }
+  }
+  // W2: rotational friction about the contact normal (_rotationalFriction, solver_cpu.js:347-379)
+  void rotationalFriction(double *T, const std::vector<double> &n, const std::vector<uint8_t> &active, double kt) {
+    const Side &A = ev[0], &B = ev[1];
+    std::vector<double> e(K);
+    for (int c = 0; c < K; c++) {
+      const double *tA = &A.t[3 * size_t(c)], *tB = &B.t[3 * size_t(c)], *nc = &n[3 * size_t(c)];
+      const double cr[3] = {tA[1] * tB[2] - tA[2] * tB[1], tA[2] * tB[0] - tA[0] * tB[2], tA[0] * tB[1] - tA[1] * tB[0]};
+      const double th = std::atan2(cr[0] * nc[0] + cr[1] * nc[1] + cr[2] * nc[2], tA[0] * tB[0] + tA[1] * tB[1] + tA[2] * tB[2]);
+      if (std::isnan(theta0[c]) && active[c]) theta0[c] = th;
+      const bool ok = active[c] && !std::isnan(theta0[c]);
+      const double sinT = std::max(std::sin(theta[c]), 1e-6);
+      double req = 0.38 * std::sqrt(wk[2 * size_t(c)] * wk[2 * size_t(c) + 1] / sinT);
+      if (ctype[c] == 1) { const double cw = faceSide[c] == 0 ? wk[2 * size_t(c)] : wk[2 * size_t(c) + 1]; req = 0.25 * cw / sinT; }
+      else if (ctype[c] == 2) req = 0.38 * std::sqrt(std::max(Anom[c], 1e-12));
+      const double kr = kt * req * req;
+      double dth = ok ? th - theta0[c] : 0.0;
+      dth = std::fmod(std::fmod(dth + PI, 2 * PI) + 2 * PI, 2 * PI) - PI;
+      double Mc = kr * dth;
+      const double Mlim = locked[c] ? INF : p.rot_factor * mu[c] * std::fabs(Fn[c]) * req;
+      if (ok && std::fabs(Mc) > Mlim) {
+        const double rate = std::min(std::max(p.slip_rate, 1e-3), 1.0);
+        double adv = rate * (1.0 - Mlim / std::max(std::fabs(Mc), 1e-12)) * dth;
+        adv = std::min(std::max(adv, -0.05), 0.05);
+        theta0[c] += adv; rotSlip[c] += std::fabs(adv); dth -= adv;
+        Mc = kr * dth;
+      }
+      Mrot[c] = ok ? Mc : 0.0;
+      e[c] = kr * dth * dth;
+    }
+    for (int c = 0; c < K; c++) { const size_t s = A.seg[c]; for (int k = 0; k < 3; k++) T[3 * s + k] += Mrot[c] * n[3 * size_t(c) + k]; }
+    for (int c = 0; c < K; c++) { const size_t s = B.seg[c]; for (int k = 0; k < 3; k++) T[3 * s + k] -= Mrot[c] * n[3 * size_t(c) + k]; }
+    rotEnergy = 0.5 * pairwiseSum(e);
   }
   // solver_cpu.js:170-176
   void addTwistStiffness(const St &st, std::vector<double> &kSeg) const {
@@ -430,7 +596,7 @@ struct Contact {
   // W1: contact type per crossing from the roll of each section against the contact plane n (solver_cpu.js:231-271)
   void classify(const std::vector<double> &n) {
     const Side &A = ev[0], &B = ev[1];
-    std::vector<double> cFace(2 * size_t(K)), Z0(2 * size_t(K));
+    std::vector<double> Z0(2 * size_t(K));
     std::vector<uint8_t> edge(2 * size_t(K));
     for (int c = 0; c < K; c++) {
       for (int side = 0; side < 2; side++) {
@@ -473,13 +639,17 @@ struct Contact {
       Anom[c] = Aa; pressure[c] = pres; util[c] = ut;
     }
   }
-  // solver_cpu.js:381-478 (seat law, augmented Lagrangian and rotational friction off)
+  // solver_cpu.js:381-478
   void apply(St &st, double *F, double *T) {
     if (!K) return;
     prepare(st); eval(st, 0); eval(st, 1);
     const Side &A = ev[0], &B = ev[1];
     const double kn = ramp * p.strength, kt = ramp * p.stick_strength;
+    const bool seat = p.seat_law != 0, aug = p.augmented != 0;
+    const bool accum = st.iteration >= std::max(p.ramp_iter, 0);       // the multiplier's penetration window: after the ramp
     std::vector<double> nA(3 * size_t(K)), FA(3 * size_t(K)), FB(3 * size_t(K)), rAx(3 * size_t(K)), rBx(3 * size_t(K)), ePen(K), eTan(K);
+    std::vector<uint8_t> slipA(K), activeA(K);
+    std::vector<double> daA(K), dbA(K);
     double rA[3], rB[3];
     for (int c = 0; c < K; c++) {
       const double *tA = &A.t[3 * size_t(c)], *tB = &B.t[3 * size_t(c)];
@@ -497,10 +667,21 @@ struct Contact {
       const double g = S[0] * nx + S[1] * ny + S[2] * nz;
       const double hA = support(&A.R[9 * size_t(c)], nv, c, +1.0, 0, rA);
       const double hB = support(&B.R[9 * size_t(c)], nv, c, -1.0, 1, rB);
-      const double D = hA + hB;
+      double D = hA + hB;
+      if (seat && p.seat_gap) D -= dent[2 * size_t(c)] + dent[2 * size_t(c) + 1] + dentE[c];
       const double pen = D - g;
-      const bool active = (pen > 0 || locked[c]) && enabled[c];
-      const double fn = active ? kn * pen : 0.0;
+      if (accum) penAcc[c] += pen;
+      bool active;
+      double fn;
+      if (aug) {
+        const double trial = lam[c] + kn * pen;
+        active = (trial > 0 || locked[c]) && enabled[c];
+        fn = active ? (locked[c] ? trial : std::max(trial, 0.0)) : 0.0;
+      } else {
+        active = (pen > 0 || locked[c]) && enabled[c];
+        fn = active ? kn * pen : 0.0;
+      }
+      activeA[c] = active ? 1 : 0;
       const double Stv[3] = {S[0] - g * nx, S[1] - g * ny, S[2] - g * nz};
       const double taa = tA[0] * tA[0] + tA[1] * tA[1] + tA[2] * tA[2], tbb = tB[0] * tB[0] + tB[1] * tB[1] + tB[2] * tB[2], tab = tA[0] * tB[0] + tA[1] * tB[1] + tA[2] * tB[2];
       const double sa = Stv[0] * tA[0] + Stv[1] * tA[1] + Stv[2] * tA[2], sb = Stv[0] * tB[0] + Stv[1] * tB[1] + Stv[2] * tB[2];
@@ -508,7 +689,8 @@ struct Contact {
       const bool ok = det > 1e-8;
       const double ca = ok ? (sa * tbb - sb * tab) / det : 0.0, cb = ok ? (sb * taa - sa * tab) / det : 0.0;
       const double Ftv = std::sqrt((kt * Stv[0]) * (kt * Stv[0]) + (kt * Stv[1]) * (kt * Stv[1]) + (kt * Stv[2]) * (kt * Stv[2]));
-      const double limit = locked[c] ? INF : mu[c] * std::fabs(fn);
+      const double muDir = seat ? seatFriction(c, Stv, nv, tA, tB) : mu[c];
+      const double limit = locked[c] ? INF : muDir * std::fabs(fn);
       const bool inContact = active && ok;
       const bool slip = inContact && Ftv > limit;
       const bool free_ = !active && ok && enabled[c];
@@ -534,10 +716,15 @@ struct Contact {
       Ft[c] = std::sqrt(fT[0] * fT[0] + fT[1] * fT[1] + fT[2] * fT[2]);
       state[c] = slip ? 1 : 0; gap[c] = g;
       for (int k = 0; k < 3; k++) { rAx[3 * size_t(c) + k] = rA[k]; rBx[3 * size_t(c) + k] = rB[k]; }
-      ePen[c] = active ? kn * pen * pen : 0.0;
+      slipA[c] = slip ? 1 : 0; daA[c] = da; dbA[c] = db;
+      ePen[c] = active ? (aug ? fn * fn / std::max(kn, 1e-300) : kn * pen * pen) : 0.0;
       eTan[c] = Se[0] * Se[0] + Se[1] * Se[1] + Se[2] * Se[2];
     }
+    if (accum) penN += 1;
     classify(nA);                                        // solver_cpu.js:460
+    if (seat)
+      for (int c = 0; c < K; c++)
+        seatUpdate(st, c, slipA[c], daA[c], dbA[c], &A.t[3 * size_t(c)], &B.t[3 * size_t(c)], &nA[3 * size_t(c)], Fn[c], activeA[c]);
     for (int c = 0; c < K; c++) { const size_t i = A.a[c]; const double wt = 1 - A.tp[c]; for (int k = 0; k < 3; k++) F[3 * i + k] += wt * FA[3 * size_t(c) + k]; }
     for (int c = 0; c < K; c++) { const size_t i = A.b[c]; const double wt = A.tp[c]; for (int k = 0; k < 3; k++) F[3 * i + k] += wt * FA[3 * size_t(c) + k]; }
     for (int c = 0; c < K; c++) { const size_t i = B.a[c]; const double wt = 1 - B.tp[c]; for (int k = 0; k < 3; k++) F[3 * i + k] += wt * FB[3 * size_t(c) + k]; }
@@ -553,7 +740,8 @@ struct Contact {
       const double *r = &rBx[3 * size_t(c)], *f = &FB[3 * size_t(c)];
       T[3 * s] += tf * (r[1] * f[2] - r[2] * f[1]); T[3 * s + 1] += tf * (r[2] * f[0] - r[0] * f[2]); T[3 * s + 2] += tf * (r[0] * f[1] - r[1] * f[0]);
     }
-    energy = 0.5 * pairwiseSum(ePen) + 0.5 * kt * pairwiseSum(eTan);
+    if (p.rot_friction) rotationalFriction(T, nA, activeA, kt);
+    energy = 0.5 * pairwiseSum(ePen) + 0.5 * kt * pairwiseSum(eTan) + (p.rot_friction ? rotEnergy : 0.0);
   }
 };
 
@@ -645,6 +833,11 @@ struct Solver {
       contact.mu.assign(md.cross_mu, md.cross_mu + st.K);
       contact.locked.assign(md.cross_locked, md.cross_locked + st.K);
     }
+    if (hasContact) {                                     // solver_cpu.js:688
+      contact.setFixed(nodeFree);
+      std::fill(contact.penAcc.begin(), contact.penAcc.end(), 0.0);
+      contact.penN = 0;
+    }
     std::vector<double> kNode(n, 0.0), kSeg(m, 0.0);
     rod.addStiffness(st, kNode);
     if (hasContact) contact.addStiffness(st, kNode, kSeg);
@@ -674,7 +867,7 @@ struct Solver {
     return std::max(std::max(std::max(a, b), std::max(c, d)), 1e-12);
   }
 
-  // solver_cpu.js:737-841 (no floor, no rigid-body freedoms, no augmented Lagrangian)
+  // solver_cpu.js:737-841 (no floor, no rigid-body freedoms)
   bool step(int nIter) {
     const int n = st.n, m = st.m;
     const int rampN = std::max(sp.ramp_iter, 0);
@@ -752,6 +945,10 @@ struct Solver {
       }
       kePrev = ke;
       st.iteration += 1;
+      // augmented Lagrangian: Uzawa update every al_every iterations once the ramp is over (solver_cpu.js:819-821)
+      if (hasContact && contact.p.augmented && contact.p.al_every > 0 && st.iteration > rampN &&
+          (st.iteration - rampN) % contact.p.al_every == 0)
+        contact.updateMultipliers(st);
       double fmax = 0, tmax = 0;
       for (int i = 0; i < n; i++) {
         const double f = std::sqrt(F[3 * size_t(i)] * F[3 * size_t(i)] + F[3 * size_t(i) + 1] * F[3 * size_t(i) + 1] + F[3 * size_t(i) + 2] * F[3 * size_t(i) + 2]);
@@ -793,6 +990,7 @@ struct orc_view {
   uint8_t *stuck;
   int32_t *ctype;
   double *theta, *phi, *area, *pressure, *util;
+  double *lambda, *dent, *M_rot, *rot_slip;     // contact extensions (buildResults, solver_cpu.js:906-908)
 };
 
 void *orc_create(const ws_model *md) {
@@ -824,6 +1022,13 @@ void orc_view_get(void *h, orc_view *v) {
   v->ctype = s->hasContact ? s->contact.ctype.data() : nullptr; v->theta = s->hasContact ? s->contact.theta.data() : nullptr;
   v->phi = s->hasContact ? s->contact.phi.data() : nullptr; v->area = s->hasContact ? s->contact.Anom.data() : nullptr;
   v->pressure = s->hasContact ? s->contact.pressure.data() : nullptr; v->util = s->hasContact ? s->contact.util.data() : nullptr;
+  if (s->hasContact) {
+    orc::Contact &ct = s->contact;
+    ct.dentSum.resize(ct.K);
+    for (int k = 0; k < ct.K; k++) ct.dentSum[k] = ct.dent[2 * size_t(k)] + ct.dent[2 * size_t(k) + 1] + ct.dentE[k];
+  }
+  v->lambda = s->hasContact ? s->contact.lam.data() : nullptr; v->dent = s->hasContact ? s->contact.dentSum.data() : nullptr;
+  v->M_rot = s->hasContact ? s->contact.Mrot.data() : nullptr; v->rot_slip = s->hasContact ? s->contact.rotSlip.data() : nullptr;
   v->N = s->rod.N.data(); v->Vsh = s->rod.Vs.data(); v->M = s->rod.M.data(); v->reactions = s->reactions.data();
   v->mass = s->mass.data(); v->inertia3 = s->inertia3.data(); v->k_rot_static = s->kRotStatic.data();
   v->F = s->F.data(); v->T = s->T.data(); v->tm = s->tm.data();

@@ -25,7 +25,7 @@ class OrcView(C.Structure):
                [(k, _dp) for k in ("X", "X0", "V", "Q", "W", "u", "nprev", "slip", "Fn", "Ft", "gap", "state", "N",
                                    "Vsh", "M", "reactions", "mass", "inertia3", "k_rot_static", "F", "T", "tm")] + \
                [("stuck", C.POINTER(C.c_uint8)), ("ctype", C.POINTER(C.c_int32))] + \
-               [(k, _dp) for k in ("theta", "phi", "area", "pressure", "util")]
+               [(k, _dp) for k in ("theta", "phi", "area", "pressure", "util", "lambda", "dent", "M_rot", "rot_slip")]
 
 
 _lib = None
@@ -121,7 +121,8 @@ class Oracle:
         out["stuck"] = np.array(st, dtype=np.uint8)
         hc = K and v.has_contact
         out["ctype"] = np.ctypeslib.as_array(v.ctype, shape=(K,)).astype(np.uint8) if hc else np.zeros(0, dtype=np.uint8)
-        for k, s_ in (("theta", K), ("phi", 2 * K), ("area", K), ("pressure", K), ("util", K)):
+        for k, s_ in (("theta", K), ("phi", 2 * K), ("area", K), ("pressure", K), ("util", K), ("lambda", K), ("dent", K),
+                      ("M_rot", K), ("rot_slip", K)):
             a = _arr(getattr(v, k), s_) if hc else np.zeros(0)
             out[k] = a.copy() if copy else a
         return out

@@ -3,7 +3,8 @@
 * straight(L, nseg)            cases.mjs:10-13
 * cantilever(nseg, dir)        rod_bench.mjs:27-36 (60×30 mm, E 1e4 N/mm², G 625, tip load 10 N, clamped at frame (0,0))
 * crossing(load, pull, ...)    cases.mjs:14-28 (two 1000 mm laths, 10 segments, h = 30, B free in x)
-* case_by_name(name)           cases.mjs:29-50 (cantilever, cantilever_edge, torsion, cross_press/stick/slip/locked)
+* case_by_name(name)           cases.mjs:29-50 (cantilever, cantilever_edge, torsion, cross_press/stick/slip/locked,
+                               cross_w23) and browser_cases.js:41-45 (cross_al)
 """
 from __future__ import annotations
 
@@ -44,7 +45,7 @@ def timoshenko(direction=2, P=10.0, L=1000.0, w=60.0, h=30.0):
 
 
 def crossing(load=-50.0, pull=0.0, mu=0.35, freeB=True, nseg=10, L=1000.0, h=30.0, locked=False, local=False, roll=(0.0, 0.0),
-             **prm):
+             pin=False, **prm):
     P = np.array([[-L / 2 + L * i / nseg, 0.0, 0.0] for i in range(nseg + 1)])
     PB = np.array([[0.0, -L / 2 + L * i / nseg, h] for i in range(nseg + 1)])
     mid = nseg // 2
@@ -55,7 +56,7 @@ def crossing(load=-50.0, pull=0.0, mu=0.35, freeB=True, nseg=10, L=1000.0, h=30.
     nA = np.tile([0.0, -math.sin(roll[0]), math.cos(roll[0])], (nseg + 1, 1))
     nB = np.tile([math.sin(roll[1]), 0.0, math.cos(roll[1])], (nseg + 1, 1))
     md = ws.polylines([P, PB], normals=[nA, nB], knot_rows=[[0, mid, nseg], [0, mid, nseg]], knots=[((0, 1), (1, 1))],
-                      anchors=[((0, 0), fixA), ((0, 2), fixA), ((1, 0), fixB), ((1, 2), fixB)],
+                      anchors=[((0, 0), fixA), ((0, 2), fixA), ((1, 0), fixB), ((1, 2), fixB)] + ([((0, 1), fixA)] if pin else []),
                       loads=[((1, 1), (pull, 0.0, load), local)], mu=mu, E=E_MM, G=G_MM, params=mm_params(**prm))
     if locked:
         md.cross_locked[:] = 1
@@ -77,6 +78,10 @@ def case_by_name(name):
     pulls = {"cross_press": 0.0, "cross_stick": 5.0, "cross_slip": 12.0, "cross_locked": 12.0}
     if name in pulls:
         return crossing(-50.0, pulls[name], locked=name == "cross_locked")
+    if name == "cross_w23":      # W2 rotational friction + W3 seat law, seats from the start (cases.mjs:48)
+        return crossing(-50.0, 5.0, rot_friction=1, seat_law=1, dent_after_iter=0, slip_rate=0.3)
+    if name == "cross_al":       # augmented-Lagrangian gap (browser_cases.js:45)
+        return crossing(-50.0, 0.0, augmented=1, al_every=600, strength=2000.0)
     raise KeyError(name)
 
 

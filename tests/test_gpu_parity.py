@@ -383,3 +383,121 @@ def test_classification_gridshell_matches_oracle(oracle_mod):
         scale = np.abs(v[k]).max()
         assert np.abs(g[k] - v[k]).max() < 1e-8 * scale, k
     assert np.abs(g["phi"] - v["phi"]).max() < 1e-8
+
+
+# ---------------------------------------------------------------------------------------------- contact extensions
+EXT_FIELDS = ("X", "u", "slip", "Fn", "gap", "stuck", "lambda", "dent", "M_rot", "rot_slip", "ctype")
+
+
+def _ext_compare(g, v, md, ctl, tol=1e-9):
+    assert ctl["iter"] == v["iteration"] and ctl["rollbacks"] == v["rollbacks"]
+    assert cases.max_rel_disp_error(g["X"], v["X"], v["X0"]) < tol
+    assert np.array_equal(g["stuck"], v["stuck"]) and np.array_equal(g["ctype"], v["ctype"])
+    for k in ("Fn", "lambda", "dent", "M_rot", "rot_slip", "slip", "gap"):
+        scale = max(np.abs(v[k]).max(), 1e-300)
+        assert np.abs(g[k] - v[k]).max() <= tol * scale + 1e-12, (k, g[k], v[k])
+    assert np.abs(g["u"] - v["u"]).max() < tol
+
+
+def _ext_case(name):
+    r = math.radians(40.0)
+    if name in ("cross_w23", "cross_al"):
+        return cases.case_by_name(name), 8000
+    if name == "cross_al_long":         # past convergence: the Uzawa steps at 2100, 2700, ... close the gap
+        return cases.crossing(-50.0, 0.0, augmented=1, al_every=600, strength=2000.0, tol=0.0), 4000
+    if name == "seat_edge_edge":
+        return cases.crossing(-50.0, 12.0, roll=(r, r), slip_rate=0.3, seat_law=1, rot_friction=1, dent_after_iter=0), 6000
+    if name == "seat_edge_face":
+        return cases.crossing(-50.0, 12.0, roll=(0.0, r), slip_rate=0.3, seat_law=1, rot_friction=1, dent_after_iter=0), 6000
+    if name == "rot_slip":
+        return cases.crossing(-50.0, 12.0, rot_friction=1, rot_factor=0.001, slip_rate=1.0), 6000
+    if name == "al_pinned":
+        return cases.crossing(-50.0, 0.0, augmented=1, al_every=600, strength=2000.0, tol=0.0, pin=True), 3000
+    raise KeyError(name)
+
+
+@pytest.mark.parametrize("name", ["cross_w23", "cross_al", "cross_al_long", "seat_edge_edge", "seat_edge_face", "rot_slip",
+                                  "al_pinned"])
+@pytest.mark.parametrize("form", ["cta", "plain", "grid"])
+def test_contact_extensions_match_oracle(oracle_mod, name, form):
+    """the augmented-Lagrangian gap, W2 rotational friction and the W3 seat law (solver_cpu.js:283-379, 381-506,
+    819-821) in every execution form against the oracle: state, multipliers, seat depths, scissor moments"""
+    md, it = _ext_case(name)
+    v = oracle_mod.Oracle(md.copy()).run(it)
+    s = ws.GpuSolver([md.copy()], precision="f64", form=form)
+    ctl = s.step(it)[0]
+    g = s.download(0, fields=EXT_FIELDS)
+    s.dispose()
+    _ext_compare(g, v, md, ctl)
+
+
+def test_multiplier_update_due_at_a_download(oracle_mod):
+    """a chunk that ends on an Uzawa iteration (2100 = ramp 1500 + 600): the download shows the updated λ, and the
+    run continues as the oracle's does whether or not a download came in between"""
+    md, _ = _ext_case("cross_al_long")
+    o = oracle_mod.Oracle(md.copy())
+    o.step(2100)
+    v1 = o.view()
+    o.step(700)
+    v2 = o.view()
+    s = ws.GpuSolver([md.copy()], precision="f64", form="plain")
+    s.step(2100)
+    g1 = s.download(0, fields=EXT_FIELDS)
+    ctl = s.step(700)[0]
+    g2 = s.download(0, fields=EXT_FIELDS)
+    s.dispose()
+    assert v1["lambda"][0] > 0 and abs(g1["lambda"][0] - v1["lambda"][0]) < 1e-9 * v1["lambda"][0]
+    _ext_compare(g2, v2, md, ctl)
+
+
+def test_warm_start_restarts_the_multiplier_window(oracle_mod):
+    """set_params mid-window (rebuildGoals, solver_cpu.js:688): the pending update is applied first, the window
+    restarts, the multipliers stay"""
+    md, _ = _ext_case("cross_al_long")
+    var = md.copy()
+    var.params["strength"] = 2500.0
+    o = oracle_mod.Oracle(md.copy())
+    o.step(2400)
+    o.rebuild(var)
+    o.step(1000)
+    v = o.view()
+    s = ws.GpuSolver([md.copy()], precision="f64")
+    s.step(2400)
+    s.update_params(0, var)
+    ctl = s.step(1000)[0]
+    g = s.download(0, fields=EXT_FIELDS)
+    s.dispose()
+    assert ctl["iter"] == 3400
+    _ext_compare(g, v, md, ctl)
+
+
+@pytest.mark.parametrize("form,side_order", [("cta", "auto"), ("plain", "auto"), ("plain", "general"), ("grid", "auto")])
+def test_gridshell_with_extensions_matches_oracle(oracle_mod, form, side_order):
+    """the small dome with all three extensions on: 1500 iterations (warm-up, ramp, seats from 300) against the
+    oracle (the batched form keeps this instance in shared memory)"""
+    md = ws.configs.dome_small()
+    md.params.update(augmented=1, al_every=200, rot_friction=1, seat_law=1, dent_after_iter=300, ramp_iter=1000)
+    o = oracle_mod.Oracle(md.copy())
+    o.step(1500)
+    v = o.view()
+    s = ws.GpuSolver([md.copy()], precision="f64", form=form, side_order=side_order)
+    ctl = s.step(1500)[0]
+    g = s.download(0, fields=EXT_FIELDS)
+    s.dispose()
+    assert ctl["iter"] == 1500 and v["ctype"].max() == 2
+    assert cases.max_node_err_span(g["X"], v["X"], md.span) < 1e-9
+    assert np.array_equal(g["stuck"], v["stuck"]) and np.array_equal(g["ctype"], v["ctype"])
+    for k in ("Fn", "lambda", "dent", "M_rot", "rot_slip"):
+        assert np.abs(g[k] - v[k]).max() <= 1e-8 * max(np.abs(v[k]).max(), 1e-300), k
+
+
+def test_extensions_mixed_precision_within_band(oracle_mod):
+    """the mixed policy on the seated crossing: the converged contact force within the crossing band"""
+    md, it = _ext_case("seat_edge_edge")
+    v = oracle_mod.Oracle(md.copy()).run(it)
+    s = ws.GpuSolver([md.copy()], precision="mixed")
+    s.step(it)
+    g = s.download(0, fields=EXT_FIELDS)
+    s.dispose()
+    assert abs(g["Fn"][0] - v["Fn"][0]) < 1e-2 * abs(v["Fn"][0])
+    assert abs(g["dent"][0] - v["dent"][0]) < 1e-2 * abs(v["dent"][0])

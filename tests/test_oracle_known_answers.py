@@ -183,3 +183,59 @@ def test_classification_edge_on_edge(oracle_mod):
     assert v["ctype"][0] == 2
     Fn = abs(v["Fn"][0])
     assert Fn > 0 and abs(v["area"][0] - Fn / 8.0) < 1e-12 * Fn and v["pressure"][0] == 8.0 and v["util"][0] == 1.0
+
+
+# ---------------------------------------------------------------------------------------------- contact extensions
+# The reference ships no expected values for these (its checks compare its GPU form with its CPU form), so they are
+# pinned by what the laws guarantee.
+
+def _al(oracle_mod, it, **kw):
+    md = cases.crossing(-50.0, 0.0, augmented=1, al_every=600, strength=2000.0, tol=0.0, **kw)
+    return oracle_mod.Oracle(md.copy()).run(it)
+
+
+def test_augmented_lagrangian_closes_the_gap(oracle_mod):
+    """λ starts at the first Uzawa step (ramp 1500 + al_every 600) and then carries the contact force, so the
+    penetration left by the penalty (Fn / k_n = 0.0125 mm here) closes (solver_cpu.js:414-418, 499-506, 819-821)"""
+    before, after, long = _al(oracle_mod, 2099), _al(oracle_mod, 2100), _al(oracle_mod, 8000)
+    assert before["lambda"][0] == 0.0 and after["lambda"][0] > 0.0
+    pen0 = 30.0 - before["gap"][0]
+    assert abs(pen0 - before["Fn"][0] / 2000.0) < 1e-3 * pen0
+    Fn = long["Fn"][0]
+    assert abs(long["lambda"][0] - Fn) < 1e-3 * Fn
+    assert abs(30.0 - long["gap"][0]) < 1e-3 * pen0
+    assert abs(Fn - 25.0) < 0.1                       # half the load through each lath's mid-span support
+
+
+def test_augmented_lagrangian_skips_supported_crossings(oracle_mod):
+    """a contact point on a supported node carries no multiplier (free weight < AL_FREE_MIN, solver_cpu.js:29-33)"""
+    v = _al(oracle_mod, 3000, pin=True)
+    assert v["Fn"][0] > 0.0 and v["lambda"][0] == 0.0
+
+
+def test_rotational_friction_limit(oracle_mod):
+    """W2: with a full return mapping (slip_rate 1) the scissor moment never exceeds Coulomb's rot_factor·μ·|Fn|·r_eq;
+    a low factor makes the crossing turn (rotational slip), a high one holds it (solver_cpu.js:347-379)"""
+    out = {}
+    for rf in (1.0, 0.001):
+        md = cases.crossing(-50.0, 12.0, rot_friction=1, rot_factor=rf, slip_rate=1.0)
+        v = oracle_mod.Oracle(md.copy()).run(6000)
+        assert v["ctype"][0] == 0
+        req = 0.38 * math.sqrt(60.0 * 60.0 / max(math.sin(v["theta"][0]), 1e-6))
+        assert abs(v["M_rot"][0]) <= rf * 0.35 * abs(v["Fn"][0]) * req * (1 + 1e-9)
+        out[rf] = v
+    assert out[1.0]["rot_slip"][0] == 0.0 and out[1.0]["M_rot"][0] != 0.0
+    assert out[0.001]["rot_slip"][0] > 0.0
+
+
+def test_seat_law_holds_a_crossing(oracle_mod):
+    """W3: sections bearing edge on edge cut seats into each other; the seats' walls raise the friction against the
+    slide, so a pull that slides the crossing without them leaves it in its seats (solver_cpu.js:283-344); a crossing
+    face on face never seats"""
+    r = math.radians(40.0)
+    free = oracle_mod.Oracle(cases.crossing(-50.0, 12.0, roll=(r, r), slip_rate=0.3).copy()).run(6000)
+    seated = oracle_mod.Oracle(cases.crossing(-50.0, 12.0, roll=(r, r), slip_rate=0.3, seat_law=1, dent_after_iter=0).copy()).run(6000)
+    flat = oracle_mod.Oracle(cases.crossing(-50.0, 12.0, slip_rate=0.3, seat_law=1, dent_after_iter=0).copy()).run(6000)
+    assert free["ctype"][0] == 2 and seated["ctype"][0] == 2
+    assert free["dent"][0] == 0.0 and seated["dent"][0] > 0.0 and flat["dent"][0] == 0.0
+    assert seated["slip"][0] < 0.05 * free["slip"][0]

@@ -30,7 +30,9 @@ class WsParams(C.Structure):
                 ("kinetic_damping", C.c_int32), ("warmup_iter", C.c_int32), ("max_iter", C.c_int32),
                 ("contacts", C.c_int32), ("strength", C.c_double), ("stick_strength", C.c_double),
                 ("torsion_factor", C.c_double), ("epsilon", C.c_double), ("ramp_iter", C.c_int32),
-                ("disp_ramp_iter", C.c_int32), ("slip_rate", C.c_double), ("edge_threshold", C.c_double)]
+                ("disp_ramp_iter", C.c_int32), ("slip_rate", C.c_double), ("edge_threshold", C.c_double),
+                ("augmented", C.c_int32), ("al_every", C.c_int32), ("rot_friction", C.c_int32), ("seat_law", C.c_int32),
+                ("seat_gap", C.c_int32), ("dent_after_iter", C.c_int32), ("rot_factor", C.c_double), ("dent_rate", C.c_double)]
 
 
 PARAM_KEYS = [f[0] for f in WsParams._fields_ if not f[0].startswith("pad")]
@@ -86,7 +88,8 @@ class WsStateOut(C.Structure):
     _fields_ = [(k, _dp) for k in ("X", "Q", "V", "W", "u", "nprev", "slip")] + \
                [("stuck", _bp), ("state", _bp)] + \
                [(k, _dp) for k in ("Fn", "Ft", "gap", "N", "Vsh", "M", "reactions")] + \
-               [("ctype", _bp)] + [(k, _dp) for k in ("theta", "phi", "area", "pressure", "util")]
+               [("ctype", _bp)] + [(k, _dp) for k in ("theta", "phi", "area", "pressure", "util")] + \
+               [(k, _dp) for k in ("lambda", "dent", "M_rot", "rot_slip")]
 
 
 _lib = None

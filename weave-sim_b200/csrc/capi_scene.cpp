@@ -32,6 +32,8 @@ void ws_params_default(ws_params *p) {
   p->mass_scale = 1.5; p->damping = 1.0; p->tol = 1e-4; p->kinetic_damping = 1; p->warmup_iter = 300; p->max_iter = 5000;
   p->contacts = 1; p->strength = 1e7; p->stick_strength = 1e7; p->torsion_factor = 1.0; p->epsilon = 0.015;
   p->ramp_iter = 1500; p->slip_rate = 1.0; p->edge_threshold = 0.5;
+  p->augmented = 0; p->al_every = 600; p->rot_friction = 0; p->seat_law = 0; p->seat_gap = 1; p->dent_after_iter = -1;
+  p->rot_factor = 1.0; p->dent_rate = 0.01;
 }
 
 int ws_scene_kagome(const ws_kagome_cfg *cfg, ws_scene **out) {

@@ -3,7 +3,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <deque>
 #include <functional>
+#include <limits>
 #include <memory>
 #include <numeric>
 #include <type_traits>
@@ -76,6 +78,9 @@ void layout(Dev<P> &d, Carver &cv, const Sizes &z) {
   d.fc90 = cv.take<R>(2 * k); d.E90 = cv.take<R>(2 * k); d.Hs = cv.take<R>(2 * k); d.sProj = cv.take<R>(4 * k); d.sinT = cv.take<R>(k);
   d.ctype = cv.take<uint8_t>(k); d.theta = cv.take<R>(k); d.area = cv.take<R>(k); d.pres = cv.take<R>(k);
   d.util = cv.take<R>(k); d.phiS = cv.take<R>(2 * k);
+  d.lam = cv.take<A>(k); d.penAcc = cv.take<A>(k); d.dent = cv.take<R>(2 * k); d.climb = cv.take<R>(2 * k);
+  d.tanpsi = cv.take<R>(2 * k); d.dentE = cv.take<R>(k); d.theta0 = cv.take<R>(k); d.Mrot = cv.take<R>(k);
+  d.rotSlip = cv.take<A>(k);
 }
 
 // host -> device with conversion, batched: put() converts into a host buffer and queues the copy; flushPuts() sends the
@@ -124,7 +129,7 @@ struct ws_ctx {
   void *dPart = nullptr;
   unsigned *dBar = nullptr;   // grid form: barrier counter + generation, and its timeout flag
   int *dErr = nullptr;
-  int gridBlocks[2] = {0, 0};   // grid form: co-resident blocks with the general / short-slide side order
+  int gridBlocks[2][2] = {{0, 0}, {0, 0}};   // grid form: co-resident blocks [short-slide side order][extensions]
   PlainShape shape{};
   int sidesGeneral = 0;          // ws_opts.side_order == WS_SIDES_GENERAL
   int ctaGlobal = 0;             // ws_opts.cta_state == WS_CTA_GLOBAL
@@ -190,6 +195,9 @@ struct Fetch {
   struct Item { const void *src; size_t bytes, off; std::function<void(const char *)> put; };
   std::vector<Item> items;
   size_t total = 0;
+  std::deque<std::vector<double>> tmp;         // host scratch of fields derived from several planes
+  std::vector<std::function<void()>> after;    // run once the planes have landed
+  double *scratch(size_t n) { tmp.emplace_back(n); return tmp.back().data(); }
   template <class T>
   void planes(const T *base, size_t stride, size_t first, size_t count, int ncomp, double *dst) {
     for (int k = 0; k < ncomp; k++) {
@@ -229,6 +237,7 @@ struct Fetch {
     for (auto &it : items) if (it.bytes) CK(cudaMemcpyAsync(buf + it.off, it.src, it.bytes, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     for (auto &it : items) if (it.put) it.put(buf + it.off);
+    for (auto &f : after) f();
   }
 };
 
@@ -248,6 +257,11 @@ InstDesc describe(const HostGoals &g, const Sizes &off) {
   I.ms = g.prm.mass_scale; I.damping = g.prm.damping; I.tol = g.prm.tol; I.strength = g.prm.strength; I.stick = g.prm.stick_strength;
   I.tf = g.prm.torsion_factor; I.eps = g.prm.epsilon; I.slip_rate = g.prm.slip_rate; I.lRef = g.lRef; I.jLenMin = g.jLenMin;
   I.edgeThr = g.prm.edge_threshold;
+  I.aug = g.prm.augmented ? 1 : 0; I.alEvery = g.prm.al_every; I.rotFric = g.prm.rot_friction ? 1 : 0;
+  I.seat = g.prm.seat_law ? 1 : 0; I.seatGap = g.prm.seat_gap ? 1 : 0;
+  I.dentAfter = g.prm.dent_after_iter >= 0 ? g.prm.dent_after_iter : g.dentAfterDefault;
+  I.rotFactor = g.prm.rot_factor; I.dentRate = g.prm.dent_rate;
+  I.ext = (I.aug || I.rotFric || I.seat) ? 1 : 0;
   return I;
 }
 
@@ -443,9 +457,37 @@ void uploadStatic(ws_ctx *c, int b) {
   put<uint8_t>(d.stuck + I.k0, one.data(), K, st);
 }
 
+// the contact-extension state of instance b at its start: no multiplier, no seats (wall slopes 1), no W2 reference angle
+template <int P>
+void resetExt(ws_ctx *c, int b) {
+  Dev<P> &d = devOf<P>(c);
+  using R = typename Dev<P>::R; using A = typename Dev<P>::A;
+  const InstDesc &I = c->inst[b];
+  const size_t K = I.K;
+  if (!K) return;
+  const std::vector<double> z(2 * K, 0.0), one(2 * K, 1.0), nan(K, std::numeric_limits<double>::quiet_NaN());
+  put<A>(d.lam + I.k0, z.data(), K, c->st);
+  put<A>(d.penAcc + I.k0, z.data(), K, c->st);
+  put<R>(d.dent + 2 * size_t(I.k0), z.data(), 2 * K, c->st);
+  put<R>(d.climb + 2 * size_t(I.k0), z.data(), 2 * K, c->st);
+  put<R>(d.tanpsi + 2 * size_t(I.k0), one.data(), 2 * K, c->st);
+  put<R>(d.dentE + I.k0, z.data(), K, c->st);
+  put<R>(d.theta0 + I.k0, nan.data(), K, c->st);
+  put<R>(d.Mrot + I.k0, z.data(), K, c->st);
+  put<A>(d.rotSlip + I.k0, z.data(), K, c->st);
+}
+
+// the multiplier update of instance b that fell due at the end of its last iteration, applied before anything reads
+// the multipliers or changes what the update depends on
+template <int P>
+void flushAL(ws_ctx *c, int b) {
+  if (c->inst[b].aug && c->inst[b].contacts && c->inst[b].K) CK(launchAlFlush<P>(devOf<P>(c), c->dInst, c->dCtl, b, c->st));
+}
+
 template <int P>
 void uploadAll(ws_ctx *c) {
   for (size_t b = 0; b < c->g.size(); b++) {
+    resetExt<P>(c, int(b));
     uploadStatic<P>(c, int(b));
     uploadGoals<P>(c, int(b));
     uploadState<P>(c, int(b), 0, true);
@@ -492,6 +534,12 @@ void fillControl(const InstCtl &s, ws_control *o) {
   o->e_stretch = s.e_stretch; o->e_shear = s.e_shear; o->e_bend = s.e_bend; o->e_twist = s.e_twist; o->e_contact = s.e_contact;
 }
 
+// some instance runs a contact extension: the kernels' variants with them
+bool anyExt(const ws_ctx *c) {
+  for (const InstDesc &I : c->inst) if (I.ext && I.contacts && I.K) return true;
+  return false;
+}
+
 #ifndef WSB_PLAIN_FORK
 #define WSB_PLAIN_FORK 1     // the plain form's element phase as two kernels on forked branches (0: one kernel)
 #endif
@@ -500,6 +548,7 @@ const PlainFork *plainFork(const ws_ctx *c) { return (WSB_PLAIN_FORK && c->fork.
 template <int P>
 void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
   const int nInst = int(c->inst.size());
+  const bool ext = anyExt(c);
   c->lastLaunches = 0;
   CK(cudaEventRecord(c->ev0, c->st));
   if (c->form == WS_FORM_CTA) {
@@ -507,31 +556,32 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
     if (c->residentBytes) {
       const int thr = c->threads > 0 ? std::min(c->threads, 512) : 512;
       CK(launchResident<P>(devOf<P>(c), c->dInst, c->dCtl, c->dOrder, nInst, nIter, mask ? c->dMask : nullptr, thr,
-                           c->residentBytes, c->shortSides, c->st));
+                           c->residentBytes, c->shortSides, ext, c->st));
     } else {
       const int thr = c->threads > 0 ? c->threads : 256;
       CK(launchBatched<P>(devOf<P>(c), c->dInst, c->dCtl, c->dOrder, nInst, nIter, mask ? c->dMask : nullptr, thr, nInst,
-                          c->shortSides, c->st));
+                          c->shortSides, ext, c->st));
     }
     c->lastLaunches = 1;
   } else if (c->form == WS_FORM_GRID) {
     CK(cudaMemsetAsync(c->dBar, 0, 2 * sizeof(unsigned), c->st));
     CK(cudaMemsetAsync(c->dErr, 0, sizeof(int), c->st));
     if (nIter > 0)
-      CK(launchGrid<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->dBar, c->dErr, nIter, c->gridBlocks[c->shortSides], c->shortSides, c->st));
+      CK(launchGrid<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->dBar, c->dErr, nIter, c->gridBlocks[c->shortSides][ext],
+                       c->shortSides, ext, c->st));
     c->lastLaunches = 1;
   } else {
     const bool cx = c->inst[0].contacts && c->inst[0].K;
     const bool sh = c->shortSides;
     const int chunk = std::min(nIter, 50);
-    const int key = (chunk << 2) | (cx ? 2 : 0) | (sh ? 1 : 0);
+    const int key = (chunk << 3) | (ext ? 4 : 0) | (cx ? 2 : 0) | (sh ? 1 : 0);
     if (chunk > 0 && (!c->graph || c->graphKey != key)) {
       if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
       cudaGraph_t gr;
       CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
       int nl = 0;
       for (int i = 0; i < chunk; i++)
-        CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, c->st, &nl, c->dBar + 2, plainFork(c)));
+        CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, ext, c->st, &nl, c->dBar + 2, plainFork(c)));
       CK(cudaStreamEndCapture(c->st, &gr));
       CK(cudaGraphInstantiate(&c->graph, gr, 0));
       cudaGraphDestroy(gr);
@@ -543,7 +593,7 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
     while (nIter - done >= chunk && chunk > 0) { CK(cudaGraphLaunch(c->graph, c->st)); done += chunk; c->lastLaunches += c->graphLaunches; }
     int nl = 0;
     for (; done < nIter; done++)
-      CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, c->st, &nl, c->dBar + 2, plainFork(c)));
+      CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, ext, c->st, &nl, c->dBar + 2, plainFork(c)));
     c->lastLaunches += nl;
   }
   CK(cudaEventRecord(c->ev1, c->st));
@@ -584,7 +634,10 @@ void downloadPacked(ws_ctx *c, int b, ws_state_out *o) {
   add(PF_STUCK, I.K, 1, o->stuck, true); add(PF_STATE, I.K, 1, o->state, true);
   add(PF_CTYPE, I.K, 1, o->ctype, true); add(PF_THETA, I.K, 1, o->theta, false); add(PF_PHI, I.K, 2, o->phi, false);
   add(PF_AREA, I.K, 1, o->area, false); add(PF_PRES, I.K, 1, o->pressure, false); add(PF_UTIL, I.K, 1, o->util, false);
+  add(PF_LAM, I.K, 1, o->lambda, false); add(PF_DENT, I.K, 1, o->dent, false); add(PF_MROT, I.K, 1, o->M_rot, false);
+  add(PF_RSLIP, I.K, 1, o->rot_slip, false);
   if (!L.nf) return;
+  if (o->lambda) flushAL<P>(c, b);
   if (wantsClass(o)) CK(launchClassify<P>(devOf<P>(c), c->dInst, b, I.K, c->st));
   unsigned char *dv = xferBuf(c, off);
   CK(launchPack<P>(devOf<P>(c), c->dInst, c->dCtl, b, L, elems, dv, c->st));
@@ -598,6 +651,7 @@ template <int P>
 void downloadImpl(ws_ctx *c, int b, ws_state_out *o) {
   if (c->pinnedOK) { downloadPacked<P>(c, b, o); return; }
   Dev<P> &d = devOf<P>(c);
+  if (o->lambda) flushAL<P>(c, b);
   readCtl(c);
   const InstCtl &s = c->ctlHost[b];
   const InstDesc &I = c->inst[b];
@@ -624,6 +678,17 @@ void downloadImpl(ws_ctx *c, int b, ws_state_out *o) {
       if (o->area) f.planes(d.area, 0, I.k0, K, 1, o->area);
       if (o->pressure) f.planes(d.pres, 0, I.k0, K, 1, o->pressure);
       if (o->util) f.planes(d.util, 0, I.k0, K, 1, o->util);
+    }
+    if (o->lambda) f.planes(d.lam, 0, I.k0, K, 1, o->lambda);
+    if (o->M_rot) f.planes(d.Mrot, 0, I.k0, K, 1, o->M_rot);
+    if (o->rot_slip) f.planes(d.rotSlip, 0, I.k0, K, 1, o->rot_slip);
+    if (o->dent) {
+      double *dd = f.scratch(2 * K), *de = f.scratch(K);
+      f.planes(d.dent, 0, 2 * size_t(I.k0), 2 * K, 1, dd);
+      f.planes(d.dentE, 0, I.k0, K, 1, de);
+      f.after.push_back([dd, de, K, out = o->dent]() {
+        for (size_t q = 0; q < K; q++) out[q] = dd[2 * q] + dd[2 * q + 1] + de[q];
+      });
     }
   }
   if (o->N) f.planes(d.Nax, 0, I.m0, m, 1, o->N);
@@ -678,6 +743,7 @@ void reselectOrder(ws_ctx *c) {
 
 template <int P>
 void setParamsImpl(ws_ctx *c, int b, const ws_model *md) {
+  flushAL<P>(c, b);
   pullState<P>(c, b);
   HostGoals &g = c->g[b];
   const std::vector<int> oldSeg = g.cSeg;
@@ -694,6 +760,12 @@ void setParamsImpl(ws_ctx *c, int b, const ws_model *md) {
   readCtl(c);
   InstCtl s = c->ctlHost[b];
   s.ke_prev = 0.0; s.status = WS_RUNNING; s.disp_it0 = s.iter;
+  // a rebuild restarts the multipliers' penetration window (solver_cpu.js:688)
+  s.penN = 0; s.alPend = 0;
+  {
+    using A = typename Dev<P>::A;
+    if (g.K) CK(cudaMemsetAsync(devOf<P>(c).penAcc + c->inst[b].k0, 0, sizeof(A) * g.K, c->st));
+  }
   CK(cudaMemcpyAsync(c->dCtl + b, &s, sizeof(InstCtl), cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
   reselectOrder<P>(c);
@@ -721,6 +793,7 @@ void loadInstanceImpl(ws_ctx *c, int b, const ws_model *md) {
   InstCtl s;
   std::memset(&s, 0, sizeof(s));
   s.status = WS_RUNNING; s.residual = INFINITY;
+  resetExt<P>(c, b);
   uploadState<P>(c, b, 0, true);
   // both buffers: a slice left over from the slot's previous model could point into another strand's sides
   uploadOrder<P>(c, b, 0);
@@ -752,6 +825,7 @@ void uploadStatePacked(ws_ctx *c, int b, const double *X, const double *Q, const
 
 template <int P>
 void uploadStateImpl(ws_ctx *c, int b, const double *X, const double *Q, const double *u) {
+  flushAL<P>(c, b);
   if (c->pinnedOK) { uploadStatePacked<P>(c, b, X, Q, u); return; }
   HostGoals &g = c->g[b];
   readCtl(c);
@@ -896,18 +970,18 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     c->shape.blocksDM = blocks(I0.m, 256);
     c->shape.blocksR = blocks(I0.m + 2LL * I0.K, 256);
     c->shape.blocksD = blocks(I0.n + I0.m, 256);
-    for (int sh = 0; sh < 2; sh++) {
-      switch (c->prec) {
-        case WS_PREC_F64: c->gridBlocks[sh] = gridBlocks<PREC_F64>(sh != 0); break;
-        case WS_PREC_MIXED: c->gridBlocks[sh] = gridBlocks<PREC_MIXED>(sh != 0); break;
-        default: c->gridBlocks[sh] = gridBlocks<PREC_F32>(sh != 0); break;
+    for (int sh = 0; sh < 2; sh++)
+      for (int ex = 0; ex < 2; ex++) {
+        switch (c->prec) {
+          case WS_PREC_F64: c->gridBlocks[sh][ex] = gridBlocks<PREC_F64>(sh != 0, ex != 0); break;
+          case WS_PREC_MIXED: c->gridBlocks[sh][ex] = gridBlocks<PREC_MIXED>(sh != 0, ex != 0); break;
+          default: c->gridBlocks[sh][ex] = gridBlocks<PREC_F32>(sh != 0, ex != 0); break;
+        }
       }
-    }
     CK(cudaGetLastError());
     const int parts = std::max({c->shape.blocksA + c->shape.blocksDS, c->shape.blocksA + c->shape.blocksD,
                                 c->shape.blocksX + c->shape.blocksY + std::max(c->shape.blocksDN, c->shape.blocksDNS) + c->shape.blocksDM,
-                                c->gridBlocks[0],
-                                c->gridBlocks[1]});
+                                c->gridBlocks[0][0], c->gridBlocks[0][1], c->gridBlocks[1][0], c->gridBlocks[1][1]});
     CK(cudaMalloc(&c->dPart, sizeof(double) * (RS_NSUM + RX_NMAX) * size_t(parts)));
     CK(cudaMalloc(&c->dBar, 4 * sizeof(unsigned)));     // [0..1] grid barrier, [2] plain form's finishing-block counter
     CK(cudaMemsetAsync(c->dBar, 0, 4 * sizeof(unsigned), c->st));
@@ -1030,7 +1104,8 @@ static void runInPlaceImpl(ws_ctx *c, char *base, int nIter, int threads, ws_sta
   s.status = WS_RUNNING; s.residual = INFINITY;
   CK(cudaMemcpyAsync(c->dCtl, &s, sizeof(InstCtl), cudaMemcpyHostToDevice, c->st));
   uploadAll<P>(c);
-  if (nIter > 0) CK(launchBatched<P>(devOf<P>(c), c->dInst, c->dCtl, nullptr, 1, nIter, nullptr, threads, 1, c->shortSides, c->st));
+  if (nIter > 0)
+    CK(launchBatched<P>(devOf<P>(c), c->dInst, c->dCtl, nullptr, 1, nIter, nullptr, threads, 1, c->shortSides, anyExt(c), c->st));
   CK(cudaStreamSynchronize(c->st));
   if (out) downloadImpl<P>(c, 0, out);
   if (ctl) { readCtl(c); fillControl(c->ctlHost[0], ctl); }

@@ -21,15 +21,19 @@ namespace wsb {
 enum { PREC_F64 = 0, PREC_MIXED = 1, PREC_F32 = 2 };
 
 template <int P> struct PrecT;
-template <> struct PrecT<PREC_F64> { using R = double; using W = double; using A = double; using U = double; using S = double; static constexpr bool TWO = false; };
-template <> struct PrecT<PREC_MIXED> { using R = float; using W = double; using A = double; using U = double; using S = float; static constexpr bool TWO = true; };
-template <> struct PrecT<PREC_F32> { using R = float; using W = float; using A = float; using U = float; using S = float; static constexpr bool TWO = false; };
+// TINY: a floor for divisors in R that stays a normal number of R
+template <> struct PrecT<PREC_F64> { using R = double; using W = double; using A = double; using U = double; using S = double; static constexpr bool TWO = false; static constexpr double TINY = 1e-300; };
+template <> struct PrecT<PREC_MIXED> { using R = float; using W = double; using A = double; using U = double; using S = float; static constexpr bool TWO = true; static constexpr double TINY = 1e-30; };
+template <> struct PrecT<PREC_F32> { using R = float; using W = float; using A = float; using U = float; using S = float; static constexpr bool TWO = false; static constexpr double TINY = 1e-30; };
 
 // per-instance description (host-written, read-only on the device)
 struct InstDesc {
   int n0, n, m0, m, p0, p, c0, C, k0, K, s0, S;   // first global element and count: nodes, segments, joints, clamps, crossings, strands
   int warmup, ramp_iter, disp_ramp, kd, contacts, max_iter, localLoads;   // localLoads: some node carries a node-frame load
   double ms, damping, tol, strength, stick, tf, eps, slip_rate, lRef, jLenMin, edgeThr;
+  // contact extensions: augmented Lagrangian, W2 rotational friction, W3 seat law (ext: any of them)
+  int ext, aug, alEvery, rotFric, seat, seatGap, dentAfter;
+  double rotFactor, dentRate;
 };
 
 // per-instance control (device-written every iteration)
@@ -38,6 +42,7 @@ struct InstCtl {
   int cur, obuf, disp_it0, stop_at;          // cur: position / frame buffer; obuf: sorted-side buffer
   double ke, ke_prev, residual, res_f, res_t, fref;
   double e_stretch, e_shear, e_bend, e_twist, e_contact;
+  int penN, alPend;    // augmented Lagrangian: iterations in the penetration window; the multiplier update is due
 };
 
 // reduction slots
@@ -97,7 +102,13 @@ struct Dev {
   R *sinT;                  // [ktot] |tA × tB| clipped to [1e-6, 1] at the last evaluation
   uint8_t *ctype;           // [ktot] W1 outputs, filled when a download asks for them
   R *theta, *area, *pres, *util;   // [ktot]
-  R *phiS;                  // [2 ktot]
+  R *phiS;
+  // contact extensions (state): multiplier and the penetration summed since its update; seat depth, climb and wall
+  // slope per side (sd = 2c + side), edge-on-face embedment; W2 reference angle, rotational slip and moment
+  A *lam, *penAcc;          // [ktot]
+  R *dent, *climb, *tanpsi; // [2 ktot]
+  R *dentE, *theta0, *Mrot; // [ktot]
+  A *rotSlip;               // [ktot]                  // [2 ktot]
   // side records, indexed by side position p: the sides (sd = 2c + side) grouped by strand, ascending sd within a
   // strand (the strand's range is [stSideOff, stSideOff + stSideCnt))
   int *sPos;                // [2 ktot] position of side sd

@@ -50,9 +50,9 @@ __device__ __forceinline__ void addPart(Part<A> &q, const A *part, int b, int st
 
 // element e of phase A: the crossings come first (the heaviest elements start earliest; two adjacent elements, one a
 // side, per crossing), then segments, joints, clamps
-template <int P, bool SHORT>
+template <int P, bool SHORT, bool EXT>
 __device__ __forceinline__ void phaseA(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, int e, int nK, Part<typename Dev<P>::A> &pt) {
-  if (e < 2 * nK) { crossing<P, SHORT>(d, I, sx.cur, sx.iter, sx.onxt, sx.obuf, I.k0 + (e >> 1), e & 1, pt); return; }
+  if (e < 2 * nK) { crossing<P, SHORT, EXT>(d, I, sx.cur, sx.iter, sx.onxt, sx.obuf, I.k0 + (e >> 1), e & 1, sx.alPend, sx.penN, pt); return; }
   e -= 2 * nK;
   if (e < I.m) segForce<P>(d, sx.cur, I.m0 + e, pt);
   else if ((e -= I.m) < I.p) jointTorque<P>(d, sx.cur, I.p0 + e, pt);
@@ -121,13 +121,13 @@ __device__ __forceinline__ void forBalanced(const PhaseRun (&runs)[NR], F &&f) {
 }
 
 // phase A of one instance over the block: crossings, segments, joints, clamps
-template <int P, bool SHORT>
+template <int P, bool SHORT, bool EXT>
 __device__ __forceinline__ void blockPhaseA(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, Part<typename Dev<P>::A> &pt) {
   const int nK = (I.contacts && I.K) ? I.K : 0;
   const PhaseRun runs[4] = {{2 * nK, COST_CROSSING}, {I.m, COST_SEGMENT}, {I.p, COST_JOINT}, {I.C, COST_CLAMP}};
   forBalanced(runs, [&](int r, int e) {
     switch (r) {
-      case 0: crossing<P, SHORT>(d, I, sx.cur, sx.iter, sx.onxt, sx.obuf, I.k0 + (e >> 1), e & 1, pt); break;
+      case 0: crossing<P, SHORT, EXT>(d, I, sx.cur, sx.iter, sx.onxt, sx.obuf, I.k0 + (e >> 1), e & 1, sx.alPend, sx.penN, pt); break;
       case 1: segForce<P>(d, sx.cur, I.m0 + e, pt); break;
       case 2: jointTorque<P>(d, sx.cur, I.p0 + e, pt); break;
       default: clampTorque<P>(d, sx.cur, I.c0 + e, pt); break;
@@ -148,7 +148,7 @@ __device__ __forceinline__ void blockPhaseBC(const Dev<P> &d, const InstDesc &I,
 // Block b relaxes instance order[b] (and further instances grid-strided) for up to nIter iterations, stopping at its
 // own convergence.  Instance state lives in HBM / L2; the block's barriers separate the phases, so an instance never
 // waits on another and no kernel spins.
-template <int P, bool SHORT>
+template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                                   const int *__restrict__ order, int nInst, int nIter, const uint8_t *__restrict__ mask) {
   using A = typename Dev<P>::A;
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
       const StepCtx sx = makeCtx<A>(I, sc);
       Part<A> pt;
       pt.init();
-      blockPhaseA<P, SHORT>(d, I, sx, pt);
+      blockPhaseA<P, SHORT, EXT>(d, I, sx, pt);
       __syncthreads();
       if (!SHORT && cx) {
         blockPhaseBC<P>(d, I, sx);
@@ -310,7 +310,7 @@ __device__ __forceinline__ void backupSeg(const Dev<P> &g, const Dev<P> &v, int 
   }
 }
 
-template <int P, bool SHORT>
+template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                                       const int *__restrict__ order, int nInst, int nIter, const uint8_t *__restrict__ mask) {
   using A = typename Dev<P>::A;
@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
       sx.cur = sx.nxt = 0;              // in place
       Part<A> pt;
       pt.init();
-      blockPhaseA<P, SHORT>(v, I, sx, pt);
+      blockPhaseA<P, SHORT, EXT>(v, I, sx, pt);
       __syncthreads();
       if (!SHORT && cx) {
         blockPhaseBC<P>(v, I, sx);
@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
 // The element phase, whole (PART 0) or split in two kernels that run side by side on forked branches of the graph:
 // the crossings (PART 1), whose long per-element code needs many registers, and the segments, joints and clamps
 // (PART 2), which then run at the occupancy of their own, smaller register budget.
-template <int P, bool SHORT, int PART>
+template <int P, bool SHORT, bool EXT, int PART>
 __device__ __forceinline__ void plainA(const Dev<P> &d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
                                        typename Dev<P>::A *part, int partStride) {
   using A = typename Dev<P>::A;
@@ -402,28 +402,28 @@ __device__ __forceinline__ void plainA(const Dev<P> &d, const InstDesc *__restri
   const StepCtx sx = makeCtx<A>(I, c);
   Part<A> pt;
   pt.init();
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nA; e += gridDim.x * blockDim.x) phaseA<P, SHORT>(d, I, sx, base + e, nK, pt);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nA; e += gridDim.x * blockDim.x) phaseA<P, SHORT, EXT>(d, I, sx, base + e, nK, pt);
   constexpr unsigned SM = PART == 1 ? SUMS_CROSS : PART == 2 ? SUMS_ROD : (SUMS_CROSS | SUMS_ROD);
   constexpr unsigned XM = PART == 1 ? MAXS_CROSS : PART == 2 ? MAXS_ROD : (MAXS_CROSS | MAXS_ROD);
   blockReduce<SM, XM>(pt, red);
   if (threadIdx.x == 0) putPart(pt, part, blockIdx.x, partStride);
 }
-template <int P, bool SHORT>
+template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(256, WSB_MINB_A) k_plainA(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
                                                 typename Dev<P>::A *part, int partStride) {
   waitPrevGrid();
   allowNextGrid();
-  plainA<P, SHORT, 0>(d, insts, ctl, part, partStride);
+  plainA<P, SHORT, EXT, 0>(d, insts, ctl, part, partStride);
 }
-template <int P, bool SHORT>
+template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(128) k_plainX(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
                                                 typename Dev<P>::A *part, int partStride) {
-  plainA<P, SHORT, 1>(d, insts, ctl, part, partStride);
+  plainA<P, SHORT, EXT, 1>(d, insts, ctl, part, partStride);
 }
 template <int P, bool SHORT>
 __global__ void __launch_bounds__(256, WSB_MINB_Y) k_plainY(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
                                                 typename Dev<P>::A *part, int partStride) {
-  plainA<P, SHORT, 2>(d, insts, ctl, part, partStride);
+  plainA<P, SHORT, false, 2>(d, insts, ctl, part, partStride);
 }
 template <int P>
 __global__ void __launch_bounds__(256) k_plainBC(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl) {
@@ -534,7 +534,7 @@ __device__ __forceinline__ bool gridSync(unsigned *bar, unsigned nb, int *err) {
 // barriers per iteration with the short-slide order, three with the general one.  Block partials go to part[block];
 // after the barrier every block reduces all of them in the same order and takes the same kinetic-damping decision, so
 // no further broadcast is needed.
-template <int P, bool SHORT>
+template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(256, WSB_MINB_G) k_grid(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                               typename Dev<P>::A *part, unsigned *bar, int *err, int nIter) {
   using A = typename Dev<P>::A;
@@ -553,7 +553,7 @@ __global__ void __launch_bounds__(256, WSB_MINB_G) k_grid(Dev<P> d, const InstDe
     const StepCtx sx = makeCtx<A>(I, sc);
     Part<A> pt;
     pt.init();
-    for (int e = gt; e < nA; e += gs) phaseA<P, SHORT>(d, I, sx, e, cx ? I.K : 0, pt);
+    for (int e = gt; e < nA; e += gs) phaseA<P, SHORT, EXT>(d, I, sx, e, cx ? I.K : 0, pt);
     if (!gridSync(bar, nb, err)) break;
     if (!SHORT && cx) {
       for (int e = gt; e < 2 * I.K + I.m; e += gs) phaseBC<P>(d, I, sx, e);
@@ -637,6 +637,23 @@ __global__ void __launch_bounds__(256) k_classify(Dev<P> d, const InstDesc *__re
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < I.K; e += gridDim.x * blockDim.x) classify<P>(d, I, I.k0 + e);
 }
 
+// the augmented-Lagrangian update of instance b that fell due at the end of its last iteration, applied now (before a
+// download reads the multipliers, a warm start resets their window or new slide coordinates arrive); one block
+template <int P>
+__global__ void __launch_bounds__(256) k_alFlush(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl, int b) {
+  const InstDesc &I = insts[b];
+  const int pend = ctl[b].alPend, penN = ctl[b].penN, iter = ctl[b].iter;
+  __syncthreads();
+  if (!pend) return;
+  for (int e = threadIdx.x; e < I.K; e += blockDim.x) {
+    const int c = I.k0 + e;
+    d.lam[c] = alUpdated<P>(d, I, c, iter, penN, d.lam[c], d.penAcc[c], ro(d.cflag + c));
+    d.penAcc[c] = 0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) { ctl[b].alPend = 0; ctl[b].penN = 0; }
+}
+
 // Download: the requested fields of instance b, interleaved per element as the caller's arrays are (f64, or bytes for
 // the stick / slip flags), packed one after another into `out` for a single copy to the host.
 template <int P>
@@ -674,7 +691,11 @@ __global__ void __launch_bounds__(256) k_pack(Dev<P> d, const InstDesc *__restri
         case PF_PHI: od[e] = double(d.phiS[2 * (I.k0 + i) + k]); break;
         case PF_AREA: od[e] = double(d.area[I.k0 + i]); break;
         case PF_PRES: od[e] = double(d.pres[I.k0 + i]); break;
-        default: od[e] = double(d.util[I.k0 + i]); break;
+        case PF_UTIL: od[e] = double(d.util[I.k0 + i]); break;
+        case PF_LAM: od[e] = double(d.lam[I.k0 + i]); break;
+        case PF_DENT: od[e] = double(d.dent[2 * (I.k0 + i)]) + double(d.dent[2 * (I.k0 + i) + 1]) + double(d.dentE[I.k0 + i]); break;
+        case PF_MROT: od[e] = double(d.Mrot[I.k0 + i]); break;
+        default: od[e] = double(d.rotSlip[I.k0 + i]); break;
       }
     }
   }
@@ -696,6 +717,11 @@ cudaError_t launchUnpack(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, i
   return cudaGetLastError();
 }
 template <int P>
+cudaError_t launchAlFlush(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, int b, cudaStream_t st) {
+  k_alFlush<P><<<1, 256, 0, st>>>(d, insts, ctl, b);
+  return cudaGetLastError();
+}
+template <int P>
 cudaError_t launchClassify(const Dev<P> &d, const InstDesc *insts, int b, int K, cudaStream_t st) {
   if (K <= 0) return cudaSuccess;
   k_classify<P><<<std::max(1, std::min((K + 255) / 256, 148 * 8)), 256, 0, st>>>(d, insts, b);
@@ -710,36 +736,46 @@ cudaError_t launchPack(const Dev<P> &d, const InstDesc *insts, const InstCtl *ct
 }
 
 // ------------------------------------------------------------------------------------------------ launchers
+// the variant of kernel K for the side order (sh) and the contact extensions (ex)
+#define WSB_PICK(K, P, sh, ex) ((sh) ? ((ex) ? K<P, true, true> : K<P, true, false>) : ((ex) ? K<P, false, true> : K<P, false, false>))
+
 template <int P>
 cudaError_t launchBatched(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
-                          const uint8_t *mask, int threads, int blocks, bool shortSides, cudaStream_t st) {
-  if (shortSides) k_batched<P, true><<<blocks, threads, 0, st>>>(d, insts, ctl, order, nInst, nIter, mask);
-  else k_batched<P, false><<<blocks, threads, 0, st>>>(d, insts, ctl, order, nInst, nIter, mask);
+                          const uint8_t *mask, int threads, int blocks, bool shortSides, bool ext, cudaStream_t st) {
+  const auto k = WSB_PICK(k_batched, P, shortSides, ext);
+  k<<<blocks, threads, 0, st>>>(d, insts, ctl, order, nInst, nIter, mask);
   return cudaGetLastError();
 }
 
 // dynamic shared memory of the resident form for a batch whose largest instance needs `bytes` (0 when it does not fit
 // on this device); sets the kernel's limit to it
+// (both variants of the side order, with and without the contact extensions)
 template <int P>
 cudaError_t residentPrepare(size_t bytes, bool shortSides, size_t *granted) {
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  cudaFuncAttributes fa{};
-  cudaError_t e = shortSides ? cudaFuncGetAttributes(&fa, k_resident<P, true>) : cudaFuncGetAttributes(&fa, k_resident<P, false>);
-  if (e != cudaSuccess) return e;
   *granted = 0;
-  if (bytes + fa.sharedSizeBytes > size_t(optin)) return cudaSuccess;
-  e = shortSides ? cudaFuncSetAttribute(k_resident<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes))
-                 : cudaFuncSetAttribute(k_resident<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
-  if (e == cudaSuccess) *granted = bytes;
-  return e;
+  for (int ex = 0; ex < 2; ex++) {
+    const auto k = WSB_PICK(k_resident, P, shortSides, ex != 0);
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, k);
+    if (e != cudaSuccess) return e;
+    if (bytes + fa.sharedSizeBytes > size_t(optin)) return cudaSuccess;
+  }
+  for (int ex = 0; ex < 2; ex++) {
+    const auto k = WSB_PICK(k_resident, P, shortSides, ex != 0);
+    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    if (e != cudaSuccess) return e;
+  }
+  *granted = bytes;
+  return cudaSuccess;
 }
 template <int P>
 cudaError_t launchResident(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
-                           const uint8_t *mask, int threads, size_t smemBytes, bool shortSides, cudaStream_t st) {
-  if (shortSides) k_resident<P, true><<<nInst, threads, smemBytes, st>>>(d, insts, ctl, order, nInst, nIter, mask);
-  else k_resident<P, false><<<nInst, threads, smemBytes, st>>>(d, insts, ctl, order, nInst, nIter, mask);
+                           const uint8_t *mask, int threads, size_t smemBytes, bool shortSides, bool ext, cudaStream_t st) {
+  const auto k = WSB_PICK(k_resident, P, shortSides, ext);
+  k<<<nInst, threads, smemBytes, st>>>(d, insts, ctl, order, nInst, nIter, mask);
   return cudaGetLastError();
 }
 
@@ -761,7 +797,7 @@ static cudaError_t launchPDL(void (*k)(KArgs...), int blocks, cudaStream_t st, A
 
 template <int P>
 cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, const PlainShape &sh, bool contacts,
-                            bool shortSides, cudaStream_t st, int *launches, unsigned *counter, const PlainFork *fork) {
+                            bool shortSides, bool ext, cudaStream_t st, int *launches, unsigned *counter, const PlainFork *fork) {
   using A = typename Dev<P>::A;
   const bool sh2 = shortSides && contacts;
   if (fork && contacts) {
@@ -773,8 +809,8 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
     cudaError_t e;
     if ((e = cudaEventRecord(fork->fork, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(fork->side, fork->fork, 0)) != cudaSuccess) return e;
-    if (sh2) k_plainX<P, true><<<sh.blocksX, 128, 0, fork->side>>>(d, insts, ctl, px, nParts);
-    else k_plainX<P, false><<<sh.blocksX, 128, 0, fork->side>>>(d, insts, ctl, px, nParts);
+    const auto kx = WSB_PICK(k_plainX, P, sh2, ext);
+    kx<<<sh.blocksX, 128, 0, fork->side>>>(d, insts, ctl, px, nParts);
     if ((e = cudaEventRecord(fork->join, fork->side)) != cudaSuccess) return e;
     if (sh2) k_plainY<P, true><<<sh.blocksY, 256, 0, st>>>(d, insts, ctl, py, nParts);
     else k_plainY<P, false><<<sh.blocksY, 256, 0, st>>>(d, insts, ctl, py, nParts);
@@ -798,8 +834,7 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
   }
   const int nD = sh2 ? sh.blocksDS : sh.blocksD, nParts = sh.blocksA + nD;
   A *pa = static_cast<A *>(part), *pd = pa + sh.blocksA;      // value-major rows of nParts: A's blocks, then D's
-  cudaError_t e = sh2 ? launchPDL(k_plainA<P, true>, sh.blocksA, st, d, insts, ctl, pa, nParts)
-                      : launchPDL(k_plainA<P, false>, sh.blocksA, st, d, insts, ctl, pa, nParts);
+  cudaError_t e = launchPDL(WSB_PICK(k_plainA, P, sh2, ext), sh.blocksA, st, d, insts, ctl, pa, nParts);
   if (e != cudaSuccess) return e;
   int nl = 1;
   if (contacts && !sh2) {
@@ -816,40 +851,40 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
 
 template <int P>
 cudaError_t launchGrid(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, unsigned *bar, int *err, int nIter,
-                       int blocks, bool shortSides, cudaStream_t st) {
+                       int blocks, bool shortSides, bool ext, cudaStream_t st) {
   using A = typename Dev<P>::A;
   A *pa = static_cast<A *>(part);
   void *args[] = {(void *)&d, (void *)&insts, (void *)&ctl, (void *)&pa, (void *)&bar, (void *)&err, (void *)&nIter};
-  const void *k = shortSides ? (const void *)k_grid<P, true> : (const void *)k_grid<P, false>;
+  const void *k = (const void *)WSB_PICK(k_grid, P, shortSides, ext);
   return cudaLaunchCooperativeKernel(k, dim3(blocks), dim3(256), args, 0, st);
 }
 // co-resident blocks of the grid form: SMs × resident blocks per SM of the kernel variant that runs
 template <int P>
-int gridBlocks(bool shortSides) {
+int gridBlocks(bool shortSides, bool ext) {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (shortSides) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_grid<P, true>, 256, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_grid<P, false>, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, WSB_PICK(k_grid, P, shortSides, ext), 256, 0);
   return sms * (per > 0 ? per : 1);
 }
 
 #define WSB_INST(P)                                                                                                  \
   template cudaError_t launchBatched<P>(const Dev<P> &, const InstDesc *, InstCtl *, const int *, int, int, const uint8_t *, \
-                                        int, int, bool, cudaStream_t);                                               \
+                                        int, int, bool, bool, cudaStream_t);                                         \
   template cudaError_t launchPlainIter<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, const PlainShape &, bool,    \
-                                          bool, cudaStream_t, int *, unsigned *, const PlainFork *);                 \
+                                          bool, bool, cudaStream_t, int *, unsigned *, const PlainFork *);           \
   template cudaError_t launchGrid<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, unsigned *, int *, int, int, bool, \
-                                     cudaStream_t);                                                                  \
-  template int gridBlocks<P>(bool);                                                                                 \
+                                     bool, cudaStream_t);                                                            \
+  template int gridBlocks<P>(bool, bool);                                                                           \
   template cudaError_t launchUnpack<P>(const Dev<P> &, const InstDesc *, InstCtl *, int, const double *, int, int, int, bool, \
                                        bool, bool, cudaStream_t);                                                    \
   template cudaError_t launchPack<P>(const Dev<P> &, const InstDesc *, const InstCtl *, int, const PackList &, size_t,      \
                                      unsigned char *, cudaStream_t);                                                 \
   template cudaError_t launchClassify<P>(const Dev<P> &, const InstDesc *, int, int, cudaStream_t);                \
+  template cudaError_t launchAlFlush<P>(const Dev<P> &, const InstDesc *, InstCtl *, int, cudaStream_t);           \
   template cudaError_t residentPrepare<P>(size_t, bool, size_t *);                                                   \
   template cudaError_t launchResident<P>(const Dev<P> &, const InstDesc *, InstCtl *, const int *, int, int, const uint8_t *, \
-                                         int, size_t, bool, cudaStream_t);
+                                         int, size_t, bool, bool, cudaStream_t);
 WSB_INST(PREC_F64)
 WSB_INST(PREC_MIXED)
 WSB_INST(PREC_F32)

@@ -16,25 +16,29 @@ struct PlainFork { cudaStream_t side; cudaEvent_t fork, join, fork2, join2; };
 
 template <int P>
 cudaError_t launchBatched(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
-                          const uint8_t *mask, int threads, int blocks, bool shortSides, cudaStream_t st);
+                          const uint8_t *mask, int threads, int blocks, bool shortSides, bool ext, cudaStream_t st);
+// ext: some instance runs a contact extension (the crossing kernels' variant that has them)
 template <int P>
 cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, const PlainShape &sh, bool contacts,
-                            bool shortSides, cudaStream_t st, int *launches, unsigned *counter, const PlainFork *fork);
+                            bool shortSides, bool ext, cudaStream_t st, int *launches, unsigned *counter, const PlainFork *fork);
 
 template <int P>
 cudaError_t launchGrid(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, unsigned *bar, int *err, int nIter,
-                       int blocks, bool shortSides, cudaStream_t st);
+                       int blocks, bool shortSides, bool ext, cudaStream_t st);
 template <int P>
-int gridBlocks(bool shortSides);
-// resident form: checks that `bytes` of dynamic shared memory fit a block on this device and opts the kernel in
-// (*granted = bytes), else *granted = 0
+int gridBlocks(bool shortSides, bool ext);
+// resident form: checks that `bytes` of dynamic shared memory fit a block on this device and opts the kernel in, with
+// and without the contact extensions (*granted = bytes), else *granted = 0
 template <int P>
 cudaError_t residentPrepare(size_t bytes, bool shortSides, size_t *granted);
 // host <-> device transfers of one instance's state (interleaved per element, as the C ABI's arrays are)
 enum { PF_X, PF_Q, PF_V, PF_W, PF_U, PF_NPREV, PF_SLIP, PF_FN, PF_FT, PF_GAP, PF_N, PF_VSH, PF_M, PF_REACT, PF_STUCK, PF_STATE,
-       PF_CTYPE, PF_THETA, PF_PHI, PF_AREA, PF_PRES, PF_UTIL };
+       PF_CTYPE, PF_THETA, PF_PHI, PF_AREA, PF_PRES, PF_UTIL, PF_LAM, PF_DENT, PF_MROT, PF_RSLIP };
 struct PackField { int kind, count, ncomp; long long off; };   // off: byte offset in the packed buffer
-struct PackList { PackField f[24]; int nf; };
+struct PackList { PackField f[28]; int nf; };
+// the multiplier update of instance b that fell due at the end of its last iteration, applied now
+template <int P>
+cudaError_t launchAlFlush(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, int b, cudaStream_t st);
 // the W1 classification of instance b's crossings into the device output arrays
 template <int P>
 cudaError_t launchClassify(const Dev<P> &d, const InstDesc *insts, int b, int K, cudaStream_t st);
@@ -46,6 +50,6 @@ cudaError_t launchPack(const Dev<P> &d, const InstDesc *insts, const InstCtl *ct
                        unsigned char *out, cudaStream_t st);
 template <int P>
 cudaError_t launchResident(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
-                           const uint8_t *mask, int threads, size_t smemBytes, bool shortSides, cudaStream_t st);
+                           const uint8_t *mask, int threads, size_t smemBytes, bool shortSides, bool ext, cudaStream_t st);
 
 }  // namespace wsb

@@ -25,6 +25,8 @@ namespace wsb {
 static constexpr double SUPPORT_SMOOTH = 0.03;                // solver_cpu.js:16
 static constexpr double TWIST_RATE_MAX = 0.5 * SUPPORT_SMOOTH;  // solver_cpu.js:21
 static constexpr double ROLL_DAMP = 0.5;                      // solver_cpu.js:28
+static constexpr double AL_FREE_MIN = 0.25;                   // solver_cpu.js:33
+static constexpr double PI_D = 3.141592653589793;             // Math.PI
 
 // ------------------------------------------------------------------------------------------------ math helpers
 __device__ __forceinline__ float msqrt(float x) { return sqrtf(x); }
@@ -39,6 +41,18 @@ __device__ __forceinline__ void msincos(float x, float *s, float *c) { sincosf(x
 __device__ __forceinline__ void msincos(double x, double *s, double *c) { sincos(x, s, c); }
 __device__ __forceinline__ float mfloor(float x) { return floorf(x); }
 __device__ __forceinline__ double mfloor(double x) { return floor(x); }
+__device__ __forceinline__ float msin(float x) { return sinf(x); }
+__device__ __forceinline__ double msin(double x) { return sin(x); }
+__device__ __forceinline__ float mcos(float x) { return cosf(x); }
+__device__ __forceinline__ double mcos(double x) { return cos(x); }
+__device__ __forceinline__ float mtan(float x) { return tanf(x); }
+__device__ __forceinline__ double mtan(double x) { return tan(x); }
+__device__ __forceinline__ float macos(float x) { return acosf(x); }
+__device__ __forceinline__ double macos(double x) { return acos(x); }
+__device__ __forceinline__ float mfmod(float x, float y) { return fmodf(x, y); }
+__device__ __forceinline__ double mfmod(double x, double y) { return fmod(x, y); }
+// Math.sign: −1, 0 or +1
+template <class T> __device__ __forceinline__ T msign(T v) { return v > T(0) ? T(1) : (v < T(0) ? T(-1) : T(0)); }
 template <class T> __device__ __forceinline__ T mmin(T a, T b) { return a < b ? a : b; }
 template <class T> __device__ __forceinline__ T mmax(T a, T b) { return a > b ? a : b; }
 template <class T> __device__ __forceinline__ T mabs(T a) { return a < T(0) ? -a : a; }
@@ -324,17 +338,117 @@ __device__ __forceinline__ R support(const R Rf[9], const R n[3], R sign, R w, R
   return hh;
 }
 
-// crossing c: one evaluation of PolylineContact.apply (solver_cpu.js:381-478) without the seat law, the augmented
-// Lagrangian and the rotational friction, by two adjacent lanes of a warp, one a side.  Each lane evaluates its side
+// ------------------------------------------------------------------------------------------------ W1 / W2 / W3 / AL
+// W1 per side (PolylineContact._classify, solver_cpu.js:234-244): does the side bear on an edge, the width of its
+// contact face, the depth behind it, and the roll of its section against the contact plane, from the contact normal in
+// the side's section frame (nx, ny)
+template <class R>
+__device__ __forceinline__ void sideClass(R nx, R ny, R wk, R hk, double thr, int &edge, R &cFace, R &Z0, R &phi) {
+  const R sx = mabs(mtanh(nx / R(SUPPORT_SMOOTH))), sy = mabs(mtanh(ny / R(SUPPORT_SMOOTH)));
+  edge = sx * sy > R(thr) ? 1 : 0;
+  const bool yFace = mabs(ny) >= mabs(nx);
+  cFace = yFace ? wk : hk;
+  Z0 = yFace ? hk : wk;
+  phi = matan2(mmin(mabs(nx), mabs(ny)), mmax(mmax(mabs(nx), mabs(ny)), R(1e-12)));
+}
+// W1 per crossing (solver_cpu.js:245-269): type (edges bearing), face side of an edge-on-face contact, nominal area,
+// pressure and utilisation from both sides' terms, the crossing angle's sine and |Fn|
+template <class R>
+struct ClassOut { int ctype, faceSide; R area, pres, util; };
+template <class R>
+__device__ __forceinline__ ClassOut<R> classCore(int e0, int e1, R cf0, R cf1, R z0, R z1, R ph0, R ph1, R sinT, R fn,
+                                                 R fc0, R fc1, R E0, R E1, R H0, R H1) {
+  ClassOut<R> o;
+  const int nEdge = e0 + e1;
+  o.ctype = nEdge;
+  o.faceSide = nEdge == 1 ? (e1 ? 0 : 1) : -1;
+  R Aa = cf0 * cf1 / sinT, pres = fn / mmax(Aa, R(1e-12));
+  R ut = pres / mmax(mmin(H0, H1), R(1e-12));
+  if (nEdge == 1) {
+    const bool f1 = e1 == 0;          // face side 1 (side 0 bears the edge)
+    const R cfF = f1 ? cf1 : cf0, cfE = f1 ? cf0 : cf1, zF = f1 ? z1 : z0, EF = f1 ? E1 : E0;
+    const R phE = f1 ? ph0 : ph1, fcE = f1 ? fc0 : fc1;
+    const R ell = cfF / sinT, kap = EF / mmax(zF, R(1e-12));
+    const R phiE = mmax(phE, R(1e-4));
+    const R b = msqrt(R(2) * fn / mmax(ell * kap * phiE, R(1e-12)));
+    const bool full = b >= cfE;
+    const R Afe = full ? cf0 * cf1 / sinT : b * ell;
+    const R pfe = full ? fn / mmax(Afe, R(1e-12)) : kap * phiE * b;
+    Aa = Afe; pres = pfe; ut = pfe / mmax(fcE, R(1e-12));
+  } else if (nEdge == 2) {
+    const R fc = mmin(fc0, fc1);
+    Aa = fn / mmax(fc, R(1e-12)); pres = fn > R(0) ? fc : R(0); ut = fn > R(0) ? R(1) : R(0);
+  }
+  o.area = Aa; o.pres = pres; o.util = ut;
+  return o;
+}
+// W3: n × t of the cutting side, normalised: the direction across that side's seat (solver_cpu.js:302-303, 320-321)
+template <class R>
+__device__ __forceinline__ void wallAxis(const R n[3], const R t[3], R m[3]) {
+  cross3(n, t, m);
+  const R ml = mmax(msqrt(dot3(m, m)), R(1e-12));
+  m[0] /= ml; m[1] /= ml; m[2] /= ml;
+}
+// W3: slope tan ψ of the seat wall that sliding along m climbs, from the cutting side's section axes X, Y with sign sg
+// (_walls, solver_cpu.js:284-292)
+template <class R>
+__device__ __forceinline__ R wallSlope(R sg, const R X[3], const R Y[3], const R n[3], const R m[3]) {
+  const R nx = (n[0] * X[0] + n[1] * X[1] + n[2] * X[2]) * sg, ny = (n[0] * Y[0] + n[1] * Y[1] + n[2] * Y[2]) * sg;
+  const R sx = msign(nx), sy = msign(ny);
+  const R fx[3] = {sx * X[0], sx * X[1], sx * X[2]}, fy[3] = {sy * Y[0], sy * Y[1], sy * Y[2]};
+  const bool useX = (fx[0] * m[0] + fx[1] * m[1] + fx[2] * m[2]) > R(0);
+  R f[3];
+  for (int k = 0; k < 3; k++) f[k] = useX ? fx[k] : fy[k];
+  const R cosPsi = mmin(mmax(mabs(f[0] * n[0] + f[1] * n[1] + f[2] * n[2]), R(1e-6)), R(1));
+  return mtan(macos(cosPsi));
+}
+// augmented Lagrangian: crossing c's multiplier after the Uzawa step on its window-mean penetration, with the
+// safeguards (alValue / updateMultipliers, solver_cpu.js:483-506): none on a disabled crossing or on one whose contact
+// point sits on supported nodes (free weight of either side under AL_FREE_MIN, from the current slide coordinates),
+// and |λ| at most the crushing capacity min fc90 · wA wB / sin θ with θ of the last evaluation.  `iter` is the
+// iteration about to run: the update belongs to the end of the one before, at that iteration's ramp.
+template <int P>
+__device__ __forceinline__ typename Dev<P>::A alUpdated(const Dev<P> &d, const InstDesc &I, int c, int iter, int penN,
+                                                        typename Dev<P>::A lam, typename Dev<P>::A pacc, uint8_t fl) {
+  using A = typename Dev<P>::A; using U = typename Dev<P>::U;
+  const bool enabled = fl & 1, locked = fl & 2;
+  bool pinned = false;
+  for (int side = 0; side < 2; side++) {
+    const int o = side * d.ktot + c;
+    const U uu = d.u[side * d.kS + c];
+    const int nseg = ro(d.cxNseg + o);
+    const int li = int(mmin(mmax(mfloor(uu), U(0)), U(mmax(nseg - 1, 0))));
+    const double t = double(mmin(mmax(uu - U(li), U(0)), U(1)));
+    const int sg = ro(d.cxSegOff + o) + li;
+    const int a = ro(d.segI0 + sg), b = ro(d.segI1 + sg);
+    const bool fa = (ro(d.nflag + a) & 7) == 0, fb = (ro(d.nflag + b) & 7) == 0;
+    const double w = (fa ? 0.0 : (1 - t) * (1 - t)) + (fb ? 0.0 : t * t);
+    pinned = pinned || w < AL_FREE_MIN;
+  }
+  if (!enabled || pinned) return A(0);
+  const double cap = fmin(double(d.fc90[c]), double(d.fc90[d.ktot + c])) * double(d.wk[c]) * double(d.wk[d.ktot + c]) /
+                     fmax(sin(asin(double(d.sinT[c]))), 1e-6);
+  const double rampPrev = I.ramp_iter <= 0 ? 1.0 : fmin(1.0, 0.01 + 0.99 * double(iter - 1) / I.ramp_iter);
+  const double kn = rampPrev * I.strength;
+  double v = double(lam) + kn * (double(pacc) / double(max(penN, 1)));
+  if (!locked) v = fmax(v, 0.0);
+  return A(fmin(fmax(v, -cap), cap));
+}
+
+// crossing c: one evaluation of PolylineContact.apply (solver_cpu.js:381-478) by two adjacent lanes of a warp, one a
+// side.  Each lane evaluates its side
 // (Hermite point and tangent with node tangents and frames from the neighbours, the nlerp frame); the lanes swap those
 // results with pair shuffles and both run the contact law on the same values (the same instructions on the same inputs,
 // so the same results).  Each lane writes its side's records and key; the side-0 lane writes the crossing's own
 // outputs and adds to the reductions.  Side records go to the side's strand position (general order) or, with SHORT,
 // straight to its position in this iteration's sorted order, so the gathers read them without an indirection.
 // kb: the buffer that receives the keys after the slide (the next sorted order's); ob: this iteration's sorted order.
-template <int P, bool SHORT>
+// The contact extensions run when the instance has them: the augmented-Lagrangian gap (with the multiplier update that
+// fell due at the end of the last iteration, alPend, over a window of penN iterations), the W3 seat law and the W2
+// rotational friction, which both classify the contact (W1) within the iteration.
+template <int P, bool SHORT, bool EXT>
 __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int buf, int iter, int kb, int ob, int c, int side,
-                                         Part<typename Dev<P>::A> &pt) {
+                                         int alPend, int penN, Part<typename Dev<P>::A> &pt) {
   using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A; using U = typename Dev<P>::U;
   const int kt_ = d.ktot, ks = d.kS, K2 = d.sS;
   const unsigned pair = 3u << ((threadIdx.x & 31) & 30);
@@ -346,6 +460,17 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   const R muc = ro(d.mu + c), wkA = ro(d.wk + c), hkA = ro(d.hk + c), wkB = ro(d.wk + kt_ + c), hkB = ro(d.hk + kt_ + c);
   const R hc = ro(d.ch + c), wc = ro(d.cw + c);
   const A slip0 = d.slip[c];
+  // contact-extension state (this lane's side for the per-side arrays)
+  R dentMe = R(0), dentO = R(0), climbMe = R(0), tanpsiMe = R(1), dentE0 = R(0), th0 = R(0);
+  A lamc = A(0), pacc = A(0), rslip = A(0);
+  if constexpr (EXT) {
+    if (EXT && I.seat) {
+      dentMe = d.dent[2 * c + side]; dentO = d.dent[2 * c + 1 - side]; climbMe = d.climb[2 * c + side];
+      tanpsiMe = d.tanpsi[2 * c + side]; dentE0 = d.dentE[c];
+    }
+    if (EXT && I.aug) { lamc = d.lam[c]; pacc = d.penAcc[c]; }
+    if (EXT && I.rotFric) { th0 = d.theta0[c]; rslip = d.rotSlip[c]; }
+  }
   const double rampN = I.ramp_iter;
   const double rampd = rampN <= 0 ? 1.0 : fmin(1.0, 0.01 + 0.99 * double(iter) / rampN);
   const R kn = R(rampd * I.strength), kt = R(rampd * I.stick);
@@ -414,6 +539,7 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   // contact normal with side persistence (solver_cpu.js:396-402)
   R nv[3];
   cross3(tA, tB, nv);
+  const R crw[3] = {nv[0], nv[1], nv[2]};    // tA × tB before normalisation (W2 angle)
   const R nn = msqrt(dot3(nv, nv));
   if (nn < R(1e-6)) { nv[0] = np[0]; nv[1] = np[1]; nv[2] = np[2]; }
   else { const R dn = mmax(nn, R(1e-12)); nv[0] /= dn; nv[1] /= dn; nv[2] /= dn; }
@@ -425,10 +551,23 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   R rA[3], rB[3];
   const R hA = support(Rf[0], nv, R(1), wkA, hkA, rA);
   const R hB = support(Rf[1], nv, R(-1), wkB, hkB, rB);
-  const R pen = (hA + hB) - g;
+  R D = hA + hB;
+  if (EXT && I.seat && I.seatGap) D -= (s1 ? dentO + dentMe : dentMe + dentO) + dentE0;     // W3 (solver_cpu.js:410)
+  const R pen = D - g;
   const bool enabled = fl & 1, locked = fl & 2;
-  const bool active = (pen > R(0) || locked) && enabled;
-  const R Fn = active ? kn * pen : R(0);
+  bool active;
+  R Fn;
+  if (EXT && I.aug) {
+    // the Uzawa step that fell due after the last iteration, then the penetration window (solver_cpu.js:412-418)
+    if (alPend) { lamc = alUpdated<P>(d, I, c, iter, penN, lamc, pacc, fl); pacc = A(0); }
+    if (iter >= I.ramp_iter) pacc += A(pen);
+    const R trial = R(lamc) + kn * pen;
+    active = (trial > R(0) || locked) && enabled;
+    Fn = active ? (locked ? trial : mmax(trial, R(0))) : R(0);
+  } else {
+    active = (pen > R(0) || locked) && enabled;
+    Fn = active ? kn * pen : R(0);
+  }
   // tangential spring / stick-slip: S_t = a tA + b tB
   const R St[3] = {S[0] - g * nv[0], S[1] - g * nv[1], S[2] - g * nv[2]};
   const R taa = dot3(tA, tA), tbb = dot3(tB, tB), tab = dot3(tA, tB);
@@ -437,7 +576,29 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   const bool ok = det > R(1e-8);
   const R ca = ok ? (sa * tbb - sb * tab) / det : R(0), cb = ok ? (sb * taa - sa * tab) / det : R(0);
   const R Ftv = msqrt((kt * St[0]) * (kt * St[0]) + (kt * St[1]) * (kt * St[1]) + (kt * St[2]) * (kt * St[2]));
-  const R limit = muc * mabs(Fn);
+  // W3: the seats' walls raise the friction against the slide direction (_seatFriction, solver_cpu.js:294-313); this
+  // lane takes the term of its own side's seat, cut by the other side
+  R muDir = muc;
+  R wm[3] = {R(0), R(0), R(0)};       // wall axis of this side's seat: n × the other side's tangent, normalised
+  if (EXT && I.seat) {
+    R tc[3], Xo[3], Yo[3];
+    for (int k = 0; k < 3; k++) { tc[k] = s1 ? tg[0][k] : tg[1][k]; Xo[k] = s1 ? Rf[0][k] : Rf[1][k]; Yo[k] = s1 ? Rf[0][3 + k] : Rf[1][3 + k]; }
+    wallAxis(nv, tc, wm);
+    const R nrm = msqrt(dot3(St, St));
+    R addMe = R(0);
+    if (dentMe > R(0) && nrm > R(1e-12)) {
+      const R dn = mmax(nrm, R(1e-12)), sgn = s1 ? R(-1) : R(1);
+      const R dhat[3] = {St[0] / dn, St[1] / dn, St[2] / dn};
+      const R dj = dot3(dhat, wm) * sgn;
+      const R wd[3] = {msign(dj) * wm[0] * sgn, msign(dj) * wm[1] * sgn, msign(dj) * wm[2] * sgn};
+      tanpsiMe = wallSlope(s1 ? R(1) : R(-1), Xo, Yo, nv, wd);
+      const R add = mabs(dj) * (muc * tanpsiMe < R(1) ? (muc + tanpsiMe) / mmax(R(1) - muc * tanpsiMe, R(1e-6)) - muc : R(9) * muc);
+      addMe = mmin(add, R(9) * muc);
+    }
+    const R addO = __shfl_xor_sync(pair, addMe, 1);
+    muDir = (muc + (s1 ? addO : addMe)) + (s1 ? addMe : addO);
+  }
+  const R limit = muDir * mabs(Fn);
   const bool slip = active && ok && !locked && Ftv > limit;
   const bool freeS = !active && ok && enabled;
   R scale = R(0);
@@ -458,6 +619,79 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   const R fT[3] = {kt * Se[0], kt * Se[1], kt * Se[2]};
   R FA[3];
   for (int k = 0; k < 3; k++) FA[k] = -Fn * nv[k] + fT[k];
+  const R sgS = side ? R(-1) : R(1);
+  const R nxMe = dot3(nv, Xm) * sgS, nyMe = dot3(nv, Ym) * sgS;    // the normal in this side's section frame
+  const R sinTc = mmin(mmax(nn, R(1e-6)), R(1));
+  R Mrot = R(0), eRot = R(0);
+  if (EXT && (I.seat || I.rotFric)) {
+    // W1 within the iteration (solver_cpu.js:460): each lane its side's terms, swapped, both lanes the crossing's
+    int eMe;
+    R cfMe, zMe, phMe;
+    sideClass(nxMe, nyMe, side ? wkB : wkA, side ? hkB : hkA, I.edgeThr, eMe, cfMe, zMe, phMe);
+    const int eO = __shfl_xor_sync(pair, eMe, 1);
+    const R cfO = __shfl_xor_sync(pair, cfMe, 1), zO = __shfl_xor_sync(pair, zMe, 1), phO = __shfl_xor_sync(pair, phMe, 1);
+    const int e0 = s1 ? eO : eMe, e1 = s1 ? eMe : eO;
+    const R cf0 = s1 ? cfO : cfMe, cf1 = s1 ? cfMe : cfO, z0 = s1 ? zO : zMe, z1 = s1 ? zMe : zO;
+    const R ph0 = s1 ? phO : phMe, ph1 = s1 ? phMe : phO;
+    const R fc0 = ro(d.fc90 + c), fc1 = ro(d.fc90 + kt_ + c);
+    const ClassOut<R> co = classCore(e0, e1, cf0, cf1, z0, z1, ph0, ph1, sinTc, mabs(Fn), fc0, fc1, ro(d.E90 + c),
+                                     ro(d.E90 + kt_ + c), ro(d.Hs + c), ro(d.Hs + kt_ + c));
+    const R thetaC = masin(sinTc);
+    if (EXT && I.seat) {
+      // W3: climbing out of this side's seat, seat growth under an edge (_seatUpdate, solver_cpu.js:315-344)
+      R inc[3];
+      for (int k = 0; k < 3; k++) inc[k] = da * tA[k] - db * tB[k];
+      const R step = dot3(inc, wm) * sgS;
+      R dn = dentMe, cl = climbMe, dE = dentE0;
+      const bool has = dn > R(0);
+      if (has && slip) cl += step;
+      if (has && mabs(cl) >= dn / mmax(tanpsiMe, R(1e-6))) { dn = R(0); cl = R(0); }
+      if (iter >= I.dentAfter) {
+        const R sinp0 = msin(ph0) * mcos(ph0), sinp1 = msin(ph1) * mcos(ph1);
+        const R sT = msin(thetaC);
+        if (co.ctype == 2 && active && !locked) {
+          const R fc = mmin(fc0, fc1);
+          const R dEst = msqrt(mabs(Fn) / mmax(fc, R(1e-12)) * sT * sinp0 * sinp1);
+          dn = mmax(dn, mmin(dn + R(I.dentRate) * dEst, dEst));
+        }
+        if (co.ctype == 1 && active && !locked) {
+          const bool f1 = co.faceSide == 1;
+          const R ell = (f1 ? cf1 : cf0) / mmax(sT, R(1e-6));
+          dE = mmax(dE, mabs(Fn) / mmax((f1 ? fc0 : fc1) * ell, R(1e-12)) * (f1 ? sinp0 : sinp1));
+        }
+      }
+      d.dent[2 * c + side] = dn; d.climb[2 * c + side] = cl; d.tanpsi[2 * c + side] = tanpsiMe;
+      if (side == 0) d.dentE[c] = dE;
+    }
+    if (EXT && I.rotFric) {
+      // W2: the scissor moment about n with Coulomb's limit on it (_rotationalFriction, solver_cpu.js:347-379)
+      const R th = matan2(dot3(crw, nv), dot3(tA, tB));
+      if (isnan(th0) && active) th0 = th;
+      const bool ok = active && !isnan(th0);
+      const R sTc = mmax(msin(thetaC), R(1e-6));
+      R req = R(0.38) * msqrt(wkA * wkB / sTc);
+      if (co.ctype == 1) req = R(0.25) * (co.faceSide == 0 ? wkA : wkB) / sTc;
+      else if (co.ctype == 2) req = R(0.38) * msqrt(mmax(co.area, R(1e-12)));
+      const R kr = kt * req * req;
+      const R PI = R(PI_D);
+      R dth = ok ? th - th0 : R(0);
+      dth = mfmod(mfmod(dth + PI, R(2) * PI) + R(2) * PI, R(2) * PI) - PI;
+      R Mc = kr * dth;
+      if (ok && !locked) {
+        const R Mlim = R(I.rotFactor) * muc * mabs(Fn) * req;
+        if (mabs(Mc) > Mlim) {
+          const R rate = R(mclamp(I.slip_rate, 1e-3, 1.0));
+          R adv = rate * (R(1) - Mlim / mmax(mabs(Mc), R(1e-12))) * dth;
+          adv = mclamp(adv, R(-0.05), R(0.05));
+          th0 += adv; rslip += A(mabs(adv)); dth -= adv;
+          Mc = kr * dth;
+        }
+      }
+      Mrot = ok ? Mc : R(0);
+      eRot = kr * dth * dth;
+      if (side == 0) { d.theta0[c] = th0; d.rotSlip[c] = rslip; d.Mrot[c] = Mrot; }
+    }
+  }
   // side records for the gathers: t before the slide, force on the side, lever torque tf (r × F); the righting
   // stiffness of the support point (addTwistStiffness, solver_cpu.js:170-176) goes to the segments the sides sit on
   // after the slide
@@ -473,17 +707,18 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
     d.Ft[c] = msqrt(dot3(fT, fT));
     d.cstate[c] = slip ? 1 : 0;
     d.gap[c] = g;
-    pt.s[RS_PEN] += A(active ? kn * pen * pen : R(0));
+    // penalty energy (k_n pen², or Fn²/k_n with the multiplier) and the W2 spring's k_r Δθ² (solver_cpu.js:469,378)
+    pt.s[RS_PEN] += A(active ? (EXT && I.aug ? Fn * Fn / mmax(kn, R(PrecT<P>::TINY)) : kn * pen * pen) : R(0)) + A(eRot);
+    if (EXT && I.aug) { d.lam[c] = lamc; d.penAcc[c] = pacc; }
     pt.s[RS_TAN] += A(dot3(Se, Se));
     pt.x[RX_FN] = mmax(pt.x[RX_FN], A(Fn));
   }
   d.u[side * ks + c] = un;
   {
     // what the W1 classification needs of this evaluation: the normal in the side's section frame, the crossing angle
-    const R sg = side ? R(-1) : R(1);
-    d.sProj[2 * c + side] = dot3(nv, Xm) * sg;
-    d.sProj[2 * size_t(kt_) + 2 * c + side] = dot3(nv, Ym) * sg;
-    if (side == 0) d.sinT[c] = mmin(mmax(nn, R(1e-6)), R(1));
+    d.sProj[2 * c + side] = nxMe;
+    d.sProj[2 * size_t(kt_) + 2 * c + side] = nyMe;
+    if (side == 0) d.sinT[c] = sinTc;
   }
   // the side's segment after the slide (solver_cpu.js:144-149): the key of the next sort, into key buffer kb
   const int key = int(mmin(mmax(mfloor(un), U(0)), U(mmax(nseg - 1, 0))));
@@ -496,7 +731,9 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
     cross3(side ? rB : rA, F, tq);
     d.sT[rec] = tpm;
     d.kth[rec] = kth;
-    for (int k = 0; k < 3; k++) { d.sF[k * K2 + rec] = F[k]; d.sTq[k * K2 + rec] = tf * tq[k]; }
+    // lever torque, and the W2 moment about n: +M on side A's segment, −M on side B's
+    const R Ms = sgn * Mrot;
+    for (int k = 0; k < 3; k++) { d.sF[k * K2 + rec] = F[k]; d.sTq[k * K2 + rec] = tf * tq[k] + Ms * nv[k]; }
   }
 }
 
@@ -507,40 +744,17 @@ template <int P>
 __device__ __forceinline__ void classify(const Dev<P> &d, const InstDesc &I, int c) {
   using R = typename Dev<P>::R;
   const int kt_ = d.ktot, K2 = 2 * kt_;
-  R cFace[2], Z0[2], phi[2];
-  int edge[2];
-  for (int side = 0; side < 2; side++) {
-    const int sd = 2 * c + side, o = side * kt_ + c;
-    const R nx = d.sProj[sd], ny = d.sProj[K2 + sd];
-    const R sx = mabs(mtanh(nx / R(SUPPORT_SMOOTH))), sy = mabs(mtanh(ny / R(SUPPORT_SMOOTH)));
-    edge[side] = sx * sy > R(I.edgeThr) ? 1 : 0;
-    const bool yFace = mabs(ny) >= mabs(nx);
-    cFace[side] = yFace ? d.wk[o] : d.hk[o];
-    Z0[side] = yFace ? d.hk[o] : d.wk[o];
-    phi[side] = matan2(mmin(mabs(nx), mabs(ny)), mmax(mmax(mabs(nx), mabs(ny)), R(1e-12)));
-    d.phiS[sd] = phi[side];
-  }
+  int e0, e1;
+  R cf0, cf1, z0, z1, ph0, ph1;
+  sideClass(d.sProj[2 * c], d.sProj[K2 + 2 * c], d.wk[c], d.hk[c], I.edgeThr, e0, cf0, z0, ph0);
+  sideClass(d.sProj[2 * c + 1], d.sProj[K2 + 2 * c + 1], d.wk[kt_ + c], d.hk[kt_ + c], I.edgeThr, e1, cf1, z1, ph1);
   const R sinT = d.sinT[c];
-  const int nEdge = edge[0] + edge[1];
-  const R Fn = mabs(d.Fn[c]);
-  R Aa = cFace[0] * cFace[1] / sinT, pres = Fn / mmax(Aa, R(1e-12));
-  R ut = pres / mmax(mmin(d.Hs[c], d.Hs[kt_ + c]), R(1e-12));
-  if (nEdge == 1) {
-    const int fs = edge[1] ? 0 : 1, es = 1 - fs;
-    const R ell = cFace[fs] / sinT, kap = d.E90[fs * kt_ + c] / mmax(Z0[fs], R(1e-12));
-    const R phiE = mmax(phi[es], R(1e-4));
-    const R b = msqrt(R(2) * Fn / mmax(ell * kap * phiE, R(1e-12)));
-    const bool full = b >= cFace[es];
-    const R Afe = full ? cFace[0] * cFace[1] / sinT : b * ell;
-    const R pfe = full ? Fn / mmax(Afe, R(1e-12)) : kap * phiE * b;
-    Aa = Afe; pres = pfe; ut = pfe / mmax(d.fc90[es * kt_ + c], R(1e-12));
-  } else if (nEdge == 2) {
-    const R fc = mmin(d.fc90[c], d.fc90[kt_ + c]);
-    Aa = Fn / mmax(fc, R(1e-12)); pres = Fn > R(0) ? fc : R(0); ut = Fn > R(0) ? R(1) : R(0);
-  }
-  d.ctype[c] = uint8_t(nEdge);
+  const ClassOut<R> o = classCore(e0, e1, cf0, cf1, z0, z1, ph0, ph1, sinT, mabs(d.Fn[c]), d.fc90[c], d.fc90[kt_ + c],
+                                  d.E90[c], d.E90[kt_ + c], d.Hs[c], d.Hs[kt_ + c]);
+  d.phiS[2 * c] = ph0; d.phiS[2 * c + 1] = ph1;
+  d.ctype[c] = uint8_t(o.ctype);
   d.theta[c] = masin(sinT);
-  d.area[c] = Aa; d.pres[c] = pres; d.util[c] = ut;
+  d.area[c] = o.area; d.pres[c] = o.pres; d.util[c] = o.util;
 }
 
 // ------------------------------------------------------------------------------------------------ phase B / C
@@ -608,6 +822,7 @@ __device__ __forceinline__ void rankSideShort(const Dev<P> &d, int p, int kb) {
 // ------------------------------------------------------------------------------------------------ phase D
 struct StepCtx {
   int cur, nxt, obuf, onxt, pending, iter, warm;
+  int alPend, penN;  // augmented Lagrangian: the multiplier update is due before this iteration's evaluation
   double dispR;      // prescribed-motion fraction of this iteration
 };
 
@@ -819,6 +1034,13 @@ __device__ __forceinline__ void decide(const InstDesc &I, InstCtl &c, const Part
   c.obuf ^= 1;
   c.ke = ke; c.ke_prev = ke;
   c.iter += 1;
+  if (I.aug && I.contacts && I.K) {
+    // the penetration window of the multiplier: this iteration counts when it ran after the ramp; an update that was
+    // due before it (applied by its crossings) restarted the window; the next is due every al_every iterations after
+    // the ramp (solver_cpu.js:387,470,819-821)
+    c.penN = (c.alPend ? 0 : c.penN) + (c.iter - 1 >= I.ramp_iter ? 1 : 0);
+    c.alPend = (I.alEvery > 0 && c.iter > I.ramp_iter && (c.iter - I.ramp_iter) % I.alEvery == 0) ? 1 : 0;
+  }
   const double maxM = I.p ? double(p.x[RX_M]) / fmax(I.jLenMin, 1e-12) : 0.0;
   const double maxFn = (I.contacts && I.K) ? double(p.x[RX_FN]) : 0.0;
   const double fref = fmax(fmax(fmax(double(p.x[RX_LOAD]), double(p.x[RX_N])), fmax(maxM, maxFn)), 1e-12);
@@ -844,6 +1066,7 @@ __device__ __forceinline__ StepCtx makeCtx(const InstDesc &I, const InstCtl &c) 
   StepCtx sc;
   sc.cur = c.cur; sc.nxt = c.cur ^ 1; sc.obuf = c.obuf; sc.onxt = c.obuf ^ 1; sc.pending = c.pending; sc.iter = c.iter;
   sc.warm = (c.iter < I.warmup && I.contacts && I.K) ? 1 : 0;
+  sc.alPend = c.alPend; sc.penN = c.penN;
   const int start = max(c.disp_it0, (I.contacts && I.K) ? I.warmup : 0);
   sc.dispR = I.disp_ramp > 0 ? fmin(1.0, fmax(0.0, double(c.iter - start + 1) / I.disp_ramp)) : 1.0;
   return sc;

@@ -284,7 +284,8 @@ void HostGoals::contactInitialize(int sweeps) {
   nPrev = nrmv;
 }
 
-// node masses ms·Σk (rod: (EA + GA)/l0 per end node; contact: strength + stick on the nodes of each side's segment) and
+// node masses ms·Σk (rod: (EA + GA)/l0 per end node; contact: strength + stick on the nodes of each side's segment, and
+// with W2 the rotational spring k_t·0.38²·wA·wB/0.5 / l0² of each crossing) and
 // static frame stiffness per body axis (joints B/l̄, clamps B/l_c, shear lever κGA L²/l0): rod_cosserat.js:186-209,
 // solver_cpu.js:151-167, 694-705
 void HostGoals::buildMasses(double ramp, const std::vector<double> &Fn) {
@@ -300,6 +301,16 @@ void HostGoals::buildMasses(double ramp, const std::vector<double> &Fn) {
       for (int c = 0; c < K; c++) kNode[segI0[cxSegOff[2 * c + side] + sideSegLocal(2 * c + side)]] += k;
       for (int c = 0; c < K; c++) kNode[segI1[cxSegOff[2 * c + side] + sideSegLocal(2 * c + side)]] += k;
     }
+    // W2: the rotational spring of each crossing on the nodes of both sides' segments
+    if (prm.rot_friction)
+      for (int side = 0; side < 2; side++)
+        for (int pass = 0; pass < 2; pass++)
+          for (int c = 0; c < K; c++) {
+            const int seg = cxSegOff[2 * c + side] + sideSegLocal(2 * c + side);
+            const double kr = prm.stick_strength * (0.38 * 0.38) * wk[2 * size_t(c)] * wk[2 * size_t(c) + 1] / 0.5;
+            const double l = std::max(l0[seg], 1e-12);
+            kNode[pass ? segI1[seg] : segI0[seg]] += kr / (l * l);
+          }
   }
   const double ms = prm.mass_scale;
   mass.resize(n);
@@ -325,6 +336,7 @@ void HostGoals::buildMasses(double ramp, const std::vector<double> &Fn) {
 
 void HostGoals::build(const ws_model &md) {
   loadModel(md, false);
+  dentAfterDefault = md.params.warmup_iter + md.params.ramp_iter;
   buildTables(*this);
   buildAnchors(md);
   if (prm.contacts && K) contactInitialize();

@@ -35,6 +35,8 @@ struct HostGoals {
   std::vector<int> cxSegOff, cxNseg, cxStrand;       // [2K] first segment, segment count and strand of each side
   std::vector<double> wk, hk, w, h, mu;
   std::vector<double> fc90, E90, Hs;                 // [2K] timber across the grain, each side (W1 classification)
+  int dentAfterDefault = 1500;                       // first seat iteration when dent_after_iter < 0: warm-up + ramp of
+                                                     // the model the instance was built from (solver_cpu.js:686)
   std::vector<uint8_t> enabled, locked;
   // goals
   std::vector<double> mass, kRotStatic;              // [n], [3m]

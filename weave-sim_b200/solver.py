@@ -27,7 +27,7 @@ def device_count() -> int:
 
 
 STATE_FIELDS = ("X", "Q", "V", "W", "u", "nprev", "slip", "Fn", "Ft", "gap", "N", "Vsh", "M", "reactions", "stuck", "state",
-                "ctype", "theta", "phi", "area", "pressure", "util")
+                "ctype", "theta", "phi", "area", "pressure", "util", "lambda", "dent", "M_rot", "rot_slip")
 
 
 def _state_buffers(md, fields=None):
@@ -35,7 +35,8 @@ def _state_buffers(md, fields=None):
     n, m, p, K = md.n, md.m, md.p, md.K
     size = {"X": 3 * n, "Q": 4 * m, "V": 3 * n, "W": 3 * m, "u": 2 * K, "nprev": 3 * K, "slip": K, "Fn": K, "Ft": K,
             "gap": K, "N": m, "Vsh": 2 * m, "M": 3 * p, "reactions": 3 * n, "stuck": K, "state": K,
-            "ctype": K, "theta": K, "phi": 2 * K, "area": K, "pressure": K, "util": K}
+            "ctype": K, "theta": K, "phi": 2 * K, "area": K, "pressure": K, "util": K,
+            "lambda": K, "dent": K, "M_rot": K, "rot_slip": K}
     names = STATE_FIELDS if fields is None else tuple(fields)
     bad = [k for k in names if k not in size]
     if bad:
