@@ -60,6 +60,7 @@ def crossing(load=-50.0, pull=0.0, mu=0.35, freeB=True, nseg=10, L=1000.0, h=30.
                       loads=[((1, 1), (pull, 0.0, load), local)], mu=mu, E=E_MM, G=G_MM, params=mm_params(**prm))
     if locked:
         md.cross_locked[:] = 1
+    md.roll = roll
     return md
 
 

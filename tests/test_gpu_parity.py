@@ -393,9 +393,11 @@ def _ext_compare(g, v, md, ctl, tol=1e-9):
     assert ctl["iter"] == v["iteration"] and ctl["rollbacks"] == v["rollbacks"]
     assert cases.max_rel_disp_error(g["X"], v["X"], v["X0"]) < tol
     assert np.array_equal(g["stuck"], v["stuck"]) and np.array_equal(g["ctype"], v["ctype"])
-    for k in ("Fn", "lambda", "dent", "M_rot", "rot_slip", "slip", "gap"):
+    for k in ("Fn", "lambda", "dent", "rot_slip", "slip", "gap"):
         scale = max(np.abs(v[k]).max(), 1e-300)
         assert np.abs(g[k] - v[k]).max() <= tol * scale + 1e-12, (k, g[k], v[k])
+    # M = k_r (θ − θ0) with θ and θ0 both O(1) and their difference small: it keeps ~1e-16 of θ in absolute terms
+    assert np.abs(g["M_rot"] - v["M_rot"]).max() <= 1e-6 * max(np.abs(v["M_rot"]).max(), 1e-300) + 1e-12
     assert np.abs(g["u"] - v["u"]).max() < tol
 
 
@@ -409,19 +411,21 @@ def _ext_case(name):
         return cases.crossing(-50.0, 12.0, roll=(r, r), slip_rate=0.3, seat_law=1, rot_friction=1, dent_after_iter=0), 6000
     if name == "seat_edge_face":
         return cases.crossing(-50.0, 12.0, roll=(0.0, r), slip_rate=0.3, seat_law=1, rot_friction=1, dent_after_iter=0), 6000
+    if name == "rot_edge_face":
+        return cases.crossing(-50.0, 12.0, roll=(0.0, r), slip_rate=0.3, rot_friction=1), 6000
     if name == "rot_slip":
         return cases.crossing(-50.0, 12.0, rot_friction=1, rot_factor=0.001, slip_rate=1.0), 6000
     if name == "al_pinned":
-        return cases.crossing(-50.0, 0.0, augmented=1, al_every=600, strength=2000.0, tol=0.0, pin=True), 3000
+        return cases.crossing(-50.0, 0.0, augmented=1, al_every=600, strength=2000.0, pin=True), 8000
     raise KeyError(name)
 
 
-@pytest.mark.parametrize("name", ["cross_w23", "cross_al", "cross_al_long", "seat_edge_edge", "seat_edge_face", "rot_slip",
-                                  "al_pinned"])
+@pytest.mark.parametrize("name", ["cross_w23", "cross_al", "cross_al_long", "rot_edge_face", "rot_slip", "al_pinned"])
 @pytest.mark.parametrize("form", ["cta", "plain", "grid"])
 def test_contact_extensions_match_oracle(oracle_mod, name, form):
-    """the augmented-Lagrangian gap, W2 rotational friction and the W3 seat law (solver_cpu.js:283-379, 381-506,
-    819-821) in every execution form against the oracle: state, multipliers, seat depths, scissor moments"""
+    """the augmented-Lagrangian gap and W2 rotational friction (solver_cpu.js:347-379, 381-506, 819-821) in every
+    execution form against the oracle: state, multipliers, scissor moments (cross_w23 has the seat law on too, on a
+    crossing that bears face on face and so never seats)"""
     md, it = _ext_case(name)
     v = oracle_mod.Oracle(md.copy()).run(it)
     s = ws.GpuSolver([md.copy()], precision="f64", form=form)
@@ -429,6 +433,48 @@ def test_contact_extensions_match_oracle(oracle_mod, name, form):
     g = s.download(0, fields=EXT_FIELDS)
     s.dispose()
     _ext_compare(g, v, md, ctl)
+
+
+def _spread(oracle_mod, md, run, eps=(1e-14, 1e-12)):
+    """the oracle against itself started eps × the positions away: the chaos floor of a sensitive law"""
+    v = run(oracle_mod.Oracle(md.copy()))
+    out = []
+    for e in eps:
+        m2 = md.copy()
+        m2.X = m2.X * (1 + e)
+        out.append(run(oracle_mod.Oracle(m2)))
+    return v, out
+
+
+@pytest.mark.parametrize("name", ["seat_edge_edge", "seat_edge_face"])
+@pytest.mark.parametrize("form", ["cta", "plain", "grid"])
+def test_seat_law_matches_oracle(oracle_mod, name, form):
+    """W3 with W2 on crossings that bear on edges (solver_cpu.js:283-344).  The seat law makes a crossing's
+    trajectory sensitive: the oracle started 1e-14 of the positions away departs from itself by ~1e-3 within a few
+    thousand iterations.  So: agreement to 1e-9 over the first 100 iterations (the seats growing under the edges in
+    the warm-up) and, at the end, the device within ten times the oracle's own spread; seats cut by two edges hold
+    the crossing against a pull that slides it without them"""
+    md, it = _ext_case(name)
+    o = oracle_mod.Oracle(md.copy())
+    o.step(100)
+    v100 = o.view()
+    s = ws.GpuSolver([md.copy()], precision="f64", form=form)
+    ctl = s.step(100)[0]
+    g = s.download(0, fields=EXT_FIELDS)
+    _ext_compare(g, v100, md, ctl)
+    s.step(it - 100)
+    g = s.download(0, fields=EXT_FIELDS)
+    s.dispose()
+    v, others = _spread(oracle_mod, md, lambda orc: orc.run(it))
+    dX = max(cases.max_rel_disp_error(w["X"], v["X"], v["X0"]) for w in others)
+    assert cases.max_rel_disp_error(g["X"], v["X"], v["X0"]) <= 10 * dX + 1e-9
+    for k in ("Fn", "dent"):
+        fl = max(np.abs(w[k] - v[k]).max() for w in others)
+        assert np.abs(g[k] - v[k]).max() <= 10 * fl + 1e-9 * np.abs(v[k]).max(), k
+    assert np.array_equal(g["ctype"], v["ctype"]) and g["dent"][0] > 0
+    if name == "seat_edge_edge":        # edges cut seats whose walls hold the crossing against the pull
+        free = oracle_mod.Oracle(cases.crossing(-50.0, 12.0, roll=md.roll, slip_rate=0.3).copy()).run(it)
+        assert g["slip"][0] < 0.05 * free["slip"][0]
 
 
 def test_multiplier_update_due_at_a_download(oracle_mod):
@@ -473,22 +519,35 @@ def test_warm_start_restarts_the_multiplier_window(oracle_mod):
 
 @pytest.mark.parametrize("form,side_order", [("cta", "auto"), ("plain", "auto"), ("plain", "general"), ("grid", "auto")])
 def test_gridshell_with_extensions_matches_oracle(oracle_mod, form, side_order):
-    """the small dome with all three extensions on: 1500 iterations (warm-up, ramp, seats from 300) against the
-    oracle (the batched form keeps this instance in shared memory)"""
+    """the small dome with all three extensions on (warm-up, ramp to 1000, seats from 300, Uzawa every 200; the
+    batched form keeps this instance in shared memory): 400 iterations to 1e-9, then 1500 within ten times the
+    oracle's own spread (the seated dome is as sensitive as the crossings)"""
     md = ws.configs.dome_small()
     md.params.update(augmented=1, al_every=200, rot_friction=1, seat_law=1, dent_after_iter=300, ramp_iter=1000)
     o = oracle_mod.Oracle(md.copy())
-    o.step(1500)
+    o.step(400)
     v = o.view()
     s = ws.GpuSolver([md.copy()], precision="f64", form=form, side_order=side_order)
-    ctl = s.step(1500)[0]
+    s.step(400)
+    g = s.download(0, fields=EXT_FIELDS)
+    assert cases.max_node_err_span(g["X"], v["X"], md.span) < 1e-9
+    assert np.array_equal(g["ctype"], v["ctype"]) and np.array_equal(g["stuck"], v["stuck"])
+    for k in ("Fn", "dent", "rot_slip"):
+        assert np.abs(g[k] - v[k]).max() <= 1e-8 * max(np.abs(v[k]).max(), 1e-300), k
+    ctl = s.step(1100)[0]
     g = s.download(0, fields=EXT_FIELDS)
     s.dispose()
-    assert ctl["iter"] == 1500 and v["ctype"].max() == 2
-    assert cases.max_node_err_span(g["X"], v["X"], md.span) < 1e-9
-    assert np.array_equal(g["stuck"], v["stuck"]) and np.array_equal(g["ctype"], v["ctype"])
+
+    def run1500(orc):
+        orc.step(1500)
+        return orc.view()
+    v, others = _spread(oracle_mod, md, run1500)
+    assert ctl["iter"] == 1500 and v["ctype"].max() == 2 and v["lambda"].max() > 0
+    fX = max(cases.max_node_err_span(w["X"], v["X"], md.span) for w in others)
+    assert cases.max_node_err_span(g["X"], v["X"], md.span) <= 10 * fX + 1e-9
     for k in ("Fn", "lambda", "dent", "M_rot", "rot_slip"):
-        assert np.abs(g[k] - v[k]).max() <= 1e-8 * max(np.abs(v[k]).max(), 1e-300), k
+        fl = max(np.abs(w[k] - v[k]).max() for w in others)
+        assert np.abs(g[k] - v[k]).max() <= 10 * fl + 1e-9 * np.abs(v[k]).max(), k
 
 
 def test_extensions_mixed_precision_within_band(oracle_mod):
