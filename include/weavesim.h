@@ -29,6 +29,7 @@ extern "C" {
 #define WS_CONVERGED 1
 #define WS_MAX_ITER 2
 #define WS_NONFINITE 3
+#define WS_DONE 4        /* the load protocol (ws_protocol) recorded its last increment */
 
 /* precision of a solver context (one template instantiation of every kernel) */
 #define WS_PREC_F64 0        /* FP64 everywhere */
@@ -76,6 +77,25 @@ typedef struct ws_params {
   double dent_rate;       /* CONTACT.dent_rate 0.01: share of the estimated seat depth added per iteration */
 } ws_params;
 
+/* UTM replay protocol of one instance: the GpuSolver protocol (web/js/wgsl.js:1048-1093, set up by
+ * solver_gpu.js:256-318 and driven by calibrate.js:438-515).  Per load increment: settle (at most `settle`
+ * iterations, fewer once the residual meets the tolerance), then average the probe's travel along `axis` and the
+ * reaction along `axis` over `avg` iterations, record them, and apply the next value of the schedule: a force on the
+ * probe (mode 1) or the probe's position P0 + value·axis, the probe held there (mode 2; P0 = the probe's position when
+ * the instance was created or uploaded).  Convergence does not stop such an instance; it stops with WS_DONE after the
+ * last increment (or at max_iter, which must therefore cover n_inc × (settle + avg)). */
+#define WS_PROTOCOL_MAX_INC 64
+typedef struct ws_protocol {
+  int32_t mode;           /* 0 none, 1 force control, 2 displacement control */
+  int32_t probe;          /* probe node */
+  int32_t n_inc;          /* increments (1..WS_PROTOCOL_MAX_INC) */
+  int32_t settle;         /* settling iterations per increment */
+  int32_t avg;            /* iterations the read-out is averaged over */
+  int32_t pad0;
+  double axis[3];         /* probe axis (unit vector) */
+  double sched[WS_PROTOCOL_MAX_INC];   /* force [N] (mode 1) or travel [m] (mode 2) of each increment */
+} ws_protocol;
+
 /* The model of one instance: the flat state of buildState (web/js/model.js:10-75), the section stiffness per segment
  * (strandStiffness, model.js:236-252), the loads (Loads, model.js:191-231), the resolved anchors (anchorMasks /
  * Anchors, model.js:150-189) and the crossings (PolylineContact constructor, solver_cpu.js:62-96), before the goals
@@ -114,13 +134,14 @@ typedef struct ws_model {
                                         modulus, hardness (PolylineContact's matOf, solver_cpu.js:71-76); NULL: the
                                         reference's defaults 8, 800, 30 (N/mm²) */
   ws_params params;
+  const ws_protocol *protocol;     /* NULL: relax to convergence */
 } ws_model;
 
 /* per-instance control block, written by the device after every iteration (the CT struct of the WebGPU solver,
  * web/js/wgsl.js:154-172, read by GpuSolver.readControl, solver_gpu.js:374-386) */
 typedef struct ws_control {
   int32_t iter;        /* DR iterations done */
-  int32_t status;      /* WS_RUNNING / WS_CONVERGED / WS_MAX_ITER / WS_NONFINITE */
+  int32_t status;      /* WS_RUNNING / WS_CONVERGED / WS_MAX_ITER / WS_NONFINITE / WS_DONE */
   int32_t rollbacks;   /* kinetic-damping resets since creation */
   int32_t pending_zero;/* 1: the last iteration rolled back (velocities are zero, state is the previous one) */
   double ke;           /* kinetic energy of the last iteration (0 after a reset) */
@@ -128,6 +149,8 @@ typedef struct ws_control {
   double residual;     /* max(force part, torque part); +inf during the warm-up */
   double res_force, res_torque, fref;
   double e_stretch, e_shear, e_bend, e_twist, e_contact;
+  int32_t utm_inc;     /* load increments recorded (ws_protocol) */
+  int32_t utm_phase;   /* 0 settling, 1 averaging, 2 finished */
 } ws_control;
 
 /* ------------------------------------------------------------------------------------------------ errors */
@@ -264,6 +287,9 @@ typedef struct ws_state_out {
   double *dent;    /* [K] seat depth: the dents of both sides + the edge-on-face embedment */
   double *M_rot;   /* [K] W2 scissor moment about the contact normal */
   double *rot_slip;/* [K] accumulated W2 rotational slip [rad] */
+  /* load protocol read-out (GpuSolver.readOutputs, solver_gpu.js:407-416): per recorded increment the mean probe
+   * travel along the axis, the mean reaction along the axis, the applied value and the iteration */
+  double *utm;     /* [4 WS_PROTOCOL_MAX_INC] */
 } ws_state_out;
 int ws_download(ws_ctx *ctx, int32_t instance, ws_state_out *out);
 /* Uploads positions and frames (and zeroes velocities) of one instance from host buffers: a warm start from a state the

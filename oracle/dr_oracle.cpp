@@ -799,8 +799,71 @@ struct Solver {
     st.slip.assign(md.K, 0.0); st.stuck.assign(md.K, 1);
     st.iteration = 0; st.residual = INF;
     sp = md.params;
+    proto = ws_protocol{};
+    if (md.protocol && md.protocol->mode) proto = *md.protocol;
     buildGoals(md, false);
     setTargets(md);
+    startProtocol();
+  }
+
+  // ---------------------------------------------------------------------------------------------- load protocol
+  // The UTM replay of the reference's GPU form (web/js/wgsl.js:1048-1093, set up by solver_gpu.js:215,286,296-318),
+  // restated over this CPU iteration: the reference's CPU solver has no protocol of its own.
+  ws_protocol proto{};
+  double probe0[3] = {0, 0, 0}, utmPf[3] = {0, 0, 0}, utmCurF = 0, utmSum[4] = {0, 0, 0, 0};
+  int utmPhase = 0, utmIt = 0, utmInc = 0, utmAccN = 0;
+  bool utmDone = false;
+  std::vector<double> utmOut = std::vector<double>(4 * WS_PROTOCOL_MAX_INC, 0.0);
+
+  // P0 = the probe's position now; the first value applied (the probe placed there under displacement control)
+  void startProtocol() {
+    utmPhase = utmIt = utmInc = utmAccN = 0; utmDone = false;
+    for (double &v : utmSum) v = 0;
+    std::fill(utmOut.begin(), utmOut.end(), 0.0);
+    if (!proto.mode) return;
+    const size_t pb = 3 * size_t(proto.probe);
+    for (int k = 0; k < 3; k++) probe0[k] = st.X[pb + k];
+    utmCurF = proto.sched[0];
+    for (int k = 0; k < 3; k++) utmPf[k] = proto.mode == 1 ? proto.axis[k] * proto.sched[0] : 0.0;
+    if (proto.mode == 2)
+      for (int k = 0; k < 3; k++) { st.X[pb + k] = probe0[k] + proto.axis[k] * proto.sched[0]; st.V[pb + k] = 0; }
+  }
+  // after an iteration: settle, average the read-out, record, next increment (wgsl.js:1048-1093)
+  void protocolStep() {
+    if (!proto.mode || utmDone) return;
+    const bool conv = st.residual <= sp.tol;
+    const size_t pb = 3 * size_t(proto.probe);
+    utmIt += 1;
+    if (utmPhase == 0) {
+      if (conv || utmIt >= proto.settle) {
+        utmPhase = 1; utmIt = 0; utmAccN = 0;
+        for (double &v : utmSum) v = 0;
+      }
+    } else if (utmPhase == 1) {
+      double r = 0;
+      for (int k = 0; k < 3; k++) {
+        utmSum[k] += st.X[pb + k] - probe0[k];
+        r += reactions[pb + k] * proto.axis[k];
+      }
+      utmSum[3] += r;
+      utmAccN += 1;
+      if (utmIt >= proto.avg) {
+        double *o = &utmOut[4 * size_t(utmInc)];
+        const double nn = utmAccN;
+        o[0] = (utmSum[0] * proto.axis[0] + utmSum[1] * proto.axis[1] + utmSum[2] * proto.axis[2]) / nn;
+        o[1] = utmSum[3] / nn;
+        o[2] = utmCurF;
+        o[3] = st.iteration;
+        utmInc += 1; utmIt = 0; utmPhase = 0;
+        if (utmInc >= proto.n_inc) { utmPhase = 2; utmDone = true; }
+        else {
+          const double v = proto.sched[std::min(utmInc, WS_PROTOCOL_MAX_INC - 1)];
+          utmCurF = v;
+          if (proto.mode == 1) for (int k = 0; k < 3; k++) utmPf[k] = proto.axis[k] * v;
+          else for (int k = 0; k < 3; k++) { st.X[pb + k] = probe0[k] + proto.axis[k] * v; st.V[pb + k] = 0; }
+        }
+      }
+    }
   }
 
   // solver_cpu.js:670-710; rebuild = true keeps the contact and its state (rebuildGoals, :719-732)
@@ -821,6 +884,11 @@ struct Solver {
       for (int c = 0; c < 3; c++) if (mk & (1 << c)) nodeFree[3 * size_t(nid) + c] = 0;
       if ((mk & 7) && std::find(fixedNodes.begin(), fixedNodes.end(), nid) == fixedNodes.end()) fixedNodes.push_back(nid);
       for (int j : adj[nid]) if (mk & 0x38) rotClamps.push_back({nid, j, {bool(mk & 8), bool(mk & 16), bool(mk & 32)}});
+    }
+    if (proto.mode == 2) {                               // displacement control holds the probe (solver_gpu.js:215)
+      const int pn = proto.probe;
+      for (int c = 0; c < 3; c++) nodeFree[3 * size_t(pn) + c] = 0;
+      if (std::find(fixedNodes.begin(), fixedNodes.end(), pn) == fixedNodes.end()) fixedNodes.push_back(pn);
     }
     reactions.assign(3 * size_t(n), 0.0); fixedAny.assign(n, 0);
     for (int i = 0; i < n; i++) fixedAny[i] = (nodeFree[3 * size_t(i)] && nodeFree[3 * size_t(i) + 1] && nodeFree[3 * size_t(i) + 2]) ? 0 : 1;
@@ -891,6 +959,8 @@ struct Solver {
           for (int k = 0; k < 3; k++) total[3 * nid + k] += Rl[k] * Fv[0] + Rl[3 + k] * Fv[1] + Rl[6 + k] * Fv[2];
         }
       }
+      if (proto.mode == 1)                               // the protocol's probe force (wgsl.js:914)
+        for (int k = 0; k < 3; k++) total[3 * size_t(proto.probe) + k] += utmPf[k];
       for (size_t i = 0; i < 3 * size_t(n); i++) F[i] += total[i];
       if (hasContact) contact.apply(st, F.data(), T.data());
       std::fill(reactions.begin(), reactions.end(), 0.0);
@@ -962,8 +1032,14 @@ struct Solver {
       resF = n ? fmax / fref : 0; resT = m ? tmax / (fref * lRef) : 0;
       const double resid = std::max(resF, resT);
       st.residual = st.iteration > sp.warmup_iter ? resid : INF;
+      if (proto.mode) {                                  // a load protocol runs on past convergence
+        protocolStep();
+        if (utmDone) break;
+        continue;
+      }
       if (st.residual <= sp.tol) { converged = true; broke = true; break; }
     }
+    if (proto.mode) return utmDone;
     if (!broke) converged = st.residual <= sp.tol;
     return converged;
   }
@@ -991,6 +1067,8 @@ struct orc_view {
   int32_t *ctype;
   double *theta, *phi, *area, *pressure, *util;
   double *lambda, *dent, *M_rot, *rot_slip;     // contact extensions (buildResults, solver_cpu.js:906-908)
+  double *utm;                                  // load protocol read-out [4 WS_PROTOCOL_MAX_INC]
+  int32_t utm_inc, utm_phase, utm_done;
 };
 
 void *orc_create(const ws_model *md) {
@@ -1029,6 +1107,7 @@ void orc_view_get(void *h, orc_view *v) {
   }
   v->lambda = s->hasContact ? s->contact.lam.data() : nullptr; v->dent = s->hasContact ? s->contact.dentSum.data() : nullptr;
   v->M_rot = s->hasContact ? s->contact.Mrot.data() : nullptr; v->rot_slip = s->hasContact ? s->contact.rotSlip.data() : nullptr;
+  v->utm = s->utmOut.data(); v->utm_inc = s->utmInc; v->utm_phase = s->utmPhase; v->utm_done = s->utmDone ? 1 : 0;
   v->N = s->rod.N.data(); v->Vsh = s->rod.Vs.data(); v->M = s->rod.M.data(); v->reactions = s->reactions.data();
   v->mass = s->mass.data(); v->inertia3 = s->inertia3.data(); v->k_rot_static = s->kRotStatic.data();
   v->F = s->F.data(); v->T = s->T.data(); v->tm = s->tm.data();

@@ -25,7 +25,8 @@ class OrcView(C.Structure):
                [(k, _dp) for k in ("X", "X0", "V", "Q", "W", "u", "nprev", "slip", "Fn", "Ft", "gap", "state", "N",
                                    "Vsh", "M", "reactions", "mass", "inertia3", "k_rot_static", "F", "T", "tm")] + \
                [("stuck", C.POINTER(C.c_uint8)), ("ctype", C.POINTER(C.c_int32))] + \
-               [(k, _dp) for k in ("theta", "phi", "area", "pressure", "util", "lambda", "dent", "M_rot", "rot_slip")]
+               [(k, _dp) for k in ("theta", "phi", "area", "pressure", "util", "lambda", "dent", "M_rot", "rot_slip")] + \
+               [("utm", _dp), ("utm_inc", C.c_int32), ("utm_phase", C.c_int32), ("utm_done", C.c_int32)]
 
 
 _lib = None
@@ -121,6 +122,8 @@ class Oracle:
         out["stuck"] = np.array(st, dtype=np.uint8)
         hc = K and v.has_contact
         out["ctype"] = np.ctypeslib.as_array(v.ctype, shape=(K,)).astype(np.uint8) if hc else np.zeros(0, dtype=np.uint8)
+        out["utm"] = _arr(v.utm, 4 * 64).copy()
+        out["utm_inc"], out["utm_phase"], out["utm_done"] = v.utm_inc, v.utm_phase, v.utm_done
         for k, s_ in (("theta", K), ("phi", 2 * K), ("area", K), ("pressure", K), ("util", K), ("lambda", K), ("dent", K),
                       ("M_rot", K), ("rot_slip", K)):
             a = _arr(getattr(v, k), s_) if hc else np.zeros(0)

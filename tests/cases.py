@@ -96,3 +96,18 @@ def max_rel_disp_error(Xa, Xb, X0):
 def max_node_err_span(Xa, Xb, span):
     """max over nodes of |X_a − X_b|₂ / span"""
     return float(np.linalg.norm((Xa - Xb).reshape(-1, 3), axis=1).max() / span)
+
+
+def utm_beam(mode, sched, nseg=10, settle=10 ** 6, avg=10, tol=1e-8, max_iter=2_000_000):
+    """three-point bending under the load protocol: a 1000 mm lath pinned at one end and on a roller at the other
+    (twist held at both), the probe at mid-span along −z; force (mode 1) or travel (mode 2) per increment"""
+    md = straight(1000.0, nseg, anchors=[((0, 0), ws.mask(1, 1, 1, 0, 0, 1)), ((0, 1), ws.mask(0, 1, 1, 0, 0, 1))],
+                  params=mm_params(contacts=0, max_iter=max_iter, tol=tol))
+    md.protocol = dict(mode=mode, probe=nseg // 2, sched=list(sched), settle=settle, avg=avg, axis=(0.0, 0.0, -1.0))
+    return md
+
+
+def beam_midspan_stiffness(L=1000.0, w=60.0, h=30.0):
+    """Timoshenko: P / δ of a simply supported beam under a mid-span load (bending about the 60 mm face)"""
+    I = w * h ** 3 / 12
+    return 1.0 / (L ** 3 / (48 * E_MM * I) + L / (4 * KAPPA * G_MM * w * h))

@@ -560,3 +560,93 @@ def test_extensions_mixed_precision_within_band(oracle_mod):
     s.dispose()
     assert abs(g["Fn"][0] - v["Fn"][0]) < 1e-2 * abs(v["Fn"][0])
     assert abs(g["dent"][0] - v["dent"][0]) < 1e-2 * abs(v["dent"][0])
+
+
+# ---------------------------------------------------------------------------------------------- load protocol
+def _utm_compare(g, v, n_inc, tol=1e-9):
+    a, b = g["utm"].reshape(-1, 4)[:n_inc], v["utm"].reshape(-1, 4)[:n_inc]
+    assert np.array_equal(a[:, 3], b[:, 3]) and np.array_equal(a[:, 2], b[:, 2]), (a, b)
+    for c in (0, 1):
+        assert np.abs(a[:, c] - b[:, c]).max() <= tol * max(np.abs(b[:, c]).max(), 1e-300) + 1e-15, (a, b)
+
+
+@pytest.mark.parametrize("mode,sched", [(1, [10.0, 20.0, 30.0]), (2, [0.5, 1.0, 1.5])])
+@pytest.mark.parametrize("form", ["cta", "plain"])
+def test_protocol_beam_matches_oracle(oracle_mod, mode, sched, form):
+    """the load protocol (settle, average, record, next increment; wgsl.js:1048-1093) on three-point bending, force and
+    displacement control: the read-out, the iterations it was taken at and the final state against the oracle"""
+    md = cases.utm_beam(mode, sched, tol=1e-6)
+    v = oracle_mod.Oracle(md.copy()).run(2_000_000, chunk=5000)
+    s = ws.GpuSolver([md.copy()], precision="f64", form=form)
+    ctl = s.step(v["iteration"] + 10)[0]
+    g = s.download(0, fields=("X", "utm"))
+    s.dispose()
+    assert ctl["status"] == 4 and ctl["utm_inc"] == 3 and ctl["utm_phase"] == 2 and ctl["iter"] == v["iteration"]
+    _utm_compare(g, v, 3)
+    assert cases.max_rel_disp_error(g["X"], v["X"], v["X0"]) < 1e-9
+
+
+def test_protocol_on_a_crossing_matches_oracle(oracle_mod):
+    """force control on the upper lath of a crossing, at the crossing: contact and slide under the probe"""
+    md = cases.crossing(0.0, 0.0, tol=1e-6)
+    probe = int(np.argmin(np.linalg.norm(md.X.reshape(-1, 3) - [0.0, 0.0, 30.0], axis=1)))
+    md.protocol = dict(mode=1, probe=probe, sched=[10.0, 25.0, 40.0], settle=4000, avg=20, axis=(0.0, 0.0, -1.0))
+    v = oracle_mod.Oracle(md.copy()).run(20000)
+    for form in ("cta", "plain"):
+        s = ws.GpuSolver([md.copy()], precision="f64", form=form)
+        ctl = s.step(20000)[0]
+        g = s.download(0, fields=("X", "utm", "Fn"))
+        s.dispose()
+        assert ctl["status"] == 4 and ctl["iter"] == v["iteration"]
+        _utm_compare(g, v, 3)
+        assert abs(g["Fn"][0] - v["Fn"][0]) < 1e-9 * abs(v["Fn"][0]) and v["Fn"][0] > 10.0
+
+
+def test_protocol_population_of_domes(oracle_mod):
+    """a calibration population: six domes in one batched launch, each with its own probe at the apex and its own
+    schedule, force or displacement control (calibrate.js:485-495), against the oracle instance by instance"""
+    models = []
+    for seed in range(1, 7):
+        md = ws.configs.dome_small(seed=seed)
+        apex = int(np.argmax(md.X[2::3]))
+        if seed % 2:
+            md.protocol = dict(mode=2, probe=apex, sched=[0.001 * seed, 0.002 * seed, 0.003 * seed], settle=300, avg=20,
+                               axis=(0.0, 0.0, -1.0))
+        else:
+            md.protocol = dict(mode=1, probe=apex, sched=[0.5 * seed, 1.0 * seed, 1.5 * seed], settle=300, avg=20,
+                               axis=(0.0, 0.0, -1.0))
+        models.append(md)
+    s = ws.GpuSolver([m.copy() for m in models], precision="f64")
+    assert s.resident
+    ctl = s.step(5000)
+    for b, md in enumerate(models):
+        v = oracle_mod.Oracle(md.copy()).run(5000)
+        g = s.download(b, fields=("X", "utm"))
+        assert ctl[b]["status"] == 4 and ctl[b]["iter"] == v["iteration"] == 960
+        _utm_compare(g, v, 3, tol=1e-8)
+        assert cases.max_node_err_span(g["X"], v["X"], md.span) < 1e-9
+    s.dispose()
+
+
+def test_protocol_restarts_on_upload():
+    """an upload restarts the protocol from the uploaded probe (solver_gpu.js:286,296-311): uploading the starting
+    state again repeats the read-out"""
+    md = cases.utm_beam(2, [0.5, 1.0], tol=1e-6)
+    for form in ("cta", "plain"):
+        s = ws.GpuSolver([md.copy()], precision="f64", form=form)
+        c1 = s.step(100000)[0]
+        g1 = s.download(0, fields=("utm",))
+        s.upload_state(0, md.X, md.Q)
+        c2 = s.step(100000)[0]
+        g2 = s.download(0, fields=("utm",))
+        s.dispose()
+        assert c1["status"] == 4 and c2["status"] == 4 and c2["utm_inc"] == 2
+        a, b = g1["utm"].reshape(-1, 4)[:2], g2["utm"].reshape(-1, 4)[:2]
+        assert np.allclose(a[:, :3], b[:, :3], rtol=1e-12, atol=1e-15)
+        assert np.array_equal(b[:, 3] - a[:, 3], [c1["iter"]] * 2)
+
+
+def test_protocol_refused_by_the_grid_form():
+    md = cases.utm_beam(1, [10.0])
+    with pytest.raises(Exception):
+        ws.GpuSolver([md.copy()], precision="f64", form="grid")

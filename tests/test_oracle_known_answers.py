@@ -239,3 +239,33 @@ def test_seat_law_holds_a_crossing(oracle_mod):
     assert free["ctype"][0] == 2 and seated["ctype"][0] == 2
     assert free["dent"][0] == 0.0 and seated["dent"][0] > 0.0 and flat["dent"][0] == 0.0
     assert seated["slip"][0] < 0.05 * free["slip"][0]
+
+
+# ---------------------------------------------------------------------------------------------- load protocol
+# The UTM replay (web/js/wgsl.js:1048-1093) restated over the oracle's iteration, pinned by three-point bending: the
+# stiffness it reads out converges on Timoshenko's at second order in the segment length, as the rod's cantilevers do.
+
+@pytest.mark.parametrize("nseg,err", [(10, -1.93), (20, -0.49), (40, -0.12)])
+def test_protocol_reads_the_beam_stiffness(oracle_mod, nseg, err):
+    md = cases.utm_beam(1, [10.0, 20.0], nseg=nseg)
+    v = oracle_mod.Oracle(md.copy()).run(2_000_000, chunk=5000)
+    assert v["utm_done"] == 1 and v["utm_inc"] == 2 and not v["converged"]
+    out = v["utm"].reshape(-1, 4)
+    k = cases.beam_midspan_stiffness()
+    for i, F in enumerate((10.0, 20.0)):
+        assert out[i, 2] == F and out[i, 1] == 0.0          # a free probe carries no reaction
+        assert abs(100 * (F / out[i, 0] / k - 1) - err) < 0.02
+    assert out[0, 3] < out[1, 3] == v["iteration"]
+
+
+def test_protocol_displacement_control(oracle_mod):
+    """the probe held at P0 + travel: the reaction along the axis is the force of the same stiffness (0.5 mm to 0.04 %;
+    the roller end lets the beam stiffen slightly, as δ², at the larger travels)"""
+    md = cases.utm_beam(2, [0.5, 1.0, 1.5])
+    v = oracle_mod.Oracle(md.copy()).run(2_000_000, chunk=5000)
+    out = v["utm"].reshape(-1, 4)[:3]
+    assert v["utm_done"] == 1
+    assert np.allclose(out[:, 0], [0.5, 1.0, 1.5], rtol=0, atol=1e-12)
+    kf = 10.0 / oracle_mod.Oracle(cases.utm_beam(1, [10.0]).copy()).run(2_000_000, chunk=5000)["utm"][0]
+    ratio = out[:, 1] / out[:, 0] / kf
+    assert abs(ratio[0] - 1) < 1e-3 and np.all(np.abs(ratio - 1) < 5e-3) and np.all(np.diff(ratio) > 0)

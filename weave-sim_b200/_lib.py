@@ -38,6 +38,15 @@ class WsParams(C.Structure):
 PARAM_KEYS = [f[0] for f in WsParams._fields_ if not f[0].startswith("pad")]
 
 
+PROTOCOL_MAX_INC = 64
+
+
+class WsProtocol(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("probe", C.c_int32), ("n_inc", C.c_int32), ("settle", C.c_int32),
+                ("avg", C.c_int32), ("pad0", C.c_int32), ("axis", C.c_double * 3),
+                ("sched", C.c_double * PROTOCOL_MAX_INC)]
+
+
 class WsModel(C.Structure):
     _fields_ = [("n", C.c_int32), ("m", C.c_int32), ("p", C.c_int32), ("n_strands", C.c_int32), ("K", C.c_int32),
                 ("pad0", C.c_int32),
@@ -49,7 +58,8 @@ class WsModel(C.Structure):
                 ("anchor_target", _dp),
                 ("cross_strand", _ip), ("cross_wk", _dp), ("cross_hk", _dp), ("cross_u", _dp), ("cross_nprev", _dp),
                 ("cross_enabled", _bp), ("cross_locked", _bp), ("cross_mu", _dp),
-                ("cross_fc90", _dp), ("cross_E90", _dp), ("cross_H", _dp), ("params", WsParams)]
+                ("cross_fc90", _dp), ("cross_E90", _dp), ("cross_H", _dp), ("params", WsParams),
+                ("protocol", C.POINTER(WsProtocol))]
 
 
 class WsKagomeCfg(C.Structure):
@@ -73,7 +83,8 @@ class WsControl(C.Structure):
     _fields_ = [("iter", C.c_int32), ("status", C.c_int32), ("rollbacks", C.c_int32), ("pending_zero", C.c_int32),
                 ("ke", C.c_double), ("ke_prev", C.c_double), ("residual", C.c_double), ("res_force", C.c_double),
                 ("res_torque", C.c_double), ("fref", C.c_double), ("e_stretch", C.c_double), ("e_shear", C.c_double),
-                ("e_bend", C.c_double), ("e_twist", C.c_double), ("e_contact", C.c_double)]
+                ("e_bend", C.c_double), ("e_twist", C.c_double), ("e_contact", C.c_double),
+                ("utm_inc", C.c_int32), ("utm_phase", C.c_int32)]
 
     def as_dict(self):
         return {f[0]: getattr(self, f[0]) for f in self._fields_}
@@ -89,7 +100,7 @@ class WsStateOut(C.Structure):
                [("stuck", _bp), ("state", _bp)] + \
                [(k, _dp) for k in ("Fn", "Ft", "gap", "N", "Vsh", "M", "reactions")] + \
                [("ctype", _bp)] + [(k, _dp) for k in ("theta", "phi", "area", "pressure", "util")] + \
-               [(k, _dp) for k in ("lambda", "dent", "M_rot", "rot_slip")]
+               [(k, _dp) for k in ("lambda", "dent", "M_rot", "rot_slip", "utm")]
 
 
 _lib = None
@@ -190,6 +201,7 @@ class Model:
     def __init__(self):
         self.n = self.m = self.p = self.n_strands = self.K = 0
         self.params = default_params()
+        self.protocol = None       # dict(mode, probe, sched, settle, avg, axis): a load protocol (ws_protocol)
         self.node_offset = None
         self.span = 0.0
 
@@ -250,6 +262,19 @@ class Model:
         md.n_local_loads = len(self.local_load_node)
         md.n_anchors = len(self.anchor_node)
         md.params = params_struct(self.params)
+        if self.protocol:
+            pr = WsProtocol()
+            sched = list(self.protocol["sched"])
+            if not 1 <= len(sched) <= PROTOCOL_MAX_INC:
+                raise ValueError(f"a load protocol has 1..{PROTOCOL_MAX_INC} increments")
+            pr.mode, pr.probe, pr.n_inc = int(self.protocol["mode"]), int(self.protocol["probe"]), len(sched)
+            pr.settle, pr.avg = int(self.protocol["settle"]), int(self.protocol["avg"])
+            for k in range(3):
+                pr.axis[k] = float(self.protocol["axis"][k])
+            for k, v in enumerate(sched):
+                pr.sched[k] = float(v)
+            self._protocol_struct = pr          # kept alive with the model
+            md.protocol = C.pointer(pr)
         return md
 
     def goals(self) -> dict:

@@ -30,7 +30,7 @@ struct CudaError : std::runtime_error { using std::runtime_error::runtime_error;
   } while (0)
 
 // element counts of the whole batch
-struct Sizes { int n = 0, m = 0, p = 0, c = 0, k = 0, s = 0; };
+struct Sizes { int n = 0, m = 0, p = 0, c = 0, k = 0, s = 0, b = 0; };   // b: instances (as an offset: the index)
 
 // carves typed arrays out of one allocation (base == nullptr: only counts the bytes)
 struct Carver {
@@ -78,6 +78,8 @@ void layout(Dev<P> &d, Carver &cv, const Sizes &z) {
   d.fc90 = cv.take<R>(2 * k); d.E90 = cv.take<R>(2 * k); d.Hs = cv.take<R>(2 * k); d.sProj = cv.take<R>(4 * k); d.sinT = cv.take<R>(k);
   d.ctype = cv.take<uint8_t>(k); d.theta = cv.take<R>(k); d.area = cv.take<R>(k); d.pres = cv.take<R>(k);
   d.util = cv.take<R>(k); d.phiS = cv.take<R>(2 * k);
+  d.utmSched = cv.take<double>(WS_PROTOCOL_MAX_INC * size_t(std::max(z.b, 1)));
+  d.utmOut = cv.take<double>(4 * WS_PROTOCOL_MAX_INC * size_t(std::max(z.b, 1)));
   d.lam = cv.take<A>(k); d.penAcc = cv.take<A>(k); d.dent = cv.take<R>(2 * k); d.climb = cv.take<R>(2 * k);
   d.tanpsi = cv.take<R>(2 * k); d.dentE = cv.take<R>(k); d.theta0 = cv.take<R>(k); d.Mrot = cv.take<R>(k);
   d.rotSlip = cv.take<A>(k);
@@ -262,7 +264,21 @@ InstDesc describe(const HostGoals &g, const Sizes &off) {
   I.dentAfter = g.prm.dent_after_iter >= 0 ? g.prm.dent_after_iter : g.dentAfterDefault;
   I.rotFactor = g.prm.rot_factor; I.dentRate = g.prm.dent_rate;
   I.ext = (I.aug || I.rotFric || I.seat) ? 1 : 0;
+  I.utmMode = g.proto.mode; I.utmProbe = off.n + g.proto.probe; I.utmNInc = g.proto.n_inc; I.utmSettle = g.proto.settle;
+  I.utmAvg = g.proto.avg; I.utmIdx = off.b;
+  for (int k = 0; k < 3; k++) I.utmAxis[k] = g.proto.axis[k];
   return I;
+}
+
+// the load protocol's control fields at its start: settling, no increment recorded, the first value applied
+void protocolCtl(const HostGoals &g, InstCtl &s) {
+  s.utmPhase = 0; s.utmIt = 0; s.utmInc = 0; s.utmAccN = 0;
+  for (int k = 0; k < 4; k++) s.utmSum[k] = 0.0;
+  s.utmCurF = g.proto.mode ? g.proto.sched[0] : 0.0;
+  for (int k = 0; k < 3; k++) {
+    s.utmPf[k] = g.proto.mode == 1 ? g.proto.axis[k] * g.proto.sched[0] : 0.0;
+    s.utmP0[k] = g.probe0[k];
+  }
 }
 
 // upload the goal arrays of instance b (everything a warm start may change)
@@ -455,6 +471,7 @@ void uploadStatic(ws_ctx *c, int b) {
   put<int>(d.stSegOff + I.s0, sg.data(), S, st);
   std::vector<uint8_t> one(K, 1);
   put<uint8_t>(d.stuck + I.k0, one.data(), K, st);
+  put<double>(d.utmSched + size_t(I.utmIdx) * WS_PROTOCOL_MAX_INC, g.proto.sched, WS_PROTOCOL_MAX_INC, st);
 }
 
 // the contact-extension state of instance b at its start: no multiplier, no seats (wall slopes 1), no W2 reference angle
@@ -532,6 +549,7 @@ void fillControl(const InstCtl &s, ws_control *o) {
   o->iter = s.iter; o->status = s.status; o->rollbacks = s.rollbacks; o->pending_zero = s.pending;
   o->ke = s.ke; o->ke_prev = s.ke_prev; o->residual = s.residual; o->res_force = s.res_f; o->res_torque = s.res_t; o->fref = s.fref;
   o->e_stretch = s.e_stretch; o->e_shear = s.e_shear; o->e_bend = s.e_bend; o->e_twist = s.e_twist; o->e_contact = s.e_contact;
+  o->utm_inc = s.utmInc; o->utm_phase = s.utmPhase;
 }
 
 // some instance runs a contact extension: the kernels' variants with them
@@ -636,6 +654,7 @@ void downloadPacked(ws_ctx *c, int b, ws_state_out *o) {
   add(PF_AREA, I.K, 1, o->area, false); add(PF_PRES, I.K, 1, o->pressure, false); add(PF_UTIL, I.K, 1, o->util, false);
   add(PF_LAM, I.K, 1, o->lambda, false); add(PF_DENT, I.K, 1, o->dent, false); add(PF_MROT, I.K, 1, o->M_rot, false);
   add(PF_RSLIP, I.K, 1, o->rot_slip, false);
+  add(PF_UTM, WS_PROTOCOL_MAX_INC, 4, o->utm, false);
   if (!L.nf) return;
   if (o->lambda) flushAL<P>(c, b);
   if (wantsClass(o)) CK(launchClassify<P>(devOf<P>(c), c->dInst, b, I.K, c->st));
@@ -695,6 +714,7 @@ void downloadImpl(ws_ctx *c, int b, ws_state_out *o) {
   if (o->Vsh) f.planes(d.Vsh, d.mtot, I.m0, m, 2, o->Vsh);
   if (o->M && p) f.planes(d.Mj, d.ptot, I.p0, p, 3, o->M);
   if (o->reactions) f.planes(d.react, d.ntot, I.n0, n, 3, o->reactions);
+  if (o->utm) f.planes(d.utmOut, 0, size_t(I.utmIdx) * 4 * WS_PROTOCOL_MAX_INC, 4 * WS_PROTOCOL_MAX_INC, 1, o->utm);
   f.run(c);
 }
 
@@ -753,6 +773,7 @@ void setParamsImpl(ws_ctx *c, int b, const ws_model *md) {
   g = std::move(trial);
   Sizes off;
   off.n = c->inst[b].n0; off.m = c->inst[b].m0; off.p = c->inst[b].p0; off.c = c->inst[b].c0; off.k = c->inst[b].k0; off.s = c->inst[b].s0;
+  off.b = b;
   c->inst[b] = describe(g, off);
   CK(cudaMemcpyAsync(c->dInst + b, &c->inst[b], sizeof(InstDesc), cudaMemcpyHostToDevice, c->st));
   uploadGoals<P>(c, b);
@@ -778,9 +799,12 @@ void loadInstanceImpl(ws_ctx *c, int b, const ws_model *md) {
   const HostGoals &o = c->g[b];
   if (g.n != o.n || g.m != o.m || g.p != o.p || g.K != o.K || g.S != o.S || g.C != o.C)
     throw std::invalid_argument("the model's element counts differ from the slot's");
+  if (c->form == WS_FORM_GRID && g.proto.mode)
+    throw std::invalid_argument("a load protocol runs in the cta and plain forms, not the grid form");
   c->g[b] = std::move(g);
   Sizes off;
   off.n = c->inst[b].n0; off.m = c->inst[b].m0; off.p = c->inst[b].p0; off.c = c->inst[b].c0; off.k = c->inst[b].k0; off.s = c->inst[b].s0;
+  off.b = b;
   c->inst[b] = describe(c->g[b], off);
   CK(cudaMemcpyAsync(c->dInst + b, &c->inst[b], sizeof(InstDesc), cudaMemcpyHostToDevice, c->st));
   uploadStatic<P>(c, b);
@@ -793,6 +817,7 @@ void loadInstanceImpl(ws_ctx *c, int b, const ws_model *md) {
   InstCtl s;
   std::memset(&s, 0, sizeof(s));
   s.status = WS_RUNNING; s.residual = INFINITY;
+  protocolCtl(c->g[b], s);
   resetExt<P>(c, b);
   uploadState<P>(c, b, 0, true);
   // both buffers: a slice left over from the slot's previous model could point into another strand's sides
@@ -833,9 +858,11 @@ void uploadStateImpl(ws_ctx *c, int b, const double *X, const double *Q, const d
   g.X.assign(X, X + 3 * size_t(g.n));
   g.Q.assign(Q, Q + 4 * size_t(g.m));
   if (u && g.K) g.u.assign(u, u + 2 * size_t(g.K));
+  g.startProtocol();          // an upload restarts the load protocol from the uploaded probe (solver_gpu.js:286,296-311)
   uploadState<P>(c, b, s.cur, u != nullptr);
   if (u && g.K) { g.sortSides(); uploadOrder<P>(c, b, s.obuf); flushPuts(c); }
   s.pending = 0; s.ke_prev = 0.0; s.status = WS_RUNNING;
+  protocolCtl(g, s);
   CK(cudaMemcpyAsync(c->dCtl + b, &s, sizeof(InstCtl), cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
 }
@@ -942,10 +969,14 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     for (int b = 0; b < n_instances; b++) {
       if (!models[b]) throw std::invalid_argument("null model");
       c->g[b].build(*models[b]);
+      if (o.form == WS_FORM_GRID && c->g[b].proto.mode)
+        throw std::invalid_argument("a load protocol runs in the cta and plain forms, not the grid form");
+      off.b = b;
       c->inst.push_back(describe(c->g[b], off));
       off.n += c->g[b].n; off.m += c->g[b].m; off.p += c->g[b].p; off.c += c->g[b].C; off.k += c->g[b].K; off.s += c->g[b].S;
     }
     c->z = off;
+    c->z.b = n_instances;
     // longest instances first: the hardware block scheduler then balances the tail
     c->order.resize(n_instances);
     std::iota(c->order.begin(), c->order.end(), 0);
@@ -957,7 +988,12 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     CK(cudaMemcpyAsync(c->dInst, c->inst.data(), sizeof(InstDesc) * n_instances, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->dOrder, c->order.data(), sizeof(int) * n_instances, cudaMemcpyHostToDevice, c->st));
     std::vector<InstCtl> ctl(n_instances);
-    for (auto &s : ctl) { std::memset(&s, 0, sizeof(s)); s.status = WS_RUNNING; s.residual = INFINITY; }
+    for (int b = 0; b < n_instances; b++) {
+      InstCtl &s = ctl[b];
+      std::memset(&s, 0, sizeof(s));
+      s.status = WS_RUNNING; s.residual = INFINITY;
+      protocolCtl(c->g[b], s);
+    }
     CK(cudaMemcpyAsync(c->dCtl, ctl.data(), sizeof(InstCtl) * n_instances, cudaMemcpyHostToDevice, c->st));
     const InstDesc &I0 = c->inst[0];
     auto blocks = [](long long cnt, int thr) { return int(std::max<long long>(1, std::min<long long>((cnt + thr - 1) / thr, 148LL * 8))); };
@@ -1079,7 +1115,7 @@ namespace wsb {
 
 size_t instanceFootprint(int prec, const HostGoals &g) {
   Sizes z;
-  z.n = g.n; z.m = g.m; z.p = g.p; z.c = g.C; z.k = g.K; z.s = g.S;
+  z.n = g.n; z.m = g.m; z.p = g.p; z.c = g.C; z.k = g.K; z.s = g.S; z.b = 1;
   Carver cv{nullptr};
   switch (prec) {
     case WS_PREC_F64: { Dev<PREC_F64> d{}; layout<PREC_F64>(d, cv, z); break; }
@@ -1102,6 +1138,7 @@ static void runInPlaceImpl(ws_ctx *c, char *base, int nIter, int threads, ws_sta
   InstCtl s;
   std::memset(&s, 0, sizeof(s));
   s.status = WS_RUNNING; s.residual = INFINITY;
+  protocolCtl(c->g[0], s);
   CK(cudaMemcpyAsync(c->dCtl, &s, sizeof(InstCtl), cudaMemcpyHostToDevice, c->st));
   uploadAll<P>(c);
   if (nIter > 0)
@@ -1118,7 +1155,7 @@ int runInPlace(int prec, const HostGoals &g, char *base, int nIter, int threads,
   tmp.g.push_back(g);
   Sizes off;
   tmp.inst.push_back(describe(tmp.g[0], off));
-  tmp.z.n = g.n; tmp.z.m = g.m; tmp.z.p = g.p; tmp.z.c = g.C; tmp.z.k = g.K; tmp.z.s = g.S;
+  tmp.z.n = g.n; tmp.z.m = g.m; tmp.z.p = g.p; tmp.z.c = g.C; tmp.z.k = g.K; tmp.z.s = g.S; tmp.z.b = 1;
   tmp.shortSides = shortOrderOK(&tmp);
   try {
     switch (prec) {

@@ -34,6 +34,10 @@ struct InstDesc {
   // contact extensions: augmented Lagrangian, W2 rotational friction, W3 seat law (ext: any of them)
   int ext, aug, alEvery, rotFric, seat, seatGap, dentAfter;
   double rotFactor, dentRate;
+  // load protocol (ws_protocol): mode (0 none), probe node (global index), increments, settle / average lengths, the
+  // instance's slot in the schedule and read-out arrays, probe axis
+  int utmMode, utmProbe, utmNInc, utmSettle, utmAvg, utmIdx;
+  double utmAxis[3];
 };
 
 // per-instance control (device-written every iteration)
@@ -43,6 +47,10 @@ struct InstCtl {
   double ke, ke_prev, residual, res_f, res_t, fref;
   double e_stretch, e_shear, e_bend, e_twist, e_contact;
   int penN, alPend;    // augmented Lagrangian: iterations in the penetration window; the multiplier update is due
+  // load protocol: phase (0 settle, 1 average, 2 finished), iterations in the phase, increments recorded, samples
+  // averaged; probe force (mode 1), applied value, probe origin P0, sums of the probe travel (x, y, z) and reaction
+  int utmPhase, utmIt, utmInc, utmAccN;
+  double utmPf[3], utmCurF, utmP0[3], utmSum[4];
 };
 
 // reduction slots
@@ -108,7 +116,9 @@ struct Dev {
   A *lam, *penAcc;          // [ktot]
   R *dent, *climb, *tanpsi; // [2 ktot]
   R *dentE, *theta0, *Mrot; // [ktot]
-  A *rotSlip;               // [ktot]                  // [2 ktot]
+  A *rotSlip;               // [ktot]
+  // load protocol: schedule [instances][WS_PROTOCOL_MAX_INC], read-out [instances][WS_PROTOCOL_MAX_INC][4]
+  double *utmSched, *utmOut;                  // [2 ktot]
   // side records, indexed by side position p: the sides (sd = 2c + side) grouped by strand, ascending sd within a
   // strand (the strand's range is [stSideOff, stSideOff + stSideCnt))
   int *sPos;                // [2 ktot] position of side sd

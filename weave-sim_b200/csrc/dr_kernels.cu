@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
     const bool cx = I.contacts && I.K;
     for (int it = 0; it < nIter; it++) {
       if (sc.status != WS_RUNNING) break;
-      const StepCtx sx = makeCtx<A>(I, sc);
+      const StepCtx sx = makeCtx<A>(I, sc, sc.utmPf);
       Part<A> pt;
       pt.init();
       blockPhaseA<P, SHORT, EXT>(d, I, sx, pt);
@@ -185,6 +185,10 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
       blockReduce(pt, red);
       if (threadIdx.x == 0) decide(I, sc, pt, nIter);
       __syncthreads();
+      if (I.utmMode) {
+        if (threadIdx.x == 0) protocolStep<P>(d, sc.cur, I, sc);
+        __syncthreads();
+      }
     }
     if (threadIdx.x == 0) ctl[b] = sc;
     __syncthreads();
@@ -332,7 +336,7 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
     const bool cx = I.contacts && I.K;
     for (int it = 0; it < nIter; it++) {
       if (sc.status != WS_RUNNING) break;
-      StepCtx sx = makeCtx<A>(I, sc);
+      StepCtx sx = makeCtx<A>(I, sc, sc.utmPf);
       sx.cur = sx.nxt = 0;              // in place
       Part<A> pt;
       pt.init();
@@ -373,6 +377,10 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
           if (e < I.n) backupNode<P>(d, v, bk, I.n0 + e, true);
           else backupSeg<P>(d, v, bk, I.m0 + (e - I.n), true);
         }
+        __syncthreads();
+      }
+      if (I.utmMode) {
+        if (threadIdx.x == 0) protocolStep<P>(v, 0, I, sc);
         __syncthreads();
       }
     }
@@ -451,7 +459,7 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
   const InstDesc &I = insts[0];
   const InstCtl c = ctl[0];
   if (c.status != WS_RUNNING) return;
-  const StepCtx sx = makeCtx<A>(I, c);
+  const StepCtx sx = makeCtx<A>(I, c, ctl[0].utmPf);
   Part<A> pt;
   pt.init();
   const int nR = countD<SHORT>(I) - I.n - I.m;
@@ -480,6 +488,7 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
   if (threadIdx.x == 0) {
     InstCtl cc = c;
     decide(I, cc, q, 0);
+    protocolStep<P>(d, cc.cur, I, cc);
     ctl[0] = cc;
     *counter = 0;
   }
@@ -586,9 +595,13 @@ __global__ void __launch_bounds__(256) k_unpack(Dev<P> d, const InstDesc *__rest
   const int cur = ctl[b].cur;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
   const int nX = 3 * I.n, nQ = 4 * I.m, nU = withU ? 2 * I.K : 0;
+  // an upload restarts the load protocol from the uploaded probe: P0 = its position, placed at the first value under
+  // displacement control (solver_gpu.js:286,296-311)
+  const double v0 = I.utmMode ? d.utmSched[size_t(I.utmIdx) * WS_PROTOCOL_MAX_INC] : 0.0;
   for (int e = gt; e < nX; e += gs) {
     const int i = I.n0 + e / 3, k = e % 3;
-    Acc<P>::xs(d, cur, k, i, W(in[e]));
+    const double x = (I.utmMode == 2 && i == I.utmProbe) ? in[e] + I.utmAxis[k] * v0 : in[e];
+    Acc<P>::xs(d, cur, k, i, W(x));
     d.V[size_t(k) * d.nS + i] = R(0);
   }
   for (int e = gt; e < nQ; e += gs) {
@@ -598,9 +611,18 @@ __global__ void __launch_bounds__(256) k_unpack(Dev<P> d, const InstDesc *__rest
   }
   for (int e = gt; e < nU; e += gs) d.u[size_t(e % 2) * d.kS + I.k0 + e / 2] = U(in[nX + nQ + e]);
   if (gt == 0) {
-    ctl[b].pending = 0;
-    ctl[b].ke_prev = 0.0;
-    ctl[b].status = WS_RUNNING;
+    InstCtl &c = ctl[b];
+    c.pending = 0;
+    c.ke_prev = 0.0;
+    c.status = WS_RUNNING;
+    if (I.utmMode) {
+      c.utmPhase = 0; c.utmIt = 0; c.utmInc = 0; c.utmAccN = 0; c.utmCurF = v0;
+      for (int k = 0; k < 4; k++) c.utmSum[k] = 0.0;
+      for (int k = 0; k < 3; k++) {
+        c.utmP0[k] = in[3 * (I.utmProbe - I.n0) + k];
+        c.utmPf[k] = I.utmMode == 1 ? I.utmAxis[k] * v0 : 0.0;
+      }
+    }
   }
 }
 // the segment each side sits on now (solver_cpu.js:144-149), from the slide coordinates, into key buffer obuf
@@ -695,7 +717,8 @@ __global__ void __launch_bounds__(256) k_pack(Dev<P> d, const InstDesc *__restri
         case PF_LAM: od[e] = double(d.lam[I.k0 + i]); break;
         case PF_DENT: od[e] = double(d.dent[2 * (I.k0 + i)]) + double(d.dent[2 * (I.k0 + i) + 1]) + double(d.dentE[I.k0 + i]); break;
         case PF_MROT: od[e] = double(d.Mrot[I.k0 + i]); break;
-        default: od[e] = double(d.rotSlip[I.k0 + i]); break;
+        case PF_RSLIP: od[e] = double(d.rotSlip[I.k0 + i]); break;
+        default: od[e] = d.utmOut[size_t(I.utmIdx) * 4 * WS_PROTOCOL_MAX_INC + e]; break;
       }
     }
   }

@@ -33,7 +33,7 @@ template <int P>
 cudaError_t residentPrepare(size_t bytes, bool shortSides, size_t *granted);
 // host <-> device transfers of one instance's state (interleaved per element, as the C ABI's arrays are)
 enum { PF_X, PF_Q, PF_V, PF_W, PF_U, PF_NPREV, PF_SLIP, PF_FN, PF_FT, PF_GAP, PF_N, PF_VSH, PF_M, PF_REACT, PF_STUCK, PF_STATE,
-       PF_CTYPE, PF_THETA, PF_PHI, PF_AREA, PF_PRES, PF_UTIL, PF_LAM, PF_DENT, PF_MROT, PF_RSLIP };
+       PF_CTYPE, PF_THETA, PF_PHI, PF_AREA, PF_PRES, PF_UTIL, PF_LAM, PF_DENT, PF_MROT, PF_RSLIP, PF_UTM };
 struct PackField { int kind, count, ncomp; long long off; };   // off: byte offset in the packed buffer
 struct PackList { PackField f[28]; int nf; };
 // the multiplier update of instance b that fell due at the end of its last iteration, applied now

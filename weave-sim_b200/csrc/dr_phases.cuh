@@ -823,6 +823,7 @@ __device__ __forceinline__ void rankSideShort(const Dev<P> &d, int p, int kb) {
 struct StepCtx {
   int cur, nxt, obuf, onxt, pending, iter, warm;
   int alPend, penN;  // augmented Lagrangian: the multiplier update is due before this iteration's evaluation
+  const double *utmPf;  // load protocol: the force on the probe (mode 1)
   double dispR;      // prescribed-motion fraction of this iteration
 };
 
@@ -866,6 +867,8 @@ __device__ __forceinline__ void nodeUpdate(const Dev<P> &d, const InstDesc &I, c
     const R f0 = ro(d.ll + i), f1 = ro(d.ll + nt + i), f2 = ro(d.ll + 2 * nt + i);
     for (int k = 0; k < 3; k++) tot[k] += Rn[k] * f0 + Rn[3 + k] * f1 + Rn[6 + k] * f2;
   }
+  if (I.utmMode == 1 && i == I.utmProbe)   // the load protocol's force on its probe (wgsl.js:914)
+    for (int k = 0; k < 3; k++) tot[k] += R(sc.utmPf[k]);
   for (int k = 0; k < 3; k++) F[k] += tot[k];
   pt.x[RX_LOAD] = mmax(pt.x[RX_LOAD], A(mmax(mabs(tot[0]), mmax(mabs(tot[1]), mabs(tot[2])))));
   // crossing sides on the adjacent segments, as distributed by the last evaluation (weights 1 − t at a, t at b)
@@ -1054,16 +1057,70 @@ __device__ __forceinline__ void decide(const InstDesc &I, InstCtl &c, const Part
   // contact energy of the iteration: ½ Σ k_n pen² + ½ k_t Σ |S_e|² with the ramp of that iteration
   const double rampd = I.ramp_iter <= 0 ? 1.0 : fmin(1.0, 0.01 + 0.99 * double(c.iter - 1) / I.ramp_iter);
   c.e_contact = 0.5 * double(p.s[RS_PEN]) + 0.5 * rampd * I.stick * double(p.s[RS_TAN]);
-  if (c.status == WS_RUNNING) {
+  if (c.status == WS_RUNNING && !I.utmMode) {        // a load protocol runs on past convergence (protocolStep)
     if (c.residual <= I.tol) c.status = WS_CONVERGED;
     else if (c.iter >= I.max_iter) c.status = WS_MAX_ITER;
   }
   (void)n_iter_stop;
 }
 
+// The load protocol of one instance after its iteration (the UTM replay of web/js/wgsl.js:1048-1093): settle until
+// convergence or `settle` iterations, average the probe's travel from P0 and its reaction along the axis over `avg`
+// iterations, record them, then apply the next value of the schedule: the probe force (mode 1) or the probe's
+// position P0 + value·axis, at rest (mode 2).  d is the view whose buffer `buf` holds the positions the instance
+// continues from (after a roll-back, the restored ones).  One thread.
+template <int P>
+__device__ __forceinline__ void protocolStep(const Dev<P> &d, int buf, const InstDesc &I, InstCtl &c) {
+  using W = typename Dev<P>::W;
+  if (!I.utmMode || c.status != WS_RUNNING) return;
+  const bool conv = c.residual <= I.tol;
+  const int pi = I.utmProbe;
+  c.utmIt += 1;
+  if (c.utmPhase == 0) {
+    if (conv || c.utmIt >= I.utmSettle) {
+      c.utmPhase = 1; c.utmIt = 0; c.utmAccN = 0;
+      for (int k = 0; k < 4; k++) c.utmSum[k] = 0.0;
+    }
+  } else if (c.utmPhase == 1) {
+    double r = 0.0;
+    for (int k = 0; k < 3; k++) {
+      c.utmSum[k] += double(Acc<P>::xw(d, buf, k, pi)) - c.utmP0[k];
+      r += double(d.react[size_t(k) * d.ntot + pi]) * I.utmAxis[k];
+    }
+    c.utmSum[3] += r;
+    c.utmAccN += 1;
+    if (c.utmIt >= I.utmAvg) {
+      double *o = d.utmOut + (size_t(I.utmIdx) * WS_PROTOCOL_MAX_INC + c.utmInc) * 4;
+      const double n = double(c.utmAccN);
+      o[0] = (c.utmSum[0] * I.utmAxis[0] + c.utmSum[1] * I.utmAxis[1] + c.utmSum[2] * I.utmAxis[2]) / n;
+      o[1] = c.utmSum[3] / n;
+      o[2] = c.utmCurF;
+      o[3] = double(c.iter);
+      c.utmInc += 1; c.utmIt = 0; c.utmPhase = 0;
+      if (c.utmInc >= I.utmNInc) {
+        c.utmPhase = 2;
+        c.status = WS_DONE;
+      } else {
+        const double v = d.utmSched[size_t(I.utmIdx) * WS_PROTOCOL_MAX_INC + min(c.utmInc, WS_PROTOCOL_MAX_INC - 1)];
+        c.utmCurF = v;
+        if (I.utmMode == 1) {
+          for (int k = 0; k < 3; k++) c.utmPf[k] = I.utmAxis[k] * v;
+        } else {
+          for (int k = 0; k < 3; k++) {
+            Acc<P>::xs(d, buf, k, pi, W(c.utmP0[k] + I.utmAxis[k] * v));
+            d.V[size_t(k) * d.nS + pi] = 0;
+          }
+        }
+      }
+    }
+  }
+  if (c.status == WS_RUNNING && c.iter >= I.max_iter) c.status = WS_MAX_ITER;
+}
+
 template <class A>
-__device__ __forceinline__ StepCtx makeCtx(const InstDesc &I, const InstCtl &c) {
+__device__ __forceinline__ StepCtx makeCtx(const InstDesc &I, const InstCtl &c, const double *utmPf = nullptr) {
   StepCtx sc;
+  sc.utmPf = utmPf;
   sc.cur = c.cur; sc.nxt = c.cur ^ 1; sc.obuf = c.obuf; sc.onxt = c.obuf ^ 1; sc.pending = c.pending; sc.iter = c.iter;
   sc.warm = (c.iter < I.warmup && I.contacts && I.K) ? 1 : 0;
   sc.alPend = c.alPend; sc.penN = c.penN;

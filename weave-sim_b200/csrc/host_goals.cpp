@@ -46,6 +46,15 @@ void HostGoals::loadModel(const ws_model &md, bool keepState) {
     if (segOffset[0] != 0 || segOffset[S] != m) throw std::invalid_argument("model: seg_offset must run from 0 to m");
     for (int s = 0; s < S; s++) if (segOffset[s + 1] < segOffset[s]) throw std::invalid_argument("model: seg_offset must not decrease");
     for (int i = 0; i < 2 * K; i++) if (md.cross_strand[i] < 0 || md.cross_strand[i] >= S) throw std::invalid_argument("model: crossing strand out of range");
+    proto = ws_protocol{};
+    if (md.protocol && md.protocol->mode) {
+      const ws_protocol &pr = *md.protocol;
+      if (pr.mode < 0 || pr.mode > 2) throw std::invalid_argument("model: protocol mode must be 0, 1 or 2");
+      if (pr.probe < 0 || pr.probe >= n) throw std::invalid_argument("model: protocol probe node out of range");
+      if (pr.n_inc < 1 || pr.n_inc > WS_PROTOCOL_MAX_INC) throw std::invalid_argument("model: protocol needs 1..64 increments");
+      if (pr.settle < 0 || pr.avg < 1) throw std::invalid_argument("model: protocol settle must be >= 0 and avg >= 1");
+      proto = pr;
+    }
   }
   omega0 = md.omega0 ? copyOf(md.omega0, 3 * size_t(p)) : std::vector<double>(3 * size_t(p), 0.0);
   EA = copyOf(md.EA, m); GA = copyOf(md.GA, m);
@@ -115,6 +124,8 @@ void HostGoals::buildAnchors(const ws_model &md) {
       }
   }
   C = int(cSeg.size());
+  if (proto.mode == 2)   // displacement control holds the probe (solver_gpu.js:215)
+    for (int c = 0; c < 3; c++) nodeFree[3 * size_t(proto.probe) + c] = 0;
   fixedAny.assign(n, 0);
   for (int i = 0; i < n; i++) fixedAny[i] = (nodeFree[3 * size_t(i)] && nodeFree[3 * size_t(i) + 1] && nodeFree[3 * size_t(i) + 2]) ? 0 : 1;
   segClamp0.assign(m, -1); segClamp1.assign(m, -1);
@@ -334,6 +345,14 @@ void HostGoals::buildMasses(double ramp, const std::vector<double> &Fn) {
   lRef = lmin < 1e300 ? lmin : 1.0;
 }
 
+// the load protocol starts: P0 is the probe's position now; displacement control places the probe at the first value
+void HostGoals::startProtocol() {
+  if (!proto.mode) return;
+  for (int c = 0; c < 3; c++) probe0[c] = X[3 * size_t(proto.probe) + c];
+  if (proto.mode == 2)
+    for (int c = 0; c < 3; c++) X[3 * size_t(proto.probe) + c] = probe0[c] + proto.axis[c] * proto.sched[0];
+}
+
 void HostGoals::build(const ws_model &md) {
   loadModel(md, false);
   dentAfterDefault = md.params.warmup_iter + md.params.ramp_iter;
@@ -343,6 +362,7 @@ void HostGoals::build(const ws_model &md) {
   buildMasses(1.0, std::vector<double>(K, 0.0));
   buildTargets(md);
   sortSides();
+  startProtocol();          // after the goals: they are the model's, as GpuSolver uploads it (solver_gpu.js:286,311)
 }
 
 // warm start (rebuildGoals): the caller has put the current X, Q, u, nPrev into this object first

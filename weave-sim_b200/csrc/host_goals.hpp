@@ -35,6 +35,8 @@ struct HostGoals {
   std::vector<int> cxSegOff, cxNseg, cxStrand;       // [2K] first segment, segment count and strand of each side
   std::vector<double> wk, hk, w, h, mu;
   std::vector<double> fc90, E90, Hs;                 // [2K] timber across the grain, each side (W1 classification)
+  ws_protocol proto{};                               // load protocol (mode 0: none), kept over warm starts
+  double probe0[3] = {0, 0, 0};                      // the probe's position when the protocol started (P0)
   int dentAfterDefault = 1500;                       // first seat iteration when dent_after_iter < 0: warm-up + ramp of
                                                      // the model the instance was built from (solver_cpu.js:686)
   std::vector<uint8_t> enabled, locked;
@@ -54,6 +56,7 @@ struct HostGoals {
   void build(const ws_model &md);                    // everything, including the contact initialisation
   void rebuild(const ws_model &md);                  // warm start: new stiffness / loads / parameters, state kept
   void sortSides();                                  // ord / ordSeg / rngLo / rngHi from u
+  void startProtocol();                              // P0 from the probe's position, the probe placed at the first value
   int sideSegLocal(int sd) const;                    // local segment of side sd from u (solver_cpu.js:144-149)
   double sideSegMin() const;                         // shortest rest length among the segments of strands with sides
 

@@ -17,7 +17,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import WsControl, WsOpts, WsStateOut, check, lib
+from ._lib import PROTOCOL_MAX_INC, WsControl, WsOpts, WsStateOut, check, lib
 
 STATUS = {0: "running", 1: "converged", 2: "max_iter", 3: "non_finite"}
 
@@ -27,7 +27,7 @@ def device_count() -> int:
 
 
 STATE_FIELDS = ("X", "Q", "V", "W", "u", "nprev", "slip", "Fn", "Ft", "gap", "N", "Vsh", "M", "reactions", "stuck", "state",
-                "ctype", "theta", "phi", "area", "pressure", "util", "lambda", "dent", "M_rot", "rot_slip")
+                "ctype", "theta", "phi", "area", "pressure", "util", "lambda", "dent", "M_rot", "rot_slip", "utm")
 
 
 def _state_buffers(md, fields=None):
@@ -36,7 +36,7 @@ def _state_buffers(md, fields=None):
     size = {"X": 3 * n, "Q": 4 * m, "V": 3 * n, "W": 3 * m, "u": 2 * K, "nprev": 3 * K, "slip": K, "Fn": K, "Ft": K,
             "gap": K, "N": m, "Vsh": 2 * m, "M": 3 * p, "reactions": 3 * n, "stuck": K, "state": K,
             "ctype": K, "theta": K, "phi": 2 * K, "area": K, "pressure": K, "util": K,
-            "lambda": K, "dent": K, "M_rot": K, "rot_slip": K}
+            "lambda": K, "dent": K, "M_rot": K, "rot_slip": K, "utm": 4 * PROTOCOL_MAX_INC}
     names = STATE_FIELDS if fields is None else tuple(fields)
     bad = [k for k in names if k not in size]
     if bad:
