@@ -617,7 +617,6 @@ def test_protocol_population_of_domes(oracle_mod):
                                axis=(0.0, 0.0, -1.0))
         models.append(md)
     s = ws.GpuSolver([m.copy() for m in models], precision="f64")
-    assert s.resident
     ctl = s.step(5000)
     for b, md in enumerate(models):
         v = oracle_mod.Oracle(md.copy()).run(5000)
