@@ -75,6 +75,13 @@ typedef struct ws_params {
                              the model the instance was created from (solver_cpu.js:329,686) */
   double rot_factor;      /* CONTACT.rot_factor 1.0: W2 moment limit rot_factor·μ·|Fn|·r_eq */
   double dent_rate;       /* CONTACT.dent_rate 0.01: share of the estimated seat depth added per iteration */
+  /* the ground (scene.floor, Floor in solver_cpu.js:509-634): a plane at height floor_z that the sections cannot pass,
+   * penalty k_n = strength, stick spring k_t = stick_strength (with the contact ramp), Coulomb coefficient floor_mu */
+  int32_t floor;          /* 0 none, 1 on; a model with a ground must also have an anchor (the rigid-body freedoms of a
+                             model that only the ground holds are not built) */
+  int32_t pad1;
+  double floor_z;         /* height of the plane */
+  double floor_mu;        /* friction coefficient on the ground */
 } ws_params;
 
 /* UTM replay protocol of one instance: the GpuSolver protocol (web/js/wgsl.js:1048-1093, set up by
@@ -135,6 +142,8 @@ typedef struct ws_model {
                                         reference's defaults 8, 800, 30 (N/mm²) */
   ws_params params;
   const ws_protocol *protocol;     /* NULL: relax to convergence */
+  const double *node_w, *node_h;   /* [n] section width / height at every node (its lath group), for the ground's
+                                      clearance; needed when params.floor is on */
 } ws_model;
 
 /* per-instance control block, written by the device after every iteration (the CT struct of the WebGPU solver,
@@ -151,6 +160,7 @@ typedef struct ws_control {
   double e_stretch, e_shear, e_bend, e_twist, e_contact;
   int32_t utm_inc;     /* load increments recorded (ws_protocol) */
   int32_t utm_phase;   /* 0 settling, 1 averaging, 2 finished */
+  double e_floor;      /* the ground's spring energy (Floor.energy) */
 } ws_control;
 
 /* ------------------------------------------------------------------------------------------------ errors */
@@ -290,6 +300,9 @@ typedef struct ws_state_out {
   /* load protocol read-out (GpuSolver.readOutputs, solver_gpu.js:407-416): per recorded increment the mean probe
    * travel along the axis, the mean reaction along the axis, the applied value and the iteration */
   double *utm;     /* [4 WS_PROTOCOL_MAX_INC] */
+  /* the ground (Floor.F / Floor.state, solver_cpu.js:541-546) */
+  double *floor_F; /* [3n] the ground's force on every node */
+  uint8_t *floor_state; /* [n] 0 clear of the ground, 1 stuck, 2 sliding */
 } ws_state_out;
 int ws_download(ws_ctx *ctx, int32_t instance, ws_state_out *out);
 /* Uploads positions and frames (and zeroes velocities) of one instance from host buffers: a warm start from a state the

@@ -20,6 +20,7 @@
 #include <cstdint>
 #include <cstring>
 #include <limits>
+#include <stdexcept>
 #include <vector>
 
 #include "../include/weavesim.h"
@@ -806,6 +807,60 @@ struct Solver {
     startProtocol();
   }
 
+  // ---------------------------------------------------------------------------------------------- the ground
+  // Floor (solver_cpu.js:509-634) for models that an anchor also holds; its rigid-body freedoms (a model that only the
+  // ground holds) are not restated
+  bool hasFloor = false;
+  double floorFnMax = 0, floorEnergy = 0;
+  std::vector<double> flW, flH, flAx, flAy, flF;
+  std::vector<uint8_t> flState;
+  // the Floor constructor / bind (solver_cpu.js:531-556): sections from the model; stick points at the nodes when new
+  void floorBind(const ws_model &md) {
+    const int n = st.n;
+    if (!md.params.floor) { hasFloor = false; return; }
+    if (!md.node_w || !md.node_h) throw std::invalid_argument("oracle: a ground needs the node sections");
+    if (fixedNodes.empty() && rotClamps.empty()) throw std::invalid_argument("oracle: a model that only the ground holds");
+    flW.assign(md.node_w, md.node_w + n); flH.assign(md.node_h, md.node_h + n);
+    if (!hasFloor || flAx.size() != size_t(n)) {
+      flAx.resize(n); flAy.resize(n);
+      for (int i = 0; i < n; i++) { flAx[i] = st.X[3 * size_t(i)]; flAy[i] = st.X[3 * size_t(i) + 1]; }
+      flF.assign(3 * size_t(n), 0.0); flState.assign(n, 0); floorFnMax = floorEnergy = 0;
+    }
+    hasFloor = true;
+  }
+  // Floor.apply without the rigid-body sums (solver_cpu.js:572-620)
+  void floorApply(double ramp) {
+    const int n = st.n;
+    const double z0 = sp.floor_z, mu = std::max(sp.floor_mu, 0.0), kn = ramp * sp.strength, kt = ramp * sp.stick_strength;
+    std::vector<double> qn;
+    nodeQuats(st, qn);
+    double e = 0, fmax = 0, R[9];
+    for (int i = 0; i < n; i++) {
+      toFrame(&qn[4 * size_t(i)], R);
+      const double *x = &st.X[3 * size_t(i)];
+      const double pen = (z0 - x[2]) + (0.5 * flW[i] * std::fabs(R[2]) + 0.5 * flH[i] * std::fabs(R[5]));
+      double *f = &flF[3 * size_t(i)];
+      if (pen > 0) {
+        const double fn = kn * pen;
+        const double sx = x[0] - flAx[i], sy = x[1] - flAy[i];
+        const double Ftv = kt * std::sqrt(sx * sx + sy * sy), limit = mu * fn;
+        const double scale = Ftv > limit ? 1.0 - limit / std::max(Ftv, 1e-12) : 0.0;
+        const double dax = sx * scale, day = sy * scale;
+        if (scale > 0) { flAx[i] += dax; flAy[i] += day; }
+        const double ex = sx - dax, ey = sy - day;
+        f[0] = -kt * ex; f[1] = -kt * ey; f[2] = fn;
+        flState[i] = scale > 0 ? 2 : 1;
+        e += 0.5 * kn * pen * pen + 0.5 * kt * (ex * ex + ey * ey);
+        if (fn > fmax) fmax = fn;
+      } else {
+        flAx[i] = x[0]; flAy[i] = x[1];
+        f[0] = f[1] = f[2] = 0; flState[i] = 0;
+      }
+      for (int k = 0; k < 3; k++) F[3 * size_t(i) + k] += f[k];
+    }
+    floorEnergy = e; floorFnMax = fmax;
+  }
+
   // ---------------------------------------------------------------------------------------------- load protocol
   // The UTM replay of the reference's GPU form (web/js/wgsl.js:1048-1093, set up by solver_gpu.js:215,286,296-318),
   // restated over this CPU iteration: the reference's CPU solver has no protocol of its own.
@@ -909,6 +964,8 @@ struct Solver {
     std::vector<double> kNode(n, 0.0), kSeg(m, 0.0);
     rod.addStiffness(st, kNode);
     if (hasContact) contact.addStiffness(st, kNode, kSeg);
+    floorBind(md);
+    if (hasFloor) for (int i = 0; i < n; i++) kNode[i] += sp.strength + sp.stick_strength;   // Floor.addStiffness
     const double ms = sp.mass_scale;
     mass.resize(n);
     for (int i = 0; i < n; i++) mass[i] = ms * std::max(kNode[i], 1e-12);
@@ -932,7 +989,8 @@ struct Solver {
     c = st.p ? c / std::max(lmin, 1e-12) : 0;
     double d = 0;
     if (hasContact) { d = -INF; for (double v : contact.Fn) d = std::max(d, v); }
-    return std::max(std::max(std::max(a, b), std::max(c, d)), 1e-12);
+    const double e = hasFloor ? floorFnMax : 0.0;
+    return std::max(std::max(std::max(a, b), std::max(c, d)), std::max(e, 1e-12));
   }
 
   // solver_cpu.js:737-841 (no floor, no rigid-body freedoms)
@@ -963,6 +1021,7 @@ struct Solver {
         for (int k = 0; k < 3; k++) total[3 * size_t(proto.probe) + k] += utmPf[k];
       for (size_t i = 0; i < 3 * size_t(n); i++) F[i] += total[i];
       if (hasContact) contact.apply(st, F.data(), T.data());
+      if (hasFloor) floorApply(rampN == 0 ? 1.0 : std::min(1.0, 0.01 + 0.99 * st.iteration / rampN));
       std::fill(reactions.begin(), reactions.end(), 0.0);
       for (int i = 0; i < n; i++) if (fixedAny[i]) for (int k = 0; k < 3; k++) reactions[3 * size_t(i) + k] = -F[3 * size_t(i) + k];
       for (size_t i = 0; i < 3 * size_t(n); i++) if (!nodeFree[i]) F[i] = 0;
@@ -1068,7 +1127,9 @@ struct orc_view {
   double *theta, *phi, *area, *pressure, *util;
   double *lambda, *dent, *M_rot, *rot_slip;     // contact extensions (buildResults, solver_cpu.js:906-908)
   double *utm;                                  // load protocol read-out [4 WS_PROTOCOL_MAX_INC]
-  int32_t utm_inc, utm_phase, utm_done;
+  int32_t utm_inc, utm_phase, utm_done, has_floor;
+  double *floor_F, e_floor;                     // the ground
+  uint8_t *floor_state;
 };
 
 void *orc_create(const ws_model *md) {
@@ -1108,6 +1169,8 @@ void orc_view_get(void *h, orc_view *v) {
   v->lambda = s->hasContact ? s->contact.lam.data() : nullptr; v->dent = s->hasContact ? s->contact.dentSum.data() : nullptr;
   v->M_rot = s->hasContact ? s->contact.Mrot.data() : nullptr; v->rot_slip = s->hasContact ? s->contact.rotSlip.data() : nullptr;
   v->utm = s->utmOut.data(); v->utm_inc = s->utmInc; v->utm_phase = s->utmPhase; v->utm_done = s->utmDone ? 1 : 0;
+  v->has_floor = s->hasFloor; v->floor_F = s->hasFloor ? s->flF.data() : nullptr; v->e_floor = s->floorEnergy;
+  v->floor_state = s->hasFloor ? s->flState.data() : nullptr;
   v->N = s->rod.N.data(); v->Vsh = s->rod.Vs.data(); v->M = s->rod.M.data(); v->reactions = s->reactions.data();
   v->mass = s->mass.data(); v->inertia3 = s->inertia3.data(); v->k_rot_static = s->kRotStatic.data();
   v->F = s->F.data(); v->T = s->T.data(); v->tm = s->tm.data();

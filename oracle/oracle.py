@@ -26,7 +26,8 @@ class OrcView(C.Structure):
                                    "Vsh", "M", "reactions", "mass", "inertia3", "k_rot_static", "F", "T", "tm")] + \
                [("stuck", C.POINTER(C.c_uint8)), ("ctype", C.POINTER(C.c_int32))] + \
                [(k, _dp) for k in ("theta", "phi", "area", "pressure", "util", "lambda", "dent", "M_rot", "rot_slip")] + \
-               [("utm", _dp), ("utm_inc", C.c_int32), ("utm_phase", C.c_int32), ("utm_done", C.c_int32)]
+               [("utm", _dp), ("utm_inc", C.c_int32), ("utm_phase", C.c_int32), ("utm_done", C.c_int32),
+                ("has_floor", C.c_int32), ("floor_F", _dp), ("e_floor", C.c_double), ("floor_state", C.POINTER(C.c_uint8))]
 
 
 _lib = None
@@ -124,6 +125,9 @@ class Oracle:
         out["ctype"] = np.ctypeslib.as_array(v.ctype, shape=(K,)).astype(np.uint8) if hc else np.zeros(0, dtype=np.uint8)
         out["utm"] = _arr(v.utm, 4 * 64).copy()
         out["utm_inc"], out["utm_phase"], out["utm_done"] = v.utm_inc, v.utm_phase, v.utm_done
+        out["e_floor"] = v.e_floor
+        out["floor_F"] = _arr(v.floor_F, 3 * n).copy() if v.has_floor else np.zeros(3 * n)
+        out["floor_state"] = np.ctypeslib.as_array(v.floor_state, shape=(n,)).copy() if v.has_floor else np.zeros(n, np.uint8)
         for k, s_ in (("theta", K), ("phi", 2 * K), ("area", K), ("pressure", K), ("util", K), ("lambda", K), ("dent", K),
                       ("M_rot", K), ("rot_slip", K)):
             a = _arr(getattr(v, k), s_) if hc else np.zeros(0)

@@ -111,3 +111,16 @@ def beam_midspan_stiffness(L=1000.0, w=60.0, h=30.0):
     """Timoshenko: P / δ of a simply supported beam under a mid-span load (bending about the 60 mm face)"""
     I = w * h ** 3 / 12
     return 1.0 / (L ** 3 / (48 * E_MM * I) + L / (4 * KAPPA * G_MM * w * h))
+
+
+def ground_beam(pull=0.0, q=10.0, mu=0.5, nseg=10, L=1000.0, **prm):
+    """a 1000 mm lath lying on the ground (scene.floor at its underside, z = −15) under 10 N down at every node, held
+    only in y and against twist at one end (the ground carries it); `pull` along x at the free end"""
+    prm.setdefault("max_iter", 20000)
+    md = straight(L, nseg, anchors=[((0, 0), ws.mask(0, 1, 0, 0, 0, 1))],
+                  params=mm_params(contacts=0, floor=1, floor_z=-15.0, floor_mu=mu, **prm))
+    md.load_const[2::3] -= q
+    md.load_const[3 * nseg] += pull
+    md.node_w = np.full(md.n, 60.0)
+    md.node_h = np.full(md.n, 30.0)
+    return md

@@ -649,3 +649,51 @@ def test_protocol_refused_by_the_grid_form():
     md = cases.utm_beam(1, [10.0])
     with pytest.raises(Exception):
         ws.GpuSolver([md.copy()], precision="f64", form="grid")
+
+
+# ---------------------------------------------------------------------------------------------- the ground
+GROUND_FIELDS = ("X", "floor_F", "floor_state", "reactions")
+
+
+@pytest.mark.parametrize("pull", [0.0, 20.0, 80.0])
+@pytest.mark.parametrize("form", ["cta", "plain", "grid"])
+def test_ground_matches_oracle(oracle_mod, pull, form):
+    """the ground (Floor.apply, solver_cpu.js:572-620) under a lath: carrying, sticking, sliding"""
+    md = cases.ground_beam(pull)
+    v = oracle_mod.Oracle(md.copy()).run(6000)
+    s = ws.GpuSolver([md.copy()], precision="f64", form=form)
+    ctl = s.step(6000)[0]
+    g = s.download(0, fields=GROUND_FIELDS)
+    s.dispose()
+    assert ctl["iter"] == v["iteration"] and ctl["rollbacks"] == v["rollbacks"]
+    assert cases.max_rel_disp_error(g["X"], v["X"], v["X0"]) < 1e-9
+    assert np.array_equal(g["floor_state"], v["floor_state"])
+    assert np.abs(g["floor_F"] - v["floor_F"]).max() < 1e-9 * np.abs(v["floor_F"]).max()
+    assert abs(ctl["e_floor"] - v["e_floor"]) < 1e-9 * v["e_floor"]
+
+
+@pytest.mark.parametrize("form", ["cta", "plain"])
+def test_gridshell_on_the_ground_matches_oracle(oracle_mod, form):
+    """the small dome with the ground 3 mm above its lowest node: the laths near the supports bear on it"""
+    md = ws.configs.dome_small()
+    md.params.update(floor=1, floor_z=float(md.X[2::3].min()) + 0.003, floor_mu=0.4)
+    o = oracle_mod.Oracle(md.copy())
+    o.step(1000)
+    v = o.view()
+    s = ws.GpuSolver([md.copy()], precision="f64", form=form)
+    ctl = s.step(1000)[0]
+    g = s.download(0, fields=GROUND_FIELDS)
+    s.dispose()
+    assert ctl["iter"] == 1000 and (v["floor_state"] > 0).sum() > 10
+    assert cases.max_node_err_span(g["X"], v["X"], md.span) < 1e-9
+    assert np.array_equal(g["floor_state"], v["floor_state"])
+    assert np.abs(g["floor_F"] - v["floor_F"]).max() < 1e-8 * np.abs(v["floor_F"]).max()
+
+
+def test_ground_alone_is_refused():
+    """a model that only the ground holds needs the rigid-body freedoms, which this build does not have"""
+    md = cases.ground_beam(0.0)
+    md.anchor_node = md.anchor_node[:0]
+    md.anchor_mask = md.anchor_mask[:0]
+    with pytest.raises(Exception):
+        ws.GpuSolver([md.copy()], precision="f64")

@@ -269,3 +269,30 @@ def test_protocol_displacement_control(oracle_mod):
     kf = 10.0 / oracle_mod.Oracle(cases.utm_beam(1, [10.0]).copy()).run(2_000_000, chunk=5000)["utm"][0]
     ratio = out[:, 1] / out[:, 0] / kf
     assert abs(ratio[0] - 1) < 1e-3 and np.all(np.abs(ratio - 1) < 5e-3) and np.all(np.diff(ratio) > 0)
+
+
+# ---------------------------------------------------------------------------------------------- the ground
+# Floor (solver_cpu.js:509-634): a lath lying on the ground under 10 N per node, held only in y and against twist at
+# one end.  The ground carries the load; a pull below μ·ΣFn sticks, one above it slides on the friction cone.
+
+def test_ground_carries_the_load(oracle_mod):
+    v = oracle_mod.Oracle(cases.ground_beam(0.0).copy()).run(6000)
+    F = v["floor_F"].reshape(-1, 3)
+    assert v["converged"] and np.all(v["floor_state"] == 1)
+    assert abs(F[:, 2].sum() - 110.0) < 1e-3 * 110.0 and np.all(F[:, 2] > 0)
+    assert v["e_floor"] > 0
+
+
+def test_ground_friction_sticks_below_the_cone(oracle_mod):
+    v = oracle_mod.Oracle(cases.ground_beam(20.0).copy()).run(6000)
+    F = v["floor_F"].reshape(-1, 3)
+    assert v["converged"] and np.all(v["floor_state"] == 1)
+    assert abs(F[:, 0].sum() + 20.0) < 0.01
+
+
+def test_ground_friction_slides_on_the_cone(oracle_mod):
+    v = oracle_mod.Oracle(cases.ground_beam(80.0).copy()).run(6000)
+    F = v["floor_F"].reshape(-1, 3)
+    assert not v["converged"] and np.all(v["floor_state"] == 2)
+    assert abs(abs(F[:, 0].sum()) - 0.5 * F[:, 2].sum()) < 1e-9 * F[:, 2].sum()
+    assert v["X"][-3] > 1000.0 + 10.0                     # the free end has slid along x

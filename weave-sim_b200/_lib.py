@@ -32,7 +32,8 @@ class WsParams(C.Structure):
                 ("torsion_factor", C.c_double), ("epsilon", C.c_double), ("ramp_iter", C.c_int32),
                 ("disp_ramp_iter", C.c_int32), ("slip_rate", C.c_double), ("edge_threshold", C.c_double),
                 ("augmented", C.c_int32), ("al_every", C.c_int32), ("rot_friction", C.c_int32), ("seat_law", C.c_int32),
-                ("seat_gap", C.c_int32), ("dent_after_iter", C.c_int32), ("rot_factor", C.c_double), ("dent_rate", C.c_double)]
+                ("seat_gap", C.c_int32), ("dent_after_iter", C.c_int32), ("rot_factor", C.c_double), ("dent_rate", C.c_double),
+                ("floor", C.c_int32), ("pad1", C.c_int32), ("floor_z", C.c_double), ("floor_mu", C.c_double)]
 
 
 PARAM_KEYS = [f[0] for f in WsParams._fields_ if not f[0].startswith("pad")]
@@ -59,7 +60,7 @@ class WsModel(C.Structure):
                 ("cross_strand", _ip), ("cross_wk", _dp), ("cross_hk", _dp), ("cross_u", _dp), ("cross_nprev", _dp),
                 ("cross_enabled", _bp), ("cross_locked", _bp), ("cross_mu", _dp),
                 ("cross_fc90", _dp), ("cross_E90", _dp), ("cross_H", _dp), ("params", WsParams),
-                ("protocol", C.POINTER(WsProtocol))]
+                ("protocol", C.POINTER(WsProtocol)), ("node_w", _dp), ("node_h", _dp)]
 
 
 class WsKagomeCfg(C.Structure):
@@ -84,7 +85,7 @@ class WsControl(C.Structure):
                 ("ke", C.c_double), ("ke_prev", C.c_double), ("residual", C.c_double), ("res_force", C.c_double),
                 ("res_torque", C.c_double), ("fref", C.c_double), ("e_stretch", C.c_double), ("e_shear", C.c_double),
                 ("e_bend", C.c_double), ("e_twist", C.c_double), ("e_contact", C.c_double),
-                ("utm_inc", C.c_int32), ("utm_phase", C.c_int32)]
+                ("utm_inc", C.c_int32), ("utm_phase", C.c_int32), ("e_floor", C.c_double)]
 
     def as_dict(self):
         return {f[0]: getattr(self, f[0]) for f in self._fields_}
@@ -100,7 +101,7 @@ class WsStateOut(C.Structure):
                [("stuck", _bp), ("state", _bp)] + \
                [(k, _dp) for k in ("Fn", "Ft", "gap", "N", "Vsh", "M", "reactions")] + \
                [("ctype", _bp)] + [(k, _dp) for k in ("theta", "phi", "area", "pressure", "util")] + \
-               [(k, _dp) for k in ("lambda", "dent", "M_rot", "rot_slip", "utm")]
+               [(k, _dp) for k in ("lambda", "dent", "M_rot", "rot_slip", "utm", "floor_F")] + [("floor_state", _bp)]
 
 
 _lib = None
@@ -192,11 +193,11 @@ class Model:
 
     FLOAT = ("X", "X0", "Q", "l0", "joint_len", "omega0", "EA", "EIx", "EIy", "GJ", "GA", "load_const",
              "local_load_F", "cross_wk", "cross_hk", "cross_u", "cross_nprev", "cross_mu", "anchor_target",
-             "cross_fc90", "cross_E90", "cross_H")
+             "cross_fc90", "cross_E90", "cross_H", "node_w", "node_h")
     INT = ("seg_i0", "seg_i1", "seg_offset", "joint_seg0", "joint_seg1", "local_load_node", "anchor_node",
            "cross_strand")
     BYTE = ("anchor_mask", "cross_enabled", "cross_locked")
-    OPTIONAL = ("omega0", "anchor_target", "cross_fc90", "cross_E90", "cross_H")   # NULL in the C struct: None here
+    OPTIONAL = ("omega0", "anchor_target", "cross_fc90", "cross_E90", "cross_H", "node_w", "node_h")   # NULL: None
 
     def __init__(self):
         self.n = self.m = self.p = self.n_strands = self.K = 0
@@ -217,7 +218,8 @@ class Model:
                  "seg_i0": self.m, "seg_i1": self.m, "seg_offset": self.n_strands + 1, "joint_seg0": self.p,
                  "joint_seg1": self.p, "local_load_node": nl, "anchor_node": na, "cross_strand": 2 * self.K,
                  "anchor_mask": na, "cross_enabled": self.K, "cross_locked": self.K,
-                 "anchor_target": 3 * na, "cross_fc90": 2 * self.K, "cross_E90": 2 * self.K, "cross_H": 2 * self.K}
+                 "anchor_target": 3 * na, "cross_fc90": 2 * self.K, "cross_E90": 2 * self.K, "cross_H": 2 * self.K,
+                 "node_w": self.n, "node_h": self.n}
         for k, dt in [(k, np.float64) for k in cls.FLOAT] + [(k, np.int32) for k in cls.INT] + \
                      [(k, np.uint8) for k in cls.BYTE]:
             ptr, n = getattr(md, k), sizes[k]

@@ -34,6 +34,7 @@ void ws_params_default(ws_params *p) {
   p->ramp_iter = 1500; p->slip_rate = 1.0; p->edge_threshold = 0.5;
   p->augmented = 0; p->al_every = 600; p->rot_friction = 0; p->seat_law = 0; p->seat_gap = 1; p->dent_after_iter = -1;
   p->rot_factor = 1.0; p->dent_rate = 0.01;
+  p->floor = 0; p->floor_z = 0.0; p->floor_mu = 0.5;
 }
 
 int ws_scene_kagome(const ws_kagome_cfg *cfg, ws_scene **out) {

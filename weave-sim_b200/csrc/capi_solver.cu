@@ -78,6 +78,8 @@ void layout(Dev<P> &d, Carver &cv, const Sizes &z) {
   d.fc90 = cv.take<R>(2 * k); d.E90 = cv.take<R>(2 * k); d.Hs = cv.take<R>(2 * k); d.sProj = cv.take<R>(4 * k); d.sinT = cv.take<R>(k);
   d.ctype = cv.take<uint8_t>(k); d.theta = cv.take<R>(k); d.area = cv.take<R>(k); d.pres = cv.take<R>(k);
   d.util = cv.take<R>(k); d.phiS = cv.take<R>(2 * k);
+  d.flW = cv.take<R>(n); d.flH = cv.take<R>(n); d.flAx = cv.take<W>(n); d.flAy = cv.take<W>(n);
+  d.flF = cv.take<R>(3 * n); d.flState = cv.take<uint8_t>(n);
   d.utmSched = cv.take<double>(WS_PROTOCOL_MAX_INC * size_t(std::max(z.b, 1)));
   d.utmOut = cv.take<double>(4 * WS_PROTOCOL_MAX_INC * size_t(std::max(z.b, 1)));
   d.lam = cv.take<A>(k); d.penAcc = cv.take<A>(k); d.dent = cv.take<R>(2 * k); d.climb = cv.take<R>(2 * k);
@@ -266,6 +268,7 @@ InstDesc describe(const HostGoals &g, const Sizes &off) {
   I.ext = (I.aug || I.rotFric || I.seat) ? 1 : 0;
   I.utmMode = g.proto.mode; I.utmProbe = off.n + g.proto.probe; I.utmNInc = g.proto.n_inc; I.utmSettle = g.proto.settle;
   I.utmAvg = g.proto.avg; I.utmIdx = off.b;
+  I.floorOn = g.prm.floor ? 1 : 0; I.floorZ = g.prm.floor_z; I.floorMu = g.prm.floor_mu;
   for (int k = 0; k < 3; k++) I.utmAxis[k] = g.proto.axis[k];
   return I;
 }
@@ -414,6 +417,17 @@ void uploadState(ws_ctx *c, int b, int buf, bool withU) {
   CK(cudaStreamSynchronize(st));
 }
 
+// the section at every node of instance b, for the ground's clearance
+template <int P>
+void floorSections(ws_ctx *c, int b) {
+  Dev<P> &d = devOf<P>(c);
+  using R = typename Dev<P>::R;
+  const HostGoals &g = c->g[b];
+  if (g.nodeW.empty()) return;
+  put<R>(d.flW + c->inst[b].n0, g.nodeW.data(), g.n, c->st);
+  put<R>(d.flH + c->inst[b].n0, g.nodeH.data(), g.n, c->st);
+}
+
 // the static arrays of instance b (topology, rest state, section constants)
 template <int P>
 void uploadStatic(ws_ctx *c, int b) {
@@ -472,6 +486,21 @@ void uploadStatic(ws_ctx *c, int b) {
   std::vector<uint8_t> one(K, 1);
   put<uint8_t>(d.stuck + I.k0, one.data(), K, st);
   put<double>(d.utmSched + size_t(I.utmIdx) * WS_PROTOCOL_MAX_INC, g.proto.sched, WS_PROTOCOL_MAX_INC, st);
+  floorSections<P>(c, b);
+}
+
+// the ground's stick points of instance b start under its nodes as the host goals hold them
+template <int P>
+void floorStart(ws_ctx *c, int b) {
+  Dev<P> &d = devOf<P>(c);
+  using W = typename Dev<P>::W;
+  const HostGoals &g = c->g[b];
+  const InstDesc &I = c->inst[b];
+  if (!g.prm.floor) return;
+  std::vector<double> ax(g.n), ay(g.n);
+  for (int i = 0; i < g.n; i++) { ax[i] = g.X[3 * size_t(i)]; ay[i] = g.X[3 * size_t(i) + 1]; }
+  put<W>(d.flAx + I.n0, ax.data(), g.n, c->st);
+  put<W>(d.flAy + I.n0, ay.data(), g.n, c->st);
 }
 
 // the contact-extension state of instance b at its start: no multiplier, no seats (wall slopes 1), no W2 reference angle
@@ -506,6 +535,7 @@ void uploadAll(ws_ctx *c) {
   for (size_t b = 0; b < c->g.size(); b++) {
     resetExt<P>(c, int(b));
     uploadStatic<P>(c, int(b));
+    floorStart<P>(c, int(b));
     uploadGoals<P>(c, int(b));
     uploadState<P>(c, int(b), 0, true);
     uploadState<P>(c, int(b), 1, false);
@@ -549,12 +579,13 @@ void fillControl(const InstCtl &s, ws_control *o) {
   o->iter = s.iter; o->status = s.status; o->rollbacks = s.rollbacks; o->pending_zero = s.pending;
   o->ke = s.ke; o->ke_prev = s.ke_prev; o->residual = s.residual; o->res_force = s.res_f; o->res_torque = s.res_t; o->fref = s.fref;
   o->e_stretch = s.e_stretch; o->e_shear = s.e_shear; o->e_bend = s.e_bend; o->e_twist = s.e_twist; o->e_contact = s.e_contact;
-  o->utm_inc = s.utmInc; o->utm_phase = s.utmPhase;
+  o->utm_inc = s.utmInc; o->utm_phase = s.utmPhase; o->e_floor = s.e_floor;
 }
 
-// some instance runs a contact extension: the kernels' variants with them
+// some instance runs an extension (contact extensions, the ground, a load protocol): the kernels' variants with them
 bool anyExt(const ws_ctx *c) {
-  for (const InstDesc &I : c->inst) if (I.ext && I.contacts && I.K) return true;
+  for (const InstDesc &I : c->inst)
+    if ((I.ext && I.contacts && I.K) || I.floorOn || I.utmMode) return true;
   return false;
 }
 
@@ -655,6 +686,7 @@ void downloadPacked(ws_ctx *c, int b, ws_state_out *o) {
   add(PF_LAM, I.K, 1, o->lambda, false); add(PF_DENT, I.K, 1, o->dent, false); add(PF_MROT, I.K, 1, o->M_rot, false);
   add(PF_RSLIP, I.K, 1, o->rot_slip, false);
   add(PF_UTM, WS_PROTOCOL_MAX_INC, 4, o->utm, false);
+  add(PF_FLF, I.n, 3, o->floor_F, false); add(PF_FLS, I.n, 1, o->floor_state, true);
   if (!L.nf) return;
   if (o->lambda) flushAL<P>(c, b);
   if (wantsClass(o)) CK(launchClassify<P>(devOf<P>(c), c->dInst, b, I.K, c->st));
@@ -715,6 +747,8 @@ void downloadImpl(ws_ctx *c, int b, ws_state_out *o) {
   if (o->M && p) f.planes(d.Mj, d.ptot, I.p0, p, 3, o->M);
   if (o->reactions) f.planes(d.react, d.ntot, I.n0, n, 3, o->reactions);
   if (o->utm) f.planes(d.utmOut, 0, size_t(I.utmIdx) * 4 * WS_PROTOCOL_MAX_INC, 4 * WS_PROTOCOL_MAX_INC, 1, o->utm);
+  if (o->floor_F) f.planes(d.flF, d.ntot, I.n0, n, 3, o->floor_F);
+  if (o->floor_state) f.bytes(d.flState + I.n0, n, o->floor_state);
   f.run(c);
 }
 
@@ -767,6 +801,7 @@ void setParamsImpl(ws_ctx *c, int b, const ws_model *md) {
   pullState<P>(c, b);
   HostGoals &g = c->g[b];
   const std::vector<int> oldSeg = g.cSeg;
+  const bool hadFloor = g.prm.floor != 0;
   HostGoals trial = g;
   trial.rebuild(*md);
   if (trial.cSeg != oldSeg) throw std::invalid_argument("the anchors changed the rotation clamps: create a new context");
@@ -777,6 +812,8 @@ void setParamsImpl(ws_ctx *c, int b, const ws_model *md) {
   c->inst[b] = describe(g, off);
   CK(cudaMemcpyAsync(c->dInst + b, &c->inst[b], sizeof(InstDesc), cudaMemcpyHostToDevice, c->st));
   uploadGoals<P>(c, b);
+  floorSections<P>(c, b);     // the ground's sections may have changed
+  if (!hadFloor) floorStart<P>(c, b);     // a new ground starts its stick points under the nodes (solver_cpu.js:689-690)
   flushPuts(c);
   readCtl(c);
   InstCtl s = c->ctlHost[b];
@@ -809,6 +846,7 @@ void loadInstanceImpl(ws_ctx *c, int b, const ws_model *md) {
   CK(cudaMemcpyAsync(c->dInst + b, &c->inst[b], sizeof(InstDesc), cudaMemcpyHostToDevice, c->st));
   uploadStatic<P>(c, b);
   uploadGoals<P>(c, b);
+  floorStart<P>(c, b);
   Dev<P> &d = devOf<P>(c);
   using A = typename Dev<P>::A;
   if (o.K) CK(cudaMemsetAsync(d.slip + c->inst[b].k0, 0, sizeof(A) * o.K, c->st));
@@ -860,6 +898,8 @@ void uploadStateImpl(ws_ctx *c, int b, const double *X, const double *Q, const d
   if (u && g.K) g.u.assign(u, u + 2 * size_t(g.K));
   g.startProtocol();          // an upload restarts the load protocol from the uploaded probe (solver_gpu.js:286,296-311)
   uploadState<P>(c, b, s.cur, u != nullptr);
+  floorStart<P>(c, b);
+  flushPuts(c);
   if (u && g.K) { g.sortSides(); uploadOrder<P>(c, b, s.obuf); flushPuts(c); }
   s.pending = 0; s.ke_prev = 0.0; s.status = WS_RUNNING;
   protocolCtl(g, s);

@@ -38,6 +38,9 @@ struct InstDesc {
   // instance's slot in the schedule and read-out arrays, probe axis
   int utmMode, utmProbe, utmNInc, utmSettle, utmAvg, utmIdx;
   double utmAxis[3];
+  // the ground: on / off, height, friction coefficient
+  int floorOn;
+  double floorZ, floorMu;
 };
 
 // per-instance control (device-written every iteration)
@@ -51,10 +54,11 @@ struct InstCtl {
   // averaged; probe force (mode 1), applied value, probe origin P0, sums of the probe travel (x, y, z) and reaction
   int utmPhase, utmIt, utmInc, utmAccN;
   double utmPf[3], utmCurF, utmP0[3], utmSum[4];
+  double e_floor;      // the ground's spring energy
 };
 
 // reduction slots
-enum { RS_KE = 0, RS_STRETCH, RS_SHEAR, RS_BEND, RS_TWIST, RS_PEN, RS_TAN, RS_NSUM };
+enum { RS_KE = 0, RS_STRETCH, RS_SHEAR, RS_BEND, RS_TWIST, RS_PEN, RS_TAN, RS_FLOOR, RS_NSUM };
 enum { RX_F = 0, RX_T, RX_N, RX_M, RX_FN, RX_LOAD, RX_NMAX };
 
 template <int P>
@@ -118,7 +122,12 @@ struct Dev {
   R *dentE, *theta0, *Mrot; // [ktot]
   A *rotSlip;               // [ktot]
   // load protocol: schedule [instances][WS_PROTOCOL_MAX_INC], read-out [instances][WS_PROTOCOL_MAX_INC][4]
-  double *utmSched, *utmOut;                  // [2 ktot]
+  double *utmSched, *utmOut;
+  // the ground: section at every node [ntot], stick points (state) [ntot], force [3][ntot] and contact state [ntot]
+  R *flW, *flH;
+  W *flAx, *flAy;
+  R *flF;
+  uint8_t *flState;                  // [2 ktot]
   // side records, indexed by side position p: the sides (sd = 2c + side) grouped by strand, ascending sd within a
   // strand (the strand's range is [stSideOff, stSideOff + stSideCnt))
   int *sPos;                // [2 ktot] position of side sd

@@ -74,9 +74,9 @@ __device__ __forceinline__ void phaseBC(const Dev<P> &d, const InstDesc &I, cons
   if (e < n2) rankSide<P>(d, 2 * I.k0 + e, sx.onxt, sx.onxt);
   else segCount<P>(d, I.m0 + (e - n2), sx.onxt, sx.onxt);
 }
-template <int P, bool SHORT>
+template <int P, bool SHORT, bool EXT>
 __device__ __forceinline__ void phaseD(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, int e, Part<typename Dev<P>::A> &pt) {
-  if (e < I.n) nodeUpdate<P, SHORT>(d, I, sx, I.n0 + e, pt);
+  if (e < I.n) nodeUpdate<P, SHORT, EXT>(d, I, sx, I.n0 + e, pt);
   else if ((e -= I.n) < I.m) segUpdate<P, SHORT>(d, I, sx, I.m0 + e, pt);
   else rankSideShort<P>(d, 2 * I.k0 + (e - I.m), sx.onxt);
 }
@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
       {
         const PhaseRun runs[3] = {{I.n, COST_NODE_UPD}, {I.m, COST_SEG_UPD}, {(SHORT && cx) ? 2 * I.K : 0, COST_RANK}};
         forBalanced(runs, [&](int r, int e) {
-          if (r == 0) nodeUpdate<P, SHORT>(d, I, sx, I.n0 + e, pt);
+          if (r == 0) nodeUpdate<P, SHORT, EXT>(d, I, sx, I.n0 + e, pt);
           else if (r == 1) segUpdate<P, SHORT>(d, I, sx, I.m0 + e, pt);
           else rankSideShort<P>(d, 2 * I.k0 + e, sx.onxt);
         });
@@ -185,10 +185,11 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
       blockReduce(pt, red);
       if (threadIdx.x == 0) decide(I, sc, pt, nIter);
       __syncthreads();
-      if (I.utmMode) {
-        if (threadIdx.x == 0) protocolStep<P>(d, sc.cur, I, sc);
-        __syncthreads();
-      }
+      if constexpr (EXT)
+        if (I.utmMode) {
+          if (threadIdx.x == 0) protocolStep<P>(d, sc.cur, I, sc);
+          __syncthreads();
+        }
     }
     if (threadIdx.x == 0) ctl[b] = sc;
     __syncthreads();
@@ -349,7 +350,7 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
       auto upd = [&](int r, int e) {
         if (r == 0) {
           if (I.kd) backupNode<P>(d, v, bk, I.n0 + e, false);
-          nodeUpdate<P, SHORT>(v, I, sx, I.n0 + e, pt);
+          nodeUpdate<P, SHORT, EXT>(v, I, sx, I.n0 + e, pt);
         } else if (r == 1) {
           if (I.kd) backupSeg<P>(d, v, bk, I.m0 + e, false);
           segUpdate<P, SHORT>(v, I, sx, I.m0 + e, pt);
@@ -379,10 +380,11 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
         }
         __syncthreads();
       }
-      if (I.utmMode) {
-        if (threadIdx.x == 0) protocolStep<P>(v, 0, I, sc);
-        __syncthreads();
-      }
+      if constexpr (EXT)
+        if (I.utmMode) {
+          if (threadIdx.x == 0) protocolStep<P>(v, 0, I, sc);
+          __syncthreads();
+        }
     }
     residentStore<P, SHORT>(d, v, I, sc);
     if (threadIdx.x == 0) ctl[b] = sc;
@@ -449,7 +451,7 @@ __global__ void __launch_bounds__(256) k_plainBC(Dev<P> d, const InstDesc *__res
 // fixed order and takes the kinetic-damping decision.  Every block reads the control block before it counts itself,
 // so the last block's write cannot race a reader.  The phase runs whole (PART 0) or split in two kernels on forked
 // branches: the nodes with the side ranks (PART 1) and the segments (PART 2), each at its own register budget.
-template <int P, bool SHORT, int PART>
+template <int P, bool SHORT, bool EXT, int PART>
 __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                        typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts, int partStride,
                                        unsigned *counter, unsigned nBlocks) {
@@ -465,13 +467,13 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
   const int nR = countD<SHORT>(I) - I.n - I.m;
   const int nD = PART == 1 ? I.n + nR : PART == 2 ? I.m : countD<SHORT>(I);
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nD; e += gridDim.x * blockDim.x) {
-    if (PART == 0) phaseD<P, SHORT>(d, I, sx, e, pt);
+    if (PART == 0) phaseD<P, SHORT, EXT>(d, I, sx, e, pt);
     else if (PART == 2) segUpdate<P, SHORT>(d, I, sx, I.m0 + e, pt);
-    else if (e < I.n) nodeUpdate<P, SHORT>(d, I, sx, I.n0 + e, pt);
+    else if (e < I.n) nodeUpdate<P, SHORT, EXT>(d, I, sx, I.n0 + e, pt);
     else rankSideShort<P>(d, 2 * I.k0 + (e - I.n), sx.onxt);
   }
   constexpr unsigned SM = SUMS_UPDATE;
-  constexpr unsigned XM = PART == 1 ? ((1u << RX_F) | (1u << RX_LOAD)) : PART == 2 ? (1u << RX_T) : MAXS_UPDATE;
+  constexpr unsigned XM = PART == 1 ? ((1u << RX_F) | (1u << RX_LOAD) | (1u << RX_FN)) : PART == 2 ? (1u << RX_T) : MAXS_UPDATE;
   blockReduce<SM, XM>(pt, red);
   if (threadIdx.x == 0) {
     putPart(pt, part, blockIdx.x, partStride);
@@ -486,32 +488,32 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
   for (int b = threadIdx.x; b < nParts; b += blockDim.x) addPart(q, partAll, b, partStride);
   blockReduce(q, red);
   if (threadIdx.x == 0) {
-    InstCtl cc = c;
+    InstCtl cc = ctl[0];      // reloaded (no block has written it): c's fields stay dead through the update
     decide(I, cc, q, 0);
-    protocolStep<P>(d, cc.cur, I, cc);
+    if constexpr (EXT) protocolStep<P>(d, cc.cur, I, cc);
     ctl[0] = cc;
     *counter = 0;
   }
 }
-template <int P, bool SHORT>
+template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(256, WSB_MINB_D) k_plainD(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                                 typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts,
                                                 int partStride, unsigned *counter) {
   waitPrevGrid();
   allowNextGrid();
-  plainD<P, SHORT, 0>(d, insts, ctl, part, partAll, nParts, partStride, counter, gridDim.x);
+  plainD<P, SHORT, EXT, 0>(d, insts, ctl, part, partAll, nParts, partStride, counter, gridDim.x);
 }
-template <int P, bool SHORT>
+template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(256, WSB_MINB_DN) k_plainDN(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                                   typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts,
                                                   int partStride, unsigned *counter, unsigned nBlocks) {
-  plainD<P, SHORT, 1>(d, insts, ctl, part, partAll, nParts, partStride, counter, nBlocks);
+  plainD<P, SHORT, EXT, 1>(d, insts, ctl, part, partAll, nParts, partStride, counter, nBlocks);
 }
-template <int P, bool SHORT>
+template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(256, WSB_MINB_DM) k_plainDM(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                                   typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts,
                                                   int partStride, unsigned *counter, unsigned nBlocks) {
-  plainD<P, SHORT, 2>(d, insts, ctl, part, partAll, nParts, partStride, counter, nBlocks);
+  plainD<P, SHORT, EXT, 2>(d, insts, ctl, part, partAll, nParts, partStride, counter, nBlocks);
 }
 
 // ------------------------------------------------------------------------------------------------ grid form
@@ -568,7 +570,7 @@ __global__ void __launch_bounds__(256, WSB_MINB_G) k_grid(Dev<P> d, const InstDe
       for (int e = gt; e < 2 * I.K + I.m; e += gs) phaseBC<P>(d, I, sx, e);
       if (!gridSync(bar, nb, err)) break;
     }
-    for (int e = gt; e < nD; e += gs) phaseD<P, SHORT>(d, I, sx, e, pt);
+    for (int e = gt; e < nD; e += gs) phaseD<P, SHORT, EXT>(d, I, sx, e, pt);
     blockReduce(pt, red);
     if (threadIdx.x == 0) putPart(pt, part, blockIdx.x, int(nb));
     if (!gridSync(bar, nb, err)) break;
@@ -603,6 +605,7 @@ __global__ void __launch_bounds__(256) k_unpack(Dev<P> d, const InstDesc *__rest
     const double x = (I.utmMode == 2 && i == I.utmProbe) ? in[e] + I.utmAxis[k] * v0 : in[e];
     Acc<P>::xs(d, cur, k, i, W(x));
     d.V[size_t(k) * d.nS + i] = R(0);
+    if (I.floorOn && k < 2) (k == 0 ? d.flAx : d.flAy)[i] = W(x);   // the ground's stick points start under the nodes
   }
   for (int e = gt; e < nQ; e += gs) {
     const int j = I.m0 + e / 4, k = e % 4;
@@ -718,7 +721,9 @@ __global__ void __launch_bounds__(256) k_pack(Dev<P> d, const InstDesc *__restri
         case PF_DENT: od[e] = double(d.dent[2 * (I.k0 + i)]) + double(d.dent[2 * (I.k0 + i) + 1]) + double(d.dentE[I.k0 + i]); break;
         case PF_MROT: od[e] = double(d.Mrot[I.k0 + i]); break;
         case PF_RSLIP: od[e] = double(d.rotSlip[I.k0 + i]); break;
-        default: od[e] = d.utmOut[size_t(I.utmIdx) * 4 * WS_PROTOCOL_MAX_INC + e]; break;
+        case PF_UTM: od[e] = d.utmOut[size_t(I.utmIdx) * 4 * WS_PROTOCOL_MAX_INC + e]; break;
+        case PF_FLF: od[e] = double(d.flF[size_t(k) * d.ntot + I.n0 + i]); break;
+        default: ob[e] = d.flState[I.n0 + i]; break;
       }
     }
   }
@@ -845,11 +850,11 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
     }
     if ((e = cudaEventRecord(fork->fork2, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(fork->side, fork->fork2, 0)) != cudaSuccess) return e;
-    if (sh2) k_plainDN<P, true><<<sh.blocksDNS, 256, 0, fork->side>>>(d, insts, ctl, pn, px, nParts, nParts, counter, nB);
-    else k_plainDN<P, false><<<sh.blocksDN, 256, 0, fork->side>>>(d, insts, ctl, pn, px, nParts, nParts, counter, nB);
+    const auto kdn = WSB_PICK(k_plainDN, P, sh2, ext);
+    kdn<<<sh2 ? sh.blocksDNS : sh.blocksDN, 256, 0, fork->side>>>(d, insts, ctl, pn, px, nParts, nParts, counter, nB);
     if ((e = cudaEventRecord(fork->join2, fork->side)) != cudaSuccess) return e;
-    if (sh2) k_plainDM<P, true><<<sh.blocksDM, 256, 0, st>>>(d, insts, ctl, pm, px, nParts, nParts, counter, nB);
-    else k_plainDM<P, false><<<sh.blocksDM, 256, 0, st>>>(d, insts, ctl, pm, px, nParts, nParts, counter, nB);
+    const auto kdm = WSB_PICK(k_plainDM, P, sh2, ext);
+    kdm<<<sh.blocksDM, 256, 0, st>>>(d, insts, ctl, pm, px, nParts, nParts, counter, nB);
     if ((e = cudaStreamWaitEvent(st, fork->join2, 0)) != cudaSuccess) return e;
     nl += 2;
     if (launches) *launches += nl;
@@ -864,8 +869,8 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
     if ((e = launchPDL(k_plainBC<P>, sh.blocksR, st, d, insts, ctl)) != cudaSuccess) return e;
     nl += 1;
   }
-  e = sh2 ? launchPDL(k_plainD<P, true>, sh.blocksDS, st, d, insts, ctl, pd, pa, nParts, nParts, counter)
-          : launchPDL(k_plainD<P, false>, sh.blocksD, st, d, insts, ctl, pd, pa, nParts, nParts, counter);
+  e = launchPDL(WSB_PICK(k_plainD, P, sh2, ext), sh2 ? sh.blocksDS : sh.blocksD, st, d, insts, ctl, pd, pa, nParts, nParts,
+                counter);
   if (e != cudaSuccess) return e;
   nl += 1;
   if (launches) *launches += nl;

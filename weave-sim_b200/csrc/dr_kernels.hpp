@@ -17,7 +17,8 @@ struct PlainFork { cudaStream_t side; cudaEvent_t fork, join, fork2, join2; };
 template <int P>
 cudaError_t launchBatched(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
                           const uint8_t *mask, int threads, int blocks, bool shortSides, bool ext, cudaStream_t st);
-// ext: some instance runs a contact extension (the crossing kernels' variant that has them)
+// ext: some instance runs an extension (contact extensions, the ground, a load protocol): the kernels' variants that
+// have them
 template <int P>
 cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, const PlainShape &sh, bool contacts,
                             bool shortSides, bool ext, cudaStream_t st, int *launches, unsigned *counter, const PlainFork *fork);
@@ -33,9 +34,10 @@ template <int P>
 cudaError_t residentPrepare(size_t bytes, bool shortSides, size_t *granted);
 // host <-> device transfers of one instance's state (interleaved per element, as the C ABI's arrays are)
 enum { PF_X, PF_Q, PF_V, PF_W, PF_U, PF_NPREV, PF_SLIP, PF_FN, PF_FT, PF_GAP, PF_N, PF_VSH, PF_M, PF_REACT, PF_STUCK, PF_STATE,
-       PF_CTYPE, PF_THETA, PF_PHI, PF_AREA, PF_PRES, PF_UTIL, PF_LAM, PF_DENT, PF_MROT, PF_RSLIP, PF_UTM };
+       PF_CTYPE, PF_THETA, PF_PHI, PF_AREA, PF_PRES, PF_UTIL, PF_LAM, PF_DENT, PF_MROT, PF_RSLIP, PF_UTM,
+       PF_FLF, PF_FLS };
 struct PackField { int kind, count, ncomp; long long off; };   // off: byte offset in the packed buffer
-struct PackList { PackField f[28]; int nf; };
+struct PackList { PackField f[32]; int nf; };
 // the multiplier update of instance b that fell due at the end of its last iteration, applied now
 template <int P>
 cudaError_t launchAlFlush(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, int b, cudaStream_t st);

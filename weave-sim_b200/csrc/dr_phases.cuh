@@ -845,7 +845,42 @@ __device__ __forceinline__ void sidesOn(const Dev<P> &d, int ob, int j, int lj, 
 // Both updates read everything first and store at the end, so no store stands between a load and the loads after it
 // (the compiler must assume they alias) and the loads of one element go out together.
 
-template <int P, bool SHORT>
+// the ground on node i (Floor.apply, solver_cpu.js:572-620): a penalty under the lowest point of the section in the
+// node's frame, a stick point on the plane dragged after the node by Coulomb's return mapping; adds to F.
+template <int P>
+__device__ __forceinline__ void floorForce(const Dev<P> &d, const InstDesc &I, const StepCtx &sc, int i,
+                                        const typename Dev<P>::W x[3], typename Dev<P>::R F[3], Part<typename Dev<P>::A> &pt) {
+  using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A;
+  const int nt = d.ntot;
+  const double rampN = I.ramp_iter;
+  const double ramp = rampN <= 0 ? 1.0 : fmin(1.0, 0.01 + 0.99 * double(sc.iter) / rampN);
+  const R kn = R(ramp * I.strength), kt = R(ramp * I.stick);
+  R q[4], Rn[9];
+  nodeQuat<P>(d, sc.cur, i, q);
+  qframe(q, Rn);
+  const R pen = R(W(I.floorZ) - x[2]) + (R(0.5) * ro(d.flW + i) * mabs(Rn[2]) + R(0.5) * ro(d.flH + i) * mabs(Rn[5]));
+  const W ax = d.flAx[i], ay = d.flAy[i];
+  R ff[3] = {R(0), R(0), R(0)};
+  if (pen > R(0)) {
+    const R fn = kn * pen;
+    const R sx = R(x[0] - ax), sy = R(x[1] - ay);
+    const R Ftv = kt * msqrt(sx * sx + sy * sy), limit = R(fmax(I.floorMu, 0.0)) * fn;
+    const R scale = Ftv > limit ? R(1) - limit / mmax(Ftv, R(1e-12)) : R(0);
+    const R dax = sx * scale, day = sy * scale;
+    if (scale > R(0)) { d.flAx[i] = ax + W(dax); d.flAy[i] = ay + W(day); }
+    const R ex = sx - dax, ey = sy - day;
+    ff[0] = -kt * ex; ff[1] = -kt * ey; ff[2] = fn;
+    d.flState[i] = scale > R(0) ? 2 : 1;
+    pt.s[RS_FLOOR] += A(R(0.5) * kn * pen * pen + R(0.5) * kt * (ex * ex + ey * ey));
+    pt.x[RX_FN] = mmax(pt.x[RX_FN], A(fn));
+  } else {
+    d.flAx[i] = x[0]; d.flAy[i] = x[1];
+    d.flState[i] = 0;
+  }
+  for (int k = 0; k < 3; k++) { d.flF[size_t(k) * nt + i] = ff[k]; F[k] += ff[k]; }
+}
+
+template <int P, bool SHORT, bool EXT>
 __device__ __forceinline__ void nodeUpdate(const Dev<P> &d, const InstDesc &I, const StepCtx &sc, int i, Part<typename Dev<P>::A> &pt) {
   using R = typename Dev<P>::R; using W = typename Dev<P>::W; using A = typename Dev<P>::A;
   const int nt = d.ntot, ns = d.nS, ms = d.mS, K2 = d.sS;
@@ -867,12 +902,15 @@ __device__ __forceinline__ void nodeUpdate(const Dev<P> &d, const InstDesc &I, c
     const R f0 = ro(d.ll + i), f1 = ro(d.ll + nt + i), f2 = ro(d.ll + 2 * nt + i);
     for (int k = 0; k < 3; k++) tot[k] += Rn[k] * f0 + Rn[3 + k] * f1 + Rn[6 + k] * f2;
   }
-  if (I.utmMode == 1 && i == I.utmProbe)   // the load protocol's force on its probe (wgsl.js:914)
-    for (int k = 0; k < 3; k++) tot[k] += R(sc.utmPf[k]);
+  if constexpr (EXT)
+    if (I.utmMode == 1 && i == I.utmProbe)   // the load protocol's force on its probe (wgsl.js:914)
+      for (int k = 0; k < 3; k++) tot[k] += R(sc.utmPf[k]);
   for (int k = 0; k < 3; k++) F[k] += tot[k];
   pt.x[RX_LOAD] = mmax(pt.x[RX_LOAD], A(mmax(mabs(tot[0]), mmax(mabs(tot[1]), mabs(tot[2])))));
   // crossing sides on the adjacent segments, as distributed by the last evaluation (weights 1 − t at a, t at b)
   const bool cx = I.contacts && I.K;
+  if constexpr (EXT)
+    if (I.floorOn) floorForce<P>(d, I, sc, i, x, F, pt);
   if (cx && so >= 0)
     sidesOn<SHORT>(d, sc.obuf, so, SHORT ? ro(d.segLocal + so) : 0, [&](int q) {
       const R wgt = R(1) - d.sT[q];
@@ -977,7 +1015,8 @@ __device__ __forceinline__ void segUpdate(const Dev<P> &d, const InstDesc &I, co
 // Slot sets: a kernel that feeds only some slots reduces only those (SM: sum slots, XM: max slots, bit i for slot i);
 // the others keep their identity values (0, or −∞ for RX_FN), so the result is the same as reducing every slot.
 constexpr unsigned SUMS_ALL = (1u << RS_NSUM) - 1, MAXS_ALL = (1u << RX_NMAX) - 1;
-constexpr unsigned SUMS_UPDATE = 1u << RS_KE, MAXS_UPDATE = (1u << RX_F) | (1u << RX_T) | (1u << RX_LOAD);
+constexpr unsigned SUMS_UPDATE = (1u << RS_KE) | (1u << RS_FLOOR),
+                   MAXS_UPDATE = (1u << RX_F) | (1u << RX_T) | (1u << RX_LOAD) | (1u << RX_FN);
 constexpr unsigned SUMS_CROSS = (1u << RS_PEN) | (1u << RS_TAN), MAXS_CROSS = 1u << RX_FN;
 constexpr unsigned SUMS_ROD = (1u << RS_STRETCH) | (1u << RS_SHEAR) | (1u << RS_BEND) | (1u << RS_TWIST),
                    MAXS_ROD = (1u << RX_N) | (1u << RX_M);
@@ -1045,7 +1084,7 @@ __device__ __forceinline__ void decide(const InstDesc &I, InstCtl &c, const Part
     c.alPend = (I.alEvery > 0 && c.iter > I.ramp_iter && (c.iter - I.ramp_iter) % I.alEvery == 0) ? 1 : 0;
   }
   const double maxM = I.p ? double(p.x[RX_M]) / fmax(I.jLenMin, 1e-12) : 0.0;
-  const double maxFn = (I.contacts && I.K) ? double(p.x[RX_FN]) : 0.0;
+  const double maxFn = ((I.contacts && I.K) || I.floorOn) ? double(p.x[RX_FN]) : 0.0;
   const double fref = fmax(fmax(fmax(double(p.x[RX_LOAD]), double(p.x[RX_N])), fmax(maxM, maxFn)), 1e-12);
   c.fref = fref;
   c.res_f = I.n ? double(p.x[RX_F]) / fref : 0.0;
@@ -1057,6 +1096,7 @@ __device__ __forceinline__ void decide(const InstDesc &I, InstCtl &c, const Part
   // contact energy of the iteration: ½ Σ k_n pen² + ½ k_t Σ |S_e|² with the ramp of that iteration
   const double rampd = I.ramp_iter <= 0 ? 1.0 : fmin(1.0, 0.01 + 0.99 * double(c.iter - 1) / I.ramp_iter);
   c.e_contact = 0.5 * double(p.s[RS_PEN]) + 0.5 * rampd * I.stick * double(p.s[RS_TAN]);
+  c.e_floor = double(p.s[RS_FLOOR]);
   if (c.status == WS_RUNNING && !I.utmMode) {        // a load protocol runs on past convergence (protocolStep)
     if (c.residual <= I.tol) c.status = WS_CONVERGED;
     else if (c.iter >= I.max_iter) c.status = WS_MAX_ITER;

@@ -126,6 +126,14 @@ void HostGoals::buildAnchors(const ws_model &md) {
   C = int(cSeg.size());
   if (proto.mode == 2)   // displacement control holds the probe (solver_gpu.js:215)
     for (int c = 0; c < 3; c++) nodeFree[3 * size_t(proto.probe) + c] = 0;
+  if (prm.floor) {
+    if (!md.node_w || !md.node_h) throw std::invalid_argument("model: a ground needs node_w and node_h");
+    bool held = C > 0;
+    for (uint8_t f : nodeFree) held = held || !f;
+    if (!held)
+      throw std::invalid_argument("model: a model that only the ground holds needs the rigid-body freedoms, which are not built");
+    nodeW.assign(md.node_w, md.node_w + n); nodeH.assign(md.node_h, md.node_h + n);
+  }
   fixedAny.assign(n, 0);
   for (int i = 0; i < n; i++) fixedAny[i] = (nodeFree[3 * size_t(i)] && nodeFree[3 * size_t(i) + 1] && nodeFree[3 * size_t(i) + 2]) ? 0 : 1;
   segClamp0.assign(m, -1); segClamp1.assign(m, -1);
@@ -323,6 +331,8 @@ void HostGoals::buildMasses(double ramp, const std::vector<double> &Fn) {
             kNode[pass ? segI1[seg] : segI0[seg]] += kr / (l * l);
           }
   }
+  if (prm.floor)                                      // Floor.addStiffness (solver_cpu.js:565)
+    for (int i = 0; i < n; i++) kNode[i] += prm.strength + prm.stick_strength;
   const double ms = prm.mass_scale;
   mass.resize(n);
   for (int i = 0; i < n; i++) mass[i] = ms * std::max(kNode[i], 1e-12);

@@ -36,6 +36,7 @@ struct HostGoals {
   std::vector<double> wk, hk, w, h, mu;
   std::vector<double> fc90, E90, Hs;                 // [2K] timber across the grain, each side (W1 classification)
   ws_protocol proto{};                               // load protocol (mode 0: none), kept over warm starts
+  std::vector<double> nodeW, nodeH;                  // [n] section at every node, for the ground (params.floor)
   double probe0[3] = {0, 0, 0};                      // the probe's position when the protocol started (P0)
   int dentAfterDefault = 1500;                       // first seat iteration when dent_after_iter < 0: warm-up + ramp of
                                                      // the model the instance was built from (solver_cpu.js:686)

@@ -615,6 +615,8 @@ void Scene::fillModel() {
   m.cross_fc90 = fc90.size() == 2 * size_t(st.K) && st.K ? fc90.data() : nullptr;
   m.cross_E90 = E90.size() == 2 * size_t(st.K) && st.K ? E90.data() : nullptr;
   m.cross_H = H.size() == 2 * size_t(st.K) && st.K ? H.data() : nullptr;
+  m.node_w = nodeW.size() == size_t(st.n) ? nodeW.data() : nullptr;
+  m.node_h = nodeH.size() == size_t(st.n) ? nodeH.data() : nullptr;
   m.params = params;
 }
 
@@ -626,6 +628,7 @@ void Scene::setUniformSection(double w, double h, double E, double G, double den
   // across the grain, in the proportions of the reference's default timber (params.js:6: E 10000, fc90 8, E90 800,
   // H 30), so that any unit system of E carries over
   fc90.assign(2 * size_t(st.K), 8e-4 * E); E90.assign(2 * size_t(st.K), 0.08 * E); H.assign(2 * size_t(st.K), 3e-3 * E);
+  nodeW.assign(st.n, w); nodeH.assign(st.n, h);
   loadConst.assign(3 * size_t(st.n), 0.0);
   if (gravity) {
     const double g[3] = {0.0, 0.0, -1.0};

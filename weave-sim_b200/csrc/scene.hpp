@@ -92,6 +92,7 @@ struct Scene {
   State st;
   std::vector<double> EA, EIx, EIy, GJ, GA, omega0, loadConst, localF, wk, hk, mu, anchorTarget;
   std::vector<double> fc90, E90, H;          // [2K] timber of each crossing side across the grain
+  std::vector<double> nodeW, nodeH;          // [n] section at every node (the ground's clearance)
   std::vector<int> localNode, anchorNode;
   std::vector<uint8_t> anchorMask, enabled, locked;
   ws_params params{};

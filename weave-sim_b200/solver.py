@@ -27,7 +27,8 @@ def device_count() -> int:
 
 
 STATE_FIELDS = ("X", "Q", "V", "W", "u", "nprev", "slip", "Fn", "Ft", "gap", "N", "Vsh", "M", "reactions", "stuck", "state",
-                "ctype", "theta", "phi", "area", "pressure", "util", "lambda", "dent", "M_rot", "rot_slip", "utm")
+                "ctype", "theta", "phi", "area", "pressure", "util", "lambda", "dent", "M_rot", "rot_slip", "utm", "floor_F",
+                "floor_state")
 
 
 def _state_buffers(md, fields=None):
@@ -36,12 +37,14 @@ def _state_buffers(md, fields=None):
     size = {"X": 3 * n, "Q": 4 * m, "V": 3 * n, "W": 3 * m, "u": 2 * K, "nprev": 3 * K, "slip": K, "Fn": K, "Ft": K,
             "gap": K, "N": m, "Vsh": 2 * m, "M": 3 * p, "reactions": 3 * n, "stuck": K, "state": K,
             "ctype": K, "theta": K, "phi": 2 * K, "area": K, "pressure": K, "util": K,
-            "lambda": K, "dent": K, "M_rot": K, "rot_slip": K, "utm": 4 * PROTOCOL_MAX_INC}
+            "lambda": K, "dent": K, "M_rot": K, "rot_slip": K, "utm": 4 * PROTOCOL_MAX_INC, "floor_F": 3 * n,
+            "floor_state": n}
     names = STATE_FIELDS if fields is None else tuple(fields)
     bad = [k for k in names if k not in size]
     if bad:
         raise ValueError(f"unknown state fields {bad}; known: {STATE_FIELDS}")
-    out = {k: np.zeros(size[k], dtype=np.uint8 if k in ("stuck", "state", "ctype") else np.float64) for k in names}
+    out = {k: np.zeros(size[k], dtype=np.uint8 if k in ("stuck", "state", "ctype", "floor_state") else np.float64)
+           for k in names}
     so = WsStateOut()
     for k, a in out.items():
         ct = C.c_uint8 if a.dtype == np.uint8 else C.c_double
