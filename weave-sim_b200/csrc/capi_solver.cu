@@ -82,6 +82,7 @@ void layout(Dev<P> &d, Carver &cv, const Sizes &z) {
   d.flF = cv.take<R>(3 * n); d.flState = cv.take<uint8_t>(n);
   d.utmSched = cv.take<double>(WS_PROTOCOL_MAX_INC * size_t(std::max(z.b, 1)));
   d.utmOut = cv.take<double>(4 * WS_PROTOCOL_MAX_INC * size_t(std::max(z.b, 1)));
+  d.ext = cv.take<InstExt>(size_t(std::max(z.b, 1)));
   d.lam = cv.take<A>(k); d.penAcc = cv.take<A>(k); d.dent = cv.take<R>(2 * k); d.climb = cv.take<R>(2 * k);
   d.tanpsi = cv.take<R>(2 * k); d.dentE = cv.take<R>(k); d.theta0 = cv.take<R>(k); d.Mrot = cv.take<R>(k);
   d.rotSlip = cv.take<A>(k);
@@ -128,6 +129,8 @@ struct ws_ctx {
   Dev<PREC_F32> d32{};
   InstDesc *dInst = nullptr;
   InstCtl *dCtl = nullptr;
+  InstExt *dExt = nullptr;         // the load protocols' state (in the arena)
+  std::vector<InstExt> extHost;
   int *dOrder = nullptr;
   uint8_t *dMask = nullptr;
   void *dPart = nullptr;
@@ -273,15 +276,15 @@ InstDesc describe(const HostGoals &g, const Sizes &off) {
   return I;
 }
 
-// the load protocol's control fields at its start: settling, no increment recorded, the first value applied
-void protocolCtl(const HostGoals &g, InstCtl &s) {
-  s.utmPhase = 0; s.utmIt = 0; s.utmInc = 0; s.utmAccN = 0;
-  for (int k = 0; k < 4; k++) s.utmSum[k] = 0.0;
-  s.utmCurF = g.proto.mode ? g.proto.sched[0] : 0.0;
+// the load protocol's state at its start: settling, no increment recorded, the first value applied
+InstExt protocolState(const HostGoals &g) {
+  InstExt u{};
+  u.curF = g.proto.mode ? g.proto.sched[0] : 0.0;
   for (int k = 0; k < 3; k++) {
-    s.utmPf[k] = g.proto.mode == 1 ? g.proto.axis[k] * g.proto.sched[0] : 0.0;
-    s.utmP0[k] = g.probe0[k];
+    u.pf[k] = g.proto.mode == 1 ? g.proto.axis[k] * g.proto.sched[0] : 0.0;
+    u.p0[k] = g.probe0[k];
   }
+  return u;
 }
 
 // upload the goal arrays of instance b (everything a warm start may change)
@@ -486,6 +489,8 @@ void uploadStatic(ws_ctx *c, int b) {
   std::vector<uint8_t> one(K, 1);
   put<uint8_t>(d.stuck + I.k0, one.data(), K, st);
   put<double>(d.utmSched + size_t(I.utmIdx) * WS_PROTOCOL_MAX_INC, g.proto.sched, WS_PROTOCOL_MAX_INC, st);
+  const InstExt u = protocolState(g);
+  put<InstExt>(d.ext + I.utmIdx, &u, 1, st);
   floorSections<P>(c, b);
 }
 
@@ -567,19 +572,24 @@ void setupDev(ws_ctx *c) {
   CK(cudaMemsetAsync(c->arena, 0, c->bytes, c->st));
   Carver cv{c->arena};
   layout<P>(d, cv, c->z);
+  c->dExt = d.ext;
   uploadAll<P>(c);
 }
 
 void readCtl(ws_ctx *c) {
   c->ctlHost.resize(c->inst.size());
   CK(cudaMemcpyAsync(c->ctlHost.data(), c->dCtl, sizeof(InstCtl) * c->inst.size(), cudaMemcpyDeviceToHost, c->st));
+  c->extHost.assign(c->inst.size(), InstExt{});
+  bool utm = false;
+  for (const InstDesc &I : c->inst) utm = utm || I.utmMode || I.floorOn;
+  if (utm && c->dExt) CK(cudaMemcpyAsync(c->extHost.data(), c->dExt, sizeof(InstExt) * c->inst.size(), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
 }
-void fillControl(const InstCtl &s, ws_control *o) {
+void fillControl(const InstCtl &s, const InstExt &u, ws_control *o) {
   o->iter = s.iter; o->status = s.status; o->rollbacks = s.rollbacks; o->pending_zero = s.pending;
   o->ke = s.ke; o->ke_prev = s.ke_prev; o->residual = s.residual; o->res_force = s.res_f; o->res_torque = s.res_t; o->fref = s.fref;
   o->e_stretch = s.e_stretch; o->e_shear = s.e_shear; o->e_bend = s.e_bend; o->e_twist = s.e_twist; o->e_contact = s.e_contact;
-  o->utm_inc = s.utmInc; o->utm_phase = s.utmPhase; o->e_floor = s.e_floor;
+  o->utm_inc = u.inc; o->utm_phase = u.phase; o->e_floor = u.eFloor;
 }
 
 // some instance runs an extension (contact extensions, the ground, a load protocol): the kernels' variants with them
@@ -855,7 +865,6 @@ void loadInstanceImpl(ws_ctx *c, int b, const ws_model *md) {
   InstCtl s;
   std::memset(&s, 0, sizeof(s));
   s.status = WS_RUNNING; s.residual = INFINITY;
-  protocolCtl(c->g[b], s);
   resetExt<P>(c, b);
   uploadState<P>(c, b, 0, true);
   // both buffers: a slice left over from the slot's previous model could point into another strand's sides
@@ -899,10 +908,13 @@ void uploadStateImpl(ws_ctx *c, int b, const double *X, const double *Q, const d
   g.startProtocol();          // an upload restarts the load protocol from the uploaded probe (solver_gpu.js:286,296-311)
   uploadState<P>(c, b, s.cur, u != nullptr);
   floorStart<P>(c, b);
+  if (g.proto.mode) {
+    const InstExt pu = protocolState(g);
+    put<InstExt>(devOf<P>(c).ext + c->inst[b].utmIdx, &pu, 1, c->st);
+  }
   flushPuts(c);
   if (u && g.K) { g.sortSides(); uploadOrder<P>(c, b, s.obuf); flushPuts(c); }
   s.pending = 0; s.ke_prev = 0.0; s.status = WS_RUNNING;
-  protocolCtl(g, s);
   CK(cudaMemcpyAsync(c->dCtl + b, &s, sizeof(InstCtl), cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
 }
@@ -1032,7 +1044,6 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
       InstCtl &s = ctl[b];
       std::memset(&s, 0, sizeof(s));
       s.status = WS_RUNNING; s.residual = INFINITY;
-      protocolCtl(c->g[b], s);
     }
     CK(cudaMemcpyAsync(c->dCtl, ctl.data(), sizeof(InstCtl) * n_instances, cudaMemcpyHostToDevice, c->st));
     const InstDesc &I0 = c->inst[0];
@@ -1083,7 +1094,7 @@ int ws_step(ws_ctx *c, int32_t n_iter, const uint8_t *mask, ws_control *ctl) {
     c->lastMs = -1;
     if (ctl) {
       readCtl(c);
-      for (size_t b = 0; b < c->inst.size(); b++) fillControl(c->ctlHost[b], ctl + b);
+      for (size_t b = 0; b < c->inst.size(); b++) fillControl(c->ctlHost[b], c->extHost[b], ctl + b);
     }
   });
 }
@@ -1092,7 +1103,7 @@ int ws_read_control(ws_ctx *c, ws_control *ctl) {
   if (!c || !ctl) return fail(WS_ERR_ARG, "ws_read_control: bad arguments");
   return guarded("ws_read_control", [&]() {
     readCtl(c);
-    for (size_t b = 0; b < c->inst.size(); b++) fillControl(c->ctlHost[b], ctl + b);
+    for (size_t b = 0; b < c->inst.size(); b++) fillControl(c->ctlHost[b], c->extHost[b], ctl + b);
   });
 }
 
@@ -1170,6 +1181,7 @@ template <int P>
 static void runInPlaceImpl(ws_ctx *c, char *base, int nIter, int threads, ws_state_out *out, ws_control *ctl) {
   Carver cv{base};
   layout<P>(devOf<P>(c), cv, c->z);
+  c->dExt = devOf<P>(c).ext;
   const size_t off = (cv.off + 255) & ~size_t(255);
   c->dInst = reinterpret_cast<InstDesc *>(base + off);
   c->dCtl = reinterpret_cast<InstCtl *>(base + off + ((sizeof(InstDesc) + 255) & ~size_t(255)));
@@ -1178,14 +1190,13 @@ static void runInPlaceImpl(ws_ctx *c, char *base, int nIter, int threads, ws_sta
   InstCtl s;
   std::memset(&s, 0, sizeof(s));
   s.status = WS_RUNNING; s.residual = INFINITY;
-  protocolCtl(c->g[0], s);
   CK(cudaMemcpyAsync(c->dCtl, &s, sizeof(InstCtl), cudaMemcpyHostToDevice, c->st));
   uploadAll<P>(c);
   if (nIter > 0)
     CK(launchBatched<P>(devOf<P>(c), c->dInst, c->dCtl, nullptr, 1, nIter, nullptr, threads, 1, c->shortSides, anyExt(c), c->st));
   CK(cudaStreamSynchronize(c->st));
   if (out) downloadImpl<P>(c, 0, out);
-  if (ctl) { readCtl(c); fillControl(c->ctlHost[0], ctl); }
+  if (ctl) { readCtl(c); fillControl(c->ctlHost[0], c->extHost[0], ctl); }
 }
 
 int runInPlace(int prec, const HostGoals &g, char *base, int nIter, int threads, cudaStream_t st, ws_state_out *out,

@@ -50,11 +50,16 @@ struct InstCtl {
   double ke, ke_prev, residual, res_f, res_t, fref;
   double e_stretch, e_shear, e_bend, e_twist, e_contact;
   int penN, alPend;    // augmented Lagrangian: iterations in the penetration window; the multiplier update is due
-  // load protocol: phase (0 settle, 1 average, 2 finished), iterations in the phase, increments recorded, samples
-  // averaged; probe force (mode 1), applied value, probe origin P0, sums of the probe travel (x, y, z) and reaction
-  int utmPhase, utmIt, utmInc, utmAccN;
-  double utmPf[3], utmCurF, utmP0[3], utmSum[4];
-  double e_floor;      // the ground's spring energy
+};
+
+// per-instance state of the extensions, apart from the control block that every iteration carries (kernel variants
+// without extensions never touch it): the load protocol's phase (0 settle, 1 average, 2 finished), iterations in the
+// phase, increments recorded, samples averaged; probe force (mode 1), applied value, probe origin P0, sums of the
+// probe travel (x, y, z) and reaction; the ground's spring energy
+struct InstExt {
+  int phase, it, inc, accN;
+  double pf[3], curF, p0[3], sum[4];
+  double eFloor;
 };
 
 // reduction slots
@@ -123,6 +128,7 @@ struct Dev {
   A *rotSlip;               // [ktot]
   // load protocol: schedule [instances][WS_PROTOCOL_MAX_INC], read-out [instances][WS_PROTOCOL_MAX_INC][4]
   double *utmSched, *utmOut;
+  InstExt *ext;             // [instances]
   // the ground: section at every node [ntot], stick points (state) [ntot], force [3][ntot] and contact state [ntot]
   R *flW, *flH;
   W *flAx, *flAy;

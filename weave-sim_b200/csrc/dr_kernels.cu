@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
     const bool cx = I.contacts && I.K;
     for (int it = 0; it < nIter; it++) {
       if (sc.status != WS_RUNNING) break;
-      const StepCtx sx = makeCtx<A>(I, sc, sc.utmPf);
+      const StepCtx sx = makeCtx<A>(I, sc, EXT ? d.ext[I.utmIdx].pf : nullptr);
       Part<A> pt;
       pt.init();
       blockPhaseA<P, SHORT, EXT>(d, I, sx, pt);
@@ -183,13 +183,12 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
       }
       __syncthreads();
       blockReduce(pt, red);
-      if (threadIdx.x == 0) decide(I, sc, pt, nIter);
+      if (threadIdx.x == 0) decide<EXT>(I, sc, pt, nIter);
       __syncthreads();
-      if constexpr (EXT)
-        if (I.utmMode) {
-          if (threadIdx.x == 0) protocolStep<P>(d, sc.cur, I, sc);
-          __syncthreads();
-        }
+      if constexpr (EXT) {
+        if (threadIdx.x == 0) protocolStep<P>(d, sc.cur, I, sc, pt);
+        __syncthreads();
+      }
     }
     if (threadIdx.x == 0) ctl[b] = sc;
     __syncthreads();
@@ -337,7 +336,7 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
     const bool cx = I.contacts && I.K;
     for (int it = 0; it < nIter; it++) {
       if (sc.status != WS_RUNNING) break;
-      StepCtx sx = makeCtx<A>(I, sc, sc.utmPf);
+      StepCtx sx = makeCtx<A>(I, sc, EXT ? d.ext[I.utmIdx].pf : nullptr);
       sx.cur = sx.nxt = 0;              // in place
       Part<A> pt;
       pt.init();
@@ -371,7 +370,7 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
       }
       __syncthreads();
       blockReduce(pt, red);
-      if (threadIdx.x == 0) decide(I, sc, pt, nIter);
+      if (threadIdx.x == 0) decide<EXT>(I, sc, pt, nIter);
       __syncthreads();
       if (sc.pending) {                 // roll-back: the positions and frames of the iteration's start
         for (int e = threadIdx.x; e < I.n + I.m; e += blockDim.x) {
@@ -380,11 +379,10 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
         }
         __syncthreads();
       }
-      if constexpr (EXT)
-        if (I.utmMode) {
-          if (threadIdx.x == 0) protocolStep<P>(v, 0, I, sc);
-          __syncthreads();
-        }
+      if constexpr (EXT) {
+        if (threadIdx.x == 0) protocolStep<P>(v, 0, I, sc, pt);
+        __syncthreads();
+      }
     }
     residentStore<P, SHORT>(d, v, I, sc);
     if (threadIdx.x == 0) ctl[b] = sc;
@@ -461,7 +459,7 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
   const InstDesc &I = insts[0];
   const InstCtl c = ctl[0];
   if (c.status != WS_RUNNING) return;
-  const StepCtx sx = makeCtx<A>(I, c, ctl[0].utmPf);
+  const StepCtx sx = makeCtx<A>(I, c, EXT ? d.ext[I.utmIdx].pf : nullptr);
   Part<A> pt;
   pt.init();
   const int nR = countD<SHORT>(I) - I.n - I.m;
@@ -472,8 +470,9 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
     else if (e < I.n) nodeUpdate<P, SHORT, EXT>(d, I, sx, I.n0 + e, pt);
     else rankSideShort<P>(d, 2 * I.k0 + (e - I.n), sx.onxt);
   }
-  constexpr unsigned SM = SUMS_UPDATE;
-  constexpr unsigned XM = PART == 1 ? ((1u << RX_F) | (1u << RX_LOAD) | (1u << RX_FN)) : PART == 2 ? (1u << RX_T) : MAXS_UPDATE;
+  constexpr unsigned SM = SUMS_UPDATE | (EXT && PART != 2 ? SUMS_FLOOR : 0u);
+  constexpr unsigned XF = EXT && PART != 2 ? MAXS_FLOOR : 0u;
+  constexpr unsigned XM = (PART == 1 ? ((1u << RX_F) | (1u << RX_LOAD)) : PART == 2 ? (1u << RX_T) : MAXS_UPDATE) | XF;
   blockReduce<SM, XM>(pt, red);
   if (threadIdx.x == 0) {
     putPart(pt, part, blockIdx.x, partStride);
@@ -488,9 +487,9 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
   for (int b = threadIdx.x; b < nParts; b += blockDim.x) addPart(q, partAll, b, partStride);
   blockReduce(q, red);
   if (threadIdx.x == 0) {
-    InstCtl cc = ctl[0];      // reloaded (no block has written it): c's fields stay dead through the update
-    decide(I, cc, q, 0);
-    if constexpr (EXT) protocolStep<P>(d, cc.cur, I, cc);
+    InstCtl cc = c;
+    decide<EXT>(I, cc, q, 0);
+    if constexpr (EXT) protocolStep<P>(d, cc.cur, I, cc, q);
     ctl[0] = cc;
     *counter = 0;
   }
@@ -578,7 +577,9 @@ __global__ void __launch_bounds__(256, WSB_MINB_G) k_grid(Dev<P> d, const InstDe
     q.init();
     for (int b = threadIdx.x; b < int(nb); b += blockDim.x) addPart(q, part, b, int(nb));
     blockReduce(q, red);
-    if (threadIdx.x == 0) decide(I, sc, q, nIter);
+    if (threadIdx.x == 0) decide<EXT>(I, sc, q, nIter);
+    if constexpr (EXT)      // the ground's energy (a load protocol is not run in this form)
+      if (blockIdx.x == 0 && threadIdx.x == 0) d.ext[I.utmIdx].eFloor = double(q.s[RS_FLOOR]);
     __syncthreads();
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl[0] = sc;
@@ -619,11 +620,12 @@ __global__ void __launch_bounds__(256) k_unpack(Dev<P> d, const InstDesc *__rest
     c.ke_prev = 0.0;
     c.status = WS_RUNNING;
     if (I.utmMode) {
-      c.utmPhase = 0; c.utmIt = 0; c.utmInc = 0; c.utmAccN = 0; c.utmCurF = v0;
-      for (int k = 0; k < 4; k++) c.utmSum[k] = 0.0;
+      InstExt &u = d.ext[I.utmIdx];
+      u.phase = 0; u.it = 0; u.inc = 0; u.accN = 0; u.curF = v0;
+      for (int k = 0; k < 4; k++) u.sum[k] = 0.0;
       for (int k = 0; k < 3; k++) {
-        c.utmP0[k] = in[3 * (I.utmProbe - I.n0) + k];
-        c.utmPf[k] = I.utmMode == 1 ? I.utmAxis[k] * v0 : 0.0;
+        u.p0[k] = in[3 * (I.utmProbe - I.n0) + k];
+        u.pf[k] = I.utmMode == 1 ? I.utmAxis[k] * v0 : 0.0;
       }
     }
   }

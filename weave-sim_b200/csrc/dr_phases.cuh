@@ -1015,8 +1015,8 @@ __device__ __forceinline__ void segUpdate(const Dev<P> &d, const InstDesc &I, co
 // Slot sets: a kernel that feeds only some slots reduces only those (SM: sum slots, XM: max slots, bit i for slot i);
 // the others keep their identity values (0, or −∞ for RX_FN), so the result is the same as reducing every slot.
 constexpr unsigned SUMS_ALL = (1u << RS_NSUM) - 1, MAXS_ALL = (1u << RX_NMAX) - 1;
-constexpr unsigned SUMS_UPDATE = (1u << RS_KE) | (1u << RS_FLOOR),
-                   MAXS_UPDATE = (1u << RX_F) | (1u << RX_T) | (1u << RX_LOAD) | (1u << RX_FN);
+constexpr unsigned SUMS_UPDATE = 1u << RS_KE, MAXS_UPDATE = (1u << RX_F) | (1u << RX_T) | (1u << RX_LOAD);
+constexpr unsigned SUMS_FLOOR = 1u << RS_FLOOR, MAXS_FLOOR = 1u << RX_FN;     // the ground's, in the node update
 constexpr unsigned SUMS_CROSS = (1u << RS_PEN) | (1u << RS_TAN), MAXS_CROSS = 1u << RX_FN;
 constexpr unsigned SUMS_ROD = (1u << RS_STRETCH) | (1u << RS_SHEAR) | (1u << RS_BEND) | (1u << RS_TWIST),
                    MAXS_ROD = (1u << RX_N) | (1u << RX_M);
@@ -1065,8 +1065,9 @@ __device__ __forceinline__ void blockReduce(Part<A> &p, A *smem) {
 }
 
 // ------------------------------------------------------------------------------------------------ phase E
-// kinetic-damping decision, residual and convergence of one instance from its reduced partials (solver_cpu.js:809-837)
-template <class A>
+// kinetic-damping decision, residual and convergence of one instance from its reduced partials (solver_cpu.js:809-837);
+// EXT: the kernel variant that has the extensions (the ground, a load protocol)
+template <bool EXT, class A>
 __device__ __forceinline__ void decide(const InstDesc &I, InstCtl &c, const Part<A> &p, int n_iter_stop) {
   double ke = 0.5 * double(p.s[RS_KE]);
   const bool rollback = I.kd && ke < c.ke_prev;
@@ -1084,7 +1085,7 @@ __device__ __forceinline__ void decide(const InstDesc &I, InstCtl &c, const Part
     c.alPend = (I.alEvery > 0 && c.iter > I.ramp_iter && (c.iter - I.ramp_iter) % I.alEvery == 0) ? 1 : 0;
   }
   const double maxM = I.p ? double(p.x[RX_M]) / fmax(I.jLenMin, 1e-12) : 0.0;
-  const double maxFn = ((I.contacts && I.K) || I.floorOn) ? double(p.x[RX_FN]) : 0.0;
+  const double maxFn = ((I.contacts && I.K) || (EXT && I.floorOn)) ? double(p.x[RX_FN]) : 0.0;
   const double fref = fmax(fmax(fmax(double(p.x[RX_LOAD]), double(p.x[RX_N])), fmax(maxM, maxFn)), 1e-12);
   c.fref = fref;
   c.res_f = I.n ? double(p.x[RX_F]) / fref : 0.0;
@@ -1096,8 +1097,7 @@ __device__ __forceinline__ void decide(const InstDesc &I, InstCtl &c, const Part
   // contact energy of the iteration: ½ Σ k_n pen² + ½ k_t Σ |S_e|² with the ramp of that iteration
   const double rampd = I.ramp_iter <= 0 ? 1.0 : fmin(1.0, 0.01 + 0.99 * double(c.iter - 1) / I.ramp_iter);
   c.e_contact = 0.5 * double(p.s[RS_PEN]) + 0.5 * rampd * I.stick * double(p.s[RS_TAN]);
-  c.e_floor = double(p.s[RS_FLOOR]);
-  if (c.status == WS_RUNNING && !I.utmMode) {        // a load protocol runs on past convergence (protocolStep)
+  if (c.status == WS_RUNNING && !(EXT && I.utmMode)) {   // a load protocol runs on past convergence (protocolStep)
     if (c.residual <= I.tol) c.status = WS_CONVERGED;
     else if (c.iter >= I.max_iter) c.status = WS_MAX_ITER;
   }
@@ -1108,46 +1108,49 @@ __device__ __forceinline__ void decide(const InstDesc &I, InstCtl &c, const Part
 // convergence or `settle` iterations, average the probe's travel from P0 and its reaction along the axis over `avg`
 // iterations, record them, then apply the next value of the schedule: the probe force (mode 1) or the probe's
 // position P0 + value·axis, at rest (mode 2).  d is the view whose buffer `buf` holds the positions the instance
-// continues from (after a roll-back, the restored ones).  One thread.
-template <int P>
-__device__ __forceinline__ void protocolStep(const Dev<P> &d, int buf, const InstDesc &I, InstCtl &c) {
+// continues from (after a roll-back, the restored ones).  One thread, in the kernel variants that have the extensions;
+// it also records the ground's energy of the iteration (p: the reduced partials).
+template <int P, class A>
+__device__ __forceinline__ void protocolStep(const Dev<P> &d, int buf, const InstDesc &I, InstCtl &c, const Part<A> &p) {
   using W = typename Dev<P>::W;
+  d.ext[I.utmIdx].eFloor = double(p.s[RS_FLOOR]);     // the ground's energy of the iteration, beside the protocol
   if (!I.utmMode || c.status != WS_RUNNING) return;
   const bool conv = c.residual <= I.tol;
   const int pi = I.utmProbe;
-  c.utmIt += 1;
-  if (c.utmPhase == 0) {
-    if (conv || c.utmIt >= I.utmSettle) {
-      c.utmPhase = 1; c.utmIt = 0; c.utmAccN = 0;
-      for (int k = 0; k < 4; k++) c.utmSum[k] = 0.0;
+  InstExt &u = d.ext[I.utmIdx];
+  u.it += 1;
+  if (u.phase == 0) {
+    if (conv || u.it >= I.utmSettle) {
+      u.phase = 1; u.it = 0; u.accN = 0;
+      for (int k = 0; k < 4; k++) u.sum[k] = 0.0;
     }
-  } else if (c.utmPhase == 1) {
+  } else if (u.phase == 1) {
     double r = 0.0;
     for (int k = 0; k < 3; k++) {
-      c.utmSum[k] += double(Acc<P>::xw(d, buf, k, pi)) - c.utmP0[k];
+      u.sum[k] += double(Acc<P>::xw(d, buf, k, pi)) - u.p0[k];
       r += double(d.react[size_t(k) * d.ntot + pi]) * I.utmAxis[k];
     }
-    c.utmSum[3] += r;
-    c.utmAccN += 1;
-    if (c.utmIt >= I.utmAvg) {
-      double *o = d.utmOut + (size_t(I.utmIdx) * WS_PROTOCOL_MAX_INC + c.utmInc) * 4;
-      const double n = double(c.utmAccN);
-      o[0] = (c.utmSum[0] * I.utmAxis[0] + c.utmSum[1] * I.utmAxis[1] + c.utmSum[2] * I.utmAxis[2]) / n;
-      o[1] = c.utmSum[3] / n;
-      o[2] = c.utmCurF;
+    u.sum[3] += r;
+    u.accN += 1;
+    if (u.it >= I.utmAvg) {
+      double *o = d.utmOut + (size_t(I.utmIdx) * WS_PROTOCOL_MAX_INC + u.inc) * 4;
+      const double n = double(u.accN);
+      o[0] = (u.sum[0] * I.utmAxis[0] + u.sum[1] * I.utmAxis[1] + u.sum[2] * I.utmAxis[2]) / n;
+      o[1] = u.sum[3] / n;
+      o[2] = u.curF;
       o[3] = double(c.iter);
-      c.utmInc += 1; c.utmIt = 0; c.utmPhase = 0;
-      if (c.utmInc >= I.utmNInc) {
-        c.utmPhase = 2;
+      u.inc += 1; u.it = 0; u.phase = 0;
+      if (u.inc >= I.utmNInc) {
+        u.phase = 2;
         c.status = WS_DONE;
       } else {
-        const double v = d.utmSched[size_t(I.utmIdx) * WS_PROTOCOL_MAX_INC + min(c.utmInc, WS_PROTOCOL_MAX_INC - 1)];
-        c.utmCurF = v;
+        const double v = d.utmSched[size_t(I.utmIdx) * WS_PROTOCOL_MAX_INC + min(u.inc, WS_PROTOCOL_MAX_INC - 1)];
+        u.curF = v;
         if (I.utmMode == 1) {
-          for (int k = 0; k < 3; k++) c.utmPf[k] = I.utmAxis[k] * v;
+          for (int k = 0; k < 3; k++) u.pf[k] = I.utmAxis[k] * v;
         } else {
           for (int k = 0; k < 3; k++) {
-            Acc<P>::xs(d, buf, k, pi, W(c.utmP0[k] + I.utmAxis[k] * v));
+            Acc<P>::xs(d, buf, k, pi, W(u.p0[k] + I.utmAxis[k] * v));
             d.V[size_t(k) * d.nS + pi] = 0;
           }
         }
