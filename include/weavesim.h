@@ -303,6 +303,10 @@ typedef struct ws_state_out {
   /* the ground (Floor.F / Floor.state, solver_cpu.js:541-546) */
   double *floor_F; /* [3n] the ground's force on every node */
   uint8_t *floor_state; /* [n] 0 clear of the ground, 1 stuck, 2 sliding */
+  /* results post-processing on the device (buildResults, solver_cpu.js:878-898; fields.js nodeValues) */
+  double *seg_M;   /* [3m] Mx, My, T of every segment, from the moments of its end joints and clamps */
+  double *node_M;  /* [4n] Mx, My, T, N at the nodes: the mean of a node's segments along its strand */
+  double *disp;    /* [3n] X − X0 (X0: the displacement origin, moved by ws_internalize) */
 } ws_state_out;
 int ws_download(ws_ctx *ctx, int32_t instance, ws_state_out *out);
 /* Uploads positions and frames (and zeroes velocities) of one instance from host buffers: a warm start from a state the

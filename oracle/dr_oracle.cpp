@@ -1232,5 +1232,30 @@ void orc_segment_moments(void *h, double *seg_m) {
     for (int j = 0; j < m; j++) { const int a = st.segI0[j], b = st.segI1[j]; for (int q = 0; q < nc; q++) if (!has[b]) seg_m[3 * size_t(j) + cols[q]] = nodeM[3 * size_t(a) + cols[q]]; }
   }
 }
+// results: the segment layers Mx My T N at the nodes (fields.js nodeValues without shear): the mean of a node's two
+// segments along its strand, the one segment at a strand's end, closed strands wrapping; out [4n] layer-major
+void orc_node_layers(void *h, double *out) {
+  auto *s = static_cast<orc::Solver *>(h);
+  const orc::St &st = s->st;
+  const int n = st.n, m = st.m;
+  std::vector<double> seg(3 * size_t(m));
+  orc_segment_moments(h, seg.data());
+  std::fill(out, out + 4 * size_t(n), 0.0);
+  for (int S = 0; S < int(st.segOffset.size()) - 1; S++) {
+    const int j0 = st.segOffset[S], ms = st.segOffset[S + 1] - j0;
+    if (ms < 1) continue;
+    const bool closed = ms > 2 && st.segI1[j0 + ms - 1] == st.segI0[j0];
+    for (int L = 0; L < 4; L++) {
+      auto A = [&](int j) { return L < 3 ? seg[3 * size_t(j0 + j) + L] : s->rod.N[j0 + j]; };
+      double *o = out + size_t(L) * n;
+      if (closed) {
+        for (int i = 0; i < ms; i++) o[st.segI0[j0 + i]] = 0.5 * (A((i - 1 + ms) % ms) + A(i));
+      } else {
+        for (int j = 0; j < ms; j++) { o[st.segI0[j0 + j]] += A(j); o[st.segI1[j0 + j]] += A(j); }
+        for (int j = 1; j < ms; j++) o[st.segI0[j0 + j]] *= 0.5;
+      }
+    }
+  }
+}
 
 }  // extern "C"

@@ -55,6 +55,7 @@ def lib():
         L.orc_set_clamps.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint8)]
         L.orc_set_state.argtypes = [C.c_void_p, _dp, _dp, _dp]
         L.orc_segment_moments.argtypes = [C.c_void_p, _dp]
+        L.orc_node_layers.argtypes = [C.c_void_p, _dp]
         _lib = L
     return _lib
 
@@ -156,6 +157,13 @@ class Oracle:
         keep = [np.ascontiguousarray(a, dtype=np.float64) if a is not None else None for a in (X, Q, omega0)]
         ptrs = [a.ctypes.data_as(_dp) if a is not None else None for a in keep]
         lib().orc_set_state(self.h, *ptrs)
+
+    def node_layers(self):
+        """Mx, My, T, N at the nodes (fields.js nodeValues): [4, n]"""
+        v = self._v()
+        out = np.zeros(4 * v.n)
+        lib().orc_node_layers(self.h, out.ctypes.data_as(_dp))
+        return out.reshape(4, v.n)
 
     def segment_moments(self):
         v = self._v()

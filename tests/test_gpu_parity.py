@@ -699,3 +699,32 @@ def test_ground_alone_is_refused():
     md.anchor_mask = md.anchor_mask[:0]
     with pytest.raises(Exception):
         ws.GpuSolver([md.copy()], precision="f64")
+
+
+# ---------------------------------------------------------------------------------------------- results
+RESULT_FIELDS = ("seg_M", "node_M", "disp", "N", "M")
+
+
+@pytest.mark.parametrize("name", ["cantilever", "torsion", "cross_press", "dome"])
+@pytest.mark.parametrize("form", ["cta", "plain"])
+def test_results_match_oracle(oracle_mod, name, form):
+    """results post-processing on the device (buildResults, solver_cpu.js:878-898; fields.js nodeValues): segment
+    moments from the joints and clamps, the segment layers at the nodes, displacements; after an internalize the
+    displacements start again from the current geometry"""
+    md = ws.configs.dome_small() if name == "dome" else cases.case_by_name(name)
+    it = 600 if name == "dome" else 3000
+    o = oracle_mod.Oracle(md.copy())
+    o.step(it)
+    v = o.view()
+    seg, lay = o.segment_moments(), o.node_layers()
+    s = ws.GpuSolver([md.copy()], precision="f64", form=form)
+    s.step(it)
+    g = s.download(0, fields=RESULT_FIELDS)
+    scale = lambda a: max(np.abs(a).max(), 1e-300)
+    assert np.abs(g["seg_M"] - seg).max() <= 1e-8 * scale(seg)
+    assert np.abs(g["node_M"].reshape(-1, 4).T - lay).max() <= 1e-8 * scale(lay)
+    assert np.abs(g["disp"] - (v["X"] - v["X0"])).max() <= 1e-9 * scale(v["X"] - v["X0"]) + 1e-12 * scale(v["X"])
+    s.internalize(0)
+    g2 = s.download(0, fields=("disp",))
+    s.dispose()
+    assert np.abs(g2["disp"]).max() == 0.0

@@ -101,7 +101,8 @@ class WsStateOut(C.Structure):
                [("stuck", _bp), ("state", _bp)] + \
                [(k, _dp) for k in ("Fn", "Ft", "gap", "N", "Vsh", "M", "reactions")] + \
                [("ctype", _bp)] + [(k, _dp) for k in ("theta", "phi", "area", "pressure", "util")] + \
-               [(k, _dp) for k in ("lambda", "dent", "M_rot", "rot_slip", "utm", "floor_F")] + [("floor_state", _bp)]
+               [(k, _dp) for k in ("lambda", "dent", "M_rot", "rot_slip", "utm", "floor_F")] + [("floor_state", _bp)] + \
+               [(k, _dp) for k in ("seg_M", "node_M", "disp")]
 
 
 _lib = None

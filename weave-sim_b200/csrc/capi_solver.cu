@@ -80,6 +80,8 @@ void layout(Dev<P> &d, Carver &cv, const Sizes &z) {
   d.util = cv.take<R>(k); d.phiS = cv.take<R>(2 * k);
   d.flW = cv.take<R>(n); d.flH = cv.take<R>(n); d.flAx = cv.take<W>(n); d.flAy = cv.take<W>(n);
   d.flF = cv.take<R>(3 * n); d.flState = cv.take<uint8_t>(n);
+  d.nodeJoint = cv.take<int>(n); d.nodeClamp = cv.take<int>(n); d.X0 = cv.take<W>(3 * n);
+  d.segM = cv.take<R>(3 * m); d.nodeLay = cv.take<R>(4 * n);
   d.utmSched = cv.take<double>(WS_PROTOCOL_MAX_INC * size_t(std::max(z.b, 1)));
   d.utmOut = cv.take<double>(4 * WS_PROTOCOL_MAX_INC * size_t(std::max(z.b, 1)));
   d.ext = cv.take<InstExt>(size_t(std::max(z.b, 1)));
@@ -420,6 +422,19 @@ void uploadState(ws_ctx *c, int b, int buf, bool withU) {
   CK(cudaStreamSynchronize(st));
 }
 
+// the displacement origin of instance b as the host goals hold it
+template <int P>
+void displacementOrigin(ws_ctx *c, int b) {
+  Dev<P> &d = devOf<P>(c);
+  using W = typename Dev<P>::W;
+  const HostGoals &g = c->g[b];
+  for (int k = 0; k < 3; k++) {
+    std::vector<double> x0(g.n);
+    for (int i = 0; i < g.n; i++) x0[i] = g.X0[3 * size_t(i) + k];
+    put<W>(d.X0 + size_t(k) * d.ntot + c->inst[b].n0, x0.data(), g.n, c->st);
+  }
+}
+
 // the section at every node of instance b, for the ground's clearance
 template <int P>
 void floorSections(ws_ctx *c, int b) {
@@ -492,6 +507,15 @@ void uploadStatic(ws_ctx *c, int b) {
   const InstExt u = protocolState(g);
   put<InstExt>(d.ext + I.utmIdx, &u, 1, st);
   floorSections<P>(c, b);
+  {
+    // the joint and the clamp at every node, for the segment moments of the results (buildResults)
+    std::vector<int> nj(n, -1), nc(n, -1);
+    for (size_t j = 0; j < p; j++) nj[g.segI1[g.jSeg0[j]]] = I.p0 + int(j);
+    for (size_t q = 0; q < g.cNode.size(); q++) nc[g.cNode[q]] = I.c0 + int(q);
+    put<int>(d.nodeJoint + I.n0, nj.data(), n, st);
+    put<int>(d.nodeClamp + I.n0, nc.data(), n, st);
+  }
+  displacementOrigin<P>(c, b);
 }
 
 // the ground's stick points of instance b start under its nodes as the host goals hold them
@@ -697,8 +721,10 @@ void downloadPacked(ws_ctx *c, int b, ws_state_out *o) {
   add(PF_RSLIP, I.K, 1, o->rot_slip, false);
   add(PF_UTM, WS_PROTOCOL_MAX_INC, 4, o->utm, false);
   add(PF_FLF, I.n, 3, o->floor_F, false); add(PF_FLS, I.n, 1, o->floor_state, true);
+  add(PF_SEGM, I.m, 3, o->seg_M, false); add(PF_NODEM, I.n, 4, o->node_M, false); add(PF_DISP, I.n, 3, o->disp, false);
   if (!L.nf) return;
   if (o->lambda) flushAL<P>(c, b);
+  if (o->seg_M || o->node_M) CK(launchResults<P>(devOf<P>(c), c->dInst, b, I.n, I.m, c->st));
   if (wantsClass(o)) CK(launchClassify<P>(devOf<P>(c), c->dInst, b, I.K, c->st));
   unsigned char *dv = xferBuf(c, off);
   CK(launchPack<P>(devOf<P>(c), c->dInst, c->dCtl, b, L, elems, dv, c->st));
@@ -759,6 +785,15 @@ void downloadImpl(ws_ctx *c, int b, ws_state_out *o) {
   if (o->utm) f.planes(d.utmOut, 0, size_t(I.utmIdx) * 4 * WS_PROTOCOL_MAX_INC, 4 * WS_PROTOCOL_MAX_INC, 1, o->utm);
   if (o->floor_F) f.planes(d.flF, d.ntot, I.n0, n, 3, o->floor_F);
   if (o->floor_state) f.bytes(d.flState + I.n0, n, o->floor_state);
+  if (o->seg_M || o->node_M) CK(launchResults<P>(d, c->dInst, b, I.n, I.m, c->st));
+  if (o->seg_M) f.planes(d.segM, d.mtot, I.m0, m, 3, o->seg_M);
+  if (o->node_M) f.planes(d.nodeLay, d.ntot, I.n0, n, 4, o->node_M);
+  if (o->disp) {
+    double *x = f.scratch(3 * n), *x0 = f.scratch(3 * n);
+    f.pairs(d.X + size_t(s.cur * 3) * d.ntot, PrecT<P>::TWO ? d.Xlo + size_t(s.cur * 3) * d.ntot : nullptr, d.ntot, I.n0, n, 3, x);
+    f.planes(d.X0, d.ntot, I.n0, n, 3, x0);
+    f.after.push_back([x, x0, n, out = o->disp]() { for (size_t q = 0; q < 3 * n; q++) out[q] = x[q] - x0[q]; });
+  }
   f.run(c);
 }
 
@@ -924,6 +959,8 @@ void internalizeImpl(ws_ctx *c, int b) {
   pullState<P>(c, b);
   HostGoals &g = c->g[b];
   g.X0 = g.X;
+  displacementOrigin<P>(c, b);
+  flushPuts(c);
   Dev<P> &d = devOf<P>(c);
   using A = typename Dev<P>::A;
   if (g.K) CK(cudaMemsetAsync(d.slip + c->inst[b].k0, 0, sizeof(A) * g.K, c->st));

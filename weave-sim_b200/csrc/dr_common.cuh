@@ -133,7 +133,12 @@ struct Dev {
   R *flW, *flH;
   W *flAx, *flAy;
   R *flF;
-  uint8_t *flState;                  // [2 ktot]
+  uint8_t *flState;
+  // results post-processing: the joint and the clamp at every node [ntot] (−1 none), the displacement origin [3][ntot],
+  // segment moments [3][mtot] and node layers [4][ntot] (outputs)
+  int *nodeJoint, *nodeClamp;
+  W *X0;
+  R *segM, *nodeLay;                  // [2 ktot]
   // side records, indexed by side position p: the sides (sd = 2c + side) grouped by strand, ascending sd within a
   // strand (the strand's range is [stSideOff, stSideOff + stSideCnt))
   int *sPos;                // [2 ktot] position of side sd

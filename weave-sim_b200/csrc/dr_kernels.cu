@@ -681,6 +681,52 @@ __global__ void __launch_bounds__(256) k_alFlush(Dev<P> d, const InstDesc *__res
   if (threadIdx.x == 0) { ctl[b].alPend = 0; ctl[b].penN = 0; }
 }
 
+// Results post-processing (buildResults, solver_cpu.js:878-898): the moment at a node is its joint's (M of the two
+// segments' joint), replaced in Mx, My by its clamp's where it has one; a segment takes the mean of its end nodes, and
+// the value of the other end where one end has no joint (Mx, My: no joint or clamp)
+template <int P>
+__device__ __forceinline__ typename Dev<P>::R nodeMoment(const Dev<P> &d, int i, int k) {
+  using R = typename Dev<P>::R;
+  const int jn = d.nodeJoint[i], cl = d.nodeClamp[i];
+  if (k < 2 && cl >= 0) return d.cM[size_t(k) * d.ctot + cl];
+  return jn >= 0 ? d.Mj[size_t(k) * d.ptot + jn] : R(0);
+}
+template <int P>
+__global__ void __launch_bounds__(256) k_segResults(Dev<P> d, const InstDesc *__restrict__ insts, int b) {
+  const InstDesc &I = insts[b];
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < I.m; e += gridDim.x * blockDim.x) {
+    const int j = I.m0 + e, a = d.segI0[j], c = d.segI1[j];
+    const bool a0 = d.nodeJoint[a] >= 0, c0 = d.nodeJoint[c] >= 0;
+    const bool aB = a0 || d.nodeClamp[a] >= 0, cB = c0 || d.nodeClamp[c] >= 0;
+    for (int k = 0; k < 3; k++) {
+      const bool ha = k < 2 ? aB : a0, hc = k < 2 ? cB : c0;
+      const auto ma = nodeMoment<P>(d, a, k), mc = nodeMoment<P>(d, c, k);
+      auto v = decltype(ma)(0.5) * (ma + mc);
+      if (!ha) v = mc;
+      if (!hc) v = ma;
+      d.segM[size_t(k) * d.mtot + j] = v;
+    }
+  }
+}
+// the segment layers Mx My T N at the nodes (fields.js nodeValues): the mean of a node's two segments along its strand
+// (a closed strand wraps), the one segment at a strand's end
+template <int P>
+__global__ void __launch_bounds__(256) k_nodeResults(Dev<P> d, const InstDesc *__restrict__ insts, int b) {
+  using R = typename Dev<P>::R;
+  const InstDesc &I = insts[b];
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < I.n; e += gridDim.x * blockDim.x) {
+    const int i = I.n0 + e, si = d.nsIn[i], so = d.nsOut[i];
+    for (int L = 0; L < 4; L++) {
+      auto A = [&](int j) { return L < 3 ? d.segM[size_t(L) * d.mtot + j] : d.Nax[j]; };
+      R v = R(0);
+      if (si >= 0 && so >= 0) v = R(0.5) * (A(si) + A(so));
+      else if (si >= 0) v = A(si);
+      else if (so >= 0) v = A(so);
+      d.nodeLay[size_t(L) * d.ntot + i] = v;
+    }
+  }
+}
+
 // Download: the requested fields of instance b, interleaved per element as the caller's arrays are (f64, or bytes for
 // the stick / slip flags), packed one after another into `out` for a single copy to the host.
 template <int P>
@@ -725,7 +771,10 @@ __global__ void __launch_bounds__(256) k_pack(Dev<P> d, const InstDesc *__restri
         case PF_RSLIP: od[e] = double(d.rotSlip[I.k0 + i]); break;
         case PF_UTM: od[e] = d.utmOut[size_t(I.utmIdx) * 4 * WS_PROTOCOL_MAX_INC + e]; break;
         case PF_FLF: od[e] = double(d.flF[size_t(k) * d.ntot + I.n0 + i]); break;
-        default: ob[e] = d.flState[I.n0 + i]; break;
+        case PF_FLS: ob[e] = d.flState[I.n0 + i]; break;
+        case PF_SEGM: od[e] = double(d.segM[size_t(k) * d.mtot + I.m0 + i]); break;
+        case PF_NODEM: od[e] = double(d.nodeLay[size_t(k) * d.ntot + I.n0 + i]); break;
+        default: od[e] = double(Acc<P>::xw(d, c.cur, k, I.n0 + i)) - double(d.X0[size_t(k) * d.ntot + I.n0 + i]); break;
       }
     }
   }
@@ -744,6 +793,12 @@ cudaError_t launchUnpack(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, i
     if (shortSides) k_rankOrder<P, true><<<rb, 256, 0, st>>>(d, insts, ctl, b);
     else k_rankOrder<P, false><<<rb, 256, 0, st>>>(d, insts, ctl, b);
   }
+  return cudaGetLastError();
+}
+template <int P>
+cudaError_t launchResults(const Dev<P> &d, const InstDesc *insts, int b, int n, int m, cudaStream_t st) {
+  if (m > 0) k_segResults<P><<<std::max(1, std::min((m + 255) / 256, 148 * 8)), 256, 0, st>>>(d, insts, b);
+  if (n > 0) k_nodeResults<P><<<std::max(1, std::min((n + 255) / 256, 148 * 8)), 256, 0, st>>>(d, insts, b);
   return cudaGetLastError();
 }
 template <int P>
@@ -912,6 +967,7 @@ int gridBlocks(bool shortSides, bool ext) {
                                      unsigned char *, cudaStream_t);                                                 \
   template cudaError_t launchClassify<P>(const Dev<P> &, const InstDesc *, int, int, cudaStream_t);                \
   template cudaError_t launchAlFlush<P>(const Dev<P> &, const InstDesc *, InstCtl *, int, cudaStream_t);           \
+  template cudaError_t launchResults<P>(const Dev<P> &, const InstDesc *, int, int, int, cudaStream_t);             \
   template cudaError_t residentPrepare<P>(size_t, bool, size_t *);                                                   \
   template cudaError_t launchResident<P>(const Dev<P> &, const InstDesc *, InstCtl *, const int *, int, int, const uint8_t *, \
                                          int, size_t, bool, bool, cudaStream_t);

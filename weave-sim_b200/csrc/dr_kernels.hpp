@@ -35,9 +35,12 @@ cudaError_t residentPrepare(size_t bytes, bool shortSides, size_t *granted);
 // host <-> device transfers of one instance's state (interleaved per element, as the C ABI's arrays are)
 enum { PF_X, PF_Q, PF_V, PF_W, PF_U, PF_NPREV, PF_SLIP, PF_FN, PF_FT, PF_GAP, PF_N, PF_VSH, PF_M, PF_REACT, PF_STUCK, PF_STATE,
        PF_CTYPE, PF_THETA, PF_PHI, PF_AREA, PF_PRES, PF_UTIL, PF_LAM, PF_DENT, PF_MROT, PF_RSLIP, PF_UTM,
-       PF_FLF, PF_FLS };
+       PF_FLF, PF_FLS, PF_SEGM, PF_NODEM, PF_DISP };
 struct PackField { int kind, count, ncomp; long long off; };   // off: byte offset in the packed buffer
-struct PackList { PackField f[32]; int nf; };
+struct PackList { PackField f[36]; int nf; };
+// the results post-processing of instance b into the device output arrays: segment moments, then the node layers
+template <int P>
+cudaError_t launchResults(const Dev<P> &d, const InstDesc *insts, int b, int n, int m, cudaStream_t st);
 // the multiplier update of instance b that fell due at the end of its last iteration, applied now
 template <int P>
 cudaError_t launchAlFlush(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, int b, cudaStream_t st);

@@ -28,7 +28,7 @@ def device_count() -> int:
 
 STATE_FIELDS = ("X", "Q", "V", "W", "u", "nprev", "slip", "Fn", "Ft", "gap", "N", "Vsh", "M", "reactions", "stuck", "state",
                 "ctype", "theta", "phi", "area", "pressure", "util", "lambda", "dent", "M_rot", "rot_slip", "utm", "floor_F",
-                "floor_state")
+                "floor_state", "seg_M", "node_M", "disp")
 
 
 def _state_buffers(md, fields=None):
@@ -38,7 +38,7 @@ def _state_buffers(md, fields=None):
             "gap": K, "N": m, "Vsh": 2 * m, "M": 3 * p, "reactions": 3 * n, "stuck": K, "state": K,
             "ctype": K, "theta": K, "phi": 2 * K, "area": K, "pressure": K, "util": K,
             "lambda": K, "dent": K, "M_rot": K, "rot_slip": K, "utm": 4 * PROTOCOL_MAX_INC, "floor_F": 3 * n,
-            "floor_state": n}
+            "floor_state": n, "seg_M": 3 * m, "node_M": 4 * n, "disp": 3 * n}
     names = STATE_FIELDS if fields is None else tuple(fields)
     bad = [k for k in names if k not in size]
     if bad:
