@@ -192,6 +192,42 @@ typedef struct ws_kagome_cfg {
 
 typedef struct ws_scene ws_scene;   /* owns the arrays of one ws_model */
 
+/* A scene from a triangle mesh: the scene.json path of the reference (Scene.fromJSON, web/js/scene.js:142-190;
+ * Mesh.fromBytes, mesh.js:23-31; buildTopology, topology.js; Anchors / Loads / strandStiffness, model.js:112-252), with
+ * the file reading, the vertex weld and the unit conversions done by the caller (weave-sim_b200/scenefile.py). */
+enum { WS_SEL_FRAME = 0, WS_SEL_ALL_START = 1, WS_SEL_ALL_END = 2, WS_SEL_ALL_ENDS = 3, WS_SEL_STRAND = 4, WS_SEL_BOUNDARY = 5 };
+typedef struct ws_mesh_cfg {
+  int32_t n_vertices, n_faces;
+  const double *vertices;      /* [3 n_vertices] welded and scaled (Mesh.fromBytes) */
+  const int32_t *faces;        /* [3 n_faces] consistently oriented triangles */
+  int32_t subdivisions;        /* weave.subdivisions */
+  int32_t half_height;         /* weave.offset_mode == 'half_height' */
+  int32_t seed_strand_phase;   /* weave.seed_strand_phase */
+  int32_t n_flips;
+  const int32_t *flips;        /* [2 n_flips] weave.flip_knots (strand, knot) */
+  double overhang;             /* weave.overhang; without it the boundary crossings carry no contact */
+  double width, height;        /* section */
+  double EA, EIx, EIy, GJ, GA; /* section stiffness times the beam factors (sectionStiffness × beamFactors) */
+  double activation[3];        /* prestress shares (flat, edge, twist): rest curvature (1 − a) × the as-built one */
+  double line_weight;          /* self-weight per length in scene units (UnitSystem.selfWeightLineLoad); 0: none */
+  double gravity_dir[3];
+  int32_t udl_on, pad0;
+  double udl[3];               /* loads.udl per length, on the nodes' tributary lengths */
+  double mu;                   /* contact.mu */
+  double fc90, E90, H;         /* material across the grain */
+  int32_t n_anchors, pad1;
+  const int32_t *anchor_kind;  /* WS_SEL_* per selector, in the scene's order */
+  const int32_t *anchor_id;    /* [2 n_anchors] (strand, knot) of a frame, the strand of WS_SEL_STRAND */
+  const uint8_t *anchor_mask;  /* [n_anchors] bit k fixes DOF k of [X Y Z rX rY rZ] */
+  int32_t n_loads, pad2;
+  const int32_t *load_frames;  /* [2 n_loads] */
+  const double *load_F;        /* [3 n_loads] */
+  const uint8_t *load_local;   /* [n_loads] 1: in the node frame */
+  ws_params params;
+} ws_mesh_cfg;
+int ws_scene_mesh(const ws_mesh_cfg *cfg, ws_scene **out);
+
+
 /* defaults: params.js:8-23 converted to SI (strength 1e4 N/mm = 1e7 N/m, epsilon 15 mm) */
 void ws_params_default(ws_params *out);
 int ws_scene_kagome(const ws_kagome_cfg *cfg, ws_scene **out);

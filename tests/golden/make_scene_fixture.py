@@ -1,0 +1,33 @@
+"""Makes the scene fixture of the reference's example scene examples/scenes/dome_basic.json: its parameters
+(dome_basic_scene.json, the mesh path pointed at the welded mesh below) and its mesh, read, scaled and welded as the
+reference reads it (dome_basic_mesh.npz: V [3 nV], F [3 nF]).  Run from the repository root where the reference
+checkout is present:  python tests/golden/make_scene_fixture.py /path/to/reference
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+import weavesim_b200 as ws  # noqa: E402
+from weavesim_b200 import scenefile  # noqa: E402
+
+
+def main(ref):
+    src = os.path.join(ref, "examples", "scenes", "dome_basic.json")
+    with open(src) as f:
+        d = json.load(f)
+    mesh = d["mesh"]
+    V, F = scenefile.read_mesh(os.path.join(os.path.dirname(src), mesh["path"]), float(mesh.get("scale", 1.0)))
+    np.savez_compressed(os.path.join(HERE, "dome_basic_mesh.npz"), V=V, F=F)
+    d["mesh"] = {"path": "dome_basic_mesh.npz", "scale": 1.0}
+    with open(os.path.join(HERE, "dome_basic_scene.json"), "w") as f:
+        json.dump(d, f, indent=1)
+    md = ws.load_scene(os.path.join(HERE, "dome_basic_scene.json"))
+    print(f"dome_basic: {len(V) // 3} vertices, {len(F) // 3} faces -> n {md.n}, m {md.m}, K {md.K}")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -728,3 +728,22 @@ def test_results_match_oracle(oracle_mod, name, form):
     g2 = s.download(0, fields=("disp",))
     s.dispose()
     assert np.abs(g2["disp"]).max() == 0.0
+
+
+# ---------------------------------------------------------------------------------------------- a reference scene
+def test_reference_scene_matches_oracle(oracle_mod):
+    """the reference's example scene dome_basic (read by the scene.json reader from its committed fixture):
+    1000 iterations on the device against the oracle, batched and plain"""
+    import os
+    md = ws.load_scene(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "dome_basic_scene.json"))
+    o = oracle_mod.Oracle(md.copy())
+    o.step(1000)
+    v = o.view()
+    for form in ("cta", "plain"):
+        s = ws.GpuSolver([md.copy()], precision="f64", form=form)
+        ctl = s.step(1000)[0]
+        g = s.download(0, fields=("X", "Fn", "stuck"))
+        s.dispose()
+        assert ctl["iter"] == 1000 and ctl["rollbacks"] == v["rollbacks"]
+        assert cases.max_rel_disp_error(g["X"], v["X"], v["X0"]) < 1e-9
+        assert np.array_equal(g["stuck"], v["stuck"])

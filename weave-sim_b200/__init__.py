@@ -5,5 +5,6 @@ damping) runs as hand-written sm_100a CUDA behind the C ABI of include/weavesim.
 of the reference's solver interface (web/js/solver_gpu.js GpuSolver) over that ABI.
 """
 from ._lib import Model, default_params, kagome, polylines, mask, lib, last_error  # noqa: F401
+from .scenefile import load_scene  # noqa: F401
 from . import configs  # noqa: F401
 from .solver import GpuSolver, device_count  # noqa: F401,E402

@@ -46,6 +46,15 @@ int ws_scene_kagome(const ws_kagome_cfg *cfg, ws_scene **out) {
   } catch (const std::exception &e) { return wsb::fail(WS_ERR_ARG, std::string("ws_scene_kagome: ") + e.what()); }
 }
 
+int ws_scene_mesh(const ws_mesh_cfg *cfg, ws_scene **out) {
+  if (!cfg || !out) return wsb::fail(WS_ERR_ARG, "ws_scene_mesh: null argument");
+  try {
+    wsb::Scene *sc = wsb::buildMeshScene(*cfg);
+    *out = new ws_scene{sc};
+    return WS_OK;
+  } catch (const std::exception &e) { return wsb::fail(WS_ERR_ARG, std::string("ws_scene_mesh: ") + e.what()); }
+}
+
 int ws_scene_polylines(const ws_polyline_cfg *cfg, ws_scene **out) {
   if (!cfg || !out) return wsb::fail(WS_ERR_ARG, "ws_scene_polylines: null argument");
   try {

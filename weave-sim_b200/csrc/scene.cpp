@@ -754,6 +754,105 @@ Scene *buildKagome(const ws_kagome_cfg &cfg) {
   return sc.release();
 }
 
+// rotation vector log(q_a* ⊗ q_b) of two unit quaternions, the short way round (relRotation, rod_cosserat.js:33-45)
+static void relRotationVec(const double *qa, const double *qb, double out[3]) {
+  const double aw = qa[0], ax = -qa[1], ay = -qa[2], az = -qa[3];
+  const double bw = qb[0], bx = qb[1], by = qb[2], bz = qb[3];
+  double w = aw * bw - ax * bx - ay * by - az * bz, x = aw * bx + ax * bw + ay * bz - az * by;
+  double y = aw * by - ax * bz + ay * bw + az * bx, z = aw * bz + ax * by - ay * bx + az * bw;
+  if (w < 0) { w = -w; x = -x; y = -y; z = -z; }
+  const double s = std::sqrt(x * x + y * y + z * z), th = 2 * std::atan2(s, w);
+  const double f = s > 1e-12 ? th / s : 2 / std::max(w, 1e-12);
+  out[0] = f * x; out[1] = f * y; out[2] = f * z;
+}
+
+// a scene from a triangle mesh and the parameters of a scene.json (Scene.fromJSON + CpuSolver set-up, scene.js:142-190,
+// model.js:112-252): the topology of the mesh, uniform section and material, selectors resolved to frames, loads
+Scene *buildMeshScene(const ws_mesh_cfg &cfg) {
+  if (cfg.n_vertices < 3 || cfg.n_faces < 1 || !cfg.vertices || !cfg.faces) throw std::invalid_argument("mesh: no triangles");
+  if (cfg.subdivisions < 1 || !(cfg.width > 0) || !(cfg.height > 0)) throw std::invalid_argument("mesh: subdivisions and section must be positive");
+  for (int i = 0; i < 3 * cfg.n_faces; i++)
+    if (cfg.faces[i] < 0 || cfg.faces[i] >= cfg.n_vertices) throw std::invalid_argument("mesh: face vertex out of range");
+  auto sc = std::make_unique<Scene>();
+  sc->mesh = Mesh::fromArrays(std::vector<double>(cfg.vertices, cfg.vertices + 3 * size_t(cfg.n_vertices)),
+                              std::vector<int>(cfg.faces, cfg.faces + 3 * size_t(cfg.n_faces)));
+  WeaveParams wp;
+  wp.subdivisions = cfg.subdivisions; wp.overhang = cfg.overhang; wp.half_height = cfg.half_height != 0;
+  wp.seed_strand_phase = cfg.seed_strand_phase;
+  for (int f = 0; f < cfg.n_flips; f++) wp.flip_knots.push_back({cfg.flips[2 * f], cfg.flips[2 * f + 1]});
+  sc->topo = buildTopology(sc->mesh, wp, cfg.height);
+  sc->st = buildState(sc->topo);
+  State &st = sc->st;
+  sc->params = cfg.params;
+  // uniform section and material (strandStiffness with one lath group)
+  sc->EA.assign(st.m, cfg.EA); sc->EIx.assign(st.m, cfg.EIx); sc->EIy.assign(st.m, cfg.EIy); sc->GJ.assign(st.m, cfg.GJ);
+  sc->GA.assign(st.m, cfg.GA);
+  sc->wk.assign(2 * size_t(st.K), cfg.width); sc->hk.assign(2 * size_t(st.K), cfg.height);
+  sc->fc90.assign(2 * size_t(st.K), cfg.fc90); sc->E90.assign(2 * size_t(st.K), cfg.E90); sc->H.assign(2 * size_t(st.K), cfg.H);
+  sc->nodeW.assign(st.n, cfg.width); sc->nodeH.assign(st.n, cfg.height);
+  // rest curvature: the unprestressed share of the as-built curvature (CosseratRod constructor, rod_cosserat.js:58-66)
+  if (cfg.activation[0] < 1 || cfg.activation[1] < 1 || cfg.activation[2] < 1) {
+    sc->omega0.assign(3 * size_t(st.p), 0.0);
+    for (int j = 0; j < st.p; j++) {
+      double psi[3];
+      relRotationVec(&st.Q[4 * size_t(st.jSeg0[j])], &st.Q[4 * size_t(st.jSeg1[j])], psi);
+      for (int k = 0; k < 3; k++) {
+        const double a = std::min(std::max(cfg.activation[k], 0.0), 1.0);
+        sc->omega0[3 * size_t(j) + k] = (1.0 - a) * (psi[k] / st.jLen[j]);
+      }
+    }
+  }
+  // loads (Loads, model.js:191-231): self-weight per segment half to each end node, udl on the tributary lengths,
+  // point loads at frames
+  sc->loadConst.assign(3 * size_t(st.n), 0.0);
+  if (cfg.line_weight != 0) {
+    double g[3] = {cfg.gravity_dir[0], cfg.gravity_dir[1], cfg.gravity_dir[2]};
+    const double gl = std::max(std::sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]), 1e-12);
+    for (double &v : g) v /= gl;
+    for (int j = 0; j < st.m; j++) {
+      const double q = 0.5 * st.l0[j] * cfg.line_weight;
+      for (int i : {st.segI0[j], st.segI1[j]})
+        for (int c = 0; c < 3; c++) sc->loadConst[3 * size_t(i) + c] += q * g[c];
+    }
+  }
+  if (cfg.udl_on) {
+    std::vector<double> trib(st.n, 0.0);
+    for (int j = 0; j < st.m; j++) trib[st.segI0[j]] += 0.5 * st.l0[j];
+    for (int j = 0; j < st.m; j++) trib[st.segI1[j]] += 0.5 * st.l0[j];
+    for (int i = 0; i < st.n; i++) for (int c = 0; c < 3; c++) sc->loadConst[3 * size_t(i) + c] += trib[i] * cfg.udl[c];
+  }
+  for (int l = 0; l < cfg.n_loads; l++)
+    sc->addPointLoad(cfg.load_frames[2 * l], cfg.load_frames[2 * l + 1], &cfg.load_F[3 * l], cfg.load_local && cfg.load_local[l]);
+  // anchors: selectors to frames (resolveSelector / anchorMasks, model.js:114-159)
+  for (int a = 0; a < cfg.n_anchors; a++) {
+    std::vector<std::pair<int, int>> fr;
+    const int kind = cfg.anchor_kind[a], s = cfg.anchor_id[2 * a], k = cfg.anchor_id[2 * a + 1];
+    switch (kind) {
+      case WS_SEL_FRAME: fr.push_back({s, k}); break;
+      case WS_SEL_ALL_START: case WS_SEL_ALL_END: case WS_SEL_ALL_ENDS:
+        if (kind != WS_SEL_ALL_END) for (const Strand &t : sc->topo.strands) if (!t.closed) fr.push_back({t.index, 0});
+        if (kind != WS_SEL_ALL_START) for (const Strand &t : sc->topo.strands) if (!t.closed) fr.push_back({t.index, int(t.edges.size()) - 1});
+        break;
+      case WS_SEL_STRAND:
+        if (s < 0 || s >= int(sc->topo.strands.size())) throw std::invalid_argument("mesh: anchor strand out of range");
+        for (size_t q = 0; q < sc->topo.strands[s].edges.size(); q++) fr.push_back({s, int(q)});
+        break;
+      case WS_SEL_BOUNDARY:
+        for (const Knot &kn : sc->topo.knots) if (kn.isBoundary) { fr.push_back({kn.a.s, kn.a.k}); fr.push_back({kn.b.s, kn.b.k}); }
+        break;
+      default: throw std::invalid_argument("mesh: unknown anchor selector");
+    }
+    sc->addAnchorFrames(fr, cfg.anchor_mask[a]);
+  }
+  // crossings: without overhang the boundary knots carry no contact (solver_cpu.js:83); one μ
+  sc->enabled.assign(st.K, 1);
+  if (cfg.overhang <= 0) for (int c = 0; c < st.K; c++) if (st.crossBoundary[c]) sc->enabled[c] = 0;
+  sc->locked.assign(st.K, 0);            // contact.locked: the caller sets cross_locked
+  sc->mu.assign(st.K, cfg.mu);
+  sc->fillModel();
+  return sc.release();
+}
+
 Scene *buildPolylineScene(const ws_polyline_cfg &cfg) {
   if (cfg.n_strands < 1 || !cfg.node_count || !cfg.points) throw std::invalid_argument("polylines: no strands");
   auto sc = std::make_unique<Scene>();

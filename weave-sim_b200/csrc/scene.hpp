@@ -106,6 +106,7 @@ struct Scene {
 
 Scene *buildKagome(const ws_kagome_cfg &cfg);
 Scene *buildPolylineScene(const ws_polyline_cfg &cfg);
+Scene *buildMeshScene(const ws_mesh_cfg &cfg);
 
 }  // namespace wsb
 
