@@ -6,7 +6,7 @@ FP32 element math with two-float positions/frames and FP64 reductions.  A step i
 DR iterations per second of the whole job (all ranks).  Between timed steps a 256 MiB buffer is written to flush L2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--chunk C] [--impl ours|reference]
-    python bench.py --workload precision|batch|serve|ratio   (one JSON line each; weave-sim_b200/workloads.py)
+    python bench.py --workload precision|batch|serve|ratio|scene   (one JSON line each; weave-sim_b200/workloads.py)
 
 --impl reference runs the reference's CPU algorithm (the f64 restatement under oracle/, the reference's JS being
 unrunnable without a JS engine) on the host cores: one replica of the workload per thread, a bounded sample of
@@ -214,6 +214,19 @@ def cpu_replicas(iters_per_replica, threads):
     return threads * iters_per_replica / dt, dt
 
 
+def cpu_scene(path):
+    """CPU baseline leg of the scene workload: the reference's CPU algorithm (oracle/, f64) relaxing the scene on one
+    thread to convergence or its cap; returns (seconds, iterations)"""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import weavesim_b200 as ws
+    from oracle import Oracle
+    md = ws.load_scene(path)
+    o = Oracle(md.copy())
+    t0 = time.perf_counter()
+    v = o.run(int(md.params["max_iter"]), chunk=500)
+    return time.perf_counter() - t0, int(v["iteration"])
+
+
 def cpu_dome(iters, threads=0):
     """CPU baseline leg of the ratio workload: the reference's CPU algorithm (oracle/, f64) on the 3 m dome, one thread
     alone and one replica per host thread; returns (1-thread iters/s, all-thread instance iters/s, threads)"""
@@ -276,6 +289,14 @@ def run_workload(args):
                      cpu_port_all_threads_inst_iters_per_s=cpuN, batched_over_cpu_all_threads=r["batched_inst_iters_per_s"] / cpuN,
                      batched_over_cpu_1_thread=r["batched_inst_iters_per_s"] / cpu1)
             metric = "batched vs plain single-instance GPU form vs the CPU port, DR iters/s on the 3 m dome"
+        elif args.workload == "scene":
+            path = os.path.join(ROOT, "tests", "golden", "dome_basic_scene.json")
+            r = workloads.run_scene(path)
+            cpu_s, cpu_it = cpu_scene(path)
+            r.update(cpu_port_1_thread_solve_s=cpu_s, cpu_port_iterations=cpu_it,
+                     f64_plain_over_cpu=cpu_s / (r["f64_plain"]["gpu_ms"] * 1e-3),
+                     mixed_plain_over_cpu=cpu_s / (r["mixed_plain"]["gpu_ms"] * 1e-3))
+            metric = "time to relax the reference's example scene dome_basic: GPU forms and precisions vs the CPU port"
         else:
             r = workloads.run_serve()
             metric = "p50/p99/p99.9 solve latency and solves/s under Poisson arrivals"
@@ -295,7 +316,8 @@ def main():
     ap.add_argument("--form", default="plain", choices=["plain", "grid", "cta"])
     ap.add_argument("--ref-iters", type=int, default=10, help="DR iterations per replica per step of the CPU arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="shell_large", choices=["shell_large", "precision", "batch", "serve", "ratio"],
+    ap.add_argument("--workload", default="shell_large",
+                    choices=["shell_large", "precision", "batch", "serve", "ratio", "scene"],
                     help="shell_large: the headline line; the others measure the stiff-dome precision variants, the "
                          "512-gridshell mixed batch and the serving loop (single GPU)")
     ap.add_argument("--instances", type=int, default=0, help="instances of the precision / batch workloads")

@@ -182,6 +182,33 @@ def test_large_shell_plain_against_oracle(oracle_mod):
         assert cases.max_node_err_span(g["X"], v["X"], md.span) < tol
 
 
+# The plain form's launch modes (WEAVESIM_PLAIN_LAUNCH, read when a context is made): each split phase as two kernels on
+# forked graph branches (the default), as one launch whose blocks take the two roles, or as one kernel a phase.  The
+# block partials are reduced in a different grouping in each, so the modes agree with the oracle, not bit for bit.
+
+@pytest.fixture(scope="module")
+def shell_large_330(oracle_mod):
+    md = ws.configs.shell_large()
+    o = oracle_mod.Oracle(md.copy())
+    o.step(330)
+    return md, o.view()
+
+
+@pytest.mark.parametrize("mode", ["fork", "roles", "serial"])
+@pytest.mark.parametrize("prec,tol", [("f64", 1e-9), ("mixed", 1e-5)])
+@pytest.mark.parametrize("order", ["auto", "general"])
+def test_plain_launch_modes_against_oracle(shell_large_330, monkeypatch, mode, prec, tol, order):
+    md, v = shell_large_330
+    monkeypatch.setenv("WEAVESIM_PLAIN_LAUNCH", mode)
+    s = ws.GpuSolver([md.copy()], precision=prec, form="plain", side_order=order)
+    ctl = s.step(330)[0]
+    g = s.download(0, fields=("X", "u"))
+    s.dispose()
+    assert ctl["iter"] == 330
+    assert cases.max_node_err_span(g["X"], v["X"], md.span) < tol
+    assert np.abs(g["u"] - v["u"]).max() < (1e-9 if prec == "f64" else 1e-4)
+
+
 # ------------------------------------------------------------------------------------------------ side orders
 # The crossing sides are kept sorted along their strands for the conflict-free gathers.  With the slide limit under half
 # the shortest segment (every scene above) a side moves at most one segment per iteration and the order is ranked

@@ -2,6 +2,7 @@
 // every instance (for warm starts and downloads), a CUDA stream and the graph of the plain form.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <functional>
@@ -147,7 +148,9 @@ struct ws_ctx {
   cudaGraphExec_t graph = nullptr;
   int graphIters = 0, graphKey = -1, graphLaunches = 0;
   PlainFork fork{};              // plain form: the crossing kernel's stream and the fork / join events
+  bool plainRoles = false;       // plain form: each split phase as one launch with block roles instead of the fork
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t evChunk[8] = {};   // pipelined downloads: one per chunk of the device-to-host copy
   double lastMs = 0;
   int64_t lastLaunches = 0;
   std::vector<InstCtl> ctlHost;
@@ -162,6 +165,28 @@ struct ws_ctx {
 };
 
 namespace {
+
+// A transfer through the pinned staging buffer in chunks, so that the host's copy of one chunk overlaps the DMA of
+// another (one core's memcpy, about 15 GB/s, takes longer than the PCIe copy).  A piece is a caller's array and its
+// byte offset in the staging buffer.
+struct Piece { char *user; size_t off, bytes; };
+constexpr int kChunks = 8;
+constexpr size_t kChunkMin = 512 * 1024;
+
+int chunkCount(size_t bytes) { return int(std::max<size_t>(1, std::min<size_t>(kChunks, bytes / kChunkMin))); }
+size_t chunkEdge(size_t bytes, int nc, int k) {
+  const size_t step = ((bytes + nc - 1) / nc + 15) & ~size_t(15);
+  return std::min(bytes, step * size_t(k));
+}
+// copies the parts of the pieces inside staging bytes [lo, hi): into the staging buffer (toStage) or out of it
+void copyRange(const std::vector<Piece> &ps, char *stage, size_t lo, size_t hi, bool toStage) {
+  for (const Piece &q : ps) {
+    const size_t a = std::max(lo, q.off), e = std::min(hi, q.off + q.bytes);
+    if (a >= e) continue;
+    if (toStage) std::memcpy(stage + a, q.user + (a - q.off), e - a);
+    else std::memcpy(q.user + (a - q.off), stage + a, e - a);
+  }
+}
 
 char *stageBuf(ws_ctx *c, size_t bytes) {
   if (!c->pinnedOK) {
@@ -627,6 +652,16 @@ bool anyExt(const ws_ctx *c) {
 #define WSB_PLAIN_FORK 1     // the plain form's element phase as two kernels on forked branches (0: one kernel)
 #endif
 const PlainFork *plainFork(const ws_ctx *c) { return (WSB_PLAIN_FORK && c->fork.side) ? &c->fork : nullptr; }
+// how the plain form launches its split phases, from WEAVESIM_PLAIN_LAUNCH: "roles" (one launch a phase, blocks in two
+// roles), "fork" (two kernels on forked graph branches), "serial" (one kernel a phase); default fork
+bool plainRolesFromEnv() {
+  const char *v = std::getenv("WEAVESIM_PLAIN_LAUNCH");
+  return v && std::strcmp(v, "roles") == 0;
+}
+const PlainFork *plainForkFromEnv(const ws_ctx *c) {
+  const char *v = std::getenv("WEAVESIM_PLAIN_LAUNCH");
+  return (v && std::strcmp(v, "serial") == 0) ? nullptr : plainFork(c);
+}
 
 template <int P>
 void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
@@ -664,7 +699,8 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
       CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
       int nl = 0;
       for (int i = 0; i < chunk; i++)
-        CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, ext, c->st, &nl, c->dBar + 2, plainFork(c)));
+        CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, ext, c->st, &nl, c->dBar + 2,
+                              plainForkFromEnv(c), c->plainRoles));
       CK(cudaStreamEndCapture(c->st, &gr));
       CK(cudaGraphInstantiate(&c->graph, gr, 0));
       cudaGraphDestroy(gr);
@@ -676,7 +712,8 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
     while (nIter - done >= chunk && chunk > 0) { CK(cudaGraphLaunch(c->graph, c->st)); done += chunk; c->lastLaunches += c->graphLaunches; }
     int nl = 0;
     for (; done < nIter; done++)
-      CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, ext, c->st, &nl, c->dBar + 2, plainFork(c)));
+      CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, ext, c->st, &nl, c->dBar + 2,
+                            plainForkFromEnv(c), c->plainRoles));
     c->lastLaunches += nl;
   }
   CK(cudaEventRecord(c->ev1, c->st));
@@ -729,9 +766,18 @@ void downloadPacked(ws_ctx *c, int b, ws_state_out *o) {
   unsigned char *dv = xferBuf(c, off);
   CK(launchPack<P>(devOf<P>(c), c->dInst, c->dCtl, b, L, elems, dv, c->st));
   char *h = stageBuf(c, off);
-  CK(cudaMemcpyAsync(h, dv, off, cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
-  for (const Dst &q : dst) std::memcpy(q.p, h + q.off, q.bytes);
+  std::vector<Piece> ps;
+  for (const Dst &q : dst) ps.push_back({static_cast<char *>(q.p), q.off, q.bytes});
+  const int nc = chunkCount(off);
+  for (int k = 0; k < nc; k++) {
+    const size_t a = chunkEdge(off, nc, k), e = chunkEdge(off, nc, k + 1);
+    if (e > a) CK(cudaMemcpyAsync(h + a, dv + a, e - a, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaEventRecord(c->evChunk[k], c->st));
+  }
+  for (int k = 0; k < nc; k++) {
+    CK(cudaEventSynchronize(c->evChunk[k]));
+    copyRange(ps, h, chunkEdge(off, nc, k), chunkEdge(off, nc, k + 1), false);
+  }
 }
 
 template <int P>
@@ -920,11 +966,16 @@ void uploadStatePacked(ws_ctx *c, int b, const double *X, const double *Q, const
   const size_t nX = 3 * size_t(I.n), nQ = 4 * size_t(I.m), nU = (u && I.K) ? 2 * size_t(I.K) : 0;
   const size_t bytes = (nX + nQ + nU) * sizeof(double);
   char *h = stageBuf(c, bytes);
-  std::memcpy(h, X, nX * sizeof(double));
-  std::memcpy(h + nX * sizeof(double), Q, nQ * sizeof(double));
-  if (nU) std::memcpy(h + (nX + nQ) * sizeof(double), u, nU * sizeof(double));
   unsigned char *dv = xferBuf(c, bytes);
-  CK(cudaMemcpyAsync(dv, h, bytes, cudaMemcpyHostToDevice, c->st));
+  const std::vector<Piece> ps = {{(char *)X, 0, nX * sizeof(double)}, {(char *)Q, nX * sizeof(double), nQ * sizeof(double)},
+                                 {(char *)u, (nX + nQ) * sizeof(double), nU * sizeof(double)}};
+  const int nc = chunkCount(bytes);
+  for (int k = 0; k < nc; k++) {
+    const size_t a = chunkEdge(bytes, nc, k), e = chunkEdge(bytes, nc, k + 1);
+    if (e <= a) continue;
+    copyRange(ps, h, a, e, true);
+    CK(cudaMemcpyAsync(dv + a, h + a, e - a, cudaMemcpyHostToDevice, c->st));
+  }
   CK(launchUnpack<P>(devOf<P>(c), c->dInst, c->dCtl, b, reinterpret_cast<const double *>(dv), I.n, I.m, I.K, nU > 0, true,
                      c->shortSides, c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -1004,6 +1055,8 @@ void destroyCtx(ws_ctx *c) {
   if (c->dErr) cudaFree(c->dErr);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  for (cudaEvent_t e : c->evChunk)
+    if (e) cudaEventDestroy(e);
   if (c->st) cudaStreamDestroy(c->st);
   if (c->fork.side) cudaStreamDestroy(c->fork.side);
   if (c->fork.fork) cudaEventDestroy(c->fork.fork);
@@ -1049,10 +1102,12 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
       CK(cudaEventCreateWithFlags(&c->fork.join, cudaEventDisableTiming));
       CK(cudaEventCreateWithFlags(&c->fork.fork2, cudaEventDisableTiming));
       CK(cudaEventCreateWithFlags(&c->fork.join2, cudaEventDisableTiming));
+      c->plainRoles = plainRolesFromEnv();
     }
     c->pinnedOK = true;
     CK(cudaEventCreate(&c->ev0));
     CK(cudaEventCreate(&c->ev1));
+    for (cudaEvent_t &e : c->evChunk) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     c->g.resize(n_instances);
     Sizes off;
     for (int b = 0; b < n_instances; b++) {
@@ -1088,6 +1143,7 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     c->shape.blocksA = blocks(I0.m + I0.p + I0.C + 2LL * I0.K, 256);
     c->shape.blocksDS = blocks(I0.n + I0.m + 2LL * I0.K, 256);
     c->shape.blocksX = blocks(2LL * I0.K, 128);
+    c->shape.blocksXR = blocks(2LL * I0.K, 256);
     c->shape.blocksY = blocks(I0.m + I0.p + I0.C, 256);
     c->shape.blocksDN = blocks(I0.n, 256);
     c->shape.blocksDNS = blocks(I0.n + 2LL * I0.K, 256);

@@ -398,7 +398,7 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
 // (PART 2), which then run at the occupancy of their own, smaller register budget.
 template <int P, bool SHORT, bool EXT, int PART>
 __device__ __forceinline__ void plainA(const Dev<P> &d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
-                                       typename Dev<P>::A *part, int partStride) {
+                                       typename Dev<P>::A *part, int partStride, int blk, int nblk) {
   using A = typename Dev<P>::A;
   __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
   const InstDesc &I = insts[0];
@@ -410,28 +410,38 @@ __device__ __forceinline__ void plainA(const Dev<P> &d, const InstDesc *__restri
   const StepCtx sx = makeCtx<A>(I, c);
   Part<A> pt;
   pt.init();
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nA; e += gridDim.x * blockDim.x) phaseA<P, SHORT, EXT>(d, I, sx, base + e, nK, pt);
+  for (int e = blk * blockDim.x + threadIdx.x; e < nA; e += nblk * blockDim.x) phaseA<P, SHORT, EXT>(d, I, sx, base + e, nK, pt);
   constexpr unsigned SM = PART == 1 ? SUMS_CROSS : PART == 2 ? SUMS_ROD : (SUMS_CROSS | SUMS_ROD);
   constexpr unsigned XM = PART == 1 ? MAXS_CROSS : PART == 2 ? MAXS_ROD : (MAXS_CROSS | MAXS_ROD);
   blockReduce<SM, XM>(pt, red);
-  if (threadIdx.x == 0) putPart(pt, part, blockIdx.x, partStride);
+  if (threadIdx.x == 0) putPart(pt, part, blk, partStride);
 }
 template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(256, WSB_MINB_A) k_plainA(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
                                                 typename Dev<P>::A *part, int partStride) {
   waitPrevGrid();
   allowNextGrid();
-  plainA<P, SHORT, EXT, 0>(d, insts, ctl, part, partStride);
+  plainA<P, SHORT, EXT, 0>(d, insts, ctl, part, partStride, blockIdx.x, gridDim.x);
 }
 template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(128) k_plainX(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
                                                 typename Dev<P>::A *part, int partStride) {
-  plainA<P, SHORT, EXT, 1>(d, insts, ctl, part, partStride);
+  plainA<P, SHORT, EXT, 1>(d, insts, ctl, part, partStride, blockIdx.x, gridDim.x);
 }
 template <int P, bool SHORT>
 __global__ void __launch_bounds__(256, WSB_MINB_Y) k_plainY(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
                                                 typename Dev<P>::A *part, int partStride) {
-  plainA<P, SHORT, false, 2>(d, insts, ctl, part, partStride);
+  plainA<P, SHORT, false, 2>(d, insts, ctl, part, partStride, blockIdx.x, gridDim.x);
+}
+// The element phase as one launch whose blocks take roles: the first nbX blocks the crossings, the others the segments,
+// joints and clamps, so both run side by side without a fork in the graph; partials at part[block] in that order.
+template <int P, bool SHORT, bool EXT>
+__global__ void __launch_bounds__(256, WSB_MINB_Y) k_plainXY(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
+                                                 typename Dev<P>::A *part, int partStride, int nbX) {
+  waitPrevGrid();
+  allowNextGrid();
+  if (int(blockIdx.x) < nbX) plainA<P, SHORT, EXT, 1>(d, insts, ctl, part, partStride, blockIdx.x, nbX);
+  else plainA<P, SHORT, false, 2>(d, insts, ctl, part + nbX, partStride, blockIdx.x - nbX, gridDim.x - nbX);
 }
 template <int P>
 __global__ void __launch_bounds__(256) k_plainBC(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl) {
@@ -452,7 +462,7 @@ __global__ void __launch_bounds__(256) k_plainBC(Dev<P> d, const InstDesc *__res
 template <int P, bool SHORT, bool EXT, int PART>
 __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                        typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts, int partStride,
-                                       unsigned *counter, unsigned nBlocks) {
+                                       unsigned *counter, unsigned nBlocks, int blk, int nblk) {
   using A = typename Dev<P>::A;
   __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
   __shared__ bool last;
@@ -464,7 +474,7 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
   pt.init();
   const int nR = countD<SHORT>(I) - I.n - I.m;
   const int nD = PART == 1 ? I.n + nR : PART == 2 ? I.m : countD<SHORT>(I);
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nD; e += gridDim.x * blockDim.x) {
+  for (int e = blk * blockDim.x + threadIdx.x; e < nD; e += nblk * blockDim.x) {
     if (PART == 0) phaseD<P, SHORT, EXT>(d, I, sx, e, pt);
     else if (PART == 2) segUpdate<P, SHORT>(d, I, sx, I.m0 + e, pt);
     else if (e < I.n) nodeUpdate<P, SHORT, EXT>(d, I, sx, I.n0 + e, pt);
@@ -475,7 +485,7 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
   constexpr unsigned XM = (PART == 1 ? ((1u << RX_F) | (1u << RX_LOAD)) : PART == 2 ? (1u << RX_T) : MAXS_UPDATE) | XF;
   blockReduce<SM, XM>(pt, red);
   if (threadIdx.x == 0) {
-    putPart(pt, part, blockIdx.x, partStride);
+    putPart(pt, part, blk, partStride);
     __threadfence();
     last = atomicAdd(counter, 1u) == nBlocks - 1;
   }
@@ -500,19 +510,33 @@ __global__ void __launch_bounds__(256, WSB_MINB_D) k_plainD(Dev<P> d, const Inst
                                                 int partStride, unsigned *counter) {
   waitPrevGrid();
   allowNextGrid();
-  plainD<P, SHORT, EXT, 0>(d, insts, ctl, part, partAll, nParts, partStride, counter, gridDim.x);
+  plainD<P, SHORT, EXT, 0>(d, insts, ctl, part, partAll, nParts, partStride, counter, gridDim.x, blockIdx.x, gridDim.x);
 }
 template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(256, WSB_MINB_DN) k_plainDN(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                                   typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts,
                                                   int partStride, unsigned *counter, unsigned nBlocks) {
-  plainD<P, SHORT, EXT, 1>(d, insts, ctl, part, partAll, nParts, partStride, counter, nBlocks);
+  plainD<P, SHORT, EXT, 1>(d, insts, ctl, part, partAll, nParts, partStride, counter, nBlocks, blockIdx.x, gridDim.x);
 }
 template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(256, WSB_MINB_DM) k_plainDM(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                                   typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts,
                                                   int partStride, unsigned *counter, unsigned nBlocks) {
-  plainD<P, SHORT, EXT, 2>(d, insts, ctl, part, partAll, nParts, partStride, counter, nBlocks);
+  plainD<P, SHORT, EXT, 2>(d, insts, ctl, part, partAll, nParts, partStride, counter, nBlocks, blockIdx.x, gridDim.x);
+}
+// The update phase as one launch with roles: the first nbN blocks the nodes (with the side ranks of the short order),
+// the others the segments; the last of all its blocks closes the iteration.
+template <int P, bool SHORT, bool EXT>
+__global__ void __launch_bounds__(256, WSB_MINB_DN) k_plainDNM(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+                                                   typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts,
+                                                   int partStride, unsigned *counter, int nbN) {
+  waitPrevGrid();
+  allowNextGrid();
+  if (int(blockIdx.x) < nbN)
+    plainD<P, SHORT, EXT, 1>(d, insts, ctl, part, partAll, nParts, partStride, counter, gridDim.x, blockIdx.x, nbN);
+  else
+    plainD<P, SHORT, EXT, 2>(d, insts, ctl, part + nbN, partAll, nParts, partStride, counter, gridDim.x, blockIdx.x - nbN,
+                             gridDim.x - nbN);
 }
 
 // ------------------------------------------------------------------------------------------------ grid form
@@ -882,9 +906,30 @@ static cudaError_t launchPDL(void (*k)(KArgs...), int blocks, cudaStream_t st, A
 
 template <int P>
 cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, const PlainShape &sh, bool contacts,
-                            bool shortSides, bool ext, cudaStream_t st, int *launches, unsigned *counter, const PlainFork *fork) {
+                            bool shortSides, bool ext, cudaStream_t st, int *launches, unsigned *counter, const PlainFork *fork,
+                            bool roles) {
   using A = typename Dev<P>::A;
   const bool sh2 = shortSides && contacts;
+  if (roles && contacts) {
+    // two launches with block roles, each scheduled while its predecessor drains (the general order's ranking kernel
+    // between them)
+    const int nbX = sh.blocksXR, nDN = sh2 ? sh.blocksDNS : sh.blocksDN;
+    const int nXY = nbX + sh.blocksY, nParts = nXY + nDN + sh.blocksDM;
+    A *px = static_cast<A *>(part), *pn = px + nXY;
+    cudaError_t e = launchPDL(WSB_PICK(k_plainXY, P, sh2, ext), nXY, st, d, insts, ctl, px, nParts, nbX);
+    if (e != cudaSuccess) return e;
+    int nl = 1;
+    if (!sh2) {
+      if ((e = launchPDL(k_plainBC<P>, sh.blocksR, st, d, insts, ctl)) != cudaSuccess) return e;
+      nl += 1;
+    }
+    e = launchPDL(WSB_PICK(k_plainDNM, P, sh2, ext), nDN + sh.blocksDM, st, d, insts, ctl, pn, px, nParts, nParts, counter,
+                  nDN);
+    if (e != cudaSuccess) return e;
+    nl += 1;
+    if (launches) *launches += nl;
+    return cudaGetLastError();
+  }
   if (fork && contacts) {
     // crossings on a forked branch, segments / joints / clamps on the main one, joined before the update; the update
     // forks again: nodes on the side branch, segments and side ranks on the main one
@@ -957,7 +1002,7 @@ int gridBlocks(bool shortSides, bool ext) {
   template cudaError_t launchBatched<P>(const Dev<P> &, const InstDesc *, InstCtl *, const int *, int, int, const uint8_t *, \
                                         int, int, bool, bool, cudaStream_t);                                         \
   template cudaError_t launchPlainIter<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, const PlainShape &, bool,    \
-                                          bool, bool, cudaStream_t, int *, unsigned *, const PlainFork *);           \
+                                          bool, bool, cudaStream_t, int *, unsigned *, const PlainFork *, bool);     \
   template cudaError_t launchGrid<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, unsigned *, int *, int, int, bool, \
                                      bool, cudaStream_t);                                                            \
   template int gridBlocks<P>(bool, bool);                                                                           \

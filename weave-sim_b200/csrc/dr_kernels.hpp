@@ -7,8 +7,9 @@
 namespace wsb {
 
 // blocks of the plain form's kernels: element phase, general side order, update phase (general order; with the side
-// ranks of the short-slide order)
-struct PlainShape { int blocksA, blocksR, blocksD, blocksDS, blocksX, blocksY, blocksDN, blocksDNS, blocksDM; };
+// ranks of the short-slide order); crossings, rods, nodes (with the side ranks) and segments of the split phases;
+// the crossing blocks of 256 threads in the launch with block roles
+struct PlainShape { int blocksA, blocksR, blocksD, blocksDS, blocksX, blocksY, blocksDN, blocksDNS, blocksDM, blocksXR; };
 // a second stream and events: the element phase forks into a crossing kernel on `side` and a rod kernel on the main
 // stream, joined before the update, which forks again into a node kernel on `side` and a segment kernel on the main
 // stream, joined at the end of the iteration
@@ -18,10 +19,12 @@ template <int P>
 cudaError_t launchBatched(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
                           const uint8_t *mask, int threads, int blocks, bool shortSides, bool ext, cudaStream_t st);
 // ext: some instance runs an extension (contact extensions, the ground, a load protocol): the kernels' variants that
-// have them
+// have them.  roles: each split phase as one launch whose blocks take the two parts' roles (no fork); else `fork`
+// (when given) runs the parts on forked branches, else each phase is one kernel.
 template <int P>
 cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, const PlainShape &sh, bool contacts,
-                            bool shortSides, bool ext, cudaStream_t st, int *launches, unsigned *counter, const PlainFork *fork);
+                            bool shortSides, bool ext, cudaStream_t st, int *launches, unsigned *counter, const PlainFork *fork,
+                            bool roles);
 
 template <int P>
 cudaError_t launchGrid(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, unsigned *bar, int *err, int nIter,

@@ -31,8 +31,12 @@ STATE_FIELDS = ("X", "Q", "V", "W", "u", "nprev", "slip", "Fn", "Ft", "gap", "N"
                 "floor_state", "seg_M", "node_M", "disp")
 
 
+_PTR = {np.dtype(np.uint8): C.POINTER(C.c_uint8), np.dtype(np.float64): C.POINTER(C.c_double)}
+
+
 def _state_buffers(md, fields=None):
-    """host arrays for one instance's state and the ws_state_out pointing at them; fields left out stay NULL"""
+    """host arrays for one instance's state and the ws_state_out pointing at them; fields left out stay NULL.  The
+    arrays are left uninitialised: ws_download writes every element of every array it is given."""
     n, m, p, K = md.n, md.m, md.p, md.K
     size = {"X": 3 * n, "Q": 4 * m, "V": 3 * n, "W": 3 * m, "u": 2 * K, "nprev": 3 * K, "slip": K, "Fn": K, "Ft": K,
             "gap": K, "N": m, "Vsh": 2 * m, "M": 3 * p, "reactions": 3 * n, "stuck": K, "state": K,
@@ -43,12 +47,11 @@ def _state_buffers(md, fields=None):
     bad = [k for k in names if k not in size]
     if bad:
         raise ValueError(f"unknown state fields {bad}; known: {STATE_FIELDS}")
-    out = {k: np.zeros(size[k], dtype=np.uint8 if k in ("stuck", "state", "ctype", "floor_state") else np.float64)
+    out = {k: np.empty(size[k], dtype=np.uint8 if k in ("stuck", "state", "ctype", "floor_state") else np.float64)
            for k in names}
     so = WsStateOut()
     for k, a in out.items():
-        ct = C.c_uint8 if a.dtype == np.uint8 else C.c_double
-        setattr(so, k, a.ctypes.data_as(C.POINTER(ct)) if a.size else None)
+        setattr(so, k, C.cast(a.ctypes.data, _PTR[a.dtype]) if a.size else None)
     return out, so
 
 

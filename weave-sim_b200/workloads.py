@@ -10,6 +10,10 @@
 * ``ratio`` — the batched form (592 domes) against the plain single-instance form on the 3 m dome.
 * ``serve`` — the serving loop under Poisson arrivals at the given rates: fresh stiff domes (new seed each) and, with
   probability 0.3, variants (±5 % E, ±0.1 μ, ±2 % support displacement) of a resident equilibrium, warm-started.
+* ``scene`` — the reference's example scene dome_basic (read from its scene.json by the scene reader): one solve to
+  convergence (or the scene's 8000-iteration cap) in FP64 and mixed, plain and batched forms; the mixed result against
+  FP64 beside the chaos floor (FP64 against FP64 started with every node moved by ~1e-9·span and ~1e-7·span, the
+  size of an FP32 rounding); 64 copies relaxed together.
 
 Every solve here stops at convergence (relative residual ≤ tol) or at its iteration cap, as CpuSolver.run does.
 """
@@ -49,6 +53,48 @@ def _compare(a, b, models):
     return {"pos_err_span_median": float(np.median(pos)), "pos_err_span_max": float(np.max(pos)),
             "within_1e-4_span": int(np.sum(np.array(pos) <= 1e-4)), "slide_err_max_segments": float(np.max(du)),
             "slip_state_mismatch_total": int(np.sum(state)), "stick_mismatch_total": int(np.sum(stuck))}
+
+
+def run_scene(path, copies=64):
+    """a real scene: time to relax it on the device, FP64 and mixed, one instance (plain and batched forms) and a batch
+    of copies; the mixed positions against FP64 (max node error / span)"""
+    from .scenefile import load_scene
+    md = load_scene(path)
+    cap = int(md.params["max_iter"])
+    out = {"scene": path.rsplit("/", 1)[-1], "nodes": md.n, "segments": md.m, "crossings": md.K, "iteration_cap": cap}
+    X = {}
+    for prec in ("f64", "mixed"):
+        for form in ("plain", "cta"):
+            s = GpuSolver([md.copy()], precision=prec, form=form)
+            s.step(10)                                     # first-launch costs out of the timing
+            s.load_instance(0, md.copy())                  # back to the scene's start, iteration 0
+            ctl = s.step(cap)[0]
+            ms = s.last_step_stats()[0]
+            X[(prec, form)] = s.download(0, fields=("X",))["X"]
+            s.dispose()
+            out[f"{prec}_{form}"] = {"gpu_ms": ms, "iterations": ctl["iter"], "status": ctl["status"],
+                                     "residual": ctl["residual"], "iters_per_s": ctl["iter"] / (ms * 1e-3)}
+    for eps in (1e-9, 1e-7):
+        p = md.copy()
+        p.X = p.X + eps * md.span * np.random.default_rng(1).standard_normal(p.X.shape)
+        s = GpuSolver([p], precision="f64", form="plain")
+        s.step(cap)
+        X[eps] = s.download(0, fields=("X",))["X"]
+        s.dispose()
+
+    def err(a, b):
+        return float(np.linalg.norm((X[a] - X[b]).reshape(-1, 3), axis=1).max() / md.span)
+    out["mixed_vs_f64_pos_err_span"] = err(("mixed", "plain"), ("f64", "plain"))
+    out["chaos_floor_f64_1e-9span_pos_err_span"] = err(1e-9, ("f64", "plain"))
+    out["chaos_floor_f64_1e-7span_pos_err_span"] = err(1e-7, ("f64", "plain"))
+    out["f64_cta_vs_plain_pos_err_span"] = err(("f64", "cta"), ("f64", "plain"))
+    s = GpuSolver([md.copy() for _ in range(copies)], precision="mixed")
+    ctl = s.step(cap)
+    ms = s.last_step_stats()[0]
+    s.dispose()
+    out["batch"] = {"copies": copies, "gpu_ms": ms, "solves_per_s": copies / (ms * 1e-3),
+                    "inst_iters_per_s": sum(c["iter"] for c in ctl) / (ms * 1e-3)}
+    return out
 
 
 def run_precision(instances=64, iters=CAP, seed0=1, horizons=(500, 1000, 2000, 3000, 5000)):
