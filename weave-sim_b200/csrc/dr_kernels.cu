@@ -7,8 +7,9 @@
 
 // Minimum resident blocks of 256 threads per SM asked of the large-instance kernels, i.e. their register budget
 // (65536 / (256 × blocks) registers a thread), each chosen by measurement on the 20 m shell: the whole element kernel
-// unbounded (the crossing code is heavy in live values), its rod half (Y) at 2, the whole update kernel at 4 (64
-// registers, a few spills), its node and segment halves (DN, DM) at 3, the grid form at 2.
+// unbounded (the crossing code is heavy in live values), its rod half (Y) at 4 (64 registers; 3 in FP64, where 64
+// registers spill), the element launch with block roles at 2, the whole update kernel at 4 (64 registers, a few
+// spills), its node and segment halves (DN, DM) at 3, the grid form at 2.
 #ifndef WSB_MINB_A
 #define WSB_MINB_A 1
 #endif
@@ -16,7 +17,10 @@
 #define WSB_MINB_D 4
 #endif
 #ifndef WSB_MINB_Y
-#define WSB_MINB_Y 2
+#define WSB_MINB_Y(P) ((P) == PREC_F64 ? 3 : 4)
+#endif
+#ifndef WSB_MINB_XY
+#define WSB_MINB_XY 2
 #endif
 #ifndef WSB_MINB_DN
 #define WSB_MINB_DN 3
@@ -48,15 +52,23 @@ __device__ __forceinline__ void addPart(Part<A> &q, const A *part, int b, int st
   for (int i = 0; i < RX_NMAX; i++) q.x[i] = mmax(q.x[i], __ldcg(part + size_t(RS_NSUM + i) * stride + b));
 }
 
-// element e of phase A: the crossings come first (the heaviest elements start earliest; two adjacent elements, one a
-// side, per crossing), then segments, joints, clamps
-template <int P, bool SHORT, bool EXT>
-__device__ __forceinline__ void phaseA(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, int e, int nK, Part<typename Dev<P>::A> &pt) {
-  if (e < 2 * nK) { crossing<P, SHORT, EXT>(d, I, sx.cur, sx.iter, sx.onxt, sx.obuf, I.k0 + (e >> 1), e & 1, sx.alPend, sx.penN, pt); return; }
-  e -= 2 * nK;
+// rod element e of phase A: segments, joints, clamps
+template <int P>
+__device__ __forceinline__ void rodElement(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, int e, Part<typename Dev<P>::A> &pt) {
   if (e < I.m) segForce<P>(d, sx.cur, I.m0 + e, pt);
   else if ((e -= I.m) < I.p) jointTorque<P>(d, sx.cur, I.p0 + e, pt);
   else clampTorque<P>(d, sx.cur, I.c0 + (e - I.p), pt);
+}
+// crossing element e of phase A: two adjacent elements, one a side, per crossing
+template <int P, bool SHORT, bool EXT>
+__device__ __forceinline__ void crossElement(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, int e, Part<typename Dev<P>::A> &pt) {
+  crossing<P, SHORT, EXT>(d, I, sx.cur, sx.iter, sx.onxt, sx.obuf, I.k0 + (e >> 1), e & 1, sx.alPend, sx.penN, pt);
+}
+// element e of phase A: the crossings come first (the heaviest elements start earliest), then the rods
+template <int P, bool SHORT, bool EXT>
+__device__ __forceinline__ void phaseA(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, int e, int nK, Part<typename Dev<P>::A> &pt) {
+  if (e < 2 * nK) crossElement<P, SHORT, EXT>(d, I, sx, e, pt);
+  else rodElement<P>(d, I, sx, e - 2 * nK, pt);
 }
 __device__ __forceinline__ int countA(const InstDesc &I) {
   const int nK = (I.contacts && I.K) ? I.K : 0;
@@ -406,11 +418,15 @@ __device__ __forceinline__ void plainA(const Dev<P> &d, const InstDesc *__restri
   if (c.status != WS_RUNNING) return;
   const int nK = (I.contacts && I.K) ? I.K : 0;
   const int nA = PART == 1 ? 2 * nK : PART == 2 ? I.m + I.p + I.C : countA(I);
-  const int base = PART == 2 ? 2 * nK : 0;
   const StepCtx sx = makeCtx<A>(I, c);
   Part<A> pt;
   pt.init();
-  for (int e = blk * blockDim.x + threadIdx.x; e < nA; e += nblk * blockDim.x) phaseA<P, SHORT, EXT>(d, I, sx, base + e, nK, pt);
+  // each part compiles only its own element code (a branch the part never takes still costs registers)
+  for (int e = blk * blockDim.x + threadIdx.x; e < nA; e += nblk * blockDim.x) {
+    if (PART == 1) crossElement<P, SHORT, EXT>(d, I, sx, e, pt);
+    else if (PART == 2) rodElement<P>(d, I, sx, e, pt);
+    else phaseA<P, SHORT, EXT>(d, I, sx, e, nK, pt);
+  }
   constexpr unsigned SM = PART == 1 ? SUMS_CROSS : PART == 2 ? SUMS_ROD : (SUMS_CROSS | SUMS_ROD);
   constexpr unsigned XM = PART == 1 ? MAXS_CROSS : PART == 2 ? MAXS_ROD : (MAXS_CROSS | MAXS_ROD);
   blockReduce<SM, XM>(pt, red);
@@ -429,14 +445,14 @@ __global__ void __launch_bounds__(128) k_plainX(Dev<P> d, const InstDesc *__rest
   plainA<P, SHORT, EXT, 1>(d, insts, ctl, part, partStride, blockIdx.x, gridDim.x);
 }
 template <int P, bool SHORT>
-__global__ void __launch_bounds__(256, WSB_MINB_Y) k_plainY(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
+__global__ void __launch_bounds__(256, WSB_MINB_Y(P)) k_plainY(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
                                                 typename Dev<P>::A *part, int partStride) {
   plainA<P, SHORT, false, 2>(d, insts, ctl, part, partStride, blockIdx.x, gridDim.x);
 }
 // The element phase as one launch whose blocks take roles: the first nbX blocks the crossings, the others the segments,
 // joints and clamps, so both run side by side without a fork in the graph; partials at part[block] in that order.
 template <int P, bool SHORT, bool EXT>
-__global__ void __launch_bounds__(256, WSB_MINB_Y) k_plainXY(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
+__global__ void __launch_bounds__(256, WSB_MINB_XY) k_plainXY(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
                                                  typename Dev<P>::A *part, int partStride, int nbX) {
   waitPrevGrid();
   allowNextGrid();
@@ -453,6 +469,23 @@ __global__ void __launch_bounds__(256) k_plainBC(Dev<P> d, const InstDesc *__res
   if (c.status != WS_RUNNING) return;
   const StepCtx sx = makeCtx<A>(I, c);
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 2 * I.K + I.m; e += gridDim.x * blockDim.x) phaseBC<P>(d, I, sx, e);
+}
+// The end of an iteration without the extensions, run by the update phase's last block: every block partial reduced in
+// a fixed order, then the kinetic-damping decision.  Out of line, so that its registers do not count against the
+// element loop's budget.  The control block is read again here: no block writes it before this one.
+template <class A>
+__device__ __noinline__ void closeIteration(const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl, const A *partAll,
+                                            int nParts, int partStride, unsigned *counter, A *red) {
+  Part<A> q;
+  q.init();
+  for (int b = threadIdx.x; b < nParts; b += blockDim.x) addPart(q, partAll, b, partStride);
+  blockReduce(q, red);
+  if (threadIdx.x == 0) {
+    InstCtl cc = ctl[0];
+    decide<false>(insts[0], cc, q, 0);
+    ctl[0] = cc;
+    *counter = 0;
+  }
 }
 // The update kernel also closes the iteration: every block publishes its partials, and the last block to finish
 // (counted on `counter` over all `nBlocks` blocks of the update phase) reduces the partials of phases A and D in a
@@ -492,6 +525,10 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
   __syncthreads();
   if (!last) return;
   __threadfence();
+  if constexpr (!EXT) {
+    closeIteration<A>(insts, ctl, partAll, nParts, partStride, counter, red);
+    return;
+  }
   Part<A> q;
   q.init();
   for (int b = threadIdx.x; b < nParts; b += blockDim.x) addPart(q, partAll, b, partStride);
