@@ -124,3 +124,35 @@ def ground_beam(pull=0.0, q=10.0, mu=0.5, nseg=10, L=1000.0, **prm):
     md.node_w = np.full(md.n, 60.0)
     md.node_h = np.full(md.n, 30.0)
     return md
+
+
+def permute_nodes(md, seed=0):
+    """The same model with its nodes renumbered by a seeded permutation (node i becomes perm[i]): every node-indexed
+    array reordered and every node index remapped.  Strands then no longer number their nodes consecutively, so the
+    solver gathers a crossing side's nodes instead of computing them.  Returns (model, perm)."""
+    perm = np.random.default_rng(seed).permutation(md.n).astype(np.int32)
+    p = md.copy()
+
+    def reorder(a, width):
+        if a is None or a.size == 0:
+            return a
+        b = np.empty_like(a).reshape(md.n, width)
+        b[perm] = a.reshape(md.n, width)
+        return b.reshape(-1)
+    for k in ("X", "X0", "load_const"):
+        setattr(p, k, reorder(getattr(md, k), 3))
+    for k in ("node_w", "node_h"):
+        setattr(p, k, reorder(getattr(md, k), 1))
+    for k in ("seg_i0", "seg_i1", "local_load_node", "anchor_node"):
+        a = getattr(md, k)
+        if a is not None and a.size:
+            setattr(p, k, perm[a].astype(np.int32))
+    if md.protocol:
+        p.protocol = dict(md.protocol, probe=int(perm[md.protocol["probe"]]))
+    p.node_offset = None
+    return p, perm
+
+
+def unpermute(X, perm):
+    """node positions of a permuted model back in the original numbering"""
+    return X.reshape(-1, 3)[perm].reshape(-1)

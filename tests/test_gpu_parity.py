@@ -774,3 +774,24 @@ def test_reference_scene_matches_oracle(oracle_mod):
         assert ctl["iter"] == 1000 and ctl["rollbacks"] == v["rollbacks"]
         assert cases.max_rel_disp_error(g["X"], v["X"], v["X0"]) < 1e-9
         assert np.array_equal(g["stuck"], v["stuck"])
+
+
+# ------------------------------------------------------------------------------------------------ node numbering
+# A crossing side's nodes and neighbouring segments are computed from the strand's first node when every crossing
+# strand numbers its nodes consecutively (the builders' layout), and gathered otherwise; a renumbered model takes the
+# gathered path and must give the same gridshell.
+
+@pytest.mark.parametrize("form", ["plain", "cta", "grid"])
+def test_renumbered_nodes_match_oracle(oracle_mod, form):
+    md = ws.configs.dome_small()
+    o = oracle_mod.Oracle(md.copy())
+    o.step(320)
+    v = o.view()
+    pm, perm = cases.permute_nodes(md, seed=3)
+    s = ws.GpuSolver([pm], precision="f64", form=form)
+    ctl = s.step(320)[0]
+    g = s.download(0, fields=("X", "u"))
+    s.dispose()
+    assert ctl["iter"] == 320
+    assert cases.max_node_err_span(cases.unpermute(g["X"], perm), v["X"], md.span) < 1e-9
+    assert np.abs(g["u"] - v["u"]).max() < 1e-9

@@ -296,3 +296,15 @@ def test_ground_friction_slides_on_the_cone(oracle_mod):
     assert not v["converged"] and np.all(v["floor_state"] == 2)
     assert abs(abs(F[:, 0].sum()) - 0.5 * F[:, 2].sum()) < 1e-9 * F[:, 2].sum()
     assert v["X"][-3] > 1000.0 + 10.0                     # the free end has slid along x
+
+
+def test_node_numbering_does_not_change_the_oracle(ws, oracle_mod):
+    # the renumbering helper used by the GPU tests of gathered side neighbourhoods: the oracle gives the same gridshell
+    # whatever the node numbering (up to the order of its sums)
+    md = ws.configs.dome_small()
+    pm, perm = cases.permute_nodes(md, seed=3)
+    a = oracle_mod.Oracle(md.copy())
+    a.step(200)
+    b = oracle_mod.Oracle(pm)
+    b.step(200)
+    assert cases.max_node_err_span(cases.unpermute(b.view()["X"], perm), a.view()["X"], md.span) < 1e-9

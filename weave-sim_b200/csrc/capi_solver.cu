@@ -67,7 +67,7 @@ void layout(Dev<P> &d, Carver &cv, const Sizes &z) {
   d.GJ = cv.take<R>(p); d.om = cv.take<R>(3 * p); d.tau = cv.take<R>(3 * p); d.kd = cv.take<R>(3 * p); d.Mj = cv.take<R>(3 * p);
   d.cSeg = cv.take<int>(c); d.cLen = cv.take<R>(c); d.cB = cv.take<R>(3 * c); d.cQ = cv.take<W>(4 * c);
   d.tauC = cv.take<R>(3 * c); d.cM = cv.take<R>(2 * c);
-  d.cxSegOff = cv.take<int>(2 * k); d.cxNseg = cv.take<int>(2 * k); d.wk = cv.take<R>(2 * k); d.hk = cv.take<R>(2 * k);
+  d.cxSegOff = cv.take<int>(2 * k); d.cxNseg = cv.take<int>(2 * k); d.cxNodeOff = cv.take<int>(2 * k); d.wk = cv.take<R>(2 * k); d.hk = cv.take<R>(2 * k);
   d.cw = cv.take<R>(k); d.ch = cv.take<R>(k); d.mu = cv.take<R>(k); d.cflag = cv.take<uint8_t>(k);
   d.u = cv.take<U>(2 * k); d.nPrev = cv.take<R>(3 * k); d.slip = cv.take<A>(k); d.stuck = cv.take<uint8_t>(k);
   d.cstate = cv.take<uint8_t>(k); d.Fn = cv.take<R>(k); d.Ft = cv.take<R>(k); d.gap = cv.take<R>(k);
@@ -298,6 +298,7 @@ InstDesc describe(const HostGoals &g, const Sizes &off) {
   I.ext = (I.aug || I.rotFric || I.seat) ? 1 : 0;
   I.utmMode = g.proto.mode; I.utmProbe = off.n + g.proto.probe; I.utmNInc = g.proto.n_inc; I.utmSettle = g.proto.settle;
   I.utmAvg = g.proto.avg; I.utmIdx = off.b;
+  I.cxLin = g.cxLinear ? 1 : 0;
   I.floorOn = g.prm.floor ? 1 : 0; I.floorZ = g.prm.floor_z; I.floorMu = g.prm.floor_mu;
   for (int k = 0; k < 3; k++) I.utmAxis[k] = g.proto.axis[k];
   return I;
@@ -499,15 +500,17 @@ void uploadStatic(ws_ctx *c, int b) {
   put<int>(d.jS1 + I.p0, shift(g.jSeg1, I.m0).data(), p, st);
   put<R>(d.jLen + I.p0, g.jLen.data(), p, st);
   for (int side = 0; side < 2; side++) {
-    std::vector<int> so(K), nsg(K);
+    std::vector<int> so(K), nsg(K), no(K);
     std::vector<double> w(K), h(K), fc(K), e9(K), hs(K);
     for (size_t q = 0; q < K; q++) { so[q] = I.m0 + g.cxSegOff[2 * q + side]; nsg[q] = g.cxNseg[2 * q + side]; w[q] = g.wk[2 * q + side]; h[q] = g.hk[2 * q + side]; }
+    for (size_t q = 0; q < K; q++) no[q] = I.n0 + g.cxNodeOff[2 * q + side];
     for (size_t q = 0; q < K; q++) { fc[q] = g.fc90[2 * q + side]; e9[q] = g.E90[2 * q + side]; hs[q] = g.Hs[2 * q + side]; }
     put<R>(d.fc90 + size_t(side) * d.ktot + I.k0, fc.data(), K, st);
     put<R>(d.E90 + size_t(side) * d.ktot + I.k0, e9.data(), K, st);
     put<R>(d.Hs + size_t(side) * d.ktot + I.k0, hs.data(), K, st);
     put<int>(d.cxSegOff + size_t(side) * d.ktot + I.k0, so.data(), K, st);
     put<int>(d.cxNseg + size_t(side) * d.ktot + I.k0, nsg.data(), K, st);
+    put<int>(d.cxNodeOff + size_t(side) * d.ktot + I.k0, no.data(), K, st);
     put<R>(d.wk + size_t(side) * d.ktot + I.k0, w.data(), K, st);
     put<R>(d.hk + size_t(side) * d.ktot + I.k0, h.data(), K, st);
   }

@@ -40,6 +40,9 @@ struct InstDesc {
   double utmAxis[3];
   // the ground: on / off, height, friction coefficient
   int floorOn;
+  // every strand that carries a crossing side is linear: its segment k joins its nodes N0 + k and N0 + k + 1, and no
+  // other segment starts or ends on those nodes; a side's nodes and neighbouring segments then follow by arithmetic
+  int cxLin;
   double floorZ, floorMu;
 };
 
@@ -106,6 +109,7 @@ struct Dev {
   R *tauC, *cM;    // [3][ctot], [2][ctot]
   // crossings
   int *cxSegOff, *cxNseg;   // [2][ktot]
+  int *cxNodeOff;           // [2][ktot] first node of the side's strand (read when the instance's strands are linear)
   R *wk, *hk;               // [2][ktot]
   R *cw, *ch, *mu;          // [ktot]
   uint8_t *cflag;           // bit 0 enabled, bit 1 locked

@@ -169,28 +169,36 @@ struct Part {
 template <class T> __device__ __forceinline__ T ro(const T *p) { return __ldg(p); }
 
 // ------------------------------------------------------------------------------------------------ node helpers
-// node tangent: normalised sum of the unit chords of the adjacent segments (PolylineContact._prepare)
+// node tangent: normalised sum of the unit chords of the adjacent segments (PolylineContact._prepare), from its
+// outgoing chord (o0 → o1) and incoming chord (i0 → i1) given by their end nodes; a chord whose first node is negative
+// is absent
 template <int P>
-__device__ __forceinline__ void nodeTangent(const Dev<P> &d, int buf, int i, typename Dev<P>::R T[3]) {
+__device__ __forceinline__ void chordTangent(const Dev<P> &d, int buf, int o0, int o1, int i0, int i1, typename Dev<P>::R T[3]) {
   using R = typename Dev<P>::R;
   T[0] = T[1] = T[2] = R(0);
-  const int so = ro(d.nsOut + i), si = ro(d.nsIn + i);
-  auto chord = [&](int j) {
+  auto chord = [&](int a, int b) {
     R e[3];
-    Acc<P>::edge(d, buf, ro(d.segI0 + j), ro(d.segI1 + j), e);
+    Acc<P>::edge(d, buf, a, b, e);
     const R l = mmax(msqrt(dot3(e, e)), R(1e-12));
     for (int k = 0; k < 3; k++) T[k] += e[k] / l;
   };
-  if (so >= 0) chord(so);
-  if (si >= 0) chord(si);
+  if (o0 >= 0) chord(o0, o1);
+  if (i0 >= 0) chord(i0, i1);
   const R l = mmax(msqrt(dot3(T, T)), R(1e-12));
   for (int k = 0; k < 3; k++) T[k] /= l;
 }
+// the same for node i, from its outgoing and incoming segments
+template <int P>
+__device__ __forceinline__ void nodeTangent(const Dev<P> &d, int buf, int i, typename Dev<P>::R T[3]) {
+  const int so = ro(d.nsOut + i), si = ro(d.nsIn + i);
+  chordTangent<P>(d, buf, so >= 0 ? ro(d.segI0 + so) : -1, so >= 0 ? ro(d.segI1 + so) : -1,
+                  si >= 0 ? ro(d.segI0 + si) : -1, si >= 0 ? ro(d.segI1 + si) : -1, T);
+}
 // hemisphere-consistent mean of the adjacent segment frames (nodeQuats, model.js:89-105)
 template <int P>
-__device__ __forceinline__ void nodeQuat(const Dev<P> &d, int buf, int i, typename Dev<P>::R q[4]) {
+__device__ __forceinline__ void segsQuat(const Dev<P> &d, int buf, int so, int si, typename Dev<P>::R q[4]) {
   using R = typename Dev<P>::R;
-  const int so = ro(d.nsOut + i), si = ro(d.nsIn + i), ref = so >= 0 ? so : si;
+  const int ref = so >= 0 ? so : si;
   q[0] = q[1] = q[2] = q[3] = R(0);
   if (ref < 0) return;
   R qr[4];
@@ -205,6 +213,11 @@ __device__ __forceinline__ void nodeQuat(const Dev<P> &d, int buf, int i, typena
   if (so >= 0) add(so);
   if (si >= 0) add(si);
   qnormalize(q);
+}
+// the same for node i, from its outgoing and incoming segments
+template <int P>
+__device__ __forceinline__ void nodeQuat(const Dev<P> &d, int buf, int i, typename Dev<P>::R q[4]) {
+  segsQuat<P>(d, buf, ro(d.nsOut + i), ro(d.nsIn + i), q);
 }
 
 // ------------------------------------------------------------------------------------------------ phase A
@@ -484,13 +497,24 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
     const int li = int(mmin(mmax(mfloor(uu), U(0)), U(mmax(nseg - 1, 0))));
     const R t = R(mmin(mmax(uu - U(li), U(0)), U(1)));
     const int sg = ro(d.cxSegOff + o) + li;
-    const int a = ro(d.segI0 + sg), b = ro(d.segI1 + sg);
+    // the segment's nodes a → b, the segment ending at a (sIn, from aPrev) and the one starting at b (sOut, to bNext):
+    // by arithmetic on a linear strand, else gathered (the same indices either way)
+    int a, b, sIn, sOut, aPrev, bNext;
+    if (I.cxLin) {
+      a = ro(d.cxNodeOff + o) + li; b = a + 1;
+      sIn = li > 0 ? sg - 1 : -1; sOut = li < nseg - 1 ? sg + 1 : -1;
+      aPrev = a - 1; bNext = b + 1;
+    } else {
+      a = ro(d.segI0 + sg); b = ro(d.segI1 + sg);
+      sIn = ro(d.nsIn + a); sOut = ro(d.nsOut + b);
+      aPrev = sIn >= 0 ? ro(d.segI0 + sIn) : -1; bNext = sOut >= 0 ? ro(d.segI1 + sOut) : -1;
+    }
     for (int k = 0; k < 3; k++) xm[k] = Acc<P>::xw(d, buf, k, a);
     R e[3], Ta[3], Tb[3];
     Acc<P>::edge(d, buf, a, b, e);
     const R Ls = msqrt(dot3(e, e));
-    nodeTangent<P>(d, buf, a, Ta);
-    nodeTangent<P>(d, buf, b, Tb);
+    chordTangent<P>(d, buf, a, b, sIn >= 0 ? aPrev : -1, a, Ta);
+    chordTangent<P>(d, buf, sOut >= 0 ? b : -1, bNext, a, b, Tb);
     const R t2 = t * t, t3 = t2 * t;
     const R h10 = t3 - R(2) * t2 + t, h01 = R(-2) * t3 + R(3) * t2, h11 = t3 - t2;
     const R d10 = R(3) * t2 - R(4) * t + R(1), d01 = R(-6) * t2 + R(6) * t, d11 = R(3) * t2 - R(2) * t;
@@ -501,8 +525,8 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
     const R tl = mmax(msqrt(dot3(Tm, Tm)), R(1e-12));
     for (int k = 0; k < 3; k++) Tm[k] /= tl;
     R qa[4], qb[4], q[4], Rn[9];
-    nodeQuat<P>(d, buf, a, qa);
-    nodeQuat<P>(d, buf, b, qb);
+    segsQuat<P>(d, buf, sg, sIn, qa);
+    segsQuat<P>(d, buf, sOut, sg, qb);
     const R sgn = (qa[0] * qb[0] + qa[1] * qb[1] + qa[2] * qb[2] + qa[3] * qb[3]) < R(0) ? R(-1) : R(1);
     for (int k = 0; k < 4; k++) q[k] = (R(1) - t) * qa[k] + t * sgn * qb[k];
     qnormalize(q);

@@ -103,6 +103,26 @@ static void buildTables(HostGoals &g) {
   g.segStrand.resize(g.m); g.segLocal.resize(g.m);
   for (int s = 0; s < g.S; s++)
     for (int j = g.segOffset[s]; j < g.segOffset[s + 1]; j++) { g.segStrand[j] = s; g.segLocal[j] = j - g.segOffset[s]; }
+  // linear crossing strands: segment k of the strand joins nodes N0 + k and N0 + k + 1, and its end nodes start or end
+  // no other segment (the layout buildState gives, model.js:10-75), so a crossing side's nodes and neighbouring
+  // segments are the strand's first node and segment plus the side's segment index
+  auto linear = [&](int s) {
+    const int j0 = g.segOffset[s], j1 = g.segOffset[s + 1];
+    if (j1 <= j0) return false;
+    const int n0 = g.segI0[j0];
+    for (int j = j0; j < j1; j++)
+      if (g.segI0[j] != n0 + (j - j0) || g.segI1[j] != n0 + (j - j0) + 1) return false;
+    return g.nodeSegIn[n0] < 0 && g.nodeSegOut[n0 + (j1 - j0)] < 0;
+  };
+  std::vector<signed char> lin(g.S, -1);
+  g.cxNodeOff.assign(2 * size_t(g.K), 0);
+  g.cxLinear = true;
+  for (int i = 0; i < 2 * g.K; i++) {
+    const int s = g.cxStrand[i];
+    if (lin[s] < 0) lin[s] = linear(s) ? 1 : 0;
+    g.cxLinear = g.cxLinear && lin[s] == 1;
+    g.cxNodeOff[i] = g.segI0[g.segOffset[s]];
+  }
 }
 
 // Anchors (model.js:162-189) and the clamp joints of the rotation anchors (rod_cosserat.js:92-100), frozen at Q

@@ -33,6 +33,8 @@ struct HostGoals {
   std::vector<double> ancStart, ancDelta;            // [3 * slots]
   // contact
   std::vector<int> cxSegOff, cxNseg, cxStrand;       // [2K] first segment, segment count and strand of each side
+  std::vector<int> cxNodeOff;                        // [2K] first node of each side's strand
+  bool cxLinear = false;                             // every crossing strand is linear (InstDesc::cxLin)
   std::vector<double> wk, hk, w, h, mu;
   std::vector<double> fc90, E90, Hs;                 // [2K] timber across the grain, each side (W1 classification)
   ws_protocol proto{};                               // load protocol (mode 0: none), kept over warm starts
