@@ -46,6 +46,29 @@ __device__ __forceinline__ void putPart(const Part<A> &p, A *part, int b, int st
   for (int i = 0; i < RS_NSUM; i++) part[size_t(i) * stride + b] = p.s[i];
   for (int i = 0; i < RX_NMAX; i++) part[size_t(RS_NSUM + i) * stride + b] = p.x[i];
 }
+// the same, writing only the slots in SM / XM (the plain form: the close reads only those)
+template <unsigned SM, unsigned XM, class A>
+__device__ __forceinline__ void putPartSlots(const Part<A> &p, A *part, int b, int stride) {
+#pragma unroll
+  for (int i = 0; i < RS_NSUM; i++)
+    if (SM & (1u << i)) part[size_t(i) * stride + b] = p.s[i];
+#pragma unroll
+  for (int i = 0; i < RX_NMAX; i++)
+    if (XM & (1u << i)) part[size_t(RS_NSUM + i) * stride + b] = p.x[i];
+}
+// partial rows [lo, hi) added into q, only the slots in SM / XM; thread t takes rows lo + t, lo + t + blockDim, ...
+template <unsigned SM, unsigned XM, class A>
+__device__ __forceinline__ void addPartSlots(Part<A> &q, const A *part, int lo, int hi, int stride) {
+#pragma unroll 2
+  for (int b = lo + threadIdx.x; b < hi; b += blockDim.x) {
+#pragma unroll
+    for (int i = 0; i < RS_NSUM; i++)
+      if (SM & (1u << i)) q.s[i] += __ldcg(part + size_t(i) * stride + b);
+#pragma unroll
+    for (int i = 0; i < RX_NMAX; i++)
+      if (XM & (1u << i)) q.x[i] = mmax(q.x[i], __ldcg(part + size_t(RS_NSUM + i) * stride + b));
+  }
+}
 template <class A>
 __device__ __forceinline__ void addPart(Part<A> &q, const A *part, int b, int stride) {
   for (int i = 0; i < RS_NSUM; i++) q.s[i] += __ldcg(part + size_t(i) * stride + b);
@@ -403,6 +426,29 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
 }
 
 // ------------------------------------------------------------------------------------------------ plain form
+// the sum and max slots each part of a phase feeds: element phase whole (0), crossings (1), rods (2); update phase
+// whole (0), nodes with the side ranks (1), segments (2)
+constexpr unsigned elemSums(int part) { return part == 1 ? SUMS_CROSS : part == 2 ? SUMS_ROD : (SUMS_CROSS | SUMS_ROD); }
+constexpr unsigned elemMaxs(int part) { return part == 1 ? MAXS_CROSS : part == 2 ? MAXS_ROD : (MAXS_CROSS | MAXS_ROD); }
+constexpr unsigned updateSums(int part, bool ext) { return SUMS_UPDATE | (ext && part != 2 ? SUMS_FLOOR : 0u); }
+constexpr unsigned updateMaxs(int part, bool ext) {
+  return (part == 1 ? ((1u << RX_F) | (1u << RX_LOAD)) : part == 2 ? (1u << RX_T) : MAXS_UPDATE) |
+         (ext && part != 2 ? MAXS_FLOOR : 0u);
+}
+// every block partial of one iteration, in ranges of fixed order, each read only in the slots its kernel feeds (the
+// others hold nothing): SPLIT, the four kernels of the split phases; else the two whole phases
+template <bool SPLIT, bool EXT, class A>
+__device__ __forceinline__ void reduceIteration(Part<A> &q, const A *part, int ex, int ey, int en, int em, int stride) {
+  if constexpr (SPLIT) {
+    addPartSlots<elemSums(1), elemMaxs(1)>(q, part, 0, ex, stride);
+    addPartSlots<elemSums(2), elemMaxs(2)>(q, part, ex, ey, stride);
+    addPartSlots<updateSums(1, EXT), updateMaxs(1, EXT)>(q, part, ey, en, stride);
+    addPartSlots<updateSums(2, EXT), updateMaxs(2, EXT)>(q, part, en, em, stride);
+  } else {
+    addPartSlots<elemSums(0), elemMaxs(0)>(q, part, 0, ex, stride);
+    addPartSlots<updateSums(0, EXT), updateMaxs(0, EXT)>(q, part, ex, em, stride);
+  }
+}
 // One kernel per phase over the elements of instance 0; block partials go to part[block] and the last block of the
 // update kernel reduces them in a fixed order.  Every kernel returns at once when the instance has stopped.
 // The element phase, whole (PART 0) or split in two kernels that run side by side on forked branches of the graph:
@@ -427,10 +473,9 @@ __device__ __forceinline__ void plainA(const Dev<P> &d, const InstDesc *__restri
     else if (PART == 2) rodElement<P>(d, I, sx, e, pt);
     else phaseA<P, SHORT, EXT>(d, I, sx, e, nK, pt);
   }
-  constexpr unsigned SM = PART == 1 ? SUMS_CROSS : PART == 2 ? SUMS_ROD : (SUMS_CROSS | SUMS_ROD);
-  constexpr unsigned XM = PART == 1 ? MAXS_CROSS : PART == 2 ? MAXS_ROD : (MAXS_CROSS | MAXS_ROD);
+  constexpr unsigned SM = elemSums(PART), XM = elemMaxs(PART);
   blockReduce<SM, XM>(pt, red);
-  if (threadIdx.x == 0) putPart(pt, part, blk, partStride);
+  if (threadIdx.x == 0) putPartSlots<SM, XM>(pt, part, blk, partStride);
 }
 template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(256, WSB_MINB_A) k_plainA(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
@@ -473,12 +518,12 @@ __global__ void __launch_bounds__(256) k_plainBC(Dev<P> d, const InstDesc *__res
 // The end of an iteration without the extensions, run by the update phase's last block: every block partial reduced in
 // a fixed order, then the kinetic-damping decision.  Out of line, so that its registers do not count against the
 // element loop's budget.  The control block is read again here: no block writes it before this one.
-template <class A>
+template <bool SPLIT, class A>
 __device__ __noinline__ void closeIteration(const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl, const A *partAll,
-                                            int nParts, int partStride, unsigned *counter, A *red) {
+                                            int ex, int ey, int en, int em, int partStride, unsigned *counter, A *red) {
   Part<A> q;
   q.init();
-  for (int b = threadIdx.x; b < nParts; b += blockDim.x) addPart(q, partAll, b, partStride);
+  reduceIteration<SPLIT, false>(q, partAll, ex, ey, en, em, partStride);
   blockReduce(q, red);
   if (threadIdx.x == 0) {
     InstCtl cc = ctl[0];
@@ -494,8 +539,8 @@ __device__ __noinline__ void closeIteration(const InstDesc *__restrict__ insts, 
 // branches: the nodes with the side ranks (PART 1) and the segments (PART 2), each at its own register budget.
 template <int P, bool SHORT, bool EXT, int PART>
 __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
-                                       typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts, int partStride,
-                                       unsigned *counter, unsigned nBlocks, int blk, int nblk) {
+                                       typename Dev<P>::A *part, typename Dev<P>::A *partAll, const PartEnds &pe,
+                                       int partStride, unsigned *counter, unsigned nBlocks, int blk, int nblk) {
   using A = typename Dev<P>::A;
   __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
   __shared__ bool last;
@@ -513,12 +558,10 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
     else if (e < I.n) nodeUpdate<P, SHORT, EXT>(d, I, sx, I.n0 + e, pt);
     else rankSideShort<P>(d, 2 * I.k0 + (e - I.n), sx.onxt);
   }
-  constexpr unsigned SM = SUMS_UPDATE | (EXT && PART != 2 ? SUMS_FLOOR : 0u);
-  constexpr unsigned XF = EXT && PART != 2 ? MAXS_FLOOR : 0u;
-  constexpr unsigned XM = (PART == 1 ? ((1u << RX_F) | (1u << RX_LOAD)) : PART == 2 ? (1u << RX_T) : MAXS_UPDATE) | XF;
+  constexpr unsigned SM = updateSums(PART, EXT), XM = updateMaxs(PART, EXT);
   blockReduce<SM, XM>(pt, red);
   if (threadIdx.x == 0) {
-    putPart(pt, part, blk, partStride);
+    putPartSlots<SM, XM>(pt, part, blk, partStride);
     __threadfence();
     last = atomicAdd(counter, 1u) == nBlocks - 1;
   }
@@ -526,12 +569,12 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
   if (!last) return;
   __threadfence();
   if constexpr (!EXT) {
-    closeIteration<A>(insts, ctl, partAll, nParts, partStride, counter, red);
+    closeIteration<PART != 0, A>(insts, ctl, partAll, pe.x, pe.y, pe.n, pe.m, partStride, counter, red);
     return;
   }
   Part<A> q;
   q.init();
-  for (int b = threadIdx.x; b < nParts; b += blockDim.x) addPart(q, partAll, b, partStride);
+  reduceIteration<PART != 0, EXT>(q, partAll, pe.x, pe.y, pe.n, pe.m, partStride);
   blockReduce(q, red);
   if (threadIdx.x == 0) {
     InstCtl cc = c;
@@ -543,36 +586,36 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
 }
 template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(256, WSB_MINB_D) k_plainD(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
-                                                typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts,
+                                                typename Dev<P>::A *part, typename Dev<P>::A *partAll, PartEnds pe,
                                                 int partStride, unsigned *counter) {
   waitPrevGrid();
   allowNextGrid();
-  plainD<P, SHORT, EXT, 0>(d, insts, ctl, part, partAll, nParts, partStride, counter, gridDim.x, blockIdx.x, gridDim.x);
+  plainD<P, SHORT, EXT, 0>(d, insts, ctl, part, partAll, pe, partStride, counter, gridDim.x, blockIdx.x, gridDim.x);
 }
 template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(256, WSB_MINB_DN) k_plainDN(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
-                                                  typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts,
+                                                  typename Dev<P>::A *part, typename Dev<P>::A *partAll, PartEnds pe,
                                                   int partStride, unsigned *counter, unsigned nBlocks) {
-  plainD<P, SHORT, EXT, 1>(d, insts, ctl, part, partAll, nParts, partStride, counter, nBlocks, blockIdx.x, gridDim.x);
+  plainD<P, SHORT, EXT, 1>(d, insts, ctl, part, partAll, pe, partStride, counter, nBlocks, blockIdx.x, gridDim.x);
 }
 template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(256, WSB_MINB_DM) k_plainDM(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
-                                                  typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts,
+                                                  typename Dev<P>::A *part, typename Dev<P>::A *partAll, PartEnds pe,
                                                   int partStride, unsigned *counter, unsigned nBlocks) {
-  plainD<P, SHORT, EXT, 2>(d, insts, ctl, part, partAll, nParts, partStride, counter, nBlocks, blockIdx.x, gridDim.x);
+  plainD<P, SHORT, EXT, 2>(d, insts, ctl, part, partAll, pe, partStride, counter, nBlocks, blockIdx.x, gridDim.x);
 }
 // The update phase as one launch with roles: the first nbN blocks the nodes (with the side ranks of the short order),
 // the others the segments; the last of all its blocks closes the iteration.
 template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(256, WSB_MINB_DN) k_plainDNM(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
-                                                   typename Dev<P>::A *part, typename Dev<P>::A *partAll, int nParts,
+                                                   typename Dev<P>::A *part, typename Dev<P>::A *partAll, PartEnds pe,
                                                    int partStride, unsigned *counter, int nbN) {
   waitPrevGrid();
   allowNextGrid();
   if (int(blockIdx.x) < nbN)
-    plainD<P, SHORT, EXT, 1>(d, insts, ctl, part, partAll, nParts, partStride, counter, gridDim.x, blockIdx.x, nbN);
+    plainD<P, SHORT, EXT, 1>(d, insts, ctl, part, partAll, pe, partStride, counter, gridDim.x, blockIdx.x, nbN);
   else
-    plainD<P, SHORT, EXT, 2>(d, insts, ctl, part + nbN, partAll, nParts, partStride, counter, gridDim.x, blockIdx.x - nbN,
+    plainD<P, SHORT, EXT, 2>(d, insts, ctl, part + nbN, partAll, pe, partStride, counter, gridDim.x, blockIdx.x - nbN,
                              gridDim.x - nbN);
 }
 
@@ -960,7 +1003,8 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
       if ((e = launchPDL(k_plainBC<P>, sh.blocksR, st, d, insts, ctl)) != cudaSuccess) return e;
       nl += 1;
     }
-    e = launchPDL(WSB_PICK(k_plainDNM, P, sh2, ext), nDN + sh.blocksDM, st, d, insts, ctl, pn, px, nParts, nParts, counter,
+    const PartEnds pe{nbX, nXY, nXY + nDN, nParts};
+    e = launchPDL(WSB_PICK(k_plainDNM, P, sh2, ext), nDN + sh.blocksDM, st, d, insts, ctl, pn, px, pe, nParts, counter,
                   nDN);
     if (e != cudaSuccess) return e;
     nl += 1;
@@ -973,6 +1017,7 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
     const int nDN = sh2 ? sh.blocksDNS : sh.blocksDN, nParts = sh.blocksX + sh.blocksY + nDN + sh.blocksDM;
     A *px = static_cast<A *>(part), *py = px + sh.blocksX, *pn = py + sh.blocksY, *pm = pn + nDN;
     const unsigned nB = unsigned(nDN + sh.blocksDM);
+    const PartEnds pe{sh.blocksX, sh.blocksX + sh.blocksY, sh.blocksX + sh.blocksY + nDN, nParts};
     cudaError_t e;
     if ((e = cudaEventRecord(fork->fork, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(fork->side, fork->fork, 0)) != cudaSuccess) return e;
@@ -990,10 +1035,10 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
     if ((e = cudaEventRecord(fork->fork2, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(fork->side, fork->fork2, 0)) != cudaSuccess) return e;
     const auto kdn = WSB_PICK(k_plainDN, P, sh2, ext);
-    kdn<<<sh2 ? sh.blocksDNS : sh.blocksDN, 256, 0, fork->side>>>(d, insts, ctl, pn, px, nParts, nParts, counter, nB);
+    kdn<<<sh2 ? sh.blocksDNS : sh.blocksDN, 256, 0, fork->side>>>(d, insts, ctl, pn, px, pe, nParts, counter, nB);
     if ((e = cudaEventRecord(fork->join2, fork->side)) != cudaSuccess) return e;
     const auto kdm = WSB_PICK(k_plainDM, P, sh2, ext);
-    kdm<<<sh.blocksDM, 256, 0, st>>>(d, insts, ctl, pm, px, nParts, nParts, counter, nB);
+    kdm<<<sh.blocksDM, 256, 0, st>>>(d, insts, ctl, pm, px, pe, nParts, counter, nB);
     if ((e = cudaStreamWaitEvent(st, fork->join2, 0)) != cudaSuccess) return e;
     nl += 2;
     if (launches) *launches += nl;
@@ -1008,7 +1053,8 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
     if ((e = launchPDL(k_plainBC<P>, sh.blocksR, st, d, insts, ctl)) != cudaSuccess) return e;
     nl += 1;
   }
-  e = launchPDL(WSB_PICK(k_plainD, P, sh2, ext), sh2 ? sh.blocksDS : sh.blocksD, st, d, insts, ctl, pd, pa, nParts, nParts,
+  const PartEnds pe{sh.blocksA, sh.blocksA, sh.blocksA, nParts};
+  e = launchPDL(WSB_PICK(k_plainD, P, sh2, ext), sh2 ? sh.blocksDS : sh.blocksD, st, d, insts, ctl, pd, pa, pe, nParts,
                 counter);
   if (e != cudaSuccess) return e;
   nl += 1;

@@ -14,6 +14,9 @@ struct PlainShape { int blocksA, blocksR, blocksD, blocksDS, blocksX, blocksY, b
 // stream, joined before the update, which forks again into a node kernel on `side` and a segment kernel on the main
 // stream, joined at the end of the iteration
 struct PlainFork { cudaStream_t side; cudaEvent_t fork, join, fork2, join2; };
+// where each kernel's block partials end in one plain-form iteration: split phases (crossings, rods, nodes, segments:
+// x, y, n, m) or whole phases (element phase x, update phase m; y = n = x)
+struct PartEnds { int x, y, n, m; };
 
 template <int P>
 cudaError_t launchBatched(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
