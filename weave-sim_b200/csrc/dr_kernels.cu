@@ -56,18 +56,49 @@ __device__ __forceinline__ void putPartSlots(const Part<A> &p, A *part, int b, i
   for (int i = 0; i < RX_NMAX; i++)
     if (XM & (1u << i)) part[size_t(RS_NSUM + i) * stride + b] = p.x[i];
 }
-// partial rows [lo, hi) added into q, only the slots in SM / XM; thread t takes rows lo + t, lo + t + blockDim, ...
+// partial row b added into q, only the slots in SM / XM
+template <unsigned SM, unsigned XM, class A>
+__device__ __forceinline__ void addPartRow(Part<A> &q, const A *part, int b, int stride) {
+#pragma unroll
+  for (int i = 0; i < RS_NSUM; i++)
+    if (SM & (1u << i)) q.s[i] += __ldcg(part + size_t(i) * stride + b);
+#pragma unroll
+  for (int i = 0; i < RX_NMAX; i++)
+    if (XM & (1u << i)) q.x[i] = mmax(q.x[i], __ldcg(part + size_t(RS_NSUM + i) * stride + b));
+}
+// partial rows [lo, hi) added into q, only the slots in SM / XM; thread t takes rows lo + t, lo + t + blockDim, ... in
+// that order.  Its first three rows are loaded in one unrolled batch, all in flight together, before they are added
+// (three rows of up to six slots fit the registers beside q); rows beyond follow one by one.
 template <unsigned SM, unsigned XM, class A>
 __device__ __forceinline__ void addPartSlots(Part<A> &q, const A *part, int lo, int hi, int stride) {
-#pragma unroll 2
-  for (int b = lo + threadIdx.x; b < hi; b += blockDim.x) {
+  constexpr int BATCH = 3;
+  constexpr int NS = __builtin_popcount(SM), NX = __builtin_popcount(XM);
+  A vs[BATCH][NS > 0 ? NS : 1], vx[BATCH][NX > 0 ? NX : 1];
+#pragma unroll
+  for (int r = 0; r < BATCH; r++) {
+    const int b = lo + threadIdx.x + r * blockDim.x;
+    int k = 0;
 #pragma unroll
     for (int i = 0; i < RS_NSUM; i++)
-      if (SM & (1u << i)) q.s[i] += __ldcg(part + size_t(i) * stride + b);
+      if (SM & (1u << i)) vs[r][k++] = b < hi ? __ldcg(part + size_t(i) * stride + b) : A(0);
+    k = 0;
 #pragma unroll
     for (int i = 0; i < RX_NMAX; i++)
-      if (XM & (1u << i)) q.x[i] = mmax(q.x[i], __ldcg(part + size_t(RS_NSUM + i) * stride + b));
+      if (XM & (1u << i)) vx[r][k++] = b < hi ? __ldcg(part + size_t(RS_NSUM + i) * stride + b) : A(0);
   }
+#pragma unroll
+  for (int r = 0; r < BATCH; r++) {
+    if (lo + int(threadIdx.x) + r * int(blockDim.x) >= hi) break;
+    int k = 0;
+#pragma unroll
+    for (int i = 0; i < RS_NSUM; i++)
+      if (SM & (1u << i)) q.s[i] += vs[r][k++];
+    k = 0;
+#pragma unroll
+    for (int i = 0; i < RX_NMAX; i++)
+      if (XM & (1u << i)) q.x[i] = mmax(q.x[i], vx[r][k++]);
+  }
+  for (int b = lo + threadIdx.x + BATCH * blockDim.x; b < hi; b += blockDim.x) addPartRow<SM, XM>(q, part, b, stride);
 }
 template <class A>
 __device__ __forceinline__ void addPart(Part<A> &q, const A *part, int b, int stride) {
