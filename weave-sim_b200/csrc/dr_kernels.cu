@@ -56,49 +56,23 @@ __device__ __forceinline__ void putPartSlots(const Part<A> &p, A *part, int b, i
   for (int i = 0; i < RX_NMAX; i++)
     if (XM & (1u << i)) part[size_t(RS_NSUM + i) * stride + b] = p.x[i];
 }
-// partial row b added into q, only the slots in SM / XM
+// row b of the partial range [lo, hi) added into q, only the slots in SM / XM.  A row past the range is read at hi − 1
+// instead (every range holds at least one row: each kernel launches a block or more): a repeated row leaves a maximum
+// unchanged, and its sums are not added.  The loads do not depend on b being in the range, so the rows of several
+// ranges go out together.
 template <unsigned SM, unsigned XM, class A>
-__device__ __forceinline__ void addPartRow(Part<A> &q, const A *part, int b, int stride) {
+__device__ __forceinline__ void addRangeRow(Part<A> &q, const A *part, int b, int hi, int stride) {
+  const bool in = b < hi;
+  const int bc = in ? b : hi - 1;
 #pragma unroll
   for (int i = 0; i < RS_NSUM; i++)
-    if (SM & (1u << i)) q.s[i] += __ldcg(part + size_t(i) * stride + b);
+    if (SM & (1u << i)) {
+      const A v = __ldcg(part + size_t(i) * stride + bc);
+      q.s[i] += in ? v : A(0);
+    }
 #pragma unroll
   for (int i = 0; i < RX_NMAX; i++)
-    if (XM & (1u << i)) q.x[i] = mmax(q.x[i], __ldcg(part + size_t(RS_NSUM + i) * stride + b));
-}
-// partial rows [lo, hi) added into q, only the slots in SM / XM; thread t takes rows lo + t, lo + t + blockDim, ... in
-// that order.  Its first three rows are loaded in one unrolled batch, all in flight together, before they are added
-// (three rows of up to six slots fit the registers beside q); rows beyond follow one by one.
-template <unsigned SM, unsigned XM, class A>
-__device__ __forceinline__ void addPartSlots(Part<A> &q, const A *part, int lo, int hi, int stride) {
-  constexpr int BATCH = 3;
-  constexpr int NS = __builtin_popcount(SM), NX = __builtin_popcount(XM);
-  A vs[BATCH][NS > 0 ? NS : 1], vx[BATCH][NX > 0 ? NX : 1];
-#pragma unroll
-  for (int r = 0; r < BATCH; r++) {
-    const int b = lo + threadIdx.x + r * blockDim.x;
-    int k = 0;
-#pragma unroll
-    for (int i = 0; i < RS_NSUM; i++)
-      if (SM & (1u << i)) vs[r][k++] = b < hi ? __ldcg(part + size_t(i) * stride + b) : A(0);
-    k = 0;
-#pragma unroll
-    for (int i = 0; i < RX_NMAX; i++)
-      if (XM & (1u << i)) vx[r][k++] = b < hi ? __ldcg(part + size_t(RS_NSUM + i) * stride + b) : A(0);
-  }
-#pragma unroll
-  for (int r = 0; r < BATCH; r++) {
-    if (lo + int(threadIdx.x) + r * int(blockDim.x) >= hi) break;
-    int k = 0;
-#pragma unroll
-    for (int i = 0; i < RS_NSUM; i++)
-      if (SM & (1u << i)) q.s[i] += vs[r][k++];
-    k = 0;
-#pragma unroll
-    for (int i = 0; i < RX_NMAX; i++)
-      if (XM & (1u << i)) q.x[i] = mmax(q.x[i], vx[r][k++]);
-  }
-  for (int b = lo + threadIdx.x + BATCH * blockDim.x; b < hi; b += blockDim.x) addPartRow<SM, XM>(q, part, b, stride);
+    if (XM & (1u << i)) q.x[i] = mmax(q.x[i], __ldcg(part + size_t(RS_NSUM + i) * stride + bc));
 }
 template <class A>
 __device__ __forceinline__ void addPart(Part<A> &q, const A *part, int b, int stride) {
@@ -467,17 +441,25 @@ constexpr unsigned updateMaxs(int part, bool ext) {
          (ext && part != 2 ? MAXS_FLOOR : 0u);
 }
 // every block partial of one iteration, in ranges of fixed order, each read only in the slots its kernel feeds (the
-// others hold nothing): SPLIT, the four kernels of the split phases; else the two whole phases
+// others hold nothing): SPLIT, the four kernels of the split phases; else the two whole phases.  In round o thread t
+// reads row o + t of every range at once, so the close takes as many rounds of loads as the longest range has rows
+// per thread (one for a small instance), not the sum over the ranges.
 template <bool SPLIT, bool EXT, class A>
 __device__ __forceinline__ void reduceIteration(Part<A> &q, const A *part, int ex, int ey, int en, int em, int stride) {
   if constexpr (SPLIT) {
-    addPartSlots<elemSums(1), elemMaxs(1)>(q, part, 0, ex, stride);
-    addPartSlots<elemSums(2), elemMaxs(2)>(q, part, ex, ey, stride);
-    addPartSlots<updateSums(1, EXT), updateMaxs(1, EXT)>(q, part, ey, en, stride);
-    addPartSlots<updateSums(2, EXT), updateMaxs(2, EXT)>(q, part, en, em, stride);
+    const int len = max(max(ex, ey - ex), max(en - ey, em - en));
+    for (int o = threadIdx.x; o < len; o += blockDim.x) {
+      addRangeRow<elemSums(1), elemMaxs(1)>(q, part, o, ex, stride);
+      addRangeRow<elemSums(2), elemMaxs(2)>(q, part, ex + o, ey, stride);
+      addRangeRow<updateSums(1, EXT), updateMaxs(1, EXT)>(q, part, ey + o, en, stride);
+      addRangeRow<updateSums(2, EXT), updateMaxs(2, EXT)>(q, part, en + o, em, stride);
+    }
   } else {
-    addPartSlots<elemSums(0), elemMaxs(0)>(q, part, 0, ex, stride);
-    addPartSlots<updateSums(0, EXT), updateMaxs(0, EXT)>(q, part, ex, em, stride);
+    const int len = max(ex, em - ex);
+    for (int o = threadIdx.x; o < len; o += blockDim.x) {
+      addRangeRow<elemSums(0), elemMaxs(0)>(q, part, o, ex, stride);
+      addRangeRow<updateSums(0, EXT), updateMaxs(0, EXT)>(q, part, ex + o, em, stride);
+    }
   }
 }
 // One kernel per phase over the elements of instance 0; block partials go to part[block] and the last block of the
