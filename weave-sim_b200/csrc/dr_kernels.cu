@@ -16,8 +16,11 @@
 #ifndef WSB_MINB_D
 #define WSB_MINB_D 4
 #endif
+// The rod kernel's block: 512 threads at 2 blocks per SM (64 registers) in the mixed and FP32 policies, which halves
+// its block partials against 256 × 4 at the same occupancy; 256 threads at 3 blocks per SM in FP64.
+#define WSB_Y_THREADS(P) ((P) == PREC_F64 ? 256 : 512)
 #ifndef WSB_MINB_Y
-#define WSB_MINB_Y(P) ((P) == PREC_F64 ? 3 : 4)
+#define WSB_MINB_Y(P) ((P) == PREC_F64 ? 3 : 2)
 #endif
 #ifndef WSB_MINB_XY
 #define WSB_MINB_XY 2
@@ -503,7 +506,7 @@ __global__ void __launch_bounds__(128) k_plainX(Dev<P> d, const InstDesc *__rest
   plainA<P, SHORT, EXT, 1>(d, insts, ctl, part, partStride, blockIdx.x, gridDim.x);
 }
 template <int P, bool SHORT>
-__global__ void __launch_bounds__(256, WSB_MINB_Y(P)) k_plainY(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
+__global__ void __launch_bounds__(WSB_Y_THREADS(P), WSB_MINB_Y(P)) k_plainY(Dev<P> d, const InstDesc *__restrict__ insts, const InstCtl *__restrict__ ctl,
                                                 typename Dev<P>::A *part, int partStride) {
   plainA<P, SHORT, false, 2>(d, insts, ctl, part, partStride, blockIdx.x, gridDim.x);
 }
@@ -1027,18 +1030,20 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
   if (fork && contacts) {
     // crossings on a forked branch, segments / joints / clamps on the main one, joined before the update; the update
     // forks again: nodes on the side branch, segments and side ranks on the main one
-    const int nDN = sh2 ? sh.blocksDNS : sh.blocksDN, nParts = sh.blocksX + sh.blocksY + nDN + sh.blocksDM;
-    A *px = static_cast<A *>(part), *py = px + sh.blocksX, *pn = py + sh.blocksY, *pm = pn + nDN;
+    // rod blocks of WSB_Y_THREADS(P): ceil(elements / 512) = ceil(blocksY / 2) (blocksY counts blocks of 256)
+    const int nbY = WSB_Y_THREADS(P) == 256 ? sh.blocksY : (sh.blocksY + 1) / 2;
+    const int nDN = sh2 ? sh.blocksDNS : sh.blocksDN, nParts = sh.blocksX + nbY + nDN + sh.blocksDM;
+    A *px = static_cast<A *>(part), *py = px + sh.blocksX, *pn = py + nbY, *pm = pn + nDN;
     const unsigned nB = unsigned(nDN + sh.blocksDM);
-    const PartEnds pe{sh.blocksX, sh.blocksX + sh.blocksY, sh.blocksX + sh.blocksY + nDN, nParts};
+    const PartEnds pe{sh.blocksX, sh.blocksX + nbY, sh.blocksX + nbY + nDN, nParts};
     cudaError_t e;
     if ((e = cudaEventRecord(fork->fork, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(fork->side, fork->fork, 0)) != cudaSuccess) return e;
     const auto kx = WSB_PICK(k_plainX, P, sh2, ext);
     kx<<<sh.blocksX, 128, 0, fork->side>>>(d, insts, ctl, px, nParts);
     if ((e = cudaEventRecord(fork->join, fork->side)) != cudaSuccess) return e;
-    if (sh2) k_plainY<P, true><<<sh.blocksY, 256, 0, st>>>(d, insts, ctl, py, nParts);
-    else k_plainY<P, false><<<sh.blocksY, 256, 0, st>>>(d, insts, ctl, py, nParts);
+    if (sh2) k_plainY<P, true><<<nbY, WSB_Y_THREADS(P), 0, st>>>(d, insts, ctl, py, nParts);
+    else k_plainY<P, false><<<nbY, WSB_Y_THREADS(P), 0, st>>>(d, insts, ctl, py, nParts);
     if ((e = cudaStreamWaitEvent(st, fork->join, 0)) != cudaSuccess) return e;
     int nl = 2;
     if (!sh2) {
