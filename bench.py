@@ -41,7 +41,7 @@ def bytes_per_iter(n, m, K):
 
 # DRAM bytes (read + write) of one iteration of this workload in the mixed plain form, summed over its four kernels from
 # a cold-cache `ncu --set full` capture of one launch each (the plain-form summary under profiles/)
-TRAFFIC_PER_ITER = (4.15 + 9.75 + 6.49 + 10.54) * 1e6
+TRAFFIC_PER_ITER = (4.15 + 9.75 + 6.49 + 10.53) * 1e6
 
 
 def peaks():
