@@ -28,10 +28,16 @@ sys.path.insert(0, ROOT)
 
 METRIC = "solves/s and DR iters/s at ≤1e-4·span error vs f64; p50/p99 solve latency"
 UNIT = "DR iters/s"
-WORKLOAD = {"workload": "shell_large: 20 m hexagonal Kagome plan, 60 laths/family at 0.33 m, 3.8 cm segments, "
+SHELL_FIXTURE = os.path.join(ROOT, "oracle", "scenes", "shell_large.npz")
+
+
+def bench_config(args, world):
+    """the workload, the same in both arms (the arithmetic of each arm is in its `dtype`)"""
+    return {"workload": "shell_large: 20 m hexagonal Kagome plan, 60 laths/family at 0.33 m, 3.8 cm segments, "
                         "supports lifted 0-2 m (81180 nodes, 81000 segments, 8190 crossings)",
-            "precision": "FP32 element math + two-float positions/frames + FP64 reductions",
-            "l2": "flushed between timed steps (256 MiB write)"}
+            "nodes": 81180, "segments": 81000, "crossings": 8190, "chunk_iters": args.chunk,
+            "step": f"one chunk of {args.chunk} DR iterations of the shell",
+            "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"instance replicas x{world}"}
 
 # algorithmic bytes of one DR iteration: minimal state traffic if every state array is streamed once
 # (node 112 B, segment 168 B, crossing 96 B per iteration)
@@ -140,7 +146,7 @@ def run_ours(args, rank, world, local):
     md = ws.configs.shell_large()
     n, m, K = md.n, md.m, md.K
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
-    s = ws.GpuSolver([md], precision=args.precision, form=args.form, device=local)
+    s = ws.GpuSolver([md.copy()], precision=args.precision, form=args.form, device=local)
     for _ in range(args.warmup):
         s.step(args.chunk, read=False)
         s.last_step_stats()
@@ -159,6 +165,7 @@ def run_ours(args, rank, world, local):
     barrier(world)
     total_ms = allmax(sum(times), world)
     ctl = s.read_control()[0]
+    err = error_vs_f64(md, s.download(0, fields=("X", "u", "stuck")), ctl["iter"], local)
     # end to end through the C ABI with host buffers: upload state, relax one chunk, download the result (positions,
     # frames, slide coordinates, contact normals and stick/slip: what a caller reads back, and warm-starts from)
     result_fields = ("X", "Q", "u", "nprev", "stuck", "state")
@@ -190,17 +197,52 @@ def run_ours(args, rank, world, local):
                      "note": "one DR iteration (four kernels, two pairs on forked graph branches) is the unit: algorithmic "
                              "state bytes per iteration / device time per iteration; traffic = DRAM bytes read + written "
                              "per iteration, summed over the four kernels from one cold-cache ncu capture"},
-        "clocks": clk.summary(), "sizes": {"n": n, "m": m, "K": K},
+        "clocks": clk.summary(), "sizes": {"n": n, "m": m, "K": K}, "error_vs_f64": err,
     }
+
+
+PRECISION_NOTE = {"mixed": "FP32 element math + two-float positions/frames + FP64 reductions", "f64": "FP64 throughout",
+                  "f32": "naive FP32 throughout"}
+
+
+def error_vs_f64(md, st, iters, device):
+    """the timed run's result against FP64 at the same iteration: the shell relaxed from the same start for the same
+    iterations in FP64 (the plain form, which the GPU tests hold to the f64 oracle), max node distance / span, slide
+    coordinates and stick/slip states; beside it the chaos floor, FP64 against FP64 started with every coordinate moved
+    by N(0, (1e-9 span)^2)"""
+    import numpy as np
+    import weavesim_b200 as ws
+
+    def run(model):
+        r = ws.GpuSolver([model], precision="f64", form="plain", device=device)
+        r.step(iters, read=False)
+        out = r.download(0, fields=("X", "u", "stuck"))
+        r.dispose()
+        return out
+
+    def cmp(a, b):
+        d = np.linalg.norm((a["X"] - b["X"]).reshape(-1, 3), axis=1)
+        return {"pos_max_span": float(d.max() / md.span), "slide_max_segments": float(np.abs(a["u"] - b["u"]).max()),
+                "stick_slip_mismatch": int(np.sum(a["stuck"] != b["stuck"]))}
+
+    ref = run(md.copy())
+    pert = md.copy()
+    pert.X = pert.X + 1e-9 * md.span * np.random.default_rng(7).standard_normal(pert.X.shape)
+    out = cmp(st, ref)
+    floor = cmp(run(pert), ref)
+    return dict(out, iterations=int(iters), crossings=int(md.K), within_1e_4_span=out["pos_max_span"] <= 1e-4,
+                chaos_floor=floor)
 
 
 def cpu_replicas(iters_per_replica, threads):
     """the reference's CPU algorithm (oracle/: f64 restatement of web/js/solver_cpu.js) on `threads` host threads, one
-    replica of the workload each; returns aggregate DR iterations per second"""
+    replica of the workload each; returns aggregate DR iterations per second.  The shell is read from the oracle's
+    scene fixture (made by the package's scene builder, oracle/scenes/make_scenes.py), so this leg loads the oracle's
+    library alone, never the CUDA library."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import weavesim_b200 as ws
     from oracle import Oracle
-    md = ws.configs.shell_large()
+    md = ws.Model.load(SHELL_FIXTURE)
     ors = [Oracle(md.copy()) for _ in range(threads)]
     for o in ors:
         o.step(1)
@@ -266,7 +308,7 @@ def run_reference(args, rank, world):
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * cores * args.ref_iters / value, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": dict(WORKLOAD, precision="f64 (CPU)"), "impl": "reference",
+            "config": bench_config(args, world), "impl": "reference",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
@@ -343,10 +385,10 @@ def main():
     out = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": {"mixed": "f32+two-float+f64", "f64": "f64", "f32": "f32"}[args.precision], "data": "synthetic (seeded)",
-           "config": dict(WORKLOAD, chunk_iters=args.chunk, form=args.form, nodes=r["sizes"]["n"],
-                          segments=r["sizes"]["m"], crossings=r["sizes"]["K"], parallelism=f"replicas x{world}"),
+           "config": bench_config(args, world), "form": args.form, "precision": PRECISION_NOTE[args.precision],
            "e2e": r["e2e"], "gpu_launches": r["launches"], "roofline": r["roofline"], "cpu_baseline": cpu,
-           "clocks": r["clocks"], "residual_after": r["ctl"]["residual"], "iterations_after": r["ctl"]["iter"]}
+           "clocks": r["clocks"], "error_vs_f64": r["error_vs_f64"], "residual_after": r["ctl"]["residual"],
+           "iterations_after": r["ctl"]["iter"]}
     print(json.dumps(out), flush=True)
 
 

@@ -277,7 +277,7 @@ typedef struct ws_ctx ws_ctx;
 typedef struct ws_opts {
   int32_t precision;    /* WS_PREC_* */
   int32_t form;         /* WS_FORM_* */
-  int32_t threads;      /* threads per block (0: autotuned) */
+  int32_t threads;      /* threads per block of the batched form (0: 512 with shared-memory state, 256 with global) */
   int32_t device;       /* CUDA device ordinal */
   uint64_t budget_bytes;/* device memory this context may take (0: no limit) */
   int32_t cta_state;    /* batched form: WS_CTA_AUTO keeps each instance's changing state in shared memory when every
@@ -366,12 +366,16 @@ int ws_internalize(ws_ctx *ctx, int32_t instance);
  * No counterpart in the reference.  The instance's whole device footprint lives in one static array of
  * WS_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds until exit; models that need more are rejected
  * with WS_ERR_ARG.  The call builds the goals, clears the array, uploads `model`, runs n_iter iterations of the batched
- * kernel on `stream` (NULL: the default stream), waits for them and fills `out` and `ctl` (either may be NULL); the
- * result equals ws_create + ws_step + ws_download with the same threads.  It allocates no device memory.
- * The first call on a device looks up the array's device address there (cudaGetSymbolAddress); make that first call
- * before any stream capture.  Every call shares the array and leaves its contents behind: calls from this process take
- * turns on a lock, but calls whose GPU work overlaps (several processes, or this entry point mixed with raw launches that
- * touch the array) race. */
+ * kernel on `stream` (NULL: the default stream; a stream of another device than the current one is rejected with
+ * WS_ERR_ARG), waits for them and fills `out` and `ctl` (either may be NULL).  The result is bit for bit that of
+ * ws_create with opts.form = WS_FORM_CTA, opts.cta_state = 1 (global state) and the same `threads` (0 here: 256),
+ * followed by ws_step and ws_download.  The call allocates no device memory; the array itself is reserved when the
+ * driver loads the library's device code on a device, which with CUDA's lazy module loading happens at the first call
+ * there: make one call (n_iter = 0 will do) at start-up, before a pool takes the device's memory, and before any stream
+ * capture.  Every call looks up the array's device address on the current device (cudaGetSymbolAddress), so a device
+ * reset in between is harmless.  Every call shares the array and leaves its contents behind: calls from this process
+ * take turns on a lock, but calls whose GPU work overlaps (several processes, or this entry point mixed with raw
+ * launches that touch the array) race. */
 #define WS_NOALLOC_SCRATCH_BYTES (16u << 20)
 int ws_relax_noalloc(const ws_model *model, int32_t precision, int32_t n_iter, int32_t threads, void *stream,
                      ws_state_out *out, ws_control *ctl);

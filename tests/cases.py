@@ -8,7 +8,9 @@
 """
 from __future__ import annotations
 
+import json
 import math
+import os
 
 import numpy as np
 
@@ -156,3 +158,13 @@ def permute_nodes(md, seed=0):
 def unpermute(X, perm):
     """node positions of a permuted model back in the original numbering"""
     return X.reshape(-1, 3)[perm].reshape(-1)
+
+
+def record(name, data):
+    """append one named result (a JSON line) to the file WEAVESIM_PARITY_RECORD names, when it is set: the raw numbers
+    behind the tolerances of the parity tests"""
+    path = os.environ.get("WEAVESIM_PARITY_RECORD")
+    if not path:
+        return
+    with open(path, "a") as f:
+        f.write(json.dumps({"test": name, **data}) + "\n")

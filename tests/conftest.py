@@ -25,3 +25,4 @@ def oracle_mod():
     import oracle
     oracle.build()
     return oracle
+

@@ -1,7 +1,8 @@
 """Makes the scene fixture of the reference's example scene examples/scenes/dome_basic.json: its parameters
 (dome_basic_scene.json, the mesh path pointed at the welded mesh below) and its mesh, read, scaled and welded as the
-reference reads it (dome_basic_mesh.npz: V [3 nV], F [3 nF]).  Run from the repository root where the reference
-checkout is present:  python tests/golden/make_scene_fixture.py /path/to/reference
+reference reads it (dome_basic_mesh.npz: V [3 nV], F [3 nF]).  Run where a checkout of the reference is present, naming
+it by argument or by the environment variable WEAVESIM_REFERENCE:
+    python tests/golden/make_scene_fixture.py /path/to/weave-sim
 """
 import json
 import os
@@ -30,4 +31,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("WEAVESIM_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_scene_fixture.py <checkout of the reference> (or set WEAVESIM_REFERENCE)")
+    main(ref)

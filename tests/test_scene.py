@@ -103,3 +103,17 @@ def test_polyline_cases():
 def test_bad_scene_arguments():
     with pytest.raises(RuntimeError, match="positive"):
         ws.kagome(side=0, subdivisions=4, edge=0.4, width=0.04, height=0.004, E=1e10, G=6e8, density=500)
+
+
+def test_shell_fixture_is_the_scene_builders_shell():
+    """the CPU side of the benchmark reads the 20 m shell from oracle/scenes/shell_large.npz (so that process never loads
+    the CUDA library); the fixture must be exactly what the scene builder makes"""
+    import os
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "scenes", "shell_large.npz")
+    a, b = ws.Model.load(path), ws.configs.shell_large()
+    assert (a.n, a.m, a.p, a.K, a.n_strands, a.span) == (b.n, b.m, b.p, b.K, b.n_strands, b.span)
+    assert a.params == b.params
+    for k, v in b.__dict__.items():
+        if isinstance(v, np.ndarray):
+            w = getattr(a, k)
+            assert w.dtype == v.dtype and np.array_equal(w, v), k

@@ -238,10 +238,45 @@ class Model:
         return self
 
     def copy(self) -> "Model":
-        other = Model()
+        other = Model.__new__(Model)
         for k, v in self.__dict__.items():
             setattr(other, k, v.copy() if isinstance(v, (np.ndarray, dict)) else v)
         return other
+
+    COUNTS = ("n", "m", "p", "n_strands", "K")
+
+    def save(self, path):
+        """the model as a compressed .npz: every array, the counts, the span and the parameters (no load protocol)"""
+        if self.protocol:
+            raise ValueError("Model.save: a model with a load protocol is not saved")
+        arrays = {k: v for k, v in self.__dict__.items() if isinstance(v, np.ndarray)}
+        meta = {f"count_{k}": np.int64(getattr(self, k)) for k in self.COUNTS}
+        np.savez_compressed(path, **arrays, **meta, span=np.float64(self.span),
+                            param_keys=np.array(list(self.params)), param_values=np.array(list(self.params.values()),
+                                                                                           dtype=np.float64))
+
+    @classmethod
+    def load(cls, path) -> "Model":
+        """a model saved by ``save``; reading it does not load the solver library"""
+        self = cls.__new__(cls)
+        with np.load(path) as z:
+            for k in self.COUNTS:
+                setattr(self, k, int(z[f"count_{k}"]))
+            self.span = float(z["span"])
+            ints = {f[0] for f in WsParams._fields_ if f[1] is C.c_int32}
+            self.params = {str(k): (int(v) if str(k) in ints else float(v))
+                           for k, v in zip(z["param_keys"], z["param_values"])}
+            self.protocol = None
+            self.node_offset = z["node_offset"].copy() if "node_offset" in z else None
+            for k in self.FLOAT + self.INT + self.BYTE:
+                setattr(self, k, z[k].copy() if k in z else None)
+        for k in self.INT + self.BYTE:
+            if getattr(self, k) is None:
+                raise ValueError(f"Model.load: {path} has no {k}")
+        for k in self.FLOAT:
+            if getattr(self, k) is None and k not in self.OPTIONAL:
+                raise ValueError(f"Model.load: {path} has no {k}")
+        return self
 
     def struct(self) -> WsModel:
         """A WsModel pointing into this object's arrays (keep the Model alive while the struct is used)."""

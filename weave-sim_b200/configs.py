@@ -8,7 +8,9 @@
 * ``dome_stiff``   — ``dome_small`` with 25×3 mm laths, E 12 GPa, per-crossing μ ~ U(0.1, 0.5).
 * ``batch_mixed``  — independent gridshells drawn from a seed: laths per family U{6..40}, span U(2, 12) m, thickness
                      U(3, 6) mm, width U(30, 60) mm, E U(8, 14) GPa, μ U(0.1, 0.5), inward displacement U(3 %, 10 %)
-                     of the span, ~5 cm segments.
+                     of the span, ~5 cm segments.  The inward displacement is read as the reduction of the span: the
+                     supports on opposite sides each move radially by half of it, so every support moves by
+                     U(1.5 %, 5 %) of the span.
 
 Contact penalties (strength = stick_strength = 1e5 N/m) follow the reference's thin-lath example scene
 (examples/scenes/dualv5dome_cm.json: 40 mm laths, 1000 N/cm); its default 1e4 N/mm belongs to 60×30 mm sections.
@@ -67,7 +69,7 @@ def batch_draw(rng: np.random.Generator):
     w = float(rng.uniform(0.030, 0.060))
     E = float(rng.uniform(8e9, 14e9))
     mu = float(rng.uniform(0.1, 0.5))
-    inward = float(rng.uniform(0.03, 0.10)) * span * 0.5
+    inward = float(rng.uniform(0.03, 0.10)) * span * 0.5     # radial move of each support: half the span reduction
     return dict(side=side, subdivisions=_sub(edge, 0.05), edge=edge, width=w, height=t, E=E, G=0.06 * E,
                 density=500.0, mu=mu, inward=inward, z_noise=0.001, gravity=True,
                 seed=int(rng.integers(1, 2 ** 31)), params=default_params(disp_ramp_iter=3000, max_iter=50000, strength=1e5, stick_strength=1e5))

@@ -23,22 +23,17 @@ int runInPlace(int prec, const HostGoals &g, char *base, int nIter, int threads,
 static __device__ __align__(256) unsigned char g_noalloc_scratch[WS_NOALLOC_SCRATCH_BYTES];
 
 namespace {
-constexpr int kMaxDevices = 64;
 std::mutex g_mu;                          // host calls take turns: every call uses the same array
-void *g_addr[kMaxDevices] = {nullptr};    // device address of the array, per device, found at the first call there
 
-// the array's device address on `dev` (the current device): in host code the symbol is only a host-side stand-in, so
-// the address comes from cudaGetSymbolAddress, once per device
-int scratchAddress(int dev, void **out) {
-  if (dev < 0 || dev >= kMaxDevices) return wsb::fail(WS_ERR_ARG, "ws_relax_noalloc: device ordinal out of range");
-  if (!g_addr[dev]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      return wsb::fail(WS_ERR_CUDA, std::string("ws_relax_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
-    g_addr[dev] = p;
-  }
-  *out = g_addr[dev];
+// the array's device address on the current device: in host code the symbol is only a host-side stand-in, so the
+// address comes from cudaGetSymbolAddress.  It is looked up on every call (cheap once the device code is loaded), so
+// a device reset that reloads the module at another address cannot leave a stale pointer behind.
+int scratchAddress(void **out) {
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    return wsb::fail(WS_ERR_CUDA, std::string("ws_relax_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+  *out = p;
   return WS_OK;
 }
 }  // namespace
@@ -63,8 +58,17 @@ extern "C" int ws_relax_noalloc(const ws_model *model, int32_t precision, int32_
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return wsb::fail(WS_ERR_NODEV, std::string("ws_relax_noalloc: no CUDA device: ") + cudaGetErrorString(e));
+  if (stream) {
+    // the scratch address belongs to the current device: a stream of another device would run on the wrong memory
+    int sdev = -1;
+    e = cudaStreamGetDevice(static_cast<cudaStream_t>(stream), &sdev);
+    if (e != cudaSuccess) return wsb::fail(WS_ERR_ARG, std::string("ws_relax_noalloc: bad stream: ") + cudaGetErrorString(e));
+    if (sdev != dev)
+      return wsb::fail(WS_ERR_ARG, "ws_relax_noalloc: the stream belongs to device " + std::to_string(sdev) +
+                       ", the current device is " + std::to_string(dev));
+  }
   void *base = nullptr;
-  int rc = scratchAddress(dev, &base);
+  int rc = scratchAddress(&base);
   if (rc != WS_OK) return rc;
   std::string err;
   rc = wsb::runInPlace(precision, g, static_cast<char *>(base), n_iter, threads, static_cast<cudaStream_t>(stream), out, ctl, err);

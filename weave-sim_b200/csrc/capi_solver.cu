@@ -1260,6 +1260,10 @@ int ws_destroy(ws_ctx *c) {
 // entry point (capi_noalloc.cu); nothing here allocates device memory.
 namespace wsb {
 
+// the end of the arena inside caller-provided memory: the same 4096 spare bytes after the last array as ws_create's
+// arena has, then 256-byte alignment for the descriptor and control block that follow
+static size_t arenaEnd(size_t carved) { return (carved + 4096 + 255) & ~size_t(255); }
+
 size_t instanceFootprint(int prec, const HostGoals &g) {
   Sizes z;
   z.n = g.n; z.m = g.m; z.p = g.p; z.c = g.C; z.k = g.K; z.s = g.S; z.b = 1;
@@ -1270,7 +1274,7 @@ size_t instanceFootprint(int prec, const HostGoals &g) {
     default: { Dev<PREC_F32> d{}; layout<PREC_F32>(d, cv, z); break; }
   }
   const size_t tail = ((sizeof(InstDesc) + 255) & ~size_t(255)) + ((sizeof(InstCtl) + 255) & ~size_t(255));
-  return ((cv.off + 255) & ~size_t(255)) + tail;
+  return arenaEnd(cv.off) + tail;
 }
 
 template <int P>
@@ -1278,7 +1282,7 @@ static void runInPlaceImpl(ws_ctx *c, char *base, int nIter, int threads, ws_sta
   Carver cv{base};
   layout<P>(devOf<P>(c), cv, c->z);
   c->dExt = devOf<P>(c).ext;
-  const size_t off = (cv.off + 255) & ~size_t(255);
+  const size_t off = arenaEnd(cv.off);
   c->dInst = reinterpret_cast<InstDesc *>(base + off);
   c->dCtl = reinterpret_cast<InstCtl *>(base + off + ((sizeof(InstDesc) + 255) & ~size_t(255)));
   CK(cudaMemsetAsync(base, 0, off, c->st));

@@ -29,3 +29,30 @@ def greedy_split(weights, world):
 def shard_for(rank, world, models):
     """the instance indices of `rank` (the same answer on every rank: deterministic, no communication needed)"""
     return greedy_split([instance_weight(m) for m in models], world)[rank]
+
+
+def relax_sharded(models, relax, rank, world, group=None):
+    """every rank relaxes its share of `models` with `relax(list of models) -> list of results` (one per model, any
+    picklable value) and rank 0 gathers them; returns, on rank 0, the results in the order of `models` (None elsewhere).
+    The only communication is the host-side gather after the relaxation (torch.distributed.gather_object over the
+    process group: gloo on the host, or the NCCL group of the GPU ranks)."""
+    import torch.distributed as dist
+    mine = shard_for(rank, world, models)
+    res = relax([models[i] for i in mine])
+    if len(res) != len(mine):
+        raise ValueError("relax_sharded: one result per model expected")
+    if world == 1:
+        return list(res)
+    box = [None] * world if rank == 0 else None
+    dist.gather_object(list(zip(mine, res)), box, dst=0, group=group)
+    if rank != 0:
+        return None
+    out = [None] * len(models)
+    for part in box:
+        for i, r in part:
+            if out[i] is not None:
+                raise RuntimeError(f"relax_sharded: instance {i} came back from two ranks")
+            out[i] = r
+    if any(r is None for r in out):
+        raise RuntimeError("relax_sharded: an instance came back from no rank")
+    return out

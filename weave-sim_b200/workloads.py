@@ -5,8 +5,8 @@
   math, two-float state, FP64 reductions) and in naive FP32.  Reported against FP64: max node position error / span,
   slide-coordinate error, stick/slip mismatches; and the chaos floor: FP64 against FP64 started 1 nm away.
 * ``batch`` — 512 independent gridshells drawn from a seed (laths per family U{6..40}, span U(2, 12) m, thickness
-  U(3, 6) mm, width U(30, 60) mm, E U(8, 14) GPa, μ U(0.1, 0.5), inward displacement U(3, 10) % of the span, ~5 cm
-  segments), one thread block each, relaxed together to the iteration cap.
+  U(3, 6) mm, width U(30, 60) mm, E U(8, 14) GPa, μ U(0.1, 0.5), inward displacement U(3, 10) % of the span (the
+  span's reduction: each support moves radially by half of it), ~5 cm segments), relaxed together to the iteration cap.
 * ``ratio`` — the batched form (592 domes) against the plain single-instance form on the 3 m dome.
 * ``serve`` — the serving loop under Poisson arrivals at the given rates: fresh stiff domes (new seed each) and, with
   probability 0.3, variants (±5 % E, ±0.1 μ, ±2 % support displacement) of a resident equilibrium, warm-started.
