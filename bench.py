@@ -322,7 +322,7 @@ def run_workload(args):
             r = workloads.run_precision(instances=args.instances or 64)
             metric = "position / slide / stick-slip agreement with FP64 after the 5000-iteration cap, and throughput"
         elif args.workload == "batch":
-            r = workloads.run_batch(count=args.instances or 512)
+            r = workloads.run_batch(count=args.instances or 512, wide_cluster=args.wide_cluster)
             metric = "solves/s and DR iters/s of 512 mixed gridshells to the 5000-iteration cap"
         elif args.workload == "ratio":
             r = workloads.run_ratio()
@@ -363,6 +363,7 @@ def main():
                     help="shell_large: the headline line; the others measure the stiff-dome precision variants, the "
                          "512-gridshell mixed batch and the serving loop (single GPU)")
     ap.add_argument("--instances", type=int, default=0, help="instances of the precision / batch workloads")
+    ap.add_argument("--wide-cluster", type=int, default=0, help="batch workload: blocks per wide instance (1: none)")
     args = ap.parse_args()
     if args.workload != "shell_large":
         run_workload(args)

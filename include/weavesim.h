@@ -161,6 +161,8 @@ typedef struct ws_control {
   int32_t utm_inc;     /* load increments recorded (ws_protocol) */
   int32_t utm_phase;   /* 0 settling, 1 averaging, 2 finished */
   double e_floor;      /* the ground's spring energy (Floor.energy) */
+  double t_start_ms;   /* batched form: when the instance's block (or cluster) took it up in the last ws_step, and */
+  double t_end_ms;     /* when it left it, in ms after the earliest start of that step (device timer); other forms 0 */
 } ws_control;
 
 /* ------------------------------------------------------------------------------------------------ errors */
@@ -286,6 +288,10 @@ typedef struct ws_opts {
   int32_t side_order;   /* WS_SIDES_AUTO: the short-slide side order when the slide limit (contact epsilon) is under half
                            the shortest segment of the strands with crossings, else the general order;
                            WS_SIDES_GENERAL: always the general order */
+  int32_t wide_cluster; /* batched form: thread blocks (of 512 threads) in the cluster that relaxes one wide instance,
+                           2..8; 1: every instance in one block; 0: the default (2) */
+  int32_t wide_min;     /* batched form: an instance is wide when its nodes + segments reach this (0: the default,
+                           32768); an instance with a load protocol is never wide */
 } ws_opts;
 enum { WS_SIDES_AUTO = 0, WS_SIDES_GENERAL = 1 };
 enum { WS_CTA_AUTO = 0, WS_CTA_GLOBAL = 1 };
@@ -388,6 +394,9 @@ int ws_side_order(const ws_ctx *ctx);
 /* 1 when the batched form holds its instances in shared memory (the resident form), else 0.  No counterpart in the
  * reference. */
 int ws_cta_resident(const ws_ctx *ctx);
+/* batched form: the number of wide instances (each relaxed by a thread-block cluster) and, in *cluster (may be NULL),
+ * the blocks per cluster (0 when there are none) */
+int ws_wide_instances(const ws_ctx *ctx, int32_t *cluster);
 /* device bytes held by the context */
 uint64_t ws_device_bytes(const ws_ctx *ctx);
 /* GPU time of the last ws_step (ms, CUDA events on the context's stream) and the number of kernel launches it made */

@@ -4,7 +4,7 @@ The benchmarked configurations, each checked past the 300-iteration warm-up that
 (web/js/solver_cpu.js:775-776) and into the contact ramp (1500 iterations) and the support motion:
 
 * the 20 m shell (the headline workload): FP64 in the plain and grid forms with the oracle's iteration and roll-back
-  counts and within 1e-9 of the span, slide coordinates within 1e-9 segments, the same stick/slip states, at 330,
+  counts and within 1e-9 of the span, slide coordinates within 1e-6 segments, the same stick/slip states, at 330,
   1000 and 2000 iterations; the mixed policy (FP32 element math, two-float state, FP64 reductions) within the
   1e-4 span gate wherever the oracle's own chaos floor (the oracle started 1e-9 of the span away) is below it;
 * the stiff dome (25 x 3 mm laths, E 12 GPa, per-crossing mu ~ U(0.1, 0.5)): FP64 exact to 1500 iterations in the
@@ -28,6 +28,11 @@ pytestmark = pytest.mark.gpu
 
 HORIZONS = (330, 1000, 2000)
 GATE = 1e-4                 # max node distance / span, the acceptance gate of the mixed policy
+# FP64 against the oracle at depth: positions within 1e-9 of the span; slide coordinates (in segments) within 1e-6.  The
+# slides are where the trajectory's chaos shows first: on the shell the oracle started 1e-9 of the span away differs
+# from itself by 5e-6 segments at 330 iterations and 6e-3 at 2000, while FP64 on the device (another summation order)
+# differs from the oracle by 2e-13 and 3e-8.
+SLIDE_F64 = 1e-6
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -104,7 +109,7 @@ def test_shell_f64_matches_oracle_at_depth(shell, form):
         assert g["iteration"] == v["iteration"] == h
         assert g["rollbacks"] == v["rollbacks"], h
         assert rows[h]["pos_span"] < 1e-9, (h, rows[h])
-        assert rows[h]["slide"] < 1e-9, (h, rows[h])
+        assert rows[h]["slide"] < SLIDE_F64, (h, rows[h])
         assert rows[h]["stuck_mismatch"] == 0, (h, rows[h])
 
 
@@ -118,8 +123,10 @@ def test_shell_mixed_within_gate_at_depth(shell, form):
         assert got[h]["iteration"] == h
         if floor[h]["pos_span"] < GATE:
             assert rows[h]["pos_span"] <= GATE, (h, rows[h])
-            assert rows[h]["slide"] < 1e-2, (h, rows[h])
-            assert rows[h]["stuck_mismatch"] <= max(1, md.K // 1000), (h, rows[h])
+            # slides and stick/slip states agree up to the oracle's own spread at this horizon (the stick/slip set of
+            # a chaotic trajectory is only defined to that spread)
+            assert rows[h]["slide"] <= max(1e-2, 2 * floor[h]["slide"]), (h, rows[h])
+            assert rows[h]["stuck_mismatch"] <= 2 * floor[h]["stuck_mismatch"] + max(1, md.K // 1000), (h, rows[h])
 
 
 # ------------------------------------------------------------------------------------------------ the stiff dome
@@ -134,7 +141,7 @@ def test_stiff_dome_f64_matches_oracle(oracle_mod, form):
     for h in ref:
         assert got[h]["iteration"] == ref[h]["iteration"] == h
         assert got[h]["rollbacks"] == ref[h]["rollbacks"], h
-        assert rows[h]["pos_span"] < 1e-9 and rows[h]["slide"] < 1e-9 and rows[h]["stuck_mismatch"] == 0, (h, rows[h])
+        assert rows[h]["pos_span"] < 1e-9 and rows[h]["slide"] < SLIDE_F64 and rows[h]["stuck_mismatch"] == 0, (h, rows[h])
 
 
 def test_precision_policies_against_oracle(oracle_mod):
@@ -184,25 +191,83 @@ def _batch_sample():
     return [models[b] for b in picks]
 
 
-@pytest.mark.parametrize("prec", ["f64", "mixed"])
-def test_uneven_batch_sample_against_oracle(oracle_mod, prec):
+@pytest.fixture(scope="module")
+def batch_sample(oracle_mod):
     sample = _batch_sample()
-    assert sample[0].n > 20000 and sample[-1].n < 1000
     ref = [dict() for _ in sample]
     _parallel([(_oracle_horizons, (oracle_mod, m.copy(), (1000,), ref[b])) for b, m in enumerate(sample)])
-    s = ws.GpuSolver([m.copy() for m in sample], precision=prec, threads=256, cta_state="global")
+    return sample, ref
+
+
+@pytest.mark.parametrize("prec,wide_cluster", [("f64", 1), ("f64", 2), ("f64", 8), ("mixed", 1), ("mixed", 2)])
+def test_uneven_batch_sample_against_oracle(batch_sample, prec, wide_cluster):
+    """one batched launch; wide_cluster 1 keeps every instance in one block, 2 and 8 give the instances from 32768
+    nodes + segments up (the largest two of the sample) a cluster of that many blocks each"""
+    sample, ref = batch_sample
+    assert sample[0].n > 20000 and sample[-1].n < 1000
+    s = ws.GpuSolver([m.copy() for m in sample], precision=prec, threads=256, cta_state="global",
+                     wide_cluster=wide_cluster)
+    n_wide = sum(m.n + m.m >= 32768 for m in sample)
+    assert s.wide == ((n_wide, wide_cluster) if wide_cluster > 1 else (0, 0))
     ctl = s.step(1000)
     rows = []
     for b, m in enumerate(sample):
         d = _diff(s.download(b, fields=("X", "u", "stuck")), ref[b][1000], m)
         rows.append(dict(d, nodes=m.n, crossings=m.K, rollbacks=ctl[b]["rollbacks"],
-                         oracle_rollbacks=ref[b][1000]["rollbacks"]))
+                         oracle_rollbacks=ref[b][1000]["rollbacks"], device_ms=ctl[b]["t_end_ms"] - ctl[b]["t_start_ms"],
+                         start_ms=ctl[b]["t_start_ms"]))
     s.dispose()
-    cases.record(f"uneven_batch_sample_{prec}", {"instances": rows})
+    cases.record(f"uneven_batch_sample_{prec}_cluster{wide_cluster}", {"instances": rows})
     for b, r in enumerate(rows):
         assert ctl[b]["iter"] == 1000
         if prec == "f64":
             assert r["rollbacks"] == r["oracle_rollbacks"], (b, r)
-            assert r["pos_span"] < 1e-9 and r["slide"] < 1e-9 and r["stuck_mismatch"] == 0, (b, r)
+            assert r["pos_span"] < 1e-9 and r["slide"] < SLIDE_F64 and r["stuck_mismatch"] == 0, (b, r)
         else:
             assert r["pos_span"] <= GATE, (b, r)
+
+
+def test_wide_instance_is_batch_invariant_and_deterministic():
+    """a wide instance (a cluster of blocks) gives the same bits alone, in a batch with one-block instances and on a
+    rerun: its reduction order depends only on its own counts, the block size and the cluster size"""
+    big = ws.configs.dome_small(seed=21)
+    small = [ws.configs.dome_stiff(seed=5, side=3), ws.configs.dome_small(seed=9, side=3)]
+    assert all(m.n + m.m < big.n + big.m for m in small)
+    for prec in ("f64", "mixed"):
+        outs = []
+        for batch in ([big], [big], [small[0], big, small[1]]):
+            s = ws.GpuSolver([m.copy() for m in batch], precision=prec, cta_state="global", wide_cluster=4,
+                             wide_min=big.n + big.m)
+            assert s.wide == (1, 4)
+            ctl = s.step(600)
+            b = batch.index(big)
+            outs.append((ctl[b], s.download(b, fields=("X", "Q", "u", "slip", "Fn"))))
+            assert all(c["iter"] == 600 for c in ctl)
+            assert ctl[b]["t_end_ms"] > ctl[b]["t_start_ms"] >= 0.0
+            s.dispose()
+        for c, g in outs[1:]:
+            assert c["rollbacks"] == outs[0][0]["rollbacks"] and c["residual"] == outs[0][0]["residual"]
+            for k in g:
+                assert np.array_equal(g[k], outs[0][1][k]), (prec, k)
+
+
+@pytest.mark.parametrize("cluster", [2, 4, 8])
+@pytest.mark.parametrize("order", ["auto", "general"])
+def test_wide_instance_matches_oracle(oracle_mod, cluster, order):
+    """the 3 m dome relaxed by clusters of 2, 4 and 8 blocks, both side orders, FP64 against the oracle with its
+    iteration and roll-back counts"""
+    md = ws.configs.dome_small()
+    ref = {}
+    _oracle_horizons(oracle_mod, md.copy(), (400, 1000), ref)
+    s = ws.GpuSolver([md.copy()], precision="f64", cta_state="global", wide_cluster=cluster, wide_min=1,
+                     side_order=order)
+    assert s.wide == (1, cluster)
+    done = 0
+    for h in (400, 1000):
+        ctl = s.step(h - done)[0]
+        done = h
+        g = s.download(0, fields=("X", "u", "stuck"))
+        d = _diff(g, ref[h], md)
+        assert ctl["iter"] == h and ctl["rollbacks"] == ref[h]["rollbacks"], h
+        assert d["pos_span"] < 1e-9 and d["slide"] < SLIDE_F64 and d["stuck_mismatch"] == 0, (h, d)
+    s.dispose()

@@ -85,7 +85,8 @@ class WsControl(C.Structure):
                 ("ke", C.c_double), ("ke_prev", C.c_double), ("residual", C.c_double), ("res_force", C.c_double),
                 ("res_torque", C.c_double), ("fref", C.c_double), ("e_stretch", C.c_double), ("e_shear", C.c_double),
                 ("e_bend", C.c_double), ("e_twist", C.c_double), ("e_contact", C.c_double),
-                ("utm_inc", C.c_int32), ("utm_phase", C.c_int32), ("e_floor", C.c_double)]
+                ("utm_inc", C.c_int32), ("utm_phase", C.c_int32), ("e_floor", C.c_double),
+                ("t_start_ms", C.c_double), ("t_end_ms", C.c_double)]
 
     def as_dict(self):
         return {f[0]: getattr(self, f[0]) for f in self._fields_}
@@ -93,7 +94,8 @@ class WsControl(C.Structure):
 
 class WsOpts(C.Structure):
     _fields_ = [("precision", C.c_int32), ("form", C.c_int32), ("threads", C.c_int32), ("device", C.c_int32),
-                ("budget_bytes", C.c_uint64), ("cta_state", C.c_int32), ("side_order", C.c_int32)]
+                ("budget_bytes", C.c_uint64), ("cta_state", C.c_int32), ("side_order", C.c_int32),
+                ("wide_cluster", C.c_int32), ("wide_min", C.c_int32)]
 
 
 class WsStateOut(C.Structure):
@@ -145,6 +147,8 @@ def lib():
             L.ws_stream.restype = C.c_void_p
             L.ws_cta_resident.argtypes = [C.c_void_p]
             L.ws_cta_resident.restype = C.c_int
+            L.ws_wide_instances.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
+            L.ws_wide_instances.restype = C.c_int
             L.ws_side_order.argtypes = [C.c_void_p]
             L.ws_side_order.restype = C.c_int
             L.ws_device_bytes.argtypes = [C.c_void_p]

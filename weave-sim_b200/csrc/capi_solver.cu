@@ -134,7 +134,16 @@ struct ws_ctx {
   InstCtl *dCtl = nullptr;
   InstExt *dExt = nullptr;         // the load protocols' state (in the arena)
   std::vector<InstExt> extHost;
-  int *dOrder = nullptr;
+  int *dOrder = nullptr;         // batched form: the instances of the one-block kernels, longest first
+  int nNarrow = 0;               // ... and their count
+  std::vector<char> isWide;      // per instance
+  std::vector<uint8_t> ranLast;  // per instance: selected by the last ws_step's mask
+  int *dWide = nullptr;          // batched form: the wide instances (a cluster each), longest first
+  int nWide = 0;
+  int wideCl = 0;                // blocks in a wide instance's cluster (0: no wide instances)
+  int wideMin = 0;               // nodes + segments from which an instance is wide
+  cudaStream_t sideCta = nullptr;            // batched form: the one-block kernels beside the cluster kernel
+  cudaEvent_t ctaFork = nullptr, ctaJoin = nullptr;
   uint8_t *dMask = nullptr;
   void *dPart = nullptr;
   unsigned *dBar = nullptr;   // grid form: barrier counter + generation, and its timeout flag
@@ -628,6 +637,17 @@ void setupDev(ws_ctx *c) {
   uploadAll<P>(c);
 }
 
+// the earliest start of an instance in the last launch of the batched form (0: none recorded)
+unsigned long long stepStart(const ws_ctx *c) {
+  unsigned long long t0 = 0;
+  for (size_t b = 0; b < c->ctlHost.size(); b++) {
+    const InstCtl &s = c->ctlHost[b];
+    if (b < c->ranLast.size() && !c->ranLast[b]) continue;     // left out of the last step by its mask
+    if (s.tBeg && (!t0 || s.tBeg < t0)) t0 = s.tBeg;
+  }
+  return t0;
+}
+
 void readCtl(ws_ctx *c) {
   c->ctlHost.resize(c->inst.size());
   CK(cudaMemcpyAsync(c->ctlHost.data(), c->dCtl, sizeof(InstCtl) * c->inst.size(), cudaMemcpyDeviceToHost, c->st));
@@ -637,7 +657,9 @@ void readCtl(ws_ctx *c) {
   if (utm && c->dExt) CK(cudaMemcpyAsync(c->extHost.data(), c->dExt, sizeof(InstExt) * c->inst.size(), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
 }
-void fillControl(const InstCtl &s, const InstExt &u, ws_control *o) {
+void fillControl(const InstCtl &s, const InstExt &u, ws_control *o, unsigned long long t0) {
+  o->t_start_ms = (s.tBeg && t0 && s.tBeg >= t0) ? double(s.tBeg - t0) * 1e-6 : 0.0;
+  o->t_end_ms = (s.tEnd && t0 && s.tEnd >= t0) ? double(s.tEnd - t0) * 1e-6 : 0.0;
   o->iter = s.iter; o->status = s.status; o->rollbacks = s.rollbacks; o->pending_zero = s.pending;
   o->ke = s.ke; o->ke_prev = s.ke_prev; o->residual = s.residual; o->res_force = s.res_f; o->res_torque = s.res_t; o->fref = s.fref;
   o->e_stretch = s.e_stretch; o->e_shear = s.e_shear; o->e_bend = s.e_bend; o->e_twist = s.e_twist; o->e_contact = s.e_contact;
@@ -672,18 +694,37 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
   const bool ext = anyExt(c);
   c->lastLaunches = 0;
   CK(cudaEventRecord(c->ev0, c->st));
+  c->ranLast.assign(mask ? mask : nullptr, mask ? mask + nInst : nullptr);
+  if (!mask) c->ranLast.assign(nInst, 1);
   if (c->form == WS_FORM_CTA) {
     if (mask) CK(cudaMemcpyAsync(c->dMask, mask, nInst, cudaMemcpyHostToDevice, c->st));
-    if (c->residentBytes) {
-      const int thr = c->threads > 0 ? std::min(c->threads, 512) : 512;
-      CK(launchResident<P>(devOf<P>(c), c->dInst, c->dCtl, c->dOrder, nInst, nIter, mask ? c->dMask : nullptr, thr,
-                           c->residentBytes, c->shortSides, ext, c->st));
-    } else {
-      const int thr = c->threads > 0 ? c->threads : 256;
-      CK(launchBatched<P>(devOf<P>(c), c->dInst, c->dCtl, c->dOrder, nInst, nIter, mask ? c->dMask : nullptr, thr, nInst,
-                          c->shortSides, ext, c->st));
+    const uint8_t *dm = mask ? c->dMask : nullptr;
+    // the wide instances' clusters first on the context's stream, the one-block kernels beside them on a second
+    // stream, joined before the step's end event
+    cudaStream_t nst = c->st;
+    if (c->nWide > 0 && nIter > 0) {
+      CK(cudaEventRecord(c->ctaFork, c->st));
+      CK(cudaStreamWaitEvent(c->sideCta, c->ctaFork, 0));
+      CK(launchWide<P>(devOf<P>(c), c->dInst, c->dCtl, c->dWide, c->nWide, nIter, dm, 512, c->wideCl, c->shortSides, ext, c->st));
+      nst = c->sideCta;
+      c->lastLaunches += 1;
     }
-    c->lastLaunches = 1;
+    if (c->nNarrow > 0) {
+      if (c->residentBytes) {
+        const int thr = c->threads > 0 ? std::min(c->threads, 512) : 512;
+        CK(launchResident<P>(devOf<P>(c), c->dInst, c->dCtl, c->dOrder, c->nNarrow, nIter, dm, thr, c->residentBytes,
+                             c->shortSides, ext, nst));
+      } else {
+        const int thr = c->threads > 0 ? c->threads : 256;
+        CK(launchBatched<P>(devOf<P>(c), c->dInst, c->dCtl, c->dOrder, c->nNarrow, nIter, dm, thr, c->nNarrow,
+                            c->shortSides, ext, nst));
+      }
+      c->lastLaunches += 1;
+    }
+    if (nst != c->st) {
+      CK(cudaEventRecord(c->ctaJoin, nst));
+      CK(cudaStreamWaitEvent(c->st, c->ctaJoin, 0));
+    }
   } else if (c->form == WS_FORM_GRID) {
     CK(cudaMemsetAsync(c->dBar, 0, 2 * sizeof(unsigned), c->st));
     CK(cudaMemsetAsync(c->dErr, 0, sizeof(int), c->st));
@@ -866,7 +907,11 @@ void selectResident(ws_ctx *c) {
   c->residentBytes = 0;
   if (c->form != WS_FORM_CTA || c->ctaGlobal) return;
   size_t need = 0;
-  for (const InstDesc &I : c->inst) need = std::max<size_t>(need, residentLayout<P>(I.n, I.m, I.p, I.C, I.K, c->shortSides).bytes);
+  for (size_t b = 0; b < c->inst.size(); b++) {
+    if (c->isWide[b]) continue;                 // the wide instances run with global state in the cluster kernel
+    const InstDesc &I = c->inst[b];
+    need = std::max<size_t>(need, residentLayout<P>(I.n, I.m, I.p, I.C, I.K, c->shortSides).bytes);
+  }
   size_t granted = 0;
   CK(residentPrepare<P>(need, c->shortSides, &granted));
   c->residentBytes = granted;
@@ -1045,6 +1090,23 @@ int guarded(const char *what, F &&f) {
     default: FN<PREC_F32>(__VA_ARGS__); break;                \
   }
 
+// clusters of `cl` blocks of 512 threads that the device can hold at once, for the cluster kernel's variants that need
+// the most resources (0: the shape cannot launch)
+int wideFit(int prec, int cl) {
+  int fit = 1 << 30;
+  for (int sh = 0; sh < 2; sh++)
+    for (int ex = 0; ex < 2; ex++) {
+      int n = 0;
+      switch (prec) {
+        case WS_PREC_F64: n = wideClusters<PREC_F64>(512, cl, sh != 0, ex != 0); break;
+        case WS_PREC_MIXED: n = wideClusters<PREC_MIXED>(512, cl, sh != 0, ex != 0); break;
+        default: n = wideClusters<PREC_F32>(512, cl, sh != 0, ex != 0); break;
+      }
+      fit = std::min(fit, n);
+    }
+  return fit;
+}
+
 void destroyCtx(ws_ctx *c) {
   if (!c) return;
   if (c->graph) cudaGraphExecDestroy(c->graph);
@@ -1052,6 +1114,10 @@ void destroyCtx(ws_ctx *c) {
   if (c->dInst) cudaFree(c->dInst);
   if (c->dCtl) cudaFree(c->dCtl);
   if (c->dOrder) cudaFree(c->dOrder);
+  if (c->dWide) cudaFree(c->dWide);
+  if (c->sideCta) cudaStreamDestroy(c->sideCta);
+  if (c->ctaFork) cudaEventDestroy(c->ctaFork);
+  if (c->ctaJoin) cudaEventDestroy(c->ctaJoin);
   if (c->dMask) cudaFree(c->dMask);
   if (c->dPart) cudaFree(c->dPart);
   if (c->dBar) cudaFree(c->dBar);
@@ -1128,12 +1194,40 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     c->order.resize(n_instances);
     std::iota(c->order.begin(), c->order.end(), 0);
     std::stable_sort(c->order.begin(), c->order.end(), [&](int a, int b) { return c->inst[a].n + c->inst[a].m > c->inst[b].n + c->inst[b].m; });
+    // batched form: instances from wide_min nodes + segments up run on a cluster of blocks each (an instance's width
+    // depends on its own size only, so its result does not depend on the rest of the batch)
+    c->isWide.assign(n_instances, 0);
+    std::vector<int> wide, narrow;
+    if (o.form == WS_FORM_CTA) {
+      c->wideCl = o.wide_cluster == 0 ? 2 : o.wide_cluster;
+      c->wideMin = o.wide_min > 0 ? o.wide_min : 32768;
+      if (c->wideCl < 1 || c->wideCl > 8) throw std::invalid_argument("wide_cluster must be 0 (default), 1 (off) or 2..8");
+      // a cluster shape the device cannot hold is halved until it can (1: no wide instances)
+      while (c->wideCl >= 2 && wideFit(c->prec, c->wideCl) == 0) c->wideCl /= 2;
+    }
+    for (int b : c->order) {
+      const InstDesc &I = c->inst[b];
+      const bool w = o.form == WS_FORM_CTA && c->wideCl >= 2 && I.n + I.m >= c->wideMin && !I.utmMode;
+      c->isWide[b] = w;
+      (w ? wide : narrow).push_back(b);
+    }
+    c->nWide = int(wide.size());
+    c->nNarrow = int(narrow.size());
+    if (c->nWide == 0) c->wideCl = 0;
     CK(cudaMalloc(&c->dInst, sizeof(InstDesc) * n_instances));
     CK(cudaMalloc(&c->dCtl, sizeof(InstCtl) * n_instances));
     CK(cudaMalloc(&c->dOrder, sizeof(int) * n_instances));
     CK(cudaMalloc(&c->dMask, n_instances));
     CK(cudaMemcpyAsync(c->dInst, c->inst.data(), sizeof(InstDesc) * n_instances, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->dOrder, c->order.data(), sizeof(int) * n_instances, cudaMemcpyHostToDevice, c->st));
+    if (c->nNarrow)
+      CK(cudaMemcpyAsync(c->dOrder, narrow.data(), sizeof(int) * c->nNarrow, cudaMemcpyHostToDevice, c->st));
+    if (c->nWide) {
+      CK(cudaMalloc(&c->dWide, sizeof(int) * c->nWide));
+      CK(cudaMemcpyAsync(c->dWide, wide.data(), sizeof(int) * c->nWide, cudaMemcpyHostToDevice, c->st));
+      CK(cudaStreamCreateWithFlags(&c->sideCta, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&c->ctaFork, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&c->ctaJoin, cudaEventDisableTiming));
+    }
     std::vector<InstCtl> ctl(n_instances);
     for (int b = 0; b < n_instances; b++) {
       InstCtl &s = ctl[b];
@@ -1190,7 +1284,7 @@ int ws_step(ws_ctx *c, int32_t n_iter, const uint8_t *mask, ws_control *ctl) {
     c->lastMs = -1;
     if (ctl) {
       readCtl(c);
-      for (size_t b = 0; b < c->inst.size(); b++) fillControl(c->ctlHost[b], c->extHost[b], ctl + b);
+      for (size_t b = 0; b < c->inst.size(); b++) fillControl(c->ctlHost[b], c->extHost[b], ctl + b, stepStart(c));
     }
   });
 }
@@ -1199,7 +1293,7 @@ int ws_read_control(ws_ctx *c, ws_control *ctl) {
   if (!c || !ctl) return fail(WS_ERR_ARG, "ws_read_control: bad arguments");
   return guarded("ws_read_control", [&]() {
     readCtl(c);
-    for (size_t b = 0; b < c->inst.size(); b++) fillControl(c->ctlHost[b], c->extHost[b], ctl + b);
+    for (size_t b = 0; b < c->inst.size(); b++) fillControl(c->ctlHost[b], c->extHost[b], ctl + b, stepStart(c));
   });
 }
 
@@ -1232,6 +1326,10 @@ void *ws_stream(ws_ctx *c) { return c ? c->st : nullptr; }
 uint64_t ws_device_bytes(const ws_ctx *c) { return c ? c->bytes : 0; }
 int ws_side_order(const ws_ctx *c) { return c && c->shortSides ? 1 : 0; }
 int ws_cta_resident(const ws_ctx *c) { return c && c->residentBytes ? 1 : 0; }
+int ws_wide_instances(const ws_ctx *c, int32_t *cluster) {
+  if (cluster) *cluster = c ? c->wideCl : 0;
+  return c ? c->nWide : 0;
+}
 int ws_last_step_stats(const ws_ctx *c_, double *ms, int64_t *launches) {
   if (!c_) return fail(WS_ERR_ARG, "ws_last_step_stats: null context");
   ws_ctx *c = const_cast<ws_ctx *>(c_);
@@ -1296,7 +1394,7 @@ static void runInPlaceImpl(ws_ctx *c, char *base, int nIter, int threads, ws_sta
     CK(launchBatched<P>(devOf<P>(c), c->dInst, c->dCtl, nullptr, 1, nIter, nullptr, threads, 1, c->shortSides, anyExt(c), c->st));
   CK(cudaStreamSynchronize(c->st));
   if (out) downloadImpl<P>(c, 0, out);
-  if (ctl) { readCtl(c); fillControl(c->ctlHost[0], c->extHost[0], ctl); }
+  if (ctl) { readCtl(c); fillControl(c->ctlHost[0], c->extHost[0], ctl, stepStart(c)); }
 }
 
 int runInPlace(int prec, const HostGoals &g, char *base, int nIter, int threads, cudaStream_t st, ws_state_out *out,

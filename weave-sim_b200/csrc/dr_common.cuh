@@ -53,6 +53,9 @@ struct InstCtl {
   double ke, ke_prev, residual, res_f, res_t, fref;
   double e_stretch, e_shear, e_bend, e_twist, e_contact;
   int penN, alPend;    // augmented Lagrangian: iterations in the penetration window; the multiplier update is due
+  // batched forms: global timer (ns) when the instance's block (or cluster) took it up in the last launch, and when it
+  // left it; 0 in the other forms
+  unsigned long long tBeg, tEnd;
 };
 
 // per-instance state of the extensions, apart from the control block that every iteration carries (kernel variants

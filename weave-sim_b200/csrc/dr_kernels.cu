@@ -42,6 +42,12 @@ namespace wsb {
 // attribute, both instructions do nothing.
 __device__ __forceinline__ void waitPrevGrid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void allowNextGrid() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+// the GPU's global nanosecond timer (per-instance device times of the batched forms)
+__device__ __forceinline__ unsigned long long globalTimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 // Block partials, value-major: slot i of block b at part[i * stride + b], so the finishing block reads them coalesced.
 template <class A>
@@ -144,9 +150,10 @@ __device__ __forceinline__ int chunksBelow(long long x, long long cb, int cost, 
   const long long c = (num + den - 1) / den;
   return int(c < nc ? c : nc);
 }
+// over nw warps of which this thread's is w (a block's warps, or a cluster's)
 template <int NR, class F>
-__device__ __forceinline__ void forBalanced(const PhaseRun (&runs)[NR], F &&f) {
-  const int nw = blockDim.x >> 5, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+__device__ __forceinline__ void forBalancedOver(const PhaseRun (&runs)[NR], int nw, int w, F &&f) {
+  const int lane = threadIdx.x & 31;
   long long total = 0;
   for (int r = 0; r < NR; r++) total += (long long)((runs[r].count + 31) >> 5) * runs[r].cost;
   long long cb = 0;
@@ -162,13 +169,18 @@ __device__ __forceinline__ void forBalanced(const PhaseRun (&runs)[NR], F &&f) {
     cb += (long long)nc * cost;
   }
 }
+template <int NR, class F>
+__device__ __forceinline__ void forBalanced(const PhaseRun (&runs)[NR], F &&f) {
+  forBalancedOver(runs, int(blockDim.x >> 5), int(threadIdx.x >> 5), f);
+}
 
 // phase A of one instance over the block: crossings, segments, joints, clamps
 template <int P, bool SHORT, bool EXT>
-__device__ __forceinline__ void blockPhaseA(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, Part<typename Dev<P>::A> &pt) {
+__device__ __forceinline__ void blockPhaseA(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, Part<typename Dev<P>::A> &pt,
+                                            int nw, int w) {
   const int nK = (I.contacts && I.K) ? I.K : 0;
   const PhaseRun runs[4] = {{2 * nK, COST_CROSSING}, {I.m, COST_SEGMENT}, {I.p, COST_JOINT}, {I.C, COST_CLAMP}};
-  forBalanced(runs, [&](int r, int e) {
+  forBalancedOver(runs, nw, w, [&](int r, int e) {
     switch (r) {
       case 0: crossing<P, SHORT, EXT>(d, I, sx.cur, sx.iter, sx.onxt, sx.obuf, I.k0 + (e >> 1), e & 1, sx.alPend, sx.penN, pt); break;
       case 1: segForce<P>(d, sx.cur, I.m0 + e, pt); break;
@@ -179,9 +191,9 @@ __device__ __forceinline__ void blockPhaseA(const Dev<P> &d, const InstDesc &I, 
 }
 // phase B / C (general order) of one instance over the block
 template <int P>
-__device__ __forceinline__ void blockPhaseBC(const Dev<P> &d, const InstDesc &I, const StepCtx &sx) {
+__device__ __forceinline__ void blockPhaseBC(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, int nw, int w) {
   const PhaseRun runs[2] = {{2 * I.K, COST_RANK}, {I.m, COST_SLICE}};
-  forBalanced(runs, [&](int r, int e) {
+  forBalancedOver(runs, nw, w, [&](int r, int e) {
     if (r == 0) rankSide<P>(d, 2 * I.k0 + e, sx.onxt, sx.onxt);
     else segCount<P>(d, I.m0 + e, sx.onxt, sx.onxt);
   });
@@ -198,10 +210,11 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
   __shared__ InstCtl sc;
   __shared__ InstDesc si;
   __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
+  const int nwB = blockDim.x >> 5, wB = threadIdx.x >> 5;
   for (int bi = blockIdx.x; bi < nInst; bi += gridDim.x) {
     const int b = order ? order[bi] : bi;
     if (mask && !mask[b]) continue;
-    if (threadIdx.x == 0) { sc = ctl[b]; si = insts[b]; }
+    if (threadIdx.x == 0) { sc = ctl[b]; si = insts[b]; sc.tBeg = globalTimer(); }
     __syncthreads();
     const InstDesc &I = si;
     const bool cx = I.contacts && I.K;
@@ -210,10 +223,10 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
       const StepCtx sx = makeCtx<A>(I, sc, EXT ? d.ext[I.utmIdx].pf : nullptr);
       Part<A> pt;
       pt.init();
-      blockPhaseA<P, SHORT, EXT>(d, I, sx, pt);
+      blockPhaseA<P, SHORT, EXT>(d, I, sx, pt, nwB, wB);
       __syncthreads();
       if (!SHORT && cx) {
-        blockPhaseBC<P>(d, I, sx);
+        blockPhaseBC<P>(d, I, sx, nwB, wB);
         __syncthreads();
       }
       {
@@ -233,8 +246,114 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
         __syncthreads();
       }
     }
-    if (threadIdx.x == 0) ctl[b] = sc;
+    if (threadIdx.x == 0) { sc.tEnd = globalTimer(); ctl[b] = sc; }
     __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ wide instances
+// The batched form for an instance too large for one block to keep pace with the rest of the batch: a thread-block
+// cluster (its blocks on SMs of one GPC, launched together) relaxes it.  Every phase's elements are split by cost over
+// all the cluster's warps (the split depends only on the counts, the block size and the cluster size); the phases are
+// separated by the cluster's hardware barrier, whose arrive has release and whose wait has acquire semantics at cluster
+// scope, so a phase reads in global memory what the other blocks wrote in the one before, and nothing spins.  Each
+// block reduces its partials, and every block then adds the cluster's block partials from distributed shared memory in
+// rank order and takes the same kinetic-damping decision on its own copy of the control block, so no broadcast is
+// needed.  The state stays in global memory (double-buffered, as in k_batched).  A load protocol is not run here (the
+// host keeps such instances in the one-block kernels).
+__device__ __forceinline__ void clusterSync() {
+  asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+__device__ __forceinline__ unsigned clusterRank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ unsigned clusterSize() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+// a value of block `rank`'s shared memory: the address of `p` in that block (mapa), read through the cluster window
+template <class A>
+__device__ __forceinline__ A remoteLoad(const A *p, unsigned rank) {
+  const unsigned local = static_cast<unsigned>(__cvta_generic_to_shared(p));
+  unsigned remote;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(local), "r"(rank));
+  if constexpr (sizeof(A) == 8) {
+    unsigned long long v;
+    asm volatile("ld.shared::cluster.u64 %0, [%1];" : "=l"(v) : "r"(remote) : "memory");
+    return __longlong_as_double(static_cast<long long>(v));
+  } else {
+    unsigned v;
+    asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(remote) : "memory");
+    return __uint_as_float(v);
+  }
+}
+
+template <int P, bool SHORT, bool EXT>
+__global__ void __launch_bounds__(512) k_wide(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+                                               const int *__restrict__ wide, int nWide, int nIter, const uint8_t *__restrict__ mask) {
+  using A = typename Dev<P>::A;
+  static_assert(sizeof(A) == 4 || sizeof(A) == 8, "reduction type");
+  __shared__ InstCtl sc;
+  __shared__ InstDesc si;
+  __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
+  __shared__ A cpart[RS_NSUM + RX_NMAX];     // this block's partials, read by every block of the cluster
+  const unsigned rank = clusterRank(), ncl = clusterSize();
+  const int nwB = blockDim.x >> 5;
+  const int nw = nwB * int(ncl), w = int(rank) * nwB + int(threadIdx.x >> 5);
+  const int nClusters = int(gridDim.x / ncl), cid = int(blockIdx.x / ncl);
+  for (int wi = cid; wi < nWide; wi += nClusters) {
+    const int b = wide[wi];
+    if (mask && !mask[b]) continue;                 // the same answer in every block of the cluster
+    if (threadIdx.x == 0) { sc = ctl[b]; si = insts[b]; sc.tBeg = globalTimer(); }
+    __syncthreads();
+    const InstDesc &I = si;
+    const bool cx = I.contacts && I.K;
+    for (int it = 0; it < nIter; it++) {
+      if (sc.status != WS_RUNNING) break;           // every block holds the same control block
+      const StepCtx sx = makeCtx<A>(I, sc, EXT ? d.ext[I.utmIdx].pf : nullptr);
+      Part<A> pt;
+      pt.init();
+      blockPhaseA<P, SHORT, EXT>(d, I, sx, pt, nw, w);
+      clusterSync();
+      if (!SHORT && cx) {
+        blockPhaseBC<P>(d, I, sx, nw, w);
+        clusterSync();
+      }
+      {
+        const PhaseRun runs[3] = {{I.n, COST_NODE_UPD}, {I.m, COST_SEG_UPD}, {(SHORT && cx) ? 2 * I.K : 0, COST_RANK}};
+        forBalancedOver(runs, nw, w, [&](int r, int e) {
+          if (r == 0) nodeUpdate<P, SHORT, EXT>(d, I, sx, I.n0 + e, pt);
+          else if (r == 1) segUpdate<P, SHORT>(d, I, sx, I.m0 + e, pt);
+          else rankSideShort<P>(d, 2 * I.k0 + e, sx.onxt);
+        });
+      }
+      blockReduce(pt, red);
+      if (threadIdx.x == 0) {
+        for (int i = 0; i < RS_NSUM; i++) cpart[i] = pt.s[i];
+        for (int i = 0; i < RX_NMAX; i++) cpart[RS_NSUM + i] = pt.x[i];
+      }
+      // the phase-D writes of every block, and every block's partials, visible cluster-wide
+      clusterSync();
+      if (threadIdx.x == 0) {
+        Part<A> q;
+        q.init();
+        for (unsigned r = 0; r < ncl; r++) {
+          for (int i = 0; i < RS_NSUM; i++) q.s[i] += remoteLoad(cpart + i, r);
+          for (int i = 0; i < RX_NMAX; i++) q.x[i] = mmax(q.x[i], remoteLoad(cpart + RS_NSUM + i, r));
+        }
+        decide<EXT>(I, sc, q, nIter);
+        if constexpr (EXT)     // the ground's energy of the iteration
+          if (rank == 0) d.ext[I.utmIdx].eFloor = double(q.s[RS_FLOOR]);
+      }
+      // the next write of cpart (after the next iteration's first cluster barrier) cannot overtake these reads
+      __syncthreads();
+    }
+    if (threadIdx.x == 0 && rank == 0) { sc.tEnd = globalTimer(); ctl[b] = sc; }
+    // no block leaves, or takes up the next instance, while another still reads its partials
+    clusterSync();
   }
 }
 
@@ -365,10 +484,11 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
   __shared__ InstCtl sc;
   __shared__ InstDesc si;
   __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
+  const int nwB = blockDim.x >> 5, wB = threadIdx.x >> 5;
   for (int bi = blockIdx.x; bi < nInst; bi += gridDim.x) {
     const int b = order ? order[bi] : bi;
     if (mask && !mask[b]) continue;
-    if (threadIdx.x == 0) { sc = ctl[b]; si = insts[b]; }
+    if (threadIdx.x == 0) { sc = ctl[b]; si = insts[b]; sc.tBeg = globalTimer(); }
     __syncthreads();
     const InstDesc &I = si;
     const ResLayout L = residentLayout<P>(I.n, I.m, I.p, I.C, I.K, SHORT);
@@ -383,10 +503,10 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
       sx.cur = sx.nxt = 0;              // in place
       Part<A> pt;
       pt.init();
-      blockPhaseA<P, SHORT, EXT>(v, I, sx, pt);
+      blockPhaseA<P, SHORT, EXT>(v, I, sx, pt, nwB, wB);
       __syncthreads();
       if (!SHORT && cx) {
-        blockPhaseBC<P>(v, I, sx);
+        blockPhaseBC<P>(v, I, sx, nwB, wB);
         __syncthreads();
       }
       auto upd = [&](int r, int e) {
@@ -428,7 +548,7 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
       }
     }
     residentStore<P, SHORT>(d, v, I, sc);
-    if (threadIdx.x == 0) ctl[b] = sc;
+    if (threadIdx.x == 0) { sc.tEnd = globalTimer(); ctl[b] = sc; }
     __syncthreads();
   }
 }
@@ -952,6 +1072,45 @@ cudaError_t launchBatched(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, 
   return cudaGetLastError();
 }
 
+template <int P>
+cudaError_t launchWide(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *wide, int nWide, int nIter,
+                       const uint8_t *mask, int threads, int cluster, bool shortSides, bool ext, cudaStream_t st) {
+  if (nWide <= 0) return cudaSuccess;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(nWide * cluster));
+  cfg.blockDim = dim3(unsigned(threads));
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = unsigned(cluster);
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, WSB_PICK(k_wide, P, shortSides, ext), d, insts, ctl, wide, nWide, nIter, mask);
+}
+// clusters of `cluster` blocks of `threads` threads that can be resident at once (0: the shape cannot launch)
+template <int P>
+int wideClusters(int threads, int cluster, bool shortSides, bool ext) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(cluster));
+  cfg.blockDim = dim3(unsigned(threads));
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = unsigned(cluster);
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, WSB_PICK(k_wide, P, shortSides, ext), &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
 // dynamic shared memory of the resident form for a batch whose largest instance needs `bytes` (0 when it does not fit
 // on this device); sets the kernel's limit to it
 // (both variants of the side order, with and without the contact extensions)
@@ -1107,6 +1266,9 @@ int gridBlocks(bool shortSides, bool ext) {
   template cudaError_t launchGrid<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, unsigned *, int *, int, int, bool, \
                                      bool, cudaStream_t);                                                            \
   template int gridBlocks<P>(bool, bool);                                                                           \
+  template cudaError_t launchWide<P>(const Dev<P> &, const InstDesc *, InstCtl *, const int *, int, int, const uint8_t *, \
+                                     int, int, bool, bool, cudaStream_t);                                            \
+  template int wideClusters<P>(int, int, bool, bool);                                                              \
   template cudaError_t launchUnpack<P>(const Dev<P> &, const InstDesc *, InstCtl *, int, const double *, int, int, int, bool, \
                                        bool, bool, cudaStream_t);                                                    \
   template cudaError_t launchPack<P>(const Dev<P> &, const InstDesc *, const InstCtl *, int, const PackList &, size_t,      \

@@ -21,6 +21,12 @@ struct PartEnds { int x, y, n, m; };
 template <int P>
 cudaError_t launchBatched(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *order, int nInst, int nIter,
                           const uint8_t *mask, int threads, int blocks, bool shortSides, bool ext, cudaStream_t st);
+// the wide instances wide[0, nWide) of the batched form, each on a thread-block cluster of `cluster` blocks of `threads`
+template <int P>
+cudaError_t launchWide(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, const int *wide, int nWide, int nIter,
+                       const uint8_t *mask, int threads, int cluster, bool shortSides, bool ext, cudaStream_t st);
+template <int P>
+int wideClusters(int threads, int cluster, bool shortSides, bool ext);
 // ext: some instance runs an extension (contact extensions, the ground, a load protocol): the kernels' variants that
 // have them.  roles: each split phase as one launch whose blocks take the two parts' roles (no fork); else `fork`
 // (when given) runs the parts on forked branches, else each phase is one kernel.

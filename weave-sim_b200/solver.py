@@ -69,7 +69,7 @@ def relax_noalloc(model, n_iter, precision="mixed", threads=256, stream=None):
 
 class GpuSolver:
     def __init__(self, models, precision="mixed", form="cta", threads=0, device=0, budget_bytes=0, side_order="auto",
-                 cta_state="auto"):
+                 cta_state="auto", wide_cluster=0, wide_min=0):
         if not isinstance(models, (list, tuple)):
             models = [models]
         self.models = list(models)
@@ -82,6 +82,7 @@ class GpuSolver:
         opts.threads, opts.device, opts.budget_bytes = int(threads), int(device), int(budget_bytes)
         opts.side_order = {"auto": 0, "general": 1}[side_order]
         opts.cta_state = {"auto": 0, "global": 1}[cta_state]
+        opts.wide_cluster, opts.wide_min = int(wide_cluster), int(wide_min)
         self.precision, self.form = precision, form
         h = C.c_void_p()
         check(lib().ws_create(arr, self.B, C.byref(opts), C.byref(h)), "ws_create")
@@ -165,6 +166,13 @@ class GpuSolver:
     def resident(self):
         """True when the batched form holds its instances in shared memory"""
         return bool(lib().ws_cta_resident(self.h))
+
+    @property
+    def wide(self):
+        """(instances relaxed by a thread-block cluster each, blocks per cluster) in the batched form"""
+        cl = C.c_int32()
+        n = lib().ws_wide_instances(self.h, C.byref(cl))
+        return int(n), int(cl.value)
 
     @property
     def side_order(self):

@@ -154,13 +154,30 @@ def run_ratio(batch=592, iters=400):
             "batched_over_plain": batched / plain}
 
 
-def run_batch(count=512, iters=CAP, precision="mixed", threads=512, seed=4):
+def _plain_iter_ms(models, precision, iters=200):
+    """device ms per iteration of the plain single-instance form on each model (after 20 warm-up iterations)"""
+    out = []
+    for m in models:
+        s = GpuSolver([m.copy()], precision=precision, form="plain")
+        s.step(20, read=False)
+        s.step(iters, read=False)
+        out.append(s.last_step_stats()[0] / iters)
+        s.dispose()
+    return out
+
+
+def run_batch(count=512, iters=CAP, precision="mixed", threads=0, seed=4, wide_cluster=0, wide_min=0, plain_sample=16):
+    """the uneven batch in one batched step to the iteration cap; per-instance device times (from the block or cluster
+    taking the instance up to its leaving it); and the plain single-instance form on a size-stratified sample of the
+    same instances, whose per-iteration times, interpolated over the sizes of all instances, give the time the plain form
+    would take to relax the whole batch one instance after another"""
     models = configs.batch_mixed(count, seed=seed)
     for m in models:
         m.params = dict(m.params, max_iter=iters)
     t0 = time.perf_counter()
-    s = GpuSolver(models, precision=precision, threads=threads)
+    s = GpuSolver(models, precision=precision, threads=threads, wide_cluster=wide_cluster, wide_min=wide_min)
     create_s = time.perf_counter() - t0
+    n_wide, cl = s.wide
     ctl = s.step(iters)
     ms, nl = s.last_step_stats()
     dev_bytes = s.device_bytes
@@ -168,12 +185,30 @@ def run_batch(count=512, iters=CAP, precision="mixed", threads=512, seed=4):
     its = sum(c["iter"] for c in ctl)
     node_its = sum(c["iter"] * m.n for c, m in zip(ctl, models))
     n = np.array([m.n for m in models])
-    return {"instances": count, "iteration_cap": iters, "gpu_ms": ms, "solves_per_s": count / (ms * 1e-3),
-            "inst_iters_per_s": its / (ms * 1e-3), "node_iters_per_s": node_its / (ms * 1e-3),
-            "converged": sum(c["status"] == 1 for c in ctl), "nonfinite": sum(c["status"] == 3 for c in ctl),
-            "nodes_min": int(n.min()), "nodes_median": int(np.median(n)), "nodes_max": int(n.max()),
-            "nodes_total": int(n.sum()), "crossings_total": int(sum(m.K for m in models)), "device_bytes": dev_bytes,
-            "create_s": create_s, "launches": nl}
+    dev = np.array([c["t_end_ms"] - c["t_start_ms"] for c in ctl])
+    end = np.array([c["t_end_ms"] for c in ctl])
+    big = int(np.argmax(n))
+    out = {"instances": count, "iteration_cap": iters, "gpu_ms": ms, "solves_per_s": count / (ms * 1e-3),
+           "inst_iters_per_s": its / (ms * 1e-3), "node_iters_per_s": node_its / (ms * 1e-3),
+           "converged": sum(c["status"] == 1 for c in ctl), "nonfinite": sum(c["status"] == 3 for c in ctl),
+           "nodes_min": int(n.min()), "nodes_median": int(np.median(n)), "nodes_max": int(n.max()),
+           "nodes_total": int(n.sum()), "crossings_total": int(sum(m.K for m in models)), "device_bytes": dev_bytes,
+           "create_s": create_s, "launches": nl, "wide_instances": n_wide, "wide_cluster": cl,
+           "instance_device_ms": {"min": float(dev.min()), "median": float(np.median(dev)), "max": float(dev.max()),
+                                  "largest_instance": float(dev[big]), "largest_instance_end": float(end[big]),
+                                  "last_end": float(end.max()), "p90_end": float(np.percentile(end, 90))},
+           "longest_instance_nodes": int(n[int(np.argmax(dev))])}
+    if plain_sample:
+        order = np.argsort(n)
+        pick = sorted(set(int(order[int(q * (count - 1))]) for q in np.linspace(0.0, 1.0, plain_sample)), key=lambda b: n[b])
+        per = _plain_iter_ms([models[b] for b in pick], precision)
+        xs, ys = np.array([n[b] for b in pick], dtype=float), np.array(per)
+        plain_total_ms = float(np.sum(np.interp(n, xs, ys))) * iters
+        out["plain_form"] = {"sample_nodes": [int(v) for v in xs], "sample_ms_per_iter": [float(v) for v in ys],
+                             "batch_one_after_another_ms": plain_total_ms,
+                             "solves_per_s": count / (plain_total_ms * 1e-3)}
+        out["batched_over_plain"] = out["solves_per_s"] / out["plain_form"]["solves_per_s"]
+    return out
 
 
 def run_serve(rates=(50.0, 200.0, 1000.0), counts=(300, 600, 1000), slots=296, chunk=250, budget_bytes=150 * 10 ** 9,
