@@ -292,7 +292,22 @@ typedef struct ws_opts {
                            2..8; 1: every instance in one block; 0: the default (2) */
   int32_t wide_min;     /* batched form: an instance is wide when its nodes + segments reach this (0: the default,
                            32768); an instance with a load protocol is never wide */
+  int32_t tune;         /* 1: the launch shape (the fields above from threads on, and the plain form's launch mode) is
+                           the autotuner's: taken from its cache for the batch's size bucket on this device, or found
+                           by timing every candidate shape on this batch at creation (the state is restored after the
+                           trials); 0: the fields above as given */
 } ws_opts;
+
+/* A launch shape.  The batched form: threads per block of the one-block kernels (128, 256, 512), cta_state
+ * (WS_CTA_AUTO or WS_CTA_GLOBAL), wide_cluster (1: no wide instances, else blocks of 512 threads per wide instance's
+ * cluster) and wide_min (nodes + segments from which an instance is wide).  The plain form: plain_launch (0 forked
+ * graph branches, 1 one launch a phase with block roles, 2 one kernel a phase).  source: 0 as given by the options, 1
+ * found by the tuner when the context was made, 2 from the tuner's cache.  trial_ms: the time of the shape's trial run
+ * (tuned shapes), default_ms: that of the default shape in the same trials, trials: candidates timed. */
+typedef struct ws_shape {
+  int32_t threads, cta_state, wide_cluster, wide_min, plain_launch, source, trials, pad0;
+  double trial_ms, default_ms;
+} ws_shape;
 enum { WS_SIDES_AUTO = 0, WS_SIDES_GENERAL = 1 };
 enum { WS_CTA_AUTO = 0, WS_CTA_GLOBAL = 1 };
 
@@ -397,6 +412,21 @@ int ws_cta_resident(const ws_ctx *ctx);
 /* batched form: the number of wide instances (each relaxed by a thread-block cluster) and, in *cluster (may be NULL),
  * the blocks per cluster (0 when there are none) */
 int ws_wide_instances(const ws_ctx *ctx, int32_t *cluster);
+/* the launch shape the context runs (ws_shape) */
+int ws_get_shape(const ws_ctx *ctx, ws_shape *out);
+/* The autotuner's cache, keyed by a batch's size bucket on a device (ws_tune_key: form, precision, variants,
+ * instance count, largest instance and total work in half-octave steps; no device needed).  ws_tune_candidates lists
+ * the shapes the tuner times for such a batch: stage 1 (block size and state placement, no wide instances) when
+ * `after` is NULL, else stage 2 (cluster shapes and thresholds at the stage-1 winner `after`); it returns how many there
+ * are and writes up to `cap` of them.  ws_tune_cache_get returns 1 and the shape when the key is cached, else 0; _put
+ * stores one (also appended to the file WEAVESIM_TUNE_CACHE names, when set); _clear empties the process's cache. */
+int ws_tune_key(const ws_model *const *models, int32_t n_instances, const ws_opts *opts, const char *device, char *buf,
+                size_t cap);
+int ws_tune_candidates(const ws_model *const *models, int32_t n_instances, const ws_opts *opts, const ws_shape *after,
+                       ws_shape *out, int32_t cap);
+int ws_tune_cache_get(const char *key, ws_shape *out);
+int ws_tune_cache_put(const char *key, const ws_shape *shape);
+int ws_tune_cache_clear(void);
 /* device bytes held by the context */
 uint64_t ws_device_bytes(const ws_ctx *ctx);
 /* GPU time of the last ws_step (ms, CUDA events on the context's stream) and the number of kernel launches it made */

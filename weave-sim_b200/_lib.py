@@ -95,7 +95,19 @@ class WsControl(C.Structure):
 class WsOpts(C.Structure):
     _fields_ = [("precision", C.c_int32), ("form", C.c_int32), ("threads", C.c_int32), ("device", C.c_int32),
                 ("budget_bytes", C.c_uint64), ("cta_state", C.c_int32), ("side_order", C.c_int32),
-                ("wide_cluster", C.c_int32), ("wide_min", C.c_int32)]
+                ("wide_cluster", C.c_int32), ("wide_min", C.c_int32), ("tune", C.c_int32)]
+
+
+class WsShape(C.Structure):
+    _fields_ = [(k, C.c_int32) for k in ("threads", "cta_state", "wide_cluster", "wide_min", "plain_launch", "source",
+                                         "trials", "pad0")] + [("trial_ms", C.c_double), ("default_ms", C.c_double)]
+
+    SOURCES = {0: "options", 1: "tuned", 2: "cache"}
+
+    def as_dict(self):
+        d = {f[0]: getattr(self, f[0]) for f in self._fields_ if f[0] != "pad0"}
+        d["source"] = self.SOURCES.get(d["source"], d["source"])
+        return d
 
 
 class WsStateOut(C.Structure):
@@ -149,6 +161,13 @@ def lib():
             L.ws_cta_resident.restype = C.c_int
             L.ws_wide_instances.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
             L.ws_wide_instances.restype = C.c_int
+            L.ws_get_shape.argtypes = [C.c_void_p, C.POINTER(WsShape)]
+            L.ws_tune_key.argtypes = [C.POINTER(C.POINTER(WsModel)), C.c_int32, C.POINTER(WsOpts), C.c_char_p,
+                                      C.c_char_p, C.c_size_t]
+            L.ws_tune_candidates.argtypes = [C.POINTER(C.POINTER(WsModel)), C.c_int32, C.POINTER(WsOpts),
+                                             C.POINTER(WsShape), C.POINTER(WsShape), C.c_int32]
+            L.ws_tune_cache_get.argtypes = [C.c_char_p, C.POINTER(WsShape)]
+            L.ws_tune_cache_put.argtypes = [C.c_char_p, C.POINTER(WsShape)]
             L.ws_side_order.argtypes = [C.c_void_p]
             L.ws_side_order.restype = C.c_int
             L.ws_device_bytes.argtypes = [C.c_void_p]

@@ -7,6 +7,7 @@
 #include <deque>
 #include <functional>
 #include <limits>
+#include <map>
 #include <memory>
 #include <numeric>
 #include <type_traits>
@@ -18,6 +19,7 @@
 #include "dr_kernels.hpp"
 #include "errors.hpp"
 #include "host_goals.hpp"
+#include "tune.hpp"
 
 using namespace wsb;
 
@@ -157,7 +159,8 @@ struct ws_ctx {
   cudaGraphExec_t graph = nullptr;
   int graphIters = 0, graphKey = -1, graphLaunches = 0;
   PlainFork fork{};              // plain form: the crossing kernel's stream and the fork / join events
-  bool plainRoles = false;       // plain form: each split phase as one launch with block roles instead of the fork
+  int plainMode = 0;             // plain form: 0 forked graph branches, 1 one launch a phase with block roles, 2 one kernel a phase
+  ws_shape launch{};             // the launch shape in use (ws_get_shape)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t evChunk[8] = {};   // pipelined downloads: one per chunk of the device-to-host copy
   double lastMs = 0;
@@ -677,16 +680,15 @@ bool anyExt(const ws_ctx *c) {
 #define WSB_PLAIN_FORK 1     // the plain form's element phase as two kernels on forked branches (0: one kernel)
 #endif
 const PlainFork *plainFork(const ws_ctx *c) { return (WSB_PLAIN_FORK && c->fork.side) ? &c->fork : nullptr; }
-// how the plain form launches its split phases, from WEAVESIM_PLAIN_LAUNCH: "roles" (one launch a phase, blocks in two
-// roles), "fork" (two kernels on forked graph branches), "serial" (one kernel a phase); default fork
-bool plainRolesFromEnv() {
+// the plain form's launch mode when the options leave it to the environment: WEAVESIM_PLAIN_LAUNCH "roles" (one launch
+// a phase, blocks in two roles), "serial" (one kernel a phase), else forked graph branches
+int plainModeFromEnv() {
   const char *v = std::getenv("WEAVESIM_PLAIN_LAUNCH");
-  return v && std::strcmp(v, "roles") == 0;
+  if (v && std::strcmp(v, "roles") == 0) return 1;
+  if (v && std::strcmp(v, "serial") == 0) return 2;
+  return 0;
 }
-const PlainFork *plainForkFromEnv(const ws_ctx *c) {
-  const char *v = std::getenv("WEAVESIM_PLAIN_LAUNCH");
-  return (v && std::strcmp(v, "serial") == 0) ? nullptr : plainFork(c);
-}
+const PlainFork *plainForkOf(const ws_ctx *c) { return c->plainMode == 2 ? nullptr : plainFork(c); }
 
 template <int P>
 void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
@@ -736,7 +738,7 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
     const bool cx = c->inst[0].contacts && c->inst[0].K;
     const bool sh = c->shortSides;
     const int chunk = std::min(nIter, 50);
-    const int key = (chunk << 3) | (ext ? 4 : 0) | (cx ? 2 : 0) | (sh ? 1 : 0);
+    const int key = ((chunk * 4 + c->plainMode) << 3) | (ext ? 4 : 0) | (cx ? 2 : 0) | (sh ? 1 : 0);
     if (chunk > 0 && (!c->graph || c->graphKey != key)) {
       if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
       cudaGraph_t gr;
@@ -744,7 +746,7 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
       int nl = 0;
       for (int i = 0; i < chunk; i++)
         CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, ext, c->st, &nl, c->dBar + 2,
-                              plainForkFromEnv(c), c->plainRoles));
+                              plainForkOf(c), c->plainMode == 1));
       CK(cudaStreamEndCapture(c->st, &gr));
       CK(cudaGraphInstantiate(&c->graph, gr, 0));
       cudaGraphDestroy(gr);
@@ -757,7 +759,7 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
     int nl = 0;
     for (; done < nIter; done++)
       CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, ext, c->st, &nl, c->dBar + 2,
-                            plainForkFromEnv(c), c->plainRoles));
+                            plainForkOf(c), c->plainMode == 1));
     c->lastLaunches += nl;
   }
   CK(cudaEventRecord(c->ev1, c->st));
@@ -915,6 +917,165 @@ void selectResident(ws_ctx *c) {
   size_t granted = 0;
   CK(residentPrepare<P>(need, c->shortSides, &granted));
   c->residentBytes = granted;
+}
+
+// clusters of `cl` blocks of 512 threads that the device can hold at once, for the cluster kernel's variants that need
+// the most resources (0: the shape cannot launch)
+int wideFit(int prec, int cl) {
+  int fit = 1 << 30;
+  for (int sh = 0; sh < 2; sh++)
+    for (int ex = 0; ex < 2; ex++) {
+      int n = 0;
+      switch (prec) {
+        case WS_PREC_F64: n = wideClusters<PREC_F64>(512, cl, sh != 0, ex != 0); break;
+        case WS_PREC_MIXED: n = wideClusters<PREC_MIXED>(512, cl, sh != 0, ex != 0); break;
+        default: n = wideClusters<PREC_F32>(512, cl, sh != 0, ex != 0); break;
+      }
+      fit = std::min(fit, n);
+    }
+  return fit;
+}
+
+// the launch shape `sh` (the batched form's block size, state placement and wide instances; the plain form's launch
+// mode): an instance is wide from sh.wide_min nodes + segments up (never with a load protocol), so its width depends on
+// its own size and the shape only, never on the rest of the batch
+template <int P>
+void applyShape(ws_ctx *c, const ws_shape &sh) {
+  c->launch = sh;
+  c->launch.source = 0;
+  c->threads = sh.threads;
+  c->ctaGlobal = sh.cta_state == WS_CTA_GLOBAL;
+  c->plainMode = sh.plain_launch;
+  c->wideCl = c->form == WS_FORM_CTA ? sh.wide_cluster : 1;
+  c->wideMin = sh.wide_min > 0 ? sh.wide_min : 32768;
+  // a cluster shape the device cannot hold is halved until it can (1: no wide instances)
+  while (c->wideCl >= 2 && wideFit(c->prec, c->wideCl) == 0) c->wideCl /= 2;
+  const int nInst = int(c->inst.size());
+  c->isWide.assign(nInst, 0);
+  std::vector<int> wide, narrow;
+  for (int b : c->order) {
+    const InstDesc &I = c->inst[b];
+    const bool w = c->form == WS_FORM_CTA && c->wideCl >= 2 && I.n + I.m >= c->wideMin && !I.utmMode;
+    c->isWide[b] = w;
+    (w ? wide : narrow).push_back(b);
+  }
+  c->nWide = int(wide.size());
+  c->nNarrow = int(narrow.size());
+  if (c->nWide == 0) c->wideCl = 0;
+  c->launch.wide_cluster = c->wideCl ? c->wideCl : 1;
+  if (c->nNarrow) CK(cudaMemcpyAsync(c->dOrder, narrow.data(), sizeof(int) * c->nNarrow, cudaMemcpyHostToDevice, c->st));
+  if (c->nWide) CK(cudaMemcpyAsync(c->dWide, wide.data(), sizeof(int) * c->nWide, cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));    // the host vectors above go out of scope
+  selectResident<P>(c);
+}
+
+// what the choice of shape depends on, for the tuner's size bucket
+TuneInfo tuneInfo(const ws_ctx *c) {
+  TuneInfo t;
+  t.form = c->form; t.prec = c->prec; t.nInst = int(c->inst.size()); t.shortSides = c->shortSides ? 1 : 0; t.ext = anyExt(c);
+  for (const InstDesc &I : c->inst) {
+    t.maxElems = std::max<long long>(t.maxElems, I.n + I.m);
+    t.totalElems += I.n + I.m;
+  }
+  return t;
+}
+std::string deviceName(int dev) {
+  cudaDeviceProp p{};
+  if (cudaGetDeviceProperties(&p, dev) != cudaSuccess) { cudaGetLastError(); return "none"; }
+  return std::string(p.name) + "-sm" + std::to_string(p.multiProcessorCount);
+}
+
+// The autotuner: every candidate shape (tune.cpp) runs the same short trial from the context's starting state, timed with
+// CUDA events on the context's stream after an untimed run of the same length (for the plain form, the graph capture);
+// the fastest is kept, stored in the cache under the batch's size bucket, and the starting state is put back.  The
+// state is restored between trials from a device copy of the arena and the control blocks (or, when the device has no
+// room for the copy, by uploading the starting state again from the host goals).
+template <int P>
+void tuneCtx(ws_ctx *c) {
+  const TuneInfo info = tuneInfo(c);
+  const std::string key = tuneKey(deviceName(c->device), info);
+  ws_shape hit{};
+  if (tuneLookup(key, &hit)) {
+    applyShape<P>(c, hit);
+    c->launch = hit;
+    c->launch.wide_cluster = c->wideCl ? c->wideCl : 1;
+    c->launch.source = 2;
+    return;
+  }
+  const int nInst = int(c->inst.size());
+  std::vector<InstCtl> ctl0(nInst);
+  CK(cudaMemcpyAsync(ctl0.data(), c->dCtl, sizeof(InstCtl) * nInst, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  char *snap = nullptr;
+  size_t freeB = 0, totalB = 0;
+  if (cudaMemGetInfo(&freeB, &totalB) == cudaSuccess && freeB > c->bytes + (size_t(1) << 30)) {
+    if (cudaMalloc(&snap, c->bytes) != cudaSuccess) { cudaGetLastError(); snap = nullptr; }
+  }
+  if (snap) CK(cudaMemcpyAsync(snap, c->arena, c->bytes, cudaMemcpyDeviceToDevice, c->st));
+  auto restore = [&]() {
+    if (snap) {
+      CK(cudaMemcpyAsync(c->arena, snap, c->bytes, cudaMemcpyDeviceToDevice, c->st));
+    } else {
+      CK(cudaMemsetAsync(c->arena, 0, c->bytes, c->st));
+      uploadAll<P>(c);
+    }
+    CK(cudaMemcpyAsync(c->dCtl, ctl0.data(), sizeof(InstCtl) * nInst, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  };
+  const int iters = c->form == WS_FORM_PLAIN ? 200 : 50;
+  auto trial = [&](const ws_shape &sh) {
+    applyShape<P>(c, sh);
+    restore();
+    stepImpl<P>(c, iters, nullptr);      // untimed: first launches, graph capture
+    restore();
+    stepImpl<P>(c, iters, nullptr);
+    float ms = 0;
+    CK(cudaEventSynchronize(c->ev1));
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    return double(ms);
+  };
+  // shapes that launch the same kernels the same way are timed once
+  auto effective = [&]() {
+    return std::to_string(c->form == WS_FORM_CTA ? (c->threads > 0 ? c->threads : (c->residentBytes ? 512 : 256)) : 0) + "/" +
+           std::to_string(c->residentBytes ? 1 : 0) + "/" + std::to_string(c->wideCl) + "/" + std::to_string(c->nWide) + "/" +
+           std::to_string(c->plainMode);
+  };
+  std::map<std::string, double> seen;
+  ws_shape best{};
+  double bestMs = INFINITY, defMs = NAN;
+  int trials = 0;
+  auto run = [&](const std::vector<ws_shape> &cands) {
+    for (const ws_shape &sh : cands) {
+      applyShape<P>(c, sh);
+      const std::string e = effective();
+      double ms;
+      auto it = seen.find(e);
+      if (it != seen.end()) {
+        ms = it->second;
+      } else {
+        ms = trial(sh);
+        seen[e] = ms;
+        trials++;
+      }
+      if (ms < bestMs) { bestMs = ms; best = sh; }
+    }
+  };
+  // the default shape first, for comparison
+  ws_shape def{};
+  def.threads = 0; def.cta_state = WS_CTA_AUTO; def.wide_cluster = 2; def.wide_min = 32768; def.plain_launch = 0;
+  run({def});
+  defMs = bestMs;
+  run(tuneStage1(info));
+  run(tuneStage2(info, best));
+  applyShape<P>(c, best);
+  restore();
+  if (snap) cudaFree(snap);
+  // the plain form's graph of the trial length is kept; a step of another length captures its own
+  c->launch.source = 1;
+  c->launch.trials = trials;
+  c->launch.trial_ms = bestMs;
+  c->launch.default_ms = defMs;
+  tuneStore(key, c->launch);
 }
 
 // a warm start may change the slide limit or switch contacts: on a change of side order, every instance's order and
@@ -1090,23 +1251,6 @@ int guarded(const char *what, F &&f) {
     default: FN<PREC_F32>(__VA_ARGS__); break;                \
   }
 
-// clusters of `cl` blocks of 512 threads that the device can hold at once, for the cluster kernel's variants that need
-// the most resources (0: the shape cannot launch)
-int wideFit(int prec, int cl) {
-  int fit = 1 << 30;
-  for (int sh = 0; sh < 2; sh++)
-    for (int ex = 0; ex < 2; ex++) {
-      int n = 0;
-      switch (prec) {
-        case WS_PREC_F64: n = wideClusters<PREC_F64>(512, cl, sh != 0, ex != 0); break;
-        case WS_PREC_MIXED: n = wideClusters<PREC_MIXED>(512, cl, sh != 0, ex != 0); break;
-        default: n = wideClusters<PREC_F32>(512, cl, sh != 0, ex != 0); break;
-      }
-      fit = std::min(fit, n);
-    }
-  return fit;
-}
-
 void destroyCtx(ws_ctx *c) {
   if (!c) return;
   if (c->graph) cudaGraphExecDestroy(c->graph);
@@ -1171,7 +1315,7 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
       CK(cudaEventCreateWithFlags(&c->fork.join, cudaEventDisableTiming));
       CK(cudaEventCreateWithFlags(&c->fork.fork2, cudaEventDisableTiming));
       CK(cudaEventCreateWithFlags(&c->fork.join2, cudaEventDisableTiming));
-      c->plainRoles = plainRolesFromEnv();
+      c->plainMode = plainModeFromEnv();
     }
     c->pinnedOK = true;
     CK(cudaEventCreate(&c->ev0));
@@ -1194,36 +1338,16 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     c->order.resize(n_instances);
     std::iota(c->order.begin(), c->order.end(), 0);
     std::stable_sort(c->order.begin(), c->order.end(), [&](int a, int b) { return c->inst[a].n + c->inst[a].m > c->inst[b].n + c->inst[b].m; });
-    // batched form: instances from wide_min nodes + segments up run on a cluster of blocks each (an instance's width
-    // depends on its own size only, so its result does not depend on the rest of the batch)
-    c->isWide.assign(n_instances, 0);
-    std::vector<int> wide, narrow;
-    if (o.form == WS_FORM_CTA) {
-      c->wideCl = o.wide_cluster == 0 ? 2 : o.wide_cluster;
-      c->wideMin = o.wide_min > 0 ? o.wide_min : 32768;
-      if (c->wideCl < 1 || c->wideCl > 8) throw std::invalid_argument("wide_cluster must be 0 (default), 1 (off) or 2..8");
-      // a cluster shape the device cannot hold is halved until it can (1: no wide instances)
-      while (c->wideCl >= 2 && wideFit(c->prec, c->wideCl) == 0) c->wideCl /= 2;
-    }
-    for (int b : c->order) {
-      const InstDesc &I = c->inst[b];
-      const bool w = o.form == WS_FORM_CTA && c->wideCl >= 2 && I.n + I.m >= c->wideMin && !I.utmMode;
-      c->isWide[b] = w;
-      (w ? wide : narrow).push_back(b);
-    }
-    c->nWide = int(wide.size());
-    c->nNarrow = int(narrow.size());
-    if (c->nWide == 0) c->wideCl = 0;
+    if (o.wide_cluster < 0 || o.wide_cluster > 8 || o.wide_min < 0)
+      throw std::invalid_argument("wide_cluster must be 0 (default), 1 (off) or 2..8; wide_min 0 (default) or more");
+    if (o.tune < 0 || o.tune > 1) throw std::invalid_argument("tune must be 0 or 1");
     CK(cudaMalloc(&c->dInst, sizeof(InstDesc) * n_instances));
     CK(cudaMalloc(&c->dCtl, sizeof(InstCtl) * n_instances));
     CK(cudaMalloc(&c->dOrder, sizeof(int) * n_instances));
+    CK(cudaMalloc(&c->dWide, sizeof(int) * n_instances));
     CK(cudaMalloc(&c->dMask, n_instances));
     CK(cudaMemcpyAsync(c->dInst, c->inst.data(), sizeof(InstDesc) * n_instances, cudaMemcpyHostToDevice, c->st));
-    if (c->nNarrow)
-      CK(cudaMemcpyAsync(c->dOrder, narrow.data(), sizeof(int) * c->nNarrow, cudaMemcpyHostToDevice, c->st));
-    if (c->nWide) {
-      CK(cudaMalloc(&c->dWide, sizeof(int) * c->nWide));
-      CK(cudaMemcpyAsync(c->dWide, wide.data(), sizeof(int) * c->nWide, cudaMemcpyHostToDevice, c->st));
+    if (o.form == WS_FORM_CTA) {
       CK(cudaStreamCreateWithFlags(&c->sideCta, cudaStreamNonBlocking));
       CK(cudaEventCreateWithFlags(&c->ctaFork, cudaEventDisableTiming));
       CK(cudaEventCreateWithFlags(&c->ctaJoin, cudaEventDisableTiming));
@@ -1265,7 +1389,11 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     CK(cudaMalloc(&c->dErr, sizeof(int)));
     c->shortSides = shortOrderOK(c);
     DISPATCH(c, setupDev, c);
-    DISPATCH(c, selectResident, c);
+    ws_shape sh{};
+    sh.threads = o.threads; sh.cta_state = o.cta_state; sh.wide_cluster = o.wide_cluster == 0 ? 2 : o.wide_cluster;
+    sh.wide_min = o.wide_min > 0 ? o.wide_min : 32768; sh.plain_launch = c->plainMode;
+    DISPATCH(c, applyShape, c, sh);
+    if (o.tune) DISPATCH(c, tuneCtx, c);
     size_t total = c->bytes + (sizeof(InstDesc) + sizeof(InstCtl) + 8) * n_instances;
     if (o.budget_bytes && total > o.budget_bytes) throw std::bad_alloc();
     CK(cudaStreamSynchronize(c->st));
@@ -1326,6 +1454,78 @@ void *ws_stream(ws_ctx *c) { return c ? c->st : nullptr; }
 uint64_t ws_device_bytes(const ws_ctx *c) { return c ? c->bytes : 0; }
 int ws_side_order(const ws_ctx *c) { return c && c->shortSides ? 1 : 0; }
 int ws_cta_resident(const ws_ctx *c) { return c && c->residentBytes ? 1 : 0; }
+int ws_get_shape(const ws_ctx *c, ws_shape *out) {
+  if (!c || !out) return fail(WS_ERR_ARG, "ws_get_shape: bad arguments");
+  *out = c->launch;
+  return WS_OK;
+}
+
+// the tuner's view of a batch that has no context yet: host goals and descriptors only, nothing on a device
+static int infoFromModels(const ws_model *const *models, int32_t n, const ws_opts *opts, TuneInfo *out, const char *who) {
+  if (!models || n <= 0 || !out) return fail(WS_ERR_ARG, std::string(who) + ": need at least one model");
+  ws_opts o{};
+  if (opts) o = *opts;
+  if (o.form < 0 || o.form > 2 || o.precision < 0 || o.precision > 2) return fail(WS_ERR_ARG, std::string(who) + ": bad options");
+  return guarded(who, [&]() {
+    ws_ctx tmp;
+    tmp.form = o.form; tmp.prec = o.precision;
+    tmp.sidesGeneral = o.side_order == WS_SIDES_GENERAL;
+    tmp.g.resize(n);
+    Sizes off;
+    for (int b = 0; b < n; b++) {
+      if (!models[b]) throw std::invalid_argument("null model");
+      tmp.g[b].build(*models[b]);
+      off.b = b;
+      tmp.inst.push_back(describe(tmp.g[b], off));
+      off.n += tmp.g[b].n; off.m += tmp.g[b].m; off.p += tmp.g[b].p; off.c += tmp.g[b].C; off.k += tmp.g[b].K; off.s += tmp.g[b].S;
+    }
+    tmp.shortSides = shortOrderOK(&tmp);
+    *out = tuneInfo(&tmp);
+  });
+}
+
+int ws_tune_key(const ws_model *const *models, int32_t n, const ws_opts *opts, const char *device, char *buf, size_t cap) {
+  TuneInfo t;
+  int rc = infoFromModels(models, n, opts, &t, "ws_tune_key");
+  if (rc != WS_OK) return rc;
+  std::string dev;
+  if (device) {
+    dev = device;
+  } else {
+    int d = 0;
+    dev = (ws_device_count() > 0 && cudaGetDevice(&d) == cudaSuccess) ? deviceName(d) : "none";
+  }
+  const std::string k = tuneKey(dev, t);
+  if (!buf || cap < k.size() + 1) return fail(WS_ERR_ARG, "ws_tune_key: buffer too small");
+  std::memcpy(buf, k.c_str(), k.size() + 1);
+  return WS_OK;
+}
+
+int ws_tune_candidates(const ws_model *const *models, int32_t n, const ws_opts *opts, const ws_shape *after, ws_shape *out,
+                       int32_t cap) {
+  TuneInfo t;
+  int rc = infoFromModels(models, n, opts, &t, "ws_tune_candidates");
+  if (rc != WS_OK) return rc;
+  const std::vector<ws_shape> v = after ? tuneStage2(t, *after) : tuneStage1(t);
+  for (int i = 0; i < int(v.size()) && i < cap && out; i++) out[i] = v[i];
+  return int(v.size());
+}
+
+int ws_tune_cache_get(const char *key, ws_shape *out) {
+  if (!key) return fail(WS_ERR_ARG, "ws_tune_cache_get: null key");
+  return tuneLookup(key, out) ? 1 : 0;
+}
+int ws_tune_cache_put(const char *key, const ws_shape *shape) {
+  if (!key || !shape || !*key || std::strchr(key, ' ') || std::strchr(key, '\n'))
+    return fail(WS_ERR_ARG, "ws_tune_cache_put: a key is one word");
+  tuneStore(key, *shape);
+  return WS_OK;
+}
+int ws_tune_cache_clear(void) {
+  tuneClear();
+  return WS_OK;
+}
+
 int ws_wide_instances(const ws_ctx *c, int32_t *cluster) {
   if (cluster) *cluster = c ? c->wideCl : 0;
   return c ? c->nWide : 0;

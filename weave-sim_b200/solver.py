@@ -67,9 +67,64 @@ def relax_noalloc(model, n_iter, precision="mixed", threads=256, stream=None):
     return out, ctl.as_dict()
 
 
+def _opts(precision="mixed", form="cta", side_order="auto"):
+    o = WsOpts()
+    o.precision = _lib.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    o.form = _lib.FORMS[form] if isinstance(form, str) else int(form)
+    o.side_order = {"auto": 0, "general": 1}[side_order]
+    return o
+
+
+def _model_array(models):
+    structs = [m.struct() for m in models]
+    return structs, (C.POINTER(_lib.WsModel) * len(structs))(*[C.pointer(s) for s in structs])
+
+
+def tune_key(models, precision="mixed", form="cta", device=None) -> str:
+    """the autotuner's size bucket of a batch (ws_tune_key; needs no GPU when `device` names one)"""
+    keep, arr = _model_array(models)
+    o = _opts(precision, form)
+    buf = C.create_string_buffer(512)
+    check(lib().ws_tune_key(arr, len(models), C.byref(o), device.encode() if device else None, buf, 512), "ws_tune_key")
+    return buf.value.decode()
+
+
+def tune_candidates(models, precision="mixed", form="cta", after=None):
+    """the shapes the autotuner times (ws_tune_candidates): stage 1, or stage 2 at the stage-1 shape `after` (a dict)"""
+    keep, arr = _model_array(models)
+    o = _opts(precision, form)
+    aft = None
+    if after is not None:
+        aft = _lib.WsShape()
+        for k in ("threads", "cta_state", "wide_cluster", "wide_min", "plain_launch"):
+            setattr(aft, k, int(after[k]))
+    out = (_lib.WsShape * 64)()
+    n = lib().ws_tune_candidates(arr, len(models), C.byref(o), C.byref(aft) if aft is not None else None, out, 64)
+    if n < 0:
+        check(n, "ws_tune_candidates")
+    return [out[i].as_dict() for i in range(min(n, 64))]
+
+
+def tune_cache_get(key):
+    sh = _lib.WsShape()
+    return sh.as_dict() if lib().ws_tune_cache_get(key.encode(), C.byref(sh)) == 1 else None
+
+
+def tune_cache_put(key, shape: dict):
+    sh = _lib.WsShape()
+    for k, v in shape.items():
+        if k != "source":
+            setattr(sh, k, v)
+    check(lib().ws_tune_cache_put(key.encode(), C.byref(sh)), "ws_tune_cache_put")
+
+
+def tune_cache_clear():
+    lib().ws_tune_cache_clear()
+
+
 class GpuSolver:
     def __init__(self, models, precision="mixed", form="cta", threads=0, device=0, budget_bytes=0, side_order="auto",
-                 cta_state="auto", wide_cluster=0, wide_min=0):
+                 cta_state="auto", wide_cluster=0, wide_min=0, tune=False):
         if not isinstance(models, (list, tuple)):
             models = [models]
         self.models = list(models)
@@ -82,7 +137,7 @@ class GpuSolver:
         opts.threads, opts.device, opts.budget_bytes = int(threads), int(device), int(budget_bytes)
         opts.side_order = {"auto": 0, "general": 1}[side_order]
         opts.cta_state = {"auto": 0, "global": 1}[cta_state]
-        opts.wide_cluster, opts.wide_min = int(wide_cluster), int(wide_min)
+        opts.wide_cluster, opts.wide_min, opts.tune = int(wide_cluster), int(wide_min), int(bool(tune))
         self.precision, self.form = precision, form
         h = C.c_void_p()
         check(lib().ws_create(arr, self.B, C.byref(opts), C.byref(h)), "ws_create")
@@ -166,6 +221,14 @@ class GpuSolver:
     def resident(self):
         """True when the batched form holds its instances in shared memory"""
         return bool(lib().ws_cta_resident(self.h))
+
+    @property
+    def shape(self):
+        """the launch shape in use (ws_get_shape): threads, cta_state, wide_cluster, wide_min, plain_launch, and whether
+        it came from the options, the tuner or the tuner's cache"""
+        sh = _lib.WsShape()
+        check(lib().ws_get_shape(self.h, C.byref(sh)), "ws_get_shape")
+        return sh.as_dict()
 
     @property
     def wide(self):

@@ -166,7 +166,8 @@ def _plain_iter_ms(models, precision, iters=200):
     return out
 
 
-def run_batch(count=512, iters=CAP, precision="mixed", threads=0, seed=4, wide_cluster=0, wide_min=0, plain_sample=16):
+def run_batch(count=512, iters=CAP, precision="mixed", threads=0, seed=4, wide_cluster=0, wide_min=0, plain_sample=16,
+              tune=False):
     """the uneven batch in one batched step to the iteration cap; per-instance device times (from the block or cluster
     taking the instance up to its leaving it); and the plain single-instance form on a size-stratified sample of the
     same instances, whose per-iteration times, interpolated over the sizes of all instances, give the time the plain form
@@ -175,9 +176,10 @@ def run_batch(count=512, iters=CAP, precision="mixed", threads=0, seed=4, wide_c
     for m in models:
         m.params = dict(m.params, max_iter=iters)
     t0 = time.perf_counter()
-    s = GpuSolver(models, precision=precision, threads=threads, wide_cluster=wide_cluster, wide_min=wide_min)
+    s = GpuSolver(models, precision=precision, threads=threads, wide_cluster=wide_cluster, wide_min=wide_min, tune=tune)
     create_s = time.perf_counter() - t0
     n_wide, cl = s.wide
+    shape = s.shape
     ctl = s.step(iters)
     ms, nl = s.last_step_stats()
     dev_bytes = s.device_bytes
@@ -193,7 +195,7 @@ def run_batch(count=512, iters=CAP, precision="mixed", threads=0, seed=4, wide_c
            "converged": sum(c["status"] == 1 for c in ctl), "nonfinite": sum(c["status"] == 3 for c in ctl),
            "nodes_min": int(n.min()), "nodes_median": int(np.median(n)), "nodes_max": int(n.max()),
            "nodes_total": int(n.sum()), "crossings_total": int(sum(m.K for m in models)), "device_bytes": dev_bytes,
-           "create_s": create_s, "launches": nl, "wide_instances": n_wide, "wide_cluster": cl,
+           "create_s": create_s, "launches": nl, "wide_instances": n_wide, "wide_cluster": cl, "shape": shape,
            "instance_device_ms": {"min": float(dev.min()), "median": float(np.median(dev)), "max": float(dev.max()),
                                   "largest_instance": float(dev[big]), "largest_instance_end": float(end[big]),
                                   "last_end": float(end.max()), "p90_end": float(np.percentile(end, 90))},
