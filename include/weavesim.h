@@ -198,6 +198,15 @@ typedef struct ws_scene ws_scene;   /* owns the arrays of one ws_model */
  * Mesh.fromBytes, mesh.js:23-31; buildTopology, topology.js; Anchors / Loads / strandStiffness, model.js:112-252), with
  * the file reading, the vertex weld and the unit conversions done by the caller (weave-sim_b200/scenefile.py). */
 enum { WS_SEL_FRAME = 0, WS_SEL_ALL_START = 1, WS_SEL_ALL_END = 2, WS_SEL_ALL_ENDS = 3, WS_SEL_STRAND = 4, WS_SEL_BOUNDARY = 5 };
+/* one lath group: its section, stiffness, prestress shares, self-weight per length and material across the grain,
+ * in the same meaning as the ws_mesh_cfg fields of those names */
+typedef struct ws_lath_group {
+  double width, height;
+  double EA, EIx, EIy, GJ, GA;
+  double activation[3];
+  double line_weight;
+  double fc90, E90, H;
+} ws_lath_group;
 typedef struct ws_mesh_cfg {
   int32_t n_vertices, n_faces;
   const double *vertices;      /* [3 n_vertices] welded and scaled (Mesh.fromBytes) */
@@ -213,8 +222,10 @@ typedef struct ws_mesh_cfg {
   double activation[3];        /* prestress shares (flat, edge, twist): rest curvature (1 − a) × the as-built one */
   double line_weight;          /* self-weight per length in scene units (UnitSystem.selfWeightLineLoad); 0: none */
   double gravity_dir[3];
-  int32_t udl_on, pad0;
-  double udl[3];               /* loads.udl per length, on the nodes' tributary lengths */
+  int32_t udl_on;              /* 1: loads.udl per length, on the nodes' tributary lengths; 2: per area, the mesh's
+                                  area shared in proportion to the tributary lengths (Loads, model.js:213-220) */
+  int32_t pad0;
+  double udl[3];
   double mu;                   /* contact.mu */
   double fc90, E90, H;         /* material across the grain */
   int32_t n_anchors, pad1;
@@ -226,6 +237,14 @@ typedef struct ws_mesh_cfg {
   const double *load_F;        /* [3 n_loads] */
   const uint8_t *load_local;   /* [n_loads] 1: in the node frame */
   ws_params params;
+  /* lath groups of a hybrid weave (scene.hybrid, web/js/scene.js:50-68; strandStiffness, model.js:236-252): group g
+   * >= 2 of strand s (assign_strand[i] = s, assign_group[i] = g) takes groups[g - 2]'s section, stiffness,
+   * activation, self-weight and material across the grain for its segments, joints (the group of the joint's first
+   * segment), crossing sides and nodes, and its height for the knot offsets (the mean of the two strands' heights,
+   * topology.js:225); every other strand takes the fields above.  n_groups = 0: one group. */
+  int32_t n_groups, n_assign;
+  const struct ws_lath_group *groups;
+  const int32_t *assign_strand, *assign_group;
 } ws_mesh_cfg;
 int ws_scene_mesh(const ws_mesh_cfg *cfg, ws_scene **out);
 

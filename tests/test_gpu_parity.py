@@ -776,6 +776,46 @@ def test_reference_scene_matches_oracle(oracle_mod):
         assert np.array_equal(g["stuck"], v["stuck"])
 
 
+@pytest.mark.parametrize("name", ["v5dome_cm", "v5dome_BugTest", "v5dome_failure", "dualv5dome_cm",
+                                  "dualv5dome_cm_hybrid", "tree_cm"])
+def test_example_scenes_match_oracle(oracle_mod, name):
+    """the reference's other example scenes (lath groups by strand, udl per area, the contact extensions they switch on)
+    read by the scene reader: 1000 iterations in FP64 against the oracle, batched and plain (the reference holds its
+    GPU form to the CPU over 1000 iterations of v5dome_cm, web/tests/selftest.html:38-43)"""
+    import os
+    md = ws.load_scene(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", name + "_scene.json"))
+    o = oracle_mod.Oracle(md.copy())
+    o.step(1000)
+    v = o.view()
+    for form in ("cta", "plain"):
+        s = ws.GpuSolver([md.copy()], precision="f64", form=form)
+        ctl = s.step(1000)[0]
+        g = s.download(0, fields=("X", "stuck"))
+        s.dispose()
+        assert ctl["iter"] == 1000 and ctl["rollbacks"] == v["rollbacks"], form
+        assert cases.max_rel_disp_error(g["X"], v["X"], v["X0"]) < 1e-9, form
+        assert np.array_equal(g["stuck"], v["stuck"]), form
+
+
+def test_v5dome_mixed_tracks_f64(oracle_mod):
+    """the reference's own GPU-parity scene in the mixed policy: its f32 GPU form tracks the f64 CPU solver to 1.2e-5 of
+    the largest displacement through 1000 iterations with the same kinetic-damping resets (web/README.md:82-84)"""
+    import os
+    md = ws.load_scene(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "v5dome_cm_scene.json"))
+    o = oracle_mod.Oracle(md.copy())
+    o.step(1000)
+    v = o.view()
+    for form in ("cta", "plain"):
+        s = ws.GpuSolver([md.copy()], precision="mixed", form=form)
+        ctl = s.step(1000)[0]
+        g = s.download(0, fields=("X",))
+        s.dispose()
+        err = cases.max_rel_disp_error(g["X"], v["X"], v["X0"])
+        cases.record(f"v5dome_mixed_{form}", {"rel_disp_err": err, "rollbacks": ctl["rollbacks"],
+                                              "oracle_rollbacks": v["rollbacks"]})
+        assert ctl["rollbacks"] == v["rollbacks"] and err < 1.2e-5, (form, err)
+
+
 # ------------------------------------------------------------------------------------------------ node numbering
 # A crossing side's nodes and neighbouring segments are computed from the strand's first node when every crossing
 # strand numbers its nodes consecutively (the builders' layout), and gathered otherwise; a renumbered model takes the

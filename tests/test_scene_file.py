@@ -62,3 +62,73 @@ def test_oracle_runs_the_scene(oracle_mod):
     o.step(300)
     v = o.view()
     assert np.all(np.isfinite(v["X"])) and v["iteration"] == 300
+
+
+# ---------------------------------------------------------------------------------------------- the other example scenes
+SCENES = ("v5dome_cm", "v5dome_BugTest", "v5dome_failure", "dualv5dome_cm", "dualv5dome_cm_hybrid", "tree_cm")
+
+
+def _scene(name):
+    return os.path.join(HERE, "golden", name + "_scene.json")
+
+
+@pytest.mark.parametrize("name,counts", [("v5dome_cm", (1020, 1000, 130)), ("v5dome_BugTest", (1020, 1000, 130)),
+                                         ("v5dome_failure", (1020, 1000, 130)), ("dualv5dome_cm", (3984, 3936, 504)),
+                                         ("dualv5dome_cm_hybrid", (3984, 3936, 504)), ("tree_cm", (3612, 3576, 450))])
+def test_every_example_scene_reads(name, counts, oracle_mod):
+    md = ws.load_scene(_scene(name))
+    assert (md.n, md.m, md.K) == counts
+    o = oracle_mod.Oracle(md.copy())
+    o.step(200)
+    assert np.all(np.isfinite(o.view()["X"]))
+
+
+def _strand_of_segments(md):
+    return np.repeat(np.arange(md.n_strands), np.diff(md.seg_offset))
+
+
+def test_lath_groups_by_strand():
+    """dualv5dome_cm_hybrid (scene.hybrid: group 2 assigned to six strands): their segments carry group 2's stiffness,
+    their crossing sides its section, their nodes its width and height, and their self-weight its density and section
+    (strandStiffness, model.js:236-252; Loads, model.js:203-207; the contact's sections, solver_cpu.js:682-684)"""
+    import json
+    d = json.load(open(_scene("dualv5dome_cm_hybrid")))
+    grp = d["hybrid"]["groups"][0]
+    assigned = sorted(int(k) for k, v in d["hybrid"]["assign"].items() if int(v) == 2)
+    md = ws.load_scene(_scene("dualv5dome_cm_hybrid"))
+    plain = ws.load_scene(_scene("dualv5dome_cm"))
+    w2, h2 = float(grp["section"]["width"]), float(grp["section"]["height"])
+    E2 = float(grp["material"]["E"])
+    seg_strand = _strand_of_segments(md)
+    in2 = np.isin(seg_strand, assigned)
+    assert in2.any() and not in2.all()
+    assert np.allclose(md.EA[in2], E2 * w2 * h2) and np.allclose(md.EA[~in2], md.EA[~in2][0])
+    assert md.EA[~in2][0] != md.EA[in2][0]
+    side_in2 = np.isin(md.cross_strand, assigned)
+    assert np.allclose(md.cross_wk[side_in2], w2) and np.allclose(md.cross_hk[side_in2], h2)
+    node_strand = np.repeat(np.arange(md.n_strands), np.diff(md.node_offset))
+    assert np.allclose(md.node_w[np.isin(node_strand, assigned)], w2)
+    # the knots on an assigned strand sit at the mean height of the two crossing strands: the geometry moves there
+    assert not np.array_equal(md.X, plain.X)
+
+
+def test_udl_per_area():
+    """dualv5dome_cm: udl per area; the mesh's area shared in proportion to the nodes' tributary lengths (Loads,
+    model.js:216-219): the total is area x q"""
+    import json
+    d = json.load(open(_scene("dualv5dome_cm")))
+    q = np.array(d["loads"]["udl"]["q"], dtype=float)
+    z = np.load(os.path.join(HERE, "golden", "dualv5dome_cm_mesh.npz"))
+    V, F = z["V"].reshape(-1, 3), z["F"].reshape(-1, 3)
+    area = 0.5 * np.linalg.norm(np.cross(V[F[:, 1]] - V[F[:, 0]], V[F[:, 2]] - V[F[:, 0]]), axis=1).sum()
+    md = ws.load_scene(_scene("dualv5dome_cm"))
+    d["loads"]["udl"]["enabled"] = False
+    off = json.loads(json.dumps(d))
+    import tempfile
+    with tempfile.TemporaryDirectory() as t:
+        p = os.path.join(t, "s.json")
+        off["mesh"]["path"] = os.path.join(HERE, "golden", "dualv5dome_cm_mesh.npz")
+        json.dump(off, open(p, "w"))
+        base = ws.load_scene(p)
+    added = (md.load_const - base.load_const).reshape(-1, 3).sum(0)
+    assert np.allclose(added, area * q, rtol=1e-12, atol=1e-12 * abs(area * q).max())

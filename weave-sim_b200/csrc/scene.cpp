@@ -347,8 +347,12 @@ static void buildPolylines(Topology &topo, const WeaveParams &p) {
     for (int k = 0; k < nk; k++) {
       int e = s.edges[k];
       Nn[k] = en(e);
-      sign[k] = isOverFrame(topo.knots[topo.knotIndex.at(e)], s.index, k) ? 1.0 : -1.0;
-      K[k] = add3(mid(e), scl3(Nn[k], 0.5 * h * sign[k]));
+      const Knot &kn = topo.knots[topo.knotIndex.at(e)];
+      sign[k] = isOverFrame(kn, s.index, k) ? 1.0 : -1.0;
+      // with lath groups the knot's offset is the mean height of its two strands (topology.js:225)
+      const double he = (!topo.strandThickness.empty() && p.half_height)
+                            ? 0.5 * (topo.strandThickness[kn.a.s] + topo.strandThickness[kn.b.s]) : h;
+      K[k] = add3(mid(e), scl3(Nn[k], 0.5 * he * sign[k]));
       K0[k] = mid(e);
       off[k] = (0.5 * h) * sign[k];
     }
@@ -453,10 +457,25 @@ static void consistentFrames(Topology &topo) {
   }
 }
 
-Topology buildTopology(const Mesh &mesh, const WeaveParams &p, double thickness) {
+double Mesh::area() const {
+  double a = 0;
+  for (int f = 0; f < nF; f++) {
+    const double *p = &V[3 * size_t(F[3 * f])], *q = &V[3 * size_t(F[3 * f + 1])], *r = &V[3 * size_t(F[3 * f + 2])];
+    const double ux = q[0] - p[0], uy = q[1] - p[1], uz = q[2] - p[2], vx = r[0] - p[0], vy = r[1] - p[1], vz = r[2] - p[2];
+    a += 0.5 * std::hypot(uy * vz - uz * vy, uz * vx - ux * vz, ux * vy - uy * vx);
+  }
+  return a;
+}
+
+Topology buildTopology(const Mesh &mesh, const WeaveParams &p, double thickness, const std::vector<double> *strandThickness) {
   Topology topo;
   topo.mesh = &mesh; topo.thickness = thickness; topo.overhang = p.overhang;
   traceStrands(topo);
+  if (strandThickness) {
+    // a strand the caller's table does not reach keeps the base thickness
+    topo.strandThickness.assign(topo.strands.size(), thickness);
+    for (size_t s = 0; s < topo.strands.size() && s < strandThickness->size(); s++) topo.strandThickness[s] = (*strandThickness)[s];
+  }
   assignParity(topo, p.seed_strand_phase);
   for (auto &fk : p.flip_knots) {                           // applyFlips: topology.js:203-211
     auto it = topo.frameToKnot.find(fkey(fk.first, fk.second));
@@ -780,37 +799,82 @@ Scene *buildMeshScene(const ws_mesh_cfg &cfg) {
   wp.subdivisions = cfg.subdivisions; wp.overhang = cfg.overhang; wp.half_height = cfg.half_height != 0;
   wp.seed_strand_phase = cfg.seed_strand_phase;
   for (int f = 0; f < cfg.n_flips; f++) wp.flip_knots.push_back({cfg.flips[2 * f], cfg.flips[2 * f + 1]});
-  sc->topo = buildTopology(sc->mesh, wp, cfg.height);
+  // lath groups: group 0 is the cfg's own section and material, group g >= 1 is cfg.groups[g - 1] (the scene's group
+  // g + 1); the strands' groups from the assignments (an assignment out of range leaves the strand in group 0)
+  ws_lath_group base{};
+  base.width = cfg.width; base.height = cfg.height;
+  base.EA = cfg.EA; base.EIx = cfg.EIx; base.EIy = cfg.EIy; base.GJ = cfg.GJ; base.GA = cfg.GA;
+  for (int k = 0; k < 3; k++) base.activation[k] = cfg.activation[k];
+  base.line_weight = cfg.line_weight; base.fc90 = cfg.fc90; base.E90 = cfg.E90; base.H = cfg.H;
+  std::vector<ws_lath_group> groups{base};
+  if (cfg.n_groups > 0) {
+    if (!cfg.groups) throw std::invalid_argument("mesh: lath groups without their table");
+    for (int g = 0; g < cfg.n_groups; g++) {
+      const ws_lath_group &G = cfg.groups[g];
+      if (!(G.width > 0) || !(G.height > 0)) throw std::invalid_argument("mesh: a lath group's section must be positive");
+      groups.push_back(G);
+    }
+  }
+  std::vector<int> strandAssign;         // by strand index: group (0 = base)
+  int maxStrand = -1;
+  for (int i = 0; i < cfg.n_assign; i++) maxStrand = std::max(maxStrand, cfg.assign_strand[i]);
+  strandAssign.assign(size_t(maxStrand + 1), 0);
+  for (int i = 0; i < cfg.n_assign; i++) {
+    const int s = cfg.assign_strand[i], g = cfg.assign_group[i];
+    if (s >= 0 && g >= 2 && g - 1 < int(groups.size())) strandAssign[s] = g - 1;
+  }
+  std::vector<double> thick;
+  if (groups.size() > 1)
+    for (size_t s = 0; s < strandAssign.size(); s++) thick.push_back(groups[strandAssign[s]].height);
+  sc->topo = buildTopology(sc->mesh, wp, cfg.height, groups.size() > 1 ? &thick : nullptr);
   sc->st = buildState(sc->topo);
   State &st = sc->st;
   sc->params = cfg.params;
-  // uniform section and material (strandStiffness with one lath group)
-  sc->EA.assign(st.m, cfg.EA); sc->EIx.assign(st.m, cfg.EIx); sc->EIy.assign(st.m, cfg.EIy); sc->GJ.assign(st.m, cfg.GJ);
-  sc->GA.assign(st.m, cfg.GA);
-  sc->wk.assign(2 * size_t(st.K), cfg.width); sc->hk.assign(2 * size_t(st.K), cfg.height);
-  sc->fc90.assign(2 * size_t(st.K), cfg.fc90); sc->E90.assign(2 * size_t(st.K), cfg.E90); sc->H.assign(2 * size_t(st.K), cfg.H);
-  sc->nodeW.assign(st.n, cfg.width); sc->nodeH.assign(st.n, cfg.height);
-  // rest curvature: the unprestressed share of the as-built curvature (CosseratRod constructor, rod_cosserat.js:58-66)
-  if (cfg.activation[0] < 1 || cfg.activation[1] < 1 || cfg.activation[2] < 1) {
+  auto grpOf = [&](int strand) -> const ws_lath_group & {
+    return groups[strand >= 0 && strand < int(strandAssign.size()) ? strandAssign[strand] : 0];
+  };
+  // section and material per segment, crossing side and node (strandStiffness, model.js:236-252; the contact's secOf
+  // and matOf, solver_cpu.js:682-684; the ground's node sections, solver_cpu.js:560)
+  sc->EA.resize(st.m); sc->EIx.resize(st.m); sc->EIy.resize(st.m); sc->GJ.resize(st.m); sc->GA.resize(st.m);
+  for (int j = 0; j < st.m; j++) {
+    const ws_lath_group &G = grpOf(st.segStrand[j]);
+    sc->EA[j] = G.EA; sc->EIx[j] = G.EIx; sc->EIy[j] = G.EIy; sc->GJ[j] = G.GJ; sc->GA[j] = G.GA;
+  }
+  sc->wk.resize(2 * size_t(st.K)); sc->hk.resize(2 * size_t(st.K));
+  sc->fc90.resize(2 * size_t(st.K)); sc->E90.resize(2 * size_t(st.K)); sc->H.resize(2 * size_t(st.K));
+  for (size_t q = 0; q < 2 * size_t(st.K); q++) {
+    const ws_lath_group &G = grpOf(st.crossStrand[q]);
+    sc->wk[q] = G.width; sc->hk[q] = G.height; sc->fc90[q] = G.fc90; sc->E90[q] = G.E90; sc->H[q] = G.H;
+  }
+  sc->nodeW.resize(st.n); sc->nodeH.resize(st.n);
+  for (int i = 0; i < st.n; i++) { sc->nodeW[i] = grpOf(st.nodeStrand[i]).width; sc->nodeH[i] = grpOf(st.nodeStrand[i]).height; }
+  // rest curvature: the unprestressed share of the as-built curvature (CosseratRod constructor, rod_cosserat.js:58-66),
+  // each joint with the activation of its first segment's group
+  bool prestress = false;
+  for (const ws_lath_group &G : groups) prestress = prestress || G.activation[0] < 1 || G.activation[1] < 1 || G.activation[2] < 1;
+  if (prestress) {
     sc->omega0.assign(3 * size_t(st.p), 0.0);
     for (int j = 0; j < st.p; j++) {
       double psi[3];
       relRotationVec(&st.Q[4 * size_t(st.jSeg0[j])], &st.Q[4 * size_t(st.jSeg1[j])], psi);
+      const ws_lath_group &G = grpOf(st.segStrand[st.jSeg0[j]]);
       for (int k = 0; k < 3; k++) {
-        const double a = std::min(std::max(cfg.activation[k], 0.0), 1.0);
+        const double a = std::min(std::max(G.activation[k], 0.0), 1.0);
         sc->omega0[3 * size_t(j) + k] = (1.0 - a) * (psi[k] / st.jLen[j]);
       }
     }
   }
-  // loads (Loads, model.js:191-231): self-weight per segment half to each end node, udl on the tributary lengths,
-  // point loads at frames
+  // loads (Loads, model.js:191-231): self-weight per segment (its group's) half to each end node, udl on the
+  // tributary lengths (per length) or the mesh's area shared in proportion to them (per area), point loads at frames
   sc->loadConst.assign(3 * size_t(st.n), 0.0);
-  if (cfg.line_weight != 0) {
+  bool weight = false;
+  for (const ws_lath_group &G : groups) weight = weight || G.line_weight != 0;
+  if (weight) {
     double g[3] = {cfg.gravity_dir[0], cfg.gravity_dir[1], cfg.gravity_dir[2]};
     const double gl = std::max(std::sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]), 1e-12);
     for (double &v : g) v /= gl;
     for (int j = 0; j < st.m; j++) {
-      const double q = 0.5 * st.l0[j] * cfg.line_weight;
+      const double q = 0.5 * st.l0[j] * grpOf(st.segStrand[j]).line_weight;
       for (int i : {st.segI0[j], st.segI1[j]})
         for (int c = 0; c < 3; c++) sc->loadConst[3 * size_t(i) + c] += q * g[c];
     }
@@ -819,7 +883,17 @@ Scene *buildMeshScene(const ws_mesh_cfg &cfg) {
     std::vector<double> trib(st.n, 0.0);
     for (int j = 0; j < st.m; j++) trib[st.segI0[j]] += 0.5 * st.l0[j];
     for (int j = 0; j < st.m; j++) trib[st.segI1[j]] += 0.5 * st.l0[j];
-    for (int i = 0; i < st.n; i++) for (int c = 0; c < 3; c++) sc->loadConst[3 * size_t(i) + c] += trib[i] * cfg.udl[c];
+    if (cfg.udl_on == 1) {
+      for (int i = 0; i < st.n; i++) for (int c = 0; c < 3; c++) sc->loadConst[3 * size_t(i) + c] += trib[i] * cfg.udl[c];
+    } else {
+      const double area = sc->mesh.area();
+      double total = 0;
+      for (int i = 0; i < st.n; i++) total += trib[i];
+      for (int i = 0; i < st.n; i++) {
+        const double w = trib[i] / std::max(total, 1e-12) * area;
+        for (int c = 0; c < 3; c++) sc->loadConst[3 * size_t(i) + c] += w * cfg.udl[c];
+      }
+    }
   }
   for (int l = 0; l < cfg.n_loads; l++)
     sc->addPointLoad(cfg.load_frames[2 * l], cfg.load_frames[2 * l + 1], &cfg.load_F[3 * l], cfg.load_local && cfg.load_local[l]);

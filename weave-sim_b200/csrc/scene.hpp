@@ -33,6 +33,7 @@ struct Mesh {
   int otherFace(int edge, int face) const { int a = EF[2 * edge], b = EF[2 * edge + 1]; return a == face ? b : a; }
   bool edgeHas(int e, int v) const { return E[2 * e] == v || E[2 * e + 1] == v; }
   int faceEdgeContaining(int face, int vertex, int exclude) const;
+  double area() const;                         // sum of the triangles' areas (Mesh.area, mesh.js:50-58)
 };
 
 struct Frame { int s = 0, k = 0; };
@@ -59,6 +60,7 @@ struct WeaveParams {
 struct Topology {
   const Mesh *mesh = nullptr;
   double thickness = 0, overhang = 0;
+  std::vector<double> strandThickness;         // per strand (lath groups); empty: `thickness` for every strand
   std::vector<Strand> strands;
   std::vector<Knot> knots;                     // first-pass (Map insertion) order
   std::unordered_map<int, int> knotIndex;      // edge -> index in knots
@@ -77,7 +79,8 @@ struct State {
 struct Section { double EA, EIx, EIy, GJ, GA; };
 
 Mesh hexLatticeMesh(int side, double a);
-Topology buildTopology(const Mesh &mesh, const WeaveParams &p, double thickness);
+Topology buildTopology(const Mesh &mesh, const WeaveParams &p, double thickness,
+                       const std::vector<double> *strandThickness = nullptr);
 Topology topologyFromPolylines(const std::vector<std::vector<double>> &polylines, const std::vector<std::vector<V3>> *normals,
                                double thickness, const std::vector<std::vector<int>> *knotRows);
 State buildState(const Topology &topo);

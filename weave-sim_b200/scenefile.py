@@ -4,9 +4,11 @@ Follows the reference's reading path: Scene.fromJSON (web/js/scene.js:142-190) f
 (web/js/params.js:6-25), Mesh.fromBytes (web/js/mesh.js:23-31, 62-125) for the STL / OBJ file, the vertex weld and the
 scale, UnitSystem (web/js/units.js) for the self-weight, sectionStiffness / beamFactors / beamActivations
 (params.js:43-57) for the laths; the topology, the anchors' selectors and the loads are built by the library
-(ws_scene_mesh).  Supported: one lath group (no hybrid weave), selectors frame / all_start / all_end / all_ends /
-strand / knots / boundary, loads gravity / udl per length / point (world or local), the ground, every contact and
-solver parameter the solver has.  Anything else raises NotImplementedError rather than being ignored.
+(ws_scene_mesh).  Supported: lath groups by strand (a hybrid weave: each group's material, section and beam for its
+strands' segments, joints, crossing sides, nodes, self-weight and knot offsets), selectors frame / all_start / all_end /
+all_ends / strand / knots / boundary, loads gravity / udl per length or per area / point (world or local), the ground,
+every contact and solver parameter the solver has.  Anything else (lath groups by piece of a discretisation, the region
+selector) raises NotImplementedError rather than being ignored.
 """
 from __future__ import annotations
 
@@ -49,7 +51,15 @@ class WsMeshCfg(C.Structure):
                 ("mu", C.c_double), ("fc90", C.c_double), ("E90", C.c_double), ("H", C.c_double),
                 ("n_anchors", C.c_int32), ("pad1", C.c_int32), ("anchor_kind", _lib._ip), ("anchor_id", _lib._ip),
                 ("anchor_mask", _lib._bp), ("n_loads", C.c_int32), ("pad2", C.c_int32), ("load_frames", _lib._ip),
-                ("load_F", _lib._dp), ("load_local", _lib._bp), ("params", _lib.WsParams)]
+                ("load_F", _lib._dp), ("load_local", _lib._bp), ("params", _lib.WsParams),
+                ("n_groups", C.c_int32), ("n_assign", C.c_int32), ("groups", C.c_void_p),
+                ("assign_strand", _lib._ip), ("assign_group", _lib._ip)]
+
+
+class WsLathGroup(C.Structure):
+    _fields_ = [("width", C.c_double), ("height", C.c_double), ("EA", C.c_double), ("EIx", C.c_double),
+                ("EIy", C.c_double), ("GJ", C.c_double), ("GA", C.c_double), ("activation", C.c_double * 3),
+                ("line_weight", C.c_double), ("fc90", C.c_double), ("E90", C.c_double), ("H", C.c_double)]
 
 
 def _defaults(defaults, d):
@@ -136,6 +146,37 @@ def _rect_torsion(a, b):
     return a * b ** 3 * (1.0 / 3.0 - 0.21 * r * (1.0 - r ** 4 / 12.0))
 
 
+def _lath_group(mat, sec, beam, prestress, line_factor):
+    """one lath group's section, stiffness, prestress shares, self-weight per length and material across the grain:
+    sectionStiffness x beamFactors and beamActivations (params.js:43-57), UnitSystem.selfWeightLineLoad (units.js:21-25);
+    line_factor converts density x area to the self-weight per length in scene units (0: gravity off)"""
+    w, h = float(sec["width"]), float(sec["height"])
+    A = w * h
+    Ix = sec["Ix"] if sec["Ix"] is not None else w * h ** 3 / 12.0
+    Iy = sec["Iy"] if sec["Iy"] is not None else h * w ** 3 / 12.0
+    J = sec["J"] if sec["J"] is not None else _rect_torsion(w, h)
+    if beam["mode"] == "advanced":
+        fEA, fIx, fIy, fGJ, fGA = (float(beam[k]) for k in ("stiffness_axial", "stiffness_flat", "stiffness_edge",
+                                                             "stiffness_twist", "stiffness_shear"))
+        act = [beam["activation_flat"], beam["activation_edge"], beam["activation_twist"]]
+    else:
+        k = float(beam["stiffness"])
+        fEA, fIx, fIy, fGJ, fGA = 1.0, k, k, k, 1.0
+        act = [beam["activation"]] * 3
+    if prestress == "asbuilt":                      # rod_cosserat.js:59: no prestress share at all
+        act = [0.0, 0.0, 0.0]
+    act = [min(max(float(a), 0.0), 1.0) for a in act]
+    E, G = float(mat["E"]), float(mat["G"])
+    g = WsLathGroup()
+    g.width, g.height = w, h
+    g.EA, g.EIx, g.EIy, g.GJ, g.GA = E * A * fEA, E * Ix * fIx, E * Iy * fIy, G * J * fGJ, 5.0 / 6.0 * G * A * fGA
+    for k in range(3):
+        g.activation[k] = act[k]
+    g.line_weight = float(mat["density"]) * A * line_factor
+    g.fc90, g.E90, g.H = float(mat["fc90"]), float(mat["E90"]), float(mat["H"])
+    return g
+
+
 def load_scene(path, mesh_path=None) -> Model:
     """A model of the scene file `path` (its mesh path taken relative to the file, or `mesh_path`)."""
     with open(path) as f:
@@ -159,26 +200,26 @@ def load_scene(path, mesh_path=None) -> Model:
     beam = _defaults(BEAM, d.get("beam"))
     contact = _defaults(CONTACT, d.get("contact"))
     solver = _defaults(SOLVER, d.get("solver"))
-    if (d.get("hybrid") or {}).get("enabled"):
-        raise NotImplementedError("hybrid lath groups")
-    # section stiffness × beam factors; activations (params.js:43-57)
-    w, h = float(sec["width"]), float(sec["height"])
-    A = w * h
-    Ix = sec["Ix"] if sec["Ix"] is not None else w * h ** 3 / 12.0
-    Iy = sec["Iy"] if sec["Iy"] is not None else h * w ** 3 / 12.0
-    J = sec["J"] if sec["J"] is not None else _rect_torsion(w, h)
-    if beam["mode"] == "advanced":
-        fEA, fIx, fIy, fGJ, fGA = (float(beam[k]) for k in ("stiffness_axial", "stiffness_flat", "stiffness_edge",
-                                                             "stiffness_twist", "stiffness_shear"))
-        act = [beam["activation_flat"], beam["activation_edge"], beam["activation_twist"]]
-    else:
-        k = float(beam["stiffness"])
-        fEA, fIx, fIy, fGJ, fGA = 1.0, k, k, k, 1.0
-        act = [beam["activation"]] * 3
-    if solver["prestress"] == "asbuilt":
-        act = [0.0, 0.0, 0.0]
-    act = [min(max(float(a), 0.0), 1.0) for a in act]
-    E, G = float(mat["E"]), float(mat["G"])
+    loads = d.get("loads") or {}
+    grav = loads.get("gravity") or {}
+    line_factor = L * L * G_SI / Fu * L if grav.get("enabled", True) else 0.0     # UnitSystem.selfWeightLineLoad
+    # lath groups (Scene.fromJSON, scene.js:170-176; group(g), strandGroup(s), scene.js:51-62): group 1 is the scene's
+    # own material, section and beam; groups 2.. come from hybrid.groups, their materials without the older-scene
+    # conversion; a strand's group from hybrid.assign
+    hyb = d.get("hybrid") or {}
+    groups, assign = [], []
+    if hyb.get("enabled"):
+        if any(v for v in (hyb.get("pieces") or {}).values()):
+            raise NotImplementedError("lath groups by piece of a discretisation (hybrid.pieces)")
+        raw = hyb.get("groups") or []
+        groups = [_lath_group(_defaults(MATERIAL, g.get("material")), _defaults(SECTION, g.get("section")),
+                              _defaults(BEAM, g.get("beam")), solver["prestress"], line_factor) for g in raw]
+        for k, v in (hyb.get("assign") or {}).items():
+            gi = int(v)
+            if 2 <= gi <= 1 + len(groups):
+                assign.append((int(k), gi))
+    base = _lath_group(mat, sec, beam, solver["prestress"], line_factor)
+    w, h = base.width, base.height
     cfg = WsMeshCfg()
     keep = []
 
@@ -196,25 +237,32 @@ def load_scene(path, mesh_path=None) -> Model:
     cfg.n_flips, cfg.flips = len(flips), arr(flips.ravel(), np.int32)
     cfg.overhang = float(weave["overhang"])
     cfg.width, cfg.height = w, h
-    cfg.EA, cfg.EIx, cfg.EIy, cfg.GJ, cfg.GA = E * A * fEA, E * Ix * fIx, E * Iy * fIy, G * J * fGJ, 5.0 / 6.0 * G * A * fGA
+    cfg.EA, cfg.EIx, cfg.EIy, cfg.GJ, cfg.GA = base.EA, base.EIx, base.EIy, base.GJ, base.GA
     for k in range(3):
-        cfg.activation[k] = act[k]
-    loads = d.get("loads") or {}
-    grav = loads.get("gravity") or {}
+        cfg.activation[k] = base.activation[k]
+    cfg.line_weight = base.line_weight
     if grav.get("enabled", True):
-        cfg.line_weight = float(mat["density"]) * A * L * L * G_SI / Fu * L       # UnitSystem.selfWeightLineLoad
         gd = grav.get("direction") or [0.0, 0.0, -1.0]
         for k in range(3):
             cfg.gravity_dir[k] = float(gd[k])
     udl = loads.get("udl") or {}
     if udl.get("enabled"):
-        if udl.get("per", "length") != "length":
-            raise NotImplementedError("udl per area")
-        cfg.udl_on = 1
+        per = udl.get("per", "length")
+        if per not in ("length", "area"):
+            raise ValueError(f"udl per {per}")
+        cfg.udl_on = 1 if per == "length" else 2
         for k in range(3):
             cfg.udl[k] = float(udl["q"][k])
     cfg.mu = float(contact["mu"])
-    cfg.fc90, cfg.E90, cfg.H = float(mat["fc90"]), float(mat["E90"]), float(mat["H"])
+    cfg.fc90, cfg.E90, cfg.H = base.fc90, base.E90, base.H
+    if groups:
+        garr = (WsLathGroup * len(groups))(*groups)
+        keep.append(garr)
+        cfg.n_groups = len(groups)
+        cfg.groups = C.cast(garr, C.c_void_p)
+        cfg.n_assign = len(assign)
+        cfg.assign_strand = arr(np.array([a for a, _ in assign], dtype=np.int32), np.int32)
+        cfg.assign_group = arr(np.array([g for _, g in assign], dtype=np.int32), np.int32)
     kinds, ids, masks = [], [], []
     for a in d.get("anchors") or []:
         sel = a.get("select") or {}
