@@ -32,6 +32,8 @@ static const double TWIST_RATE_MAX = 0.5 * SUPPORT_SMOOTH;
 static const double ROLL_DAMP = 0.5;
 static const double INF = std::numeric_limits<double>::infinity();
 static const double AL_FREE_MIN = 0.25;               // solver_cpu.js:33
+// the rigid-body freedoms of a model that only the ground holds (solver_cpu.js:35-39)
+static const double RB_MASS = 2.0, RB_VMAX = 0.05, RB_LEVER = 0.05;
 static const double PI = 3.141592653589793;           // Math.PI
 // Math.sign: −1, 0 or +1 (0 for ±0)
 static double jsSign(double v) { return v > 0 ? 1.0 : (v < 0 ? -1.0 : 0.0); }
@@ -759,7 +761,7 @@ struct Solver {
   std::vector<int> fixedNodes;
   std::vector<Clamp> rotClamps;
   std::vector<double> reactions, mass, kRotStatic, inertia3, F, T, tm, kTw;
-  double lRef = 1.0, kePrev = 0.0, ke = 0.0, fref = 0.0, resF = 0.0, resT = 0.0;
+  double lRef = 1.0, kePrev = 0.0, ke = 0.0, fref = 0.0, resF = 0.0, resT = 0.0, resRigid = 0.0;
   bool converged = false;
   int rollbacks = 0;
   // prescribed support motion (an extension of the reference's anchors): fixed translations move linearly from
@@ -808,30 +810,71 @@ struct Solver {
   }
 
   // ---------------------------------------------------------------------------------------------- the ground
-  // Floor (solver_cpu.js:509-634) for models that an anchor also holds; its rigid-body freedoms (a model that only the
-  // ground holds) are not restated
+  // Floor (solver_cpu.js:509-634), with the rigid-body freedoms of a model that only the ground holds
   bool hasFloor = false;
-  double floorFnMax = 0, floorEnergy = 0;
+  double floorFnMax = 0, floorEnergy = 0, floorRamp = 1.0;
   std::vector<double> flW, flH, flAx, flAy, flF;
   std::vector<uint8_t> flState;
-  // the Floor constructor / bind (solver_cpu.js:531-556): sections from the model; stick points at the nodes when new
+  // rigid-body freedoms (Floor constructor, solver_cpu.js:546-553): the reference point c (the centroid of the nodes,
+  // followed at every evaluation), the model radius about it at construction, the rigid velocities, and the sums of the
+  // last evaluation
+  double rbC[3] = {0, 0, 0}, rbR = 1e-9, rbV[3] = {0, 0, 0}, rbW[3] = {0, 0, 0}, rbQt[3] = {0, 0, 0}, rbQr[3] = {0, 0, 0};
+  double rbD2[3] = {0, 0, 0}, rbVmax = 0, rbWmax = 0;
+  int rbNc = 0;
+  // the Floor constructor / bind (solver_cpu.js:531-562): sections from the model; stick points, the reference point and
+  // the model radius at the nodes when new
   void floorBind(const ws_model &md) {
     const int n = st.n;
     if (!md.params.floor) { hasFloor = false; return; }
     if (!md.node_w || !md.node_h) throw std::invalid_argument("oracle: a ground needs the node sections");
-    if (fixedNodes.empty() && rotClamps.empty()) throw std::invalid_argument("oracle: a model that only the ground holds");
     flW.assign(md.node_w, md.node_w + n); flH.assign(md.node_h, md.node_h + n);
     if (!hasFloor || flAx.size() != size_t(n)) {
       flAx.resize(n); flAy.resize(n);
       for (int i = 0; i < n; i++) { flAx[i] = st.X[3 * size_t(i)]; flAy[i] = st.X[3 * size_t(i) + 1]; }
       flF.assign(3 * size_t(n), 0.0); flState.assign(n, 0); floorFnMax = floorEnergy = 0;
+      double c[3] = {0, 0, 0};
+      for (int i = 0; i < n; i++) for (int k = 0; k < 3; k++) c[k] += st.X[3 * size_t(i) + k] / std::max(n, 1);
+      double R2 = 0;
+      for (int i = 0; i < n; i++) {
+        const double *x = &st.X[3 * size_t(i)];
+        R2 = std::max(R2, (x[0] - c[0]) * (x[0] - c[0]) + (x[1] - c[1]) * (x[1] - c[1]) + (x[2] - c[2]) * (x[2] - c[2]));
+      }
+      for (int k = 0; k < 3; k++) { rbC[k] = c[k]; rbV[k] = rbW[k] = rbQt[k] = rbQr[k] = rbD2[k] = 0; }
+      rbR = std::max(std::sqrt(R2), 1e-9);
+      rbNc = 0;
     }
+    double hmin = INF;
+    for (int i = 0; i < n; i++) hmin = std::min(hmin, std::min(flH[i], flW[i]));
+    rbVmax = RB_VMAX * (std::isfinite(hmin) && hmin > 0 ? hmin : 1.0);
+    rbWmax = rbVmax / rbR;
     hasFloor = true;
   }
-  // Floor.apply without the rigid-body sums (solver_cpu.js:572-620)
-  void floorApply(double ramp) {
+  // Floor.rigidMasses (solver_cpu.js:564-572): fictitious masses of the rigid translations and rotations
+  void rigidMasses(double ms, double out[6]) const {
+    const double kn = floorRamp * sp.strength, kt = floorRamp * sp.stick_strength, f = ms * RB_MASS;
+    const double nc = std::max(rbNc, 1), rmin = (RB_LEVER * rbR) * (RB_LEVER * rbR) * kn;
+    out[0] = std::max(f * nc * kt, 1e-30); out[1] = out[0]; out[2] = std::max(f * nc * kn, 1e-30);
+    out[3] = std::max(f * std::max(kn * rbD2[1] + kt * rbD2[2], rmin), 1e-30);
+    out[4] = std::max(f * std::max(kn * rbD2[0] + kt * rbD2[2], rmin), 1e-30);
+    out[5] = std::max(f * std::max(kt * (rbD2[0] + rbD2[1]), rmin), 1e-30);
+  }
+  // Floor.rigidResidual (solver_cpu.js:574)
+  double rigidResidual(double fr) const {
+    return std::max(std::hypot(rbQt[0], rbQt[1], rbQt[2]) / fr, std::hypot(rbQr[0], rbQr[1], rbQr[2]) / (fr * rbR));
+  }
+  // Floor.apply with the rigid-body sums of the external forces `loads` + the ground (solver_cpu.js:583-631)
+  void floorApply(double ramp, const std::vector<double> &loads) {
     const int n = st.n;
     const double z0 = sp.floor_z, mu = std::max(sp.floor_mu, 0.0), kn = ramp * sp.strength, kt = ramp * sp.stick_strength;
+    floorRamp = ramp;
+    double q0 = 0, q1 = 0, q2 = 0, q3 = 0, q4 = 0, q5 = 0, dxx = 0, dyy = 0, dzz = 0;
+    int nc = 0;
+    double *c = rbC;
+    if (n) {
+      double cx = 0, cy = 0, cz = 0;
+      for (int i = 0; i < n; i++) { cx += st.X[3 * size_t(i)]; cy += st.X[3 * size_t(i) + 1]; cz += st.X[3 * size_t(i) + 2]; }
+      c[0] = cx / n; c[1] = cy / n; c[2] = cz / n;
+    }
     std::vector<double> qn;
     nodeQuats(st, qn);
     double e = 0, fmax = 0, R[9];
@@ -852,13 +895,20 @@ struct Solver {
         flState[i] = scale > 0 ? 2 : 1;
         e += 0.5 * kn * pen * pen + 0.5 * kt * (ex * ex + ey * ey);
         if (fn > fmax) fmax = fn;
+        const double dx = x[0] - c[0], dy = x[1] - c[1], dz = x[2] - c[2];
+        dxx += dx * dx; dyy += dy * dy; dzz += dz * dz; nc++;
       } else {
         flAx[i] = x[0]; flAy[i] = x[1];
         f[0] = f[1] = f[2] = 0; flState[i] = 0;
       }
       for (int k = 0; k < 3; k++) F[3 * size_t(i) + k] += f[k];
+      const double gx = loads[3 * size_t(i)] + f[0], gy = loads[3 * size_t(i) + 1] + f[1], gz = loads[3 * size_t(i) + 2] + f[2];
+      const double dx = x[0] - c[0], dy = x[1] - c[1], dz = x[2] - c[2];
+      q0 += gx; q1 += gy; q2 += gz; q3 += dy * gz - dz * gy; q4 += dz * gx - dx * gz; q5 += dx * gy - dy * gx;
     }
     floorEnergy = e; floorFnMax = fmax;
+    rbQt[0] = q0; rbQt[1] = q1; rbQt[2] = q2; rbQr[0] = q3; rbQr[1] = q4; rbQr[2] = q5;
+    rbD2[0] = dxx; rbD2[1] = dyy; rbD2[2] = dzz; rbNc = nc;
   }
 
   // ---------------------------------------------------------------------------------------------- load protocol
@@ -993,14 +1043,17 @@ struct Solver {
     return std::max(std::max(std::max(a, b), std::max(c, d)), std::max(e, 1e-12));
   }
 
-  // solver_cpu.js:737-841 (no floor, no rigid-body freedoms)
+  // solver_cpu.js:737-841
   bool step(int nIter) {
     const int n = st.n, m = st.m;
     const int rampN = std::max(sp.ramp_iter, 0);
-    double R[9], dq[4], qq[4], q0[4];
+    double R[9], dq[4], qq[4], q0[4], Mrb[6], qw[4];
     std::vector<double> Xprev(3 * size_t(n)), Qprev(4 * size_t(m)), kin(3 * size_t(n)), kinR(3 * size_t(m)), nq;
     std::fill(kTw.begin(), kTw.end(), 0.0);
     double *W = st.Wr.data();
+    // the rigid-body freedoms of a model that only the ground holds: off as soon as an anchor exists
+    const bool rb = hasFloor && fixedNodes.empty() && rotClamps.empty();
+    if (hasFloor && !rb) for (int k = 0; k < 3; k++) rbV[k] = rbW[k] = 0;
     bool broke = false;
     for (int it = 0; it < nIter; it++) {
       if (hasContact) contact.ramp = rampN == 0 ? 1.0 : std::min(1.0, 0.01 + 0.99 * st.iteration / rampN);
@@ -1021,7 +1074,7 @@ struct Solver {
         for (int k = 0; k < 3; k++) total[3 * size_t(proto.probe) + k] += utmPf[k];
       for (size_t i = 0; i < 3 * size_t(n); i++) F[i] += total[i];
       if (hasContact) contact.apply(st, F.data(), T.data());
-      if (hasFloor) floorApply(rampN == 0 ? 1.0 : std::min(1.0, 0.01 + 0.99 * st.iteration / rampN));
+      if (hasFloor) floorApply(rampN <= 0 ? 1.0 : std::min(1.0, 0.01 + 0.99 * st.iteration / rampN), total);
       std::fill(reactions.begin(), reactions.end(), 0.0);
       for (int i = 0; i < n; i++) if (fixedAny[i]) for (int k = 0; k < 3; k++) reactions[3 * size_t(i) + k] = -F[3 * size_t(i) + k];
       for (size_t i = 0; i < 3 * size_t(n); i++) if (!nodeFree[i]) F[i] = 0;
@@ -1035,7 +1088,10 @@ struct Solver {
           inertia3[3 * size_t(j) + k] = sp.mass_scale * std::max(kRotStatic[3 * size_t(j) + k] + kTw[j] + rod.kDyn[3 * size_t(j) + k], 1e-12);
       Xprev = st.X; Qprev = st.Q;
       const bool warm = st.iteration < sp.warmup_iter && hasContact;
-      if (warm) { std::fill(F.begin(), F.end(), 0.0); std::fill(st.V.begin(), st.V.end(), 0.0); }
+      if (warm) {
+        std::fill(F.begin(), F.end(), 0.0); std::fill(st.V.begin(), st.V.end(), 0.0);
+        if (rb) for (int k = 0; k < 3; k++) rbV[k] = rbW[k] = 0;
+      }
       for (int i = 0; i < n; i++) for (int k = 0; k < 3; k++) st.V[3 * size_t(i) + k] += F[3 * size_t(i) + k] / mass[i];
       for (size_t j = 0; j < 3 * size_t(m); j++) W[j] += tm[j] / inertia3[j];
       for (int j = 0; j < m; j++) {
@@ -1057,19 +1113,44 @@ struct Solver {
             for (int c = 0; c < 3; c++)
               if (!nodeFree[3 * size_t(i) + c]) st.X[3 * size_t(i) + c] = ancStart[3 * size_t(i) + c] + r * ancDelta[3 * size_t(i) + c];
       }
+      // rigid-body freedoms, integrated like the nodes: velocity from this iteration's resultant (v += Q / M, speed
+      // limit), then the step x += v + w x (x - c) from the position before the node step, frames turned by w
+      // (solver_cpu.js:785-800)
+      if (rb) {
+        rigidMasses(sp.mass_scale, Mrb);
+        if (!warm)
+          for (int k = 0; k < 3; k++) {
+            rbV[k] = std::min(std::max((rbV[k] + rbQt[k] / Mrb[k]) * sp.damping, -rbVmax), rbVmax);
+            rbW[k] = std::min(std::max((rbW[k] + rbQr[k] / Mrb[3 + k]) * sp.damping, -rbWmax), rbWmax);
+          }
+      }
+      const bool rbMove = rb && (rbV[0] != 0 || rbV[1] != 0 || rbV[2] != 0 || rbW[0] != 0 || rbW[1] != 0 || rbW[2] != 0);
+      if (rbMove) {
+        const double *v = rbV, *w = rbW, *c = rbC;
+        for (int i = 0; i < n; i++) {
+          const double dx = Xprev[3 * size_t(i)] - c[0], dy = Xprev[3 * size_t(i) + 1] - c[1], dz = Xprev[3 * size_t(i) + 2] - c[2];
+          st.X[3 * size_t(i)] += v[0] + w[1] * dz - w[2] * dy;
+          st.X[3 * size_t(i) + 1] += v[1] + w[2] * dx - w[0] * dz;
+          st.X[3 * size_t(i) + 2] += v[2] + w[0] * dy - w[1] * dx;
+        }
+        qexp(w[0], w[1], w[2], qw);
+      }
       for (int j = 0; j < m; j++) {
         qexp(W[3 * size_t(j)], W[3 * size_t(j) + 1], W[3 * size_t(j) + 2], dq);
         for (int k = 0; k < 4; k++) q0[k] = st.Q[4 * size_t(j) + k];
         qmul(q0, dq, qq);
+        if (rbMove) { for (int k = 0; k < 4; k++) q0[k] = qq[k]; qmul(qw, q0, qq); }   // the rigid step's world rotation
         qnormalize(qq);
         for (int k = 0; k < 4; k++) st.Q[4 * size_t(j) + k] = qq[k];
       }
       for (int i = 0; i < n; i++) for (int k = 0; k < 3; k++) kin[3 * size_t(i) + k] = mass[i] * st.V[3 * size_t(i) + k] * st.V[3 * size_t(i) + k];
       for (size_t j = 0; j < 3 * size_t(m); j++) kinR[j] = inertia3[j] * W[j] * W[j];
       ke = 0.5 * (pairwiseSum(kin) + pairwiseSum(kinR));
+      if (rb) for (int k = 0; k < 3; k++) ke += 0.5 * (Mrb[k] * rbV[k] * rbV[k] + Mrb[3 + k] * rbW[k] * rbW[k]);
       if (sp.kinetic_damping && ke < kePrev) {
         st.X = Xprev; st.Q = Qprev;
         std::fill(st.V.begin(), st.V.end(), 0.0); std::fill(st.Wr.begin(), st.Wr.end(), 0.0);
+        if (rb) for (int k = 0; k < 3; k++) rbV[k] = rbW[k] = 0;
         ke = 0.0; rollbacks++;
       }
       kePrev = ke;
@@ -1089,7 +1170,8 @@ struct Solver {
       }
       fref = forceRef();
       resF = n ? fmax / fref : 0; resT = m ? tmax / (fref * lRef) : 0;
-      const double resid = std::max(resF, resT);
+      resRigid = rb ? rigidResidual(fref) : 0;
+      const double resid = std::max(std::max(resF, resT), resRigid);
       st.residual = st.iteration > sp.warmup_iter ? resid : INF;
       if (proto.mode) {                                  // a load protocol runs on past convergence
         protocolStep();
@@ -1130,6 +1212,7 @@ struct orc_view {
   int32_t utm_inc, utm_phase, utm_done, has_floor;
   double *floor_F, e_floor;                     // the ground
   uint8_t *floor_state;
+  double res_rigid, rb_v[3], rb_w[3];           // the rigid-body freedoms: residual part, velocities
 };
 
 void *orc_create(const ws_model *md) {
@@ -1152,6 +1235,8 @@ void orc_view_get(void *h, orc_view *v) {
   v->n = st.n; v->m = st.m; v->p = st.p; v->K = st.K; v->iteration = st.iteration; v->converged = s->converged;
   v->rollbacks = s->rollbacks; v->has_contact = s->hasContact;
   v->residual = st.residual; v->ke_prev = s->kePrev; v->ke = s->ke; v->fref = s->fref; v->res_force = s->resF; v->res_torque = s->resT; v->l_ref = s->lRef;
+  v->res_rigid = s->resRigid;
+  for (int k = 0; k < 3; k++) { v->rb_v[k] = s->rbV[k]; v->rb_w[k] = s->rbW[k]; }
   v->e_stretch = s->rod.eStretch; v->e_shear = s->rod.eShear; v->e_bend = s->rod.eBend; v->e_twist = s->rod.eTwist;
   v->e_contact = s->hasContact ? s->contact.energy : 0.0;
   v->X = st.X.data(); v->X0 = st.X0.data(); v->V = st.V.data(); v->Q = st.Q.data(); v->W = st.Wr.data();

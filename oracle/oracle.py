@@ -27,7 +27,8 @@ class OrcView(C.Structure):
                [("stuck", C.POINTER(C.c_uint8)), ("ctype", C.POINTER(C.c_int32))] + \
                [(k, _dp) for k in ("theta", "phi", "area", "pressure", "util", "lambda", "dent", "M_rot", "rot_slip")] + \
                [("utm", _dp), ("utm_inc", C.c_int32), ("utm_phase", C.c_int32), ("utm_done", C.c_int32),
-                ("has_floor", C.c_int32), ("floor_F", _dp), ("e_floor", C.c_double), ("floor_state", C.POINTER(C.c_uint8))]
+                ("has_floor", C.c_int32), ("floor_F", _dp), ("e_floor", C.c_double), ("floor_state", C.POINTER(C.c_uint8)),
+                ("res_rigid", C.c_double), ("rb_v", C.c_double * 3), ("rb_w", C.c_double * 3)]
 
 
 _lib = None
@@ -127,6 +128,8 @@ class Oracle:
         out["utm"] = _arr(v.utm, 4 * 64).copy()
         out["utm_inc"], out["utm_phase"], out["utm_done"] = v.utm_inc, v.utm_phase, v.utm_done
         out["e_floor"] = v.e_floor
+        out["res_rigid"] = v.res_rigid
+        out["rb_v"], out["rb_w"] = np.array(list(v.rb_v)), np.array(list(v.rb_w))
         out["floor_F"] = _arr(v.floor_F, 3 * n).copy() if v.has_floor else np.zeros(3 * n)
         out["floor_state"] = np.ctypeslib.as_array(v.floor_state, shape=(n,)).copy() if v.has_floor else np.zeros(n, np.uint8)
         for k, s_ in (("theta", K), ("phi", 2 * K), ("area", K), ("pressure", K), ("util", K), ("lambda", K), ("dent", K),

@@ -168,3 +168,17 @@ def record(name, data):
         return
     with open(path, "a") as f:
         f.write(json.dumps({"test": name, **data}) + "\n")
+
+
+def ground_only(tilt=0.0, drop=5.0, q=10.0, nseg=10, L=1000.0, mu=0.5, **prm):
+    """a 1000 mm lath that only the ground holds (no anchor): its underside starts `drop` mm above the ground at the
+    first node, and `drop + tilt` mm above it at the last; 10 N down at every node (solver_cpu.js:520-533: the
+    rigid-body freedoms carry it down, level it and bring it to rest)"""
+    prm.setdefault("max_iter", 60000)
+    md = straight(L, nseg, params=mm_params(contacts=0, floor=1, floor_z=-15.0 - drop, floor_mu=mu, **prm))
+    md.X[2::3] += tilt * md.X[0::3] / L
+    md.X0 = md.X.copy()
+    md.load_const[2::3] -= q
+    md.node_w = np.full(md.n, 60.0)
+    md.node_h = np.full(md.n, 30.0)
+    return md

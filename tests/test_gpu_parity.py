@@ -719,13 +719,37 @@ def test_gridshell_on_the_ground_matches_oracle(oracle_mod, form):
     assert np.abs(g["floor_F"] - v["floor_F"]).max() < 1e-8 * np.abs(v["floor_F"]).max()
 
 
-def test_ground_alone_is_refused():
-    """a model that only the ground holds needs the rigid-body freedoms, which this build does not have"""
-    md = cases.ground_beam(0.0)
-    md.anchor_node = md.anchor_node[:0]
-    md.anchor_mask = md.anchor_mask[:0]
-    with pytest.raises(Exception):
-        ws.GpuSolver([md.copy()], precision="f64")
+@pytest.mark.parametrize("tilt", [0.0, 8.0])
+@pytest.mark.parametrize("form", ["cta", "plain"])
+def test_ground_alone_rigid_body_matches_oracle(oracle_mod, form, tilt):
+    """a lath that only the ground holds (no anchor) falls, levels and comes to rest through the rigid-body freedoms
+    (Floor, solver_cpu.js:520-533,564-631,785-800): FP64 against the oracle with its iteration and roll-back counts,
+    the rigid part of the residual included in the convergence test"""
+    md = cases.ground_only(tilt=tilt)
+    v = oracle_mod.Oracle(md.copy()).run(60000)
+    assert v["converged"]
+    s = ws.GpuSolver([md.copy()], precision="f64", form=form)
+    ctl = s.step(60000)[0]
+    g = s.download(0, fields=GROUND_FIELDS)
+    s.dispose()
+    assert ctl["status"] == 1 and ctl["iter"] == v["iteration"] and ctl["rollbacks"] == v["rollbacks"]
+    assert cases.max_rel_disp_error(g["X"], v["X"], v["X0"]) < 1e-9
+    assert np.abs(g["floor_F"] - v["floor_F"]).max() < 1e-8 * np.abs(v["floor_F"]).max()
+    assert np.array_equal(g["floor_state"], v["floor_state"])
+
+
+def test_ground_alone_mixed_and_in_a_batch(oracle_mod):
+    """the same lath in the mixed policy, batched beside anchored models (which keep their own path): it converges at
+    rest on the ground, within the mixed band of the oracle's result"""
+    md = cases.ground_only(tilt=8.0)
+    v = oracle_mod.Oracle(md.copy()).run(60000)
+    s = ws.GpuSolver([cases.ground_beam(0.0), md.copy(), cases.cantilever(10, 2)], precision="mixed")
+    ctl = s.step(60000)
+    g = s.download(1, fields=("X",))
+    s.dispose()
+    assert ctl[1]["status"] == 1 and abs(ctl[1]["iter"] - v["iteration"]) <= 0.1 * v["iteration"]
+    assert cases.max_rel_disp_error(g["X"], v["X"], v["X0"]) < 1e-3
+    assert ctl[0]["status"] != 3 and ctl[2]["status"] != 3
 
 
 # ---------------------------------------------------------------------------------------------- results

@@ -380,3 +380,22 @@ def test_lateral_torsional_buckling_southwell(oracle_mod):
     slope = np.polyfit(xs, ys, 1)[0]
     est = 1 / math.sqrt(slope)
     assert abs(est - 21.1) < 0.1, (est, Pcr)
+
+
+# ---------------------------------------------------------------------------------------------- rigid-body freedoms
+# A model that only the ground holds (no anchor) carries six rigid freedoms driven by the resultant of the loads and
+# the ground (Floor, solver_cpu.js:520-533,564-631; the step, :785-800).  A 1000 mm lath (60 x 30 mm) starting 5 mm
+# above the ground under 10 N at each of its 11 nodes falls, comes to rest on its underside and carries its load: the
+# ground pushes back 110 N, the penetration is Fn / k_n = 10 N / 1e4 N/mm = 0.001 mm, so the centreline rests at
+# z = floor + 15 - 0.001.  Started tilted (8 mm from end to end) it levels.
+
+@pytest.mark.parametrize("tilt", [0.0, 8.0])
+def test_ground_alone_comes_to_rest(oracle_mod, tilt):
+    md = cases.ground_only(tilt=tilt)
+    v = oracle_mod.Oracle(md.copy()).run(60000)
+    assert v["converged"] and v["residual"] <= 1e-4 and v["res_rigid"] <= 1e-4
+    z = v["X"][2::3]
+    floor = md.params["floor_z"]
+    assert np.abs(z - (floor + 15.0 - 0.001)).max() < 1e-5
+    assert abs(v["floor_F"][2::3].sum() - 110.0) < 1e-4 * 110.0
+    assert np.all(v["floor_state"] > 0)

@@ -82,7 +82,7 @@ void layout(Dev<P> &d, Carver &cv, const Sizes &z) {
   d.ctype = cv.take<uint8_t>(k); d.theta = cv.take<R>(k); d.area = cv.take<R>(k); d.pres = cv.take<R>(k);
   d.util = cv.take<R>(k); d.phiS = cv.take<R>(2 * k);
   d.flW = cv.take<R>(n); d.flH = cv.take<R>(n); d.flAx = cv.take<W>(n); d.flAy = cv.take<W>(n);
-  d.flF = cv.take<R>(3 * n); d.flState = cv.take<uint8_t>(n);
+  d.flF = cv.take<R>(3 * n); d.flState = cv.take<uint8_t>(n); d.ldTot = cv.take<R>(3 * n);
   d.nodeJoint = cv.take<int>(n); d.nodeClamp = cv.take<int>(n); d.X0 = cv.take<W>(3 * n);
   d.segM = cv.take<R>(3 * m); d.nodeLay = cv.take<R>(4 * n);
   d.utmSched = cv.take<double>(WS_PROTOCOL_MAX_INC * size_t(std::max(z.b, 1)));
@@ -312,6 +312,7 @@ InstDesc describe(const HostGoals &g, const Sizes &off) {
   I.utmAvg = g.proto.avg; I.utmIdx = off.b;
   I.cxLin = g.cxLinear ? 1 : 0;
   I.floorOn = g.prm.floor ? 1 : 0; I.floorZ = g.prm.floor_z; I.floorMu = g.prm.floor_mu;
+  I.rbOn = g.rigid ? 1 : 0; I.rbR = g.rbR; I.rbVmax = g.rbVmax; I.rbWmax = g.rbWmax;
   for (int k = 0; k < 3; k++) I.utmAxis[k] = g.proto.axis[k];
   return I;
 }
@@ -738,7 +739,8 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
     const bool cx = c->inst[0].contacts && c->inst[0].K;
     const bool sh = c->shortSides;
     const int chunk = std::min(nIter, 50);
-    const int key = ((chunk * 4 + c->plainMode) << 3) | (ext ? 4 : 0) | (cx ? 2 : 0) | (sh ? 1 : 0);
+    const bool rb = c->inst[0].rbOn != 0;
+    const int key = ((((chunk * 4 + c->plainMode) << 1) | (rb ? 1 : 0)) << 3) | (ext ? 4 : 0) | (cx ? 2 : 0) | (sh ? 1 : 0);
     if (chunk > 0 && (!c->graph || c->graphKey != key)) {
       if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
       cudaGraph_t gr;
@@ -746,7 +748,7 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
       int nl = 0;
       for (int i = 0; i < chunk; i++)
         CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, ext, c->st, &nl, c->dBar + 2,
-                              plainForkOf(c), c->plainMode == 1));
+                              plainForkOf(c), c->plainMode == 1, rb));
       CK(cudaStreamEndCapture(c->st, &gr));
       CK(cudaGraphInstantiate(&c->graph, gr, 0));
       cudaGraphDestroy(gr);
@@ -759,7 +761,7 @@ void stepImpl(ws_ctx *c, int nIter, const uint8_t *mask) {
     int nl = 0;
     for (; done < nIter; done++)
       CK(launchPlainIter<P>(devOf<P>(c), c->dInst, c->dCtl, c->dPart, c->shape, cx, sh, ext, c->st, &nl, c->dBar + 2,
-                            plainForkOf(c), c->plainMode == 1));
+                            plainForkOf(c), c->plainMode == 1, rb));
     c->lastLaunches += nl;
   }
   CK(cudaEventRecord(c->ev1, c->st));
@@ -908,6 +910,8 @@ template <int P>
 void selectResident(ws_ctx *c) {
   c->residentBytes = 0;
   if (c->form != WS_FORM_CTA || c->ctaGlobal) return;
+  for (const InstDesc &I : c->inst)
+    if (I.rbOn) return;          // the rigid-body freedoms step from the iteration's start, which global state keeps
   size_t need = 0;
   for (size_t b = 0; b < c->inst.size(); b++) {
     if (c->isWide[b]) continue;                 // the wide instances run with global state in the cluster kernel
@@ -955,7 +959,7 @@ void applyShape(ws_ctx *c, const ws_shape &sh) {
   std::vector<int> wide, narrow;
   for (int b : c->order) {
     const InstDesc &I = c->inst[b];
-    const bool w = c->form == WS_FORM_CTA && c->wideCl >= 2 && I.n + I.m >= c->wideMin && !I.utmMode;
+    const bool w = c->form == WS_FORM_CTA && c->wideCl >= 2 && I.n + I.m >= c->wideMin && !I.utmMode && !I.rbOn;
     c->isWide[b] = w;
     (w ? wide : narrow).push_back(b);
   }
@@ -1328,6 +1332,8 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
       c->g[b].build(*models[b]);
       if (o.form == WS_FORM_GRID && c->g[b].proto.mode)
         throw std::invalid_argument("a load protocol runs in the cta and plain forms, not the grid form");
+      if (o.form == WS_FORM_GRID && c->g[b].rigid)
+        throw std::invalid_argument("a model that only the ground holds runs in the cta and plain forms, not the grid form");
       off.b = b;
       c->inst.push_back(describe(c->g[b], off));
       off.n += c->g[b].n; off.m += c->g[b].m; off.p += c->g[b].p; off.c += c->g[b].C; off.k += c->g[b].K; off.s += c->g[b].S;

@@ -44,6 +44,10 @@ struct InstDesc {
   // other segment starts or ends on those nodes; a side's nodes and neighbouring segments then follow by arithmetic
   int cxLin;
   double floorZ, floorMu;
+  // rigid-body freedoms of a model that only the ground holds (Floor, solver_cpu.js:520-533): on / off, the model
+  // radius about its centroid at set-up, the speed limits per iteration of the rigid translation and rotation
+  int rbOn;
+  double rbR, rbVmax, rbWmax;
 };
 
 // per-instance control (device-written every iteration)
@@ -66,6 +70,8 @@ struct InstExt {
   int phase, it, inc, accN;
   double pf[3], curF, p0[3], sum[4];
   double eFloor;
+  // the rigid-body freedoms: translation and rotation velocities, and the rigid part of the last residual
+  double rbV[3], rbW[3], rbRes;
 };
 
 // reduction slots
@@ -141,6 +147,7 @@ struct Dev {
   W *flAx, *flAy;
   R *flF;
   uint8_t *flState;
+  R *ldTot;        // [3][ntot] the external loads of a node on the ground in the last evaluation (rigid-body sums)
   // results post-processing: the joint and the clamp at every node [ntot] (−1 none), the displacement origin [3][ntot],
   // segment moments [3][mtot] and node layers [4][ntot] (outputs)
   int *nodeJoint, *nodeClamp;

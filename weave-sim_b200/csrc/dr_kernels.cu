@@ -199,6 +199,73 @@ __device__ __forceinline__ void blockPhaseBC(const Dev<P> &d, const InstDesc &I,
   });
 }
 
+// ------------------------------------------------------------------------------------------------ rigid-body freedoms
+// K doubles summed over the block in a fixed order (warp shuffles, then the warps' results in order); the result is
+// valid in thread 0.  smem: >= 32 K doubles.
+template <int K>
+__device__ __forceinline__ void blockSumD(double (&v)[K], double *smem) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    for (int k = 0; k < K; k++) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  __syncthreads();
+  if (lane == 0)
+    for (int k = 0; k < K; k++) smem[wid * K + k] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < K; k++) v[k] = 0.0;
+    for (int w = 0; w < nw; w++)
+      for (int k = 0; k < K; k++) v[k] += smem[w * K + k];
+  }
+  __syncthreads();
+}
+// The rigid-body freedoms of instance I over one block, after its update phase and its block reduction `pt` (valid in
+// thread 0): the centroid of the positions at the iteration's start (buffer sx.cur), the sums about it, then in thread 0
+// the velocity update and the kinetic-damping decision with the rigid kinetic energy and residual, then, unless the
+// iteration rolls back, the rigid step of every node and frame of the new buffer (sx.nxt).  sc: the block's control
+// block; ux: the instance's extension state.
+template <int P, bool EXT>
+__device__ void rigidBlockStep(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, InstCtl &sc, InstExt &ux,
+                               Part<typename Dev<P>::A> &pt, int nIter) {
+  using A = typename Dev<P>::A;
+  __shared__ double rsm[32 * RB_NSUM];
+  __shared__ double rc[3], rv[3], rw[3], rq[4];
+  __shared__ int rmove;
+  double cs[3] = {0.0, 0.0, 0.0};
+  for (int e = threadIdx.x; e < I.n; e += blockDim.x)
+    for (int k = 0; k < 3; k++) cs[k] += double(Acc<P>::xw(d, sx.cur, k, I.n0 + e));
+  blockSumD<3>(cs, rsm);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; k++) rc[k] = cs[k] / double(max(I.n, 1));
+  __syncthreads();
+  double s[RB_NSUM] = {0.0};
+  const double c[3] = {rc[0], rc[1], rc[2]};
+  for (int e = threadIdx.x; e < I.n; e += blockDim.x) rigidNode<P>(d, sx.cur, I.n0 + e, c, s);
+  blockSumD<RB_NSUM>(s, rsm);
+  if (threadIdx.x == 0) {
+    double rbq[2];
+    const double ke2 = rigidUpdate(I, sx.iter, sx.warm != 0, s, ux, rbq);
+    pt.s[RS_KE] += A(ke2);
+    decide<EXT>(I, sc, pt, nIter, rbq);
+    if (sc.pending) for (int k = 0; k < 3; k++) ux.rbV[k] = ux.rbW[k] = 0.0;
+    ux.rbRes = fmax(rbq[0] / sc.fref, rbq[1] / (sc.fref * I.rbR));
+    rmove = !sc.pending && rigidMoves(ux);
+    for (int k = 0; k < 3; k++) { rv[k] = ux.rbV[k]; rw[k] = ux.rbW[k]; }
+    const double a = sqrt(rw[0] * rw[0] + rw[1] * rw[1] + rw[2] * rw[2]), half = 0.5 * a;
+    const double sn = a > 1e-12 ? sin(half) / a : 0.5;
+    rq[0] = cos(half); rq[1] = rw[0] * sn; rq[2] = rw[1] * sn; rq[3] = rw[2] * sn;
+  }
+  __syncthreads();
+  if (rmove) {
+    const double v[3] = {rv[0], rv[1], rv[2]}, w[3] = {rw[0], rw[1], rw[2]}, q[4] = {rq[0], rq[1], rq[2], rq[3]};
+    for (int e = threadIdx.x; e < I.n + I.m; e += blockDim.x) {
+      if (e < I.n) rigidMoveNode<P>(d, sx.cur, sx.nxt, I.n0 + e, c, v, w);
+      else rigidMoveSeg<P>(d, sx.nxt, I.m0 + (e - I.n), q);
+    }
+  }
+  __syncthreads();
+}
+
 // ------------------------------------------------------------------------------------------------ batched form
 // Block b relaxes instance order[b] (and further instances grid-strided) for up to nIter iterations, stopping at its
 // own convergence.  Instance state lives in HBM / L2; the block's barriers separate the phases, so an instance never
@@ -239,6 +306,14 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
       }
       __syncthreads();
       blockReduce(pt, red);
+      if constexpr (EXT) {
+        if (I.rbOn) {                   // a model only the ground holds: its rigid-body freedoms decide with it
+          rigidBlockStep<P, EXT>(d, I, sx, sc, d.ext[I.utmIdx], pt, nIter);
+          if (threadIdx.x == 0) d.ext[I.utmIdx].eFloor = double(pt.s[RS_FLOOR]);
+          __syncthreads();
+          continue;
+        }
+      }
       if (threadIdx.x == 0) decide<EXT>(I, sc, pt, nIter);
       __syncthreads();
       if constexpr (EXT) {
@@ -708,6 +783,7 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
     closeIteration<PART != 0, A>(insts, ctl, partAll, pe.x, pe.y, pe.n, pe.m, partStride, counter, red);
     return;
   }
+  if (I.rbOn) return;             // a model only the ground holds: k_rigidClose closes the iteration after this kernel
   Part<A> q;
   q.init();
   reduceIteration<PART != 0, EXT>(q, partAll, pe.x, pe.y, pe.n, pe.m, partStride);
@@ -753,6 +829,33 @@ __global__ void __launch_bounds__(256, WSB_MINB_DN) k_plainDNM(Dev<P> d, const I
   else
     plainD<P, SHORT, EXT, 2>(d, insts, ctl, part + nbN, partAll, pe, partStride, counter, gridDim.x, blockIdx.x - nbN,
                              gridDim.x - nbN);
+}
+
+// The close of a plain-form iteration of a model that only the ground holds (one block, launched after the update
+// kernels): every block partial reduced as the update kernel's last block would, then the rigid-body freedoms (their
+// sums need the ground's forces of every node) with the kinetic-damping decision, and the rigid step of the new buffer.
+template <int P, bool SPLIT>
+__global__ void __launch_bounds__(1024) k_rigidClose(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+                                                     const typename Dev<P>::A *partAll, PartEnds pe, int partStride,
+                                                     unsigned *counter) {
+  using A = typename Dev<P>::A;
+  __shared__ A red[32 * (RS_NSUM + RX_NMAX)];
+  __shared__ InstCtl sc;
+  const InstDesc &I = insts[0];
+  if (threadIdx.x == 0) sc = ctl[0];
+  __syncthreads();
+  if (sc.status != WS_RUNNING) return;
+  const StepCtx sx = makeCtx<A>(I, sc);
+  Part<A> q;
+  q.init();
+  reduceIteration<SPLIT, true>(q, partAll, pe.x, pe.y, pe.n, pe.m, partStride);
+  blockReduce(q, red);
+  rigidBlockStep<P, true>(d, I, sx, sc, d.ext[I.utmIdx], q, 0);
+  if (threadIdx.x == 0) {
+    d.ext[I.utmIdx].eFloor = double(q.s[RS_FLOOR]);
+    ctl[0] = sc;
+    *counter = 0;
+  }
 }
 
 // ------------------------------------------------------------------------------------------------ grid form
@@ -859,6 +962,8 @@ __global__ void __launch_bounds__(256) k_unpack(Dev<P> d, const InstDesc *__rest
     c.pending = 0;
     c.ke_prev = 0.0;
     c.status = WS_RUNNING;
+    if (I.rbOn)                         // the rigid-body freedoms restart at rest, as the nodes do
+      for (int k = 0; k < 3; k++) d.ext[I.utmIdx].rbV[k] = d.ext[I.utmIdx].rbW[k] = 0.0;
     if (I.utmMode) {
       InstExt &u = d.ext[I.utmIdx];
       u.phase = 0; u.it = 0; u.inc = 0; u.accN = 0; u.curF = v0;
@@ -1162,9 +1267,18 @@ static cudaError_t launchPDL(void (*k)(KArgs...), int blocks, cudaStream_t st, A
 template <int P>
 cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, const PlainShape &sh, bool contacts,
                             bool shortSides, bool ext, cudaStream_t st, int *launches, unsigned *counter, const PlainFork *fork,
-                            bool roles) {
+                            bool roles, bool rigid) {
   using A = typename Dev<P>::A;
   const bool sh2 = shortSides && contacts;
+  // a model that only the ground holds: its iteration closes in one more launch (k_rigidClose)
+  auto rigidClose = [&](bool split, const PartEnds &pe, int nParts) -> cudaError_t {
+    if (!rigid) return cudaSuccess;
+    const A *pa = static_cast<const A *>(part);
+    if (split) k_rigidClose<P, true><<<1, 1024, 0, st>>>(d, insts, ctl, pa, pe, nParts, counter);
+    else k_rigidClose<P, false><<<1, 1024, 0, st>>>(d, insts, ctl, pa, pe, nParts, counter);
+    if (launches) *launches += 1;
+    return cudaGetLastError();
+  };
   if (roles && contacts) {
     // two launches with block roles, each scheduled while its predecessor drains (the general order's ranking kernel
     // between them)
@@ -1184,6 +1298,7 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
     if (e != cudaSuccess) return e;
     nl += 1;
     if (launches) *launches += nl;
+    if ((e = rigidClose(true, pe, nParts)) != cudaSuccess) return e;
     return cudaGetLastError();
   }
   if (fork && contacts) {
@@ -1219,6 +1334,7 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
     if ((e = cudaStreamWaitEvent(st, fork->join2, 0)) != cudaSuccess) return e;
     nl += 2;
     if (launches) *launches += nl;
+    if ((e = rigidClose(true, pe, nParts)) != cudaSuccess) return e;
     return cudaGetLastError();
   }
   const int nD = sh2 ? sh.blocksDS : sh.blocksD, nParts = sh.blocksA + nD;
@@ -1236,6 +1352,7 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
   if (e != cudaSuccess) return e;
   nl += 1;
   if (launches) *launches += nl;
+  if ((e = rigidClose(false, pe, nParts)) != cudaSuccess) return e;
   return cudaGetLastError();
 }
 
@@ -1262,7 +1379,7 @@ int gridBlocks(bool shortSides, bool ext) {
   template cudaError_t launchBatched<P>(const Dev<P> &, const InstDesc *, InstCtl *, const int *, int, int, const uint8_t *, \
                                         int, int, bool, bool, cudaStream_t);                                         \
   template cudaError_t launchPlainIter<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, const PlainShape &, bool,    \
-                                          bool, bool, cudaStream_t, int *, unsigned *, const PlainFork *, bool);     \
+                                          bool, bool, cudaStream_t, int *, unsigned *, const PlainFork *, bool, bool); \
   template cudaError_t launchGrid<P>(const Dev<P> &, const InstDesc *, InstCtl *, void *, unsigned *, int *, int, int, bool, \
                                      bool, cudaStream_t);                                                            \
   template int gridBlocks<P>(bool, bool);                                                                           \

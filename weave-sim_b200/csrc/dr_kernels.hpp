@@ -28,12 +28,12 @@ cudaError_t launchWide(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, con
 template <int P>
 int wideClusters(int threads, int cluster, bool shortSides, bool ext);
 // ext: some instance runs an extension (contact extensions, the ground, a load protocol): the kernels' variants that
-// have them.  roles: each split phase as one launch whose blocks take the two parts' roles (no fork); else `fork`
+// have them.  rigid: the instance is a model that only the ground holds (one more launch closes its iteration).  roles: each split phase as one launch whose blocks take the two parts' roles (no fork); else `fork`
 // (when given) runs the parts on forked branches, else each phase is one kernel.
 template <int P>
 cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, const PlainShape &sh, bool contacts,
                             bool shortSides, bool ext, cudaStream_t st, int *launches, unsigned *counter, const PlainFork *fork,
-                            bool roles);
+                            bool roles, bool rigid);
 
 template <int P>
 cudaError_t launchGrid(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl, void *part, unsigned *bar, int *err, int nIter,

@@ -934,7 +934,10 @@ __device__ __forceinline__ void nodeUpdate(const Dev<P> &d, const InstDesc &I, c
   // crossing sides on the adjacent segments, as distributed by the last evaluation (weights 1 − t at a, t at b)
   const bool cx = I.contacts && I.K;
   if constexpr (EXT)
-    if (I.floorOn) floorForce<P>(d, I, sc, i, x, F, pt);
+    if (I.floorOn) {
+      for (int k = 0; k < 3; k++) d.ldTot[k * nt + i] = tot[k];     // the external loads, for the rigid-body sums
+      floorForce<P>(d, I, sc, i, x, F, pt);
+    }
   if (cx && so >= 0)
     sidesOn<SHORT>(d, sc.obuf, so, SHORT ? ro(d.segLocal + so) : 0, [&](int q) {
       const R wgt = R(1) - d.sT[q];
@@ -1092,7 +1095,8 @@ __device__ __forceinline__ void blockReduce(Part<A> &p, A *smem) {
 // kinetic-damping decision, residual and convergence of one instance from its reduced partials (solver_cpu.js:809-837);
 // EXT: the kernel variant that has the extensions (the ground, a load protocol)
 template <bool EXT, class A>
-__device__ __forceinline__ void decide(const InstDesc &I, InstCtl &c, const Part<A> &p, int n_iter_stop) {
+__device__ __forceinline__ void decide(const InstDesc &I, InstCtl &c, const Part<A> &p, int n_iter_stop,
+                                       const double *rbq = nullptr) {
   double ke = 0.5 * double(p.s[RS_KE]);
   const bool rollback = I.kd && ke < c.ke_prev;
   if (!isfinite(ke)) { c.status = WS_NONFINITE; }
@@ -1114,7 +1118,9 @@ __device__ __forceinline__ void decide(const InstDesc &I, InstCtl &c, const Part
   c.fref = fref;
   c.res_f = I.n ? double(p.x[RX_F]) / fref : 0.0;
   c.res_t = I.m ? double(p.x[RX_T]) / (fref * I.lRef) : 0.0;
-  const double resid = fmax(c.res_f, c.res_t);
+  // rbq: the rigid-body freedoms' unbalanced resultants |Q_t|, |Q_r| (Floor.rigidResidual, solver_cpu.js:574)
+  const double resRb = rbq ? fmax(rbq[0] / fref, rbq[1] / (fref * I.rbR)) : 0.0;
+  const double resid = fmax(fmax(c.res_f, c.res_t), resRb);
   c.residual = c.iter > I.warmup ? resid : INFINITY;
   c.e_stretch = double(p.s[RS_STRETCH]); c.e_shear = double(p.s[RS_SHEAR]);
   c.e_bend = double(p.s[RS_BEND]); c.e_twist = double(p.s[RS_TWIST]);
@@ -1182,6 +1188,80 @@ __device__ __forceinline__ void protocolStep(const Dev<P> &d, int buf, const Ins
     }
   }
   if (c.status == WS_RUNNING && c.iter >= I.max_iter) c.status = WS_MAX_ITER;
+}
+
+// ------------------------------------------------------------------------------------------------ rigid-body freedoms
+// A model that only the ground holds carries six more freedoms: a translation v and a rotation w of the whole model
+// about the centroid c of its nodes, driven by the resultant of the external forces (loads + ground) with fictitious
+// masses from the ground springs in contact (Floor, solver_cpu.js:520-533,564-631; the step, solver_cpu.js:785-800).
+// Sums of one iteration: [0..2] Q_t = sum (L + G), [3..5] Q_r = sum (x - c) x (L + G), [6..8] sum over the nodes in
+// contact of (x - c)^2 per axis, [9] how many nodes are in contact.
+enum { RB_NSUM = 10 };
+constexpr double RB_MASS = 2.0, RB_LEVER = 0.05;    // solver_cpu.js:37,39 (RB_VMAX is in the host's speed limits)
+
+// node i's share of the sums, at its position `x` at the start of the iteration (buffer `buf`) about c
+template <int P>
+__device__ __forceinline__ void rigidNode(const Dev<P> &d, int buf, int i, const double c[3], double s[RB_NSUM]) {
+  const int nt = d.ntot;
+  double dx[3], g[3];
+  for (int k = 0; k < 3; k++) {
+    dx[k] = double(Acc<P>::xw(d, buf, k, i)) - c[k];
+    g[k] = double(d.ldTot[k * nt + i]) + double(d.flF[k * nt + i]);
+  }
+  s[0] += g[0]; s[1] += g[1]; s[2] += g[2];
+  s[3] += dx[1] * g[2] - dx[2] * g[1]; s[4] += dx[2] * g[0] - dx[0] * g[2]; s[5] += dx[0] * g[1] - dx[1] * g[0];
+  if (d.flState[i]) { s[6] += dx[0] * dx[0]; s[7] += dx[1] * dx[1]; s[8] += dx[2] * dx[2]; s[9] += 1.0; }
+}
+// one thread: the fictitious masses (Floor.rigidMasses), the velocity update (v += Q / M, damping, speed limit; not in
+// the warm-up, which zeroes them), the kinetic energy the rigid step adds (sum M v^2, to be halved with the rest), and
+// |Q_t|, |Q_r| for the residual
+__device__ __forceinline__ double rigidUpdate(const InstDesc &I, int iter, bool warm, const double s[RB_NSUM], InstExt &u,
+                                             double rbq[2]) {
+  const double rampN = I.ramp_iter;
+  const double ramp = rampN <= 0 ? 1.0 : fmin(1.0, 0.01 + 0.99 * double(iter) / rampN);
+  const double kn = ramp * I.strength, kt = ramp * I.stick, f = I.ms * RB_MASS;
+  const double nc = fmax(s[9], 1.0), rmin = (RB_LEVER * I.rbR) * (RB_LEVER * I.rbR) * kn;
+  double M[6];
+  M[0] = fmax(f * nc * kt, 1e-30); M[1] = M[0]; M[2] = fmax(f * nc * kn, 1e-30);
+  M[3] = fmax(f * fmax(kn * s[7] + kt * s[8], rmin), 1e-30); M[4] = fmax(f * fmax(kn * s[6] + kt * s[8], rmin), 1e-30);
+  M[5] = fmax(f * fmax(kt * (s[6] + s[7]), rmin), 1e-30);
+  if (warm) {
+    for (int k = 0; k < 3; k++) u.rbV[k] = u.rbW[k] = 0.0;
+  } else {
+    for (int k = 0; k < 3; k++) {
+      u.rbV[k] = fmin(fmax((u.rbV[k] + s[k] / M[k]) * I.damping, -I.rbVmax), I.rbVmax);
+      u.rbW[k] = fmin(fmax((u.rbW[k] + s[3 + k] / M[3 + k]) * I.damping, -I.rbWmax), I.rbWmax);
+    }
+  }
+  rbq[0] = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+  rbq[1] = sqrt(s[3] * s[3] + s[4] * s[4] + s[5] * s[5]);
+  double ke = 0.0;
+  for (int k = 0; k < 3; k++) ke += M[k] * u.rbV[k] * u.rbV[k] + M[3 + k] * u.rbW[k] * u.rbW[k];
+  return ke;
+}
+__device__ __forceinline__ bool rigidMoves(const InstExt &u) {
+  return u.rbV[0] != 0.0 || u.rbV[1] != 0.0 || u.rbV[2] != 0.0 || u.rbW[0] != 0.0 || u.rbW[1] != 0.0 || u.rbW[2] != 0.0;
+}
+// the rigid step of node i: x (buffer nxt) += v + w x (x_prev - c), x_prev in buffer cur
+template <int P>
+__device__ __forceinline__ void rigidMoveNode(const Dev<P> &d, int cur, int nxt, int i, const double c[3], const double v[3],
+                                              const double w[3]) {
+  using W = typename Dev<P>::W;
+  double dx[3];
+  for (int k = 0; k < 3; k++) dx[k] = double(Acc<P>::xw(d, cur, k, i)) - c[k];
+  const double m[3] = {v[0] + w[1] * dx[2] - w[2] * dx[1], v[1] + w[2] * dx[0] - w[0] * dx[2], v[2] + w[0] * dx[1] - w[1] * dx[0]};
+  for (int k = 0; k < 3; k++) Acc<P>::xs(d, nxt, k, i, W(double(Acc<P>::xw(d, nxt, k, i)) + m[k]));
+}
+// the rigid step of segment j's frame (buffer nxt): q <- normalize(exp(w) ⊗ q)
+template <int P>
+__device__ __forceinline__ void rigidMoveSeg(const Dev<P> &d, int nxt, int j, const double qw[4]) {
+  using W = typename Dev<P>::W;
+  W q[4], qr[4];
+  for (int k = 0; k < 4; k++) q[k] = Acc<P>::qw(d, nxt, k, j);
+  const W a[4] = {W(qw[0]), W(qw[1]), W(qw[2]), W(qw[3])};
+  qmul(a, q, qr);
+  qnormalize<W, P == PREC_MIXED>(qr);
+  for (int k = 0; k < 4; k++) Acc<P>::qs(d, nxt, k, j, qr[k]);
 }
 
 template <class A>

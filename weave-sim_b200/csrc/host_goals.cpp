@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <stdexcept>
 
 namespace wsb {
@@ -150,9 +151,22 @@ void HostGoals::buildAnchors(const ws_model &md) {
     if (!md.node_w || !md.node_h) throw std::invalid_argument("model: a ground needs node_w and node_h");
     bool held = C > 0;
     for (uint8_t f : nodeFree) held = held || !f;
-    if (!held)
-      throw std::invalid_argument("model: a model that only the ground holds needs the rigid-body freedoms, which are not built");
     nodeW.assign(md.node_w, md.node_w + n); nodeH.assign(md.node_h, md.node_h + n);
+    // a model that only the ground holds gets the rigid-body freedoms (Floor, solver_cpu.js:520-533,546-562): the
+    // model radius about the centroid of the nodes, the speed limits from the thinnest section
+    rigid = !held;
+    if (rigid && proto.mode) throw std::invalid_argument("model: a load protocol on a model that only the ground holds");
+    double c[3] = {0, 0, 0}, R2 = 0, hmin = std::numeric_limits<double>::infinity();
+    for (int i = 0; i < n; i++) for (int k = 0; k < 3; k++) c[k] += X[3 * size_t(i) + k] / std::max(n, 1);
+    for (int i = 0; i < n; i++) {
+      double r2 = 0;
+      for (int k = 0; k < 3; k++) r2 += (X[3 * size_t(i) + k] - c[k]) * (X[3 * size_t(i) + k] - c[k]);
+      R2 = std::max(R2, r2);
+      hmin = std::min(hmin, std::min(nodeH[i], nodeW[i]));
+    }
+    rbR = std::max(std::sqrt(R2), 1e-9);
+    rbVmax = 0.05 * (std::isfinite(hmin) && hmin > 0 ? hmin : 1.0);      // RB_VMAX, solver_cpu.js:38
+    rbWmax = rbVmax / rbR;
   }
   fixedAny.assign(n, 0);
   for (int i = 0; i < n; i++) fixedAny[i] = (nodeFree[3 * size_t(i)] && nodeFree[3 * size_t(i) + 1] && nodeFree[3 * size_t(i) + 2]) ? 0 : 1;

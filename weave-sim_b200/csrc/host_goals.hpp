@@ -39,6 +39,8 @@ struct HostGoals {
   std::vector<double> fc90, E90, Hs;                 // [2K] timber across the grain, each side (W1 classification)
   ws_protocol proto{};                               // load protocol (mode 0: none), kept over warm starts
   std::vector<double> nodeW, nodeH;                  // [n] section at every node, for the ground (params.floor)
+  bool rigid = false;                                // only the ground holds the model: the rigid-body freedoms
+  double rbR = 1e-9, rbVmax = 0, rbWmax = 0;         // model radius about the centroid; rigid speed limits
   double probe0[3] = {0, 0, 0};                      // the probe's position when the protocol started (P0)
   int dentAfterDefault = 1500;                       // first seat iteration when dent_after_iter < 0: warm-up + ramp of
                                                      // the model the instance was built from (solver_cpu.js:686)
