@@ -83,6 +83,30 @@ __device__ __forceinline__ void addRangeRow(Part<A> &q, const A *part, int b, in
   for (int i = 0; i < RX_NMAX; i++)
     if (XM & (1u << i)) q.x[i] = mmax(q.x[i], __ldcg(part + size_t(RS_NSUM + i) * stride + bc));
 }
+// the same in two steps, so that the loads of several rows go out before the first of their adds
+template <unsigned SM, unsigned XM, class A>
+struct RangeRow {
+  A v[RS_NSUM + RX_NMAX];
+  bool in;
+  __device__ __forceinline__ void load(const A *part, int b, int hi, int stride) {
+    in = b < hi;
+    const int bc = in ? b : hi - 1;
+#pragma unroll
+    for (int i = 0; i < RS_NSUM; i++)
+      if (SM & (1u << i)) v[i] = __ldcg(part + size_t(i) * stride + bc);
+#pragma unroll
+    for (int i = 0; i < RX_NMAX; i++)
+      if (XM & (1u << i)) v[RS_NSUM + i] = __ldcg(part + size_t(RS_NSUM + i) * stride + bc);
+  }
+  __device__ __forceinline__ void add(Part<A> &q) const {
+#pragma unroll
+    for (int i = 0; i < RS_NSUM; i++)
+      if (SM & (1u << i)) q.s[i] += in ? v[i] : A(0);
+#pragma unroll
+    for (int i = 0; i < RX_NMAX; i++)
+      if (XM & (1u << i)) q.x[i] = mmax(q.x[i], v[RS_NSUM + i]);
+  }
+};
 template <class A>
 __device__ __forceinline__ void addPart(Part<A> &q, const A *part, int b, int stride) {
   for (int i = 0; i < RS_NSUM; i++) q.s[i] += __ldcg(part + size_t(i) * stride + b);
@@ -645,8 +669,23 @@ constexpr unsigned updateMaxs(int part, bool ext) {
 template <bool SPLIT, bool EXT, class A>
 __device__ __forceinline__ void reduceIteration(Part<A> &q, const A *part, int ex, int ey, int en, int em, int stride) {
   if constexpr (SPLIT) {
-    const int len = max(max(ex, ey - ex), max(en - ey, em - en));
-    for (int o = threadIdx.x; o < len; o += blockDim.x) {
+    const int len = max(max(ex, ey - ex), max(en - ey, em - en)), bd = blockDim.x;
+    int o0 = threadIdx.x;
+    // two rounds at a time: the rows of both go out in one batch of loads, then they are added in round order
+    for (; o0 + bd < len; o0 += 2 * bd) {
+      RangeRow<elemSums(1), elemMaxs(1), A> x0, x1;
+      RangeRow<elemSums(2), elemMaxs(2), A> y0, y1;
+      RangeRow<updateSums(1, EXT), updateMaxs(1, EXT), A> n0, n1;
+      RangeRow<updateSums(2, EXT), updateMaxs(2, EXT), A> m0, m1;
+      x0.load(part, o0, ex, stride); y0.load(part, ex + o0, ey, stride);
+      n0.load(part, ey + o0, en, stride); m0.load(part, en + o0, em, stride);
+      const int o1 = o0 + bd;
+      x1.load(part, o1, ex, stride); y1.load(part, ex + o1, ey, stride);
+      n1.load(part, ey + o1, en, stride); m1.load(part, en + o1, em, stride);
+      x0.add(q); y0.add(q); n0.add(q); m0.add(q);
+      x1.add(q); y1.add(q); n1.add(q); m1.add(q);
+    }
+    for (int o = o0; o < len; o += bd) {
       addRangeRow<elemSums(1), elemMaxs(1)>(q, part, o, ex, stride);
       addRangeRow<elemSums(2), elemMaxs(2)>(q, part, ex + o, ey, stride);
       addRangeRow<updateSums(1, EXT), updateMaxs(1, EXT)>(q, part, ey + o, en, stride);
@@ -732,13 +771,25 @@ __global__ void __launch_bounds__(256) k_plainBC(Dev<P> d, const InstDesc *__res
 template <bool SPLIT, class A>
 __device__ __noinline__ void closeIteration(const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl, const A *partAll,
                                             int ex, int ey, int en, int em, int partStride, unsigned *counter, A *red) {
+  // the control block and the descriptor go to shared memory a word a thread, their loads in flight beside the
+  // partials' (the decision then reads them there instead of waiting on one global load after another)
+  __shared__ InstCtl sc;
+  __shared__ InstDesc si;
+  constexpr int NC = sizeof(InstCtl) / 4, ND = sizeof(InstDesc) / 4;
+  static_assert(NC <= 64 && 64 + ND <= 256, "the copy takes one word a thread of a 256-thread block");
+  const int t = threadIdx.x;
+  int wc = 0, wd = 0;
+  if (t < NC) wc = __ldcg(reinterpret_cast<const int *>(ctl) + t);
+  if (t >= 64 && t < 64 + ND) wd = __ldg(reinterpret_cast<const int *>(insts) + (t - 64));
   Part<A> q;
   q.init();
   reduceIteration<SPLIT, false>(q, partAll, ex, ey, en, em, partStride);
-  blockReduce(q, red);
-  if (threadIdx.x == 0) {
-    InstCtl cc = ctl[0];
-    decide<false>(insts[0], cc, q, 0);
+  if (t < NC) reinterpret_cast<int *>(&sc)[t] = wc;
+  if (t >= 64 && t < 64 + ND) reinterpret_cast<int *>(&si)[t - 64] = wd;
+  blockReduce<SUMS_ALL & ~SUMS_FLOOR, MAXS_ALL>(q, red);      // (its barriers also publish the copies)
+  if (t == 0) {
+    InstCtl cc = sc;
+    decide<false>(si, cc, q, 0);
     ctl[0] = cc;
     *counter = 0;
   }

@@ -195,17 +195,23 @@ __device__ __forceinline__ void nodeTangent(const Dev<P> &d, int buf, int i, typ
                   si >= 0 ? ro(d.segI0 + si) : -1, si >= 0 ? ro(d.segI1 + si) : -1, T);
 }
 // hemisphere-consistent mean of the adjacent segment frames (nodeQuats, model.js:89-105)
-template <int P>
-__device__ __forceinline__ void segsQuat(const Dev<P> &d, int buf, int so, int si, typename Dev<P>::R q[4]) {
-  using R = typename Dev<P>::R;
+// WIDE: from the frames in the wide type (the two-float frames of the mixed policy in double), in that type
+template <int P, bool WIDE = false>
+__device__ __forceinline__ void segsQuat(const Dev<P> &d, int buf, int so, int si,
+                                         std::conditional_t<WIDE, typename Dev<P>::W, typename Dev<P>::R> q[4]) {
+  using R = std::conditional_t<WIDE, typename Dev<P>::W, typename Dev<P>::R>;
+  auto rd = [&](int k, int j) -> R {
+    if constexpr (WIDE) return Acc<P>::qw(d, buf, k, j);
+    else return Acc<P>::qr(d, buf, k, j);
+  };
   const int ref = so >= 0 ? so : si;
   q[0] = q[1] = q[2] = q[3] = R(0);
   if (ref < 0) return;
   R qr[4];
-  for (int k = 0; k < 4; k++) qr[k] = Acc<P>::qr(d, buf, k, ref);
+  for (int k = 0; k < 4; k++) qr[k] = rd(k, ref);
   auto add = [&](int j) {
     R qj[4];
-    for (int k = 0; k < 4; k++) qj[k] = Acc<P>::qr(d, buf, k, j);
+    for (int k = 0; k < 4; k++) qj[k] = rd(k, j);
     const R dd = qj[0] * qr[0] + qj[1] * qr[1] + qj[2] * qr[2] + qj[3] * qr[3];
     const R sg = dd < R(0) ? R(-1) : R(1);
     for (int k = 0; k < 4; k++) q[k] += sg * qj[k];
@@ -879,10 +885,13 @@ __device__ __forceinline__ void floorForce(const Dev<P> &d, const InstDesc &I, c
   const double rampN = I.ramp_iter;
   const double ramp = rampN <= 0 ? 1.0 : fmin(1.0, 0.01 + 0.99 * double(sc.iter) / rampN);
   const R kn = R(ramp * I.strength), kt = R(ramp * I.stick);
-  R q[4], Rn[9];
-  nodeQuat<P>(d, sc.cur, i, q);
+  // the gap from the plane and the section's depth below the node cancel (a penetration of ~1e-3 of the depth): both
+  // are formed in the wide type, the depth from the node frame of the wide-type segment frames (a frame in float
+  // leaves ~1e-7 of the depth, which the mixed policy's ground forces would carry as noise of ~1e-4 of their size)
+  W q[4], Rn[9];
+  segsQuat<P, true>(d, sc.cur, ro(d.nsOut + i), ro(d.nsIn + i), q);
   qframe(q, Rn);
-  const R pen = R(W(I.floorZ) - x[2]) + (R(0.5) * ro(d.flW + i) * mabs(Rn[2]) + R(0.5) * ro(d.flH + i) * mabs(Rn[5]));
+  const R pen = R((W(I.floorZ) - x[2]) + (W(0.5) * W(ro(d.flW + i)) * mabs(Rn[2]) + W(0.5) * W(ro(d.flH + i)) * mabs(Rn[5])));
   const W ax = d.flAx[i], ay = d.flAy[i];
   R ff[3] = {R(0), R(0), R(0)};
   if (pen > R(0)) {
@@ -1050,13 +1059,23 @@ constexpr unsigned SUMS_ROD = (1u << RS_STRETCH) | (1u << RS_SHEAR) | (1u << RS_
 
 template <unsigned SM = SUMS_ALL, unsigned XM = MAXS_ALL, class A>
 __device__ __forceinline__ void warpReduce(Part<A> &p) {
+  // every slot's shuffle of a level goes out before the first add of that level, so the slots' latencies overlap
+  // (one shuffle after another, each waited for by its add, cost a full shuffle latency per slot and level)
+#pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
+    A ts[RS_NSUM], tx[RX_NMAX];
 #pragma unroll
     for (int i = 0; i < RS_NSUM; i++)
-      if (SM & (1u << i)) p.s[i] += __shfl_xor_sync(0xffffffffu, p.s[i], o);
+      if (SM & (1u << i)) ts[i] = __shfl_xor_sync(0xffffffffu, p.s[i], o);
 #pragma unroll
     for (int i = 0; i < RX_NMAX; i++)
-      if (XM & (1u << i)) p.x[i] = mmax(p.x[i], __shfl_xor_sync(0xffffffffu, p.x[i], o));
+      if (XM & (1u << i)) tx[i] = __shfl_xor_sync(0xffffffffu, p.x[i], o);
+#pragma unroll
+    for (int i = 0; i < RS_NSUM; i++)
+      if (SM & (1u << i)) p.s[i] += ts[i];
+#pragma unroll
+    for (int i = 0; i < RX_NMAX; i++)
+      if (XM & (1u << i)) p.x[i] = mmax(p.x[i], tx[i]);
   }
 }
 // block-wide reduction in a fixed order; the result is valid in thread 0 (smem: >= 32 * (RS_NSUM + RX_NMAX) values)
