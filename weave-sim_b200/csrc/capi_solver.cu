@@ -74,6 +74,7 @@ void layout(Dev<P> &d, Carver &cv, const Sizes &z) {
   d.u = cv.take<U>(2 * k); d.nPrev = cv.take<R>(3 * k); d.slip = cv.take<A>(k); d.stuck = cv.take<uint8_t>(k);
   d.cstate = cv.take<uint8_t>(k); d.Fn = cv.take<R>(k); d.Ft = cv.take<R>(k); d.gap = cv.take<R>(k);
   d.sPos = cv.take<int>(2 * k); d.sKey = cv.take<int>(4 * k); d.sInv = cv.take<int>(4 * k); d.sKeyS = cv.take<int>(2 * k);
+  d.sSideAt = cv.take<int>(2 * k);
   d.sStrand = cv.take<int>(2 * k); d.sT = cv.take<R>(2 * k);
   d.kth = cv.take<R>(2 * k); d.sF = cv.take<R>(6 * k); d.sTq = cv.take<R>(6 * k);
   d.stSideOff = cv.take<int>(s); d.stSideCnt = cv.take<int>(s); d.stSegOff = cv.take<int>(s);

@@ -159,6 +159,7 @@ struct Dev {
   int *sKey;                // [2][2 ktot] local segment of the side after the slide, by sorted-side buffer
   int *sInv;                // [2][2 ktot] short order: the side's position in the sorted order of that buffer
   int *sKeyS;               // [2 ktot] short order: the key after the slide, at the side's sorted position
+  int *sSideAt;             // [2 ktot] short order: the side's strand position, at its sorted position
   int *sStrand;             // [2 ktot] strand of the side
   R *sT, *kth;              // [2 ktot] Hermite parameter before the slide; righting stiffness of the side's crossing
   R *sF, *sTq;              // [3][2 ktot] force on the side; lever torque
@@ -174,7 +175,7 @@ struct Dev {
 // launch with the same function.  The side order keeps two buffers (this iteration's and the next's); the short-slide
 // variant keeps sorted positions and the keys at them, the general one the sorted list of side positions.
 struct ResLayout {
-  unsigned X, Xlo, V, Q, Qlo, Wr, nF, en, tau, kd, tauC, u, nPrev, sKey, sInv, sKeyS, sT, kth, sF, sTq, ord, ordSeg, rngLo,
+  unsigned X, Xlo, V, Q, Qlo, Wr, nF, en, tau, kd, tauC, u, nPrev, sKey, sInv, sKeyS, sSideAt, sT, kth, sF, sTq, ord, ordSeg, rngLo,
       rngHi, bytes;
 };
 __host__ __device__ inline unsigned resTake(unsigned &o, size_t bytes) {
@@ -196,6 +197,7 @@ __host__ __device__ inline ResLayout residentLayout(int n, int m, int p, int C, 
   L.u = resTake(o, K2 * sizeof(U)); L.nPrev = resTake(o, 3 * size_t(K) * sizeof(R));
   L.sKey = resTake(o, 2 * K2 * sizeof(int));
   L.sInv = resTake(o, (shortSides ? 2 : 0) * K2 * sizeof(int)); L.sKeyS = resTake(o, (shortSides ? 1 : 0) * K2 * sizeof(int));
+  L.sSideAt = resTake(o, (shortSides ? 1 : 0) * K2 * sizeof(int));
   L.sT = resTake(o, K2 * sizeof(R)); L.kth = resTake(o, K2 * sizeof(R));
   L.sF = resTake(o, 3 * K2 * sizeof(R)); L.sTq = resTake(o, 3 * K2 * sizeof(R));
   L.ord = resTake(o, (shortSides ? 0 : 2) * K2 * sizeof(int)); L.ordSeg = resTake(o, 2 * K2 * sizeof(int));

@@ -151,7 +151,7 @@ template <int P, bool SHORT, bool EXT>
 __device__ __forceinline__ void phaseD(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, int e, Part<typename Dev<P>::A> &pt) {
   if (e < I.n) nodeUpdate<P, SHORT, EXT>(d, I, sx, I.n0 + e, pt);
   else if ((e -= I.n) < I.m) segUpdate<P, SHORT>(d, I, sx, I.m0 + e, pt);
-  else rankSideShort<P>(d, 2 * I.k0 + (e - I.m), sx.onxt);
+  else rankSideWindow<P>(d, 2 * I.k0 + (e - I.m), sx.obuf, sx.onxt);
 }
 
 // ------------------------------------------------------------------------------------------------ balanced warps
@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(512) k_batched(Dev<P> d, const InstDesc *__res
         forBalanced(runs, [&](int r, int e) {
           if (r == 0) nodeUpdate<P, SHORT, EXT>(d, I, sx, I.n0 + e, pt);
           else if (r == 1) segUpdate<P, SHORT>(d, I, sx, I.m0 + e, pt);
-          else rankSideShort<P>(d, 2 * I.k0 + e, sx.onxt);
+          else rankSideWindow<P>(d, 2 * I.k0 + e, sx.obuf, sx.onxt);
         });
       }
       __syncthreads();
@@ -426,7 +426,7 @@ __global__ void __launch_bounds__(512) k_wide(Dev<P> d, const InstDesc *__restri
         forBalancedOver(runs, nw, w, [&](int r, int e) {
           if (r == 0) nodeUpdate<P, SHORT, EXT>(d, I, sx, I.n0 + e, pt);
           else if (r == 1) segUpdate<P, SHORT>(d, I, sx, I.m0 + e, pt);
-          else rankSideShort<P>(d, 2 * I.k0 + e, sx.onxt);
+          else rankSideWindow<P>(d, 2 * I.k0 + e, sx.obuf, sx.onxt);
         });
       }
       blockReduce(pt, red);
@@ -487,6 +487,7 @@ __device__ __forceinline__ Dev<P> residentView(const Dev<P> &d, const InstDesc &
   v.sKey = reinterpret_cast<int *>(sm + L.sKey) - k2;
   v.sInv = reinterpret_cast<int *>(sm + L.sInv) - k2;
   v.sKeyS = reinterpret_cast<int *>(sm + L.sKeyS) - k2;
+  v.sSideAt = reinterpret_cast<int *>(sm + L.sSideAt) - k2;
   v.sT = reinterpret_cast<R *>(sm + L.sT) - k2;
   v.kth = reinterpret_cast<R *>(sm + L.kth) - k2;
   v.sF = reinterpret_cast<R *>(sm + L.sF) - k2;
@@ -616,7 +617,7 @@ __global__ void __launch_bounds__(512, 1) k_resident(Dev<P> d, const InstDesc *_
           if (I.kd) backupSeg<P>(d, v, bk, I.m0 + e, false);
           segUpdate<P, SHORT>(v, I, sx, I.m0 + e, pt);
         } else {
-          rankSideShort<P>(v, 2 * I.k0 + e, sx.onxt);
+          rankSideWindow<P>(v, 2 * I.k0 + e, sx.obuf, sx.onxt);
         }
       };
       const int nR = (SHORT && cx) ? 2 * I.K : 0;
@@ -818,7 +819,7 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
     if (PART == 0) phaseD<P, SHORT, EXT>(d, I, sx, e, pt);
     else if (PART == 2) segUpdate<P, SHORT>(d, I, sx, I.m0 + e, pt);
     else if (e < I.n) nodeUpdate<P, SHORT, EXT>(d, I, sx, I.n0 + e, pt);
-    else rankSideShort<P>(d, 2 * I.k0 + (e - I.n), sx.onxt);
+    else rankSideWindow<P>(d, 2 * I.k0 + (e - I.n), sx.obuf, sx.onxt);
   }
   constexpr unsigned SM = updateSums(PART, EXT), XM = updateMaxs(PART, EXT);
   blockReduce<SM, XM>(pt, red);

@@ -753,7 +753,7 @@ __device__ __forceinline__ void crossing(const Dev<P> &d, const InstDesc &I, int
   // the side's segment after the slide (solver_cpu.js:144-149): the key of the next sort, into key buffer kb
   const int key = int(mmin(mmax(mfloor(un), U(0)), U(mmax(nseg - 1, 0))));
   d.sKey[size_t(kb) * d.kB + pos] = key;
-  if constexpr (SHORT) d.sKeyS[rec] = key;
+  if constexpr (SHORT) { d.sKeyS[rec] = key; d.sSideAt[rec] = pos; }
   {
     const R sgn = side ? R(-1) : R(1);
     const R F[3] = {sgn * FA[0], sgn * FA[1], sgn * FA[2]};
@@ -849,6 +849,39 @@ __device__ __forceinline__ void rankSideShort(const Dev<P> &d, int p, int kb) {
   }
 }
 
+// The same order, built each iteration from the previous one (buffer ob) instead of by counting every side of the
+// strand: a side moves at most one segment an iteration, so every side whose previous key is at most k − 2 (k: side
+// p's key after this iteration's slide) sorts before p, and every side whose previous key is at least k + 2 after it.
+// The others sit next to p's previous sorted position and are the only ones compared, by their new keys and strand
+// positions, which this iteration's crossings wrote at their previous sorted positions (sKeyS, sSideAt).  The result
+// is the full count's (sideRank's) position, slice and key, from a few neighbours instead of the whole strand.
+template <int P>
+__device__ __forceinline__ void rankSideWindow(const Dev<P> &d, int p, int ob, int kb) {
+  const int s = d.sStrand[p], off = d.stSideOff[s], end = off + d.stSideCnt[s];
+  const int k = d.sKey[size_t(kb) * d.kB + p];
+  const int sp = d.sInv[size_t(ob) * d.kB + p];
+  const int *prevKey = d.ordSeg + size_t(ob) * d.oB;
+  int below = 0, equal = 1, before = 0;           // p itself counts among the equal keys
+  auto visit = [&](int q) {
+    const int kq = d.sKeyS[q], pq = d.sSideAt[q];
+    below += kq < k ? 1 : 0;
+    equal += kq == k ? 1 : 0;
+    before += (kq == k && pq < p) ? 1 : 0;
+  };
+  int lo = sp;
+  while (lo > off && prevKey[lo - 1] >= k - 1) visit(--lo);
+  for (int q = sp + 1; q < end && prevKey[q] <= k + 1; q++) visit(q);
+  below += lo - off;
+  const int pos = off + below + before;
+  d.sInv[size_t(kb) * d.kB + p] = pos;
+  d.ordSeg[size_t(kb) * d.oB + pos] = k;
+  if (before == 0) {
+    const int j = d.stSegOff[s] + k;
+    d.rngLo[size_t(kb) * d.rB + j] = off + below;
+    d.rngHi[size_t(kb) * d.rB + j] = off + below + equal;
+  }
+}
+
 // ------------------------------------------------------------------------------------------------ phase D
 struct StepCtx {
   int cur, nxt, obuf, onxt, pending, iter, warm;
@@ -856,6 +889,9 @@ struct StepCtx {
   const double *utmPf;  // load protocol: the force on the probe (mode 1)
   double dispR;      // prescribed-motion fraction of this iteration
 };
+
+// a key no side carries (an empty slice's placeholder)
+constexpr int NO_KEY = -0x40000000;
 
 // the side records in the slice of segment j (strand-local index lj) of sorted-side buffer ob, in sorted order: with
 // SHORT the records sit at the sorted positions, and an entry counts only if it carries the segment's key (a slice left
@@ -947,16 +983,59 @@ __device__ __forceinline__ void nodeUpdate(const Dev<P> &d, const InstDesc &I, c
       for (int k = 0; k < 3; k++) d.ldTot[k * nt + i] = tot[k];     // the external loads, for the rigid-body sums
       floorForce<P>(d, I, sc, i, x, F, pt);
     }
-  if (cx && so >= 0)
-    sidesOn<SHORT>(d, sc.obuf, so, SHORT ? ro(d.segLocal + so) : 0, [&](int q) {
-      const R wgt = R(1) - d.sT[q];
-      for (int k = 0; k < 3; k++) F[k] += wgt * d.sF[k * K2 + q];
-    });
-  if (cx && si >= 0)
-    sidesOn<SHORT>(d, sc.obuf, si, SHORT ? ro(d.segLocal + si) : 0, [&](int q) {
-      const R wgt = d.sT[q];
-      for (int k = 0; k < 3; k++) F[k] += wgt * d.sF[k * K2 + q];
-    });
+  if constexpr (SHORT) {
+    if (cx) {
+      // the slices of both segments (bounds and keys together), then the first entry of each, then any further
+      // entries in order: two levels of dependent loads after the segment indices
+      const int ob = sc.obuf;
+      const int *oseg = d.ordSeg + size_t(ob) * d.oB;
+      const int sg[2] = {so, si};
+      int lo[2], hi[2], lk[2];
+#pragma unroll
+      for (int t = 0; t < 2; t++) {
+        const int jc = sg[t] >= 0 ? sg[t] : I.m0;      // (a segment of this instance: its slice is read, not used)
+        lk[t] = ro(d.segLocal + jc);
+        lo[t] = d.rngLo[size_t(ob) * d.rB + jc];
+        const int h = d.rngHi[size_t(ob) * d.rB + jc];
+        hi[t] = sg[t] >= 0 ? h : lo[t];
+      }
+      int key0[2];
+      R t0[2], f0[2][3];
+#pragma unroll
+      for (int t = 0; t < 2; t++) {
+        const bool ok = lo[t] < hi[t];
+        const int e = lo[t];
+        key0[t] = ok ? oseg[e] : NO_KEY;
+        t0[t] = ok ? d.sT[e] : R(0);
+#pragma unroll
+        for (int k = 0; k < 3; k++) f0[t][k] = ok ? d.sF[k * K2 + e] : R(0);
+      }
+#pragma unroll
+      for (int t = 0; t < 2; t++) {
+        // weights 1 − t on the outgoing segment (the node is its start), t on the incoming one
+        if (key0[t] == lk[t]) {
+          const R wgt = t == 0 ? R(1) - t0[t] : t0[t];
+          for (int k = 0; k < 3; k++) F[k] += wgt * f0[t][k];
+        }
+        for (int e = lo[t] + 1; e < hi[t]; e++)
+          if (oseg[e] == lk[t]) {
+            const R wgt = t == 0 ? R(1) - d.sT[e] : d.sT[e];
+            for (int k = 0; k < 3; k++) F[k] += wgt * d.sF[k * K2 + e];
+          }
+      }
+    }
+  } else {
+    if (cx && so >= 0)
+      sidesOn<SHORT>(d, sc.obuf, so, 0, [&](int q) {
+        const R wgt = R(1) - d.sT[q];
+        for (int k = 0; k < 3; k++) F[k] += wgt * d.sF[k * K2 + q];
+      });
+    if (cx && si >= 0)
+      sidesOn<SHORT>(d, sc.obuf, si, 0, [&](int q) {
+        const R wgt = d.sT[q];
+        for (int k = 0; k < 3; k++) F[k] += wgt * d.sF[k * K2 + q];
+      });
+  }
   const R react[3] = {-F[0], -F[1], -F[2]};
   for (int k = 0; k < 3; k++) if (!(fl & (1 << k))) F[k] = R(0);
   pt.x[RX_F] = mmax(pt.x[RX_F], A(msqrt(dot3(F, F))));
@@ -996,16 +1075,51 @@ __device__ __forceinline__ void segUpdate(const Dev<P> &d, const InstDesc &I, co
   R kTw = R(0);
   if (I.contacts && I.K) {
     const int lj = SHORT ? ro(d.segLocal + j) : 0;
-    sidesOn<SHORT>(d, sc.obuf, j, lj, [&](int q) { for (int k = 0; k < 3; k++) T[k] += d.sTq[k * K2 + q]; });
     if constexpr (SHORT) {
-      // the sides on segment j after the slide were, before it, on j − 1, j or j + 1 of the same strand
+      // The lever torques of the sides on j (its slice, entries keyed lj) and the twist stiffness of the sides on j
+      // after the slide, which before it were on j − 1, j or j + 1 of the same strand (those slices, entries keyed
+      // lj − 1, lj, lj + 1 whose key after the slide is lj).  The three slices' bounds load together, then the first
+      // entry of each, so the gathers take two levels of dependent loads; further entries follow in order.
+      const int ob = sc.obuf;
+      const int *oseg = d.ordSeg + size_t(ob) * d.oB;
       const int s = ro(d.segStrand + j);
-      for (int dj = -1; dj <= 1; dj++) {
-        const int jj = j + dj;
-        if (jj < 0 || jj >= mt || ro(d.segStrand + jj) != s) continue;
-        sidesOn<true>(d, sc.obuf, jj, lj + dj, [&](int q) { if (d.sKeyS[q] == lj) kTw += d.kth[q]; });
+      int lo[3], hi[3];
+#pragma unroll
+      for (int t = 0; t < 3; t++) {
+        // a neighbour outside the instance is never on j's strand; it is not read either (in the resident form the
+        // slice arrays hold this instance's segments only)
+        const int jj = j + t - 1;
+        const bool inr = jj >= I.m0 && jj < I.m0 + I.m;
+        const int jc = inr ? jj : j;
+        const bool same = inr && ro(d.segStrand + jc) == s;
+        lo[t] = d.rngLo[size_t(ob) * d.rB + jc];
+        const int h = d.rngHi[size_t(ob) * d.rB + jc];
+        hi[t] = same ? h : lo[t];
+      }
+      int key0[3], ks0[3];
+      R kv0[3], tq0[3];
+#pragma unroll
+      for (int t = 0; t < 3; t++) {
+        const bool ok = lo[t] < hi[t];
+        const int e = lo[t];
+        key0[t] = ok ? oseg[e] : NO_KEY;
+        ks0[t] = ok ? d.sKeyS[e] : NO_KEY;
+        kv0[t] = ok ? d.kth[e] : R(0);
+      }
+#pragma unroll
+      for (int k = 0; k < 3; k++) tq0[k] = lo[1] < hi[1] ? d.sTq[k * K2 + lo[1]] : R(0);
+      if (key0[1] == lj) for (int k = 0; k < 3; k++) T[k] += tq0[k];
+      for (int e = lo[1] + 1; e < hi[1]; e++)
+        if (oseg[e] == lj) for (int k = 0; k < 3; k++) T[k] += d.sTq[k * K2 + e];
+#pragma unroll
+      for (int t = 0; t < 3; t++) {
+        const int want = lj + t - 1;
+        if (key0[t] == want && ks0[t] == lj) kTw += kv0[t];
+        for (int e = lo[t] + 1; e < hi[t]; e++)
+          if (oseg[e] == want && d.sKeyS[e] == lj) kTw += d.kth[e];
       }
     } else {
+      sidesOn<SHORT>(d, sc.obuf, j, lj, [&](int q) { for (int k = 0; k < 3; k++) T[k] += d.sTq[k * K2 + q]; });
       sidesOn<false>(d, sc.onxt, j, 0, [&](int q) { kTw += d.kth[q]; });
     }
   }
