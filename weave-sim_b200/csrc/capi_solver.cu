@@ -1390,8 +1390,10 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     const int parts = std::max({c->shape.blocksA + c->shape.blocksDS, c->shape.blocksA + c->shape.blocksD,
                                 c->shape.blocksX + c->shape.blocksY + std::max(c->shape.blocksDN, c->shape.blocksDNS) + c->shape.blocksDM,
                                 c->gridBlocks[0][0], c->gridBlocks[0][1], c->gridBlocks[1][0], c->gridBlocks[1][1]});
-    CK(cudaMalloc(&c->dPart, sizeof(double) * (RS_NSUM + RX_NMAX) * size_t(parts)));
-    CK(cudaMalloc(&c->dBar, 4 * sizeof(unsigned)));     // [0..1] grid barrier, [2] plain form's finishing-block counter
+    // one row more than the blocks: the plain form's summary of the element and node partials
+    CK(cudaMalloc(&c->dPart, sizeof(double) * (RS_NSUM + RX_NMAX) * (size_t(parts) + 1)));
+    // [0..1] grid barrier; [2..3] the plain form's finishing-block counter (64 bits in the split update phase)
+    CK(cudaMalloc(&c->dBar, 4 * sizeof(unsigned)));
     CK(cudaMemsetAsync(c->dBar, 0, 4 * sizeof(unsigned), c->st));
     CK(cudaMalloc(&c->dErr, sizeof(int)));
     c->shortSides = shortOrderOK(c);

@@ -769,6 +769,146 @@ __global__ void __launch_bounds__(256) k_plainBC(Dev<P> d, const InstDesc *__res
 // The end of an iteration without the extensions, run by the update phase's last block: every block partial reduced in
 // a fixed order, then the kinetic-damping decision.  Out of line, so that its registers do not count against the
 // element loop's budget.  The control block is read again here: no block writes it before this one.
+// ---- the split close: one slot of one range of partials a warp
+// One slot of a range of block partials (rows [lo, hi)), a sum or a maximum, reduced by one warp: lane l takes rows
+// lo + l, lo + l + 32, ... in row order, the loads of a pass issued together, then a butterfly over the lanes leaves
+// the same value in every lane.
+template <class A>
+__device__ __forceinline__ A warpSlot(const A *part, int stride, int slot, bool mx, A ident, int lo, int hi) {
+  const int lane = threadIdx.x & 31;
+  const A *p = part + size_t(slot) * stride;
+  A acc = ident;
+  constexpr int U = 12;
+  for (int b0 = lo; b0 < hi; b0 += 32 * U) {
+    A v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int b = b0 + lane + 32 * u;
+      v[u] = b < hi ? __ldcg(p + b) : ident;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) acc = mx ? mmax(acc, v[u]) : acc + v[u];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const A w = __shfl_xor_sync(0xffffffffu, acc, o);
+    acc = mx ? mmax(acc, w) : acc + w;
+  }
+  return acc;
+}
+// a range of partial rows and the slots its kernel feeds
+struct SlotRange { int lo, hi; unsigned sums, maxs; };
+// the k-th (range, slot) item of ranges r[0..nr), sum slots before maximum slots within a range; false past the end
+__device__ __forceinline__ bool slotItem(const SlotRange *r, int nr, int k, int &ri, int &slot, bool &mx) {
+  for (int i = 0; i < nr; i++) {
+    for (int b = 0; b < RS_NSUM + RX_NMAX; b++) {
+      const bool isMax = b >= RS_NSUM;
+      const unsigned m = isMax ? r[i].maxs : r[i].sums;
+      if (!(m & (1u << (isMax ? b - RS_NSUM : b)))) continue;
+      if (k == 0) { ri = i; slot = b; mx = isMax; return true; }
+      k--;
+    }
+  }
+  return false;
+}
+__device__ __forceinline__ int slotItems(const SlotRange *r, int nr) {
+  int n = 0;
+  for (int i = 0; i < nr; i++) n += __popc(r[i].sums) + __popc(r[i].maxs);
+  return n;
+}
+// identity of a slot: 0, or -inf for the largest normal force
+template <class A> __device__ __forceinline__ A slotIdent(int slot) { return slot == RS_NSUM + RX_FN ? -A(INFINITY) : A(0); }
+// every item of the ranges, one a warp (warp w: items w, w + warps, ...), values into vals[item] (shared); then
+// thread 0 folds them into q in item order (ranges in order), so the result does not depend on timing
+template <class A>
+__device__ __forceinline__ void slotsToVals(const SlotRange *r, int nr, const A *part, int stride, A *vals) {
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, lane = threadIdx.x & 31;
+  const int n = slotItems(r, nr);
+  for (int k = warp; k < n; k += nw) {
+    int ri, slot;
+    bool mx;
+    slotItem(r, nr, k, ri, slot, mx);
+    const A v = warpSlot(part, stride, slot, mx, slotIdent<A>(slot), r[ri].lo, r[ri].hi);
+    if (lane == 0) vals[k] = v;
+  }
+}
+// thread 0, after a barrier: the items' values folded into q in item order
+template <class A>
+__device__ __forceinline__ void foldVals(const SlotRange *r, int nr, const A *vals, Part<A> &q) {
+  const int n = slotItems(r, nr);
+  for (int k = 0; k < n; k++) {
+    int ri, slot;
+    bool mx;
+    slotItem(r, nr, k, ri, slot, mx);
+    if (mx) q.x[slot - RS_NSUM] = mmax(q.x[slot - RS_NSUM], vals[k]);
+    else q.s[slot] += vals[k];
+  }
+}
+template <class A>
+__device__ __forceinline__ void reduceSlots(const SlotRange *r, int nr, const A *part, int stride, A *vals, Part<A> &q) {
+  const int n = slotItems(r, nr);
+  slotsToVals(r, nr, part, stride, vals);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < n; k++) {
+      int ri, slot;
+      bool mx;
+      slotItem(r, nr, k, ri, slot, mx);
+      if (mx) q.x[slot - RS_NSUM] = mmax(q.x[slot - RS_NSUM], vals[k]);
+      else q.s[slot] += vals[k];
+    }
+  }
+}
+
+// The node kernel's last block (split update phase without the extensions): the partials of the crossings, the rods and
+// the nodes reduced into the summary row S (slot i at S[i]), which the iteration's close reads instead of their rows.
+template <class A>
+__device__ __noinline__ void summariseNodes(const A *partAll, int ex, int ey, int en, int stride, A *S) {
+  __shared__ A vals[32];
+  const SlotRange r[3] = {{0, ex, elemSums(1), elemMaxs(1)}, {ex, ey, elemSums(2), elemMaxs(2)},
+                          {ey, en, updateSums(1, false), updateMaxs(1, false)}};
+  Part<A> q;
+  q.init();
+  reduceSlots(r, 3, partAll, stride, vals, q);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < RS_NSUM; i++) S[i] = q.s[i];
+    for (int i = 0; i < RX_NMAX; i++) S[RS_NSUM + i] = q.x[i];
+  }
+}
+// The close of a split iteration without the extensions: the summary row and the segment kernel's partials (rows
+// [en, em), one slot a warp), then the kinetic-damping decision.  The control block, the descriptor and the summary row
+// are copied to shared memory a word a thread, their loads in flight beside the partials'.
+template <class A>
+__device__ __noinline__ void closeSplit(const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl, const A *partAll,
+                                        int en, int em, int stride, const A *S, unsigned long long *counter) {
+  __shared__ InstCtl sc;
+  __shared__ InstDesc si;
+  __shared__ A vals[32], sS[RS_NSUM + RX_NMAX];
+  constexpr int NC = sizeof(InstCtl) / 4, ND = sizeof(InstDesc) / 4, NV = RS_NSUM + RX_NMAX;
+  static_assert(NC <= 64 && 64 + ND <= 224 && NV <= 32, "the copies take one word a thread of a 256-thread block");
+  const int t = threadIdx.x;
+  int wc = 0, wd = 0;
+  A ws = A(0);
+  if (t < NC) wc = __ldcg(reinterpret_cast<const int *>(ctl) + t);
+  if (t >= 64 && t < 64 + ND) wd = __ldg(reinterpret_cast<const int *>(insts) + (t - 64));
+  if (t >= 224 && t < 224 + NV) ws = __ldcg(S + (t - 224));
+  const SlotRange r[1] = {{en, em, updateSums(2, false), updateMaxs(2, false)}};
+  slotsToVals(r, 1, partAll, stride, vals);
+  if (t < NC) reinterpret_cast<int *>(&sc)[t] = wc;
+  if (t >= 64 && t < 64 + ND) reinterpret_cast<int *>(&si)[t - 64] = wd;
+  if (t >= 224 && t < 224 + NV) sS[t - 224] = ws;
+  __syncthreads();
+  if (t == 0) {
+    Part<A> q;
+    for (int i = 0; i < RS_NSUM; i++) q.s[i] = sS[i];
+    for (int i = 0; i < RX_NMAX; i++) q.x[i] = sS[RS_NSUM + i];
+    foldVals(r, 1, vals, q);
+    InstCtl cc = sc;
+    decide<false>(si, cc, q, 0);
+    ctl[0] = cc;
+    *counter = 0ull;
+  }
+}
 template <bool SPLIT, class A>
 __device__ __noinline__ void closeIteration(const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl, const A *partAll,
                                             int ex, int ey, int en, int em, int partStride, unsigned *counter, A *red) {
@@ -823,6 +963,39 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
   }
   constexpr unsigned SM = updateSums(PART, EXT), XM = updateMaxs(PART, EXT);
   blockReduce<SM, XM>(pt, red);
+  if constexpr (!EXT && PART != 0) {
+    // The split update phase counts its blocks on one 64-bit counter: node blocks in the high word, segment blocks
+    // in the low word.  The node kernel's last block summarises the partials of the crossings, the rods and the nodes
+    // (summariseNodes), then adds all node blocks to the low word at once; the block that brings the low word to the
+    // total closes the iteration from the summary and the segment partials (closeSplit).
+    __shared__ int role;                       // 0 done, 1 summarise, 2 close
+    unsigned long long *cnt = reinterpret_cast<unsigned long long *>(counter);
+    A *S = partAll + size_t(RS_NSUM + RX_NMAX) * partStride;
+    if (threadIdx.x == 0) {
+      putPartSlots<SM, XM>(pt, part, blk, partStride);
+      __threadfence();
+      const unsigned long long old = atomicAdd(cnt, PART == 1 ? (1ull << 32) : 1ull);
+      role = (PART == 1 && unsigned(old >> 32) == unsigned(nblk) - 1u) ? 1
+             : (PART == 2 && unsigned(old) + 1u == nBlocks) ? 2 : 0;
+    }
+    __syncthreads();
+    const int rl = role;
+    if (rl == 0) return;
+    __threadfence();
+    if (rl == 1) {
+      summariseNodes<A>(partAll, pe.x, pe.y, pe.n, partStride, S);
+      if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned long long old = atomicAdd(cnt, (unsigned long long)unsigned(nblk));
+        role = unsigned(old) + unsigned(nblk) == nBlocks ? 2 : 0;
+      }
+      __syncthreads();
+      if (role != 2) return;
+      __threadfence();
+    }
+    closeSplit<A>(insts, ctl, partAll, pe.n, pe.m, partStride, S, cnt);
+    return;
+  }
   if (threadIdx.x == 0) {
     putPartSlots<SM, XM>(pt, part, blk, partStride);
     __threadfence();
