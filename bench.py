@@ -323,7 +323,7 @@ def run_workload(args):
             metric = "position / slide / stick-slip agreement with FP64 after the 5000-iteration cap, and throughput"
         elif args.workload == "batch":
             r = workloads.run_batch(count=args.instances or 512, wide_cluster=args.wide_cluster, threads=args.threads,
-                                    wide_min=args.wide_min, tune=args.tune, plain_sample=0 if args.no_plain else 16)
+                                    wide_min=args.wide_min, tune=not args.no_tune, plain_sample=0 if args.no_plain else 16)
             metric = "solves/s and DR iters/s of 512 mixed gridshells to the 5000-iteration cap"
         elif args.workload == "ratio":
             r = workloads.run_ratio()
@@ -367,7 +367,9 @@ def main():
     ap.add_argument("--wide-cluster", type=int, default=0, help="batch workload: blocks per wide instance (1: none)")
     ap.add_argument("--wide-min", type=int, default=0, help="batch workload: nodes + segments of a wide instance")
     ap.add_argument("--threads", type=int, default=0, help="batch workload: threads per block of the one-block kernels")
-    ap.add_argument("--tune", action="store_true", help="batch workload: the autotuner picks the launch shape")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="batch workload: the launch shape from --threads / --wide-cluster / --wide-min instead of the "
+                         "autotuner's (the default: the autotuner picks it, or takes it from its cache)")
     ap.add_argument("--no-plain", action="store_true", help="batch workload: skip the plain-form comparison")
     args = ap.parse_args()
     if args.workload != "shell_large":
