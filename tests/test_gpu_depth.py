@@ -3,10 +3,12 @@
 The benchmarked configurations, each checked past the 300-iteration warm-up that holds every node
 (web/js/solver_cpu.js:775-776) and into the contact ramp (1500 iterations) and the support motion:
 
-* the 20 m shell (the headline workload): FP64 in the plain and grid forms with the oracle's iteration and roll-back
-  counts and within 1e-9 of the span, slide coordinates within 1e-6 segments, the same stick/slip states, at 330,
-  1000 and 2000 iterations; the mixed policy (FP32 element math, two-float state, FP64 reductions) within the
-  1e-4 span gate wherever the oracle's own chaos floor (the oracle started 1e-9 of the span away) is below it;
+* the 20 m shell (the headline workload, timed from iteration 600 on): FP64 in the plain and grid forms with the
+  oracle's iteration and roll-back counts and within 1e-9 of the span, slide coordinates within 1e-6 segments, the
+  same stick/slip states, at 330, 1000, 2000 and 3000 iterations; at 5000 and 8000, where the trajectory's chaos has
+  set in (the oracle started 1e-9 of the span away departs from itself by ~3e-5 of the span), the oracle's roll-back
+  count and a distance from the oracle within the oracle's own spread; the mixed policy (FP32 element math,
+  two-float state, FP64 reductions) within the 1e-4 span gate at every horizon where that spread is below it;
 * the stiff dome (25 x 3 mm laths, E 12 GPa, per-crossing mu ~ U(0.1, 0.5)): FP64 exact to 1500 iterations in the
   batched and plain forms; a population of them in FP64, mixed and naive FP32 against the oracle at 500 to 3000
   iterations, the mixed policy within the gate, naive FP32 reported;
@@ -26,12 +28,13 @@ import weavesim_b200 as ws
 
 pytestmark = pytest.mark.gpu
 
-HORIZONS = (330, 1000, 2000)
+HORIZONS = (330, 1000, 2000, 3000, 5000, 8000)
+EXACT = 3000                # FP64 is held to the oracle's bits (to rounding) up to here, to its chaos floor beyond
 GATE = 1e-4                 # max node distance / span, the acceptance gate of the mixed policy
 # FP64 against the oracle at depth: positions within 1e-9 of the span; slide coordinates (in segments) within 1e-6.  The
 # slides are where the trajectory's chaos shows first: on the shell the oracle started 1e-9 of the span away differs
 # from itself by 5e-6 segments at 330 iterations and 6e-3 at 2000, while FP64 on the device (another summation order)
-# differs from the oracle by 2e-13 and 3e-8.
+# differs from the oracle by 2e-13 and 3e-8 (4e-7 at 3000).
 SLIDE_F64 = 1e-6
 
 
@@ -105,12 +108,18 @@ def test_shell_f64_matches_oracle_at_depth(shell, form):
                     chaos_floor=floor[h]) for h in HORIZONS}
     cases.record(f"shell_f64_{form}", {"horizons": rows})
     for h in HORIZONS:
-        g, v = got[h], ref[h]
+        g, v, r, f = got[h], ref[h], rows[h], floor[h]
         assert g["iteration"] == v["iteration"] == h
         assert g["rollbacks"] == v["rollbacks"], h
-        assert rows[h]["pos_span"] < 1e-9, (h, rows[h])
-        assert rows[h]["slide"] < SLIDE_F64, (h, rows[h])
-        assert rows[h]["stuck_mismatch"] == 0, (h, rows[h])
+        if h <= EXACT:
+            assert r["pos_span"] < 1e-9, (h, r)
+            assert r["slide"] < SLIDE_F64, (h, r)
+            assert r["stuck_mismatch"] == 0, (h, r)
+        else:
+            # past the onset of chaos: no farther from the oracle than the oracle is from itself
+            assert r["pos_span"] <= max(1e-9, f["pos_span"]), (h, r)
+            assert r["slide"] <= max(SLIDE_F64, f["slide"]), (h, r)
+            assert r["stuck_mismatch"] <= 2 * f["stuck_mismatch"] + max(1, md.K // 1000), (h, r)
 
 
 @pytest.mark.parametrize("form", ["plain", "grid"])
