@@ -9,7 +9,8 @@
   span's reduction: each support moves radially by half of it), ~5 cm segments), relaxed together to the iteration cap.
 * ``ratio`` — the batched form (592 domes) against the plain single-instance form on the 3 m dome.
 * ``serve`` — the serving loop under Poisson arrivals at the given rates: fresh stiff domes (new seed each) and, with
-  probability 0.3, variants (±5 % E, ±0.1 μ, ±2 % support displacement) of a resident equilibrium, warm-started.
+  probability 0.3, variants (±5 % E, ±0.1 μ, ±2 % support displacement) of a resident equilibrium, warm-started; a
+  sample of the served results against FP64 (the same requests relaxed again in FP64) beside FP64's own chaos floor.
 * ``scene`` — the reference's example scene dome_basic (read from its scene.json by the scene reader): one solve to
   convergence (or the scene's 8000-iteration cap) in FP64 and mixed, plain and batched forms; the mixed result against
   FP64 beside the chaos floor (FP64 against FP64 started with every node moved by ~1e-9·span and ~1e-7·span, the
@@ -223,6 +224,7 @@ def run_serve(rates=(50.0, 200.0, 1000.0), counts=(300, 600, 1000), slots=296, c
     seed_reqs = serve.poisson_stream(1e6, 8, seed=1, variant_share=0.0, fresh_cap=CAP)
     srv.run(seed_reqs, time_limit=time_limit)
     bank = list(srv.resident.values())
+    served = []
     for rate, count in zip(rates, counts):
         srv.done, srv.ticks, srv.busy_slot_ticks = [], 0, 0
         reqs = serve.poisson_stream(rate, count, seed=int(rate), variant_share=0.3, fresh_cap=CAP, variant_cap=1500,
@@ -230,6 +232,7 @@ def run_serve(rates=(50.0, 200.0, 1000.0), counts=(300, 600, 1000), slots=296, c
         t0 = time.perf_counter()
         done = srv.run(reqs, time_limit=time_limit)
         wall = time.perf_counter() - t0
+        served += done
         lat = serve.latency_summary(done)
         fresh = [r for r in done if r.kind == "fresh"]
         var = [r for r in done if r.kind == "variant"]
@@ -241,4 +244,33 @@ def run_serve(rates=(50.0, 200.0, 1000.0), counts=(300, 600, 1000), slots=296, c
                                  fresh_p50_s=serve.latency_summary(fresh)["p50_s"] if fresh else None,
                                  variant_p50_s=serve.latency_summary(var)["p50_s"] if var else None))
     srv.dispose()
+    out["error_vs_f64"] = _served_error(served)
+    return out
+
+
+def _served_error(done, sample=64, seed=3):
+    """the served (mixed-precision) results against FP64: a sample of the finished requests relaxed again from their
+    start in FP64, one batch, each to the iteration count it was served at; beside it the chaos floor, FP64 started with
+    every node moved by 1e-9 of the span.  Max node distance / span per request (median, max, and how many are within
+    1e-4), slide coordinates (segments) and stick/slip states."""
+    rng = np.random.default_rng(seed)
+    pick = [done[i] for i in sorted(rng.choice(len(done), size=min(sample, len(done)), replace=False))]
+    models, pert = [], []
+    for r in pick:
+        m = r.model.copy()
+        m.params = dict(m.params, max_iter=int(r.iters))
+        models.append(m)
+        p = m.copy()
+        p.X = p.X + 1e-9 * m.span * rng.standard_normal(p.X.shape)
+        pert.append(p)
+    cap = max(int(r.iters) for r in pick)
+    ref, _, _, _ = _relax(models, "f64", cap)
+    flo, _, _, _ = _relax(pert, "f64", cap)
+    served = [{"X": r.result["X"], "u": r.result["u"], "state": r.result["state"], "stuck": r.result["stuck"]} for r in pick]
+    out = {"requests": len(pick), "fresh": sum(r.kind == "fresh" for r in pick), "variants": sum(r.kind == "variant" for r in pick),
+           "served_mixed": _compare(served, ref, models), "chaos_floor_f64": _compare(flo, ref, models)}
+    for kind in ("fresh", "variant"):
+        idx = [i for i, r in enumerate(pick) if r.kind == kind]
+        if idx:
+            out[f"served_mixed_{kind}"] = _compare([served[i] for i in idx], [ref[i] for i in idx], [models[i] for i in idx])
     return out
