@@ -860,6 +860,13 @@ __device__ __forceinline__ void reduceSlots(const SlotRange *r, int nr, const A 
   }
 }
 
+// fetch-and-add on a GPU-scope counter with acquire-release semantics: the calling thread's earlier writes become
+// visible to any thread that later acquires the counter, and the caller sees the writes released by the earlier adds
+__device__ __forceinline__ unsigned long long ticketAdd(unsigned long long *p, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  return old;
+}
 // The node kernel's last block (split update phase without the extensions): the partials of the crossings, the rods and
 // the nodes reduced into the summary row S (slot i at S[i]), which the iteration's close reads instead of their rows.
 template <class A>
@@ -971,27 +978,26 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
     __shared__ int role;                       // 0 done, 1 summarise, 2 close
     unsigned long long *cnt = reinterpret_cast<unsigned long long *>(counter);
     A *S = partAll + size_t(RS_NSUM + RX_NMAX) * partStride;
+    // The tickets are acquire-release fetch-and-adds by thread 0, which also wrote the block's partials (and the
+    // summary): its writes are released with its ticket, and the block that takes the last ticket acquires every
+    // earlier one before its barrier, after which its threads read the partials from L2 (no separate fences).
     if (threadIdx.x == 0) {
       putPartSlots<SM, XM>(pt, part, blk, partStride);
-      __threadfence();
-      const unsigned long long old = atomicAdd(cnt, PART == 1 ? (1ull << 32) : 1ull);
+      const unsigned long long old = ticketAdd(cnt, PART == 1 ? (1ull << 32) : 1ull);
       role = (PART == 1 && unsigned(old >> 32) == unsigned(nblk) - 1u) ? 1
              : (PART == 2 && unsigned(old) + 1u == nBlocks) ? 2 : 0;
     }
     __syncthreads();
     const int rl = role;
     if (rl == 0) return;
-    __threadfence();
     if (rl == 1) {
       summariseNodes<A>(partAll, pe.x, pe.y, pe.n, partStride, S);
       if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned long long old = atomicAdd(cnt, (unsigned long long)unsigned(nblk));
+        const unsigned long long old = ticketAdd(cnt, (unsigned long long)unsigned(nblk));
         role = unsigned(old) + unsigned(nblk) == nBlocks ? 2 : 0;
       }
       __syncthreads();
       if (role != 2) return;
-      __threadfence();
     }
     closeSplit<A>(insts, ctl, partAll, pe.n, pe.m, partStride, S, cnt);
     return;

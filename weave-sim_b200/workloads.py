@@ -67,7 +67,7 @@ def run_scene(path, copies=64):
     for prec in ("f64", "mixed"):
         for form in ("plain", "cta"):
             s = GpuSolver([md.copy()], precision=prec, form=form)
-            s.step(10)                                     # first-launch costs out of the timing
+            s.step(50)                  # first-launch costs and the plain form's graph capture out of the timing
             s.load_instance(0, md.copy())                  # back to the scene's start, iteration 0
             ctl = s.step(cap)[0]
             ms = s.last_step_stats()[0]
@@ -139,12 +139,12 @@ def run_ratio(batch=592, iters=400):
     """the batched form against the plain single-instance GPU form on the 3 m dome (mixed precision)"""
     models = [configs.dome_small(seed=1 + b) for b in range(batch)]
     s = GpuSolver([models[0].copy()], precision="mixed", form="plain")
-    s.step(20)
+    s.step(iters, read=False)               # untimed: the first launches and the capture of the iteration graph
     s.step(iters, read=False)
     ms_plain = s.last_step_stats()[0]
     s.dispose()
     s = GpuSolver(models, precision="mixed", threads=512)
-    s.step(10)
+    s.step(iters, read=False)
     s.step(iters, read=False)
     ms_batch = s.last_step_stats()[0]
     s.dispose()
@@ -156,11 +156,12 @@ def run_ratio(batch=592, iters=400):
 
 
 def _plain_iter_ms(models, precision, iters=200):
-    """device ms per iteration of the plain single-instance form on each model (after 20 warm-up iterations)"""
+    """device ms per iteration of the plain single-instance form on each model (after an untimed step of the same
+    length, which captures the iteration graph the timed step launches)"""
     out = []
     for m in models:
         s = GpuSolver([m.copy()], precision=precision, form="plain")
-        s.step(20, read=False)
+        s.step(iters, read=False)
         s.step(iters, read=False)
         out.append(s.last_step_stats()[0] / iters)
         s.dispose()
