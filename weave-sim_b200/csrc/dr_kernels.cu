@@ -25,11 +25,15 @@
 #ifndef WSB_MINB_XY
 #define WSB_MINB_XY 2
 #endif
+// The split update kernels (nodes, segments) without the extensions run five blocks of 256 threads per SM in the
+// mixed and FP32 policies (48 registers, a few dozen bytes of spill): with the crossing and rod kernels' results in
+// L2, both kernels' blocks are then resident at once, measured 0.8 us an iteration faster on the 20 m shell than three
+// blocks at 80 registers.  FP64 and the extension variants need more registers and keep three.
 #ifndef WSB_MINB_DN
-#define WSB_MINB_DN 3
+#define WSB_MINB_DN(P, EXT) (((P) == PREC_F64 || (EXT)) ? 3 : 5)
 #endif
 #ifndef WSB_MINB_DM
-#define WSB_MINB_DM 3
+#define WSB_MINB_DM(P, EXT) (((P) == PREC_F64 || (EXT)) ? 3 : 5)
 #endif
 #ifndef WSB_MINB_G
 #define WSB_MINB_G 2
@@ -1036,13 +1040,13 @@ __global__ void __launch_bounds__(256, WSB_MINB_D) k_plainD(Dev<P> d, const Inst
   plainD<P, SHORT, EXT, 0>(d, insts, ctl, part, partAll, pe, partStride, counter, gridDim.x, blockIdx.x, gridDim.x);
 }
 template <int P, bool SHORT, bool EXT>
-__global__ void __launch_bounds__(256, WSB_MINB_DN) k_plainDN(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+__global__ void __launch_bounds__(256, WSB_MINB_DN(P, EXT)) k_plainDN(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                                   typename Dev<P>::A *part, typename Dev<P>::A *partAll, PartEnds pe,
                                                   int partStride, unsigned *counter, unsigned nBlocks) {
   plainD<P, SHORT, EXT, 1>(d, insts, ctl, part, partAll, pe, partStride, counter, nBlocks, blockIdx.x, gridDim.x);
 }
 template <int P, bool SHORT, bool EXT>
-__global__ void __launch_bounds__(256, WSB_MINB_DM) k_plainDM(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+__global__ void __launch_bounds__(256, WSB_MINB_DM(P, EXT)) k_plainDM(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                                   typename Dev<P>::A *part, typename Dev<P>::A *partAll, PartEnds pe,
                                                   int partStride, unsigned *counter, unsigned nBlocks) {
   plainD<P, SHORT, EXT, 2>(d, insts, ctl, part, partAll, pe, partStride, counter, nBlocks, blockIdx.x, gridDim.x);
@@ -1050,7 +1054,7 @@ __global__ void __launch_bounds__(256, WSB_MINB_DM) k_plainDM(Dev<P> d, const In
 // The update phase as one launch with roles: the first nbN blocks the nodes (with the side ranks of the short order),
 // the others the segments; the last of all its blocks closes the iteration.
 template <int P, bool SHORT, bool EXT>
-__global__ void __launch_bounds__(256, WSB_MINB_DN) k_plainDNM(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
+__global__ void __launch_bounds__(256, WSB_MINB_DN(P, EXT)) k_plainDNM(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                                    typename Dev<P>::A *part, typename Dev<P>::A *partAll, PartEnds pe,
                                                    int partStride, unsigned *counter, int nbN) {
   waitPrevGrid();
