@@ -886,12 +886,28 @@ __device__ __noinline__ void summariseNodes(const A *partAll, int ex, int ey, in
     for (int i = 0; i < RX_NMAX; i++) S[RS_NSUM + i] = q.x[i];
   }
 }
+// The element summary block of the node kernel (fork launch without the extensions): the crossing and rod partials,
+// complete before the update phase starts, reduced into the summary row S by one extra block of the node kernel while
+// the other blocks update the nodes, so that the close that follows the update blocks reads only the summary and the
+// update kernels' own partials.
+template <class A>
+__device__ __noinline__ void summariseElements(const A *partAll, int ex, int ey, int stride, A *S) {
+  __shared__ A vals[32];
+  const SlotRange r[2] = {{0, ex, elemSums(1), elemMaxs(1)}, {ex, ey, elemSums(2), elemMaxs(2)}};
+  Part<A> q;
+  q.init();
+  reduceSlots(r, 2, partAll, stride, vals, q);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < RS_NSUM; i++) S[i] = q.s[i];
+    for (int i = 0; i < RX_NMAX; i++) S[RS_NSUM + i] = q.x[i];
+  }
+}
 // The close of a split iteration without the extensions: the summary row and the segment kernel's partials (rows
 // [en, em), one slot a warp), then the kinetic-damping decision.  The control block, the descriptor and the summary row
 // are copied to shared memory a word a thread, their loads in flight beside the partials'.
 template <class A>
 __device__ __noinline__ void closeSplit(const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl, const A *partAll,
-                                        int en, int em, int stride, const A *S, unsigned long long *counter) {
+                                        int ey, int en, int em, int stride, const A *S, unsigned long long *counter) {
   __shared__ InstCtl sc;
   __shared__ InstDesc si;
   __shared__ A vals[32], sS[RS_NSUM + RX_NMAX];
@@ -903,8 +919,11 @@ __device__ __noinline__ void closeSplit(const InstDesc *__restrict__ insts, Inst
   if (t < NC) wc = __ldcg(reinterpret_cast<const int *>(ctl) + t);
   if (t >= 64 && t < 64 + ND) wd = __ldg(reinterpret_cast<const int *>(insts) + (t - 64));
   if (t >= 224 && t < 224 + NV) ws = __ldcg(S + (t - 224));
-  const SlotRange r[1] = {{en, em, updateSums(2, false), updateMaxs(2, false)}};
-  slotsToVals(r, 1, partAll, stride, vals);
+  // ey < 0: the summary covers the node rows too (the segment rows alone remain); else the node rows [ey, en) as well
+  const SlotRange r[2] = {{ey, en, updateSums(1, false), updateMaxs(1, false)}, {en, em, updateSums(2, false), updateMaxs(2, false)}};
+  const SlotRange *rr = ey < 0 ? r + 1 : r;
+  const int nr = ey < 0 ? 1 : 2;
+  slotsToVals(rr, nr, partAll, stride, vals);
   if (t < NC) reinterpret_cast<int *>(&sc)[t] = wc;
   if (t >= 64 && t < 64 + ND) reinterpret_cast<int *>(&si)[t - 64] = wd;
   if (t >= 224 && t < 224 + NV) sS[t - 224] = ws;
@@ -913,7 +932,7 @@ __device__ __noinline__ void closeSplit(const InstDesc *__restrict__ insts, Inst
     Part<A> q;
     for (int i = 0; i < RS_NSUM; i++) q.s[i] = sS[i];
     for (int i = 0; i < RX_NMAX; i++) q.x[i] = sS[RS_NSUM + i];
-    foldVals(r, 1, vals, q);
+    foldVals(rr, nr, vals, q);
     InstCtl cc = sc;
     decide<false>(si, cc, q, 0);
     ctl[0] = cc;
@@ -951,7 +970,10 @@ __device__ __noinline__ void closeIteration(const InstDesc *__restrict__ insts, 
 // fixed order and takes the kinetic-damping decision.  Every block reads the control block before it counts itself,
 // so the last block's write cannot race a reader.  The phase runs whole (PART 0) or split in two kernels on forked
 // branches: the nodes with the side ranks (PART 1) and the segments (PART 2), each at its own register budget.
-template <int P, bool SHORT, bool EXT, int PART>
+// XYS (the fork launch without the extensions): the node kernel has one block more than its node blocks (blk == nblk),
+// which summarises the crossing and rod partials while the others update the nodes; every block of the pair then takes
+// one ticket, and the last closes the iteration from that summary and the node and segment partials.
+template <int P, bool SHORT, bool EXT, int PART, bool XYS = false>
 __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                        typename Dev<P>::A *part, typename Dev<P>::A *partAll, const PartEnds &pe,
                                        int partStride, unsigned *counter, unsigned nBlocks, int blk, int nblk) {
@@ -961,6 +983,16 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
   const InstDesc &I = insts[0];
   const InstCtl c = ctl[0];
   if (c.status != WS_RUNNING) return;
+  if constexpr (XYS && !EXT && PART == 1)
+    if (blk == nblk) {
+      unsigned long long *cnt = reinterpret_cast<unsigned long long *>(counter);
+      A *S = partAll + size_t(RS_NSUM + RX_NMAX) * partStride;
+      summariseElements<A>(partAll, pe.x, pe.y, partStride, S);
+      if (threadIdx.x == 0) last = unsigned(ticketAdd(cnt, 1ull)) + 1u == nBlocks;
+      __syncthreads();
+      if (last) closeSplit<A>(insts, ctl, partAll, pe.y, pe.n, pe.m, partStride, S, cnt);
+      return;
+    }
   const StepCtx sx = makeCtx<A>(I, c, EXT ? d.ext[I.utmIdx].pf : nullptr);
   Part<A> pt;
   pt.init();
@@ -974,6 +1006,18 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
   }
   constexpr unsigned SM = updateSums(PART, EXT), XM = updateMaxs(PART, EXT);
   blockReduce<SM, XM>(pt, red);
+  if constexpr (XYS && !EXT && PART != 0) {
+    unsigned long long *cnt = reinterpret_cast<unsigned long long *>(counter);
+    const A *S = partAll + size_t(RS_NSUM + RX_NMAX) * partStride;
+    if (threadIdx.x == 0) {
+      putPartSlots<SM, XM>(pt, part, blk, partStride);
+      last = unsigned(ticketAdd(cnt, 1ull)) + 1u == nBlocks;
+    }
+    __syncthreads();
+    if (!last) return;
+    closeSplit<A>(insts, ctl, partAll, pe.y, pe.n, pe.m, partStride, S, cnt);
+    return;
+  }
   if constexpr (!EXT && PART != 0) {
     // The split update phase counts its blocks on one 64-bit counter: node blocks in the high word, segment blocks
     // in the low word.  The node kernel's last block summarises the partials of the crossings, the rods and the nodes
@@ -1003,7 +1047,7 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
       __syncthreads();
       if (role != 2) return;
     }
-    closeSplit<A>(insts, ctl, partAll, pe.n, pe.m, partStride, S, cnt);
+    closeSplit<A>(insts, ctl, partAll, -1, pe.n, pe.m, partStride, S, cnt);
     return;
   }
   if (threadIdx.x == 0) {
@@ -1043,13 +1087,14 @@ template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(256, WSB_MINB_DN(P, EXT)) k_plainDN(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                                   typename Dev<P>::A *part, typename Dev<P>::A *partAll, PartEnds pe,
                                                   int partStride, unsigned *counter, unsigned nBlocks) {
-  plainD<P, SHORT, EXT, 1>(d, insts, ctl, part, partAll, pe, partStride, counter, nBlocks, blockIdx.x, gridDim.x);
+  plainD<P, SHORT, EXT, 1, !EXT>(d, insts, ctl, part, partAll, pe, partStride, counter, nBlocks, blockIdx.x,
+                                  EXT ? gridDim.x : gridDim.x - 1);
 }
 template <int P, bool SHORT, bool EXT>
 __global__ void __launch_bounds__(256, WSB_MINB_DM(P, EXT)) k_plainDM(Dev<P> d, const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl,
                                                   typename Dev<P>::A *part, typename Dev<P>::A *partAll, PartEnds pe,
                                                   int partStride, unsigned *counter, unsigned nBlocks) {
-  plainD<P, SHORT, EXT, 2>(d, insts, ctl, part, partAll, pe, partStride, counter, nBlocks, blockIdx.x, gridDim.x);
+  plainD<P, SHORT, EXT, 2, !EXT>(d, insts, ctl, part, partAll, pe, partStride, counter, nBlocks, blockIdx.x, gridDim.x);
 }
 // The update phase as one launch with roles: the first nbN blocks the nodes (with the side ranks of the short order),
 // the others the segments; the last of all its blocks closes the iteration.
@@ -1543,7 +1588,9 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
     const int nbY = WSB_Y_THREADS(P) == 256 ? sh.blocksY : (sh.blocksY + 1) / 2;
     const int nDN = sh2 ? sh.blocksDNS : sh.blocksDN, nParts = sh.blocksX + nbY + nDN + sh.blocksDM;
     A *px = static_cast<A *>(part), *py = px + sh.blocksX, *pn = py + nbY, *pm = pn + nDN;
-    const unsigned nB = unsigned(nDN + sh.blocksDM);
+    // without the extensions the node kernel runs one more block, which summarises the element partials
+    const int xys = ext ? 0 : 1;
+    const unsigned nB = unsigned(nDN + xys + sh.blocksDM);
     const PartEnds pe{sh.blocksX, sh.blocksX + nbY, sh.blocksX + nbY + nDN, nParts};
     cudaError_t e;
     if ((e = cudaEventRecord(fork->fork, st)) != cudaSuccess) return e;
@@ -1562,7 +1609,7 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
     if ((e = cudaEventRecord(fork->fork2, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(fork->side, fork->fork2, 0)) != cudaSuccess) return e;
     const auto kdn = WSB_PICK(k_plainDN, P, sh2, ext);
-    kdn<<<sh2 ? sh.blocksDNS : sh.blocksDN, 256, 0, fork->side>>>(d, insts, ctl, pn, px, pe, nParts, counter, nB);
+    kdn<<<(sh2 ? sh.blocksDNS : sh.blocksDN) + xys, 256, 0, fork->side>>>(d, insts, ctl, pn, px, pe, nParts, counter, nB);
     if ((e = cudaEventRecord(fork->join2, fork->side)) != cudaSuccess) return e;
     const auto kdm = WSB_PICK(k_plainDM, P, sh2, ext);
     kdm<<<sh.blocksDM, 256, 0, st>>>(d, insts, ctl, pm, px, pe, nParts, counter, nB);
