@@ -903,27 +903,35 @@ __device__ __noinline__ void summariseElements(const A *partAll, int ex, int ey,
   }
 }
 // The close of a split iteration without the extensions: the summary row and the segment kernel's partials (rows
-// [en, em), one slot a warp), then the kinetic-damping decision.  The control block, the descriptor and the summary row
+// [en, em)) and, with NODES, the node kernel's partials (rows [ey, en)), one item a warp, then the kinetic-damping
+// decision.  The control block, the descriptor and the summary row
 // are copied to shared memory a word a thread, their loads in flight beside the partials'.
-template <class A>
+template <class A, bool NODES>
 __device__ __noinline__ void closeSplit(const InstDesc *__restrict__ insts, InstCtl *__restrict__ ctl, const A *partAll,
                                         int ey, int en, int em, int stride, const A *S, unsigned long long *counter) {
   __shared__ InstCtl sc;
   __shared__ InstDesc si;
-  __shared__ A vals[32], sS[RS_NSUM + RX_NMAX];
+  __shared__ A vals[8], sS[RS_NSUM + RX_NMAX];
   constexpr int NC = sizeof(InstCtl) / 4, ND = sizeof(InstDesc) / 4, NV = RS_NSUM + RX_NMAX;
   static_assert(NC <= 64 && 64 + ND <= 224 && NV <= 32, "the copies take one word a thread of a 256-thread block");
-  const int t = threadIdx.x;
+  // the items the close reduces, fixed at compile time (a warp each): the node rows [ey, en) feed the kinetic energy
+  // and the largest force and load, the segment rows [en, em) the kinetic energy and the largest torque
+  static_assert(updateSums(1, false) == (1u << RS_KE) && updateMaxs(1, false) == ((1u << RX_F) | (1u << RX_LOAD)) &&
+                updateSums(2, false) == (1u << RS_KE) && updateMaxs(2, false) == (1u << RX_T), "the close's items");
+  constexpr int NI = NODES ? 5 : 2;
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   int wc = 0, wd = 0;
   A ws = A(0);
   if (t < NC) wc = __ldcg(reinterpret_cast<const int *>(ctl) + t);
   if (t >= 64 && t < 64 + ND) wd = __ldg(reinterpret_cast<const int *>(insts) + (t - 64));
   if (t >= 224 && t < 224 + NV) ws = __ldcg(S + (t - 224));
-  // ey < 0: the summary covers the node rows too (the segment rows alone remain); else the node rows [ey, en) as well
-  const SlotRange r[2] = {{ey, en, updateSums(1, false), updateMaxs(1, false)}, {en, em, updateSums(2, false), updateMaxs(2, false)}};
-  const SlotRange *rr = ey < 0 ? r + 1 : r;
-  const int nr = ey < 0 ? 1 : 2;
-  slotsToVals(rr, nr, partAll, stride, vals);
+  if (warp < NI) {
+    const int k = NODES ? warp : warp + 3;          // 0-2 node items, 3-4 segment items
+    const bool seg = k >= 3, mx = k == 1 || k == 2 || k == 4;
+    const int slot = k == 1 ? RS_NSUM + RX_F : k == 2 ? RS_NSUM + RX_LOAD : k == 4 ? RS_NSUM + RX_T : RS_KE;
+    const A v = warpSlot(partAll, stride, slot, mx, A(0), seg ? en : ey, seg ? em : en);
+    if (lane == 0) vals[warp] = v;
+  }
   if (t < NC) reinterpret_cast<int *>(&sc)[t] = wc;
   if (t >= 64 && t < 64 + ND) reinterpret_cast<int *>(&si)[t - 64] = wd;
   if (t >= 224 && t < 224 + NV) sS[t - 224] = ws;
@@ -932,7 +940,16 @@ __device__ __noinline__ void closeSplit(const InstDesc *__restrict__ insts, Inst
     Part<A> q;
     for (int i = 0; i < RS_NSUM; i++) q.s[i] = sS[i];
     for (int i = 0; i < RX_NMAX; i++) q.x[i] = sS[RS_NSUM + i];
-    foldVals(rr, nr, vals, q);
+    if constexpr (NODES) {
+      q.s[RS_KE] += vals[0];
+      q.x[RX_F] = mmax(q.x[RX_F], vals[1]);
+      q.x[RX_LOAD] = mmax(q.x[RX_LOAD], vals[2]);
+      q.s[RS_KE] += vals[3];
+      q.x[RX_T] = mmax(q.x[RX_T], vals[4]);
+    } else {
+      q.s[RS_KE] += vals[0];
+      q.x[RX_T] = mmax(q.x[RX_T], vals[1]);
+    }
     InstCtl cc = sc;
     decide<false>(si, cc, q, 0);
     ctl[0] = cc;
@@ -990,7 +1007,7 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
       summariseElements<A>(partAll, pe.x, pe.y, partStride, S);
       if (threadIdx.x == 0) last = unsigned(ticketAdd(cnt, 1ull)) + 1u == nBlocks;
       __syncthreads();
-      if (last) closeSplit<A>(insts, ctl, partAll, pe.y, pe.n, pe.m, partStride, S, cnt);
+      if (last) closeSplit<A, true>(insts, ctl, partAll, pe.y, pe.n, pe.m, partStride, S, cnt);
       return;
     }
   const StepCtx sx = makeCtx<A>(I, c, EXT ? d.ext[I.utmIdx].pf : nullptr);
@@ -1015,7 +1032,7 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
     }
     __syncthreads();
     if (!last) return;
-    closeSplit<A>(insts, ctl, partAll, pe.y, pe.n, pe.m, partStride, S, cnt);
+    closeSplit<A, true>(insts, ctl, partAll, pe.y, pe.n, pe.m, partStride, S, cnt);
     return;
   }
   if constexpr (!EXT && PART != 0) {
@@ -1047,7 +1064,7 @@ __device__ __forceinline__ void plainD(const Dev<P> &d, const InstDesc *__restri
       __syncthreads();
       if (role != 2) return;
     }
-    closeSplit<A>(insts, ctl, partAll, -1, pe.n, pe.m, partStride, S, cnt);
+    closeSplit<A, false>(insts, ctl, partAll, 0, pe.n, pe.m, partStride, S, cnt);
     return;
   }
   if (threadIdx.x == 0) {
