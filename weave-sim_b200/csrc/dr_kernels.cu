@@ -124,6 +124,15 @@ __device__ __forceinline__ void rodElement(const Dev<P> &d, const InstDesc &I, c
   else if ((e -= I.m) < I.p) jointTorque<P>(d, sx.cur, I.p0 + e, pt);
   else clampTorque<P>(d, sx.cur, I.c0 + (e - I.p), pt);
 }
+// rod element pair e of the plain form's rod kernel: segment e and joint e (or, past the joints, clamp e − p) in one
+// thread, so the kernel runs half as many threads as rod elements and all of its blocks are resident beside the
+// crossing kernel's (its per-thread chain is two elements long, still shorter than a crossing side's)
+template <int P>
+__device__ __forceinline__ void rodPair(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, int e, Part<typename Dev<P>::A> &pt) {
+  if (e < I.m) segForce<P>(d, sx.cur, I.m0 + e, pt);
+  if (e < I.p) jointTorque<P>(d, sx.cur, I.p0 + e, pt);
+  else if (e - I.p < I.C) clampTorque<P>(d, sx.cur, I.c0 + (e - I.p), pt);
+}
 // crossing element e of phase A: two adjacent elements, one a side, per crossing
 template <int P, bool SHORT, bool EXT>
 __device__ __forceinline__ void crossElement(const Dev<P> &d, const InstDesc &I, const StepCtx &sx, int e, Part<typename Dev<P>::A> &pt) {
@@ -718,14 +727,14 @@ __device__ __forceinline__ void plainA(const Dev<P> &d, const InstDesc *__restri
   const InstCtl c = ctl[0];
   if (c.status != WS_RUNNING) return;
   const int nK = (I.contacts && I.K) ? I.K : 0;
-  const int nA = PART == 1 ? 2 * nK : PART == 2 ? I.m + I.p + I.C : countA(I);
+  const int nA = PART == 1 ? 2 * nK : PART == 2 ? max(I.m, I.p + I.C) : countA(I);
   const StepCtx sx = makeCtx<A>(I, c);
   Part<A> pt;
   pt.init();
   // each part compiles only its own element code (a branch the part never takes still costs registers)
   for (int e = blk * blockDim.x + threadIdx.x; e < nA; e += nblk * blockDim.x) {
     if (PART == 1) crossElement<P, SHORT, EXT>(d, I, sx, e, pt);
-    else if (PART == 2) rodElement<P>(d, I, sx, e, pt);
+    else if (PART == 2) rodPair<P>(d, I, sx, e, pt);
     else phaseA<P, SHORT, EXT>(d, I, sx, e, nK, pt);
   }
   constexpr unsigned SM = elemSums(PART), XM = elemMaxs(PART);
@@ -1601,8 +1610,9 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
   if (fork && contacts) {
     // crossings on a forked branch, segments / joints / clamps on the main one, joined before the update; the update
     // forks again: nodes on the side branch, segments and side ranks on the main one
-    // rod blocks of WSB_Y_THREADS(P): ceil(elements / 512) = ceil(blocksY / 2) (blocksY counts blocks of 256)
-    const int nbY = WSB_Y_THREADS(P) == 256 ? sh.blocksY : (sh.blocksY + 1) / 2;
+    // rod blocks of WSB_Y_THREADS(P) over the rod pairs: ceil(pairs / 512) = ceil(blocksYP / 2) (blocksYP counts
+    // blocks of 256)
+    const int nbY = WSB_Y_THREADS(P) == 256 ? sh.blocksYP : (sh.blocksYP + 1) / 2;
     const int nDN = sh2 ? sh.blocksDNS : sh.blocksDN, nParts = sh.blocksX + nbY + nDN + sh.blocksDM;
     A *px = static_cast<A *>(part), *py = px + sh.blocksX, *pn = py + nbY, *pm = pn + nDN;
     // without the extensions the node kernel runs one more block, which summarises the element partials
