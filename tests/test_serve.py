@@ -57,3 +57,44 @@ def test_results_equal_alone_and_in_the_mix():
         alone = s.download(0)
         s.dispose()
         assert np.array_equal(alone["X"], r.result["X"]) and np.array_equal(alone["u"], r.result["u"])
+
+
+def test_topology_key_separates_what_a_slot_cannot_take():
+    """requests share a pool only when ws_load_instance would accept one in the other's slot: same node, segment, joint,
+    crossing, strand and clamp counts; parameter variants keep their base's key"""
+    a, b = ws.configs.dome_stiff(seed=1), ws.configs.dome_stiff(seed=2)
+    assert serve.topology_key(a) == serve.topology_key(b)
+    small = ws.configs.dome_small(seed=1, side=3)
+    assert serve.topology_key(small) != serve.topology_key(a)
+    eq = {"X": a.X.copy(), "Q": a.Q.copy(), "u": a.cross_u.copy(), "nprev": a.cross_nprev.copy()}
+    assert serve.topology_key(serve.variant_of(a, eq, np.random.default_rng(0))) == serve.topology_key(a)
+    import cases
+    one = cases.straight(1000.0, 10, anchors=[((0, 0), ws.mask(1, 1, 1, 1, 1, 1))])
+    two = cases.straight(1000.0, 10, anchors=[((0, 0), ws.mask(1, 1, 1, 1, 1, 1)), ((0, 1), ws.mask(1, 1, 1, 1, 1, 1))])
+    pin = cases.straight(1000.0, 10, anchors=[((0, 0), ws.mask(1, 1, 1, 1, 1, 1)), ((0, 1), ws.mask(1, 1, 1, 0, 0, 0))])
+    assert serve.topology_key(one)[-1] == 1 and serve.topology_key(two)[-1] == 2 and serve.topology_key(pin)[-1] == 1
+
+
+@pytest.mark.gpu
+def test_mixed_topologies_served_from_their_pools():
+    """requests of two topologies in one stream: each gets a pool of its own within the budget, every request is
+    served, and each result is the same bits as the same model relaxed alone"""
+    if ws.device_count() < 1:
+        pytest.skip("no CUDA device")
+    tpl = ws.configs.dome_stiff(seed=1)
+    srv = serve.Server(tpl, slots=4, chunk=200)
+    reqs = serve.poisson_stream(400.0, 6, seed=3, fresh_cap=600)
+    small = [ws.configs.dome_small(seed=20 + i, side=3) for i in range(4)]
+    for i, md in enumerate(small):
+        md.params = dict(md.params, max_iter=600)
+        reqs.append(serve.Request(100 + i, reqs[i].arrival + 1e-4, md, "fresh", 600))
+    done = srv.run(reqs, time_limit=60)
+    assert len(srv.pools) == 2 and srv.slots == 8
+    assert len(done) == 10
+    srv.dispose()
+    for r in done:
+        s = ws.GpuSolver([r.model], precision="mixed", threads=256)
+        s.step(r.iters)
+        alone = s.download(0)
+        s.dispose()
+        assert np.array_equal(alone["X"], r.result["X"]) and np.array_equal(alone["u"], r.result["u"]), r.rid

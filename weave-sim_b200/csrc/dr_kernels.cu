@@ -1,5 +1,6 @@
 // sm_100a kernels of the DR step: the persistent batched form (one thread block per instance, every phase of every
 // iteration inside one launch) and the plain form (one kernel per phase, one instance, captured as a CUDA graph).
+#include <mutex>
 #include <algorithm>
 
 #include "dr_kernels.hpp"
@@ -1538,9 +1539,18 @@ cudaError_t residentPrepare(size_t bytes, bool shortSides, size_t *granted) {
     if (e != cudaSuccess) return e;
     if (bytes + fa.sharedSizeBytes > size_t(optin)) return cudaSuccess;
   }
+  // The attribute belongs to the kernel, not to a context: every context of the process launches the same kernel, so
+  // it is only ever raised (to the largest instance any context holds), under a lock; lowering it for a context of
+  // small instances would make another context's launches fail.
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
   for (int ex = 0; ex < 2; ex++) {
     const auto k = WSB_PICK(k_resident, P, shortSides, ex != 0);
-    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, k);
+    if (e != cudaSuccess) return e;
+    if (fa.maxDynamicSharedSizeBytes >= int(bytes)) continue;
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
     if (e != cudaSuccess) return e;
   }
   *granted = bytes;
