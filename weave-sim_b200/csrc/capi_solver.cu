@@ -1373,7 +1373,7 @@ int ws_create(const ws_model *const *models, int32_t n_instances, const ws_opts 
     c->shape.blocksX = blocks(2LL * I0.K, 128);
     c->shape.blocksXR = blocks(2LL * I0.K, 256);
     c->shape.blocksY = blocks(I0.m + I0.p + I0.C, 256);
-    c->shape.blocksYP = blocks(std::max<long long>(I0.m, (long long)I0.p + I0.C), 256);
+    c->shape.pairsY = std::max(1, std::max(I0.m, I0.p + I0.C));
     c->shape.blocksDN = blocks(I0.n, 256);
     c->shape.blocksDNS = blocks(I0.n + 2LL * I0.K, 256);
     c->shape.blocksDM = blocks(I0.m, 256);

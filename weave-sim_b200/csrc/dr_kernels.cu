@@ -19,9 +19,15 @@
 #endif
 // The rod kernel's block: 512 threads at 2 blocks per SM (64 registers) in the mixed and FP32 policies, which halves
 // its block partials against 256 × 4 at the same occupancy; 256 threads at 3 blocks per SM in FP64.
-#define WSB_Y_THREADS(P) ((P) == PREC_F64 ? 256 : 512)
+#ifndef WSB_Y_T_MIXED
+#define WSB_Y_T_MIXED 512
+#endif
+#define WSB_Y_THREADS(P) ((P) == PREC_F64 ? 256 : WSB_Y_T_MIXED)
 #ifndef WSB_MINB_Y
-#define WSB_MINB_Y(P) ((P) == PREC_F64 ? 3 : 2)
+#ifndef WSB_MINB_YM
+#define WSB_MINB_YM 2
+#endif
+#define WSB_MINB_Y(P) ((P) == PREC_F64 ? 3 : WSB_MINB_YM)
 #endif
 #ifndef WSB_MINB_XY
 #define WSB_MINB_XY 2
@@ -1620,9 +1626,8 @@ cudaError_t launchPlainIter(const Dev<P> &d, const InstDesc *insts, InstCtl *ctl
   if (fork && contacts) {
     // crossings on a forked branch, segments / joints / clamps on the main one, joined before the update; the update
     // forks again: nodes on the side branch, segments and side ranks on the main one
-    // rod blocks of WSB_Y_THREADS(P) over the rod pairs: ceil(pairs / 512) = ceil(blocksYP / 2) (blocksYP counts
-    // blocks of 256)
-    const int nbY = WSB_Y_THREADS(P) == 256 ? sh.blocksYP : (sh.blocksYP + 1) / 2;
+    // rod blocks of WSB_Y_THREADS(P) threads over the rod pairs, one pair a thread
+    const int nbY = std::min((sh.pairsY + WSB_Y_THREADS(P) - 1) / WSB_Y_THREADS(P), 148 * 8);
     const int nDN = sh2 ? sh.blocksDNS : sh.blocksDN, nParts = sh.blocksX + nbY + nDN + sh.blocksDM;
     A *px = static_cast<A *>(part), *py = px + sh.blocksX, *pn = py + nbY, *pm = pn + nDN;
     // without the extensions the node kernel runs one more block, which summarises the element partials

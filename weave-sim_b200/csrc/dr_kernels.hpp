@@ -9,8 +9,8 @@ namespace wsb {
 // blocks of the plain form's kernels: element phase, general side order, update phase (general order; with the side
 // ranks of the short-slide order); crossings, rods, nodes (with the side ranks) and segments of the split phases;
 // the crossing blocks of 256 threads in the launch with block roles
-// blocksYP: blocks of 256 threads over the rod kernel's pairs (segment e with joint or clamp e)
-struct PlainShape { int blocksA, blocksR, blocksD, blocksDS, blocksX, blocksY, blocksDN, blocksDNS, blocksDM, blocksXR, blocksYP; };
+// pairsY: the rod kernel's pairs (segment e with joint or clamp e), one a thread
+struct PlainShape { int blocksA, blocksR, blocksD, blocksDS, blocksX, blocksY, blocksDN, blocksDNS, blocksDM, blocksXR, pairsY; };
 // a second stream and events: the element phase forks into a crossing kernel on `side` and a rod kernel on the main
 // stream, joined before the update, which forks again into a node kernel on `side` and a segment kernel on the main
 // stream, joined at the end of the iteration
