@@ -182,6 +182,11 @@ def run_batch(count=512, iters=CAP, precision="mixed", threads=0, seed=4, wide_c
     create_s = time.perf_counter() - t0
     n_wide, cl = s.wide
     shape = s.shape
+    # an untimed first step (the first launches of a process cost about 1.5 s here), then every instance back to its
+    # start: the timed step relaxes the batch from iteration 0 as if it were the first
+    s.step(20, read=False)
+    for b, m in enumerate(models):
+        s.load_instance(b, m)
     ctl = s.step(iters)
     ms, nl = s.last_step_stats()
     dev_bytes = s.device_bytes
